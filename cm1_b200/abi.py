@@ -1,0 +1,67 @@
+"""ctypes mirror of include/cm1g.h (the library's C-ABI).
+
+The structures below are byte-for-byte the C structs of cm1g.h, so the same
+objects can be handed to libcm1g.so (the CUDA library) and, in the tests, to
+the CPU oracle, which shares the struct definitions.
+"""
+import ctypes as C
+
+CM1G_MAXQ = 8
+
+CM1G_OK = 0
+CM1G_ERR_ARG = -1
+CM1G_ERR_CUDA = -2
+CM1G_ERR_NOMEM = -3
+CM1G_ERR_NONFINITE = -4
+CM1G_ERR_UNSUPPORTED = -5
+CM1G_ERR_STATE = -6
+
+_P = C.POINTER(C.c_float)
+
+
+class Config(C.Structure):
+    """cm1g_config_t: globals of module `input` read by the large step."""
+    _fields_ = [
+        ("ni", C.c_int32), ("nj", C.c_int32), ("nk", C.c_int32), ("ngxy", C.c_int32),
+        ("dx", C.c_float), ("dy", C.c_float), ("dz", C.c_float),
+        ("wbc", C.c_int32), ("ebc", C.c_int32), ("sbc", C.c_int32), ("nbc", C.c_int32),
+        ("hadvordrs", C.c_int32), ("vadvordrs", C.c_int32),
+        ("hadvordrv", C.c_int32), ("vadvordrv", C.c_int32),
+        ("advwenos", C.c_int32), ("advwenov", C.c_int32), ("weno_order", C.c_int32),
+        ("nsound", C.c_int32), ("alph", C.c_float), ("kdiv", C.c_float),
+        ("imoist", C.c_int32), ("eqtset", C.c_int32), ("numq", C.c_int32), ("nqv", C.c_int32),
+        ("iptra", C.c_int32), ("npt", C.c_int32), ("pdtra", C.c_int32),
+        ("apmasscon", C.c_int32),
+        ("irbc", C.c_int32), ("cstar", C.c_float), ("roflux", C.c_int32),
+        ("smeps", C.c_float),
+        ("testcase", C.c_int32), ("psolver", C.c_int32), ("terrain_flag", C.c_int32),
+        ("axisymm", C.c_int32), ("icor", C.c_int32),
+        ("qmag", C.c_float * CM1G_MAXQ),
+    ]
+
+
+GRID_FIELDS = ["uh", "ruh", "uf", "ruf", "vh", "rvh", "vf", "rvf",
+               "mh", "rmh", "c1", "c2", "mf", "rmf",
+               "pi0", "rho0", "rr0", "rf0", "rrf0", "th0", "rth0",
+               "qv0", "qc0", "qi0", "prs0", "u0", "v0", "dtu0", "dtv0"]
+
+
+class Grid(C.Structure):
+    """cm1g_grid_t: grid metrics and base state (host pointers)."""
+    _fields_ = [(n, _P) for n in GRID_FIELDS]
+
+
+STATE_FIELDS = ["ua", "u3d", "uten1", "va", "v3d", "vten1", "wa", "w3d", "wten1",
+                "ppi", "pp3d", "ppx", "ppten", "tha", "th3d", "thten1", "rho", "prs",
+                "qa", "q3d", "qten", "pta", "pt3d", "ptten",
+                "radbcw", "radbce", "radbcs", "radbcn"]
+
+
+class State(C.Structure):
+    """cm1g_state_t: prognostic state and pre-RK tendencies."""
+    _fields_ = [(n, _P) for n in STATE_FIELDS]
+
+
+def fptr(addr):
+    """A float* from an integer address (host numpy data or device pointer)."""
+    return C.cast(C.c_void_p(int(addr)), _P)

@@ -1,0 +1,211 @@
+/*
+ * cm1g.h -- C-ABI of the B200 dynamical-core large step (libcm1g.so).
+ *
+ * The library advances CM1's dynamical core (RK3 large step, 5th-order /
+ * WENO5 advection, split-explicit acoustic substeps, boundary/halo fills)
+ * on one NVIDIA B200 (sm_100a).  Every entry point takes plain pointers
+ * and sizes; no C++ or torch types cross this boundary.
+ *
+ * Array layout: exactly the reference's Fortran layout (column-major, i
+ * fastest) with explicit lower bounds:
+ *   s-points  (ib:ie,   jb:je,   kb:ke)       ib=1-ngxy, ie=ni+ngxy, kb=0, ke=nk+1
+ *   u-points  (ib:ie+1, jb:je,   kb:ke)
+ *   v-points  (ib:ie,   jb:je+1, kb:ke)
+ *   w-points  (ib:ie,   jb:je,   kb:ke+1)
+ *   4-D q/tracer arrays are n consecutive s-point arrays.
+ * A pointer may address host or device memory; host arrays are staged
+ * through device buffers owned by the context (correct but slow: use device
+ * pointers for throughput).
+ *
+ * Errors: every entry point returns 0 on success and a negative CM1G_ERR_*
+ * code otherwise; cm1g_last_error() gives the message.  Nothing here calls
+ * exit() or stops the process (the reference calls stopcm1 instead).
+ *
+ * Threading: one host thread per context; calls are ordered on the
+ * context's CUDA stream.  Independent contexts may run concurrently.
+ */
+#ifndef CM1G_H
+#define CM1G_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CM1G_VERSION_MAJOR 0
+#define CM1G_VERSION_MINOR 1
+
+#define CM1G_OK              0
+#define CM1G_ERR_ARG        -1   /* bad argument / unsupported option          */
+#define CM1G_ERR_CUDA       -2   /* CUDA runtime error                          */
+#define CM1G_ERR_NOMEM      -3   /* device allocation failed                    */
+#define CM1G_ERR_NONFINITE  -4   /* NaN/Inf found by a host-side check          */
+#define CM1G_ERR_UNSUPPORTED -5  /* option of the reference not built here      */
+#define CM1G_ERR_STATE      -6   /* call out of order (e.g. before cm1g_init)   */
+
+#define CM1G_MAXQ 8
+
+/*
+ * Globals of the reference's module `input` (src/input.F:44-300) and
+ * `constants` (src/constants.F) that the large step reads.  The
+ * ISO_C_BINDING module fills this once after `param` has run.
+ */
+typedef struct cm1g_config {
+  int32_t ni, nj, nk;          /* physical cells (one rank: nx=ni, ny=nj, nz=nk) */
+  int32_t ngxy;                /* horizontal halo width; 3 for 5th order / WENO5  */
+  float   dx, dy, dz;          /* grid spacing (m)                                */
+  int32_t wbc, ebc, sbc, nbc;  /* lateral bc: 1 periodic, 2 open-radiative, 3 free-slip wall */
+  int32_t hadvordrs, vadvordrs;/* scalar advection order (5)                      */
+  int32_t hadvordrv, vadvordrv;/* momentum advection order (5)                    */
+  int32_t advwenos;            /* 0 none, 1 WENO every RK stage, 2 final stage   */
+  int32_t advwenov;            /* momentum WENO (0 only)                          */
+  int32_t weno_order;          /* 5                                               */
+  int32_t nsound;              /* acoustic steps per large step (even)            */
+  float   alph;                /* vertically implicit forward weight             */
+  float   kdiv;                /* divergence damping coefficient                 */
+  int32_t imoist;              /* 0 dry, 1 moist (water vapour only)             */
+  int32_t eqtset;              /* 1 or 2 (mass/energy-conserving)                 */
+  int32_t numq;                /* number of moisture arrays (1 = qv)              */
+  int32_t nqv;                 /* 1-based index of qv                             */
+  int32_t iptra;               /* passive tracers on/off                          */
+  int32_t npt;                 /* number of passive tracers                       */
+  int32_t pdtra;               /* positive-definite tracers                       */
+  int32_t apmasscon;           /* dry-air mass conservation fix (psolver 3)       */
+  int32_t irbc;                /* open-bc phase speed: 4 = Durran-Klemp           */
+  float   cstar;               /* open-bc phase speed for irbc=1,2                */
+  int32_t roflux;              /* restrict outward flux at open bcs (0 only)      */
+  float   smeps;               /* flush-to-zero threshold (1e-30)                 */
+  int32_t testcase;            /* selects the constants set (0 = CM1 defaults)    */
+  int32_t psolver;             /* 3 = Klemp-Wilhelmson split-explicit             */
+  int32_t terrain_flag;        /* 0 only                                          */
+  int32_t axisymm;             /* 0 only                                          */
+  int32_t icor;                /* 0 only                                          */
+  float   qmag[CM1G_MAXQ];     /* magnitude of each q (param.F), for WENO eps     */
+} cm1g_config_t;
+
+/*
+ * Grid metrics and base state (host pointers, Fortran layout), as passed to
+ * the reference's sound / adv* / solve2 subroutines.
+ */
+typedef struct cm1g_grid {
+  const float *uh, *ruh;       /* (ib:ie)     */
+  const float *uf, *ruf;       /* (ib:ie+1)   */
+  const float *vh, *rvh;       /* (jb:je)     */
+  const float *vf, *rvf;       /* (jb:je+1)   */
+  const float *mh, *rmh, *c1, *c2;           /* s-points */
+  const float *mf, *rmf;                     /* w-points */
+  const float *pi0, *rho0, *rr0, *rf0, *rrf0, *th0, *rth0;
+  const float *qv0, *qc0, *qi0, *prs0;       /* s-points */
+  const float *u0;             /* u-points    */
+  const float *v0;             /* v-points    */
+  const float *dtu0, *dtv0;    /* (ib:ie,jb:je) */
+} cm1g_grid_t;
+
+/*
+ * Prognostic state and the pre-RK tendencies of solve1 (the arrays solve2
+ * and solve3 read and write).  "a" arrays hold time t, "3d" arrays t+dt.
+ */
+typedef struct cm1g_state {
+  float *ua, *u3d, *uten1;     /* u-points */
+  float *va, *v3d, *vten1;     /* v-points */
+  float *wa, *w3d, *wten1;     /* w-points */
+  float *ppi, *pp3d, *ppx, *ppten;   /* s-points */
+  float *tha, *th3d, *thten1;        /* s-points */
+  float *rho, *prs;                  /* s-points */
+  float *qa, *q3d, *qten;            /* numq s-point arrays */
+  float *pta, *pt3d, *ptten;         /* npt  s-point arrays */
+  float *radbcw, *radbce;            /* (jb:je,kb:ke) */
+  float *radbcs, *radbcn;            /* (ib:ie,kb:ke) */
+} cm1g_state_t;
+
+typedef struct cm1g_ctx cm1g_ctx_t;
+
+const char *cm1g_last_error(void);
+int cm1g_version(int32_t *major, int32_t *minor);
+
+/* Context set-up (replaces the module globals set by param/base,
+ * src/param.F:10, src/base.F).  Copies the grid/base state to the device. */
+int cm1g_init(const cm1g_config_t *cfg, const cm1g_grid_t *grid, cm1g_ctx_t **ctx);
+int cm1g_finalize(cm1g_ctx_t *ctx);
+/* Order all work of the context on this cudaStream_t (NULL = legacy stream). */
+int cm1g_set_stream(cm1g_ctx_t *ctx, void *stream);
+/* Number of kernels this context has launched so far. */
+int cm1g_launch_count(cm1g_ctx_t *ctx, int64_t *count);
+
+/* RK3 large step: replaces solve2 (src/solve2.F:77-2097; rkloop 296-2052)
+ * for psolver=3, no terrain, no axisymmetry, no Coriolis.  mass1 is the
+ * initial dry-air mass (apmasscon); mass2 receives the new one.
+ * cflmax receives calccflquick's maximum Courant number (misclibs.F:2726). */
+int cm1g_solve2(cm1g_ctx_t *ctx, int32_t nstep, float dt, double mtime,
+                double mass1, double *mass2, float *cflmax, cm1g_state_t *st);
+
+/* Positive-definite column fix of one q array: replaces pdefq
+ * (src/misclibs.F:1037-1117) with pdscheme=1.  asq accumulates the budget. */
+int cm1g_pdefq(cm1g_ctx_t *ctx, float rmax, double *asq, const float *rho, float *q3d);
+
+/* End-of-step boundary fills, ppx update and rollover of the dynamical
+ * core: replaces the dycore part of solve3 (src/solve3.F:243-311, 540-640). */
+int cm1g_solve3(cm1g_ctx_t *ctx, cm1g_state_t *st);
+
+/* One complete large step as the reference's time loop runs it
+ * (cm1.F:3357 solve2, cm1.F:3414 pdefq for qv-only moisture, cm1.F:3432
+ * solve3).  With use_graph != 0 the step is captured once in a CUDA graph
+ * and replayed (device pointers only). */
+int cm1g_step(cm1g_ctx_t *ctx, int32_t nstep, float dt, double mtime,
+              double mass1, double *mass2, float *cflmax, cm1g_state_t *st,
+              int32_t use_graph);
+
+/* Lateral boundary fills: replace bcs, bcp, bcu, bcv, bcw
+ * (src/bc.F:180, 372, 528, 722, 942).  flag as in bcw (1: w=0 top/bottom). */
+int cm1g_bcs(cm1g_ctx_t *ctx, float *s);
+int cm1g_bcp(cm1g_ctx_t *ctx, float *p);
+int cm1g_bcu(cm1g_ctx_t *ctx, float *u);
+int cm1g_bcv(cm1g_ctx_t *ctx, float *v);
+int cm1g_bcw(cm1g_ctx_t *ctx, float *w, int32_t flag);
+
+/* Scalar advection tendency: replaces advs (src/adv.F:14-903) for
+ * hadvorder=vadvorder=5 / WENO5, no budgets, no diffusion.  Argument
+ * meaning follows adv.F:14-19: rru/rrv/rrw are the rho0-weighted fluxes,
+ * divx their divergence, s0 the RK base value, s the advected field,
+ * sten is incremented by the advective tendency (times rr0).  pdef selects
+ * the positive-definite limiter (pdef.F), pdefweno the pdef form of the
+ * vertical WENO (adv_routines.F:2359-2433).  All arrays device or host. */
+int cm1g_advs(cm1g_ctx_t *ctx, int32_t nrk, int32_t wflag,
+              const float *rru, const float *rrv, const float *rrw,
+              const float *divx, const float *s0, const float *s, float *sten,
+              int32_t pdef, int32_t pdefweno, float dt, double weps);
+
+/* Momentum advection tendencies: replaces advu, advv, advw (src/adv.F:911,
+ * 1847, 2778) with hadvordrv=vadvordrv=5: uten/vten/wten are incremented by
+ * the flux-form advection of u3d/v3d/w3d by rho0*(u,v,w). */
+int cm1g_advuvw(cm1g_ctx_t *ctx, int32_t nrk, const float *u3d, const float *v3d,
+                const float *w3d, float *uten, float *vten, float *wten);
+
+/* Acoustic substeps of one RK stage: replaces sound (src/sound.F:10-857)
+ * with psolver=3.  thv = theta_rho (t11), ppterm (t22), piadv (pi0+pp').
+ * On return rru/rrv/rrw hold the small-step-averaged velocities. */
+int cm1g_sound(cm1g_ctx_t *ctx, int32_t nrk, float dt, float dttmp,
+               float *ua, float *u3d, const float *uten,
+               float *va, float *v3d, const float *vten,
+               float *wa, float *w3d, const float *wten,
+               float *ppi, float *pp3d, const float *piadv, const float *ppten,
+               float *ppx, const float *thv, const float *ppterm,
+               float *rru, float *rrv, float *rrw,
+               float *radbcw, float *radbce, float *radbcs, float *radbcn);
+
+/* Domain-integrated dry-air mass, FP64 accumulation: replaces calcmass
+ * (src/misclibs.F:3134-3191).  tmass = sum(rho*dV). */
+int cm1g_calcmass(cm1g_ctx_t *ctx, const float *rho, double *tmass);
+
+/* Domain extrema over the physical cells of an s/u/v/w array: replaces
+ * maxmin (src/maxmin.F:5-119).  stag: 1 s, 2 u, 3 v, 4 w.  loc receives
+ * 1-based (i,j,k) of the max (loc[0..2]) and of the min (loc[3..5]). */
+int cm1g_maxmin(cm1g_ctx_t *ctx, const float *a, int32_t stag,
+                float *amax, float *amin, int32_t loc[6]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CM1G_H */
