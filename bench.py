@@ -1,0 +1,293 @@
+"""Benchmark of the CM1 dynamical-core large step on B200.
+
+Metric: grid-cell updates per second per RK3 large step (cells x steps / s),
+as an absolute number and as a fraction of the HBM roofline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload supercell]
+    python bench.py --impl reference ...     # CPU restatement on the host cores
+
+One "step" is one complete large step (solve2 + pdefq + solve3) of the
+workload; the default workload is the 256x256x80 moist supercell-scale case
+(WENO5 theta + 6 scalars, open-radiative boundaries, dt=3 s, nsound=8).
+`value` is device-resident throughput (state already in HBM, CUDA-graph
+replay); `e2e` runs the same step through the C-ABI with pinned host arrays,
+so every step includes the host->device copy of the state and the copy back.
+With N>1 ranks every GPU advances its own replica (ensemble-style weak
+scaling, no collective on the data path); timing is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+# algorithmic bytes per cell per large step, per substep of the acoustic kernel
+ACOUSTIC_FLOATS_PER_CELL = 23            # reads 15, writes 8 (u,v,w,pi',ppd + 3 averages)
+
+
+def nloop_total(nsound):
+    n1 = int(np.floor(nsound / 3.0 + 0.5))
+    dt = 1.0
+    if dt / (n1 * 3.0) > dt / nsound:
+        n1 += 1
+    return n1 + nsound // 2 + nsound
+
+
+def algorithmic_bytes_per_cell(cfg):
+    """B = 4 [3 (M + 3 + 4 N_adv + E) + 23 S + F] (floats per cell-step)."""
+    moist = cfg.imoist == 1
+    M = 16 if moist else 14
+    nadv = 1 + (cfg.numq if moist else 0) + (cfg.npt if cfg.iptra else 0)
+    E = 1 if (moist and cfg.eqtset == 2) else 0
+    F = 5 if moist else 4
+    S = nloop_total(cfg.nsound)
+    return 4 * (3 * (M + 3 + 4 * nadv + E) + ACOUSTIC_FLOATS_PER_CELL * S + F)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu, self.rows, self.stop = gpu, [], threading.Event()
+
+    def _run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.t.join(timeout=10)
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) > 8:
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def cpu_time_steps(case, nsteps):
+    """Oracle (CPU restatement) timed on the host cores."""
+    from oracle import oracle
+    st = case.copy_state()
+    oracle.step(case, st)          # warm caches and threads
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        st, _, _ = oracle.step(case, st)
+    return time.perf_counter() - t0, oracle.threads()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from cm1_b200.cases import make_case
+    case = make_case(args.workload)
+    cells = case.cfg.ni * case.cfg.nj * case.cfg.nk
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_time_steps(case, 0)
+    steps = max(1, min(args.steps, args.ref_steps))
+    sec, thr = cpu_time_steps(case, steps)
+    v = cells * steps / sec
+    line = {"impl": "reference", "metric": "cell-updates/s per RK3 large step", "value": v,
+            "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sec / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded, generated in-repo)",
+            "config": workload_config(case, args),
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": thr, "kind": "port",
+                             "sample": "%d full large steps of the %s workload, OpenMP on all host threads "
+                                       "(CPU restatement of the Fortran: no Fortran compiler on this image)"
+                                       % (steps, args.workload)},
+            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def workload_config(case, args):
+    c = case.cfg
+    return {"workload": args.workload, "grid": [c.ni, c.nj, c.nk], "dx_m": c.dx, "dz_m": c.dz, "dt_s": case.dt,
+            "nsound": c.nsound, "advwenos": c.advwenos, "moist": bool(c.imoist), "passive_tracers": c.npt if c.iptra else 0,
+            "lateral_bc": {1: "periodic", 2: "open-radiative"}[c.wbc], "l2": "inputs larger than L2 (no flush needed)",
+            "parallelism": "replicas" if args.gpus > 1 else "single"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="supercell")
+    ap.add_argument("--impl", default="cm1g")
+    ap.add_argument("--ref-steps", type=int, default=3)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    from cm1_b200.cases import make_case
+    from cm1_b200 import binding
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    case = make_case(args.workload, seed=1234 + rank)
+    cfg = case.cfg
+    cells = cfg.ni * cfg.nj * cfg.nk
+    ctx = binding.Context(cfg, case.grid)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    dev = binding.to_device(case.state)
+    torch.cuda.synchronize()
+
+    # ---- device-resident throughput (graph replay)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            ctx.step(dev, case.dt, case.mass1, use_graph=True)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    n0 = ctx.launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            ctx.step(dev, case.dt, case.mass1, use_graph=True)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = ctx.launches() - n0
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_step = ms / args.steps
+    value = world * cells * args.steps / (ms * 1e-3)
+
+    # ---- per-kernel device times (profiled pass, eager launches)
+    ctx.profile(True)
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            ctx.step(dev, case.dt, case.mass1, use_graph=False)
+    torch.cuda.synchronize()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    hbm, peak_kind = peaks()
+    n_snd, ms_snd = prof.get("k_sound_step", (1, float("nan")))
+    per_launch_ms = ms_snd / max(n_snd, 1)
+    bytes_launch = ACOUSTIC_FLOATS_PER_CELL * 4 * cells
+    achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
+    tot_prof = sum(v[1] for v in prof.values())
+    B = algorithmic_bytes_per_cell(cfg)
+    step_gbs = B * cells / (ms_step * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get("k_sound_step_bytes_per_launch_%s" % args.workload)
+        except Exception:
+            traffic = None
+
+    # ---- end-to-end through the C-ABI with pinned host arrays
+    host = {k: torch.from_numpy(v.copy()).pin_memory() for k, v in case.state.items()}
+    h2d = sum(v.numel() * 4 for v in host.values())
+    d2h = sum(v.numel() * 4 for k, v in host.items() if k not in ("uten1", "vten1", "wten1", "ppten", "thten1",
+                                                                    "qten", "ptten"))
+    e2e_steps = max(2, min(args.steps, 5))
+    with torch.cuda.stream(stream):
+        ctx.step(host, case.dt, case.mass1)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        ctx.step(host, case.dt, case.mass1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = world * cells * e2e_steps / (ms_e2e * 1e-3)
+
+    # ---- CPU baseline (rank 0, N=1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sec, thr = cpu_time_steps(case, args.cpu_steps)
+        cpu = {"value": cells * args.cpu_steps / sec, "unit": "cell-updates/s", "cores": thr, "kind": "port",
+               "sample": "%d full large steps of the %s workload on the host (CPU restatement, OpenMP)"
+                         % (args.cpu_steps, args.workload)}
+
+    if rank == 0:
+        line = {"metric": "cell-updates/s per RK3 large step", "value": value, "unit": "cell-updates/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded, generated in-repo)", "config": workload_config(case, args),
+                "roofline": {"bound": "hbm", "kernel": "k_sound_step", "achieved": achieved, "peak": hbm,
+                             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                             "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": per_launch_ms,
+                             "share_of_step": ms_snd / tot_prof if tot_prof else None},
+                "step_roofline": {"algorithmic_bytes_per_cell": B, "achieved_gbs": step_gbs, "frac": step_gbs / hbm,
+                                  "roofline_cell_updates_per_s": hbm * 1e9 / B},
+                "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+                "gpu_launches": launches, "clocks": clk.summary(),
+                "kernel_ms_per_step": {k: v[1] / 2 for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}}
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

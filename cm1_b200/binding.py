@@ -1,0 +1,197 @@
+"""ctypes/PyTorch binding of libcm1g.so.
+
+Python drivers (the role cm1/run.py plays for the reference) and training
+code use this module; it calls the C-ABI declared in include/cm1g.h.  There
+is no CPU fallback: if the library or a CUDA device is missing the calls
+raise.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from .abi import Config, Grid, State, STATE_FIELDS, fptr, CM1G_OK
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcm1g.so")
+_lib = None
+
+_P = C.POINTER(C.c_float)
+
+
+class CM1GError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("cm1g error %d: %s" % (code, msg))
+        self.code = code
+
+
+def lib():
+    """Load libcm1g.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libcm1g.so not built: run `python -m cm1_b200.build` (no CPU fallback exists)")
+    L = C.CDLL(LIB_PATH)
+    ctxp = C.c_void_p
+    cfgp, grp, stp = C.POINTER(Config), C.POINTER(Grid), C.POINTER(State)
+    L.cm1g_last_error.restype = C.c_char_p
+    L.cm1g_version.argtypes = [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    L.cm1g_init.argtypes = [cfgp, grp, C.POINTER(ctxp)]
+    L.cm1g_finalize.argtypes = [ctxp]
+    L.cm1g_set_stream.argtypes = [ctxp, C.c_void_p]
+    L.cm1g_launch_count.argtypes = [ctxp, C.POINTER(C.c_int64)]
+    L.cm1g_solve2.argtypes = [ctxp, C.c_int32, C.c_float, C.c_double, C.c_double, C.POINTER(C.c_double),
+                              C.POINTER(C.c_float), stp]
+    L.cm1g_step.argtypes = L.cm1g_solve2.argtypes + [C.c_int32]
+    L.cm1g_solve3.argtypes = [ctxp, stp]
+    L.cm1g_pdefq.argtypes = [ctxp, C.c_float, C.POINTER(C.c_double), _P, _P]
+    for n in ("cm1g_bcs", "cm1g_bcp", "cm1g_bcu", "cm1g_bcv"):
+        getattr(L, n).argtypes = [ctxp, _P]
+    L.cm1g_bcw.argtypes = [ctxp, _P, C.c_int32]
+    L.cm1g_advs.argtypes = [ctxp, C.c_int32, C.c_int32, _P, _P, _P, _P, _P, _P, _P, C.c_int32, C.c_int32,
+                            C.c_float, C.c_double]
+    L.cm1g_advuvw.argtypes = [ctxp, C.c_int32, _P, _P, _P, _P, _P, _P]
+    L.cm1g_sound.argtypes = [ctxp, C.c_int32, C.c_float, C.c_float] + [_P] * 23
+    L.cm1g_calcmass.argtypes = [ctxp, _P, C.POINTER(C.c_double)]
+    L.cm1g_maxmin.argtypes = [ctxp, _P, C.c_int32, _P, _P, C.POINTER(C.c_int32)]
+    L.cm1g_profile.argtypes = [ctxp, C.c_int32]
+    L.cm1g_profile_read.argtypes = [ctxp, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(C.c_int64),
+                                    C.POINTER(C.c_double)]
+    _lib = L
+    return L
+
+
+def check(rc):
+    if rc != CM1G_OK:
+        raise CM1GError(rc, lib().cm1g_last_error().decode())
+    return rc
+
+
+def ptr(a):
+    """float* of a numpy array or a torch tensor (host or CUDA)."""
+    if a is None:
+        return C.cast(None, _P)
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(_P)
+    return fptr(a.data_ptr())
+
+
+class Context:
+    """A cm1g context for one grid (cm1g_init / cm1g_finalize)."""
+
+    def __init__(self, cfg, grid_arrays):
+        L = lib()
+        self._grid_arrays = grid_arrays
+        g = Grid()
+        for n, a in grid_arrays.items():
+            setattr(g, n, ptr(a))
+        self.cfg = cfg
+        h = C.c_void_p()
+        check(L.cm1g_init(C.byref(cfg), C.byref(g), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cm1g_finalize(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle):
+        check(lib().cm1g_set_stream(self.h, C.c_void_p(int(stream_handle))))
+
+    def launches(self):
+        n = C.c_int64()
+        check(lib().cm1g_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    @staticmethod
+    def state_struct(arrays):
+        s = State()
+        for n in STATE_FIELDS:
+            a = arrays.get(n)
+            empty = a is None or (a.numel() == 0 if hasattr(a, "numel") else a.size == 0)
+            setattr(s, n, C.cast(None, _P) if empty else ptr(a))
+        return s
+
+    def step(self, state, dt, mass1, use_graph=False, solve2_only=False, nstep=0, mtime=0.0):
+        """One large step on `state` (dict of torch CUDA tensors or numpy
+        arrays).  Returns (mass2, cflmax)."""
+        s = state if isinstance(state, State) else self.state_struct(state)
+        m2, cfl = C.c_double(), C.c_float()
+        L = lib()
+        if solve2_only:
+            check(L.cm1g_solve2(self.h, nstep, dt, mtime, mass1, C.byref(m2), C.byref(cfl), C.byref(s)))
+        else:
+            check(L.cm1g_step(self.h, nstep, dt, mtime, mass1, C.byref(m2), C.byref(cfl), C.byref(s),
+                              1 if use_graph else 0))
+        return m2.value, cfl.value
+
+    def solve3(self, state):
+        s = state if isinstance(state, State) else self.state_struct(state)
+        check(lib().cm1g_solve3(self.h, C.byref(s)))
+
+    def bc(self, which, a, flag=1):
+        L = lib()
+        f = {"s": L.cm1g_bcs, "p": L.cm1g_bcp, "u": L.cm1g_bcu, "v": L.cm1g_bcv}
+        if which == "w":
+            check(L.cm1g_bcw(self.h, ptr(a), flag))
+        else:
+            check(f[which](self.h, ptr(a)))
+
+    def advs(self, nrk, wflag, rru, rrv, rrw, divx, s0, s, sten, pdef, pdefweno, dt, weps):
+        check(lib().cm1g_advs(self.h, nrk, wflag, ptr(rru), ptr(rrv), ptr(rrw), ptr(divx), ptr(s0), ptr(s),
+                              ptr(sten), pdef, pdefweno, dt, weps))
+
+    def advuvw(self, nrk, u, v, w, uten, vten, wten):
+        check(lib().cm1g_advuvw(self.h, nrk, ptr(u), ptr(v), ptr(w), ptr(uten), ptr(vten), ptr(wten)))
+
+    def sound(self, nrk, dt, dttmp, **a):
+        names = ["ua", "u3d", "uten", "va", "v3d", "vten", "wa", "w3d", "wten", "ppi", "pp3d", "piadv", "ppten",
+                 "ppx", "thv", "ppterm", "rru", "rrv", "rrw", "radbcw", "radbce", "radbcs", "radbcn"]
+        check(lib().cm1g_sound(self.h, nrk, dt, dttmp, *[ptr(a[n]) for n in names]))
+
+    def pdefq(self, rmax, rho, q):
+        asq = C.c_double(0.0)
+        check(lib().cm1g_pdefq(self.h, rmax, C.byref(asq), ptr(rho), ptr(q)))
+        return asq.value
+
+    def calcmass(self, rho):
+        t = C.c_double()
+        check(lib().cm1g_calcmass(self.h, ptr(rho), C.byref(t)))
+        return t.value
+
+    def maxmin(self, a, stag):
+        mx, mn = C.c_float(), C.c_float()
+        loc = (C.c_int32 * 6)()
+        check(lib().cm1g_maxmin(self.h, ptr(a), stag, C.byref(mx), C.byref(mn), loc))
+        return mx.value, mn.value, tuple(loc)
+
+    def profile(self, enable):
+        check(lib().cm1g_profile(self.h, 1 if enable else 0))
+
+    def profile_read(self):
+        """{kernel: (launches, total_ms)} collected since profiling was enabled."""
+        L = lib()
+        out = {}
+        buf = C.create_string_buffer(64)
+        n, ms = C.c_int64(), C.c_double()
+        i = 0
+        while L.cm1g_profile_read(self.h, i, buf, 64, C.byref(n), C.byref(ms)) == CM1G_OK:
+            out[buf.value.decode()] = (n.value, ms.value)
+            i += 1
+        return out
+
+
+def to_device(arrays, device="cuda"):
+    import torch
+    return {k: torch.from_numpy(np.ascontiguousarray(v)).to(device) for k, v in arrays.items()}
+
+
+def to_host(arrays):
+    return {k: v.detach().cpu().numpy() for k, v in arrays.items()}

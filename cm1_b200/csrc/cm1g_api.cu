@@ -1,0 +1,786 @@
+// cm1g_api.cu -- the C-ABI of libcm1g.so: context, device buffers, host
+// staging, the RK3 orchestration of solve2 and the end-of-step solve3 work.
+//
+// The context holds the grid descriptor, the vertical profiles on the
+// device and every scratch array of the large step.  A large step is a fixed
+// sequence of kernel launches on the context's stream, so cm1g_step can
+// capture it once in a CUDA graph and replay it.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cstdarg>
+#include <cmath>
+#include <vector>
+#include <string>
+#include "cm1g_common.cuh"
+#include "../../include/cm1g.h"
+
+namespace cm1g {
+void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, int64_t *nlaunch);
+void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w, const float *uten1,
+                         const float *vten1, const float *wten1, float *uten, float *vten, float *wten,
+                         const float *th3d, const float *qv, cudaStream_t st, int64_t *nl);
+void launch_advs(const DGrid &g, const float *rru, const float *rrv, const float *rrw, int weighted,
+                 const float *divx, const float *s, const float *s0, int sadd, const float *ten1,
+                 const float *thterm, float *sten_out, float *snew, int weno, int pdef, int pdefweno,
+                 double weps, float dt, int flush, float *scratch, cudaStream_t st, int64_t *nl);
+void launch_sound(const DGrid &g, int nsound, int nrk, float dt, const float *ua, float *u3d, const float *uten,
+                  const float *va, float *v3d, const float *vten, const float *wa, float *w3d, const float *wten,
+                  const float *ppi, float *pp3d, const float *piadv, const float *ppten, float *ppx,
+                  const float *thv, const float *ppterm, float *rru, float *rrv, float *rrw, const float *radbcw,
+                  const float *radbce, const float *radbcs, const float *radbcn, float *su, float *sv, float *d1,
+                  float *d2, cudaStream_t st, int64_t *nl);
+void launch_stage_prep(const DGrid &g, const float *th3d, const float *pp3d, const float *qv, int imoist, int eqtset,
+                       float *t11, float *t22, float *thterm, float *piadv, cudaStream_t st, int64_t *nl);
+void launch_radbc4(const DGrid &g, const float *ua, const float *u3d, const float *va, const float *v3d,
+                   float *rw, float *re, float *rs, float *rn, float dt, cudaStream_t st, int64_t *nl);
+int prs_nchunk(const DGrid &g);
+void launch_prs_rho(const DGrid &g, const float *pp3d, const float *th3d, const float *qv, int imoist,
+                    float *prs, float *rho, double *part3, double *part4, int do_sums, cudaStream_t st, int64_t *nl);
+void launch_masscon(const DGrid &g, float *pp3d, const float *th3d, const float *qv, int imoist, float *prs,
+                    float *rho, const double *part3, const double *part4, double mass1, double *dev, float *devf,
+                    cudaStream_t st, int64_t *nl);
+void launch_cfl(const DGrid &g, const float *u, const float *v, const float *w, float dt, int *out,
+                cudaStream_t st, int64_t *nl);
+void launch_pdefq(const DGrid &g, float rmax, const float *rho, float *q, double *bud, double *asq,
+                  cudaStream_t st, int64_t *nl);
+void launch_ppx_update(const DGrid &g, const float *pp3d, float *ppx, cudaStream_t st, int64_t *nl);
+void launch_copy_range(const DGrid &g, int stag, int ilo, int ihi, int jlo, int jhi, const float *src, float *dst,
+                       cudaStream_t st, int64_t *nl);
+void launch_level_mass(const DGrid &g, const float *rho, double *lev, cudaStream_t st, int64_t *nl);
+void launch_maxmin(const DGrid &g, const float *a, int stag, unsigned long long *om, cudaStream_t st, int64_t *nl);
+}  // namespace cm1g
+
+using namespace cm1g;
+
+// ---------------------------------------------------------------------
+// kernel timing (cm1g_profile)
+// ---------------------------------------------------------------------
+namespace cm1g {
+struct Profile {
+  struct Pending { std::string name; cudaEvent_t a, b; };
+  std::vector<Pending> pending;
+  std::vector<std::string> names;
+  std::vector<int64_t> count;
+  std::vector<double> ms;
+  void drain() {
+    for (auto &p : pending) {
+      float t = 0.f;
+      cudaEventSynchronize(p.b);
+      cudaEventElapsedTime(&t, p.a, p.b);
+      size_t i = 0;
+      while (i < names.size() && names[i] != p.name) i++;
+      if (i == names.size()) { names.push_back(p.name); count.push_back(0); ms.push_back(0.0); }
+      count[i] += 1;
+      ms[i] += t;
+      cudaEventDestroy(p.a);
+      cudaEventDestroy(p.b);
+    }
+    pending.clear();
+  }
+};
+thread_local Profile *g_profile = nullptr;
+void prof_record(const char *name, cudaStream_t st, bool begin) {
+  Profile *p = g_profile;
+  if (begin) {
+    Profile::Pending e;
+    e.name = name;
+    cudaEventCreate(&e.a);
+    cudaEventCreate(&e.b);
+    cudaEventRecord(e.a, st);
+    p->pending.push_back(e);
+  } else {
+    cudaEventRecord(p->pending.back().b, st);
+  }
+}
+}  // namespace cm1g
+
+static thread_local char g_errbuf[512] = "";
+
+static int set_err(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_errbuf, sizeof g_errbuf, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CUCHK(x)                                                                                   \
+  do {                                                                                             \
+    cudaError_t e_ = (x);                                                                          \
+    if (e_ != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_));    \
+  } while (0)
+
+struct cm1g_ctx {
+  cm1g_config_t cfg;
+  DGrid g;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int64_t nlaunch = 0;
+  std::vector<void *> allocs;
+  // scratch
+  float *t11 = nullptr, *t22 = nullptr, *thterm = nullptr, *piadv = nullptr;
+  float *uten = nullptr, *vten = nullptr, *wten = nullptr;
+  float *rru = nullptr, *rrv = nullptr, *rrw = nullptr;
+  float *su = nullptr, *sv = nullptr, *d1 = nullptr, *d2 = nullptr;
+  float *sx[2 * (1 + 2 * CM1G_MAXQ)] = {};   // per-scalar stage buffers
+  float *pdefscr = nullptr;                   // 6 s-arrays
+  float *sten = nullptr;                      // s-array for cm1g_advs-free use
+  double *part3 = nullptr, *part4 = nullptr, *dscal = nullptr, *bud = nullptr, *lev = nullptr;
+  float *fscal = nullptr;
+  int *cflbits = nullptr;
+  unsigned long long *mm = nullptr;
+  // host staging (for host-pointer calls)
+  cm1g_state_t dst{};
+  bool dst_ready = false;
+  std::vector<std::pair<float *, size_t>> stage_pool;
+  // graph
+  cudaGraphExec_t gexec = nullptr;
+  cudaGraph_t graph = nullptr;
+  cm1g_state_t gstate{};
+  float gdt = 0.f;
+  double gmass1 = 0.0;
+  int64_t graph_nodes = 0;
+  Profile *prof = nullptr;
+};
+
+// Makes the context's profile (if any) the active one for the calling thread.
+struct ProfActive {
+  Profile *saved;
+  explicit ProfActive(cm1g_ctx *c) : saved(g_profile) { g_profile = c->prof; }
+  ~ProfActive() { g_profile = saved; }
+};
+
+static void *dalloc(cm1g_ctx *c, size_t bytes) {
+  void *p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+  cudaMemset(p, 0, bytes);
+  c->allocs.push_back(p);
+  return p;
+}
+
+static bool is_device_ptr(const void *p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+static void set_constants_(int testcase, Consts *c) {
+  // constants.F:65-175 (same binary32 arithmetic as the Fortran)
+  if (testcase == 4) { c->g = 9.81f; c->rd = 287.0f; c->cp = 1015.0f; c->cpv = 1870.0f; }
+  else if (testcase == 5) { c->g = 9.81f; c->rd = 287.0f; c->cp = 1004.0f; c->cpv = 1870.0f; }
+  else { c->g = 9.81f; c->rd = 287.04f; c->cp = 1005.7f; c->cpv = 1870.0f; }
+  c->rv = 461.5f;
+  c->cv = c->cp - c->rd;
+  c->cvv = c->cpv - c->rv;
+  c->rovcp = c->rd / c->cp;
+  c->rddcv = c->rd / c->cv;
+  c->cpdrd = c->cp / c->rd;
+  c->reps = c->rv / c->rd;
+  c->repsm1 = c->rv / c->rd - 1.0f;
+  c->cpl = 4190.0f;
+  c->cpi = 2106.0f;
+}
+
+extern "C" const char *cm1g_last_error(void) { return g_errbuf; }
+
+extern "C" int cm1g_version(int32_t *major, int32_t *minor) {
+  if (major) *major = CM1G_VERSION_MAJOR;
+  if (minor) *minor = CM1G_VERSION_MINOR;
+  return CM1G_OK;
+}
+
+static int check_config(const cm1g_config_t *c) {
+  if (c->ni < 4 || c->nj < 4 || c->nk < 6) return set_err(CM1G_ERR_ARG, "grid too small (ni,nj>=4, nk>=6)");
+  if (c->ngxy < 3) return set_err(CM1G_ERR_ARG, "ngxy must be >= 3 for 5th order");
+  if (c->psolver != 3) return set_err(CM1G_ERR_UNSUPPORTED, "psolver=%d: only 3 (sound.F) is built", c->psolver);
+  if (c->terrain_flag || c->axisymm || c->icor)
+    return set_err(CM1G_ERR_UNSUPPORTED, "terrain, axisymmetric grids and Coriolis are not built");
+  if (c->hadvordrs != 5 || c->vadvordrs != 5 || c->hadvordrv != 5 || c->vadvordrv != 5)
+    return set_err(CM1G_ERR_UNSUPPORTED, "only 5th-order advection is built");
+  if (c->advwenov != 0) return set_err(CM1G_ERR_UNSUPPORTED, "momentum WENO is not built");
+  if (c->advwenos && c->weno_order != 5) return set_err(CM1G_ERR_UNSUPPORTED, "only WENO5 is built");
+  if (c->nsound < 2 || (c->nsound % 2)) return set_err(CM1G_ERR_ARG, "nsound must be even and >= 2");
+  if (c->imoist && (c->numq != 1 || c->nqv != 1))
+    return set_err(CM1G_ERR_UNSUPPORTED, "moisture: water vapour only (numq=1, nqv=1)");
+  if (c->iptra && (c->npt < 0 || c->npt > CM1G_MAXQ)) return set_err(CM1G_ERR_ARG, "npt out of range");
+  if (c->roflux != 0) return set_err(CM1G_ERR_UNSUPPORTED, "roflux=1 is not built");
+  bool open = c->wbc == 2 || c->ebc == 2 || c->sbc == 2 || c->nbc == 2;
+  if (open && c->irbc != 4) return set_err(CM1G_ERR_UNSUPPORTED, "open boundaries need irbc=4");
+  for (int b : {c->wbc, c->ebc, c->sbc, c->nbc})
+    if (b < 1 || b > 4) return set_err(CM1G_ERR_ARG, "lateral bc must be 1..4");
+  if ((c->wbc == 1) != (c->ebc == 1) || (c->sbc == 1) != (c->nbc == 1))
+    return set_err(CM1G_ERR_ARG, "periodic bc must be set on both sides");
+  return CM1G_OK;
+}
+
+// A 3-D base-state array is horizontally uniform without terrain; return its
+// (1,1,k) column, after checking the whole array agrees with it.
+static bool column_of(const float *a, const DGrid &g, int nkk, std::vector<float> &out) {
+  out.resize(nkk);
+  long plane = (long)g.NI * g.NJ;
+  for (int k = 0; k < nkk; k++) {
+    float v = a[iS(g, 1, 1, k)];
+    out[k] = v;
+    const float *p = a + plane * k;
+    for (long t = 0; t < plane; t++)
+      if (!(p[t] == v)) return false;
+  }
+  return true;
+}
+
+extern "C" int cm1g_init(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_ctx_t **out) {
+  if (!cfg || !gr || !out) return set_err(CM1G_ERR_ARG, "null argument");
+  int rc = check_config(cfg);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_err(CM1G_ERR_CUDA, "no CUDA device: the library has no CPU path");
+  cm1g_ctx *c = new cm1g_ctx();
+  c->cfg = *cfg;
+  cudaGetDevice(&c->device);
+  DGrid &g = c->g;
+  memset(&g, 0, sizeof g);
+  g.ni = cfg->ni; g.nj = cfg->nj; g.nk = cfg->nk; g.ngxy = cfg->ngxy;
+  g.ib = 1 - g.ngxy; g.jb = 1 - g.ngxy;
+  g.NI = g.ni + 2 * g.ngxy; g.NJ = g.nj + 2 * g.ngxy; g.NK = g.nk + 2;
+  g.dx = cfg->dx; g.dy = cfg->dy; g.dz = cfg->dz;
+  g.rdx = 1.0f / cfg->dx; g.rdy = 1.0f / cfg->dy; g.rdz = 1.0f / cfg->dz;
+  g.wbc = cfg->wbc; g.ebc = cfg->ebc; g.sbc = cfg->sbc; g.nbc = cfg->nbc;
+  g.ibw = cfg->wbc != 1; g.ibe = cfg->ebc != 1; g.ibs = cfg->sbc != 1; g.ibn = cfg->nbc != 1;
+  g.smeps = cfg->smeps; g.alph = cfg->alph; g.kdiv = cfg->kdiv;
+  set_constants_(cfg->testcase, &g.c);
+
+  // vertical profiles from the 3-D base state
+  struct { const float *src; const float **dst; int nkk; } prof[] = {
+      {gr->mh, &g.mh, g.NK}, {gr->rmh, &g.rmh, g.NK}, {gr->mf, &g.mf, g.NK + 1}, {gr->rho0, &g.rho0, g.NK},
+      {gr->rr0, &g.rr0, g.NK}, {gr->rf0, &g.rf0, g.NK}, {gr->rrf0, &g.rrf0, g.NK}, {gr->c1, &g.c1, g.NK},
+      {gr->c2, &g.c2, g.NK}, {gr->pi0, &g.pi0, g.NK}, {gr->th0, &g.th0, g.NK}, {gr->rth0, &g.rth0, g.NK},
+      {gr->qv0, &g.qv0, g.NK}, {gr->qc0, &g.qc0, g.NK}, {gr->qi0, &g.qi0, g.NK}};
+  std::vector<float> col;
+  for (auto &p : prof) {
+    if (!p.src) { cm1g_finalize(c); return set_err(CM1G_ERR_ARG, "grid array missing"); }
+    if (!column_of(p.src, g, p.nkk, col)) {
+      cm1g_finalize(c);
+      return set_err(CM1G_ERR_UNSUPPORTED, "base state/metric varies horizontally (terrain is not built)");
+    }
+    col.resize(g.NK + 2, col.back());
+    float *d = (float *)dalloc(c, col.size() * sizeof(float));
+    if (!d) { cm1g_finalize(c); return set_err(CM1G_ERR_NOMEM, "profile alloc"); }
+    cudaMemcpy(d, col.data(), col.size() * sizeof(float), cudaMemcpyHostToDevice);
+    *p.dst = d;
+  }
+  struct { const float *src; const float **dst; size_t n; } h1[] = {
+      {gr->uh, &g.uh, (size_t)g.NI}, {gr->ruh, &g.ruh, (size_t)g.NI}, {gr->uf, &g.uf, (size_t)g.NI + 1},
+      {gr->ruf, &g.ruf, (size_t)g.NI + 1}, {gr->vh, &g.vh, (size_t)g.NJ}, {gr->rvh, &g.rvh, (size_t)g.NJ},
+      {gr->vf, &g.vf, (size_t)g.NJ + 1}, {gr->rvf, &g.rvf, (size_t)g.NJ + 1},
+      {gr->dtu0, &g.dtu0, (size_t)g.NI * g.NJ}, {gr->dtv0, &g.dtv0, (size_t)g.NI * g.NJ}};
+  for (auto &p : h1) {
+    if (!p.src) { cm1g_finalize(c); return set_err(CM1G_ERR_ARG, "grid array missing"); }
+    float *d = (float *)dalloc(c, (p.n + 4) * sizeof(float));
+    if (!d) { cm1g_finalize(c); return set_err(CM1G_ERR_NOMEM, "metric alloc"); }
+    cudaMemcpy(d, p.src, p.n * sizeof(float), cudaMemcpyHostToDevice);
+    *p.dst = d;
+  }
+  // scratch arrays
+  const size_t bS = nS(g) * sizeof(float), bU = nU(g) * sizeof(float), bV = nV(g) * sizeof(float),
+               bW = nW(g) * sizeof(float);
+  c->t11 = (float *)dalloc(c, bS); c->t22 = (float *)dalloc(c, bS); c->thterm = (float *)dalloc(c, bS);
+  c->piadv = (float *)dalloc(c, bS);
+  c->uten = (float *)dalloc(c, bU); c->vten = (float *)dalloc(c, bV); c->wten = (float *)dalloc(c, bW);
+  c->rru = (float *)dalloc(c, bU); c->rrv = (float *)dalloc(c, bV); c->rrw = (float *)dalloc(c, bW);
+  c->su = (float *)dalloc(c, bU); c->sv = (float *)dalloc(c, bV);
+  c->d1 = (float *)dalloc(c, bS); c->d2 = (float *)dalloc(c, bS);
+  int nsc = 1 + (cfg->imoist ? cfg->numq : 0) + (cfg->iptra ? cfg->npt : 0);
+  for (int s = 0; s < 2 * nsc; s++) c->sx[s] = (float *)dalloc(c, bS);
+  bool pdef_needed = cfg->imoist || (cfg->iptra && cfg->pdtra);
+  c->pdefscr = (float *)dalloc(c, (pdef_needed ? 6 : 6) * bS);
+  c->sten = (float *)dalloc(c, bS);
+  int nchunk = prs_nchunk(g);
+  c->part3 = (double *)dalloc(c, (size_t)(g.nk + 2) * nchunk * sizeof(double));
+  c->part4 = (double *)dalloc(c, (size_t)(g.nk + 2) * nchunk * sizeof(double));
+  c->dscal = (double *)dalloc(c, 16 * sizeof(double));
+  c->bud = (double *)dalloc(c, (size_t)g.ni * g.nj * sizeof(double));
+  c->lev = (double *)dalloc(c, (size_t)(g.nk + 2) * sizeof(double));
+  c->fscal = (float *)dalloc(c, 16 * sizeof(float));
+  c->cflbits = (int *)dalloc(c, 16 * sizeof(int));
+  c->mm = (unsigned long long *)dalloc(c, 4 * sizeof(unsigned long long));
+  for (void *p : c->allocs)
+    if (!p) { cm1g_finalize(c); return set_err(CM1G_ERR_NOMEM, "scratch alloc"); }
+  if (!c->mm) { cm1g_finalize(c); return set_err(CM1G_ERR_NOMEM, "scratch alloc"); }
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cm1g_finalize(c);
+    return set_err(CM1G_ERR_CUDA, "stream create");
+  }
+  c->own_stream = true;
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) { cm1g_finalize(c); return set_err(CM1G_ERR_CUDA, "init: %s", cudaGetErrorString(e)); }
+  *out = c;
+  return CM1G_OK;
+}
+
+static void drop_graph(cm1g_ctx *c) {
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  if (c->graph) cudaGraphDestroy(c->graph);
+  c->gexec = nullptr; c->graph = nullptr;
+}
+
+extern "C" int cm1g_finalize(cm1g_ctx_t *c) {
+  if (!c) return CM1G_OK;
+  drop_graph(c);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->prof) { c->prof->drain(); delete c->prof; }
+  for (void *p : c->allocs) if (p) cudaFree(p);
+  for (auto &b : c->stage_pool) cudaFree(b.first);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_set_stream(cm1g_ctx_t *c, void *stream) {
+  if (!c) return set_err(CM1G_ERR_STATE, "null context");
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  c->stream = (cudaStream_t)stream;
+  c->own_stream = false;
+  drop_graph(c);
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_launch_count(cm1g_ctx_t *c, int64_t *count) {
+  if (!c || !count) return set_err(CM1G_ERR_ARG, "null argument");
+  *count = c->nlaunch;
+  return CM1G_OK;
+}
+
+// ---------------------------------------------------------------------
+// Host staging: arrays given as host pointers go through device buffers.
+// ---------------------------------------------------------------------
+struct Stager {
+  cm1g_ctx *c;
+  struct Item { float *host; float *dev; size_t n; bool out; };
+  std::vector<Item> items;
+  size_t pool_i = 0;
+  int err = 0;
+  explicit Stager(cm1g_ctx *cc) : c(cc) {}
+  float *dev_buffer(size_t n) {
+    if (pool_i < c->stage_pool.size() && c->stage_pool[pool_i].second >= n) return c->stage_pool[pool_i++].first;
+    float *p = nullptr;
+    if (cudaMalloc(&p, n * sizeof(float)) != cudaSuccess) { err = 1; return nullptr; }
+    if (pool_i < c->stage_pool.size()) { cudaFree(c->stage_pool[pool_i].first); c->stage_pool[pool_i] = {p, n}; }
+    else c->stage_pool.push_back({p, n});
+    pool_i++;
+    return p;
+  }
+  // returns a device pointer for p (n floats); copies in; remembers copy-out
+  float *in(const float *p, size_t n, bool out) {
+    if (!p || n == 0) return const_cast<float *>(p);
+    if (is_device_ptr(p)) return const_cast<float *>(p);
+    float *d = dev_buffer(n);
+    if (!d) return nullptr;
+    cudaMemcpyAsync(d, p, n * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+    items.push_back({const_cast<float *>(p), d, n, out});
+    return d;
+  }
+  int finish() {
+    for (auto &it : items)
+      if (it.out) cudaMemcpyAsync(it.host, it.dev, it.n * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
+    return err ? set_err(CM1G_ERR_NOMEM, "staging alloc") : CM1G_OK;
+  }
+};
+
+static int stage_state(cm1g_ctx *c, Stager &S, const cm1g_state_t *st, cm1g_state_t *d) {
+  const DGrid &g = c->g;
+  size_t ns = nS(g), nu = nU(g), nv = nV(g), nw = nW(g);
+  size_t nq = (c->cfg.imoist ? c->cfg.numq : 0) * ns, npt = (c->cfg.iptra ? c->cfg.npt : 0) * ns;
+  size_t nrw = (size_t)g.NJ * g.NK, nrs = (size_t)g.NI * g.NK;
+  d->ua = S.in(st->ua, nu, true); d->u3d = S.in(st->u3d, nu, true); d->uten1 = S.in(st->uten1, nu, false);
+  d->va = S.in(st->va, nv, true); d->v3d = S.in(st->v3d, nv, true); d->vten1 = S.in(st->vten1, nv, false);
+  d->wa = S.in(st->wa, nw, true); d->w3d = S.in(st->w3d, nw, true); d->wten1 = S.in(st->wten1, nw, false);
+  d->ppi = S.in(st->ppi, ns, true); d->pp3d = S.in(st->pp3d, ns, true); d->ppx = S.in(st->ppx, ns, true);
+  d->ppten = S.in(st->ppten, ns, false);
+  d->tha = S.in(st->tha, ns, true); d->th3d = S.in(st->th3d, ns, true); d->thten1 = S.in(st->thten1, ns, false);
+  d->rho = S.in(st->rho, ns, true); d->prs = S.in(st->prs, ns, true);
+  d->qa = S.in(st->qa, nq, true); d->q3d = S.in(st->q3d, nq, true); d->qten = S.in(st->qten, nq, false);
+  d->pta = S.in(st->pta, npt, true); d->pt3d = S.in(st->pt3d, npt, true); d->ptten = S.in(st->ptten, npt, false);
+  d->radbcw = S.in(st->radbcw, nrw, true); d->radbce = S.in(st->radbce, nrw, true);
+  d->radbcs = S.in(st->radbcs, nrs, true); d->radbcn = S.in(st->radbcn, nrs, true);
+  if (S.err) return set_err(CM1G_ERR_NOMEM, "staging alloc");
+  return CM1G_OK;
+}
+
+static int check_state(const cm1g_ctx *c, const cm1g_state_t *st) {
+  const float *req[] = {st->ua, st->u3d, st->uten1, st->va, st->v3d, st->vten1, st->wa, st->w3d, st->wten1,
+                        st->ppi, st->pp3d, st->ppx, st->ppten, st->tha, st->th3d, st->thten1, st->rho, st->prs,
+                        st->radbcw, st->radbce, st->radbcs, st->radbcn};
+  for (const float *p : req) if (!p) return set_err(CM1G_ERR_ARG, "state array missing");
+  if (c->cfg.imoist && (!st->qa || !st->q3d || !st->qten)) return set_err(CM1G_ERR_ARG, "moisture arrays missing");
+  if (c->cfg.iptra && c->cfg.npt > 0 && (!st->pta || !st->pt3d || !st->ptten))
+    return set_err(CM1G_ERR_ARG, "tracer arrays missing");
+  return CM1G_OK;
+}
+
+// ---------------------------------------------------------------------
+// solve2 on device arrays (solve2.F:296-2075)
+// ---------------------------------------------------------------------
+static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass1) {
+  const DGrid &g = c->g;
+  const cm1g_config_t &cf = c->cfg;
+  cudaStream_t st = c->stream;
+  int64_t *nl = &c->nlaunch;
+  const long ns = nS(g);
+  const int numq = cf.imoist ? cf.numq : 0, npt = cf.iptra ? cf.npt : 0;
+  const bool open = g.ibw || g.ibe || g.ibs || g.ibn;
+  const bool openrad = (cf.wbc == 2 || cf.ebc == 2 || cf.sbc == 2 || cf.nbc == 2) && cf.irbc == 4;
+  // scalar list: 0 theta, 1..numq moisture, then tracers
+  const int nsc = 1 + numq + npt;
+  std::vector<const float *> base(nsc), ten1(nsc);
+  std::vector<float *> s3d(nsc);
+  base[0] = d->tha; s3d[0] = d->th3d; ten1[0] = d->thten1;
+  for (int n = 0; n < numq; n++) { base[1 + n] = d->qa + n * ns; s3d[1 + n] = d->q3d + n * ns; ten1[1 + n] = d->qten + n * ns; }
+  for (int n = 0; n < npt; n++) { base[1 + numq + n] = d->pta + n * ns; s3d[1 + numq + n] = d->pt3d + n * ns; ten1[1 + numq + n] = d->ptten + n * ns; }
+  auto buf_in = [&](int s, int nrk) -> float * { return nrk == 1 ? s3d[s] : c->sx[2 * s + (nrk - 2)]; };
+  auto buf_out = [&](int s, int nrk) -> float * { return nrk == 3 ? s3d[s] : c->sx[2 * s + (nrk - 1)]; };
+  const int iqv = cf.nqv;  // scalar index of qv
+
+  for (int nrk = 1; nrk <= 3; nrk++) {
+    const float dttmp = dt / (float)(3 + 1 - nrk);
+    const float *th_in = buf_in(0, nrk);
+    const float *qv_in = cf.imoist ? buf_in(iqv, nrk) : nullptr;
+    launch_stage_prep(g, th_in, d->pp3d, qv_in, cf.imoist, cf.eqtset, c->t11, c->t22, c->thterm, c->piadv, st, nl);
+    launch_bc(g, c->t11, 2, 0, st, nl);
+    launch_adv_momentum(g, d->u3d, d->v3d, d->w3d, d->uten1, d->vten1, d->wten1, c->uten, c->vten, c->wten,
+                        th_in, qv_in, st, nl);
+    launch_sound(g, cf.nsound, nrk, dt, d->ua, d->u3d, c->uten, d->va, d->v3d, c->vten, d->wa, d->w3d, c->wten,
+                 d->ppi, d->pp3d, c->piadv, d->ppten, d->ppx, c->t11, c->t22, c->rru, c->rrv, c->rrw,
+                 d->radbcw, d->radbce, d->radbcs, d->radbcn, c->su, c->sv, c->d1, c->d2, st, nl);
+    if (nrk == 3) launch_cfl(g, d->u3d, d->v3d, d->w3d, dt, c->cflbits, st, nl);
+    if (openrad) launch_radbc4(g, d->ua, d->u3d, d->va, d->v3d, d->radbcw, d->radbce, d->radbcs, d->radbcn, dttmp, st, nl);
+    const int weno = (cf.advwenos == 1 || (cf.advwenos == 2 && nrk == 3)) ? 1 : 0;
+    // theta (solve2.F:1320-1425)
+    launch_advs(g, c->rru, c->rrv, c->rrw, 1, nullptr, th_in, d->tha, 1, d->thten1,
+                (cf.imoist && cf.eqtset == 2) ? c->thterm : nullptr, nullptr, buf_out(0, nrk), weno, 0, 0,
+                (double)(10.0f * 1.0e-18f), dttmp, 1, c->pdefscr, st, nl);
+    // moisture (solve2.F:1431-1530)
+    for (int n = 0; n < numq; n++) {
+      const int s = 1 + n;
+      launch_advs(g, c->rru, c->rrv, c->rrw, 1, nullptr, buf_in(s, nrk), base[s], 0, ten1[s], nullptr, nullptr,
+                  buf_out(s, nrk), weno, nrk == 3 ? 1 : 0, (n + 1 == cf.nqv) ? 0 : 1,
+                  (double)(cf.qmag[n] * 1.0e-18f), dttmp, 1, c->pdefscr, st, nl);
+    }
+    // pressure, density, mass sums (solve2.F:1536-1656)
+    if (nrk == 3)
+      launch_prs_rho(g, d->pp3d, buf_out(0, 3), cf.imoist ? buf_out(iqv, 3) : nullptr, cf.imoist, d->prs, d->rho,
+                     c->part3, c->part4, cf.apmasscon == 1, st, nl);
+    // bcs (solve2.F:1663-1707)
+    launch_bc(g, d->u3d, 3, 0, st, nl);
+    launch_bc(g, d->v3d, 4, 0, st, nl);
+    launch_bc(g, d->w3d, 5, 1, st, nl);
+    if (nrk < 3) {
+      launch_bc(g, d->rho, 2, 0, st, nl);
+      launch_bc(g, d->pp3d, 2, 0, st, nl);
+      launch_bc(g, buf_out(0, nrk), 1, 0, st, nl);
+      for (int n = 0; n < numq; n++) launch_bc(g, buf_out(1 + n, nrk), 1, 0, st, nl);
+    }
+    // passive tracers (solve2.F:1880-1970)
+    for (int n = 0; n < npt; n++) {
+      const int s = 1 + numq + n;
+      const int pdef = (nrk == 3 && cf.pdtra == 1) ? 1 : 0;
+      launch_advs(g, c->rru, c->rrv, c->rrw, 1, nullptr, buf_in(s, nrk), base[s], 0, ten1[s], nullptr, nullptr,
+                  buf_out(s, nrk), weno, pdef, 1, (double)(1.0f * 1.0e-18f), dttmp, 0, c->pdefscr, st, nl);
+      if (nrk <= 2) launch_bc(g, buf_out(s, nrk), 1, 0, st, nl);
+    }
+    // dry-air mass fix (solve2.F:1976-2033)
+    if (nrk == 3 && cf.apmasscon == 1)
+      launch_masscon(g, d->pp3d, buf_out(0, 3), cf.imoist ? buf_out(iqv, 3) : nullptr, cf.imoist, d->prs, d->rho,
+                     c->part3, c->part4, mass1, c->dscal, c->fscal, st, nl);
+  }
+  // tracers after the RK loop (solve2.F:2064-2075)
+  for (int n = 0; n < npt; n++) {
+    float *pt = d->pt3d + n * ns;
+    if (cf.pdtra == 1) launch_pdefq(g, 0.0f, d->rho, pt, c->bud, c->dscal + 4, st, nl);
+    launch_bc(g, pt, 1, 0, st, nl);
+  }
+  (void)open;
+}
+
+static void run_solve3(cm1g_ctx *c, const cm1g_state_t *d) {
+  const DGrid &g = c->g;
+  const cm1g_config_t &cf = c->cfg;
+  cudaStream_t st = c->stream;
+  int64_t *nl = &c->nlaunch;
+  const long ns = nS(g);
+  const int numq = cf.imoist ? cf.numq : 0, npt = cf.iptra ? cf.npt : 0;
+  const int ni = g.ni, nj = g.nj;
+  // solve3.F:246-311
+  launch_bc(g, d->pp3d, 2, 0, st, nl);
+  launch_bc(g, d->th3d, 1, 0, st, nl);
+  for (int n = 0; n < numq; n++) launch_bc(g, d->q3d + n * ns, 1, 0, st, nl);
+  launch_ppx_update(g, d->pp3d, d->ppx, st, nl);
+  launch_bc(g, d->ppx, 2, 0, st, nl);
+  launch_bc(g, d->rho, 2, 0, st, nl);
+  // solve3.F:546-640 rollover
+  launch_copy_range(g, 2, 0, ni + 2, 0, nj + 2, d->u3d, d->ua, st, nl);
+  launch_copy_range(g, 3, 0, ni + 2, 0, nj + 2, d->v3d, d->va, st, nl);
+  launch_copy_range(g, 4, 0, ni + 2, 0, nj + 2, d->w3d, d->wa, st, nl);
+  for (int n = 0; n < npt; n++) launch_copy_range(g, 1, 0, ni + 1, 0, nj + 1, d->pt3d + n * ns, d->pta + n * ns, st, nl);
+  launch_copy_range(g, 1, 0, ni + 1, 0, nj + 1, d->pp3d, d->ppi, st, nl);
+  launch_copy_range(g, 1, 0, ni + 1, 0, nj + 1, d->th3d, d->tha, st, nl);
+  for (int n = 0; n < numq; n++) launch_copy_range(g, 1, 0, ni + 1, 0, nj + 1, d->q3d + n * ns, d->qa + n * ns, st, nl);
+}
+
+static void run_step(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass1) {
+  run_solve2(c, d, dt, mass1);
+  if (c->cfg.imoist)   // cm1.F:3410-3415 (ptype=0)
+    launch_pdefq(c->g, 0.0f, d->rho, d->q3d + (long)(c->cfg.nqv - 1) * nS(c->g), c->bud, c->dscal + 5, c->stream,
+                 &c->nlaunch);
+  run_solve3(c, d);
+}
+
+static int fetch_scalars(cm1g_ctx *c, double *mass2, float *cflmax) {
+  double dv[2];
+  int bits = 0;
+  CUCHK(cudaMemcpyAsync(dv, c->dscal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUCHK(cudaMemcpyAsync(&bits, c->cflbits, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CUCHK(cudaStreamSynchronize(c->stream));
+  if (mass2) *mass2 = c->cfg.apmasscon == 1 ? dv[0] : 0.0;
+  float f;
+  memcpy(&f, &bits, 4);
+  if (cflmax) *cflmax = f;
+  // the reference stops the model when the step goes unstable (solve2.F:2082);
+  // here a non-finite velocity is returned as an error code instead
+  if (!std::isfinite(f)) return set_err(CM1G_ERR_NONFINITE, "non-finite velocity after the large step");
+  return CM1G_OK;
+}
+
+static int solve_common(cm1g_ctx_t *c, float dt, double mass1, double *mass2, float *cflmax, cm1g_state_t *st,
+                        int which, int use_graph) {
+  if (!c) return set_err(CM1G_ERR_STATE, "null context");
+  if (!st) return set_err(CM1G_ERR_ARG, "null state");
+  int rc = check_state(c, st);
+  if (rc) return rc;
+  if (!(dt > 0.0f) || !std::isfinite(dt)) return set_err(CM1G_ERR_ARG, "dt must be positive");
+  if (c->cfg.apmasscon == 1 && !(mass1 > 0.0)) return set_err(CM1G_ERR_ARG, "mass1 must be positive");
+  Stager S(c);
+  cm1g_state_t d;
+  rc = stage_state(c, S, st, &d);
+  if (rc) return rc;
+  bool all_device = S.items.empty();
+  ProfActive pa(c);
+  if (use_graph && all_device && which == 3 && !c->prof) {
+    bool same = c->gexec && memcmp(&c->gstate, &d, sizeof d) == 0 && c->gdt == dt && c->gmass1 == mass1;
+    if (!same) {
+      drop_graph(c);
+      int64_t before = c->nlaunch;
+      CUCHK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      run_step(c, &d, dt, mass1);
+      cudaGraph_t gr;
+      CUCHK(cudaStreamEndCapture(c->stream, &gr));
+      c->graph = gr;
+      CUCHK(cudaGraphInstantiate(&c->gexec, gr, 0));
+      c->graph_nodes = c->nlaunch - before;
+      c->nlaunch = before;
+      c->gstate = d; c->gdt = dt; c->gmass1 = mass1;
+    }
+    CUCHK(cudaGraphLaunch(c->gexec, c->stream));
+    c->nlaunch += c->graph_nodes;
+  } else {
+    if (which == 1) run_solve2(c, &d, dt, mass1);
+    else if (which == 2) run_solve3(c, &d);
+    else run_step(c, &d, dt, mass1);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
+  if (which != 2) {
+    rc = fetch_scalars(c, mass2, cflmax);
+    if (rc) return rc;
+  }
+  return S.finish();
+}
+
+extern "C" int cm1g_solve2(cm1g_ctx_t *c, int32_t nstep, float dt, double mtime, double mass1, double *mass2,
+                           float *cflmax, cm1g_state_t *st) {
+  (void)nstep; (void)mtime;
+  return solve_common(c, dt, mass1, mass2, cflmax, st, 1, 0);
+}
+
+extern "C" int cm1g_solve3(cm1g_ctx_t *c, cm1g_state_t *st) {
+  return solve_common(c, 1.0f, 1.0, nullptr, nullptr, st, 2, 0);
+}
+
+extern "C" int cm1g_step(cm1g_ctx_t *c, int32_t nstep, float dt, double mtime, double mass1, double *mass2,
+                         float *cflmax, cm1g_state_t *st, int32_t use_graph) {
+  (void)nstep; (void)mtime;
+  return solve_common(c, dt, mass1, mass2, cflmax, st, 3, use_graph);
+}
+
+extern "C" int cm1g_pdefq(cm1g_ctx_t *c, float rmax, double *asq, const float *rho, float *q3d) {
+  if (!c || !rho || !q3d) return set_err(CM1G_ERR_ARG, "null argument");
+  ProfActive pa(c);
+  Stager S(c);
+  size_t ns = nS(c->g);
+  const float *drho = S.in(rho, ns, false);
+  float *dq = S.in(q3d, ns, true);
+  CUCHK(cudaMemsetAsync(c->dscal + 8, 0, sizeof(double), c->stream));
+  launch_pdefq(c->g, rmax, drho, dq, c->bud, c->dscal + 8, c->stream, &c->nlaunch);
+  double a = 0.0;
+  CUCHK(cudaMemcpyAsync(&a, c->dscal + 8, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  int rc = S.finish();
+  if (asq) *asq += a;
+  return rc;
+}
+
+static int bc_entry(cm1g_ctx_t *c, float *a, int which, int flag) {
+  if (!c || !a) return set_err(CM1G_ERR_ARG, "null argument");
+  ProfActive pa(c);
+  Stager S(c);
+  size_t n = which == 3 ? nU(c->g) : which == 4 ? nV(c->g) : which == 5 ? nW(c->g) : nS(c->g);
+  float *d = S.in(a, n, true);
+  launch_bc(c->g, d, which, flag, c->stream, &c->nlaunch);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
+  return S.finish();
+}
+extern "C" int cm1g_bcs(cm1g_ctx_t *c, float *s) { return bc_entry(c, s, 1, 0); }
+extern "C" int cm1g_bcp(cm1g_ctx_t *c, float *p) { return bc_entry(c, p, 2, 0); }
+extern "C" int cm1g_bcu(cm1g_ctx_t *c, float *u) { return bc_entry(c, u, 3, 0); }
+extern "C" int cm1g_bcv(cm1g_ctx_t *c, float *v) { return bc_entry(c, v, 4, 0); }
+extern "C" int cm1g_bcw(cm1g_ctx_t *c, float *w, int32_t flag) { return bc_entry(c, w, 5, flag); }
+
+extern "C" int cm1g_advs(cm1g_ctx_t *c, int32_t nrk, int32_t wflag, const float *rru, const float *rrv,
+                         const float *rrw, const float *divx, const float *s0, const float *s, float *sten,
+                         int32_t pdef, int32_t pdefweno, float dt, double weps) {
+  if (!c || !rru || !rrv || !rrw || !divx || !s || !sten || (pdef && !s0)) return set_err(CM1G_ERR_ARG, "null argument");
+  if (nrk < 1 || nrk > 3) return set_err(CM1G_ERR_ARG, "nrk must be 1..3");
+  ProfActive pa(c);
+  Stager S(c);
+  const DGrid &g = c->g;
+  const float *dru = S.in(rru, nU(g), false), *drv = S.in(rrv, nV(g), false), *drw = S.in(rrw, nW(g), false);
+  const float *ddx = S.in(divx, nS(g), false), *ds = S.in(s, nS(g), false);
+  const float *ds0 = s0 ? S.in(s0, nS(g), false) : nullptr;
+  float *dten = S.in(sten, nS(g), true);
+  const int weno = (wflag == 1) && (c->cfg.advwenos == 1 || (c->cfg.advwenos == 2 && nrk == 3));
+  if (!pdef) {
+    launch_advs(g, dru, drv, drw, 0, ddx, ds, ds0 ? ds0 : ds, 0, dten, nullptr, dten, nullptr, weno, 0, pdefweno,
+                weps, dt, 0, c->pdefscr, c->stream, &c->nlaunch);
+  } else {
+    launch_advs(g, dru, drv, drw, 0, ddx, ds, ds0, 0, dten, nullptr, dten, nullptr, weno, 1, pdefweno, weps, dt,
+                0, c->pdefscr, c->stream, &c->nlaunch);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
+  return S.finish();
+}
+
+extern "C" int cm1g_advuvw(cm1g_ctx_t *c, int32_t nrk, const float *u3d, const float *v3d, const float *w3d,
+                           float *uten, float *vten, float *wten) {
+  (void)nrk;
+  if (!c || !u3d || !v3d || !w3d || !uten || !vten || !wten) return set_err(CM1G_ERR_ARG, "null argument");
+  ProfActive pa(c);
+  Stager S(c);
+  const DGrid &g = c->g;
+  const float *du = S.in(u3d, nU(g), false), *dv = S.in(v3d, nV(g), false), *dw = S.in(w3d, nW(g), false);
+  float *tu = S.in(uten, nU(g), true), *tv = S.in(vten, nV(g), true), *tw = S.in(wten, nW(g), true);
+  launch_adv_momentum(g, du, dv, dw, tu, tv, tw, tu, tv, tw, nullptr, nullptr, c->stream, &c->nlaunch);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
+  return S.finish();
+}
+
+extern "C" int cm1g_sound(cm1g_ctx_t *c, int32_t nrk, float dt, float dttmp, float *ua, float *u3d,
+                          const float *uten, float *va, float *v3d, const float *vten, float *wa, float *w3d,
+                          const float *wten, float *ppi, float *pp3d, const float *piadv, const float *ppten,
+                          float *ppx, const float *thv, const float *ppterm, float *rru, float *rrv, float *rrw,
+                          float *radbcw, float *radbce, float *radbcs, float *radbcn) {
+  (void)dttmp;
+  if (!c) return set_err(CM1G_ERR_STATE, "null context");
+  if (nrk < 1 || nrk > 3) return set_err(CM1G_ERR_ARG, "nrk must be 1..3");
+  const void *req[] = {ua, u3d, uten, va, v3d, vten, wa, w3d, wten, ppi, pp3d, piadv, ppten, ppx, thv, ppterm,
+                       rru, rrv, rrw, radbcw, radbce, radbcs, radbcn};
+  for (const void *p : req) if (!p) return set_err(CM1G_ERR_ARG, "null argument");
+  ProfActive pa(c);
+  Stager S(c);
+  const DGrid &g = c->g;
+  size_t ns = nS(g), nu = nU(g), nv = nV(g), nw = nW(g), nrw = (size_t)g.NJ * g.NK, nrs = (size_t)g.NI * g.NK;
+  float *dua = S.in(ua, nu, false), *du3 = S.in(u3d, nu, true);
+  const float *dut = S.in(uten, nu, false);
+  float *dva = S.in(va, nv, false), *dv3 = S.in(v3d, nv, true);
+  const float *dvt = S.in(vten, nv, false);
+  float *dwa = S.in(wa, nw, false), *dw3 = S.in(w3d, nw, true);
+  const float *dwt = S.in(wten, nw, false);
+  float *dppi = S.in(ppi, ns, false), *dpp = S.in(pp3d, ns, true);
+  const float *dpia = S.in(piadv, ns, false), *dppt = S.in(ppten, ns, false);
+  float *dppx = S.in(ppx, ns, true);
+  const float *dthv = S.in(thv, ns, false), *dppterm = S.in(ppterm, ns, false);
+  float *dru = S.in(rru, nu, true), *drv = S.in(rrv, nv, true), *drw = S.in(rrw, nw, true);
+  float *rw = S.in(radbcw, nrw, false), *re = S.in(radbce, nrw, false), *rs = S.in(radbcs, nrs, false),
+        *rn = S.in(radbcn, nrs, false);
+  if (S.err) return set_err(CM1G_ERR_NOMEM, "staging");
+  launch_sound(g, c->cfg.nsound, nrk, dt, dua, du3, dut, dva, dv3, dvt, dwa, dw3, dwt, dppi, dpp, dpia, dppt, dppx,
+               dthv, dppterm, dru, drv, drw, rw, re, rs, rn, c->su, c->sv, c->d1, c->d2, c->stream, &c->nlaunch);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
+  return S.finish();
+}
+
+extern "C" int cm1g_calcmass(cm1g_ctx_t *c, const float *rho, double *tmass) {
+  if (!c || !rho || !tmass) return set_err(CM1G_ERR_ARG, "null argument");
+  Stager S(c);
+  const float *dr = S.in(rho, nS(c->g), false);
+  launch_level_mass(c->g, dr, c->lev, c->stream, &c->nlaunch);
+  std::vector<double> lev(c->g.nk + 2);
+  CUCHK(cudaMemcpyAsync(lev.data(), c->lev, lev.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  int rc = S.finish();
+  if (rc) return rc;
+  double tm = 0.0;
+  for (int k = 1; k <= c->g.nk; k++) tm = tm + lev[k];
+  *tmass = tm * (double)(c->g.dx * c->g.dy * c->g.dz);
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_maxmin(cm1g_ctx_t *c, const float *a, int32_t stag, float *amax, float *amin, int32_t loc[6]) {
+  if (!c || !a || !amax || !amin || !loc) return set_err(CM1G_ERR_ARG, "null argument");
+  if (stag < 1 || stag > 4) return set_err(CM1G_ERR_ARG, "stag must be 1..4");
+  Stager S(c);
+  const DGrid &g = c->g;
+  size_t n = stag == 2 ? nU(g) : stag == 3 ? nV(g) : stag == 4 ? nW(g) : nS(g);
+  const float *d = S.in(a, n, false);
+  launch_maxmin(g, d, stag, c->mm, c->stream, &c->nlaunch);
+  unsigned long long h[2];
+  CUCHK(cudaMemcpyAsync(h, c->mm, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  int rc = S.finish();
+  if (rc) return rc;
+  auto dec = [](unsigned int key) {
+    unsigned int b = (key & 0x80000000u) ? (key & 0x7fffffffu) : ~key;
+    float f; memcpy(&f, &b, 4); return f;
+  };
+  const int ie = g.ni + (stag == 2), je = g.nj + (stag == 3);
+  unsigned int imax = 0xffffffffu - (unsigned int)(h[0] & 0xffffffffu), imin = (unsigned int)(h[1] & 0xffffffffu);
+  *amax = dec((unsigned int)(h[0] >> 32));
+  *amin = dec((unsigned int)(h[1] >> 32));
+  loc[0] = 1 + (int)(imax % ie); loc[1] = 1 + (int)((imax / ie) % je); loc[2] = 1 + (int)(imax / ((unsigned)ie * je));
+  loc[3] = 1 + (int)(imin % ie); loc[4] = 1 + (int)((imin / ie) % je); loc[5] = 1 + (int)(imin / ((unsigned)ie * je));
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_profile(cm1g_ctx_t *c, int32_t enable) {
+  if (!c) return set_err(CM1G_ERR_STATE, "null context");
+  if (c->prof) { c->prof->drain(); delete c->prof; c->prof = nullptr; }
+  if (enable) c->prof = new Profile();
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_profile_read(cm1g_ctx_t *c, int32_t index, char *name, int32_t name_len, int64_t *launches,
+                                 double *total_ms) {
+  if (!c || !name || name_len < 2) return set_err(CM1G_ERR_ARG, "null argument");
+  if (!c->prof) return set_err(CM1G_ERR_STATE, "profiling is off");
+  c->prof->drain();
+  if (index < 0 || index >= (int32_t)c->prof->names.size()) return set_err(CM1G_ERR_ARG, "no such entry");
+  snprintf(name, (size_t)name_len, "%s", c->prof->names[index].c_str());
+  if (launches) *launches = c->prof->count[index];
+  if (total_ms) *total_ms = c->prof->ms[index];
+  return CM1G_OK;
+}

@@ -1,0 +1,136 @@
+// cm1g_common.cuh -- device-side grid descriptor, Fortran-layout indexing and
+// the face-value functions shared by the large-step kernels.
+//
+// All fields use the reference's Fortran layout (i fastest) with lower
+// bounds ib=1-ngxy, jb=1-ngxy, kb=0.  Without terrain the base state and the
+// vertical metrics are horizontally uniform, so the kernels read them as
+// 1-D profiles indexed by k (checked when the context is created).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cm1g {
+
+struct Consts {
+  float g, rd, rv, cp, cv, cpv, cvv, cpl, cpi;
+  float rovcp, rddcv, cpdrd, reps, repsm1;
+};
+
+// Everything a kernel needs to know about the grid; passed by value.
+struct DGrid {
+  int ni, nj, nk, ngxy;
+  int ib, jb;                 // kb = 0
+  int NI, NJ, NK;             // extents of s-arrays
+  float dx, dy, dz, rdx, rdy, rdz;
+  int wbc, ebc, sbc, nbc;
+  int ibw, ibe, ibs, ibn;
+  float smeps, alph, kdiv;
+  Consts c;
+  // vertical profiles (index k, k = 0..nk+1; w-profiles to nk+2)
+  const float *mh, *rmh, *mf, *rho0, *rr0, *rf0, *rrf0, *c1, *c2, *pi0, *th0, *rth0, *qv0, *qc0, *qi0;
+  // horizontal metrics (index i-ib / j-jb)
+  const float *uh, *ruh, *uf, *ruf, *vh, *rvh, *vf, *rvf;
+  const float *dtu0, *dtv0;   // (ib:ie, jb:je)
+};
+
+// Fortran-layout offsets.  s and w arrays share the plane (NI*NJ); u arrays
+// have NI+1 points in x, v arrays NJ+1 rows.
+__host__ __device__ __forceinline__ long iS(const DGrid &g, int i, int j, int k) {
+  return (long)(i - g.ib) + (long)g.NI * ((long)(j - g.jb) + (long)g.NJ * (long)k);
+}
+__host__ __device__ __forceinline__ long iW(const DGrid &g, int i, int j, int k) { return iS(g, i, j, k); }
+__host__ __device__ __forceinline__ long iU(const DGrid &g, int i, int j, int k) {
+  return (long)(i - g.ib) + (long)(g.NI + 1) * ((long)(j - g.jb) + (long)g.NJ * (long)k);
+}
+__host__ __device__ __forceinline__ long iV(const DGrid &g, int i, int j, int k) {
+  return (long)(i - g.ib) + (long)g.NI * ((long)(j - g.jb) + (long)(g.NJ + 1) * (long)k);
+}
+__host__ __device__ __forceinline__ long i2(const DGrid &g, int i, int j) {
+  return (long)(i - g.ib) + (long)g.NI * (long)(j - g.jb);
+}
+__host__ __device__ __forceinline__ long nS(const DGrid &g) { return (long)g.NI * g.NJ * g.NK; }
+__host__ __device__ __forceinline__ long nU(const DGrid &g) { return (long)(g.NI + 1) * g.NJ * g.NK; }
+__host__ __device__ __forceinline__ long nV(const DGrid &g) { return (long)g.NI * (g.NJ + 1) * g.NK; }
+__host__ __device__ __forceinline__ long nW(const DGrid &g) { return (long)g.NI * g.NJ * (g.NK + 1); }
+
+#define LDG(p) __ldg(p)
+
+// ---------------------------------------------------------------------
+// Face values (binary32 arithmetic in the reference's evaluation order;
+// adv_routines.F:5971-6205, 6331-6355).  The library is compiled with
+// --fmad=false so that each product and sum rounds as the Fortran does.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ float flx3(float s1, float s2, float s3) {
+  return ((-1.0f / 6.0f) * s1 + (5.0f / 6.0f) * s2) + (2.0f / 6.0f) * s3;
+}
+__device__ __forceinline__ float flx5(float s1, float s2, float s3, float s4, float s5) {
+  return ((((2.0f / 60.0f) * s1 + (-13.0f / 60.0f) * s2) + (47.0f / 60.0f) * s3) +
+          (27.0f / 60.0f) * s4) + (-3.0f / 60.0f) * s5;
+}
+
+// WENO5 with Borges et al. (2008) weights.  Smoothness indicators in
+// binary32 (as the Fortran evaluates them), weights and quotient in binary64.
+// The three weight divisions of the textbook form are folded into one
+// binary64 division over a common denominator d1^2 d2^2 d3^2, which agrees
+// with the per-weight form to binary64 rounding; the 1e30 clamp of the
+// reference (adv_routines.F:6186-6188) is honoured by the guard.
+__device__ __forceinline__ float weno5(float s1, float s2, float s3, float s4, float s5, double weps) {
+  const float c1312 = 13.0f / 12.0f;
+  float t, u;
+  t = (s1 - 2.0f * s2) + s3; u = (s1 - 4.0f * s2) + 3.0f * s3;
+  double b1 = (double)(c1312 * (t * t) + 0.25f * (u * u));
+  t = (s2 - 2.0f * s3) + s4; u = s2 - s4;
+  double b2 = (double)(c1312 * (t * t) + 0.25f * (u * u));
+  t = (s3 - 2.0f * s4) + s5; u = (3.0f * s3 - 4.0f * s4) + s5;
+  double b3 = (double)(c1312 * (t * t) + 0.25f * (u * u));
+  float q1 = ((2.0f / 6.0f) * s1 + (-7.0f / 6.0f) * s2) + (11.0f / 6.0f) * s3;
+  float q2 = ((-1.0f / 6.0f) * s2 + (5.0f / 6.0f) * s3) + (2.0f / 6.0f) * s4;
+  float q3 = ((2.0f / 6.0f) * s3 + (5.0f / 6.0f) * s4) + (-1.0f / 6.0f) * s5;
+  double tau = fabs(b1 - b3);
+  double d1 = b1 + weps, d2 = b2 + weps, d3 = b3 + weps;
+  double tt = tau * tau;
+  if (tau < 1.0e30 * d1 && tau < 1.0e30 * d2 && tau < 1.0e30 * d3) {
+    double e1 = d1 * d1, e2 = d2 * d2, e3 = d3 * d3;
+    double a1 = (double)0.1f * (e1 + tt) * (e2 * e3);
+    double a2 = (double)0.6f * (e2 + tt) * (e1 * e3);
+    double a3 = (double)0.3f * (e3 + tt) * (e1 * e2);
+    double num = (a1 * (double)q1 + a2 * (double)q2) + a3 * (double)q3;
+    double den = (a1 + a2) + a3;
+    return (float)(num / den);
+  }
+  double r;
+  r = fmin(1.0e30, tau / d1); double w1 = (double)0.1f * (1.0 + r * r);
+  r = fmin(1.0e30, tau / d2); double w2 = (double)0.6f * (1.0 + r * r);
+  r = fmin(1.0e30, tau / d3); double w3 = (double)0.3f * (1.0 + r * r);
+  double num = (w1 * (double)q1 + w2 * (double)q2) + w3 * (double)q3;
+  double den = (w1 + w2) + w3;
+  return (float)(num / den);
+}
+
+__device__ __forceinline__ float upstrpd(float s1, float s2, float s3, double weps) {
+  float dd = s2 - s1;
+  float rr = (s3 - s2) / (copysignf((float)weps, dd) + dd);
+  float phi = fmaxf(0.0f, fminf(rr, fminf((1.0f / 6.0f) + (2.0f / 6.0f) * rr, 1.0f)));
+  return s2 + phi * (s2 - s1);
+}
+
+__device__ __forceinline__ float absmax5(float a, float b, float c, float d, float e) {
+  return fmaxf(fmaxf(fmaxf(fmaxf(fabsf(a), fabsf(b)), fabsf(c)), fabsf(d)), fabsf(e));
+}
+
+// Per-kernel device timing (the library's counterpart of the reference's
+// timestats, input.F:359-387).  When a profile is active every kernel launch
+// site brackets its launch with a pair of CUDA events on the launch stream;
+// the elapsed times are summed per kernel name when the profile is read.
+struct Profile;
+extern thread_local Profile *g_profile;
+void prof_record(const char *name, cudaStream_t st, bool begin);
+
+struct ProfScope {
+  const char *name;
+  cudaStream_t st;
+  ProfScope(const char *n, cudaStream_t s) : name(n), st(s) { if (g_profile) prof_record(name, st, true); }
+  ~ProfScope() { if (g_profile) prof_record(name, st, false); }
+};
+
+}  // namespace cm1g

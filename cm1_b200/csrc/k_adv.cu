@@ -1,0 +1,607 @@
+// k_adv.cu -- flux-form advection tendencies (adv.F, adv_routines.F).
+//
+// One thread per output point.  Face fluxes are evaluated where they are
+// needed (the two faces of a cell in each direction) instead of being stored
+// in dumx/dumy/dumz, and the rho0-weighted fluxes rru/rrv/rrw and their
+// divergence divx are formed on the fly from the velocities, so a momentum
+// pass reads u, v, w (and theta/qv for buoyancy) and writes only the three
+// tendencies.  Every expression keeps the reference's operand order.
+#include "cm1g_common.cuh"
+
+namespace cm1g {
+
+// ---------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------
+struct Vel {  // momentum-pass view of u,v,w and the mass-flux weights
+  const float *__restrict__ u, *__restrict__ v, *__restrict__ w;
+};
+
+__device__ __forceinline__ float RRU(const DGrid &g, const Vel &q, int i, int j, int k) {
+  return LDG(&g.rho0[k]) * LDG(&q.u[iU(g, i, j, k)]);             // solve2.F:499
+}
+__device__ __forceinline__ float RRV(const DGrid &g, const Vel &q, int i, int j, int k) {
+  return LDG(&g.rho0[k]) * LDG(&q.v[iV(g, i, j, k)]);             // solve2.F:504
+}
+__device__ __forceinline__ float RRW(const DGrid &g, const Vel &q, int i, int j, int k) {
+  if (k <= 1 || k >= g.nk + 1) return 0.0f;                       // solve2.F:509-511
+  return LDG(&g.rf0[k]) * LDG(&q.w[iW(g, i, j, k)]);              // solve2.F:516
+}
+// divx of the momentum pass (solve2.F:590-596)
+__device__ __forceinline__ float DIVX(const DGrid &g, const Vel &q, int i, int j, int k) {
+  float d = ((RRU(g, q, i + 1, j, k) - RRU(g, q, i, j, k)) * g.rdx * LDG(&g.uh[i - g.ib]) +
+             (RRV(g, q, i, j + 1, k) - RRV(g, q, i, j, k)) * g.rdy * LDG(&g.vh[j - g.jb])) +
+            (RRW(g, q, i, j, k + 1) - RRW(g, q, i, j, k)) * g.rdz * LDG(&g.mh[k]);
+  if (fabsf(d) < g.smeps) d = 0.0f;
+  return d;
+}
+
+// ---------------------------------------------------------------------
+// advu: adv.F:911-1839 with hadv_flx5/vadv_flx5 stag=2
+// ---------------------------------------------------------------------
+__device__ __forceinline__ float advu_dumx(const DGrid &g, const Vel &q, int i, int j, int k) {
+  // hadv_flx5 stag=2 at s-point i (adv_routines.F:1388-1397)
+  const float *u = q.u;
+  float ubar = 0.5f * (RRU(g, q, i, j, k) + RRU(g, q, i + 1, j, k));
+  if (ubar >= 0.0f)
+    return ubar * flx5(LDG(&u[iU(g, i - 2, j, k)]), LDG(&u[iU(g, i - 1, j, k)]), LDG(&u[iU(g, i, j, k)]),
+                       LDG(&u[iU(g, i + 1, j, k)]), LDG(&u[iU(g, i + 2, j, k)]));
+  return ubar * flx5(LDG(&u[iU(g, i + 3, j, k)]), LDG(&u[iU(g, i + 2, j, k)]), LDG(&u[iU(g, i + 1, j, k)]),
+                     LDG(&u[iU(g, i, j, k)]), LDG(&u[iU(g, i - 1, j, k)]));
+}
+__device__ __forceinline__ float advu_dumy(const DGrid &g, const Vel &q, int i, int j, int k) {
+  const float *u = q.u;
+  float vbar = 0.5f * (RRV(g, q, i, j, k) + RRV(g, q, i - 1, j, k));
+  if (vbar >= 0.0f)
+    return vbar * flx5(LDG(&u[iU(g, i, j - 3, k)]), LDG(&u[iU(g, i, j - 2, k)]), LDG(&u[iU(g, i, j - 1, k)]),
+                       LDG(&u[iU(g, i, j, k)]), LDG(&u[iU(g, i, j + 1, k)]));
+  return vbar * flx5(LDG(&u[iU(g, i, j + 2, k)]), LDG(&u[iU(g, i, j + 1, k)]), LDG(&u[iU(g, i, j, k)]),
+                     LDG(&u[iU(g, i, j - 1, k)]), LDG(&u[iU(g, i, j - 2, k)]));
+}
+
+// vertical flux of a u- (stag 2) or v- (stag 3) column at w-level kk,
+// vadv_flx5 (adv_routines.F:3299-3364) + vadv_lwr_flx_23/_35.
+template <int STAG>
+__device__ __forceinline__ float vflux_uv(const DGrid &g, const Vel &q, const float *__restrict__ a, int i, int j, int kk) {
+  const int nk = g.nk;
+  auto A = [&](int k) { return LDG(&a[STAG == 2 ? iU(g, i, j, k) : iV(g, i, j, k)]); };
+  float wbar = (STAG == 2) ? 0.5f * (RRW(g, q, i, j, kk) + RRW(g, q, i - 1, j, kk))
+                           : 0.5f * (RRW(g, q, i, j, kk) + RRW(g, q, i, j - 1, kk));
+  if (kk >= 4 && kk <= nk - 2) {
+    if (wbar >= 0.0f) return wbar * flx5(A(kk - 3), A(kk - 2), A(kk - 1), A(kk), A(kk + 1));
+    return wbar * flx5(A(kk + 2), A(kk + 1), A(kk), A(kk - 1), A(kk - 2));
+  }
+  float c2k = LDG(&g.c2[kk]);
+  if (kk == 2) {
+    if (wbar >= 0.0f) { float cc2 = 0.5f * (c2k + c2k), cc1 = 1.0f - cc2; return wbar * (cc1 * A(kk - 1) + cc2 * A(kk)); }
+    return wbar * flx3(A(kk + 1), A(kk), A(kk - 1));
+  }
+  if (kk == nk) {
+    if (wbar >= 0.0f) return wbar * flx3(A(kk - 2), A(kk - 1), A(kk));
+    float cc2 = 0.5f * (c2k + c2k), cc1 = 1.0f - cc2; return wbar * (cc1 * A(kk - 1) + cc2 * A(kk));
+  }
+  if (kk == 3) {
+    if (wbar >= 0.0f) return wbar * flx3(A(kk - 2), A(kk - 1), A(kk));
+    return wbar * flx5(A(kk + 2), A(kk + 1), A(kk), A(kk - 1), A(kk - 2));
+  }
+  // kk == nk-1
+  if (wbar >= 0.0f) return wbar * flx5(A(kk - 3), A(kk - 2), A(kk - 1), A(kk), A(kk + 1));
+  return wbar * flx3(A(kk + 1), A(kk), A(kk - 1));
+}
+
+template <int STAG>
+__device__ __forceinline__ float advz_uv(const DGrid &g, const Vel &q, const float *a, int i, int j, int k) {
+  const float mhk = LDG(&g.mh[k]);
+  if (k == 1) return -vflux_uv<STAG>(g, q, a, i, j, 2) * g.rdz * mhk;
+  if (k == g.nk) return +vflux_uv<STAG>(g, q, a, i, j, g.nk) * g.rdz * mhk;
+  return -(vflux_uv<STAG>(g, q, a, i, j, k + 1) - vflux_uv<STAG>(g, q, a, i, j, k)) * g.rdz * mhk;
+}
+
+__global__ void k_advu(DGrid g, Vel q, const float *uten1, float *uten) {
+  const int i1 = g.ibw ? 2 : 1, i2 = g.ibe ? g.ni : g.ni + 1;
+  const int i = i1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = 1 + (int)blockIdx.y, k = 1 + (int)blockIdx.z;
+  if (i > i2) return;
+  const int nj = g.nj;
+  const bool doits = (g.sbc == 2 && g.ibs), doitn = (g.nbc == 2 && g.ibn);
+  float advx = -(advu_dumx(g, q, i, j, k) - advu_dumx(g, q, i - 1, j, k)) * g.rdx * LDG(&g.uf[i - g.ib]);
+  float dyp = advu_dumy(g, q, i, j + 1, k), dy0 = advu_dumy(g, q, i, j, k);
+  if (doits && j == 1 && (RRV(g, q, i, 1, k) + RRV(g, q, i - 1, 1, k)) >= 0.0f) dy0 = advu_dumy(g, q, i, 2, k);
+  if (doitn && j == nj && (RRV(g, q, i, nj + 1, k) + RRV(g, q, i - 1, nj + 1, k)) <= 0.0f) dyp = dy0;
+  float advy = -(dyp - dy0) * g.rdy * LDG(&g.vh[j - g.jb]);
+  if (doits && j == 1 && (RRV(g, q, i, 1, k) + RRV(g, q, i - 1, 1, k)) >= 0.0f)
+    advy = advy - LDG(&q.u[iU(g, i, 1, k)]) * 0.5f *
+                      ((RRV(g, q, i - 1, 2, k) - RRV(g, q, i - 1, 1, k)) + (RRV(g, q, i, 2, k) - RRV(g, q, i, 1, k))) *
+                      g.rdy * LDG(&g.vh[1 - g.jb]);
+  if (doitn && j == nj && (RRV(g, q, i, nj + 1, k) + RRV(g, q, i - 1, nj + 1, k)) <= 0.0f)
+    advy = advy - LDG(&q.u[iU(g, i, nj, k)]) * 0.5f *
+                      ((RRV(g, q, i - 1, nj + 1, k) - RRV(g, q, i - 1, nj, k)) + (RRV(g, q, i, nj + 1, k) - RRV(g, q, i, nj, k))) *
+                      g.rdy * LDG(&g.vh[nj - g.jb]);
+  float advz = advz_uv<2>(g, q, q.u, i, j, k);
+  long o = iU(g, i, j, k);
+  float uu = LDG(&q.u[o]);
+  uten[o] = uten1[o] + (((advx + advy) + advz) + uu * 0.5f * (DIVX(g, q, i, j, k) + DIVX(g, q, i - 1, j, k))) * LDG(&g.rr0[k]);
+}
+
+// ---------------------------------------------------------------------
+// advv: adv.F:1847-2770 with hadv_flx5/vadv_flx5 stag=3
+// ---------------------------------------------------------------------
+__device__ __forceinline__ float advv_dumx(const DGrid &g, const Vel &q, int i, int j, int k) {
+  const float *v = q.v;
+  float ubar = 0.5f * (RRU(g, q, i, j, k) + RRU(g, q, i, j - 1, k));
+  if (ubar >= 0.0f)
+    return ubar * flx5(LDG(&v[iV(g, i - 3, j, k)]), LDG(&v[iV(g, i - 2, j, k)]), LDG(&v[iV(g, i - 1, j, k)]),
+                       LDG(&v[iV(g, i, j, k)]), LDG(&v[iV(g, i + 1, j, k)]));
+  return ubar * flx5(LDG(&v[iV(g, i + 2, j, k)]), LDG(&v[iV(g, i + 1, j, k)]), LDG(&v[iV(g, i, j, k)]),
+                     LDG(&v[iV(g, i - 1, j, k)]), LDG(&v[iV(g, i - 2, j, k)]));
+}
+__device__ __forceinline__ float advv_dumy(const DGrid &g, const Vel &q, int i, int j, int k) {
+  const float *v = q.v;
+  float vbar = 0.5f * (RRV(g, q, i, j, k) + RRV(g, q, i, j + 1, k));
+  if (vbar >= 0.0f)
+    return vbar * flx5(LDG(&v[iV(g, i, j - 2, k)]), LDG(&v[iV(g, i, j - 1, k)]), LDG(&v[iV(g, i, j, k)]),
+                       LDG(&v[iV(g, i, j + 1, k)]), LDG(&v[iV(g, i, j + 2, k)]));
+  return vbar * flx5(LDG(&v[iV(g, i, j + 3, k)]), LDG(&v[iV(g, i, j + 2, k)]), LDG(&v[iV(g, i, j + 1, k)]),
+                     LDG(&v[iV(g, i, j, k)]), LDG(&v[iV(g, i, j - 1, k)]));
+}
+
+__global__ void k_advv(DGrid g, Vel q, const float *vten1, float *vten) {
+  const int j1 = g.ibs ? 2 : 1, j2 = g.ibn ? g.nj : g.nj + 1;
+  const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = j1 + (int)blockIdx.y, k = 1 + (int)blockIdx.z;
+  if (i > g.ni || j > j2) return;
+  const int ni = g.ni;
+  const bool doitw = (g.wbc == 2 && g.ibw), doite = (g.ebc == 2 && g.ibe);
+  float dx0 = advv_dumx(g, q, i, j, k), dxp = advv_dumx(g, q, i + 1, j, k);
+  if (doitw && i == 1 && (RRU(g, q, 1, j, k) + RRU(g, q, 1, j - 1, k)) >= 0.0f) dx0 = advv_dumx(g, q, 2, j, k);
+  if (doite && i == ni && (RRU(g, q, ni + 1, j, k) + RRU(g, q, ni + 1, j - 1, k)) <= 0.0f) dxp = dx0;
+  float advx = -(dxp - dx0) * g.rdx * LDG(&g.uh[i - g.ib]);
+  float advy = -(advv_dumy(g, q, i, j, k) - advv_dumy(g, q, i, j - 1, k)) * g.rdy * LDG(&g.vf[j - g.jb]);
+  if (doitw && i == 1 && (RRU(g, q, 1, j, k) + RRU(g, q, 1, j - 1, k)) >= 0.0f)
+    advx = advx - LDG(&q.v[iV(g, 1, j, k)]) * 0.5f *
+                      ((RRU(g, q, 2, j - 1, k) - RRU(g, q, 1, j - 1, k)) + (RRU(g, q, 2, j, k) - RRU(g, q, 1, j, k))) *
+                      g.rdx * LDG(&g.uh[1 - g.ib]);
+  if (doite && i == ni && (RRU(g, q, ni + 1, j, k) + RRU(g, q, ni + 1, j - 1, k)) <= 0.0f)
+    advx = advx - LDG(&q.v[iV(g, ni, j, k)]) * 0.5f *
+                      ((RRU(g, q, ni + 1, j - 1, k) - RRU(g, q, ni, j - 1, k)) + (RRU(g, q, ni + 1, j, k) - RRU(g, q, ni, j, k))) *
+                      g.rdx * LDG(&g.uh[ni - g.ib]);
+  float advz = advz_uv<3>(g, q, q.v, i, j, k);
+  long o = iV(g, i, j, k);
+  float vv = LDG(&q.v[o]);
+  vten[o] = vten1[o] + (((advx + advy) + advz) + vv * 0.5f * (DIVX(g, q, i, j, k) + DIVX(g, q, i, j - 1, k))) * LDG(&g.rr0[k]);
+}
+
+// ---------------------------------------------------------------------
+// advw: adv.F:2778-3610 with hadv_flx5/vadv_flx5 stag=4, plus the
+// buoyancy term of solve2.F:899-907 when th3d is given.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ float advw_dumx(const DGrid &g, const Vel &q, int i, int j, int k, float *ubar_out) {
+  const float *w = q.w;
+  float c2k = LDG(&g.c2[k]);
+  float cc2 = 0.5f * (c2k + c2k), cc1 = 1.0f - cc2;
+  float ubar = cc2 * RRU(g, q, i, j, k) + cc1 * RRU(g, q, i, j, k - 1);
+  if (ubar_out) *ubar_out = ubar;
+  if (ubar >= 0.0f)
+    return ubar * flx5(LDG(&w[iW(g, i - 3, j, k)]), LDG(&w[iW(g, i - 2, j, k)]), LDG(&w[iW(g, i - 1, j, k)]),
+                       LDG(&w[iW(g, i, j, k)]), LDG(&w[iW(g, i + 1, j, k)]));
+  return ubar * flx5(LDG(&w[iW(g, i + 2, j, k)]), LDG(&w[iW(g, i + 1, j, k)]), LDG(&w[iW(g, i, j, k)]),
+                     LDG(&w[iW(g, i - 1, j, k)]), LDG(&w[iW(g, i - 2, j, k)]));
+}
+__device__ __forceinline__ float advw_dumy(const DGrid &g, const Vel &q, int i, int j, int k, float *vbar_out) {
+  const float *w = q.w;
+  float c2k = LDG(&g.c2[k]);
+  float cc2 = 0.5f * (c2k + c2k), cc1 = 1.0f - cc2;
+  float vbar = cc2 * RRV(g, q, i, j, k) + cc1 * RRV(g, q, i, j, k - 1);
+  if (vbar_out) *vbar_out = vbar;
+  if (vbar >= 0.0f)
+    return vbar * flx5(LDG(&w[iW(g, i, j - 3, k)]), LDG(&w[iW(g, i, j - 2, k)]), LDG(&w[iW(g, i, j - 1, k)]),
+                       LDG(&w[iW(g, i, j, k)]), LDG(&w[iW(g, i, j + 1, k)]));
+  return vbar * flx5(LDG(&w[iW(g, i, j + 2, k)]), LDG(&w[iW(g, i, j + 1, k)]), LDG(&w[iW(g, i, j, k)]),
+                     LDG(&w[iW(g, i, j - 1, k)]), LDG(&w[iW(g, i, j - 2, k)]));
+}
+// vadv_flx5 stag=4 at s-level kk (adv_routines.F:3366-3384, 4979-5000, 5148-5172)
+__device__ __forceinline__ float vflux_w(const DGrid &g, const Vel &q, int i, int j, int kk) {
+  const int nk = g.nk;
+  const float *w = q.w;
+  auto A = [&](int k) { return LDG(&w[iW(g, i, j, k)]); };
+  float wbar = 0.5f * (RRW(g, q, i, j, kk) + RRW(g, q, i, j, kk + 1));
+  if (kk >= 3 && kk <= nk - 2) {
+    if (wbar >= 0.0f) return wbar * flx5(A(kk - 2), A(kk - 1), A(kk), A(kk + 1), A(kk + 2));
+    return wbar * flx5(A(kk + 3), A(kk + 2), A(kk + 1), A(kk), A(kk - 1));
+  }
+  if (kk == 1) {
+    if (wbar >= 0.0f) return wbar * 0.5f * (A(kk) + A(kk + 1));
+    return wbar * flx3(A(kk + 2), A(kk + 1), A(kk));
+  }
+  if (kk == nk) {
+    if (wbar >= 0.0f) return wbar * flx3(A(kk - 1), A(kk), A(kk + 1));
+    return wbar * 0.5f * (A(kk) + A(kk + 1));
+  }
+  if (kk == 2) {
+    if (wbar >= 0.0f) return wbar * flx3(A(kk - 1), A(kk), A(kk + 1));
+    return wbar * flx5(A(kk + 3), A(kk + 2), A(kk + 1), A(kk), A(kk - 1));
+  }
+  // kk == nk-1
+  if (wbar >= 0.0f) return wbar * flx5(A(kk - 2), A(kk - 1), A(kk), A(kk + 1), A(kk + 2));
+  return wbar * flx3(A(kk + 2), A(kk + 1), A(kk));
+}
+
+// buoyancy at s-points (solve2.F:313-440)
+__device__ __forceinline__ float buoy(const DGrid &g, const float *th3d, const float *qv, int i, int j, int k) {
+  float th3 = LDG(&th3d[iS(g, i, j, k)]);
+  if (qv) {
+    float q = fmaxf(LDG(&qv[iS(g, i, j, k)]), 0.0f);
+    float qli = fmaxf(0.0f, 0.0f + 0.0f);
+    return g.c.g * ((th3 * LDG(&g.rth0[k]) + g.c.repsm1 * (q - LDG(&g.qv0[k]))) - ((qli - LDG(&g.qc0[k])) - LDG(&g.qi0[k])));
+  }
+  return g.c.g * th3 * LDG(&g.rth0[k]);
+}
+
+__global__ void k_advw(DGrid g, Vel q, const float *wten1, float *wten,
+                       const float *__restrict__ th3d, const float *__restrict__ qv) {
+  const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = 1 + (int)blockIdx.y, k = 2 + (int)blockIdx.z;
+  if (i > g.ni) return;
+  const int ni = g.ni, nj = g.nj;
+  const bool doitw = (g.wbc == 2 && g.ibw), doite = (g.ebc == 2 && g.ibe);
+  const bool doits = (g.sbc == 2 && g.ibs), doitn = (g.nbc == 2 && g.ibn);
+  float ub0, ubp, vb0, vbp;
+  float dx0 = advw_dumx(g, q, i, j, k, &ub0), dxp = advw_dumx(g, q, i + 1, j, k, &ubp);
+  if (doitw && i == 1 && ub0 >= 0.0f) dx0 = advw_dumx(g, q, 2, j, k, nullptr);
+  if (doite && i == ni && ubp <= 0.0f) dxp = dx0;
+  float dy0 = advw_dumy(g, q, i, j, k, &vb0), dyp = advw_dumy(g, q, i, j + 1, k, &vbp);
+  if (doits && j == 1 && vb0 >= 0.0f) dy0 = advw_dumy(g, q, i, 2, k, nullptr);
+  if (doitn && j == nj && vbp <= 0.0f) dyp = dy0;
+  float advx = -(dxp - dx0) * g.rdx * LDG(&g.uh[i - g.ib]);
+  float advy = -(dyp - dy0) * g.rdy * LDG(&g.vh[j - g.jb]);
+  const float c1k = LDG(&g.c1[k]), c2k = LDG(&g.c2[k]);
+  long o = iW(g, i, j, k);
+  const float ww = LDG(&q.w[o]);
+  if (doitw && i == 1 && ub0 >= 0.0f)
+    advx = advx - ww * (c1k * (RRU(g, q, 2, j, k - 1) - RRU(g, q, 1, j, k - 1)) + c2k * (RRU(g, q, 2, j, k) - RRU(g, q, 1, j, k))) *
+                      g.rdx * LDG(&g.uh[1 - g.ib]);
+  if (doite && i == ni && ubp <= 0.0f)
+    advx = advx - ww * (c1k * (RRU(g, q, ni + 1, j, k - 1) - RRU(g, q, ni, j, k - 1)) + c2k * (RRU(g, q, ni + 1, j, k) - RRU(g, q, ni, j, k))) *
+                      g.rdx * LDG(&g.uh[ni - g.ib]);
+  if (doits && j == 1 && vb0 >= 0.0f)
+    advy = advy - ww * (c1k * (RRV(g, q, i, 2, k - 1) - RRV(g, q, i, 1, k - 1)) + c2k * (RRV(g, q, i, 2, k) - RRV(g, q, i, 1, k))) *
+                      g.rdy * LDG(&g.vh[1 - g.jb]);
+  if (doitn && j == nj && vbp <= 0.0f)
+    advy = advy - ww * (c1k * (RRV(g, q, i, nj + 1, k - 1) - RRV(g, q, i, nj, k - 1)) + c2k * (RRV(g, q, i, nj + 1, k) - RRV(g, q, i, nj, k))) *
+                      g.rdy * LDG(&g.vh[nj - g.jb]);
+  float advz = -(vflux_w(g, q, i, j, k) - vflux_w(g, q, i, j, k - 1)) * g.rdz * LDG(&g.mf[k]);
+  float t = wten1[o] + (((advx + advy) + advz) + ww * (c2k * DIVX(g, q, i, j, k) + c1k * DIVX(g, q, i, j, k - 1))) * LDG(&g.rrf0[k]);
+  if (th3d) t = t + (c1k * buoy(g, th3d, qv, i, j, k - 1) + c2k * buoy(g, th3d, qv, i, j, k));
+  wten[o] = t;
+}
+
+void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w,
+                         const float *uten1, const float *vten1, const float *wten1,
+                         float *uten, float *vten, float *wten, const float *th3d, const float *qv,
+                         cudaStream_t st, int64_t *nl) {
+  Vel q{u, v, w};
+  const int bx = 128;
+  {
+    int i1 = g.ibw ? 2 : 1, i2 = g.ibe ? g.ni : g.ni + 1;
+    dim3 grid((i2 - i1 + 1 + bx - 1) / bx, g.nj, g.nk);
+    { ProfScope _ps("k_advu", st); k_advu<<<grid, bx, 0, st>>>(g, q, uten1, uten); }
+  }
+  {
+    int j1 = g.ibs ? 2 : 1, j2 = g.ibn ? g.nj : g.nj + 1;
+    dim3 grid((g.ni + bx - 1) / bx, j2 - j1 + 1, g.nk);
+    { ProfScope _ps("k_advv", st); k_advv<<<grid, bx, 0, st>>>(g, q, vten1, vten); }
+  }
+  {
+    dim3 grid((g.ni + bx - 1) / bx, g.nj, g.nk - 1);
+    { ProfScope _ps("k_advw", st); k_advw<<<grid, bx, 0, st>>>(g, q, wten1, wten, th3d, qv); }
+  }
+  if (nl) *nl += 3;
+}
+
+// ---------------------------------------------------------------------
+// advs: adv.F:14-903 for one scalar.
+//
+// The fluxes use the small-step-averaged velocities rru/rrv/rrw as sound
+// leaves them; getdivx's rho0/rf0 weighting (misclibs.F:251-276) and divx
+// (misclibs.F:330-340) are applied on the fly.  `sadd` (the theta offset
+// th0-300, solve2.F:1365-1372) is added to s when given.
+// ---------------------------------------------------------------------
+struct SAdv {
+  const float *__restrict__ rru, *__restrict__ rrv, *__restrict__ rrw;  // averaged velocities or fluxes
+  const float *__restrict__ s;      // advected field (full halo)
+  const float *__restrict__ s0;     // RK base value (pdef only)
+  const float *__restrict__ divx;   // caller's divx (adv.F argument) or null: formed here
+  const float *__restrict__ thterm; // moist theta: thten -= div(u_avg)*thterm (solve2.F:1320-1329)
+  int weighted;                     // 1: rru/rrv/rrw are velocities to be weighted here
+  int sadd;                         // add th0(k)-th0r to s (theta)
+};
+
+__device__ __forceinline__ float sval(const DGrid &g, const SAdv &a, int i, int j, int k) {
+  float v = LDG(&a.s[iS(g, i, j, k)]);
+  if (a.sadd) v = (LDG(&g.th0[k]) - 300.0f) + v;
+  return v;
+}
+__device__ __forceinline__ float FU(const DGrid &g, const SAdv &a, int i, int j, int k) {
+  float v = LDG(&a.rru[iU(g, i, j, k)]);
+  return a.weighted ? v * LDG(&g.rho0[k]) : v;
+}
+__device__ __forceinline__ float FV(const DGrid &g, const SAdv &a, int i, int j, int k) {
+  float v = LDG(&a.rrv[iV(g, i, j, k)]);
+  return a.weighted ? v * LDG(&g.rho0[k]) : v;
+}
+__device__ __forceinline__ float FW(const DGrid &g, const SAdv &a, int i, int j, int k) {
+  if (a.weighted && (k <= 1 || k >= g.nk + 1)) return 0.0f;
+  float v = LDG(&a.rrw[iW(g, i, j, k)]);
+  return a.weighted ? v * LDG(&g.rf0[k]) : v;
+}
+// getdiv of the averaged velocities (misclibs.F:127-136), for the moist theta term
+__device__ __forceinline__ float RAWDIV(const DGrid &g, const SAdv &a, int i, int j, int k) {
+  auto W = [&](int kk) { return (kk <= 1 || kk >= g.nk + 1) ? 0.0f : LDG(&a.rrw[iW(g, i, j, kk)]); };
+  float d = ((LDG(&a.rru[iU(g, i + 1, j, k)]) - LDG(&a.rru[iU(g, i, j, k)])) * g.rdx * LDG(&g.uh[i - g.ib]) +
+             (LDG(&a.rrv[iV(g, i, j + 1, k)]) - LDG(&a.rrv[iV(g, i, j, k)])) * g.rdy * LDG(&g.vh[j - g.jb])) +
+            (W(k + 1) - W(k)) * g.rdz * LDG(&g.mh[k]);
+  if (fabsf(d) < g.smeps) d = 0.0f;
+  return d;
+}
+__device__ __forceinline__ float SDIV(const DGrid &g, const SAdv &a, int i, int j, int k) {
+  if (a.divx) return LDG(&a.divx[iS(g, i, j, k)]);
+  float d = ((FU(g, a, i + 1, j, k) - FU(g, a, i, j, k)) * g.rdx * LDG(&g.uh[i - g.ib]) +
+             (FV(g, a, i, j + 1, k) - FV(g, a, i, j, k)) * g.rdy * LDG(&g.vh[j - g.jb])) +
+            (FW(g, a, i, j, k + 1) - FW(g, a, i, j, k)) * g.rdz * LDG(&g.mh[k]);
+  if (fabsf(d) < g.smeps) d = 0.0f;
+  return d;
+}
+
+// x-face flux dumx(i,j,k) (hadv_flx5/hadv_weno5 stag=1)
+__device__ __forceinline__ float sflux_x(const DGrid &g, const SAdv &a, int i, int j, int k, int weno, int pdef, double weps) {
+  float r = FU(g, a, i, j, k), s1, s2, s3, s4, s5;
+  if (r >= 0.0f) { s1 = sval(g, a, i - 3, j, k); s2 = sval(g, a, i - 2, j, k); s3 = sval(g, a, i - 1, j, k); s4 = sval(g, a, i, j, k); s5 = sval(g, a, i + 1, j, k); }
+  else { s1 = sval(g, a, i + 2, j, k); s2 = sval(g, a, i + 1, j, k); s3 = sval(g, a, i, j, k); s4 = sval(g, a, i - 1, j, k); s5 = sval(g, a, i - 2, j, k); }
+  if (!weno) return r * flx5(s1, s2, s3, s4, s5);
+  if (pdef == 1 && !(absmax5(s1, s2, s3, s4, s5) > (float)weps)) return 0.0f;
+  return r * weno5(s1, s2, s3, s4, s5, weps);
+}
+__device__ __forceinline__ float sflux_y(const DGrid &g, const SAdv &a, int i, int j, int k, int weno, int pdef, double weps) {
+  float r = FV(g, a, i, j, k), s1, s2, s3, s4, s5;
+  if (r >= 0.0f) { s1 = sval(g, a, i, j - 3, k); s2 = sval(g, a, i, j - 2, k); s3 = sval(g, a, i, j - 1, k); s4 = sval(g, a, i, j, k); s5 = sval(g, a, i, j + 1, k); }
+  else { s1 = sval(g, a, i, j + 2, k); s2 = sval(g, a, i, j + 1, k); s3 = sval(g, a, i, j, k); s4 = sval(g, a, i, j - 1, k); s5 = sval(g, a, i, j - 2, k); }
+  if (!weno) return r * flx5(s1, s2, s3, s4, s5);
+  if (pdef == 1 && !(absmax5(s1, s2, s3, s4, s5) > (float)weps)) return 0.0f;
+  return r * weno5(s1, s2, s3, s4, s5, weps);
+}
+// vertical flux dumz(i,j,kk), kk=2..nk (vadv_flx5 / vadv_weno5 stag=1)
+__device__ __forceinline__ float sflux_z(const DGrid &g, const SAdv &a, int i, int j, int kk, int weno, int pdefweno, double weps) {
+  const int nk = g.nk;
+  auto A = [&](int k) { return sval(g, a, i, j, k); };
+  float r = FW(g, a, i, j, kk);
+  const float c1k = LDG(&g.c1[kk]), c2k = LDG(&g.c2[kk]);
+  if (!weno) {
+    if (kk >= 4 && kk <= nk - 2) {
+      if (r >= 0.0f) return r * flx5(A(kk - 3), A(kk - 2), A(kk - 1), A(kk), A(kk + 1));
+      return r * flx5(A(kk + 2), A(kk + 1), A(kk), A(kk - 1), A(kk - 2));
+    }
+    if (kk == 2) {
+      if (r >= 0.0f) return r * (c1k * A(kk - 1) + c2k * A(kk));
+      return r * flx3(A(kk + 1), A(kk), A(kk - 1));
+    }
+    if (kk == nk) {
+      if (r >= 0.0f) return r * flx3(A(kk - 2), A(kk - 1), A(kk));
+      return r * (c1k * A(kk - 1) + c2k * A(kk));
+    }
+    if (kk == 3) {
+      if (r >= 0.0f) return r * flx3(A(kk - 2), A(kk - 1), A(kk));
+      return r * flx5(A(kk + 2), A(kk + 1), A(kk), A(kk - 1), A(kk - 2));
+    }
+    if (r >= 0.0f) return r * flx5(A(kk - 3), A(kk - 2), A(kk - 1), A(kk), A(kk + 1));
+    return r * flx3(A(kk + 1), A(kk), A(kk - 1));
+  }
+  // WENO: lower-order pieces at 2 and nk are common to both forms
+  if (kk == 2) {
+    if (r >= 0.0f) return r * (c1k * A(kk - 1) + c2k * A(kk));
+    return r * upstrpd(A(kk + 1), A(kk), A(kk - 1), weps);
+  }
+  if (kk == nk) {
+    if (r > 0.0f) return r * upstrpd(A(kk - 2), A(kk - 1), A(kk), weps);
+    return r * (c1k * A(kk - 1) + c2k * A(kk));
+  }
+  if (pdefweno == 1) {
+    // vadv_weno5 pdef form (adv_routines.F:2386-2421) then vadv_lwr_weno_35_b
+    if (kk == 3 && r > 0.0f) return r * upstrpd(A(kk - 2), A(kk - 1), A(kk), weps);
+    if (kk == nk - 1 && r < 0.0f) return r * upstrpd(A(kk + 1), A(kk), A(kk - 1), weps);
+    float s1, s2, s3, s4, s5;
+    if (r >= 0.0f) { s1 = A(kk - 3); s2 = A(kk - 2); s3 = A(kk - 1); s4 = A(kk); s5 = A(kk + 1); }
+    else { s1 = A(kk + 2); s2 = A(kk + 1); s3 = A(kk); s4 = A(kk - 1); s5 = A(kk - 2); }
+    bool doit = absmax5(s1, s2, s3, s4, s5) > (float)weps;
+    return doit ? r * weno5(s1, s2, s3, s4, s5, weps) : 0.0f;
+  }
+  if (kk >= 4 && kk <= nk - 2) {
+    if (r >= 0.0f) return r * weno5(A(kk - 3), A(kk - 2), A(kk - 1), A(kk), A(kk + 1), weps);
+    return r * weno5(A(kk + 2), A(kk + 1), A(kk), A(kk - 1), A(kk - 2), weps);
+  }
+  if (kk == 3) {
+    if (r >= 0.0f) return r * upstrpd(A(kk - 2), A(kk - 1), A(kk), weps);
+    return r * weno5(A(kk + 2), A(kk + 1), A(kk), A(kk - 1), A(kk - 2), weps);
+  }
+  if (r >= 0.0f) return r * weno5(A(kk - 3), A(kk - 2), A(kk - 1), A(kk), A(kk + 1), weps);
+  return r * upstrpd(A(kk + 1), A(kk), A(kk - 1), weps);
+}
+
+struct AdvParts { float advx, advy, advz; };
+
+// advx/advy/advz of one cell with the open-bc inflow fix-ups (adv.F:129-335, 451-577)
+__device__ __forceinline__ AdvParts advs_parts(const DGrid &g, const SAdv &a, int i, int j, int k,
+                                               int weno, int pdef, int pdefweno, double weps) {
+  const int ni = g.ni, nj = g.nj, nk = g.nk;
+  const bool doitw = (g.wbc == 2 && g.ibw), doite = (g.ebc == 2 && g.ibe);
+  const bool doits = (g.sbc == 2 && g.ibs), doitn = (g.nbc == 2 && g.ibn);
+  float fx0 = sflux_x(g, a, i, j, k, weno, pdef, weps), fxp = sflux_x(g, a, i + 1, j, k, weno, pdef, weps);
+  if (doitw && i == 1 && FU(g, a, 1, j, k) >= 0.0f) fx0 = fxp;
+  if (doite && i == ni && FU(g, a, ni + 1, j, k) <= 0.0f) fxp = fx0;
+  float fy0 = sflux_y(g, a, i, j, k, weno, pdef, weps), fyp = sflux_y(g, a, i, j + 1, k, weno, pdef, weps);
+  if (doits && j == 1 && FV(g, a, i, 1, k) >= 0.0f) fy0 = fyp;
+  if (doitn && j == nj && FV(g, a, i, nj + 1, k) <= 0.0f) fyp = fy0;
+  AdvParts p;
+  p.advx = -(fxp - fx0) * g.rdx * LDG(&g.uh[i - g.ib]);
+  p.advy = -(fyp - fy0) * g.rdy * LDG(&g.vh[j - g.jb]);
+  float sc = sval(g, a, i, j, k);
+  if (doitw && i == 1 && FU(g, a, 1, j, k) >= 0.0f)
+    p.advx = p.advx - sc * (FU(g, a, 2, j, k) - FU(g, a, 1, j, k)) * g.rdx * LDG(&g.uh[1 - g.ib]);
+  if (doite && i == ni && FU(g, a, ni + 1, j, k) <= 0.0f)
+    p.advx = p.advx - sc * (FU(g, a, ni + 1, j, k) - FU(g, a, ni, j, k)) * g.rdx * LDG(&g.uh[ni - g.ib]);
+  if (doits && j == 1 && FV(g, a, i, 1, k) >= 0.0f)
+    p.advy = p.advy - sc * (FV(g, a, i, 2, k) - FV(g, a, i, 1, k)) * g.rdy * LDG(&g.vh[1 - g.jb]);
+  if (doitn && j == nj && FV(g, a, i, nj + 1, k) <= 0.0f)
+    p.advy = p.advy - sc * (FV(g, a, i, nj + 1, k) - FV(g, a, i, nj, k)) * g.rdy * LDG(&g.vh[nj - g.jb]);
+  const float mhk = LDG(&g.mh[k]);
+  if (k == 1) p.advz = -sflux_z(g, a, i, j, 2, weno, pdefweno, weps) * g.rdz * mhk;
+  else if (k == nk) p.advz = +sflux_z(g, a, i, j, nk, weno, pdefweno, weps) * g.rdz * mhk;
+  else p.advz = -(sflux_z(g, a, i, j, k + 1, weno, pdefweno, weps) - sflux_z(g, a, i, j, k, weno, pdefweno, weps)) * g.rdz * mhk;
+  return p;
+}
+
+// Non-pdef scalar pass: sten_out = sten_in + (adv + s*divx)*rr0, and when
+// snew is given, snew = s0 + dt*sten_out with the smeps flush (solve2.F:1419-1425).
+__global__ void k_advs(DGrid g, SAdv a, const float *sten_in,
+                       float *sten_out, float *__restrict__ snew, const float *__restrict__ sbase,
+                       int weno, int pdefweno, double weps, float dt, int flush) {
+  const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = 1 + (int)blockIdx.y, k = 1 + (int)blockIdx.z;
+  if (i > g.ni) return;
+  AdvParts p = advs_parts(g, a, i, j, k, weno, 0, pdefweno, weps);
+  long o = iS(g, i, j, k);
+  float ten = sten_in[o];
+  if (a.thterm) ten = ten - RAWDIV(g, a, i, j, k) * LDG(&a.thterm[o]);
+  ten = ten + (((p.advx + p.advy) + p.advz) + sval(g, a, i, j, k) * SDIV(g, a, i, j, k)) * LDG(&g.rr0[k]);
+  if (sten_out) sten_out[o] = ten;
+  if (snew) {
+    float v = LDG(&sbase[o]) + dt * ten;
+    if (flush && fabsf(v) < g.smeps) v = 0.0f;
+    snew[o] = v;
+  }
+}
+
+// pdef pass 1: advx/advy/advz and the provisional masses of pdefx1/y1/z
+// (pdef.F:35-102, 289-340, 478-496).
+__global__ void k_advs_pdef1(DGrid g, SAdv a, float *__restrict__ advx, float *__restrict__ advy, float *__restrict__ advz,
+                             float *__restrict__ dumx, float *__restrict__ dumy, float *__restrict__ dumz,
+                             int weno, int pdefweno, double weps, float dt) {
+  const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = 1 + (int)blockIdx.y, k = 1 + (int)blockIdx.z;
+  if (i > g.ni) return;
+  const int ni = g.ni, nj = g.nj;
+  AdvParts p = advs_parts(g, a, i, j, k, weno, 1, pdefweno, weps);
+  long o = iS(g, i, j, k);
+  advx[o] = p.advx; advy[o] = p.advy; advz[o] = p.advz;
+  const float s = sval(g, a, i, j, k), s0 = LDG(&a.s0[o]), r0k = LDG(&g.rho0[k]);
+  float dx = r0k * s0 + dt * (p.advx + s * (FU(g, a, i + 1, j, k) - FU(g, a, i, j, k)) * g.rdx * LDG(&g.uh[i - g.ib]));
+  if (g.wbc == 2 && g.ibw && i == 1 && FU(g, a, 1, j, k) >= 0.0f) dx = r0k * s0;
+  if (g.ebc == 2 && g.ibe && i == ni && FU(g, a, ni + 1, j, k) <= 0.0f) dx = r0k * s0;
+  float dy = r0k * s0 + dt * (p.advy + s * (FV(g, a, i, j + 1, k) - FV(g, a, i, j, k)) * g.rdy * LDG(&g.vh[j - g.jb]));
+  if (g.sbc == 2 && g.ibs && j == 1 && FV(g, a, i, 1, k) >= 0.0f) dy = r0k * s0;
+  if (g.nbc == 2 && g.ibn && j == nj && FV(g, a, i, nj + 1, k) <= 0.0f) dy = r0k * s0;
+  float dz = r0k * s0 + dt * (p.advz + s * (FW(g, a, i, j, k + 1) - FW(g, a, i, j, k)) * g.rdz * LDG(&g.mh[k]));
+  dumx[o] = dx; dumy[o] = dy; dumz[o] = dz;
+}
+
+// Mass moved into point c by the pdef scatter of pdefx2/pdefy2/pdefz
+// (pdef.F:158-174), gathered in the scatter's loop order: contribution from
+// the lower neighbour, then the point itself, then the upper neighbour.
+__device__ __forceinline__ void pdef_gather(float dm2, float dm1, float d0, float dp1, float dp2, float smeps,
+                                            float *mass, bool *flag) {
+  float m = 0.0f;
+  bool f = false;
+  if (dm1 < 0.0f) {  // the point below scatters: we are its upper neighbour
+    float foo1 = fmaxf(0.0f, dm2), foo2 = fmaxf(0.0f, d0);
+    if (foo1 + foo2 > smeps) {
+      float foo3 = fmaxf(dm1, -(foo1 + foo2)) / (foo1 + foo2);
+      m = m + foo2 * foo3;
+      if (d0 > smeps) f = true;
+    }
+  }
+  if (d0 < 0.0f) {
+    float foo1 = fmaxf(0.0f, dm1), foo2 = fmaxf(0.0f, dp1);
+    if (foo1 + foo2 > smeps) {
+      float foo3 = fmaxf(d0, -(foo1 + foo2)) / (foo1 + foo2);
+      m = m - (foo1 + foo2) * foo3;
+      f = true;
+    }
+  }
+  if (dp1 < 0.0f) {
+    float foo1 = fmaxf(0.0f, d0), foo2 = fmaxf(0.0f, dp2);
+    if (foo1 + foo2 > smeps) {
+      float foo3 = fmaxf(dp1, -(foo1 + foo2)) / (foo1 + foo2);
+      m = m + foo1 * foo3;
+      if (d0 > smeps) f = true;
+    }
+  }
+  *mass = m; *flag = f;
+}
+
+// pdef pass 2: pdefz, pdefx2, pdefy2 fixes (pdef.F:117-264, 358-454,
+// 459-581) and the tendency/update of adv.F:650-659 + solve2.F:1513-1520.
+// dumx/dumy carry halo values filled by the lateral bc (pdef.F:102, 338).
+__global__ void k_advs_pdef2(DGrid g, SAdv a, const float *__restrict__ advx, const float *__restrict__ advy,
+                             const float *__restrict__ advz, const float *__restrict__ dumx,
+                             const float *__restrict__ dumy, const float *__restrict__ dumz,
+                             const float *sten_in, float *sten_out, float *__restrict__ snew,
+                             const float *__restrict__ sbase, float dt, int flush) {
+  const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = 1 + (int)blockIdx.y, k = 1 + (int)blockIdx.z;
+  if (i > g.ni) return;
+  const int nk = g.nk;
+  const float smeps = g.smeps, rdt = 1.0f / dt;
+  long o = iS(g, i, j, k);
+  const float s = sval(g, a, i, j, k), s0 = LDG(&a.s0[o]), r0k = LDG(&g.rho0[k]);
+  float m; bool f;
+  // z (pdefz): dum(0)=dum(nk+1)=0
+  auto DZ = [&](int kk) { return (kk < 1 || kk > nk) ? 0.0f : LDG(&dumz[iS(g, i, j, kk)]); };
+  float az = LDG(&advz[o]);
+  pdef_gather(DZ(k - 2), DZ(k - 1), DZ(k), DZ(k + 1), DZ(k + 2), smeps, &m, &f);
+  if (f) az = (DZ(k) + m - r0k * s0) * rdt - s * (FW(g, a, i, j, k + 1) - FW(g, a, i, j, k)) * g.rdz * LDG(&g.mh[k]);
+  // x (pdefx2)
+  auto DX = [&](int ii) { return LDG(&dumx[iS(g, ii, j, k)]); };
+  float ax = LDG(&advx[o]);
+  pdef_gather(DX(i - 2), DX(i - 1), DX(i), DX(i + 1), DX(i + 2), smeps, &m, &f);
+  if (f) ax = (DX(i) + m - r0k * s0) * rdt - s * (FU(g, a, i + 1, j, k) - FU(g, a, i, j, k)) * g.rdx * LDG(&g.uh[i - g.ib]);
+  // y (pdefy2)
+  auto DY = [&](int jj) { return LDG(&dumy[iS(g, i, jj, k)]); };
+  float ay = LDG(&advy[o]);
+  pdef_gather(DY(j - 2), DY(j - 1), DY(j), DY(j + 1), DY(j + 2), smeps, &m, &f);
+  if (f) ay = (DY(j) + m - r0k * s0) * rdt - s * (FV(g, a, i, j + 1, k) - FV(g, a, i, j, k)) * g.rdy * LDG(&g.vh[j - g.jb]);
+  float ten = sten_in[o] + (((ax + ay) + az) + s * SDIV(g, a, i, j, k)) * LDG(&g.rr0[k]);
+  if (sten_out) sten_out[o] = ten;
+  if (snew) {
+    float v = LDG(&sbase[o]) + dt * ten;
+    if (flush && fabsf(v) < g.smeps) v = 0.0f;
+    snew[o] = v;
+  }
+}
+
+void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, int64_t *nlaunch);
+
+// One advs call + RK update.  s = field (full halo), s0 = RK base,
+// ten1 = fixed tendency.  pdef selects the two-pass positive-definite form.
+// scratch must hold 6 s-arrays when pdef is set.
+void launch_advs(const DGrid &g, const float *rru, const float *rrv, const float *rrw, int weighted,
+                 const float *divx, const float *s, const float *s0, int sadd, const float *ten1,
+                 const float *thterm, float *sten_out, float *snew, int weno, int pdef, int pdefweno,
+                 double weps, float dt, int flush, float *scratch, cudaStream_t st, int64_t *nl) {
+  SAdv a{rru, rrv, rrw, s, s0, divx, thterm, weighted, sadd};
+  const int bx = 128;
+  dim3 grid((g.ni + bx - 1) / bx, g.nj, g.nk);
+  if (!pdef) {
+    { ProfScope _ps("k_advs", st); k_advs<<<grid, bx, 0, st>>>(g, a, ten1, sten_out, snew, s0, weno, pdefweno, weps, dt, flush); }
+    if (nl) *nl += 1;
+    return;
+  }
+  long n = nS(g);
+  float *advx = scratch, *advy = scratch + n, *advz = scratch + 2 * n;
+  float *dumx = scratch + 3 * n, *dumy = scratch + 4 * n, *dumz = scratch + 5 * n;
+  { ProfScope _ps("k_advs_pdef1", st); k_advs_pdef1<<<grid, bx, 0, st>>>(g, a, advx, advy, advz, dumx, dumy, dumz, weno, pdefweno, weps, dt); }
+  launch_bc(g, dumx, 1, 0, st, nl);
+  launch_bc(g, dumy, 1, 0, st, nl);
+  { ProfScope _ps("k_advs_pdef2", st); k_advs_pdef2<<<grid, bx, 0, st>>>(g, a, advx, advy, advz, dumx, dumy, dumz, ten1, sten_out, snew, s0, dt, flush); }
+  if (nl) *nl += 2;
+}
+
+}  // namespace cm1g

@@ -1,0 +1,389 @@
+// k_misc.cu -- the remaining pieces of the large step: per-stage thermodynamic
+// set-up, pressure/density with the dry-air mass fix (FP64 reductions),
+// open-boundary phase speeds, CFL, the positive-definite column fix, the
+// end-of-step rollover and the domain diagnostics.
+#include "cm1g_common.cuh"
+
+namespace cm1g {
+
+// ---------------------------------------------------------------------
+// stage set-up: theta_rho (t11), ppterm (t22), thterm (solve2.F:313-446)
+// on the interior and piadv = pi0+pp' on 0..ni+1 x 0..nj+1 (solve2.F:1027-1038)
+// ---------------------------------------------------------------------
+__global__ void k_stage_prep(DGrid g, const float *__restrict__ th3d, const float *__restrict__ pp3d,
+                             const float *__restrict__ qv, int imoist, int eqtset,
+                             float *__restrict__ t11, float *__restrict__ t22, float *__restrict__ thterm,
+                             float *__restrict__ piadv) {
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);       // 0..ni+1
+  const int j = (int)blockIdx.y;                                     // 0..nj+1
+  const int k = 1 + (int)blockIdx.z;
+  if (i > g.ni + 1) return;
+  const long o = iS(g, i, j, k);
+  const float pp = LDG(&pp3d[o]);
+  piadv[o] = LDG(&g.pi0[k]) + pp;
+  if (i < 1 || i > g.ni || j < 1 || j > g.nj) return;
+  const Consts &c = g.c;
+  const float th3 = LDG(&th3d[o]), th0 = LDG(&g.th0[k]), pi0 = LDG(&g.pi0[k]);
+  if (imoist) {
+    const float q = fmaxf(LDG(&qv[o]), 0.0f);
+    const float d2 = 0.0f, d3 = 0.0f;   // water vapour only: no liquid or ice arrays
+    const float qli = fmaxf(0.0f, d2 + d3);
+    t11[o] = (th0 + th3) * (1.0f + c.reps * q) / ((1.0f + q) + qli);
+    if (eqtset == 2) {
+      const float cpli = c.cpl * fmaxf(0.0f, d2) + c.cpi * fmaxf(0.0f, d3);
+      const float cpm = (c.cp + c.cpv * q) + cpli;
+      const float cvm = 1.0f / ((c.cv + c.cvv * q) + cpli);
+      thterm[o] = (th0 + th3) * ((c.rd + c.rv * q) - c.rovcp * cpm) * cvm;
+      t22[o] = (pi0 + pp) * c.rovcp * cpm * cvm;
+    } else {
+      t22[o] = (pi0 + pp) * c.rddcv;
+    }
+  } else {
+    t11[o] = th0 + th3;
+    t22[o] = (pi0 + pp) * c.rddcv;
+  }
+}
+
+void launch_stage_prep(const DGrid &g, const float *th3d, const float *pp3d, const float *qv, int imoist, int eqtset,
+                       float *t11, float *t22, float *thterm, float *piadv, cudaStream_t st, int64_t *nl) {
+  dim3 grid((g.ni + 2 + 127) / 128, g.nj + 2, g.nk);
+  // j index offset: blockIdx.y = j directly (0..nj+1)
+  { ProfScope _ps("k_stage_prep", st); k_stage_prep<<<grid, 128, 0, st>>>(g, th3d, pp3d, qv, imoist, eqtset, t11, t22, thterm, piadv); }
+  if (nl) *nl += 1;
+}
+
+// ---------------------------------------------------------------------
+// radbcew4 / radbcns4 (bc.F:2054-2178): column-averaged phase speeds
+// ---------------------------------------------------------------------
+__global__ void k_radbc4(DGrid g, const float *__restrict__ ua, const float *__restrict__ u3d,
+                         const float *__restrict__ va, const float *__restrict__ v3d,
+                         float *radbcw, float *radbce, float *radbcs, float *radbcn, float dt) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int side = (int)blockIdx.y;   // 0 w, 1 e, 2 s, 3 n
+  const int ni = g.ni, nj = g.nj, nk = g.nk;
+  const float umax = 350.0f;          // csmax, constants.F:45
+  if (side <= 1) {
+    const int j = 1 + t;
+    if (j > nj) return;
+    if (side == 0 && !(g.ibw && g.wbc == 2)) return;
+    if (side == 1 && !(g.ibe && g.ebc == 2)) return;
+    const int ia = (side == 0) ? 2 : ni, ib2 = (side == 0) ? 3 : ni - 1;
+    const float ruf = LDG(&g.ruf[ia - g.ib]);
+    float avg = 0.0f;
+    for (int k = 1; k <= nk; k++) {
+      float foo = (side == 0) ? (ua[iU(g, ib2, j, k)] - ua[iU(g, ia, j, k)]) : (ua[iU(g, ia, j, k)] - ua[iU(g, ib2, j, k)]);
+      float cb = g.dx * ruf * (ua[iU(g, ia, j, k)] - u3d[iU(g, ia, j, k)]) / (dt * (copysignf(1.e-10f, foo) + foo));
+      cb = (side == 0) ? fmaxf(fminf(cb, 0.0f), -umax) : fminf(fmaxf(cb, 0.0f), umax);
+      avg = avg + cb;
+    }
+    avg = avg / (float)nk;
+    float *r = (side == 0) ? radbcw : radbce;
+    for (int k = 1; k <= nk; k++) r[(j - g.jb) + (long)g.NJ * k] = avg;
+  } else {
+    const int i = 1 + t;
+    if (i > ni) return;
+    if (side == 2 && !(g.ibs && g.sbc == 2)) return;
+    if (side == 3 && !(g.ibn && g.nbc == 2)) return;
+    const int ja = (side == 2) ? 2 : nj, jb2 = (side == 2) ? 3 : nj - 1;
+    const float rvf = LDG(&g.rvf[ja - g.jb]);
+    float avg = 0.0f;
+    for (int k = 1; k <= nk; k++) {
+      float foo = (side == 2) ? (va[iV(g, i, jb2, k)] - va[iV(g, i, ja, k)]) : (va[iV(g, i, ja, k)] - va[iV(g, i, jb2, k)]);
+      float cb = g.dy * rvf * (va[iV(g, i, ja, k)] - v3d[iV(g, i, ja, k)]) / (dt * (copysignf(1.e-10f, foo) + foo));
+      cb = (side == 2) ? fmaxf(fminf(cb, 0.0f), -umax) : fminf(fmaxf(cb, 0.0f), umax);
+      avg = avg + cb;
+    }
+    avg = avg / (float)nk;
+    float *r = (side == 2) ? radbcs : radbcn;
+    for (int k = 1; k <= nk; k++) r[(i - g.ib) + (long)g.NI * k] = avg;
+  }
+}
+
+void launch_radbc4(const DGrid &g, const float *ua, const float *u3d, const float *va, const float *v3d,
+                   float *rw, float *re, float *rs, float *rn, float dt, cudaStream_t st, int64_t *nl) {
+  int n = g.ni > g.nj ? g.ni : g.nj;
+  dim3 grid((n + 127) / 128, 4);
+  { ProfScope _ps("k_radbc4", st); k_radbc4<<<grid, 128, 0, st>>>(g, ua, u3d, va, v3d, rw, re, rs, rn, dt); }
+  if (nl) *nl += 1;
+}
+
+// ---------------------------------------------------------------------
+// pressure and density (solve2.F:1580-1606) with the per-level FP64
+// sums of apmasscon (solve2.F:1617-1648).  Block (x, k) covers a chunk of
+// level k and writes its partial sums; k_masscon_finish adds them in a
+// fixed order.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ void prs_rho(const DGrid &g, float pp, float th3, const float *qv, long o, int k,
+                                        int imoist, float *prs, float *rho) {
+  const Consts &c = g.c;
+  const float pi = LDG(&g.pi0[k]) + pp;
+  const float pr = 1.0e5f * powf(pi, c.cpdrd);
+  prs[o] = pr;
+  if (imoist) rho[o] = pr / ((LDG(&g.th0[k]) + th3) * pi * (c.rd + fmaxf(0.0f, LDG(&qv[o])) * c.rv));
+  else rho[o] = pr / (c.rd * (LDG(&g.th0[k]) + th3) * pi);
+}
+
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double *red) {
+  const int t = threadIdx.x;
+  red[t] = v;
+  __syncthreads();
+  for (int s = NT / 2; s > 0; s >>= 1) {
+    if (t < s) red[t] = red[t] + red[t + s];
+    __syncthreads();
+  }
+  double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+static const int PR_NT = 256, PR_PER = 8;
+
+__global__ void __launch_bounds__(PR_NT) k_prs_rho(DGrid g, const float *__restrict__ pp3d, const float *__restrict__ th3d,
+                                                   const float *__restrict__ qv, int imoist, float *prs, float *rho,
+                                                   double *part3, double *part4, int nchunk, int do_sums) {
+  __shared__ double red[PR_NT];
+  const int k = 1 + (int)blockIdx.y;
+  const long npl = (long)g.ni * g.nj;
+  const long base = (long)blockIdx.x * PR_NT * PR_PER;
+  double s3 = 0.0, s4 = 0.0;
+  for (int r = 0; r < PR_PER; r++) {
+    long t = base + (long)r * PR_NT + threadIdx.x;
+    if (t >= npl) break;
+    int i = 1 + (int)(t % g.ni), j = 1 + (int)(t / g.ni);
+    long o = iS(g, i, j, k);
+    float pp = LDG(&pp3d[o]);
+    prs_rho(g, pp, LDG(&th3d[o]), qv, o, k, imoist, prs, rho);
+    if (do_sums) {
+      s3 = s3 + (double)(rho[o] * LDG(&g.ruh[i - g.ib]) * LDG(&g.rvh[j - g.jb]) * LDG(&g.rmh[k]));
+      s4 = s4 + (double)(LDG(&g.pi0[k]) + pp);
+    }
+  }
+  if (!do_sums) return;
+  s3 = block_sum<PR_NT>(s3, red);
+  s4 = block_sum<PR_NT>(s4, red);
+  if (threadIdx.x == 0) {
+    part3[(long)k * nchunk + blockIdx.x] = s3;
+    part4[(long)k * nchunk + blockIdx.x] = s4;
+  }
+}
+
+// mass2, tem (solve2.F:1985-2000); dev[0] = mass2, dev[1] = p2, devf[0] = tem
+__global__ void k_masscon_finish(DGrid g, const double *part3, const double *part4, int nchunk, double mass1,
+                                 double *dev, float *devf) {
+  __shared__ double red[128];
+  double t3 = 0.0, t4 = 0.0;
+  for (int k = 1 + (int)threadIdx.x; k <= g.nk; k += blockDim.x) {
+    double a = 0.0, b = 0.0;
+    for (int c = 0; c < nchunk; c++) { a = a + part3[(long)k * nchunk + c]; b = b + part4[(long)k * nchunk + c]; }
+    t3 = t3 + a; t4 = t4 + b;
+  }
+  t3 = block_sum<128>(t3, red);
+  t4 = block_sum<128>(t4, red);
+  if (threadIdx.x == 0) {
+    double mass2 = t3, p2 = t4;
+    double n = (double)((long long)g.ni * g.nj * g.nk);
+    dev[0] = mass2; dev[1] = p2;
+    devf[0] = (float)((pow(mass1 / mass2, (double)g.c.rddcv) - 1.0) * p2 / n);
+  }
+}
+
+__global__ void k_masscon_apply(DGrid g, float *pp3d, const float *__restrict__ th3d, const float *__restrict__ qv,
+                                int imoist, float *prs, float *rho, const float *devf) {
+  const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = 1 + (int)blockIdx.y, k = 1 + (int)blockIdx.z;
+  if (i > g.ni) return;
+  const long o = iS(g, i, j, k);
+  const float tem = devf[0];
+  const float pp = pp3d[o] + tem;
+  pp3d[o] = pp;
+  prs_rho(g, pp, LDG(&th3d[o]), qv, o, k, imoist, prs, rho);
+}
+
+int prs_nchunk(const DGrid &g) { return (int)(((long)g.ni * g.nj + PR_NT * PR_PER - 1) / (PR_NT * PR_PER)); }
+
+void launch_prs_rho(const DGrid &g, const float *pp3d, const float *th3d, const float *qv, int imoist,
+                    float *prs, float *rho, double *part3, double *part4, int do_sums, cudaStream_t st, int64_t *nl) {
+  int nchunk = prs_nchunk(g);
+  dim3 grid(nchunk, g.nk);
+  { ProfScope _ps("k_prs_rho", st); k_prs_rho<<<grid, PR_NT, 0, st>>>(g, pp3d, th3d, qv, imoist, prs, rho, part3, part4, nchunk, do_sums); }
+  if (nl) *nl += 1;
+}
+
+void launch_masscon(const DGrid &g, float *pp3d, const float *th3d, const float *qv, int imoist, float *prs,
+                    float *rho, const double *part3, const double *part4, double mass1, double *dev, float *devf,
+                    cudaStream_t st, int64_t *nl) {
+  { ProfScope _ps("k_masscon_finish", st); k_masscon_finish<<<1, 128, 0, st>>>(g, part3, part4, prs_nchunk(g), mass1, dev, devf); }
+  dim3 grid((g.ni + 127) / 128, g.nj, g.nk);
+  { ProfScope _ps("k_masscon_apply", st); k_masscon_apply<<<grid, 128, 0, st>>>(g, pp3d, th3d, qv, imoist, prs, rho, devf); }
+  if (nl) *nl += 2;
+}
+
+// ---------------------------------------------------------------------
+// calccflquick (misclibs.F:2726-2814): max Courant number, stored as the
+// bits of a non-negative float so atomicMax on int orders it correctly.
+// ---------------------------------------------------------------------
+__global__ void k_cfl(DGrid g, const float *__restrict__ u, const float *__restrict__ v, const float *__restrict__ w,
+                      float dt, int *out) {
+  const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = 1 + (int)blockIdx.y, k = 1 + (int)blockIdx.z;
+  float wsp = 0.0f;
+  if (i <= g.ni) {
+    const float dtdx = 0.5f * dt * g.rdx, dtdy = 0.5f * dt * g.rdy, dtdz = 0.5f * dt * g.rdz;
+    float a1 = (LDG(&u[iU(g, i, j, k)]) + LDG(&u[iU(g, i + 1, j, k)])) * dtdx * LDG(&g.uh[i - g.ib]);
+    float a2 = (LDG(&v[iV(g, i, j, k)]) + LDG(&v[iV(g, i, j + 1, k)])) * dtdy * LDG(&g.vh[j - g.jb]);
+    float a3 = (LDG(&w[iW(g, i, j, k)]) + LDG(&w[iW(g, i, j, k + 1)])) * dtdz * LDG(&g.mh[k]);
+    wsp = sqrtf((a1 * a1 + a2 * a2) + a3 * a3);
+    if (!(wsp <= 3.0e38f)) wsp = INFINITY;   // NaN/Inf velocity: reported as an error by the host
+  }
+  for (int s = 16; s > 0; s >>= 1) wsp = fmaxf(wsp, __shfl_xor_sync(0xffffffffu, wsp, s));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_int(wsp));
+}
+
+void launch_cfl(const DGrid &g, const float *u, const float *v, const float *w, float dt, int *out,
+                cudaStream_t st, int64_t *nl) {
+  cudaMemsetAsync(out, 0, sizeof(int), st);
+  dim3 grid((g.ni + 127) / 128, g.nj, g.nk);
+  { ProfScope _ps("k_cfl", st); k_cfl<<<grid, 128, 0, st>>>(g, u, v, w, dt, out); }
+  if (nl) *nl += 1;
+}
+
+// ---------------------------------------------------------------------
+// pdefq (misclibs.F:1037-1117), pdscheme=1: per-column mass-conserving
+// clipping.  bud[j*ni+i-1] receives a2-a1 of the column.
+// ---------------------------------------------------------------------
+__global__ void k_pdefq(DGrid g, float rmax, const float *__restrict__ rho, float *q, double *bud) {
+  const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = 1 + (int)blockIdx.y;
+  if (i > g.ni) return;
+  const float ruh = LDG(&g.ruh[i - g.ib]), rvh = LDG(&g.rvh[j - g.jb]);
+  double t1 = 0.0, t2 = 0.0, a1 = 0.0, a2 = 0.0;
+  for (int k = 1; k <= g.nk; k++) {
+    const long o = iS(g, i, j, k);
+    const float r = LDG(&rho[o]), rmh = LDG(&g.rmh[k]);
+    float qq = q[o];
+    t1 = t1 + (double)(r * qq);
+    a1 = a1 + (double)(r * qq * ruh * rvh * rmh);
+    if (qq < rmax) { qq = 0.0f; q[o] = qq; }
+    t2 = t2 + (double)(r * qq);
+  }
+  double t3 = (t1 + 1.0e-20) / (t2 + 1.0e-20);
+  if (t3 < 0.0) t3 = 1.0;
+  for (int k = 1; k <= g.nk; k++) {
+    const long o = iS(g, i, j, k);
+    const float r = LDG(&rho[o]), rmh = LDG(&g.rmh[k]);
+    float qq = (float)(t3 * (double)q[o]);
+    q[o] = qq;
+    a2 = a2 + (double)(r * qq * ruh * rvh * rmh);
+  }
+  bud[(long)(j - 1) * g.ni + (i - 1)] = a2 - a1;
+}
+
+// budget: asq += sum_j (sum_i bud) * dx*dy*dz, fixed order
+__global__ void k_pdefq_budget(DGrid g, const double *bud, double *asq) {
+  __shared__ double red[128];
+  double s = 0.0;
+  for (int j = 1 + (int)threadIdx.x; j <= g.nj; j += blockDim.x) {
+    double bj = 0.0;
+    for (int i = 0; i < g.ni; i++) bj = bj + bud[(long)(j - 1) * g.ni + i];
+    s = s + bj * (double)(g.dx * g.dy * g.dz);
+  }
+  s = block_sum<128>(s, red);
+  if (threadIdx.x == 0) asq[0] = asq[0] + s;
+}
+
+void launch_pdefq(const DGrid &g, float rmax, const float *rho, float *q, double *bud, double *asq,
+                  cudaStream_t st, int64_t *nl) {
+  dim3 grid((g.ni + 127) / 128, g.nj);
+  { ProfScope _ps("k_pdefq", st); k_pdefq<<<grid, 128, 0, st>>>(g, rmax, rho, q, bud); }
+  { ProfScope _ps("k_pdefq_budget", st); k_pdefq_budget<<<1, 128, 0, st>>>(g, bud, asq); }
+  if (nl) *nl += 2;
+}
+
+// ---------------------------------------------------------------------
+// solve3 pieces: ppx = pp3d + ppx (solve3.F:276-283) and the rollover
+// copies over the reference's ranges (solve3.F:546-640).
+// ---------------------------------------------------------------------
+__global__ void k_ppx_update(DGrid g, const float *__restrict__ pp3d, float *ppx) {
+  const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = 1 + (int)blockIdx.y, k = 1 + (int)blockIdx.z;
+  if (i > g.ni) return;
+  const long o = iS(g, i, j, k);
+  ppx[o] = LDG(&pp3d[o]) + ppx[o];
+}
+
+// copy dst = src over i=lo..hi, j=lo..hij, k=1..nk of an array with
+// x-extent `pitch` and rows `nrow` (stag 1/2/3/4 layouts)
+__global__ void k_copy_range(long pitch, long plane, int ib, int jb, int ilo, int ihi, int jlo, int jhi, int nk,
+                             const float *__restrict__ src, float *__restrict__ dst) {
+  const int i = ilo + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = jlo + (int)blockIdx.y, k = 1 + (int)blockIdx.z;
+  if (i > ihi || j > jhi || k > nk) return;
+  const long o = (long)(i - ib) + pitch * (long)(j - jb) + plane * (long)k;
+  dst[o] = LDG(&src[o]);
+}
+
+void launch_ppx_update(const DGrid &g, const float *pp3d, float *ppx, cudaStream_t st, int64_t *nl) {
+  dim3 grid((g.ni + 127) / 128, g.nj, g.nk);
+  { ProfScope _ps("k_ppx_update", st); k_ppx_update<<<grid, 128, 0, st>>>(g, pp3d, ppx); }
+  if (nl) *nl += 1;
+}
+
+void launch_copy_range(const DGrid &g, int stag, int ilo, int ihi, int jlo, int jhi, const float *src, float *dst,
+                       cudaStream_t st, int64_t *nl) {
+  long pitch = (stag == 2) ? g.NI + 1 : g.NI;
+  long rows = (stag == 3) ? g.NJ + 1 : g.NJ;
+  dim3 grid((ihi - ilo + 1 + 127) / 128, jhi - jlo + 1, g.nk);
+  { ProfScope _ps("k_copy_range", st); k_copy_range<<<grid, 128, 0, st>>>(pitch, pitch * rows, g.ib, g.jb, ilo, ihi, jlo, jhi, g.nk, src, dst); }
+  if (nl) *nl += 1;
+}
+
+// ---------------------------------------------------------------------
+// calcmass (misclibs.F:3134-3191) and maxmin (maxmin.F:5-119)
+// ---------------------------------------------------------------------
+__global__ void k_level_mass(DGrid g, const float *__restrict__ rho, double *lev) {
+  __shared__ double red[256];
+  const int k = 1 + (int)blockIdx.x;
+  double s = 0.0;
+  for (long t = threadIdx.x; t < (long)g.ni * g.nj; t += blockDim.x) {
+    int i = 1 + (int)(t % g.ni), j = 1 + (int)(t / g.ni);
+    s = s + (double)(LDG(&rho[iS(g, i, j, k)]) * LDG(&g.ruh[i - g.ib]) * LDG(&g.rvh[j - g.jb]) * LDG(&g.rmh[k]));
+  }
+  s = block_sum<256>(s, red);
+  if (threadIdx.x == 0) lev[k] = s;
+}
+
+void launch_level_mass(const DGrid &g, const float *rho, double *lev, cudaStream_t st, int64_t *nl) {
+  { ProfScope _ps("k_level_mass", st); k_level_mass<<<g.nk, 256, 0, st>>>(g, rho, lev); }
+  if (nl) *nl += 1;
+}
+
+// max and min with the first (i fastest, then j, then k) location of each;
+// ties resolve to the lowest linear index as the serial loop does.
+__global__ void k_maxmin(DGrid g, const float *__restrict__ a, int stag, unsigned long long *omax,
+                         unsigned long long *omin) {
+  const int ie = g.ni + (stag == 2), je = g.nj + (stag == 3), ke = g.nk + (stag == 4);
+  const long n = (long)ie * je * ke;
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int i = 1 + (int)(t % ie), j = 1 + (int)((t / ie) % je), k = 1 + (int)(t / ((long)ie * je));
+  const long o = stag == 2 ? iU(g, i, j, k) : stag == 3 ? iV(g, i, j, k) : iS(g, i, j, k);
+  float v = LDG(&a[o]);
+  // order-preserving key: float bits mapped to unsigned, index in the low word
+  unsigned int b = __float_as_uint(v);
+  unsigned int key = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+  unsigned int idx = (unsigned int)t;
+  atomicMax(omax, ((unsigned long long)key << 32) | (unsigned long long)(0xffffffffu - idx));
+  atomicMin(omin, ((unsigned long long)key << 32) | (unsigned long long)idx);
+}
+
+void launch_maxmin(const DGrid &g, const float *a, int stag, unsigned long long *om, cudaStream_t st, int64_t *nl) {
+  const int ie = g.ni + (stag == 2), je = g.nj + (stag == 3), ke = g.nk + (stag == 4);
+  long n = (long)ie * je * ke;
+  cudaMemsetAsync(om, 0, sizeof(unsigned long long), st);
+  cudaMemsetAsync(om + 1, 0xff, sizeof(unsigned long long), st);
+  { ProfScope _ps("k_maxmin", st); k_maxmin<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, a, stag, om, om + 1); }
+  if (nl) *nl += 1;
+}
+
+}  // namespace cm1g

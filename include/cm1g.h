@@ -204,6 +204,14 @@ int cm1g_calcmass(cm1g_ctx_t *ctx, const float *rho, double *tmass);
 int cm1g_maxmin(cm1g_ctx_t *ctx, const float *a, int32_t stag,
                 float *amax, float *amin, int32_t loc[6]);
 
+/* Per-kernel device timing, the counterpart of the reference's timestats
+ * (src/input.F:359-387, cm1.F:4597-4689).  While enabled, every kernel launch
+ * is bracketed by CUDA events (graph replay is bypassed); entries are read
+ * back by index until the call returns an error. */
+int cm1g_profile(cm1g_ctx_t *ctx, int32_t enable);
+int cm1g_profile_read(cm1g_ctx_t *ctx, int32_t index, char *name, int32_t name_len,
+                      int64_t *launches, double *total_ms);
+
 #ifdef __cplusplus
 }
 #endif
