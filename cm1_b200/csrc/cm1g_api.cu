@@ -28,8 +28,9 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt, const float *ua
                   const float *va, float *v3d, const float *vten, const float *wa, float *w3d, const float *wten,
                   const float *ppi, float *pp3d, const float *piadv, const float *ppten, float *ppx,
                   const float *thv, const float *ppterm, float *rru, float *rrv, float *rrw, const float *radbcw,
-                  const float *radbce, const float *radbcs, const float *radbcn, float *su, float *sv, float *d1,
-                  float *d2, cudaStream_t st, int64_t *nl);
+                  const float *radbce, const float *radbcs, const float *radbcn, float *su, float *sv, float *su2,
+                  float *sv2, float *d1, float *d2, cudaStream_t st, int64_t *nl);
+int sound_max_nk();
 void launch_stage_prep(const DGrid &g, const float *th3d, const float *pp3d, const float *qv, int imoist, int eqtset,
                        float *t11, float *t22, float *thterm, float *piadv, cudaStream_t st, int64_t *nl);
 void launch_radbc4(const DGrid &g, const float *ua, const float *u3d, const float *va, const float *v3d,
@@ -123,7 +124,7 @@ struct cm1g_ctx {
   float *t11 = nullptr, *t22 = nullptr, *thterm = nullptr, *piadv = nullptr;
   float *uten = nullptr, *vten = nullptr, *wten = nullptr;
   float *rru = nullptr, *rrv = nullptr, *rrw = nullptr;
-  float *su = nullptr, *sv = nullptr, *d1 = nullptr, *d2 = nullptr;
+  float *su = nullptr, *sv = nullptr, *su2 = nullptr, *sv2 = nullptr, *d1 = nullptr, *d2 = nullptr;
   float *sx[2 * (1 + 2 * CM1G_MAXQ)] = {};   // per-scalar stage buffers
   float *pdefscr = nullptr;                   // 6 s-arrays
   float *sten = nullptr;                      // s-array for cm1g_advs-free use
@@ -195,6 +196,7 @@ extern "C" int cm1g_version(int32_t *major, int32_t *minor) {
 static int check_config(const cm1g_config_t *c) {
   if (c->ni < 4 || c->nj < 4 || c->nk < 6) return set_err(CM1G_ERR_ARG, "grid too small (ni,nj>=4, nk>=6)");
   if (c->ngxy < 3) return set_err(CM1G_ERR_ARG, "ngxy must be >= 3 for 5th order");
+  if (c->nk > sound_max_nk()) return set_err(CM1G_ERR_UNSUPPORTED, "nk > %d levels is not built", sound_max_nk());
   if (c->psolver != 3) return set_err(CM1G_ERR_UNSUPPORTED, "psolver=%d: only 3 (sound.F) is built", c->psolver);
   if (c->terrain_flag || c->axisymm || c->icor)
     return set_err(CM1G_ERR_UNSUPPORTED, "terrain, axisymmetric grids and Coriolis are not built");
@@ -292,6 +294,7 @@ extern "C" int cm1g_init(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_c
   c->uten = (float *)dalloc(c, bU); c->vten = (float *)dalloc(c, bV); c->wten = (float *)dalloc(c, bW);
   c->rru = (float *)dalloc(c, bU); c->rrv = (float *)dalloc(c, bV); c->rrw = (float *)dalloc(c, bW);
   c->su = (float *)dalloc(c, bU); c->sv = (float *)dalloc(c, bV);
+  c->su2 = (float *)dalloc(c, bU); c->sv2 = (float *)dalloc(c, bV);
   c->d1 = (float *)dalloc(c, bS); c->d2 = (float *)dalloc(c, bS);
   int nsc = 1 + (cfg->imoist ? cfg->numq : 0) + (cfg->iptra ? cfg->npt : 0);
   for (int s = 0; s < 2 * nsc; s++) c->sx[s] = (float *)dalloc(c, bS);
@@ -456,7 +459,7 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
                         th_in, qv_in, st, nl);
     launch_sound(g, cf.nsound, nrk, dt, d->ua, d->u3d, c->uten, d->va, d->v3d, c->vten, d->wa, d->w3d, c->wten,
                  d->ppi, d->pp3d, c->piadv, d->ppten, d->ppx, c->t11, c->t22, c->rru, c->rrv, c->rrw,
-                 d->radbcw, d->radbce, d->radbcs, d->radbcn, c->su, c->sv, c->d1, c->d2, st, nl);
+                 d->radbcw, d->radbce, d->radbcs, d->radbcn, c->su, c->sv, c->su2, c->sv2, c->d1, c->d2, st, nl);
     if (nrk == 3) launch_cfl(g, d->u3d, d->v3d, d->w3d, dt, c->cflbits, st, nl);
     if (openrad) launch_radbc4(g, d->ua, d->u3d, d->va, d->v3d, d->radbcw, d->radbce, d->radbcs, d->radbcn, dttmp, st, nl);
     const int weno = (cf.advwenos == 1 || (cf.advwenos == 2 && nrk == 3)) ? 1 : 0;
@@ -720,7 +723,8 @@ extern "C" int cm1g_sound(cm1g_ctx_t *c, int32_t nrk, float dt, float dttmp, flo
         *rn = S.in(radbcn, nrs, false);
   if (S.err) return set_err(CM1G_ERR_NOMEM, "staging");
   launch_sound(g, c->cfg.nsound, nrk, dt, dua, du3, dut, dva, dv3, dvt, dwa, dw3, dwt, dppi, dpp, dpia, dppt, dppx,
-               dthv, dppterm, dru, drv, drw, rw, re, rs, rn, c->su, c->sv, c->d1, c->d2, c->stream, &c->nlaunch);
+               dthv, dppterm, dru, drv, drw, rw, re, rs, rn, c->su, c->sv, c->su2, c->sv2, c->d1, c->d2, c->stream,
+               &c->nlaunch);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
   return S.finish();

@@ -1,16 +1,22 @@
 // k_sound.cu -- acoustic substeps of sound.F (psolver=3, no terrain).
 //
-// One kernel per small step.  A thread owns one (i,j) column and walks it
-// twice: upward it forms the new u, v (pressure-gradient update, sound.F:
-// 321-341, with the open-boundary updates of bc.F:2392-2686 folded in), the
-// explicit pi' forcing fpk (sound.F:479-502) and the forward elimination of
-// the vertically implicit w equation (sound.F:659-716); downward it
-// back-substitutes w (sound.F:718-733), updates pi' with divergence damping
-// (sound.F:746-760) and accumulates the small-step-averaged velocities
-// (sound.F:806-835).  The column recursion lives in shared memory.
+// One kernel launch per small step.  A block owns a tile of TX consecutive
+// columns (i) of one row (j), all levels, and works in three phases:
+//
+//  1. point-parallel (warp w takes levels w+1, w+1+NW, ...; lanes run along
+//     i so every global access is a coalesced row segment): new u and v by
+//     the pressure-gradient update (sound.F:321-341) with the open-boundary
+//     updates of bc.F:2392-2686 folded in, the running sums of u and v
+//     (sound.F:806-835), the explicit pi' forcing fpk (sound.F:479-502), and
+//     the per-level pieces of the implicit w equation, kept in shared memory;
+//  2. column-sequential (one thread per column): the Thomas forward
+//     elimination and back substitution of sound.F:659-733, entirely in
+//     shared memory, with the reference's operation order;
+//  3. point-parallel again: pi' update with divergence damping
+//     (sound.F:746-760), new w and the averaged w.
 //
 // Neighbour columns read u, v and ppd from the previous small step, so u, v
-// and ppd are double-buffered; w and pi' are only read by their own column
+// and ppd are double-buffered; w and pi' are read only by their own column
 // and are updated in place.  The east/north face velocity of a cell is
 // recomputed from the same old values by the neighbour that needs it, which
 // reproduces the stored value exactly.
@@ -43,163 +49,196 @@ struct SoundStep {
 #define RJK(g, a, j, k) ((a)[((j) - (g).jb) + (long)(g).NJ * (k)])
 #define RIK(g, a, i, k) ((a)[((i) - (g).ib) + (long)(g).NI * (k)])
 
-template <int NT>
-__global__ void __launch_bounds__(NT) k_sound_step(DGrid g, SoundIO io, SoundStep p) {
+static const int SND_TX = 32;     // columns per tile (one warp wide)
+static const int SND_NW = 8;      // warps per block
+static const int SND_KPT = 16;    // max levels per thread: nk <= SND_NW*SND_KPT
+
+template <int TX, int NW, int KPT>
+__global__ void __launch_bounds__(TX * NW) k_sound_tile(DGrid g, SoundIO io, SoundStep p) {
   extern __shared__ float sm[];
-  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-  const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int j = 1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const int i = 1 + (int)blockIdx.x * TX + lane;
+  const int j = 1 + (int)blockIdx.y;
   const int ni = g.ni, nj = g.nj, nk = g.nk;
-  const bool active = (i <= ni && j <= nj);
-  if (!active) return;
-  float *s_pf = sm;                 // pi'_old + fpk       [k*NT + tid]
-  float *s_d1 = sm + (nk + 2) * NT; // LU factor dum1
-  float *s_d2 = sm + 2 * (nk + 2) * NT;
-#define SM(a, k) a[(k) * NT + tid]
+  const bool active = (i <= ni);
+  const int L = nk + 2;
+  float *PF = sm;               // pi'_old + fpk
+  float *P1 = sm + 1 * L * TX;  // pk1 + qk
+  float *P2 = sm + 2 * L * TX;  // pk2 - qk
+  float *MM = sm + 3 * L * TX;  // mm, then the LU factor dum1
+  float *DD = sm + 4 * L * TX;  // w_old + fwk, then dum2, then the new w
+#define S(a, k) a[(k) * TX + lane]
 
   const float dts = p.dts, alph = g.alph, beta = 1.0f - alph, asq = alph * alph;
   const float cp = g.c.cp, rdx = g.rdx, rdy = g.rdy, rdz = g.rdz;
-  const float tem1pg = rdx * cp * 0.5f, tem2pg = rdy * cp * 0.5f;      // sound.F:321-322
-  const float temx = dts * 0.5f * rdx, temy = dts * 0.5f * rdy;        // sound.F:479-480
-  const float uh_i = LDG(&g.uh[i - g.ib]), vh_j = LDG(&g.vh[j - g.jb]);
-  const float uf_i = LDG(&g.uf[i - g.ib]), uf_ip = LDG(&g.uf[i + 1 - g.ib]);
-  const float vf_j = LDG(&g.vf[j - g.jb]), vf_jp = LDG(&g.vf[j + 1 - g.jb]);
-  const float dtu_i = dts * LDG(&g.dtu0[i2(g, i, j)]), dtu_ip = dts * LDG(&g.dtu0[i2(g, i + 1, j)]);
-  const float dtv_j = dts * LDG(&g.dtv0[i2(g, i, j)]), dtv_jp = dts * LDG(&g.dtv0[i2(g, i, j + 1)]);
-  const bool openw = (g.wbc == 2 && g.ibw && i == 1), opene = (g.ebc == 2 && g.ibe && i == ni);
-  const bool opens = (g.sbc == 2 && g.ibs && j == 1), openn = (g.nbc == 2 && g.ibn && j == nj);
 
-  // ---------------- upward pass ----------------
-  float pk1p = 0.f, pk2p = 0.f, qkp = 0.f, ppp = 0.f, pfp = 0.f, d1p = 0.f, d2p = 0.f, wlast = 0.f;
-  for (int k = 1; k <= nk; k++) {
-    // stage coefficients (sound.F:117-135, 188-189)
-    const float mhk = LDG(&g.mh[k]), rr0k = LDG(&g.rr0[k]);
-    const float temq = dts * rdz * mhk;
-    const float r2 = dts * rdz * mhk * rr0k * LDG(&g.rf0[k + 1]);
-    const float r1 = dts * rdz * mhk * rr0k * LDG(&g.rf0[k]);
-    const float temm = dts * rdz * cp * LDG(&g.mf[k]);
-    const float c1a = LDG(&g.c1[k]), c1b = LDG(&g.c1[k + 1]), c2a = LDG(&g.c2[k]), c2b = LDG(&g.c2[k + 1]);
-    const long o = iS(g, i, j, k);
-    const float pia = LDG(&io.piadv[o]);
-    const float qk = temq * LDG(&io.ppterm[o]);
-    const float pk2 = (k == nk) ? 0.0f : r2 * (-c2b * LDG(&io.piadv[iS(g, i, j, k + 1)]) + (1.0f - c1b) * pia);
-    const float pk1 = (k == 1) ? 0.0f : r1 * (+c1a * LDG(&io.piadv[iS(g, i, j, k - 1)]) + (c2a - 1.0f) * pia);
+  float ppold[KPT], acc[KPT];
+  float w1 = 0.0f;
 
-    // new u at faces i and i+1, v at faces j and j+1
-    const float thc = LDG(&io.thv[o]);
-    const float ppc = LDG(&io.ppd_in[o]);
-    float un0, unp, vn0, vnp;
-    {
-      const long ou = iU(g, i, j, k), oup = iU(g, i + 1, j, k);
-      float uo = io.u_in[ou];
-      if (openw)
-        uo = uo + dts * (-RJK(g, io.radbcw, j, k) * (io.u_in[oup] - io.u_in[ou]) * rdx * LDG(&g.uh[1 - g.ib]) + LDG(&io.uten[ou]));
-      un0 = uo + dtu_i * (LDG(&io.uten[ou]) - tem1pg * (ppc - LDG(&io.ppd_in[iS(g, i - 1, j, k)])) * uf_i *
-                                                  (thc + LDG(&io.thv[iS(g, i - 1, j, k)])));
-      float uop = io.u_in[oup];
-      if (opene)
-        uop = uop + dts * (-RJK(g, io.radbce, j, k) * (io.u_in[oup] - io.u_in[ou]) * rdx * LDG(&g.uh[ni - g.ib]) + LDG(&io.uten[oup]));
-      unp = uop + dtu_ip * (LDG(&io.uten[oup]) - tem1pg * (LDG(&io.ppd_in[iS(g, i + 1, j, k)]) - ppc) * uf_ip *
-                                                     (LDG(&io.thv[iS(g, i + 1, j, k)]) + thc));
+  // ---------------- phase 1 ----------------
+  if (active) {
+    const float tem1pg = rdx * cp * 0.5f, tem2pg = rdy * cp * 0.5f;      // sound.F:321-322
+    const float temx = dts * 0.5f * rdx, temy = dts * 0.5f * rdy;        // sound.F:479-480
+    const float uh_i = LDG(&g.uh[i - g.ib]), vh_j = LDG(&g.vh[j - g.jb]);
+    const float uf_i = LDG(&g.uf[i - g.ib]), uf_ip = LDG(&g.uf[i + 1 - g.ib]);
+    const float vf_j = LDG(&g.vf[j - g.jb]), vf_jp = LDG(&g.vf[j + 1 - g.jb]);
+    const float dtu_i = dts * LDG(&g.dtu0[i2(g, i, j)]), dtu_ip = dts * LDG(&g.dtu0[i2(g, i + 1, j)]);
+    const float dtv_j = dts * LDG(&g.dtv0[i2(g, i, j)]), dtv_jp = dts * LDG(&g.dtv0[i2(g, i, j + 1)]);
+    const bool openw = (g.wbc == 2 && g.ibw && i == 1), opene = (g.ebc == 2 && g.ibe && i == ni);
+    const bool opens = (g.sbc == 2 && g.ibs && j == 1), openn = (g.nbc == 2 && g.ibn && j == nj);
+#pragma unroll
+    for (int m = 0; m < KPT; m++) {
+      const int k = 1 + w + m * NW;
+      if (k > nk) break;
+      const long o = iS(g, i, j, k);
+      const long ou = iU(g, i, j, k), oup = ou + 1;
+      const long ov = iV(g, i, j, k), ovp = ov + g.NI;
+      // ---- loads (all independent)
+      const float pia = LDG(&io.piadv[o]);
+      const float piw = LDG(&io.piadv[o - 1]), pie = LDG(&io.piadv[o + 1]);
+      const float pis = LDG(&io.piadv[o - g.NI]), pin = LDG(&io.piadv[o + g.NI]);
+      const float pid = (k > 1) ? LDG(&io.piadv[o - (long)g.NI * g.NJ]) : 0.0f;
+      const float piu = (k < nk) ? LDG(&io.piadv[o + (long)g.NI * g.NJ]) : 0.0f;
+      const float thc = LDG(&io.thv[o]), thw = LDG(&io.thv[o - 1]), the = LDG(&io.thv[o + 1]);
+      const float ths = LDG(&io.thv[o - g.NI]), thn = LDG(&io.thv[o + g.NI]);
+      const float thd = (k > 1) ? LDG(&io.thv[o - (long)g.NI * g.NJ]) : 0.0f;
+      const float ppc = LDG(&io.ppd_in[o]), ppw = LDG(&io.ppd_in[o - 1]), ppe = LDG(&io.ppd_in[o + 1]);
+      const float pps = LDG(&io.ppd_in[o - g.NI]), ppn = LDG(&io.ppd_in[o + g.NI]);
+      const float u0v = LDG(&io.u_in[ou]), u1v = LDG(&io.u_in[oup]);
+      const float v0v = LDG(&io.v_in[ov]), v1v = LDG(&io.v_in[ovp]);
+      const float ut0 = LDG(&io.uten[ou]), ut1 = LDG(&io.uten[oup]);
+      const float vt0 = LDG(&io.vten[ov]), vt1 = LDG(&io.vten[ovp]);
+      const float pptn = LDG(&io.ppten[o]), pptm = LDG(&io.ppterm[o]);
+      const float wk = io.w_in[o];
+      const float wkp = (k < nk) ? io.w_in[o + (long)g.NI * g.NJ] : 0.0f;
+      const float pp = io.pp_in[o];
+      const float ppm = (k > 1) ? io.pp_in[o - (long)g.NI * g.NJ] : 0.0f;
+      const float wtn = LDG(&io.wten[o]);
+      const float accw = p.first ? LDG(&io.wa[o]) * beta : io.rrw[o];
+      const float accu0 = p.first ? 0.0f : io.rru[ou];
+      const float accv0 = p.first ? 0.0f : io.rrv[ov];
+      // ---- u at faces i, i+1 and v at faces j, j+1
+      float uo = u0v;
+      if (openw) uo = uo + dts * (-RJK(g, io.radbcw, j, k) * (u1v - u0v) * rdx * LDG(&g.uh[1 - g.ib]) + ut0);
+      const float un0 = uo + dtu_i * (ut0 - tem1pg * (ppc - ppw) * uf_i * (thc + thw));
+      float uop = u1v;
+      if (opene) uop = uop + dts * (-RJK(g, io.radbce, j, k) * (u1v - u0v) * rdx * LDG(&g.uh[ni - g.ib]) + ut1);
+      const float unp = uop + dtu_ip * (ut1 - tem1pg * (ppe - ppc) * uf_ip * (the + thc));
+      float vo = v0v;
+      if (opens) vo = vo + dts * (-RIK(g, io.radbcs, i, k) * (v1v - v0v) * rdy * LDG(&g.vh[1 - g.jb]) + vt0);
+      const float vn0 = vo + dtv_j * (vt0 - tem2pg * (ppc - pps) * vf_j * (thc + ths));
+      float vop = v1v;
+      if (openn) vop = vop + dts * (-RIK(g, io.radbcn, i, k) * (v1v - v0v) * rdy * LDG(&g.vh[nj - g.jb]) + vt1);
+      const float vnp = vop + dtv_jp * (vt1 - tem2pg * (ppn - ppc) * vf_jp * (thn + thc));
       io.u_out[ou] = un0;
-      if (i == ni) io.u_out[oup] = unp;
-      const long ov = iV(g, i, j, k), ovp = iV(g, i, j + 1, k);
-      float vo = io.v_in[ov];
-      if (opens)
-        vo = vo + dts * (-RIK(g, io.radbcs, i, k) * (io.v_in[ovp] - io.v_in[ov]) * rdy * LDG(&g.vh[1 - g.jb]) + LDG(&io.vten[ov]));
-      vn0 = vo + dtv_j * (LDG(&io.vten[ov]) - tem2pg * (ppc - LDG(&io.ppd_in[iS(g, i, j - 1, k)])) * vf_j *
-                                                  (thc + LDG(&io.thv[iS(g, i, j - 1, k)])));
-      float vop = io.v_in[ovp];
-      if (openn)
-        vop = vop + dts * (-RIK(g, io.radbcn, i, k) * (io.v_in[ovp] - io.v_in[ov]) * rdy * LDG(&g.vh[nj - g.jb]) + LDG(&io.vten[ovp]));
-      vnp = vop + dtv_jp * (LDG(&io.vten[ovp]) - tem2pg * (LDG(&io.ppd_in[iS(g, i, j + 1, k)]) - ppc) * vf_jp *
-                                                     (LDG(&io.thv[iS(g, i, j + 1, k)]) + thc));
       io.v_out[ov] = vn0;
-      if (j == nj) io.v_out[ovp] = vnp;
-      // running sums of u, v (sound.F:806-835)
       if (p.last) {
-        io.rru[ou] = ((p.first ? 0.0f : io.rru[ou]) + un0) * p.tavg;
-        if (i == ni) io.rru[oup] = ((p.first ? 0.0f : io.rru[oup]) + unp) * p.tavg;
-        io.rrv[ov] = ((p.first ? 0.0f : io.rrv[ov]) + vn0) * p.tavg;
-        if (j == nj) io.rrv[ovp] = ((p.first ? 0.0f : io.rrv[ovp]) + vnp) * p.tavg;
+        io.rru[ou] = (accu0 + un0) * p.tavg;
+        io.rrv[ov] = (accv0 + vn0) * p.tavg;
       } else {
-        io.rru[ou] = (p.first ? 0.0f : io.rru[ou]) + un0;
-        if (i == ni) io.rru[oup] = (p.first ? 0.0f : io.rru[oup]) + unp;
-        io.rrv[ov] = (p.first ? 0.0f : io.rrv[ov]) + vn0;
-        if (j == nj) io.rrv[ovp] = (p.first ? 0.0f : io.rrv[ovp]) + vnp;
+        io.rru[ou] = accu0 + un0;
+        io.rrv[ov] = accv0 + vn0;
       }
+      if (i == ni) {
+        io.u_out[oup] = unp;
+        const float a1 = p.first ? 0.0f : io.rru[oup];
+        io.rru[oup] = p.last ? (a1 + unp) * p.tavg : a1 + unp;
+      }
+      if (j == nj) {
+        io.v_out[ovp] = vnp;
+        const float a1 = p.first ? 0.0f : io.rrv[ovp];
+        io.rrv[ovp] = p.last ? (a1 + vnp) * p.tavg : a1 + vnp;
+      }
+      // ---- stage coefficients (sound.F:117-135, 188-189)
+      const float mhk = LDG(&g.mh[k]), rr0k = LDG(&g.rr0[k]);
+      const float temq = dts * rdz * mhk;
+      const float r2 = dts * rdz * mhk * rr0k * LDG(&g.rf0[k + 1]);
+      const float r1 = dts * rdz * mhk * rr0k * LDG(&g.rf0[k]);
+      const float temm = dts * rdz * cp * LDG(&g.mf[k]);
+      const float c1a = LDG(&g.c1[k]), c1b = LDG(&g.c1[k + 1]), c2a = LDG(&g.c2[k]), c2b = LDG(&g.c2[k + 1]);
+      const float qk = temq * pptm;
+      const float pk2 = (k == nk) ? 0.0f : r2 * (-c2b * piu + (1.0f - c1b) * pia);
+      const float pk1 = (k == 1) ? 0.0f : r1 * (+c1a * pid + (c2a - 1.0f) * pia);
+      const float p1 = pk1 + qk, p2 = pk2 - qk;
+      // ---- fpk (sound.F:486-498)
+      float div = (unp - un0) * rdx * uh_i + (vnp - vn0) * rdy * vh_j;
+      if (fabsf(div) < g.smeps) div = 0.0f;
+      const float X = un0 * (pia - piw) + unp * (pie - pia);
+      const float Y = vn0 * (pia - pis) + vnp * (pin - pia);
+      const float A = dts * (pptn - pptm * div);
+      const float B = -(X * temx * uh_i) - Y * temy * vh_j;
+      const float C = beta * (wk * p1 + wkp * p2);
+      const float fpk = (A + B) + C;
+      S(PF, k) = pp + fpk;
+      S(P1, k) = p1;
+      S(P2, k) = p2;
+      if (k >= 2) {
+        const float mm = temm * (c2a * thc + c1a * thd);
+        const float fwk = dts * wtn + beta * (-mm * (pp - ppm));
+        S(MM, k) = mm;
+        S(DD, k) = wk + fwk;
+      }
+      ppold[m] = pp;
+      acc[m] = accw;
+      if (k == 1) w1 = wk;
     }
-    // fpk (sound.F:486-498)
-    const float wk = io.w_in[iW(g, i, j, k)];
-    const float wkp = (k == nk) ? 0.0f : io.w_in[iW(g, i, j, k + 1)];
-    float div = (unp - un0) * rdx * uh_i + (vnp - vn0) * rdy * vh_j;
-    if (fabsf(div) < g.smeps) div = 0.0f;
-    const float X = un0 * (pia - LDG(&io.piadv[iS(g, i - 1, j, k)])) + unp * (LDG(&io.piadv[iS(g, i + 1, j, k)]) - pia);
-    const float Y = vn0 * (pia - LDG(&io.piadv[iS(g, i, j - 1, k)])) + vnp * (LDG(&io.piadv[iS(g, i, j + 1, k)]) - pia);
-    const float A = dts * (LDG(&io.ppten[o]) - LDG(&io.ppterm[o]) * div);
-    const float B = -(X * temx * uh_i) - Y * temy * vh_j;
-    const float C = beta * (wk * (pk1 + qk) + wkp * (pk2 - qk));
-    const float fpk = (A + B) + C;
-    const float pp = io.pp_in[o];
-    const float pf = pp + fpk;
-    SM(s_pf, k) = pf;
-    // forward elimination (sound.F:659-716)
-    if (k >= 2) {
-      const float mm = temm * (c2a * thc + c1a * LDG(&io.thv[iS(g, i, j, k - 1)]));
-      const float cc = -asq * (-mm * (pk2 - qk));
-      const float bb = 1.0f - asq * (+mm * (-(pk1 + qk) + (pk2p - qkp)));
-      const float fwk = dts * LDG(&io.wten[iW(g, i, j, k)]) + beta * (-mm * (pp - ppp));
-      const float dd = wk + fwk + alph * (-mm * (pf - pfp));
+  }
+  __syncthreads();
+
+  // ---------------- phase 2: Thomas solve for w, k = 2..nk ----------------
+  if (w == 0 && active) {
+    float d1p = 0.0f, d2p = 0.0f;
+    for (int k = 2; k <= nk; k++) {
+      const float mm = S(MM, k);
+      const float bb = 1.0f - asq * (+mm * (-S(P1, k) + S(P2, k - 1)));
+      const float dd = S(DD, k) + alph * (-mm * (S(PF, k) - S(PF, k - 1)));
       if (k == 2) {
+        const float cc = -asq * (-mm * S(P2, k));
         const float rr = 1.0f / bb;
         d1p = -cc * rr;
         d2p = dd * rr;
-        SM(s_d1, k) = d1p; SM(s_d2, k) = d2p;
+        S(MM, k) = d1p; S(DD, k) = d2p;
       } else {
-        const float aa = -asq * (+mm * (pk1p + qkp));
+        const float aa = -asq * (+mm * S(P1, k - 1));
         const float rr = 1.0f / (aa * d1p + bb);
         if (k < nk) {
+          const float cc = -asq * (-mm * S(P2, k));
           d1p = -cc * rr;
           d2p = (dd - aa * d2p) * rr;
-          SM(s_d1, k) = d1p; SM(s_d2, k) = d2p;
+          S(MM, k) = d1p; S(DD, k) = d2p;
         } else {
-          wlast = (dd - aa * d2p) * rr;
+          S(DD, k) = (dd - aa * d2p) * rr;   // w(nk)
         }
       }
     }
-    pk1p = pk1; pk2p = pk2; qkp = qk; ppp = pp; pfp = pf;
+    float wup = S(DD, nk);
+    for (int k = nk - 1; k >= 2; k--) {
+      wup = S(MM, k) * wup + S(DD, k);
+      S(DD, k) = wup;
+    }
   }
+  __syncthreads();
 
-  // ---------------- downward pass ----------------
-  float wup = 0.0f;   // w at k+1 (w(nk+1) = 0)
-  for (int k = nk; k >= 1; k--) {
-    const long o = iS(g, i, j, k);
-    float wk;
-    if (k == nk) wk = wlast;
-    else if (k >= 2) wk = SM(s_d1, k) * wup + SM(s_d2, k);
-    else wk = io.w_in[iW(g, i, j, 1)];
-    const float mhk = LDG(&g.mh[k]), rr0k = LDG(&g.rr0[k]);
-    const float temq = dts * rdz * mhk;
-    const float r2 = dts * rdz * mhk * rr0k * LDG(&g.rf0[k + 1]);
-    const float r1 = dts * rdz * mhk * rr0k * LDG(&g.rf0[k]);
-    const float pia = LDG(&io.piadv[o]);
-    const float qk = temq * LDG(&io.ppterm[o]);
-    const float pk2 = (k == nk) ? 0.0f : r2 * (-LDG(&g.c2[k + 1]) * LDG(&io.piadv[iS(g, i, j, k + 1)]) + (1.0f - LDG(&g.c1[k + 1])) * pia);
-    const float pk1 = (k == 1) ? 0.0f : r1 * (+LDG(&g.c1[k]) * LDG(&io.piadv[iS(g, i, j, k - 1)]) + (LDG(&g.c2[k]) - 1.0f) * pia);
-    const float ppold = io.pp_in[o];
-    float pn = SM(s_pf, k) + alph * (wk * (pk1 + qk) + wup * (pk2 - qk));
-    if (fabsf(pn) < g.smeps) pn = 0.0f;
-    const float d1 = g.kdiv * (pn - ppold);
-    io.pp_out[o] = pn;
-    io.ppd_out[o] = pn + d1;
-    if (p.write_ppx) io.ppx[o] = d1;
-    const long ow = iW(g, i, j, k);
-    if (k >= 2) io.w_out[ow] = wk;
-    const float acc0 = p.first ? LDG(&io.wa[ow]) * beta : io.rrw[ow];
-    io.rrw[ow] = p.last ? (acc0 + wk * alph) * p.tavg : acc0 + wk;
-    wup = wk;
+  // ---------------- phase 3 ----------------
+  if (active) {
+#pragma unroll
+    for (int m = 0; m < KPT; m++) {
+      const int k = 1 + w + m * NW;
+      if (k > nk) break;
+      const long o = iS(g, i, j, k);
+      const float wk = (k >= 2) ? S(DD, k) : w1;
+      const float wkp = (k < nk) ? S(DD, k + 1) : 0.0f;
+      float pn = S(PF, k) + alph * (wk * S(P1, k) + wkp * S(P2, k));
+      if (fabsf(pn) < g.smeps) pn = 0.0f;
+      const float d1 = g.kdiv * (pn - ppold[m]);
+      io.pp_out[o] = pn;
+      io.ppd_out[o] = pn + d1;
+      if (p.write_ppx) io.ppx[o] = d1;
+      if (k >= 2) io.w_out[o] = wk;
+      io.rrw[o] = p.last ? (acc[m] + wk * alph) * p.tavg : acc[m] + wk;
+    }
   }
-#undef SM
+#undef S
 }
 
 void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, int64_t *nlaunch);
@@ -224,39 +263,42 @@ void sound_nloop(int nsound, int nrk, float dt, int *nloop_out, float *dts_out) 
   *dts_out = dts;
 }
 
-static const int SOUND_BX = 32, SOUND_BY = 2;
+size_t sound_smem_bytes(const DGrid &g) { return (size_t)5 * (g.nk + 2) * SND_TX * sizeof(float); }
+int sound_max_nk() { return SND_NW * SND_KPT; }
 
-size_t sound_smem_bytes(const DGrid &g) { return (size_t)3 * (g.nk + 2) * SOUND_BX * SOUND_BY * sizeof(float); }
-
-// One RK stage of acoustic steps.  Buffers: ua/va/wa/ppi/ppx are the stage
-// start values; u3d/v3d/w3d/pp3d receive the result; su/sv are scratch for
-// the u/v double buffer, d1/d2 for ppd.  rru/rrv/rrw receive the averages.
+// One RK stage of acoustic steps.  At the first stage the reference starts
+// from the current u3d/v3d/w3d/pp3d (sound.F:192-208); at later stages it
+// first resets them to the start-of-step ua/va/wa/ppi (sound.F:212-230).
+// u3d/v3d/w3d/pp3d receive the result; su/sv/su2/sv2 are scratch for the
+// u/v double buffer, d1/d2 for ppd.  rru/rrv/rrw receive the averages.
 void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
                   const float *ua, float *u3d, const float *uten, const float *va, float *v3d, const float *vten,
                   const float *wa, float *w3d, const float *wten, const float *ppi, float *pp3d,
                   const float *piadv, const float *ppten, float *ppx, const float *thv, const float *ppterm,
                   float *rru, float *rrv, float *rrw, const float *radbcw, const float *radbce,
-                  const float *radbcs, const float *radbcn, float *su, float *sv, float *d1, float *d2,
-                  cudaStream_t st, int64_t *nl) {
+                  const float *radbcs, const float *radbcn, float *su, float *sv, float *su2, float *sv2,
+                  float *d1, float *d2, cudaStream_t st, int64_t *nl) {
   int nloop;
   float dts;
   sound_nloop(nsound, nrk, dt, &nloop, &dts);
-  dim3 blk(SOUND_BX, SOUND_BY);
-  dim3 grid((g.ni + SOUND_BX - 1) / SOUND_BX, (g.nj + SOUND_BY - 1) / SOUND_BY);
+  dim3 blk(SND_TX, SND_NW);
+  dim3 grid((g.ni + SND_TX - 1) / SND_TX, g.nj);
   size_t smem = sound_smem_bytes(g);
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(k_sound_step<SOUND_BX * SOUND_BY>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW, SND_KPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
     attr_set = true;
   }
-  const float *uin = ua, *vin = va, *ppdin = ppx;
+  const float *uin = (nrk == 1) ? u3d : ua, *vin = (nrk == 1) ? v3d : va, *ppdin = ppx;
   for (int n = 1; n <= nloop; n++) {
     SoundIO io;
     const bool to3d = ((nloop - n) % 2) == 0;
     io.u_in = uin; io.v_in = vin;
     io.u_out = to3d ? u3d : su; io.v_out = to3d ? v3d : sv;
-    io.w_in = (n == 1) ? wa : w3d; io.w_out = w3d;
-    io.pp_in = (n == 1) ? ppi : pp3d; io.pp_out = pp3d;
+    if (io.u_out == io.u_in) { io.u_out = su2; io.v_out = sv2; }
+    io.w_in = (n == 1 && nrk != 1) ? wa : w3d; io.w_out = w3d;
+    io.pp_in = (n == 1 && nrk != 1) ? ppi : pp3d; io.pp_out = pp3d;
     io.ppd_in = ppdin; io.ppd_out = (n % 2) ? d1 : d2;
     io.rru = rru; io.rrv = rrv; io.rrw = rrw; io.wa = wa;
     io.uten = uten; io.vten = vten; io.wten = wten; io.ppten = ppten;
@@ -266,7 +308,7 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
     SoundStep sp;
     sp.dts = dts; sp.tavg = 1.0f / (float)nloop;
     sp.first = (n == 1); sp.last = (n == nloop); sp.write_ppx = (nrk == 3 && n == nloop);
-    { ProfScope _ps("k_sound_step", st); k_sound_step<SOUND_BX * SOUND_BY><<<grid, blk, smem, st>>>(g, io, sp); }
+    { ProfScope _ps("k_sound_step", st); k_sound_tile<SND_TX, SND_NW, SND_KPT><<<grid, blk, smem, st>>>(g, io, sp); }
     if (nl) *nl += 1;
     if (n < nloop) launch_bc(g, io.ppd_out, 2, 0, st, nl);
     uin = io.u_out; vin = io.v_out; ppdin = io.ppd_out;

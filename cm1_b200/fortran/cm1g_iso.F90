@@ -1,0 +1,238 @@
+!-----------------------------------------------------------------------
+!  cm1g_iso -- ISO_C_BINDING interface to libcm1g.so for CM1's Fortran.
+!
+!  Drop-in use from solve2.F / cm1.F (see INTEGRATION.md):
+!
+!    use cm1g_iso
+!    ...  (once, after param/base/init3d)
+!    call cm1g_setup( cm1g_ctx )
+!    ...  (in the time loop, instead of solve2 + pdefq + solve3)
+!    call cm1g_large_step( cm1g_ctx, nstep, dt, mtime, mass1, mass2, cflmax, &
+!                          ua,u3d,uten1, va,v3d,vten1, wa,w3d,wten1,       &
+!                          ppi,pp3d,ppx,ppten, tha,th3d,thten1, rho,prs,   &
+!                          qa,q3d,qten, pta,pt3d,ptten,                    &
+!                          radbcw,radbce,radbcs,radbcn )
+!
+!  The arrays are the model's own (ib:ie,jb:je,kb:ke ...) arrays; the
+!  library copies them to the GPU and back each call.  Fortran `real` is
+!  C float, `double precision` is C double, `integer` is int32_t.
+!-----------------------------------------------------------------------
+module cm1g_iso
+  use iso_c_binding
+  implicit none
+  private
+  public :: cm1g_config_t, cm1g_grid_t, cm1g_state_t
+  public :: cm1g_init, cm1g_finalize, cm1g_step, cm1g_solve2, cm1g_solve3, cm1g_pdefq
+  public :: cm1g_bcs, cm1g_bcp, cm1g_bcu, cm1g_bcv, cm1g_bcw, cm1g_last_error_f
+  public :: cm1g_setup, cm1g_large_step
+
+  integer(c_int32_t), parameter :: CM1G_MAXQ = 8
+
+  type, bind(C) :: cm1g_config_t
+    integer(c_int32_t) :: ni, nj, nk, ngxy
+    real(c_float)      :: dx, dy, dz
+    integer(c_int32_t) :: wbc, ebc, sbc, nbc
+    integer(c_int32_t) :: hadvordrs, vadvordrs, hadvordrv, vadvordrv
+    integer(c_int32_t) :: advwenos, advwenov, weno_order
+    integer(c_int32_t) :: nsound
+    real(c_float)      :: alph, kdiv
+    integer(c_int32_t) :: imoist, eqtset, numq, nqv
+    integer(c_int32_t) :: iptra, npt, pdtra
+    integer(c_int32_t) :: apmasscon
+    integer(c_int32_t) :: irbc
+    real(c_float)      :: cstar
+    integer(c_int32_t) :: roflux
+    real(c_float)      :: smeps
+    integer(c_int32_t) :: testcase, psolver, terrain_flag, axisymm, icor
+    real(c_float)      :: qmag(CM1G_MAXQ)
+  end type
+
+  type, bind(C) :: cm1g_grid_t
+    type(c_ptr) :: uh, ruh, uf, ruf, vh, rvh, vf, rvf
+    type(c_ptr) :: mh, rmh, c1, c2, mf, rmf
+    type(c_ptr) :: pi0, rho0, rr0, rf0, rrf0, th0, rth0, qv0, qc0, qi0, prs0
+    type(c_ptr) :: u0, v0, dtu0, dtv0
+  end type
+
+  type, bind(C) :: cm1g_state_t
+    type(c_ptr) :: ua, u3d, uten1, va, v3d, vten1, wa, w3d, wten1
+    type(c_ptr) :: ppi, pp3d, ppx, ppten, tha, th3d, thten1, rho, prs
+    type(c_ptr) :: qa, q3d, qten, pta, pt3d, ptten
+    type(c_ptr) :: radbcw, radbce, radbcs, radbcn
+  end type
+
+  interface
+    integer(c_int) function cm1g_init(cfg, grid, ctx) bind(C, name="cm1g_init")
+      import :: c_int, c_ptr, cm1g_config_t, cm1g_grid_t
+      type(cm1g_config_t), intent(in) :: cfg
+      type(cm1g_grid_t), intent(in) :: grid
+      type(c_ptr), intent(out) :: ctx
+    end function
+    integer(c_int) function cm1g_finalize(ctx) bind(C, name="cm1g_finalize")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+    end function
+    integer(c_int) function cm1g_solve2(ctx, nstep, dt, mtime, mass1, mass2, cflmax, st) bind(C, name="cm1g_solve2")
+      import :: c_int, c_int32_t, c_float, c_double, c_ptr, cm1g_state_t
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: nstep
+      real(c_float), value :: dt
+      real(c_double), value :: mtime, mass1
+      real(c_double), intent(out) :: mass2
+      real(c_float), intent(out) :: cflmax
+      type(cm1g_state_t), intent(inout) :: st
+    end function
+    integer(c_int) function cm1g_step(ctx, nstep, dt, mtime, mass1, mass2, cflmax, st, use_graph) &
+        bind(C, name="cm1g_step")
+      import :: c_int, c_int32_t, c_float, c_double, c_ptr, cm1g_state_t
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: nstep
+      real(c_float), value :: dt
+      real(c_double), value :: mtime, mass1
+      real(c_double), intent(out) :: mass2
+      real(c_float), intent(out) :: cflmax
+      type(cm1g_state_t), intent(inout) :: st
+      integer(c_int32_t), value :: use_graph
+    end function
+    integer(c_int) function cm1g_solve3(ctx, st) bind(C, name="cm1g_solve3")
+      import :: c_int, c_ptr, cm1g_state_t
+      type(c_ptr), value :: ctx
+      type(cm1g_state_t), intent(inout) :: st
+    end function
+    integer(c_int) function cm1g_pdefq(ctx, rmax, asq, rho, q3d) bind(C, name="cm1g_pdefq")
+      import :: c_int, c_float, c_double, c_ptr
+      type(c_ptr), value :: ctx
+      real(c_float), value :: rmax
+      real(c_double), intent(inout) :: asq
+      real(c_float), intent(in) :: rho(*)
+      real(c_float), intent(inout) :: q3d(*)
+    end function
+    integer(c_int) function cm1g_bcs(ctx, s) bind(C, name="cm1g_bcs")
+      import :: c_int, c_float, c_ptr
+      type(c_ptr), value :: ctx
+      real(c_float), intent(inout) :: s(*)
+    end function
+    integer(c_int) function cm1g_bcp(ctx, p) bind(C, name="cm1g_bcp")
+      import :: c_int, c_float, c_ptr
+      type(c_ptr), value :: ctx
+      real(c_float), intent(inout) :: p(*)
+    end function
+    integer(c_int) function cm1g_bcu(ctx, u) bind(C, name="cm1g_bcu")
+      import :: c_int, c_float, c_ptr
+      type(c_ptr), value :: ctx
+      real(c_float), intent(inout) :: u(*)
+    end function
+    integer(c_int) function cm1g_bcv(ctx, v) bind(C, name="cm1g_bcv")
+      import :: c_int, c_float, c_ptr
+      type(c_ptr), value :: ctx
+      real(c_float), intent(inout) :: v(*)
+    end function
+    integer(c_int) function cm1g_bcw(ctx, w, flag) bind(C, name="cm1g_bcw")
+      import :: c_int, c_int32_t, c_float, c_ptr
+      type(c_ptr), value :: ctx
+      real(c_float), intent(inout) :: w(*)
+      integer(c_int32_t), value :: flag
+    end function
+    type(c_ptr) function cm1g_last_error() bind(C, name="cm1g_last_error")
+      import :: c_ptr
+    end function
+  end interface
+
+contains
+
+  ! Message of the last failed call, as a Fortran string.
+  function cm1g_last_error_f() result(msg)
+    character(len=256) :: msg
+    character(kind=c_char), pointer :: p(:)
+    integer :: i
+    msg = ' '
+    call c_f_pointer(cm1g_last_error(), p, [256])
+    do i = 1, 256
+      if (p(i) == c_null_char) exit
+      msg(i:i) = p(i)
+    enddo
+  end function
+
+  ! Fill the configuration from module `input` and create the context
+  ! (run once after param, base and init3d have set the base state).
+  subroutine cm1g_setup(ctx, uh,ruh,uf,ruf,vh,rvh,vf,rvf, mh,rmh,c1,c2,mf,rmf, &
+                        pi0,rho0,rr0,rf0,rrf0,th0,rth0,qv0,qc0,qi0,prs0, u0,v0, dtu0,dtv0, qmag)
+    use input
+    use constants, only : epsilon
+    type(c_ptr), intent(out) :: ctx
+    real, target, intent(in) :: uh(ib:ie),ruh(ib:ie),uf(ib:ie+1),ruf(ib:ie+1)
+    real, target, intent(in) :: vh(jb:je),rvh(jb:je),vf(jb:je+1),rvf(jb:je+1)
+    real, target, intent(in), dimension(ib:ie,jb:je,kb:ke) :: mh,rmh,c1,c2
+    real, target, intent(in), dimension(ib:ie,jb:je,kb:ke+1) :: mf,rmf
+    real, target, intent(in), dimension(ib:ie,jb:je,kb:ke) :: pi0,rho0,rr0,rf0,rrf0,th0,rth0,qv0,qc0,qi0,prs0
+    real, target, intent(in) :: u0(ib:ie+1,jb:je,kb:ke), v0(ib:ie,jb:je+1,kb:ke)
+    real, target, intent(in) :: dtu0(ib:ie,jb:je), dtv0(ib:ie,jb:je)
+    real, intent(in) :: qmag(:)
+    type(cm1g_config_t) :: cfg
+    type(cm1g_grid_t) :: g
+    integer :: rc, n
+    cfg%ni = ni; cfg%nj = nj; cfg%nk = nk; cfg%ngxy = ngxy
+    cfg%dx = dx; cfg%dy = dy; cfg%dz = dz
+    cfg%wbc = wbc; cfg%ebc = ebc; cfg%sbc = sbc; cfg%nbc = nbc
+    cfg%hadvordrs = hadvordrs; cfg%vadvordrs = vadvordrs
+    cfg%hadvordrv = hadvordrv; cfg%vadvordrv = vadvordrv
+    cfg%advwenos = advwenos; cfg%advwenov = advwenov; cfg%weno_order = weno_order
+    cfg%nsound = nsound; cfg%alph = alph; cfg%kdiv = kdiv
+    cfg%imoist = imoist; cfg%eqtset = eqtset; cfg%numq = numq; cfg%nqv = nqv
+    cfg%iptra = iptra; cfg%npt = npt; cfg%pdtra = pdtra
+    cfg%apmasscon = apmasscon; cfg%irbc = irbc; cfg%cstar = cstar; cfg%roflux = roflux
+    cfg%smeps = smeps; cfg%testcase = testcase; cfg%psolver = psolver
+    cfg%terrain_flag = merge(1, 0, terrain_flag); cfg%axisymm = axisymm; cfg%icor = icor
+    cfg%qmag = 0.0
+    do n = 1, min(size(qmag), int(CM1G_MAXQ))
+      cfg%qmag(n) = qmag(n)
+    enddo
+    g%uh = c_loc(uh); g%ruh = c_loc(ruh); g%uf = c_loc(uf); g%ruf = c_loc(ruf)
+    g%vh = c_loc(vh); g%rvh = c_loc(rvh); g%vf = c_loc(vf); g%rvf = c_loc(rvf)
+    g%mh = c_loc(mh); g%rmh = c_loc(rmh); g%c1 = c_loc(c1); g%c2 = c_loc(c2)
+    g%mf = c_loc(mf); g%rmf = c_loc(rmf)
+    g%pi0 = c_loc(pi0); g%rho0 = c_loc(rho0); g%rr0 = c_loc(rr0); g%rf0 = c_loc(rf0)
+    g%rrf0 = c_loc(rrf0); g%th0 = c_loc(th0); g%rth0 = c_loc(rth0); g%qv0 = c_loc(qv0)
+    g%qc0 = c_loc(qc0); g%qi0 = c_loc(qi0); g%prs0 = c_loc(prs0)
+    g%u0 = c_loc(u0); g%v0 = c_loc(v0); g%dtu0 = c_loc(dtu0); g%dtv0 = c_loc(dtv0)
+    rc = cm1g_init(cfg, g, ctx)
+    if (rc /= 0) then
+      print *, ' cm1g_init failed: ', trim(cm1g_last_error_f())
+      call stopcm1
+    endif
+  end subroutine
+
+  ! One large step (solve2 + pdefq for qv + solve3's dynamical-core part).
+  subroutine cm1g_large_step(ctx, nstep, dt, mtime, mass1, mass2, cflmax, &
+                             ua,u3d,uten1, va,v3d,vten1, wa,w3d,wten1,   &
+                             ppi,pp3d,ppx,ppten, tha,th3d,thten1, rho,prs, &
+                             qa,q3d,qten, pta,pt3d,ptten, radbcw,radbce,radbcs,radbcn)
+    type(c_ptr), intent(in) :: ctx
+    integer, intent(in) :: nstep
+    real, intent(in) :: dt
+    double precision, intent(in) :: mtime, mass1
+    double precision, intent(out) :: mass2
+    real, intent(out) :: cflmax
+    real, target, intent(inout) :: ua(*),u3d(*),uten1(*),va(*),v3d(*),vten1(*),wa(*),w3d(*),wten1(*)
+    real, target, intent(inout) :: ppi(*),pp3d(*),ppx(*),ppten(*),tha(*),th3d(*),thten1(*),rho(*),prs(*)
+    real, target, intent(inout) :: qa(*),q3d(*),qten(*),pta(*),pt3d(*),ptten(*)
+    real, target, intent(inout) :: radbcw(*),radbce(*),radbcs(*),radbcn(*)
+    type(cm1g_state_t) :: s
+    integer :: rc
+    s%ua = c_loc(ua); s%u3d = c_loc(u3d); s%uten1 = c_loc(uten1)
+    s%va = c_loc(va); s%v3d = c_loc(v3d); s%vten1 = c_loc(vten1)
+    s%wa = c_loc(wa); s%w3d = c_loc(w3d); s%wten1 = c_loc(wten1)
+    s%ppi = c_loc(ppi); s%pp3d = c_loc(pp3d); s%ppx = c_loc(ppx); s%ppten = c_loc(ppten)
+    s%tha = c_loc(tha); s%th3d = c_loc(th3d); s%thten1 = c_loc(thten1)
+    s%rho = c_loc(rho); s%prs = c_loc(prs)
+    s%qa = c_loc(qa); s%q3d = c_loc(q3d); s%qten = c_loc(qten)
+    s%pta = c_loc(pta); s%pt3d = c_loc(pt3d); s%ptten = c_loc(ptten)
+    s%radbcw = c_loc(radbcw); s%radbce = c_loc(radbce); s%radbcs = c_loc(radbcs); s%radbcn = c_loc(radbcn)
+    rc = cm1g_step(ctx, int(nstep, c_int32_t), dt, mtime, mass1, mass2, cflmax, s, 0_c_int32_t)
+    if (rc /= 0) then
+      print *, ' cm1g_step failed: ', trim(cm1g_last_error_f())
+      call stopcm1
+    endif
+  end subroutine
+
+end module cm1g_iso
