@@ -66,14 +66,13 @@ __global__ void __launch_bounds__(TX * NW) k_sound_tile(DGrid g, SoundIO io, Sou
   float *P1 = sm + 1 * L * TX;  // pk1 + qk
   float *P2 = sm + 2 * L * TX;  // pk2 - qk
   float *MM = sm + 3 * L * TX;  // mm, then the LU factor dum1
-  float *DD = sm + 4 * L * TX;  // w_old + fwk, then dum2, then the new w
+  float *DD = sm + 4 * L * TX;  // w_old + fwk, then dum2, then the new w (DD(1) = w(1))
+  float *PO = sm + 5 * L * TX;  // pi' before the step
+  float *AC = sm + 6 * L * TX;  // running sum of w before the step
 #define S(a, k) a[(k) * TX + lane]
 
   const float dts = p.dts, alph = g.alph, beta = 1.0f - alph, asq = alph * alph;
   const float cp = g.c.cp, rdx = g.rdx, rdy = g.rdy, rdz = g.rdz;
-
-  float ppold[KPT], acc[KPT];
-  float w1 = 0.0f;
 
   // ---------------- phase 1 ----------------
   if (active) {
@@ -86,7 +85,7 @@ __global__ void __launch_bounds__(TX * NW) k_sound_tile(DGrid g, SoundIO io, Sou
     const float dtv_j = dts * LDG(&g.dtv0[i2(g, i, j)]), dtv_jp = dts * LDG(&g.dtv0[i2(g, i, j + 1)]);
     const bool openw = (g.wbc == 2 && g.ibw && i == 1), opene = (g.ebc == 2 && g.ibe && i == ni);
     const bool opens = (g.sbc == 2 && g.ibs && j == 1), openn = (g.nbc == 2 && g.ibn && j == nj);
-#pragma unroll
+#pragma unroll 1
     for (int m = 0; m < KPT; m++) {
       const int k = 1 + w + m * NW;
       if (k > nk) break;
@@ -178,9 +177,9 @@ __global__ void __launch_bounds__(TX * NW) k_sound_tile(DGrid g, SoundIO io, Sou
         S(MM, k) = mm;
         S(DD, k) = wk + fwk;
       }
-      ppold[m] = pp;
-      acc[m] = accw;
-      if (k == 1) w1 = wk;
+      S(PO, k) = pp;
+      S(AC, k) = accw;
+      if (k == 1) S(DD, 1) = wk;
     }
   }
   __syncthreads();
@@ -221,21 +220,22 @@ __global__ void __launch_bounds__(TX * NW) k_sound_tile(DGrid g, SoundIO io, Sou
 
   // ---------------- phase 3 ----------------
   if (active) {
-#pragma unroll
+#pragma unroll 1
     for (int m = 0; m < KPT; m++) {
       const int k = 1 + w + m * NW;
       if (k > nk) break;
       const long o = iS(g, i, j, k);
-      const float wk = (k >= 2) ? S(DD, k) : w1;
+      const float wk = S(DD, k);
       const float wkp = (k < nk) ? S(DD, k + 1) : 0.0f;
       float pn = S(PF, k) + alph * (wk * S(P1, k) + wkp * S(P2, k));
       if (fabsf(pn) < g.smeps) pn = 0.0f;
-      const float d1 = g.kdiv * (pn - ppold[m]);
+      const float d1 = g.kdiv * (pn - S(PO, k));
       io.pp_out[o] = pn;
       io.ppd_out[o] = pn + d1;
       if (p.write_ppx) io.ppx[o] = d1;
       if (k >= 2) io.w_out[o] = wk;
-      io.rrw[o] = p.last ? (acc[m] + wk * alph) * p.tavg : acc[m] + wk;
+      const float ac = S(AC, k);
+      io.rrw[o] = p.last ? (ac + wk * alph) * p.tavg : ac + wk;
     }
   }
 #undef S
@@ -263,7 +263,7 @@ void sound_nloop(int nsound, int nrk, float dt, int *nloop_out, float *dts_out) 
   *dts_out = dts;
 }
 
-size_t sound_smem_bytes(const DGrid &g) { return (size_t)5 * (g.nk + 2) * SND_TX * sizeof(float); }
+size_t sound_smem_bytes(const DGrid &g) { return (size_t)7 * (g.nk + 2) * SND_TX * sizeof(float); }
 int sound_max_nk() { return SND_NW * SND_KPT; }
 
 // One RK stage of acoustic steps.  At the first stage the reference starts
