@@ -24,6 +24,10 @@ void launch_advs(const DGrid &g, const float *rru, const float *rrv, const float
                  const float *divx, const float *s, const float *s0, int sadd, const float *ten1,
                  const float *thterm, float *sten_out, float *snew, int weno, int pdef, int pdefweno,
                  double weps, float dt, int flush, float *scratch, cudaStream_t st, int64_t *nl);
+void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const float *rrw, const float *s,
+                       const float *s0, int sadd, const float *ten1, const float *thterm, float *snew, int weno,
+                       int pdef, int pdefweno, double weps, float dt, int flush, float *scratch, cudaStream_t st,
+                       int64_t *nl);
 void launch_sound(const DGrid &g, int nsound, int nrk, float dt, const float *ua, float *u3d, const float *uten,
                   const float *va, float *v3d, const float *vten, const float *wa, float *w3d, const float *wten,
                   const float *ppi, float *pp3d, const float *piadv, const float *ppten, float *ppx,
@@ -464,15 +468,15 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
     if (openrad) launch_radbc4(g, d->ua, d->u3d, d->va, d->v3d, d->radbcw, d->radbce, d->radbcs, d->radbcn, dttmp, st, nl);
     const int weno = (cf.advwenos == 1 || (cf.advwenos == 2 && nrk == 3)) ? 1 : 0;
     // theta (solve2.F:1320-1425)
-    launch_advs(g, c->rru, c->rrv, c->rrw, 1, nullptr, th_in, d->tha, 1, d->thten1,
-                (cf.imoist && cf.eqtset == 2) ? c->thterm : nullptr, nullptr, buf_out(0, nrk), weno, 0, 0,
-                (double)(10.0f * 1.0e-18f), dttmp, 1, c->pdefscr, st, nl);
+    launch_advs_tiled(g, c->rru, c->rrv, c->rrw, th_in, d->tha, 1, d->thten1,
+                      (cf.imoist && cf.eqtset == 2) ? c->thterm : nullptr, buf_out(0, nrk), weno, 0, 0,
+                      (double)(10.0f * 1.0e-18f), dttmp, 1, c->pdefscr, st, nl);
     // moisture (solve2.F:1431-1530)
     for (int n = 0; n < numq; n++) {
       const int s = 1 + n;
-      launch_advs(g, c->rru, c->rrv, c->rrw, 1, nullptr, buf_in(s, nrk), base[s], 0, ten1[s], nullptr, nullptr,
-                  buf_out(s, nrk), weno, nrk == 3 ? 1 : 0, (n + 1 == cf.nqv) ? 0 : 1,
-                  (double)(cf.qmag[n] * 1.0e-18f), dttmp, 1, c->pdefscr, st, nl);
+      launch_advs_tiled(g, c->rru, c->rrv, c->rrw, buf_in(s, nrk), base[s], 0, ten1[s], nullptr, buf_out(s, nrk),
+                        weno, nrk == 3 ? 1 : 0, (n + 1 == cf.nqv) ? 0 : 1, (double)(cf.qmag[n] * 1.0e-18f), dttmp, 1,
+                        c->pdefscr, st, nl);
     }
     // pressure, density, mass sums (solve2.F:1536-1656)
     if (nrk == 3)
@@ -492,8 +496,8 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
     for (int n = 0; n < npt; n++) {
       const int s = 1 + numq + n;
       const int pdef = (nrk == 3 && cf.pdtra == 1) ? 1 : 0;
-      launch_advs(g, c->rru, c->rrv, c->rrw, 1, nullptr, buf_in(s, nrk), base[s], 0, ten1[s], nullptr, nullptr,
-                  buf_out(s, nrk), weno, pdef, 1, (double)(1.0f * 1.0e-18f), dttmp, 0, c->pdefscr, st, nl);
+      launch_advs_tiled(g, c->rru, c->rrv, c->rrw, buf_in(s, nrk), base[s], 0, ten1[s], nullptr, buf_out(s, nrk),
+                        weno, pdef, 1, (double)(1.0f * 1.0e-18f), dttmp, 0, c->pdefscr, st, nl);
       if (nrk <= 2) launch_bc(g, buf_out(s, nrk), 1, 0, st, nl);
     }
     // dry-air mass fix (solve2.F:1976-2033)

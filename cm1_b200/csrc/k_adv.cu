@@ -577,7 +577,234 @@ __global__ void k_advs_pdef2(DGrid g, SAdv a, const float *__restrict__ advx, co
   }
 }
 
+// ---------------------------------------------------------------------
+// Tiled scalar advection (the production path of advs).
+//
+// A block owns TX x TY columns and marches upward through the levels.  At
+// each level the advected field is staged with its 3-point lateral halo in
+// shared memory; every x- and y-face flux is evaluated once (the WENO5 or
+// 5th-order value of hadv_weno5/hadv_flx5) and shared by the two cells it
+// separates; the vertical face flux of the level above is evaluated from a
+// per-thread register window of the column and carried to the next level as
+// its lower face.  Each cell therefore costs three face evaluations instead
+// of six.  MODE_UPDATE writes snew = s0 + dt*ten (solve2.F:1419-1425,
+// 1513-1520, 1951-1957); MODE_PDEF1 writes advx/advy/advz and the
+// provisional masses of pdefx1/pdefy1/pdefz for the second pdef pass.
+// ---------------------------------------------------------------------
+enum { MODE_UPDATE = 0, MODE_PDEF1 = 1 };
+
+// vertical face flux at level kk from wv[d+3] = s(kk+d), d = -3..2
+__device__ __forceinline__ float zflux_win(const DGrid &g, const float *wv, float r, int kk, int weno, int pdefweno,
+                                           double weps) {
+  const int nk = g.nk;
+  auto A = [&](int d) { return wv[d + 3]; };
+  const float c1k = LDG(&g.c1[kk]), c2k = LDG(&g.c2[kk]);
+  if (!weno) {
+    if (kk >= 4 && kk <= nk - 2) {
+      if (r >= 0.0f) return r * flx5(A(-3), A(-2), A(-1), A(0), A(1));
+      return r * flx5(A(2), A(1), A(0), A(-1), A(-2));
+    }
+    if (kk == 2) {
+      if (r >= 0.0f) return r * (c1k * A(-1) + c2k * A(0));
+      return r * flx3(A(1), A(0), A(-1));
+    }
+    if (kk == nk) {
+      if (r >= 0.0f) return r * flx3(A(-2), A(-1), A(0));
+      return r * (c1k * A(-1) + c2k * A(0));
+    }
+    if (kk == 3) {
+      if (r >= 0.0f) return r * flx3(A(-2), A(-1), A(0));
+      return r * flx5(A(2), A(1), A(0), A(-1), A(-2));
+    }
+    if (r >= 0.0f) return r * flx5(A(-3), A(-2), A(-1), A(0), A(1));
+    return r * flx3(A(1), A(0), A(-1));
+  }
+  if (kk == 2) {
+    if (r >= 0.0f) return r * (c1k * A(-1) + c2k * A(0));
+    return r * upstrpd(A(1), A(0), A(-1), weps);
+  }
+  if (kk == nk) {
+    if (r > 0.0f) return r * upstrpd(A(-2), A(-1), A(0), weps);
+    return r * (c1k * A(-1) + c2k * A(0));
+  }
+  if (pdefweno == 1) {
+    if (kk == 3 && r > 0.0f) return r * upstrpd(A(-2), A(-1), A(0), weps);
+    if (kk == nk - 1 && r < 0.0f) return r * upstrpd(A(1), A(0), A(-1), weps);
+    float s1, s2, s3, s4, s5;
+    if (r >= 0.0f) { s1 = A(-3); s2 = A(-2); s3 = A(-1); s4 = A(0); s5 = A(1); }
+    else { s1 = A(2); s2 = A(1); s3 = A(0); s4 = A(-1); s5 = A(-2); }
+    return (absmax5(s1, s2, s3, s4, s5) > (float)weps) ? r * weno5(s1, s2, s3, s4, s5, weps) : 0.0f;
+  }
+  if (kk >= 4 && kk <= nk - 2) {
+    if (r >= 0.0f) return r * weno5(A(-3), A(-2), A(-1), A(0), A(1), weps);
+    return r * weno5(A(2), A(1), A(0), A(-1), A(-2), weps);
+  }
+  if (kk == 3) {
+    if (r >= 0.0f) return r * upstrpd(A(-2), A(-1), A(0), weps);
+    return r * weno5(A(2), A(1), A(0), A(-1), A(-2), weps);
+  }
+  if (r >= 0.0f) return r * weno5(A(-3), A(-2), A(-1), A(0), A(1), weps);
+  return r * upstrpd(A(1), A(0), A(-1), weps);
+}
+
+// horizontal face flux from five upwind-ordered values
+__device__ __forceinline__ float hflux5(float r, float sm3, float sm2, float sm1, float s0, float sp1, float sp2,
+                                        int weno, int pdef, double weps) {
+  float s1, s2, s3, s4, s5;
+  if (r >= 0.0f) { s1 = sm3; s2 = sm2; s3 = sm1; s4 = s0; s5 = sp1; }
+  else { s1 = sp2; s2 = sp1; s3 = s0; s4 = sm1; s5 = sm2; }
+  if (!weno) return r * flx5(s1, s2, s3, s4, s5);
+  if (pdef == 1 && !(absmax5(s1, s2, s3, s4, s5) > (float)weps)) return 0.0f;
+  return r * weno5(s1, s2, s3, s4, s5, weps);
+}
+
+struct STileOut {
+  const float *sten_in;       // fixed tendency (thten1, qten, ptten)
+  const float *sbase;         // RK base value (tha, qa, pta)
+  float *snew;                // MODE_UPDATE output
+  float *advx, *advy, *advz, *dumx, *dumy, *dumz;   // MODE_PDEF1 outputs
+};
+
+template <int TX, int TY, int MODE>
+__global__ void __launch_bounds__(TX * TY) k_advs_tile(DGrid g, SAdv a, STileOut out, int weno, int pdef, int pdefweno,
+                                                       double weps, float dt, int flush) {
+  __shared__ float ss[TY + 6][TX + 7];
+  __shared__ float fx[TY][TX + 1];
+  __shared__ float fy[TY + 1][TX];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
+  const int i0 = 1 + (int)blockIdx.x * TX, j0 = 1 + (int)blockIdx.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int ni = g.ni, nj = g.nj, nk = g.nk;
+  const bool active = (i <= ni && j <= nj);
+  const bool doitw = (g.wbc == 2 && g.ibw), doite = (g.ebc == 2 && g.ibe);
+  const bool doits = (g.sbc == 2 && g.ibs), doitn = (g.nbc == 2 && g.ibn);
+  const int ie = ni + g.ngxy, je = nj + g.ngxy;
+  const float uh_i = active ? LDG(&g.uh[i - g.ib]) : 0.0f, vh_j = active ? LDG(&g.vh[j - g.jb]) : 0.0f;
+  const bool east = active && (tx == TX - 1 || i == ni), north = active && (ty == TY - 1 || j == nj);
+
+  // register window of the column: wv[d+3] = s(k+1+d), d = -3..2 (for the top face of level k)
+  float wv[6];
+#pragma unroll
+  for (int d = 0; d < 6; d++) {
+    const int kk = 1 + 1 + d - 3;   // level 1: s(-1..4)
+    wv[d] = (active && kk >= 0 && kk <= nk + 1) ? sval(g, a, i, j, kk) : 0.0f;
+  }
+  float fzlo = 0.0f;                            // flux through the bottom face of the level
+  float fwlo = active ? FW(g, a, i, j, 1) : 0.0f;
+
+  for (int k = 1; k <= nk; k++) {
+    // ---- stage the level with its halo
+    for (int t = tid; t < (TY + 6) * (TX + 6); t += TX * TY) {
+      const int yy = t / (TX + 6), xx = t - yy * (TX + 6);
+      const int ii = i0 - 3 + xx, jj = j0 - 3 + yy;
+      ss[yy][xx] = (ii <= ie && jj <= je) ? sval(g, a, ii, jj, k) : 0.0f;
+    }
+    __syncthreads();
+    float fu0 = 0.f, fu1 = 0.f, fv0 = 0.f, fv1 = 0.f, fwhi = 0.f, fzhi = 0.f, sc = 0.f;
+    if (active) {
+      const int X = tx + 3, Y = ty + 3;
+      fu0 = FU(g, a, i, j, k);
+      fu1 = FU(g, a, i + 1, j, k);
+      fv0 = FV(g, a, i, j, k);
+      fv1 = FV(g, a, i, j + 1, k);
+      fx[ty][tx] = hflux5(fu0, ss[Y][X - 3], ss[Y][X - 2], ss[Y][X - 1], ss[Y][X], ss[Y][X + 1], ss[Y][X + 2], weno, pdef, weps);
+      if (east)
+        fx[ty][tx + 1] = hflux5(fu1, ss[Y][X - 2], ss[Y][X - 1], ss[Y][X], ss[Y][X + 1], ss[Y][X + 2], ss[Y][X + 3], weno, pdef, weps);
+      fy[ty][tx] = hflux5(fv0, ss[Y - 3][X], ss[Y - 2][X], ss[Y - 1][X], ss[Y][X], ss[Y + 1][X], ss[Y + 2][X], weno, pdef, weps);
+      if (north)
+        fy[ty + 1][tx] = hflux5(fv1, ss[Y - 2][X], ss[Y - 1][X], ss[Y][X], ss[Y + 1][X], ss[Y + 2][X], ss[Y + 3][X], weno, pdef, weps);
+      sc = ss[Y][X];
+      fwhi = FW(g, a, i, j, k + 1);
+      if (k + 1 <= nk) fzhi = zflux_win(g, wv, fwhi, k + 1, weno, pdefweno, weps);
+    }
+    __syncthreads();
+    if (active) {
+      const long o = iS(g, i, j, k);
+      float fx0 = fx[ty][tx], fxp = fx[ty][tx + 1], fy0 = fy[ty][tx], fyp = fy[ty + 1][tx];
+      // adv.F:212-268
+      if (doitw && i == 1 && fu0 >= 0.0f) fx0 = fxp;
+      if (doite && i == ni && fu1 <= 0.0f) fxp = fx0;
+      if (doits && j == 1 && fv0 >= 0.0f) fy0 = fyp;
+      if (doitn && j == nj && fv1 <= 0.0f) fyp = fy0;
+      float advx = -(fxp - fx0) * g.rdx * uh_i;
+      float advy = -(fyp - fy0) * g.rdy * vh_j;
+      // adv.F:286-335
+      if (doitw && i == 1 && fu0 >= 0.0f) advx = advx - sc * (fu1 - fu0) * g.rdx * uh_i;
+      if (doite && i == ni && fu1 <= 0.0f) advx = advx - sc * (fu1 - fu0) * g.rdx * uh_i;
+      if (doits && j == 1 && fv0 >= 0.0f) advy = advy - sc * (fv1 - fv0) * g.rdy * vh_j;
+      if (doitn && j == nj && fv1 <= 0.0f) advy = advy - sc * (fv1 - fv0) * g.rdy * vh_j;
+      const float mhk = LDG(&g.mh[k]);
+      float advz;
+      if (k == 1) advz = -fzhi * g.rdz * mhk;
+      else if (k == nk) advz = +fzlo * g.rdz * mhk;
+      else advz = -(fzhi - fzlo) * g.rdz * mhk;
+      float div;
+      if (a.divx) div = LDG(&a.divx[o]);
+      else {
+        div = ((fu1 - fu0) * g.rdx * uh_i + (fv1 - fv0) * g.rdy * vh_j) + (fwhi - fwlo) * g.rdz * mhk;
+        if (fabsf(div) < g.smeps) div = 0.0f;
+      }
+      if (MODE == MODE_UPDATE) {
+        float ten = out.sten_in[o];
+        if (a.thterm) ten = ten - RAWDIV(g, a, i, j, k) * LDG(&a.thterm[o]);
+        ten = ten + (((advx + advy) + advz) + sc * div) * LDG(&g.rr0[k]);
+        float v = LDG(&out.sbase[o]) + dt * ten;
+        if (flush && fabsf(v) < g.smeps) v = 0.0f;
+        out.snew[o] = v;
+      } else {
+        // pdefx1 / pdefy1 / pdefz provisional masses (pdef.F:35-102, 289-340, 478-496)
+        out.advx[o] = advx; out.advy[o] = advy; out.advz[o] = advz;
+        const float s0 = LDG(&a.s0[o]), r0k = LDG(&g.rho0[k]);
+        float dx = r0k * s0 + dt * (advx + sc * (fu1 - fu0) * g.rdx * uh_i);
+        if (doitw && i == 1 && fu0 >= 0.0f) dx = r0k * s0;
+        if (doite && i == ni && fu1 <= 0.0f) dx = r0k * s0;
+        float dy = r0k * s0 + dt * (advy + sc * (fv1 - fv0) * g.rdy * vh_j);
+        if (doits && j == 1 && fv0 >= 0.0f) dy = r0k * s0;
+        if (doitn && j == nj && fv1 <= 0.0f) dy = r0k * s0;
+        out.dumx[o] = dx; out.dumy[o] = dy;
+        out.dumz[o] = r0k * s0 + dt * (advz + sc * (fwhi - fwlo) * g.rdz * mhk);
+      }
+      // slide the column window and carry the upper face to the next level
+#pragma unroll
+      for (int d = 0; d < 5; d++) wv[d] = wv[d + 1];
+      const int kn = k + 1 + 1 + 2;     // s(k+4) is the new top of the window for level k+1
+      wv[5] = (kn <= nk + 1) ? sval(g, a, i, j, kn) : 0.0f;
+      fzlo = fzhi;
+      fwlo = fwhi;
+    }
+    __syncthreads();
+  }
+}
+
 void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, int64_t *nlaunch);
+
+static const int ADV_TX = 32, ADV_TY = 8;
+
+// Production scalar pass (MODE_UPDATE, or the pdef two-pass form).
+void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const float *rrw, const float *s,
+                       const float *s0, int sadd, const float *ten1, const float *thterm, float *snew, int weno,
+                       int pdef, int pdefweno, double weps, float dt, int flush, float *scratch, cudaStream_t st,
+                       int64_t *nl) {
+  SAdv a{rru, rrv, rrw, s, s0, nullptr, thterm, 1, sadd};
+  dim3 blk(ADV_TX, ADV_TY), grid((g.ni + ADV_TX - 1) / ADV_TX, (g.nj + ADV_TY - 1) / ADV_TY);
+  STileOut o{};
+  o.sten_in = ten1; o.sbase = s0; o.snew = snew;
+  if (!pdef) {
+    { ProfScope _ps("k_advs_tile", st); k_advs_tile<ADV_TX, ADV_TY, MODE_UPDATE><<<grid, blk, 0, st>>>(g, a, o, weno, 0, pdefweno, weps, dt, flush); }
+    if (nl) *nl += 1;
+    return;
+  }
+  long n = nS(g);
+  o.advx = scratch; o.advy = scratch + n; o.advz = scratch + 2 * n;
+  o.dumx = scratch + 3 * n; o.dumy = scratch + 4 * n; o.dumz = scratch + 5 * n;
+  { ProfScope _ps("k_advs_tile_pdef1", st); k_advs_tile<ADV_TX, ADV_TY, MODE_PDEF1><<<grid, blk, 0, st>>>(g, a, o, weno, 1, pdefweno, weps, dt, flush); }
+  launch_bc(g, o.dumx, 1, 0, st, nl);
+  launch_bc(g, o.dumy, 1, 0, st, nl);
+  const int bx = 128;
+  dim3 g2((g.ni + bx - 1) / bx, g.nj, g.nk);
+  { ProfScope _ps("k_advs_pdef2", st); k_advs_pdef2<<<g2, bx, 0, st>>>(g, a, o.advx, o.advy, o.advz, o.dumx, o.dumy, o.dumz, ten1, nullptr, snew, s0, dt, flush); }
+  if (nl) *nl += 2;
+}
 
 // One advs call + RK update.  s = field (full halo), s0 = RK base,
 // ten1 = fixed tendency.  pdef selects the two-pass positive-definite form.
