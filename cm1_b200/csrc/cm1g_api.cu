@@ -508,7 +508,7 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
   // tracers after the RK loop (solve2.F:2064-2075)
   for (int n = 0; n < npt; n++) {
     float *pt = d->pt3d + n * ns;
-    if (cf.pdtra == 1) launch_pdefq(g, 0.0f, d->rho, pt, c->bud, c->dscal + 4, st, nl);
+    if (cf.pdtra == 1) launch_pdefq(g, 0.0f, d->rho, pt, nullptr, nullptr, st, nl);
     launch_bc(g, pt, 1, 0, st, nl);
   }
   (void)open;
@@ -542,7 +542,7 @@ static void run_solve3(cm1g_ctx *c, const cm1g_state_t *d) {
 static void run_step(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass1) {
   run_solve2(c, d, dt, mass1);
   if (c->cfg.imoist)   // cm1.F:3410-3415 (ptype=0)
-    launch_pdefq(c->g, 0.0f, d->rho, d->q3d + (long)(c->cfg.nqv - 1) * nS(c->g), c->bud, c->dscal + 5, c->stream,
+    launch_pdefq(c->g, 0.0f, d->rho, d->q3d + (long)(c->cfg.nqv - 1) * nS(c->g), nullptr, nullptr, c->stream,
                  &c->nlaunch);
   run_solve3(c, d);
 }

@@ -665,7 +665,7 @@ struct STileOut {
   float *advx, *advy, *advz, *dumx, *dumy, *dumz;   // MODE_PDEF1 outputs
 };
 
-template <int TX, int TY, int MODE>
+template <int TX, int TY, int KC, int MODE>
 __global__ void __launch_bounds__(TX * TY) k_advs_tile(DGrid g, SAdv a, STileOut out, int weno, int pdef, int pdefweno,
                                                        double weps, float dt, int flush) {
   __shared__ float ss[TY + 6][TX + 7];
@@ -683,16 +683,27 @@ __global__ void __launch_bounds__(TX * TY) k_advs_tile(DGrid g, SAdv a, STileOut
   const bool east = active && (tx == TX - 1 || i == ni), north = active && (ty == TY - 1 || j == nj);
 
   // register window of the column: wv[d+3] = s(k+1+d), d = -3..2 (for the top face of level k)
+  // the block covers levels kc0..kc1 of its columns (blockIdx.z selects the chunk)
+  const int kc0 = 1 + (int)blockIdx.z * KC, kc1 = min(nk, kc0 + KC - 1);
   float wv[6];
 #pragma unroll
   for (int d = 0; d < 6; d++) {
-    const int kk = 1 + 1 + d - 3;   // level 1: s(-1..4)
+    const int kk = kc0 - 2 + d;   // s(kc0-2 .. kc0+3)
     wv[d] = (active && kk >= 0 && kk <= nk + 1) ? sval(g, a, i, j, kk) : 0.0f;
   }
   float fzlo = 0.0f;                            // flux through the bottom face of the level
-  float fwlo = active ? FW(g, a, i, j, 1) : 0.0f;
+  float fwlo = active ? FW(g, a, i, j, kc0) : 0.0f;
+  if (active && kc0 >= 2) {                     // lower face of the chunk's first level
+    float w0[6];
+#pragma unroll
+    for (int d = 0; d < 6; d++) {
+      const int kk = kc0 - 3 + d;
+      w0[d] = (kk >= 0 && kk <= nk + 1) ? sval(g, a, i, j, kk) : 0.0f;
+    }
+    fzlo = zflux_win(g, w0, fwlo, kc0, weno, pdefweno, weps);
+  }
 
-  for (int k = 1; k <= nk; k++) {
+  for (int k = kc0; k <= kc1; k++) {
     // ---- stage the level with its halo
     for (int t = tid; t < (TY + 6) * (TX + 6); t += TX * TY) {
       const int yy = t / (TX + 6), xx = t - yy * (TX + 6);
@@ -772,13 +783,15 @@ __global__ void __launch_bounds__(TX * TY) k_advs_tile(DGrid g, SAdv a, STileOut
       fzlo = fzhi;
       fwlo = fwhi;
     }
-    __syncthreads();
+    // no barrier here: the next level's staging writes ss, which nobody reads
+    // after the second barrier, and fx/fy are rewritten only after the next
+    // level's first barrier, which every thread reaches after this level.
   }
 }
 
 void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, int64_t *nlaunch);
 
-static const int ADV_TX = 32, ADV_TY = 8;
+static const int ADV_TX = 32, ADV_TY = 8, ADV_KC = 16;
 
 // Production scalar pass (MODE_UPDATE, or the pdef two-pass form).
 void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const float *rrw, const float *s,
@@ -786,18 +799,19 @@ void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const
                        int pdef, int pdefweno, double weps, float dt, int flush, float *scratch, cudaStream_t st,
                        int64_t *nl) {
   SAdv a{rru, rrv, rrw, s, s0, nullptr, thterm, 1, sadd};
-  dim3 blk(ADV_TX, ADV_TY), grid((g.ni + ADV_TX - 1) / ADV_TX, (g.nj + ADV_TY - 1) / ADV_TY);
+  dim3 blk(ADV_TX, ADV_TY),
+      grid((g.ni + ADV_TX - 1) / ADV_TX, (g.nj + ADV_TY - 1) / ADV_TY, (g.nk + ADV_KC - 1) / ADV_KC);
   STileOut o{};
   o.sten_in = ten1; o.sbase = s0; o.snew = snew;
   if (!pdef) {
-    { ProfScope _ps("k_advs_tile", st); k_advs_tile<ADV_TX, ADV_TY, MODE_UPDATE><<<grid, blk, 0, st>>>(g, a, o, weno, 0, pdefweno, weps, dt, flush); }
+    { ProfScope _ps("k_advs_tile", st); k_advs_tile<ADV_TX, ADV_TY, ADV_KC, MODE_UPDATE><<<grid, blk, 0, st>>>(g, a, o, weno, 0, pdefweno, weps, dt, flush); }
     if (nl) *nl += 1;
     return;
   }
   long n = nS(g);
   o.advx = scratch; o.advy = scratch + n; o.advz = scratch + 2 * n;
   o.dumx = scratch + 3 * n; o.dumy = scratch + 4 * n; o.dumz = scratch + 5 * n;
-  { ProfScope _ps("k_advs_tile_pdef1", st); k_advs_tile<ADV_TX, ADV_TY, MODE_PDEF1><<<grid, blk, 0, st>>>(g, a, o, weno, 1, pdefweno, weps, dt, flush); }
+  { ProfScope _ps("k_advs_tile_pdef1", st); k_advs_tile<ADV_TX, ADV_TY, ADV_KC, MODE_PDEF1><<<grid, blk, 0, st>>>(g, a, o, weno, 1, pdefweno, weps, dt, flush); }
   launch_bc(g, o.dumx, 1, 0, st, nl);
   launch_bc(g, o.dumy, 1, 0, st, nl);
   const int bx = 128;

@@ -276,7 +276,7 @@ __global__ void k_pdefq(DGrid g, float rmax, const float *__restrict__ rho, floa
     q[o] = qq;
     a2 = a2 + (double)(r * qq * ruh * rvh * rmh);
   }
-  bud[(long)(j - 1) * g.ni + (i - 1)] = a2 - a1;
+  if (bud) bud[(long)(j - 1) * g.ni + (i - 1)] = a2 - a1;
 }
 
 // budget: asq += sum_j (sum_i bud) * dx*dy*dz, fixed order
@@ -296,7 +296,7 @@ void launch_pdefq(const DGrid &g, float rmax, const float *rho, float *q, double
                   cudaStream_t st, int64_t *nl) {
   dim3 grid((g.ni + 127) / 128, g.nj);
   { ProfScope _ps("k_pdefq", st); k_pdefq<<<grid, 128, 0, st>>>(g, rmax, rho, q, bud); }
-  { ProfScope _ps("k_pdefq_budget", st); k_pdefq_budget<<<1, 128, 0, st>>>(g, bud, asq); }
+  if (asq) { ProfScope _ps("k_pdefq_budget", st); k_pdefq_budget<<<1, 128, 0, st>>>(g, bud, asq); }
   if (nl) *nl += 2;
 }
 

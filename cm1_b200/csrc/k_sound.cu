@@ -54,7 +54,7 @@ static const int SND_NW = 8;      // warps per block
 static const int SND_KPT = 16;    // max levels per thread: nk <= SND_NW*SND_KPT
 
 template <int TX, int NW, int KPT>
-__global__ void __launch_bounds__(TX * NW) k_sound_tile(DGrid g, SoundIO io, SoundStep p) {
+__global__ void __launch_bounds__(TX * NW, 3) k_sound_tile(DGrid g, SoundIO io, SoundStep p) {
   extern __shared__ float sm[];
   const int lane = threadIdx.x, w = threadIdx.y;
   const int i = 1 + (int)blockIdx.x * TX + lane;
@@ -288,6 +288,8 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
   if (!attr_set) {
     cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW, SND_KPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          200 * 1024);
+    cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW, SND_KPT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
     attr_set = true;
   }
   const float *uin = (nrk == 1) ? u3d : ua, *vin = (nrk == 1) ? v3d : va, *ppdin = ppx;
