@@ -1,7 +1,7 @@
 !-----------------------------------------------------------------------
 !  cm1g_iso -- ISO_C_BINDING interface to libcm1g.so for CM1's Fortran.
 !
-!  Drop-in use from solve2.F / cm1.F (see INTEGRATION.md):
+!  Drop-in use from solve2.F / cm1.F:
 !
 !    use cm1g_iso
 !    ...  (once, after param/base/init3d)
