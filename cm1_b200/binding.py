@@ -58,6 +58,7 @@ def lib():
     L.cm1g_profile.argtypes = [ctxp, C.c_int32]
     L.cm1g_profile_read.argtypes = [ctxp, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(C.c_int64),
                                     C.POINTER(C.c_double)]
+    L.cm1g_pdefq_noalloc.argtypes = [cfgp, C.c_float, C.POINTER(C.c_double), _P, _P, _P, _P, _P, C.c_void_p]
     _lib = L
     return L
 

@@ -110,6 +110,8 @@ static int set_err(int code, const char *fmt, ...) {
   return code;
 }
 
+int cm1g::report_error(int code, const char *msg) { return set_err(code, "%s", msg); }
+
 #define CUCHK(x)                                                                                   \
   do {                                                                                             \
     cudaError_t e_ = (x);                                                                          \

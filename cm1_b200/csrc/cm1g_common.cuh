@@ -118,6 +118,10 @@ __device__ __forceinline__ float absmax5(float a, float b, float c, float d, flo
   return fmaxf(fmaxf(fmaxf(fmaxf(fabsf(a), fabsf(b)), fabsf(c)), fabsf(d)), fabsf(e));
 }
 
+// Records a message for cm1g_last_error() and returns code (C++ linkage,
+// not part of the C-ABI).
+int report_error(int code, const char *msg);
+
 // Per-kernel device timing (the library's counterpart of the reference's
 // timestats, input.F:359-387).  When a profile is active every kernel launch
 // site brackets its launch with a pair of CUDA events on the launch stream;

@@ -212,6 +212,28 @@ int cm1g_profile(cm1g_ctx_t *ctx, int32_t enable);
 int cm1g_profile_read(cm1g_ctx_t *ctx, int32_t index, char *name, int32_t name_len,
                       int64_t *launches, double *total_ms);
 
+/* Largest ni*nj that cm1g_pdefq_noalloc accepts: its scratch array holds one
+ * FP64 budget per column, 8 MiB of device memory at this size. */
+#define CM1G_PDEFQ_NOALLOC_MAX_COLUMNS (1024 * 1024)
+
+/* Positive-definite column fix without any device allocation.  This entry
+ * point has no counterpart in the reference; it exists for host programs
+ * that must not allocate device memory after start-up (a memory pool owned
+ * by someone else, an embedding that forbids it) and so cannot create a
+ * context.  It computes what cm1g_pdefq computes (pdscheme=1), with the
+ * reference's pdefq argument list (src/misclibs.F:1037): ruh(ib:ie),
+ * rvh(jb:je), rmh/rho/q3d(ib:ie,jb:je,kb:ke), all DEVICE pointers; q3d is
+ * updated in place, asq += the column-budget change.  The per-column budget
+ * lives in a fixed file-scope device array shared by every call in the
+ * process: calls that may overlap on one GPU must be serialized by the
+ * caller.  The first call with a given device current looks the array's
+ * address up (cudaGetSymbolAddress); make that call before any stream capture.
+ * ni*nj above CM1G_PDEFQ_NOALLOC_MAX_COLUMNS returns CM1G_ERR_ARG.  The call
+ * synchronizes stream to read asq back. */
+int cm1g_pdefq_noalloc(const cm1g_config_t *cfg, float rmax, double *asq,
+                       const float *ruh, const float *rvh, const float *rmh,
+                       const float *rho, float *q3d, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
