@@ -665,73 +665,145 @@ struct STileOut {
   float *advx, *advy, *advz, *dumx, *dumy, *dumz;   // MODE_PDEF1 outputs
 };
 
-template <int TX, int TY, int KC, int MODE>
-__global__ void __launch_bounds__(TX * TY) k_advs_tile(DGrid g, SAdv a, STileOut out, int weno, int pdef, int pdefweno,
+// The (TX+1)*TY x-faces and TX*(TY+1) y-faces of a
+// level are spread one per thread (the few faces beyond TX*TY go to the
+// first threads), so no lane evaluates a tile-edge face alone; staging
+// sources, face addresses and the column offset are 32-bit in-plane offsets
+// computed once per block; the raw averaged velocities of the faces are kept
+// in shared memory for the divergence terms of the cell owners.  All
+// arrays must have fewer than 2^31 points per horizontal plane.
+template <int TX, int TY, int KC, int MODE, int WENO>
+__global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STileOut out, int pdef, int pdefweno,
                                                        double weps, float dt, int flush) {
-  __shared__ float ss[TY + 6][TX + 7];
-  __shared__ float fx[TY][TX + 1];
-  __shared__ float fy[TY + 1][TX];
+  constexpr int NT = TX * TY;
+  constexpr int SW = TX + 6, SH = TY + 6, SP = SW + 1;     // staged plane, pitch SP
+  constexpr int NST = (SW * SH + NT - 1) / NT;              // staging slots per thread
+  constexpr int NFX = (TX + 1) * TY, NFY = TX * (TY + 1);   // faces of one level
+  __shared__ float ss[SH * SP];
+  __shared__ float fx[NFX], ux[NFX], fy[NFY], vy[NFY];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
   const int i0 = 1 + (int)blockIdx.x * TX, j0 = 1 + (int)blockIdx.y * TY;
   const int i = i0 + tx, j = j0 + ty;
-  const int ni = g.ni, nj = g.nj, nk = g.nk;
+  const int ni = g.ni, nj = g.nj, nk = g.nk, NI = g.NI, NJ = g.NJ;
   const bool active = (i <= ni && j <= nj);
   const bool doitw = (g.wbc == 2 && g.ibw), doite = (g.ebc == 2 && g.ibe);
   const bool doits = (g.sbc == 2 && g.ibs), doitn = (g.nbc == 2 && g.ibn);
   const int ie = ni + g.ngxy, je = nj + g.ngxy;
+  const long planeS = (long)NI * NJ, planeU = (long)(NI + 1) * NJ, planeV = (long)NI * (NJ + 1);
   const float uh_i = active ? LDG(&g.uh[i - g.ib]) : 0.0f, vh_j = active ? LDG(&g.vh[j - g.jb]) : 0.0f;
-  const bool east = active && (tx == TX - 1 || i == ni), north = active && (ty == TY - 1 || j == nj);
+  const int oc = active ? (i - g.ib) + NI * (j - g.jb) : 0;   // the column's in-plane offset
 
-  // register window of the column: wv[d+3] = s(k+1+d), d = -3..2 (for the top face of level k)
+  int soff[NST], sidx[NST];     // staging: source offset (-1: outside the arrays), slot in ss (-1: none)
+#pragma unroll
+  for (int q = 0; q < NST; q++) {
+    const int t = tid + q * NT;
+    soff[q] = -1; sidx[q] = -1;
+    if (t < SW * SH) {
+      const int yy = t / SW, xx = t - yy * SW;
+      const int ii = i0 - 3 + xx, jj = j0 - 3 + yy;
+      sidx[q] = yy * SP + xx;
+      if (ii <= ie && jj <= je) soff[q] = (ii - g.ib) + NI * (jj - g.jb);
+    }
+  }
+  int fxo[2], fxs[2], fyo[2], fys[2];   // face offsets (-1: no face) and stencil starts in ss
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const int f = tid + q * NT;
+    fxo[q] = -1; fxs[q] = 0; fyo[q] = -1; fys[q] = 0;
+    if (f < NFX) {
+      const int row = f / (TX + 1), col = f - row * (TX + 1);
+      const int ii = i0 + col, jj = j0 + row;
+      if (ii <= ni + 1 && jj <= nj) { fxo[q] = (ii - g.ib) + (NI + 1) * (jj - g.jb); fxs[q] = (row + 3) * SP + col; }
+    }
+    if (f < NFY) {
+      const int row = f / TX, col = f - row * TX;
+      const int ii = i0 + col, jj = j0 + row;
+      if (ii <= ni && jj <= nj + 1) { fyo[q] = (ii - g.ib) + NI * (jj - g.jb); fys[q] = row * SP + col + 3; }
+    }
+  }
+
+  auto SV = [&](int kk) -> float {
+    float v = LDG(&a.s[(long)kk * planeS + oc]);
+    if (a.sadd) v = (LDG(&g.th0[kk]) - 300.0f) + v;
+    return v;
+  };
+  // averaged w of a w-level (zero at the bottom and top boundaries)
+  auto WRAW = [&](int kk) -> float { return (kk <= 1 || kk >= nk + 1) ? 0.0f : LDG(&a.rrw[(long)kk * planeS + oc]); };
+
+  // register window of the column: wv[d+3] = s(k+1+d), d = -3..2 (for the top face of level k);
   // the block covers levels kc0..kc1 of its columns (blockIdx.z selects the chunk)
   const int kc0 = 1 + (int)blockIdx.z * KC, kc1 = min(nk, kc0 + KC - 1);
   float wv[6];
 #pragma unroll
   for (int d = 0; d < 6; d++) {
-    const int kk = kc0 - 2 + d;   // s(kc0-2 .. kc0+3)
-    wv[d] = (active && kk >= 0 && kk <= nk + 1) ? sval(g, a, i, j, kk) : 0.0f;
+    const int kk = kc0 - 2 + d;
+    wv[d] = (active && kk >= 0 && kk <= nk + 1) ? SV(kk) : 0.0f;
   }
+  float wlo = active ? WRAW(kc0) : 0.0f;       // raw averaged w through the bottom face of the level
+  float fwlo = wlo * LDG(&g.rf0[kc0]);
   float fzlo = 0.0f;                            // flux through the bottom face of the level
-  float fwlo = active ? FW(g, a, i, j, kc0) : 0.0f;
-  if (active && kc0 >= 2) {                     // lower face of the chunk's first level
+  if (active && kc0 >= 2) {
     float w0[6];
 #pragma unroll
     for (int d = 0; d < 6; d++) {
       const int kk = kc0 - 3 + d;
-      w0[d] = (kk >= 0 && kk <= nk + 1) ? sval(g, a, i, j, kk) : 0.0f;
+      w0[d] = (kk >= 0 && kk <= nk + 1) ? SV(kk) : 0.0f;
     }
-    fzlo = zflux_win(g, w0, fwlo, kc0, weno, pdefweno, weps);
+    fzlo = zflux_win(g, w0, fwlo, kc0, WENO, pdefweno, weps);
   }
 
   for (int k = kc0; k <= kc1; k++) {
-    // ---- stage the level with its halo
-    for (int t = tid; t < (TY + 6) * (TX + 6); t += TX * TY) {
-      const int yy = t / (TX + 6), xx = t - yy * (TX + 6);
-      const int ii = i0 - 3 + xx, jj = j0 - 3 + yy;
-      ss[yy][xx] = (ii <= ie && jj <= je) ? sval(g, a, ii, jj, k) : 0.0f;
+    const float r0k = LDG(&g.rho0[k]);
+    const float th0m = a.sadd ? (LDG(&g.th0[k]) - 300.0f) : 0.0f;
+    // ---- stage the level with its halo; fetch the raw face velocities
+    const float *sk = a.s + (long)k * planeS;
+#pragma unroll
+    for (int q = 0; q < NST; q++) {
+      if (sidx[q] >= 0) {
+        float v = 0.0f;
+        if (soff[q] >= 0) {
+          v = LDG(&sk[soff[q]]);
+          if (a.sadd) v = th0m + v;
+        }
+        ss[sidx[q]] = v;
+      }
+    }
+    float ru[2], rv[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      ru[q] = (fxo[q] >= 0) ? LDG(&a.rru[(long)k * planeU + fxo[q]]) : 0.0f;
+      rv[q] = (fyo[q] >= 0) ? LDG(&a.rrv[(long)k * planeV + fyo[q]]) : 0.0f;
+    }
+    const float whi = active ? WRAW(k + 1) : 0.0f;
+    __syncthreads();
+    // ---- face values: each x/y face once, each upper z face once per column
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int f = tid + q * NT;
+      if (fxo[q] >= 0) {
+        const float *p = &ss[fxs[q]];
+        fx[f] = hflux5(ru[q] * r0k, p[0], p[1], p[2], p[3], p[4], p[5], WENO, pdef, weps);
+        ux[f] = ru[q];
+      }
+      if (fyo[q] >= 0) {
+        const float *p = &ss[fys[q]];
+        fy[f] = hflux5(rv[q] * r0k, p[0], p[SP], p[2 * SP], p[3 * SP], p[4 * SP], p[5 * SP], WENO, pdef, weps);
+        vy[f] = rv[q];
+      }
+    }
+    const float fwhi = whi * LDG(&g.rf0[k + 1]);
+    float fzhi = 0.0f, sc = 0.0f;
+    if (active) {
+      sc = ss[(ty + 3) * SP + tx + 3];
+      if (k + 1 <= nk) fzhi = zflux_win(g, wv, fwhi, k + 1, WENO, pdefweno, weps);
     }
     __syncthreads();
-    float fu0 = 0.f, fu1 = 0.f, fv0 = 0.f, fv1 = 0.f, fwhi = 0.f, fzhi = 0.f, sc = 0.f;
     if (active) {
-      const int X = tx + 3, Y = ty + 3;
-      fu0 = FU(g, a, i, j, k);
-      fu1 = FU(g, a, i + 1, j, k);
-      fv0 = FV(g, a, i, j, k);
-      fv1 = FV(g, a, i, j + 1, k);
-      fx[ty][tx] = hflux5(fu0, ss[Y][X - 3], ss[Y][X - 2], ss[Y][X - 1], ss[Y][X], ss[Y][X + 1], ss[Y][X + 2], weno, pdef, weps);
-      if (east)
-        fx[ty][tx + 1] = hflux5(fu1, ss[Y][X - 2], ss[Y][X - 1], ss[Y][X], ss[Y][X + 1], ss[Y][X + 2], ss[Y][X + 3], weno, pdef, weps);
-      fy[ty][tx] = hflux5(fv0, ss[Y - 3][X], ss[Y - 2][X], ss[Y - 1][X], ss[Y][X], ss[Y + 1][X], ss[Y + 2][X], weno, pdef, weps);
-      if (north)
-        fy[ty + 1][tx] = hflux5(fv1, ss[Y - 2][X], ss[Y - 1][X], ss[Y][X], ss[Y + 1][X], ss[Y + 2][X], ss[Y + 3][X], weno, pdef, weps);
-      sc = ss[Y][X];
-      fwhi = FW(g, a, i, j, k + 1);
-      if (k + 1 <= nk) fzhi = zflux_win(g, wv, fwhi, k + 1, weno, pdefweno, weps);
-    }
-    __syncthreads();
-    if (active) {
-      const long o = iS(g, i, j, k);
-      float fx0 = fx[ty][tx], fxp = fx[ty][tx + 1], fy0 = fy[ty][tx], fyp = fy[ty + 1][tx];
+      const long o = (long)k * planeS + oc;
+      const int xi = ty * (TX + 1) + tx, yi = ty * TX + tx;
+      float fx0 = fx[xi], fxp = fx[xi + 1], fy0 = fy[yi], fyp = fy[yi + TX];
+      const float u0r = ux[xi], u1r = ux[xi + 1], v0r = vy[yi], v1r = vy[yi + TX];
+      const float fu0 = u0r * r0k, fu1 = u1r * r0k, fv0 = v0r * r0k, fv1 = v1r * r0k;
       // adv.F:212-268
       if (doitw && i == 1 && fu0 >= 0.0f) fx0 = fxp;
       if (doite && i == ni && fu1 <= 0.0f) fxp = fx0;
@@ -749,15 +821,15 @@ __global__ void __launch_bounds__(TX * TY) k_advs_tile(DGrid g, SAdv a, STileOut
       if (k == 1) advz = -fzhi * g.rdz * mhk;
       else if (k == nk) advz = +fzlo * g.rdz * mhk;
       else advz = -(fzhi - fzlo) * g.rdz * mhk;
-      float div;
-      if (a.divx) div = LDG(&a.divx[o]);
-      else {
-        div = ((fu1 - fu0) * g.rdx * uh_i + (fv1 - fv0) * g.rdy * vh_j) + (fwhi - fwlo) * g.rdz * mhk;
-        if (fabsf(div) < g.smeps) div = 0.0f;
-      }
+      float div = ((fu1 - fu0) * g.rdx * uh_i + (fv1 - fv0) * g.rdy * vh_j) + (fwhi - fwlo) * g.rdz * mhk;
+      if (fabsf(div) < g.smeps) div = 0.0f;
       if (MODE == MODE_UPDATE) {
         float ten = out.sten_in[o];
-        if (a.thterm) ten = ten - RAWDIV(g, a, i, j, k) * LDG(&a.thterm[o]);
+        if (a.thterm) {   // getdiv of the averaged velocities (misclibs.F:127-136)
+          float rd = ((u1r - u0r) * g.rdx * uh_i + (v1r - v0r) * g.rdy * vh_j) + (whi - wlo) * g.rdz * mhk;
+          if (fabsf(rd) < g.smeps) rd = 0.0f;
+          ten = ten - rd * LDG(&a.thterm[o]);
+        }
         ten = ten + (((advx + advy) + advz) + sc * div) * LDG(&g.rr0[k]);
         float v = LDG(&out.sbase[o]) + dt * ten;
         if (flush && fabsf(v) < g.smeps) v = 0.0f;
@@ -765,7 +837,7 @@ __global__ void __launch_bounds__(TX * TY) k_advs_tile(DGrid g, SAdv a, STileOut
       } else {
         // pdefx1 / pdefy1 / pdefz provisional masses (pdef.F:35-102, 289-340, 478-496)
         out.advx[o] = advx; out.advy[o] = advy; out.advz[o] = advz;
-        const float s0 = LDG(&a.s0[o]), r0k = LDG(&g.rho0[k]);
+        const float s0 = LDG(&a.s0[o]);
         float dx = r0k * s0 + dt * (advx + sc * (fu1 - fu0) * g.rdx * uh_i);
         if (doitw && i == 1 && fu0 >= 0.0f) dx = r0k * s0;
         if (doite && i == ni && fu1 <= 0.0f) dx = r0k * s0;
@@ -778,14 +850,15 @@ __global__ void __launch_bounds__(TX * TY) k_advs_tile(DGrid g, SAdv a, STileOut
       // slide the column window and carry the upper face to the next level
 #pragma unroll
       for (int d = 0; d < 5; d++) wv[d] = wv[d + 1];
-      const int kn = k + 1 + 1 + 2;     // s(k+4) is the new top of the window for level k+1
-      wv[5] = (kn <= nk + 1) ? sval(g, a, i, j, kn) : 0.0f;
+      const int kn = k + 4;     // s(k+4) is the new top of the window for level k+1
+      wv[5] = (kn <= nk + 1) ? SV(kn) : 0.0f;
       fzlo = fzhi;
       fwlo = fwhi;
+      wlo = whi;
     }
     // no barrier here: the next level's staging writes ss, which nobody reads
-    // after the second barrier, and fx/fy are rewritten only after the next
-    // level's first barrier, which every thread reaches after this level.
+    // after the second barrier, and fx/fy/ux/vy are rewritten only after the
+    // next level's first barrier, which every thread reaches after this level.
   }
 }
 
@@ -804,14 +877,20 @@ void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const
   STileOut o{};
   o.sten_in = ten1; o.sbase = s0; o.snew = snew;
   if (!pdef) {
-    { ProfScope _ps("k_advs_tile", st); k_advs_tile<ADV_TX, ADV_TY, ADV_KC, MODE_UPDATE><<<grid, blk, 0, st>>>(g, a, o, weno, 0, pdefweno, weps, dt, flush); }
+    ProfScope _ps("k_advs_tile", st);
+    if (weno) k_advs_tile<ADV_TX, ADV_TY, ADV_KC, MODE_UPDATE, 1><<<grid, blk, 0, st>>>(g, a, o, 0, pdefweno, weps, dt, flush);
+    else k_advs_tile<ADV_TX, ADV_TY, ADV_KC, MODE_UPDATE, 0><<<grid, blk, 0, st>>>(g, a, o, 0, pdefweno, weps, dt, flush);
     if (nl) *nl += 1;
     return;
   }
   long n = nS(g);
   o.advx = scratch; o.advy = scratch + n; o.advz = scratch + 2 * n;
   o.dumx = scratch + 3 * n; o.dumy = scratch + 4 * n; o.dumz = scratch + 5 * n;
-  { ProfScope _ps("k_advs_tile_pdef1", st); k_advs_tile<ADV_TX, ADV_TY, ADV_KC, MODE_PDEF1><<<grid, blk, 0, st>>>(g, a, o, weno, 1, pdefweno, weps, dt, flush); }
+  {
+    ProfScope _ps("k_advs_tile_pdef1", st);
+    if (weno) k_advs_tile<ADV_TX, ADV_TY, ADV_KC, MODE_PDEF1, 1><<<grid, blk, 0, st>>>(g, a, o, 1, pdefweno, weps, dt, flush);
+    else k_advs_tile<ADV_TX, ADV_TY, ADV_KC, MODE_PDEF1, 0><<<grid, blk, 0, st>>>(g, a, o, 1, pdefweno, weps, dt, flush);
+  }
   launch_bc(g, o.dumx, 1, 0, st, nl);
   launch_bc(g, o.dumy, 1, 0, st, nl);
   const int bx = 128;

@@ -252,29 +252,55 @@ void launch_cfl(const DGrid &g, const float *u, const float *v, const float *w, 
 // pdefq (misclibs.F:1037-1117), pdscheme=1: per-column mass-conserving
 // clipping.  bud[j*ni+i-1] receives a2-a1 of the column.
 // ---------------------------------------------------------------------
-__global__ void k_pdefq(DGrid g, float rmax, const float *__restrict__ rho, float *q, double *bud) {
+// The column is walked in chunks of PQ levels whose loads are issued
+// together; the sums still run k = 1..nk in order.
+__global__ void k_pdefq(DGrid g, float rmax, const float *__restrict__ rho, float *__restrict__ q, double *bud) {
+  constexpr int PQ = 8;
   const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int j = 1 + (int)blockIdx.y;
   if (i > g.ni) return;
   const float ruh = LDG(&g.ruh[i - g.ib]), rvh = LDG(&g.rvh[j - g.jb]);
+  const long plane = (long)g.NI * g.NJ, oc = iS(g, i, j, 0);
+  const int nk = g.nk;
   double t1 = 0.0, t2 = 0.0, a1 = 0.0, a2 = 0.0;
-  for (int k = 1; k <= g.nk; k++) {
-    const long o = iS(g, i, j, k);
-    const float r = LDG(&rho[o]), rmh = LDG(&g.rmh[k]);
-    float qq = q[o];
-    t1 = t1 + (double)(r * qq);
-    a1 = a1 + (double)(r * qq * ruh * rvh * rmh);
-    if (qq < rmax) { qq = 0.0f; q[o] = qq; }
-    t2 = t2 + (double)(r * qq);
+  for (int k0 = 1; k0 <= nk; k0 += PQ) {
+    float rr[PQ], qq[PQ];
+#pragma unroll
+    for (int m = 0; m < PQ; m++) {
+      const int k = k0 + m;
+      rr[m] = (k <= nk) ? LDG(&rho[oc + k * plane]) : 0.0f;
+      qq[m] = (k <= nk) ? q[oc + k * plane] : 0.0f;
+    }
+#pragma unroll
+    for (int m = 0; m < PQ; m++) {
+      const int k = k0 + m;
+      if (k > nk) break;
+      const float r = rr[m], rmh = LDG(&g.rmh[k]);
+      float v = qq[m];
+      t1 = t1 + (double)(r * v);
+      a1 = a1 + (double)(r * v * ruh * rvh * rmh);
+      if (v < rmax) { v = 0.0f; q[oc + k * plane] = v; }
+      t2 = t2 + (double)(r * v);
+    }
   }
   double t3 = (t1 + 1.0e-20) / (t2 + 1.0e-20);
   if (t3 < 0.0) t3 = 1.0;
-  for (int k = 1; k <= g.nk; k++) {
-    const long o = iS(g, i, j, k);
-    const float r = LDG(&rho[o]), rmh = LDG(&g.rmh[k]);
-    float qq = (float)(t3 * (double)q[o]);
-    q[o] = qq;
-    a2 = a2 + (double)(r * qq * ruh * rvh * rmh);
+  for (int k0 = 1; k0 <= nk; k0 += PQ) {
+    float rr[PQ], qq[PQ];
+#pragma unroll
+    for (int m = 0; m < PQ; m++) {
+      const int k = k0 + m;
+      rr[m] = (k <= nk) ? LDG(&rho[oc + k * plane]) : 0.0f;
+      qq[m] = (k <= nk) ? q[oc + k * plane] : 0.0f;
+    }
+#pragma unroll
+    for (int m = 0; m < PQ; m++) {
+      const int k = k0 + m;
+      if (k > nk) break;
+      const float v = (float)(t3 * (double)qq[m]);
+      q[oc + k * plane] = v;
+      a2 = a2 + (double)(rr[m] * v * ruh * rvh * LDG(&g.rmh[k]));
+    }
   }
   if (bud) bud[(long)(j - 1) * g.ni + (i - 1)] = a2 - a1;
 }

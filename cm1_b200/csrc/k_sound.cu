@@ -20,6 +20,8 @@
 // and are updated in place.  The east/north face velocity of a cell is
 // recomputed from the same old values by the neighbour that needs it, which
 // reproduces the stored value exactly.
+#include <cstdlib>
+#include <cstring>
 #include "cm1g_common.cuh"
 
 namespace cm1g {
@@ -67,8 +69,6 @@ __global__ void __launch_bounds__(TX * NW, 3) k_sound_tile(DGrid g, SoundIO io, 
   float *P2 = sm + 2 * L * TX;  // pk2 - qk
   float *MM = sm + 3 * L * TX;  // mm, then the LU factor dum1
   float *DD = sm + 4 * L * TX;  // w_old + fwk, then dum2, then the new w (DD(1) = w(1))
-  float *PO = sm + 5 * L * TX;  // pi' before the step
-  float *AC = sm + 6 * L * TX;  // running sum of w before the step
 #define S(a, k) a[(k) * TX + lane]
 
   const float dts = p.dts, alph = g.alph, beta = 1.0f - alph, asq = alph * alph;
@@ -85,6 +85,10 @@ __global__ void __launch_bounds__(TX * NW, 3) k_sound_tile(DGrid g, SoundIO io, 
     const float dtv_j = dts * LDG(&g.dtv0[i2(g, i, j)]), dtv_jp = dts * LDG(&g.dtv0[i2(g, i, j + 1)]);
     const bool openw = (g.wbc == 2 && g.ibw && i == 1), opene = (g.ebc == 2 && g.ibe && i == ni);
     const bool opens = (g.sbc == 2 && g.ibs && j == 1), openn = (g.nbc == 2 && g.ibn && j == nj);
+    // warps take interleaved levels (w+1, w+1+NW, ...): at any time the
+    // block's warps work on adjacent levels and share their vertical
+    // neighbours through L1
+    const long plane = (long)g.NI * g.NJ;
 #pragma unroll 1
     for (int m = 0; m < KPT; m++) {
       const int k = 1 + w + m * NW;
@@ -94,13 +98,15 @@ __global__ void __launch_bounds__(TX * NW, 3) k_sound_tile(DGrid g, SoundIO io, 
       const long ov = iV(g, i, j, k), ovp = ov + g.NI;
       // ---- loads (all independent)
       const float pia = LDG(&io.piadv[o]);
+      const float pid = (k > 1) ? LDG(&io.piadv[o - plane]) : 0.0f;
+      const float thd = (k > 1) ? LDG(&io.thv[o - plane]) : 0.0f;
+      const float ppm = (k > 1) ? io.pp_in[o - plane] : 0.0f;
+      const float wk = io.w_in[o];
       const float piw = LDG(&io.piadv[o - 1]), pie = LDG(&io.piadv[o + 1]);
       const float pis = LDG(&io.piadv[o - g.NI]), pin = LDG(&io.piadv[o + g.NI]);
-      const float pid = (k > 1) ? LDG(&io.piadv[o - (long)g.NI * g.NJ]) : 0.0f;
-      const float piu = (k < nk) ? LDG(&io.piadv[o + (long)g.NI * g.NJ]) : 0.0f;
+      const float piu = (k < nk) ? LDG(&io.piadv[o + plane]) : 0.0f;
       const float thc = LDG(&io.thv[o]), thw = LDG(&io.thv[o - 1]), the = LDG(&io.thv[o + 1]);
       const float ths = LDG(&io.thv[o - g.NI]), thn = LDG(&io.thv[o + g.NI]);
-      const float thd = (k > 1) ? LDG(&io.thv[o - (long)g.NI * g.NJ]) : 0.0f;
       const float ppc = LDG(&io.ppd_in[o]), ppw = LDG(&io.ppd_in[o - 1]), ppe = LDG(&io.ppd_in[o + 1]);
       const float pps = LDG(&io.ppd_in[o - g.NI]), ppn = LDG(&io.ppd_in[o + g.NI]);
       const float u0v = LDG(&io.u_in[ou]), u1v = LDG(&io.u_in[oup]);
@@ -108,12 +114,9 @@ __global__ void __launch_bounds__(TX * NW, 3) k_sound_tile(DGrid g, SoundIO io, 
       const float ut0 = LDG(&io.uten[ou]), ut1 = LDG(&io.uten[oup]);
       const float vt0 = LDG(&io.vten[ov]), vt1 = LDG(&io.vten[ovp]);
       const float pptn = LDG(&io.ppten[o]), pptm = LDG(&io.ppterm[o]);
-      const float wk = io.w_in[o];
-      const float wkp = (k < nk) ? io.w_in[o + (long)g.NI * g.NJ] : 0.0f;
+      const float wkp = (k < nk) ? io.w_in[o + plane] : 0.0f;
       const float pp = io.pp_in[o];
-      const float ppm = (k > 1) ? io.pp_in[o - (long)g.NI * g.NJ] : 0.0f;
       const float wtn = LDG(&io.wten[o]);
-      const float accw = p.first ? LDG(&io.wa[o]) * beta : io.rrw[o];
       const float accu0 = p.first ? 0.0f : io.rru[ou];
       const float accv0 = p.first ? 0.0f : io.rrv[ov];
       // ---- u at faces i, i+1 and v at faces j, j+1
@@ -177,8 +180,6 @@ __global__ void __launch_bounds__(TX * NW, 3) k_sound_tile(DGrid g, SoundIO io, 
         S(MM, k) = mm;
         S(DD, k) = wk + fwk;
       }
-      S(PO, k) = pp;
-      S(AC, k) = accw;
       if (k == 1) S(DD, 1) = wk;
     }
   }
@@ -191,15 +192,16 @@ __global__ void __launch_bounds__(TX * NW, 3) k_sound_tile(DGrid g, SoundIO io, 
       const float mm = S(MM, k);
       const float bb = 1.0f - asq * (+mm * (-S(P1, k) + S(P2, k - 1)));
       const float dd = S(DD, k) + alph * (-mm * (S(PF, k) - S(PF, k - 1)));
+      // __frcp_rn is the correctly rounded 1/x, the same value as 1.0f/x
       if (k == 2) {
         const float cc = -asq * (-mm * S(P2, k));
-        const float rr = 1.0f / bb;
+        const float rr = __frcp_rn(bb);
         d1p = -cc * rr;
         d2p = dd * rr;
         S(MM, k) = d1p; S(DD, k) = d2p;
       } else {
         const float aa = -asq * (+mm * S(P1, k - 1));
-        const float rr = 1.0f / (aa * d1p + bb);
+        const float rr = __frcp_rn(aa * d1p + bb);
         if (k < nk) {
           const float cc = -asq * (-mm * S(P2, k));
           d1p = -cc * rr;
@@ -229,17 +231,244 @@ __global__ void __launch_bounds__(TX * NW, 3) k_sound_tile(DGrid g, SoundIO io, 
       const float wkp = (k < nk) ? S(DD, k + 1) : 0.0f;
       float pn = S(PF, k) + alph * (wk * S(P1, k) + wkp * S(P2, k));
       if (fabsf(pn) < g.smeps) pn = 0.0f;
-      const float d1 = g.kdiv * (pn - S(PO, k));
+      // pi' before the step and the running sum of w are re-read here (the
+      // column's own points, still in L2 from phase 1)
+      const float d1 = g.kdiv * (pn - io.pp_in[o]);
+      const float ac = p.first ? LDG(&io.wa[o]) * beta : io.rrw[o];
       io.pp_out[o] = pn;
       io.ppd_out[o] = pn + d1;
       if (p.write_ppx) io.ppx[o] = d1;
       if (k >= 2) io.w_out[o] = wk;
-      const float ac = S(AC, k);
       io.rrw[o] = p.last ? (ac + wk * alph) * p.tavg : ac + wk;
     }
   }
 #undef S
 }
+
+// ---------------------------------------------------------------------
+// Column-sweep form of one small step.  Each thread owns one column (i,j)
+// and walks it twice, with no block-wide barrier:
+//
+//  up   (k = 1..nk): the explicit updates of phase 1 above, then at once the
+//       Thomas forward elimination of level k (it needs only level k and the
+//       previous level, whose coefficients are carried in registers, as are
+//       the vertical neighbours pi_adv(k-1), theta_v(k-1), pi'(k-1), w(k+1));
+//  down (k = nk..1): back substitution fused with the pi' update, divergence
+//       damping and the w average of phase 3.
+//
+// Between the sweeps the column keeps: the LU factor dum1(k) in shared
+// memory (private to the thread), dum2(k) in w_out(k) and pi'_old+fpk in
+// ppd_out(k) -- both arrays are this column's own and are overwritten with
+// their final values on the way down; w(k) is no longer needed by the up
+// sweep once level k is done, and ppd_out is not the buffer neighbours read.
+// pk1+qk and pk2-qk are recomputed on the way down from the same inputs.
+// The arithmetic and its order are those of the tile form.
+// ---------------------------------------------------------------------
+static const int SNC_TX = 32, SNC_TY = 4;
+// grids with at least this many columns (ni*nj) use the column-sweep form
+#ifndef CM1G_SOUND_COL_MIN_COLUMNS
+#define CM1G_SOUND_COL_MIN_COLUMNS (1L << 20)
+#endif
+
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX * TY, 4) k_sound_col(DGrid g, SoundIO io, SoundStep p) {
+  constexpr int NC = TX * TY;
+  extern __shared__ float sm[];
+  const int lane = threadIdx.x, t = threadIdx.x + TX * threadIdx.y;
+  const int i = 1 + (int)blockIdx.x * TX + lane;
+  const int j = 1 + (int)blockIdx.y * TY + (int)threadIdx.y;
+  const int ni = g.ni, nj = g.nj, nk = g.nk;
+  if (i > ni || j > nj) return;     // no barriers below
+  float *D1 = sm;                   // D1[k*NC + t]: LU factor of level k
+  const float dts = p.dts, alph = g.alph, beta = 1.0f - alph, asq = alph * alph;
+  const float cp = g.c.cp, rdx = g.rdx, rdy = g.rdy, rdz = g.rdz;
+  const long plane = (long)g.NI * g.NJ;
+  const long oc = iS(g, i, j, 0), ocu = iU(g, i, j, 0), ocv = iV(g, i, j, 0);
+  const long planeU = (long)(g.NI + 1) * g.NJ, planeV = (long)g.NI * (g.NJ + 1);
+
+  // pk1+qk and pk2-qk of level k (sound.F:117-135, 188-189)
+  auto coef = [&](int k, float pid, float pia, float piu, float pptm, float *p1, float *p2) {
+    const float mhk = LDG(&g.mh[k]), rr0k = LDG(&g.rr0[k]);
+    const float temq = dts * rdz * mhk;
+    const float r2 = dts * rdz * mhk * rr0k * LDG(&g.rf0[k + 1]);
+    const float r1 = dts * rdz * mhk * rr0k * LDG(&g.rf0[k]);
+    const float c1a = LDG(&g.c1[k]), c1b = LDG(&g.c1[k + 1]), c2a = LDG(&g.c2[k]), c2b = LDG(&g.c2[k + 1]);
+    const float qk = temq * pptm;
+    const float pk2 = (k == nk) ? 0.0f : r2 * (-c2b * piu + (1.0f - c1b) * pia);
+    const float pk1 = (k == 1) ? 0.0f : r1 * (+c1a * pid + (c2a - 1.0f) * pia);
+    *p1 = pk1 + qk;
+    *p2 = pk2 - qk;
+  };
+
+  // ---------------- up ----------------
+  {
+    const float tem1pg = rdx * cp * 0.5f, tem2pg = rdy * cp * 0.5f;      // sound.F:321-322
+    const float temx = dts * 0.5f * rdx, temy = dts * 0.5f * rdy;        // sound.F:479-480
+    const float uh_i = LDG(&g.uh[i - g.ib]), vh_j = LDG(&g.vh[j - g.jb]);
+    const float uf_i = LDG(&g.uf[i - g.ib]), uf_ip = LDG(&g.uf[i + 1 - g.ib]);
+    const float vf_j = LDG(&g.vf[j - g.jb]), vf_jp = LDG(&g.vf[j + 1 - g.jb]);
+    const float dtu_i = dts * LDG(&g.dtu0[i2(g, i, j)]), dtu_ip = dts * LDG(&g.dtu0[i2(g, i + 1, j)]);
+    const float dtv_j = dts * LDG(&g.dtv0[i2(g, i, j)]), dtv_jp = dts * LDG(&g.dtv0[i2(g, i, j + 1)]);
+    const bool openw = (g.wbc == 2 && g.ibw && i == 1), opene = (g.ebc == 2 && g.ibe && i == ni);
+    const bool opens = (g.sbc == 2 && g.ibs && j == 1), openn = (g.nbc == 2 && g.ibn && j == nj);
+    // carried from the level below: pi_adv(k-1), pi_adv(k), theta_v(k-1), pi'(k-1), w(k)
+    float pid = 0.0f, pia = LDG(&io.piadv[oc + plane]), thd = 0.0f, ppm = 0.0f, wk = io.w_in[oc + plane];
+    // carried Thomas state: coefficients of level k-1 and the running factors
+    float p1m = 0.0f, p2m = 0.0f, pfm = 0.0f, d1p = 0.0f, d2p = 0.0f;
+    // the loads of level k+1 are issued before level k is computed, so each
+    // thread keeps two levels of reads in flight (none of them is written by
+    // this sweep before it is read)
+    struct LvIn {
+      float piw, pie, pis, pin, piu, thc, thw, the, ths, thn, ppc, ppw, ppe, pps, ppn;
+      float u0v, u1v, v0v, v1v, ut0, ut1, vt0, vt1, pptn, pptm, wkp, pp, wtn, accu0, accv0;
+    };
+    auto load = [&](int k, LvIn &L) {
+      const long o = oc + k * plane, ou = ocu + k * planeU, oup = ou + 1, ov = ocv + k * planeV, ovp = ov + g.NI;
+      L.piw = LDG(&io.piadv[o - 1]); L.pie = LDG(&io.piadv[o + 1]);
+      L.pis = LDG(&io.piadv[o - g.NI]); L.pin = LDG(&io.piadv[o + g.NI]);
+      L.piu = (k < nk) ? LDG(&io.piadv[o + plane]) : 0.0f;
+      L.thc = LDG(&io.thv[o]); L.thw = LDG(&io.thv[o - 1]); L.the = LDG(&io.thv[o + 1]);
+      L.ths = LDG(&io.thv[o - g.NI]); L.thn = LDG(&io.thv[o + g.NI]);
+      L.ppc = LDG(&io.ppd_in[o]); L.ppw = LDG(&io.ppd_in[o - 1]); L.ppe = LDG(&io.ppd_in[o + 1]);
+      L.pps = LDG(&io.ppd_in[o - g.NI]); L.ppn = LDG(&io.ppd_in[o + g.NI]);
+      L.u0v = LDG(&io.u_in[ou]); L.u1v = LDG(&io.u_in[oup]);
+      L.v0v = LDG(&io.v_in[ov]); L.v1v = LDG(&io.v_in[ovp]);
+      L.ut0 = LDG(&io.uten[ou]); L.ut1 = LDG(&io.uten[oup]);
+      L.vt0 = LDG(&io.vten[ov]); L.vt1 = LDG(&io.vten[ovp]);
+      L.pptn = LDG(&io.ppten[o]); L.pptm = LDG(&io.ppterm[o]);
+      L.wkp = (k < nk) ? io.w_in[o + plane] : 0.0f;
+      L.pp = io.pp_in[o];
+      L.wtn = LDG(&io.wten[o]);
+      L.accu0 = p.first ? 0.0f : io.rru[ou];
+      L.accv0 = p.first ? 0.0f : io.rrv[ov];
+    };
+    LvIn cur, nxt;
+    load(1, cur);
+#pragma unroll 1
+    for (int k = 1; k <= nk; k++) {
+      if (k < nk) load(k + 1, nxt);
+      const long o = oc + k * plane, ou = ocu + k * planeU, oup = ou + 1, ov = ocv + k * planeV, ovp = ov + g.NI;
+      const float piw = cur.piw, pie = cur.pie, pis = cur.pis, pin = cur.pin, piu = cur.piu;
+      const float thc = cur.thc, thw = cur.thw, the = cur.the, ths = cur.ths, thn = cur.thn;
+      const float ppc = cur.ppc, ppw = cur.ppw, ppe = cur.ppe, pps = cur.pps, ppn = cur.ppn;
+      const float u0v = cur.u0v, u1v = cur.u1v, v0v = cur.v0v, v1v = cur.v1v;
+      const float ut0 = cur.ut0, ut1 = cur.ut1, vt0 = cur.vt0, vt1 = cur.vt1;
+      const float pptn = cur.pptn, pptm = cur.pptm, wkp = cur.wkp, pp = cur.pp, wtn = cur.wtn;
+      const float accu0 = cur.accu0, accv0 = cur.accv0;
+      // ---- u at faces i, i+1 and v at faces j, j+1 (sound.F:321-341, bc.F:2392-2686)
+      float uo = u0v;
+      if (openw) uo = uo + dts * (-RJK(g, io.radbcw, j, k) * (u1v - u0v) * rdx * LDG(&g.uh[1 - g.ib]) + ut0);
+      const float un0 = uo + dtu_i * (ut0 - tem1pg * (ppc - ppw) * uf_i * (thc + thw));
+      float uop = u1v;
+      if (opene) uop = uop + dts * (-RJK(g, io.radbce, j, k) * (u1v - u0v) * rdx * LDG(&g.uh[ni - g.ib]) + ut1);
+      const float unp = uop + dtu_ip * (ut1 - tem1pg * (ppe - ppc) * uf_ip * (the + thc));
+      float vo = v0v;
+      if (opens) vo = vo + dts * (-RIK(g, io.radbcs, i, k) * (v1v - v0v) * rdy * LDG(&g.vh[1 - g.jb]) + vt0);
+      const float vn0 = vo + dtv_j * (vt0 - tem2pg * (ppc - pps) * vf_j * (thc + ths));
+      float vop = v1v;
+      if (openn) vop = vop + dts * (-RIK(g, io.radbcn, i, k) * (v1v - v0v) * rdy * LDG(&g.vh[nj - g.jb]) + vt1);
+      const float vnp = vop + dtv_jp * (vt1 - tem2pg * (ppn - ppc) * vf_jp * (thn + thc));
+      io.u_out[ou] = un0;
+      io.v_out[ov] = vn0;
+      if (p.last) {
+        io.rru[ou] = (accu0 + un0) * p.tavg;
+        io.rrv[ov] = (accv0 + vn0) * p.tavg;
+      } else {
+        io.rru[ou] = accu0 + un0;
+        io.rrv[ov] = accv0 + vn0;
+      }
+      if (i == ni) {
+        io.u_out[oup] = unp;
+        const float a1 = p.first ? 0.0f : io.rru[oup];
+        io.rru[oup] = p.last ? (a1 + unp) * p.tavg : a1 + unp;
+      }
+      if (j == nj) {
+        io.v_out[ovp] = vnp;
+        const float a1 = p.first ? 0.0f : io.rrv[ovp];
+        io.rrv[ovp] = p.last ? (a1 + vnp) * p.tavg : a1 + vnp;
+      }
+      float p1, p2;
+      coef(k, pid, pia, piu, pptm, &p1, &p2);
+      // ---- fpk (sound.F:486-498)
+      float div = (unp - un0) * rdx * uh_i + (vnp - vn0) * rdy * vh_j;
+      if (fabsf(div) < g.smeps) div = 0.0f;
+      const float X = un0 * (pia - piw) + unp * (pie - pia);
+      const float Y = vn0 * (pia - pis) + vnp * (pin - pia);
+      const float A = dts * (pptn - pptm * div);
+      const float B = -(X * temx * uh_i) - Y * temy * vh_j;
+      const float C = beta * (wk * p1 + wkp * p2);
+      const float fpk = (A + B) + C;
+      const float pf = pp + fpk;
+      io.ppd_out[o] = pf;                               // kept for the down sweep
+      if (k >= 2) {
+        // ---- Thomas forward elimination of level k (sound.F:659-733)
+        const float temm = dts * rdz * cp * LDG(&g.mf[k]);
+        const float mm = temm * (LDG(&g.c2[k]) * thc + LDG(&g.c1[k]) * thd);
+        const float fwk = dts * wtn + beta * (-mm * (pp - ppm));
+        const float ddk = wk + fwk;
+        const float bb = 1.0f - asq * (+mm * (-p1 + p2m));
+        const float dd = ddk + alph * (-mm * (pf - pfm));
+        // __frcp_rn is the correctly rounded 1/x, the same value as 1.0f/x
+        if (k == 2) {
+          const float cc = -asq * (-mm * p2);
+          const float rr = __frcp_rn(bb);
+          d1p = -cc * rr;
+          d2p = dd * rr;
+          D1[k * NC + t] = d1p;
+          io.w_out[o] = d2p;
+        } else {
+          const float aa = -asq * (+mm * p1m);
+          const float rr = __frcp_rn(aa * d1p + bb);
+          if (k < nk) {
+            const float cc = -asq * (-mm * p2);
+            d1p = -cc * rr;
+            d2p = (dd - aa * d2p) * rr;
+            D1[k * NC + t] = d1p;
+            io.w_out[o] = d2p;
+          } else {
+            io.w_out[o] = (dd - aa * d2p) * rr;       // w(nk)
+          }
+        }
+      }
+      // carry to level k+1
+      pid = pia; pia = piu; thd = thc; ppm = pp; wk = wkp;
+      p1m = p1; p2m = p2; pfm = pf;
+      cur = nxt;
+    }
+  }
+
+  // ---------------- down ----------------
+  {
+    float wup = 0.0f;                                   // w(k+1); w(nk+1) = 0
+    float pia = LDG(&io.piadv[oc + nk * plane]), piu = 0.0f;
+#pragma unroll 1
+    for (int k = nk; k >= 1; k--) {
+      const long o = oc + k * plane;
+      const float pid = (k > 1) ? LDG(&io.piadv[o - plane]) : 0.0f;
+      const float pptm = LDG(&io.ppterm[o]);
+      const float pf = io.ppd_out[o];
+      const float po = io.pp_in[o];
+      const float ac = p.first ? LDG(&io.wa[o]) * beta : io.rrw[o];
+      float wk;
+      if (k == nk) wk = io.w_out[o];
+      else if (k >= 2) wk = D1[k * NC + t] * wup + io.w_out[o];
+      else wk = io.w_in[o];
+      float p1, p2;
+      coef(k, pid, pia, piu, pptm, &p1, &p2);
+      float pn = pf + alph * (wk * p1 + wup * p2);
+      if (fabsf(pn) < g.smeps) pn = 0.0f;
+      const float d1 = g.kdiv * (pn - po);
+      io.pp_out[o] = pn;
+      io.ppd_out[o] = pn + d1;
+      if (p.write_ppx) io.ppx[o] = d1;
+      if (k >= 2) io.w_out[o] = wk;
+      io.rrw[o] = p.last ? (ac + wk * alph) * p.tavg : ac + wk;
+      wup = wk; piu = pia; pia = pid;
+    }
+  }
+}
+
+size_t sound_col_smem_bytes(const DGrid &g) { return (size_t)(g.nk + 2) * SNC_TX * SNC_TY * sizeof(float); }
 
 void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, int64_t *nlaunch);
 
@@ -263,7 +492,7 @@ void sound_nloop(int nsound, int nrk, float dt, int *nloop_out, float *dts_out) 
   *dts_out = dts;
 }
 
-size_t sound_smem_bytes(const DGrid &g) { return (size_t)7 * (g.nk + 2) * SND_TX * sizeof(float); }
+size_t sound_smem_bytes(const DGrid &g) { return (size_t)5 * (g.nk + 2) * SND_TX * sizeof(float); }
 int sound_max_nk() { return SND_NW * SND_KPT; }
 
 // One RK stage of acoustic steps.  At the first stage the reference starts
@@ -281,15 +510,27 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
   int nloop;
   float dts;
   sound_nloop(nsound, nrk, dt, &nloop, &dts);
-  dim3 blk(SND_TX, SND_NW);
-  dim3 grid((g.ni + SND_TX - 1) / SND_TX, g.nj);
-  size_t smem = sound_smem_bytes(g);
+  // The column-sweep form keeps one thread per column, so it needs many
+  // columns to fill the GPU; smaller grids use the tile form, whose warps
+  // split the levels of a column.
+  // CM1G_SOUND_FORM=col|tile overrides the choice (read at each call).
+  bool col = (long)g.ni * g.nj >= (long)CM1G_SOUND_COL_MIN_COLUMNS;
+  if (const char *f = getenv("CM1G_SOUND_FORM")) {
+    if (!strcmp(f, "col")) col = true;
+    else if (!strcmp(f, "tile")) col = false;
+  }
+  dim3 blk = col ? dim3(SNC_TX, SNC_TY) : dim3(SND_TX, SND_NW);
+  dim3 grid = col ? dim3((g.ni + SNC_TX - 1) / SNC_TX, (g.nj + SNC_TY - 1) / SNC_TY)
+                  : dim3((g.ni + SND_TX - 1) / SND_TX, g.nj);
+  size_t smem = col ? sound_col_smem_bytes(g) : sound_smem_bytes(g);
   static bool attr_set = false;
   if (!attr_set) {
+    cudaFuncSetAttribute(k_sound_col<SNC_TX, SNC_TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW, SND_KPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          200 * 1024);
-    cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW, SND_KPT>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         cudaSharedmemCarveoutMaxShared);
+    // three blocks of 5 column arrays each; the rest of the unified L1 stays
+    // cache for the neighbour reads of phase 1
+    cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW, SND_KPT>, cudaFuncAttributePreferredSharedMemoryCarveout, 70);
     attr_set = true;
   }
   const float *uin = (nrk == 1) ? u3d : ua, *vin = (nrk == 1) ? v3d : va, *ppdin = ppx;
@@ -310,7 +551,11 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
     SoundStep sp;
     sp.dts = dts; sp.tavg = 1.0f / (float)nloop;
     sp.first = (n == 1); sp.last = (n == nloop); sp.write_ppx = (nrk == 3 && n == nloop);
-    { ProfScope _ps("k_sound_step", st); k_sound_tile<SND_TX, SND_NW, SND_KPT><<<grid, blk, smem, st>>>(g, io, sp); }
+    {
+      ProfScope _ps("k_sound_step", st);
+      if (col) k_sound_col<SNC_TX, SNC_TY><<<grid, blk, smem, st>>>(g, io, sp);
+      else k_sound_tile<SND_TX, SND_NW, SND_KPT><<<grid, blk, smem, st>>>(g, io, sp);
+    }
     if (nl) *nl += 1;
     if (n < nloop) launch_bc(g, io.ppd_out, 2, 0, st, nl);
     uin = io.u_out; vin = io.v_out; ppdin = io.ppd_out;

@@ -3,6 +3,11 @@ diagnostics (the in-process counterpart of running cm1.exe through the
 reference's cm1/run.py).
 
     python -m cm1_b200.run --workload supercell --steps 10 [--ni 128 --nj 128 --nk 80] [--graph]
+                           [--time] [--profile]
+
+--time reports the device time per large step (CUDA events around the steps,
+after one untimed step); --profile reports per-kernel device time per step,
+the counterpart of the reference's timestats table.
 """
 import argparse
 import json
@@ -20,6 +25,8 @@ def main(argv=None):
     ap.add_argument("--nk", type=int)
     ap.add_argument("--graph", action="store_true")
     ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--time", action="store_true")
+    ap.add_argument("--profile", action="store_true")
     args = ap.parse_args(argv)
 
     import torch
@@ -31,8 +38,31 @@ def main(argv=None):
     ctx = binding.Context(case.cfg, case.grid)
     dev = binding.to_device(case.state)
     mass2 = cfl = None
-    for _ in range(args.steps):
-        mass2, cfl = ctx.step(dev, case.dt, case.mass1, use_graph=args.graph)
+    timing = {}
+    if args.time or args.profile:
+        mass2, cfl = ctx.step(dev, case.dt, case.mass1, use_graph=args.graph)   # untimed
+        steps = max(args.steps - 1, 1)
+        if args.profile:
+            ctx.profile(True)
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(steps):
+            mass2, cfl = ctx.step(dev, case.dt, case.mass1, use_graph=args.graph)
+        t1.record()
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1) / steps
+        cells = case.lay.ni * case.lay.nj * case.lay.nk
+        timing = {"ms_per_step": ms, "cell_updates_per_s": cells / (ms * 1e-3)}
+        if args.profile:
+            prof = ctx.profile_read()
+            ctx.profile(False)
+            timing["kernel_ms_per_step"] = {k: v[1] / steps for k, v in
+                                            sorted(prof.items(), key=lambda kv: -kv[1][1])}
+            timing["launches_per_step"] = {k: v[0] / steps for k, v in prof.items()}
+    else:
+        for _ in range(args.steps):
+            mass2, cfl = ctx.step(dev, case.dt, case.mass1, use_graph=args.graph)
     torch.cuda.synchronize()
     lay = case.lay
     wmax, _, wloc = ctx.maxmin(dev["w3d"], 4)
@@ -41,6 +71,7 @@ def main(argv=None):
            "max_w": wmax, "max_w_at": wloc[:3], "min_pp": ppmin, "min_pp_at": ploc[3:],
            "mass1": case.mass1, "mass2": mass2, "cflmax": cfl, "kernels": ctx.launches(),
            "theta_max": float(dev["th3d"][lay.interior(1)].max().item())}
+    out.update(timing)
     print(json.dumps(out))
     ctx.close()
     return 0 if np.isfinite(out["max_w"]) else 1

@@ -73,6 +73,13 @@ def test_one_large_step(name, over, cm1g, oracle_lib):
     assert ctx.launches() > 0
 
 
+@pytest.mark.parametrize("name,over", [CASES[1], CASES[3]])
+def test_one_large_step_column_sweep_sound(name, over, cm1g, oracle_lib, monkeypatch):
+    """The same step with the column-sweep acoustic kernel (the form large grids use)."""
+    monkeypatch.setenv("CM1G_SOUND_FORM", "col")
+    test_one_large_step(name, over, cm1g, oracle_lib)
+
+
 def test_many_steps_budgets(cm1g, oracle_lib):
     """Extrema and budgets after 20 steps of the dry bubble (c0 sizes)."""
     torch = _torch()

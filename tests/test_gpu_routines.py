@@ -118,10 +118,13 @@ def test_advuvw(bc, cm1g, oracle_lib):
     assert relerr(d["wt"].cpu().numpy()[sw], rwt[sw]) <= 1e-6
 
 
+@pytest.mark.parametrize("form", ["tile", "col"])
 @pytest.mark.parametrize("bc", [1, 2])
 @pytest.mark.parametrize("nrk", [1, 2, 3])
-def test_sound_stage(bc, nrk, cm1g, oracle_lib):
+def test_sound_stage(bc, nrk, form, cm1g, oracle_lib, monkeypatch):
+    """Both forms of the acoustic kernel (3-phase tile, column sweep)."""
     _torch()
+    monkeypatch.setenv("CM1G_SOUND_FORM", form)
     case = make_case("supercell", ni=24, nj=20, nk=24, bc=bc)
     lay, st, gr = case.lay, case.state, case.grid
     rng = np.random.default_rng(5 + nrk)
