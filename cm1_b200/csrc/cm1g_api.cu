@@ -17,6 +17,8 @@
 
 namespace cm1g {
 void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, int64_t *nlaunch);
+void launch_bc_batch(const DGrid &g, float *const *arrays, const int *which, const int *wflag, int n,
+                     cudaStream_t st, int64_t *nlaunch);
 void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w, const float *uten1,
                          const float *vten1, const float *wten1, float *uten, float *vten, float *wten,
                          const float *th3d, const float *qv, cudaStream_t st, int64_t *nl);
@@ -484,23 +486,26 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
     if (nrk == 3)
       launch_prs_rho(g, d->pp3d, buf_out(0, 3), cf.imoist ? buf_out(iqv, 3) : nullptr, cf.imoist, d->prs, d->rho,
                      c->part3, c->part4, cf.apmasscon == 1, st, nl);
-    // bcs (solve2.F:1663-1707)
-    launch_bc(g, d->u3d, 3, 0, st, nl);
-    launch_bc(g, d->v3d, 4, 0, st, nl);
-    launch_bc(g, d->w3d, 5, 1, st, nl);
-    if (nrk < 3) {
-      launch_bc(g, d->rho, 2, 0, st, nl);
-      launch_bc(g, d->pp3d, 2, 0, st, nl);
-      launch_bc(g, buf_out(0, nrk), 1, 0, st, nl);
-      for (int n = 0; n < numq; n++) launch_bc(g, buf_out(1 + n, nrk), 1, 0, st, nl);
-    }
     // passive tracers (solve2.F:1880-1970)
     for (int n = 0; n < npt; n++) {
       const int s = 1 + numq + n;
       const int pdef = (nrk == 3 && cf.pdtra == 1) ? 1 : 0;
       launch_advs_tiled(g, c->rru, c->rrv, c->rrw, buf_in(s, nrk), base[s], 0, ten1[s], nullptr, buf_out(s, nrk),
                         weno, pdef, 1, (double)(1.0f * 1.0e-18f), dttmp, 0, c->pdefscr, st, nl);
-      if (nrk <= 2) launch_bc(g, buf_out(s, nrk), 1, 0, st, nl);
+    }
+    // halo fills of the stage (solve2.F:1663-1707 and the tracers' bcs of
+    // solve2.F:1959-1961), batched into one two-phase launch: every array is
+    // distinct and nothing between their reference positions and here reads
+    // their halos
+    {
+      std::vector<float *> arr{d->u3d, d->v3d, d->w3d};
+      std::vector<int> which{3, 4, 5}, flag{0, 0, 1};
+      if (nrk < 3) {
+        arr.push_back(d->rho); which.push_back(2); flag.push_back(0);
+        arr.push_back(d->pp3d); which.push_back(2); flag.push_back(0);
+        for (int s = 0; s < nsc; s++) { arr.push_back(buf_out(s, nrk)); which.push_back(1); flag.push_back(0); }
+      }
+      launch_bc_batch(g, arr.data(), which.data(), flag.data(), (int)arr.size(), st, nl);
     }
     // dry-air mass fix (solve2.F:1976-2033)
     if (nrk == 3 && cf.apmasscon == 1)
@@ -508,10 +513,15 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
                      c->part3, c->part4, mass1, c->dscal, c->fscal, st, nl);
   }
   // tracers after the RK loop (solve2.F:2064-2075)
+  std::vector<float *> tr;
   for (int n = 0; n < npt; n++) {
     float *pt = d->pt3d + n * ns;
     if (cf.pdtra == 1) launch_pdefq(g, 0.0f, d->rho, pt, nullptr, nullptr, st, nl);
-    launch_bc(g, pt, 1, 0, st, nl);
+    tr.push_back(pt);
+  }
+  if (npt) {
+    std::vector<int> which(npt, 1);
+    launch_bc_batch(g, tr.data(), which.data(), nullptr, npt, st, nl);
   }
   (void)open;
 }
@@ -525,12 +535,14 @@ static void run_solve3(cm1g_ctx *c, const cm1g_state_t *d) {
   const int numq = cf.imoist ? cf.numq : 0, npt = cf.iptra ? cf.npt : 0;
   const int ni = g.ni, nj = g.nj;
   // solve3.F:246-311
-  launch_bc(g, d->pp3d, 2, 0, st, nl);
-  launch_bc(g, d->th3d, 1, 0, st, nl);
-  for (int n = 0; n < numq; n++) launch_bc(g, d->q3d + n * ns, 1, 0, st, nl);
+  {
+    std::vector<float *> arr{d->pp3d, d->th3d, d->rho};
+    std::vector<int> which{2, 1, 2};
+    for (int n = 0; n < numq; n++) { arr.push_back(d->q3d + n * ns); which.push_back(1); }
+    launch_bc_batch(g, arr.data(), which.data(), nullptr, (int)arr.size(), st, nl);
+  }
   launch_ppx_update(g, d->pp3d, d->ppx, st, nl);
   launch_bc(g, d->ppx, 2, 0, st, nl);
-  launch_bc(g, d->rho, 2, 0, st, nl);
   // solve3.F:546-640 rollover
   launch_copy_range(g, 2, 0, ni + 2, 0, nj + 2, d->u3d, d->ua, st, nl);
   launch_copy_range(g, 3, 0, ni + 2, 0, nj + 2, d->v3d, d->va, st, nl);

@@ -863,6 +863,8 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
 }
 
 void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, int64_t *nlaunch);
+void launch_bc_batch(const DGrid &g, float *const *arrays, const int *which, const int *wflag, int n,
+                     cudaStream_t st, int64_t *nlaunch);
 
 static const int ADV_TX = 32, ADV_TY = 8, ADV_KC = 16;
 
@@ -891,8 +893,11 @@ void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const
     if (weno) k_advs_tile<ADV_TX, ADV_TY, ADV_KC, MODE_PDEF1, 1><<<grid, blk, 0, st>>>(g, a, o, 1, pdefweno, weps, dt, flush);
     else k_advs_tile<ADV_TX, ADV_TY, ADV_KC, MODE_PDEF1, 0><<<grid, blk, 0, st>>>(g, a, o, 1, pdefweno, weps, dt, flush);
   }
-  launch_bc(g, o.dumx, 1, 0, st, nl);
-  launch_bc(g, o.dumy, 1, 0, st, nl);
+  {
+    float *arr[2] = {o.dumx, o.dumy};
+    const int which[2] = {1, 1};
+    launch_bc_batch(g, arr, which, nullptr, 2, st, nl);
+  }
   const int bx = 128;
   dim3 g2((g.ni + bx - 1) / bx, g.nj, g.nk);
   { ProfScope _ps("k_advs_pdef2", st); k_advs_pdef2<<<g2, bx, 0, st>>>(g, a, o.advx, o.advy, o.advz, o.dumx, o.dumy, o.dumz, ten1, nullptr, snew, s0, dt, flush); }

@@ -11,16 +11,15 @@
 namespace cm1g {
 
 enum Stag { STAG_S = 1, STAG_U = 2, STAG_V = 3, STAG_W = 4 };
+static const int BC_MAXB = 16;
 
 __device__ __forceinline__ long idxStag(const DGrid &g, int stag, int i, int j, int k) {
   return stag == STAG_U ? iU(g, i, j, k) : stag == STAG_V ? iV(g, i, j, k) : iS(g, i, j, k);
 }
 
-// West/east fills.  Thread x runs along j over the widest range any branch
-// uses (jb..je+1), blockIdx.y is k.
-__global__ void k_bc_x(DGrid g, float *__restrict__ a, int stag, int pmode) {
-  const int j = g.jb + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int k = (int)blockIdx.y + (stag == STAG_W ? 2 : 1);
+// West/east fills of row j, level k (j over the widest range any branch
+// uses, jb..je+1).
+__device__ __forceinline__ void bc_x_row(const DGrid &g, float *__restrict__ a, int stag, int pmode, int j, int k) {
   const int ni = g.ni, nj = g.nj, ng = g.ngxy;
   const int jeS = nj + ng + (stag == STAG_V ? 1 : 0);  // je or je+1
   if (j > jeS) return;
@@ -75,20 +74,20 @@ __global__ void k_bc_x(DGrid g, float *__restrict__ a, int stag, int pmode) {
   }
 }
 
-// South/north fills (and w's top/bottom zeros).  Thread x runs along i over
-// ib..ie+1, blockIdx.y is k (for w, k=2..nk, plus one extra plane for the
-// top/bottom zeros of bcw(flag=1)).
-__global__ void k_bc_y(DGrid g, float *__restrict__ a, int stag, int pmode, int wflag) {
-  const int i = g.ib + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+// South/north fills of column i, plane kp (and w's top/bottom zeros).  i runs
+// over ib..ie+1; kp = 0.. covers k = 1..nk (w: k = 2..nk, then one extra plane
+// for the top/bottom zeros of bcw(flag=1)).
+__device__ __forceinline__ void bc_y_col(const DGrid &g, float *__restrict__ a, int stag, int pmode, int wflag, int i,
+                                         int kp) {
   const int ni = g.ni, nj = g.nj, nk = g.nk, ng = g.ngxy;
   const int ieS = ni + ng + (stag == STAG_U ? 1 : 0);
   if (i > ieS) return;
-  if (stag == STAG_W && (int)blockIdx.y == nk - 1) {  // extra plane: bc.F:1127-1137
+  if (stag == STAG_W && kp == nk - 1) {  // extra plane: bc.F:1127-1137
     if (wflag == 1 && i >= 0 && i <= ni + 1)
       for (int j = 0; j <= nj + 1; j++) { a[iW(g, i, j, 1)] = 0.0f; a[iW(g, i, j, nk + 1)] = 0.0f; }
     return;
   }
-  const int k = (int)blockIdx.y + (stag == STAG_W ? 2 : 1);
+  const int k = kp + (stag == STAG_W ? 2 : 1);
   if (pmode) {  // bcp rows (bc.F:458-518)
     if (i < 0 || i > ni + 1) return;
     if (g.sbc == 1) a[iS(g, i, 0, k)] = a[iS(g, i, nj, k)];
@@ -143,22 +142,56 @@ __global__ void k_bc_y(DGrid g, float *__restrict__ a, int stag, int pmode, int 
   }
 }
 
-// Host launcher: which = 1 bcs, 2 bcp, 3 bcu, 4 bcv, 5 bcw.
-void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, int64_t *nlaunch) {
-  int stag = which == 3 ? STAG_U : which == 4 ? STAG_V : which == 5 ? STAG_W : STAG_S;
-  int pmode = (which == 2);
-  int nkk = (stag == STAG_W) ? g.nk - 1 : g.nk;
-  dim3 blk(128);
-  dim3 gx((g.NJ + 1 + 127) / 128, nkk);
-  dim3 gy((g.NI + 1 + 127) / 128, nkk + (stag == STAG_W ? 1 : 0));
-  if (stag == STAG_V) {
-    { ProfScope _ps("k_bc_y", st); k_bc_y<<<gy, blk, 0, st>>>(g, a, stag, pmode, wflag); }
-    { ProfScope _ps("k_bc_x", st); k_bc_x<<<gx, blk, 0, st>>>(g, a, stag, pmode); }
+// One launch runs one phase for up to BC_MAXB arrays: blockIdx.z picks the
+// array, and the array's own order decides whether this phase is its x or y
+// fill (bcv fills south/north first).  Arrays in a batch must be distinct.
+struct BcBatch {
+  float *a[BC_MAXB];
+  int stag[BC_MAXB], pmode[BC_MAXB], wflag[BC_MAXB];
+  int n;
+};
+
+__global__ void k_bc_phase(DGrid g, BcBatch b, int phase) {
+  const int n = (int)blockIdx.z;
+  const int stag = b.stag[n];
+  const bool yfirst = (stag == STAG_V);
+  const bool doy = (phase == 0) ? yfirst : !yfirst;
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x), kp = (int)blockIdx.y;
+  const int nkk = (stag == STAG_W) ? g.nk - 1 : g.nk;
+  if (doy) {
+    if (kp > nkk - (stag == STAG_W ? 0 : 1)) return;
+    bc_y_col(g, b.a[n], stag, b.pmode[n], b.wflag[n], g.ib + t, kp);
   } else {
-    { ProfScope _ps("k_bc_x", st); k_bc_x<<<gx, blk, 0, st>>>(g, a, stag, pmode); }
-    { ProfScope _ps("k_bc_y", st); k_bc_y<<<gy, blk, 0, st>>>(g, a, stag, pmode, wflag); }
+    if (kp >= nkk) return;
+    bc_x_row(g, b.a[n], stag, b.pmode[n], g.jb + t, kp + (stag == STAG_W ? 2 : 1));
   }
-  if (nlaunch) *nlaunch += 2;
+}
+
+static int bc_stag(int which) { return which == 3 ? STAG_U : which == 4 ? STAG_V : which == 5 ? STAG_W : STAG_S; }
+
+// which = 1 bcs, 2 bcp, 3 bcu, 4 bcv, 5 bcw, for each array of the list.
+void launch_bc_batch(const DGrid &g, float *const *arrays, const int *which, const int *wflag, int n,
+                     cudaStream_t st, int64_t *nlaunch) {
+  for (int base = 0; base < n; base += BC_MAXB) {
+    BcBatch b{};
+    b.n = (n - base < BC_MAXB) ? n - base : BC_MAXB;
+    for (int q = 0; q < b.n; q++) {
+      b.a[q] = arrays[base + q];
+      b.stag[q] = bc_stag(which[base + q]);
+      b.pmode[q] = (which[base + q] == 2);
+      b.wflag[q] = wflag ? wflag[base + q] : 0;
+    }
+    dim3 blk(128);
+    const int span = (g.NI > g.NJ ? g.NI : g.NJ) + 1;
+    dim3 grid((span + 127) / 128, g.nk, b.n);
+    { ProfScope _ps("k_bc_phase", st); k_bc_phase<<<grid, blk, 0, st>>>(g, b, 0); }
+    { ProfScope _ps("k_bc_phase", st); k_bc_phase<<<grid, blk, 0, st>>>(g, b, 1); }
+    if (nlaunch) *nlaunch += 2;
+  }
+}
+
+void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, int64_t *nlaunch) {
+  launch_bc_batch(g, &a, &which, &wflag, 1, st, nlaunch);
 }
 
 }  // namespace cm1g

@@ -46,7 +46,25 @@ struct SoundIO {
 struct SoundStep {
   float dts, tavg;
   int first, last, write_ppx;
+  int ppd_mapped;   // ppd_in's halo is not filled: read bcp's source points instead
 };
+
+// Offsets of the west/east/south/north neighbours of ppd at (i,j).  From the
+// second small step on, ppd_in comes from the previous step of this kernel
+// and its 1-point halo is not filled; the value bcp would put there
+// (bc.F:380-518: periodic wrap, else the adjacent interior point) is read
+// from the point bcp copies it from.
+struct PpdNbr { long w, e, s, n; };
+__device__ __forceinline__ PpdNbr ppd_nbr(const DGrid &g, int mapped, int i, int j) {
+  PpdNbr d{-1L, 1L, -(long)g.NI, (long)g.NI};
+  if (mapped) {
+    if (i == 1) d.w = (g.wbc == 1) ? (long)(g.ni - 1) : 0L;
+    if (i == g.ni) d.e = (g.ebc == 1) ? -(long)(g.ni - 1) : 0L;
+    if (j == 1) d.s = (g.sbc == 1) ? (long)(g.nj - 1) * g.NI : 0L;
+    if (j == g.nj) d.n = (g.nbc == 1) ? -(long)(g.nj - 1) * g.NI : 0L;
+  }
+  return d;
+}
 
 #define RJK(g, a, j, k) ((a)[((j) - (g).jb) + (long)(g).NJ * (k)])
 #define RIK(g, a, i, k) ((a)[((i) - (g).ib) + (long)(g).NI * (k)])
@@ -85,6 +103,7 @@ __global__ void __launch_bounds__(TX * NW, 3) k_sound_tile(DGrid g, SoundIO io, 
     const float dtv_j = dts * LDG(&g.dtv0[i2(g, i, j)]), dtv_jp = dts * LDG(&g.dtv0[i2(g, i, j + 1)]);
     const bool openw = (g.wbc == 2 && g.ibw && i == 1), opene = (g.ebc == 2 && g.ibe && i == ni);
     const bool opens = (g.sbc == 2 && g.ibs && j == 1), openn = (g.nbc == 2 && g.ibn && j == nj);
+    const PpdNbr pn_ = ppd_nbr(g, p.ppd_mapped, i, j);
     // warps take interleaved levels (w+1, w+1+NW, ...): at any time the
     // block's warps work on adjacent levels and share their vertical
     // neighbours through L1
@@ -107,8 +126,8 @@ __global__ void __launch_bounds__(TX * NW, 3) k_sound_tile(DGrid g, SoundIO io, 
       const float piu = (k < nk) ? LDG(&io.piadv[o + plane]) : 0.0f;
       const float thc = LDG(&io.thv[o]), thw = LDG(&io.thv[o - 1]), the = LDG(&io.thv[o + 1]);
       const float ths = LDG(&io.thv[o - g.NI]), thn = LDG(&io.thv[o + g.NI]);
-      const float ppc = LDG(&io.ppd_in[o]), ppw = LDG(&io.ppd_in[o - 1]), ppe = LDG(&io.ppd_in[o + 1]);
-      const float pps = LDG(&io.ppd_in[o - g.NI]), ppn = LDG(&io.ppd_in[o + g.NI]);
+      const float ppc = LDG(&io.ppd_in[o]), ppw = LDG(&io.ppd_in[o + pn_.w]), ppe = LDG(&io.ppd_in[o + pn_.e]);
+      const float pps = LDG(&io.ppd_in[o + pn_.s]), ppn = LDG(&io.ppd_in[o + pn_.n]);
       const float u0v = LDG(&io.u_in[ou]), u1v = LDG(&io.u_in[oup]);
       const float v0v = LDG(&io.v_in[ov]), v1v = LDG(&io.v_in[ovp]);
       const float ut0 = LDG(&io.uten[ou]), ut1 = LDG(&io.uten[oup]);
@@ -311,6 +330,7 @@ __global__ void __launch_bounds__(TX * TY, 4) k_sound_col(DGrid g, SoundIO io, S
     const float dtv_j = dts * LDG(&g.dtv0[i2(g, i, j)]), dtv_jp = dts * LDG(&g.dtv0[i2(g, i, j + 1)]);
     const bool openw = (g.wbc == 2 && g.ibw && i == 1), opene = (g.ebc == 2 && g.ibe && i == ni);
     const bool opens = (g.sbc == 2 && g.ibs && j == 1), openn = (g.nbc == 2 && g.ibn && j == nj);
+    const PpdNbr pn_ = ppd_nbr(g, p.ppd_mapped, i, j);
     // carried from the level below: pi_adv(k-1), pi_adv(k), theta_v(k-1), pi'(k-1), w(k)
     float pid = 0.0f, pia = LDG(&io.piadv[oc + plane]), thd = 0.0f, ppm = 0.0f, wk = io.w_in[oc + plane];
     // carried Thomas state: coefficients of level k-1 and the running factors
@@ -329,8 +349,8 @@ __global__ void __launch_bounds__(TX * TY, 4) k_sound_col(DGrid g, SoundIO io, S
       L.piu = (k < nk) ? LDG(&io.piadv[o + plane]) : 0.0f;
       L.thc = LDG(&io.thv[o]); L.thw = LDG(&io.thv[o - 1]); L.the = LDG(&io.thv[o + 1]);
       L.ths = LDG(&io.thv[o - g.NI]); L.thn = LDG(&io.thv[o + g.NI]);
-      L.ppc = LDG(&io.ppd_in[o]); L.ppw = LDG(&io.ppd_in[o - 1]); L.ppe = LDG(&io.ppd_in[o + 1]);
-      L.pps = LDG(&io.ppd_in[o - g.NI]); L.ppn = LDG(&io.ppd_in[o + g.NI]);
+      L.ppc = LDG(&io.ppd_in[o]); L.ppw = LDG(&io.ppd_in[o + pn_.w]); L.ppe = LDG(&io.ppd_in[o + pn_.e]);
+      L.pps = LDG(&io.ppd_in[o + pn_.s]); L.ppn = LDG(&io.ppd_in[o + pn_.n]);
       L.u0v = LDG(&io.u_in[ou]); L.u1v = LDG(&io.u_in[oup]);
       L.v0v = LDG(&io.v_in[ov]); L.v1v = LDG(&io.v_in[ovp]);
       L.ut0 = LDG(&io.uten[ou]); L.ut1 = LDG(&io.uten[oup]);
@@ -551,13 +571,13 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
     SoundStep sp;
     sp.dts = dts; sp.tavg = 1.0f / (float)nloop;
     sp.first = (n == 1); sp.last = (n == nloop); sp.write_ppx = (nrk == 3 && n == nloop);
+    sp.ppd_mapped = (n > 1);
     {
       ProfScope _ps("k_sound_step", st);
       if (col) k_sound_col<SNC_TX, SNC_TY><<<grid, blk, smem, st>>>(g, io, sp);
       else k_sound_tile<SND_TX, SND_NW, SND_KPT><<<grid, blk, smem, st>>>(g, io, sp);
     }
     if (nl) *nl += 1;
-    if (n < nloop) launch_bc(g, io.ppd_out, 2, 0, st, nl);
     uin = io.u_out; vin = io.v_out; ppdin = io.ppd_out;
   }
 }
