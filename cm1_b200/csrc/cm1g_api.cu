@@ -21,7 +21,7 @@ void launch_bc_batch(const DGrid &g, float *const *arrays, const int *which, con
                      cudaStream_t st, int64_t *nlaunch);
 void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w, const float *uten1,
                          const float *vten1, const float *wten1, float *uten, float *vten, float *wten,
-                         const float *th3d, const float *qv, cudaStream_t st, int64_t *nl);
+                         const float *th3d, const float *qv, float *divx, cudaStream_t st, int64_t *nl);
 void launch_advs(const DGrid &g, const float *rru, const float *rrv, const float *rrw, int weighted,
                  const float *divx, const float *s, const float *s0, int sadd, const float *ten1,
                  const float *thterm, float *sten_out, float *snew, int weno, int pdef, int pdefweno,
@@ -135,7 +135,7 @@ struct cm1g_ctx {
   float *su = nullptr, *sv = nullptr, *su2 = nullptr, *sv2 = nullptr, *d1 = nullptr, *d2 = nullptr;
   float *sx[2 * (1 + 2 * CM1G_MAXQ)] = {};   // per-scalar stage buffers
   float *pdefscr = nullptr;                   // 6 s-arrays
-  float *sten = nullptr;                      // s-array for cm1g_advs-free use
+  float *mdivx = nullptr;                     // divx of the momentum pass
   double *part3 = nullptr, *part4 = nullptr, *dscal = nullptr, *bud = nullptr, *lev = nullptr;
   float *fscal = nullptr;
   int *cflbits = nullptr;
@@ -308,7 +308,7 @@ extern "C" int cm1g_init(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_c
   for (int s = 0; s < 2 * nsc; s++) c->sx[s] = (float *)dalloc(c, bS);
   bool pdef_needed = cfg->imoist || (cfg->iptra && cfg->pdtra);
   c->pdefscr = (float *)dalloc(c, (pdef_needed ? 6 : 6) * bS);
-  c->sten = (float *)dalloc(c, bS);
+  c->mdivx = (float *)dalloc(c, bS);
   int nchunk = prs_nchunk(g);
   c->part3 = (double *)dalloc(c, (size_t)(g.nk + 2) * nchunk * sizeof(double));
   c->part4 = (double *)dalloc(c, (size_t)(g.nk + 2) * nchunk * sizeof(double));
@@ -464,7 +464,7 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
     launch_stage_prep(g, th_in, d->pp3d, qv_in, cf.imoist, cf.eqtset, c->t11, c->t22, c->thterm, c->piadv, st, nl);
     launch_bc(g, c->t11, 2, 0, st, nl);
     launch_adv_momentum(g, d->u3d, d->v3d, d->w3d, d->uten1, d->vten1, d->wten1, c->uten, c->vten, c->wten,
-                        th_in, qv_in, st, nl);
+                        th_in, qv_in, c->mdivx, st, nl);
     launch_sound(g, cf.nsound, nrk, dt, d->ua, d->u3d, c->uten, d->va, d->v3d, c->vten, d->wa, d->w3d, c->wten,
                  d->ppi, d->pp3d, c->piadv, d->ppten, d->ppx, c->t11, c->t22, c->rru, c->rrv, c->rrw,
                  d->radbcw, d->radbce, d->radbcs, d->radbcn, c->su, c->sv, c->su2, c->sv2, c->d1, c->d2, st, nl);
@@ -705,7 +705,7 @@ extern "C" int cm1g_advuvw(cm1g_ctx_t *c, int32_t nrk, const float *u3d, const f
   const DGrid &g = c->g;
   const float *du = S.in(u3d, nU(g), false), *dv = S.in(v3d, nV(g), false), *dw = S.in(w3d, nW(g), false);
   float *tu = S.in(uten, nU(g), true), *tv = S.in(vten, nV(g), true), *tw = S.in(wten, nW(g), true);
-  launch_adv_momentum(g, du, dv, dw, tu, tv, tw, tu, tv, tw, nullptr, nullptr, c->stream, &c->nlaunch);
+  launch_adv_momentum(g, du, dv, dw, tu, tv, tw, tu, tv, tw, nullptr, nullptr, c->mdivx, c->stream, &c->nlaunch);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
   return S.finish();

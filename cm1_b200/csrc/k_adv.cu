@@ -237,6 +237,16 @@ __device__ __forceinline__ float buoy(const DGrid &g, const float *th3d, const f
   return g.c.g * th3 * LDG(&g.rth0[k]);
 }
 
+// buoy() from values already loaded: th = th3d(i,j,kk), q = qv(i,j,kk)
+__device__ __forceinline__ float buoy_v(const DGrid &g, float th3, float qvv, bool moist, int kk) {
+  if (moist) {
+    float q = fmaxf(qvv, 0.0f);
+    float qli = fmaxf(0.0f, 0.0f + 0.0f);
+    return g.c.g * ((th3 * LDG(&g.rth0[kk]) + g.c.repsm1 * (q - LDG(&g.qv0[kk]))) - ((qli - LDG(&g.qc0[kk])) - LDG(&g.qi0[kk])));
+  }
+  return g.c.g * th3 * LDG(&g.rth0[kk]);
+}
+
 __global__ void k_advw(DGrid g, Vel q, const float *wten1, float *wten,
                        const float *__restrict__ th3d, const float *__restrict__ qv) {
   const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
@@ -275,27 +285,392 @@ __global__ void k_advw(DGrid g, Vel q, const float *wten1, float *wten,
   wten[o] = t;
 }
 
+// ---------------------------------------------------------------------
+// Tiled momentum advection (the production path of advu/advv/advw).
+//
+// divx of the momentum pass (solve2.F:590-596) is formed once per stage at
+// the s-points i = 0..ni+1, j = 0..nj+1 by k_mom_divx.  k_mom_tile then
+// works like the scalar tile: a block owns TX x TY points of one velocity
+// component (STAG 2 u, 3 v, 4 w) and marches upward; at each level the
+// component is staged with a 3-point lateral halo in shared memory, every
+// x- and y-face flux (hadv_flx5 stag=2/3/4) is evaluated once, and the
+// vertical face flux (vadv_flx5 with the lower-order pieces at the column
+// ends) comes from a per-thread register window and is carried to the next
+// level.  The face velocities are formed exactly as the reference forms
+// them (ubar/vbar/wbar of adv_routines.F:1388-1460, 3299-3384) and the
+// open-boundary fixes of adv.F are applied to the cells they concern.
+// ---------------------------------------------------------------------
+__global__ void k_mom_divx(DGrid g, Vel q, float *__restrict__ divx) {
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = (int)blockIdx.y, k = 1 + (int)blockIdx.z;
+  if (i > g.ni + 1) return;
+  divx[iS(g, i, j, k)] = DIVX(g, q, i, j, k);
+}
+
+// vertical face flux of a u/v column at w-level kk; wv[d+3] = a(kk+d), d = -3..2
+__device__ __forceinline__ float zflux_uv(const DGrid &g, const float *wv, float wbar, int kk) {
+  const int nk = g.nk;
+  auto A = [&](int d) { return wv[d + 3]; };
+  if (kk >= 4 && kk <= nk - 2) {
+    if (wbar >= 0.0f) return wbar * flx5(A(-3), A(-2), A(-1), A(0), A(1));
+    return wbar * flx5(A(2), A(1), A(0), A(-1), A(-2));
+  }
+  const float c2k = LDG(&g.c2[kk]);
+  if (kk == 2) {
+    if (wbar >= 0.0f) { float cc2 = 0.5f * (c2k + c2k), cc1 = 1.0f - cc2; return wbar * (cc1 * A(-1) + cc2 * A(0)); }
+    return wbar * flx3(A(1), A(0), A(-1));
+  }
+  if (kk == nk) {
+    if (wbar >= 0.0f) return wbar * flx3(A(-2), A(-1), A(0));
+    float cc2 = 0.5f * (c2k + c2k), cc1 = 1.0f - cc2; return wbar * (cc1 * A(-1) + cc2 * A(0));
+  }
+  if (kk == 3) {
+    if (wbar >= 0.0f) return wbar * flx3(A(-2), A(-1), A(0));
+    return wbar * flx5(A(2), A(1), A(0), A(-1), A(-2));
+  }
+  if (wbar >= 0.0f) return wbar * flx5(A(-3), A(-2), A(-1), A(0), A(1));
+  return wbar * flx3(A(1), A(0), A(-1));
+}
+
+// vertical face flux of a w column at s-level kk; wv[d+2] = w(kk+d), d = -2..3
+__device__ __forceinline__ float zflux_w(const DGrid &g, const float *wv, float wbar, int kk) {
+  const int nk = g.nk;
+  auto A = [&](int d) { return wv[d + 2]; };
+  if (kk >= 3 && kk <= nk - 2) {
+    if (wbar >= 0.0f) return wbar * flx5(A(-2), A(-1), A(0), A(1), A(2));
+    return wbar * flx5(A(3), A(2), A(1), A(0), A(-1));
+  }
+  if (kk == 1) {
+    if (wbar >= 0.0f) return wbar * 0.5f * (A(0) + A(1));
+    return wbar * flx3(A(2), A(1), A(0));
+  }
+  if (kk == nk) {
+    if (wbar >= 0.0f) return wbar * flx3(A(-1), A(0), A(1));
+    return wbar * 0.5f * (A(0) + A(1));
+  }
+  if (kk == 2) {
+    if (wbar >= 0.0f) return wbar * flx3(A(-1), A(0), A(1));
+    return wbar * flx5(A(3), A(2), A(1), A(0), A(-1));
+  }
+  if (wbar >= 0.0f) return wbar * flx5(A(-2), A(-1), A(0), A(1), A(2));
+  return wbar * flx3(A(2), A(1), A(0));
+}
+
+__device__ __forceinline__ float hflux_mom(float r, const float *p, int stride) {
+  if (r >= 0.0f) return r * flx5(p[0], p[stride], p[2 * stride], p[3 * stride], p[4 * stride]);
+  return r * flx5(p[5 * stride], p[4 * stride], p[3 * stride], p[2 * stride], p[stride]);
+}
+
+template <int TX, int TY, int KC, int STAG>
+__global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const float *__restrict__ divx,
+                                                      const float *ten1, float *ten,
+                                                      const float *__restrict__ th3d, const float *__restrict__ qv) {
+  constexpr int NT = TX * TY;
+  constexpr int SW = TX + 6, SH = TY + 6, SP = SW + 1;
+  constexpr int NST = (SW * SH + NT - 1) / NT;
+  constexpr int NFX = (TX + 1) * TY, NFY = TX * (TY + 1);
+  __shared__ float ss[SH * SP];
+  __shared__ float fx[NFX], fxv[NFX], fy[NFY], fyv[NFY];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
+  const int i0 = 1 + (int)blockIdx.x * TX, j0 = 1 + (int)blockIdx.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int ni = g.ni, nj = g.nj, nk = g.nk;
+  const int pitch = (STAG == 2) ? g.NI + 1 : g.NI;      // x extent of the component's array
+  const int rows = (STAG == 3) ? g.NJ + 1 : g.NJ;
+  const long plane = (long)pitch * rows;
+  const float *__restrict__ A = (STAG == 2) ? q.u : (STAG == 3) ? q.v : q.w;
+  const int ilo = (STAG == 2) ? (g.ibw ? 2 : 1) : 1, ihi = (STAG == 2) ? (g.ibe ? ni : ni + 1) : ni;
+  const int jlo = (STAG == 3) ? (g.ibs ? 2 : 1) : 1, jhi = (STAG == 3) ? (g.ibn ? nj : nj + 1) : nj;
+  const bool active = (i >= ilo && i <= ihi && j >= jlo && j <= jhi);
+  const int iea = ni + g.ngxy + (STAG == 2 ? 1 : 0), jea = nj + g.ngxy + (STAG == 3 ? 1 : 0);
+  const bool doitw = (g.wbc == 2 && g.ibw), doite = (g.ebc == 2 && g.ibe);
+  const bool doits = (g.sbc == 2 && g.ibs), doitn = (g.nbc == 2 && g.ibn);
+  const int oc = active ? (i - g.ib) + pitch * (j - g.jb) : 0;
+
+  int soff[NST], sidx[NST];
+#pragma unroll
+  for (int s = 0; s < NST; s++) {
+    const int t = tid + s * NT;
+    soff[s] = -1; sidx[s] = -1;
+    if (t < SW * SH) {
+      const int yy = t / SW, xx = t - yy * SW;
+      const int ii = i0 - 3 + xx, jj = j0 - 3 + yy;
+      sidx[s] = yy * SP + xx;
+      if (ii <= iea && jj <= jea) soff[s] = (ii - g.ib) + pitch * (jj - g.jb);
+    }
+  }
+  // faces owned by this thread: index-space position (-1 in fxi: none)
+  int fxi[2], fxj[2], fyi[2], fyj[2];
+#pragma unroll
+  for (int s = 0; s < 2; s++) {
+    const int f = tid + s * NT;
+    fxi[s] = -1; fxj[s] = 0; fyi[s] = -1; fyj[s] = 0;
+    if (f < NFX) {
+      const int row = f / (TX + 1), col = f - row * (TX + 1);
+      const int ii = (STAG == 2) ? i0 - 1 + col : i0 + col, jj = j0 + row;   // s-point (u) or u-point (v, w)
+      if (ii >= 0 && ii <= ni + 1 && jj <= nj + 1) { fxi[s] = ii; fxj[s] = jj; }
+    }
+    if (f < NFY) {
+      const int row = f / TX, col = f - row * TX;
+      const int ii = i0 + col, jj = (STAG == 3) ? j0 - 1 + row : j0 + row;    // s-point (v) or v-point (u, w)
+      if (jj >= 0 && jj <= nj + 1 && ii <= ni + 1) { fyi[s] = ii; fyj[s] = jj; }
+    }
+  }
+
+  // vertical window: wv[d] = a(kb0 + d), kb0 = upper face - 3 (u, v) or - 2 (w)
+  const int kfirst = (STAG == 4) ? 2 : 1;
+  const int kc0 = kfirst + (int)blockIdx.z * KC, kc1 = min(nk, kc0 + KC - 1);
+  const int koff = (STAG == 4) ? -2 : -3;
+  const int kmaxA = (STAG == 4) ? nk + 2 : nk + 1;
+  auto AV = [&](int kk) -> float { return (kk >= 0 && kk <= kmaxA) ? LDG(&A[(long)kk * plane + oc]) : 0.0f; };
+  auto RRWc = [&](int ii, int jj, int kk) -> float {
+    if (kk <= 1 || kk >= nk + 1) return 0.0f;
+    return LDG(&g.rf0[kk]) * LDG(&q.w[iW(g, ii, jj, kk)]);
+  };
+  auto WBAR = [&](int kk) -> float {
+    if (STAG == 2) return 0.5f * (RRWc(i, j, kk) + RRWc(i - 1, j, kk));
+    if (STAG == 3) return 0.5f * (RRWc(i, j, kk) + RRWc(i, j - 1, kk));
+    return 0.5f * (RRWc(i, j, kk) + RRWc(i, j, kk + 1));
+  };
+  auto ZF = [&](const float *win, int kk) -> float {
+    return (STAG == 4) ? zflux_w(g, win, WBAR(kk), kk) : zflux_uv(g, win, WBAR(kk), kk);
+  };
+  // faces of level k: upper ku, lower ku-1; u/v faces exist for kk = 2..nk, w faces for kk = 1..nk
+  const int kfmin = (STAG == 4) ? 1 : 2;
+  float wv[6];
+  float fzlo = 0.0f;
+  {
+    const int ku = (STAG == 4) ? kc0 : kc0 + 1;
+#pragma unroll
+    for (int d = 0; d < 6; d++) wv[d] = active ? AV(ku + koff + d) : 0.0f;
+    if (active && ku - 1 >= kfmin) {
+      float w0[6];
+#pragma unroll
+      for (int d = 0; d < 6; d++) w0[d] = AV(ku - 1 + koff + d);
+      fzlo = ZF(w0, ku - 1);
+    }
+  }
+
+  // Every global read of a level is issued one level ahead (into the p*
+  // registers), so it is in flight while the previous level computes; the
+  // component arrays and the other inputs are not written by this kernel
+  // (ten may alias ten1 only point by point).
+  float pst[NST], pxa[2], pxb[2], pya[2], pyb[2], pw0 = 0.0f, pw1 = 0.0f, pt1 = 0.0f, pd0 = 0.0f, pd1 = 0.0f;
+  float pb0 = 0.0f, pb1 = 0.0f, pb2 = 0.0f, pb3 = 0.0f, pwtop = 0.0f;
+  auto fetch = [&](int kf) {
+    const float *Ak = A + (long)kf * plane;
+#pragma unroll
+    for (int s = 0; s < NST; s++) pst[s] = (soff[s] >= 0) ? LDG(&Ak[soff[s]]) : 0.0f;
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      pxa[s] = pxb[s] = pya[s] = pyb[s] = 0.0f;
+      if (fxi[s] >= 0) {
+        const int ii = fxi[s], jj = fxj[s];
+        if (STAG == 3) { pxa[s] = LDG(&q.u[iU(g, ii, jj, kf)]); pxb[s] = LDG(&q.u[iU(g, ii, jj - 1, kf)]); }
+        if (STAG == 4) { pxa[s] = LDG(&q.u[iU(g, ii, jj, kf)]); pxb[s] = LDG(&q.u[iU(g, ii, jj, kf - 1)]); }
+      }
+      if (fyi[s] >= 0) {
+        const int ii = fyi[s], jj = fyj[s];
+        if (STAG == 2) { pya[s] = LDG(&q.v[iV(g, ii, jj, kf)]); pyb[s] = LDG(&q.v[iV(g, ii - 1, jj, kf)]); }
+        if (STAG == 4) { pya[s] = LDG(&q.v[iV(g, ii, jj, kf)]); pyb[s] = LDG(&q.v[iV(g, ii, jj, kf - 1)]); }
+      }
+    }
+    if (active) {
+      const int ku = (STAG == 4) ? kf : kf + 1;       // upper face of level kf
+      if (ku <= nk) {
+        const int ia = (STAG == 2) ? i - 1 : i, ja = (STAG == 3) ? j - 1 : j, ka = (STAG == 4) ? ku + 1 : ku;
+        pw0 = (ku <= 1 || ku >= nk + 1) ? 0.0f : LDG(&q.w[iW(g, i, j, ku)]);
+        pw1 = (ka <= 1 || ka >= nk + 1) ? 0.0f : LDG(&q.w[iW(g, ia, ja, ka)]);
+      }
+      const long oS = iS(g, i, j, kf);
+      pt1 = ten1[(long)kf * plane + oc];
+      pd0 = LDG(&divx[oS]);
+      pd1 = LDG(&divx[oS - ((STAG == 2) ? 1L : (STAG == 3) ? (long)g.NI : (long)g.NI * g.NJ)]);
+      if (STAG == 4 && th3d) {
+        pb0 = LDG(&th3d[oS - (long)g.NI * g.NJ]); pb1 = LDG(&th3d[oS]);
+        if (qv) { pb2 = LDG(&qv[oS - (long)g.NI * g.NJ]); pb3 = LDG(&qv[oS]); }
+      }
+      pwtop = AV(ku + koff + 5);
+    }
+  };
+  // wbar of face kk from its two averaged w values (RRW of solve2.F:509-516)
+  auto WBARp = [&](int kk, float w0, float w1) -> float {
+    const int ka = (STAG == 4) ? kk + 1 : kk;
+    const float r0 = (kk <= 1 || kk >= nk + 1) ? 0.0f : LDG(&g.rf0[kk]) * w0;
+    const float r1 = (ka <= 1 || ka >= nk + 1) ? 0.0f : LDG(&g.rf0[ka]) * w1;
+    return 0.5f * (r0 + r1);
+  };
+  fetch(kc0);
+
+  for (int k = kc0; k <= kc1; k++) {
+    const float r0k = LDG(&g.rho0[k]);
+#pragma unroll
+    for (int s = 0; s < NST; s++)
+      if (sidx[s] >= 0) ss[sidx[s]] = pst[s];
+    // face velocities that come from the other components
+    float ubar[2] = {0.0f, 0.0f}, vbar[2] = {0.0f, 0.0f};
+    float c1k = 0.0f, c2k = 0.0f, cc1 = 0.0f, cc2 = 0.0f;
+    if (STAG == 4) {
+      c1k = LDG(&g.c1[k]); c2k = LDG(&g.c2[k]);
+      cc2 = 0.5f * (c2k + c2k); cc1 = 1.0f - cc2;
+    }
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      if (STAG == 3) ubar[s] = 0.5f * (r0k * pxa[s] + r0k * pxb[s]);
+      if (STAG == 4) ubar[s] = cc2 * (r0k * pxa[s]) + cc1 * (LDG(&g.rho0[k - 1]) * pxb[s]);
+      if (STAG == 2) vbar[s] = 0.5f * (r0k * pya[s] + r0k * pyb[s]);
+      if (STAG == 4) vbar[s] = cc2 * (r0k * pya[s]) + cc1 * (LDG(&g.rho0[k - 1]) * pyb[s]);
+    }
+    const float w0 = pw0, w1 = pw1, t1 = pt1, dv0 = pd0, dv1 = pd1, b0 = pb0, b1 = pb1, b2 = pb2, b3 = pb3;
+    if (k < kc1) fetch(k + 1);
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      const int f = tid + s * NT;
+      if (fxi[s] >= 0) {
+        const int row = f / (TX + 1), col = f - row * (TX + 1);
+        const float *p = &ss[(row + 3) * SP + col];
+        float r = ubar[s];
+        if (STAG == 2) r = 0.5f * (r0k * p[2] + r0k * p[3]);
+        fx[f] = hflux_mom(r, p, 1);
+        fxv[f] = r;
+      }
+      if (fyi[s] >= 0) {
+        const int row = f / TX, col = f - row * TX;
+        const float *p = &ss[row * SP + col + 3];
+        float r = vbar[s];
+        if (STAG == 3) r = 0.5f * (r0k * p[2 * SP] + r0k * p[3 * SP]);
+        fy[f] = hflux_mom(r, p, SP);
+        fyv[f] = r;
+      }
+    }
+    const int ku = (STAG == 4) ? k : k + 1;
+    float fzhi = 0.0f, ac = 0.0f;
+    if (active) {
+      ac = ss[(ty + 3) * SP + tx + 3];
+      if (ku <= nk) {
+        const float wb = WBARp(ku, w0, w1);
+        fzhi = (STAG == 4) ? zflux_w(g, wv, wb, ku) : zflux_uv(g, wv, wb, ku);
+      }
+    }
+    __syncthreads();
+    if (active) {
+      const int xi = ty * (TX + 1) + tx, yi = ty * TX + tx;
+      float fx0 = fx[xi], fxp = fx[xi + 1], fy0 = fy[yi], fyp = fy[yi + TX];
+      float advx, advy, advz;
+      const long oS = iS(g, i, j, k);
+      if (STAG == 2) {
+        auto RRV2 = [&](int ii, int jj) { return LDG(&g.rho0[k]) * LDG(&q.v[iV(g, ii, jj, k)]); };
+        advx = -(fxp - fx0) * g.rdx * LDG(&g.uf[i - g.ib]);
+        const bool fs = doits && j == 1 && (RRV2(i, 1) + RRV2(i - 1, 1)) >= 0.0f;
+        const bool fn = doitn && j == nj && (RRV2(i, nj + 1) + RRV2(i - 1, nj + 1)) <= 0.0f;
+        if (fs) fy0 = fyp;
+        if (fn) fyp = fy0;
+        advy = -(fyp - fy0) * g.rdy * LDG(&g.vh[j - g.jb]);
+        if (fs)
+          advy = advy - LDG(&q.u[iU(g, i, 1, k)]) * 0.5f *
+                            ((RRV2(i - 1, 2) - RRV2(i - 1, 1)) + (RRV2(i, 2) - RRV2(i, 1))) * g.rdy * LDG(&g.vh[1 - g.jb]);
+        if (fn)
+          advy = advy - LDG(&q.u[iU(g, i, nj, k)]) * 0.5f *
+                            ((RRV2(i - 1, nj + 1) - RRV2(i - 1, nj)) + (RRV2(i, nj + 1) - RRV2(i, nj))) * g.rdy *
+                            LDG(&g.vh[nj - g.jb]);
+      } else if (STAG == 3) {
+        auto RRU2 = [&](int ii, int jj) { return LDG(&g.rho0[k]) * LDG(&q.u[iU(g, ii, jj, k)]); };
+        const bool fw = doitw && i == 1 && (RRU2(1, j) + RRU2(1, j - 1)) >= 0.0f;
+        const bool fe = doite && i == ni && (RRU2(ni + 1, j) + RRU2(ni + 1, j - 1)) <= 0.0f;
+        if (fw) fx0 = fxp;
+        if (fe) fxp = fx0;
+        advx = -(fxp - fx0) * g.rdx * LDG(&g.uh[i - g.ib]);
+        advy = -(fyp - fy0) * g.rdy * LDG(&g.vf[j - g.jb]);
+        if (fw)
+          advx = advx - LDG(&q.v[iV(g, 1, j, k)]) * 0.5f *
+                            ((RRU2(2, j - 1) - RRU2(1, j - 1)) + (RRU2(2, j) - RRU2(1, j))) * g.rdx * LDG(&g.uh[1 - g.ib]);
+        if (fe)
+          advx = advx - LDG(&q.v[iV(g, ni, j, k)]) * 0.5f *
+                            ((RRU2(ni + 1, j - 1) - RRU2(ni, j - 1)) + (RRU2(ni + 1, j) - RRU2(ni, j))) * g.rdx *
+                            LDG(&g.uh[ni - g.ib]);
+      } else {
+        const float ub0 = fxv[xi], ubp = fxv[xi + 1], vb0 = fyv[yi], vbp = fyv[yi + TX];
+        const bool fw = doitw && i == 1 && ub0 >= 0.0f, fe = doite && i == ni && ubp <= 0.0f;
+        const bool fs = doits && j == 1 && vb0 >= 0.0f, fn = doitn && j == nj && vbp <= 0.0f;
+        if (fw) fx0 = fxp;
+        if (fe) fxp = fx0;
+        if (fs) fy0 = fyp;
+        if (fn) fyp = fy0;
+        advx = -(fxp - fx0) * g.rdx * LDG(&g.uh[i - g.ib]);
+        advy = -(fyp - fy0) * g.rdy * LDG(&g.vh[j - g.jb]);
+        auto RRUk = [&](int ii, int kk) { return LDG(&g.rho0[kk]) * LDG(&q.u[iU(g, ii, j, kk)]); };
+        auto RRVk = [&](int jj, int kk) { return LDG(&g.rho0[kk]) * LDG(&q.v[iV(g, i, jj, kk)]); };
+        const float ww = ac;
+        if (fw)
+          advx = advx - ww * (c1k * (RRUk(2, k - 1) - RRUk(1, k - 1)) + c2k * (RRUk(2, k) - RRUk(1, k))) * g.rdx *
+                            LDG(&g.uh[1 - g.ib]);
+        if (fe)
+          advx = advx - ww * (c1k * (RRUk(ni + 1, k - 1) - RRUk(ni, k - 1)) + c2k * (RRUk(ni + 1, k) - RRUk(ni, k))) *
+                            g.rdx * LDG(&g.uh[ni - g.ib]);
+        if (fs)
+          advy = advy - ww * (c1k * (RRVk(2, k - 1) - RRVk(1, k - 1)) + c2k * (RRVk(2, k) - RRVk(1, k))) * g.rdy *
+                            LDG(&g.vh[1 - g.jb]);
+        if (fn)
+          advy = advy - ww * (c1k * (RRVk(nj + 1, k - 1) - RRVk(nj, k - 1)) + c2k * (RRVk(nj + 1, k) - RRVk(nj, k))) *
+                            g.rdy * LDG(&g.vh[nj - g.jb]);
+      }
+      if (STAG == 4) {
+        advz = -(fzhi - fzlo) * g.rdz * LDG(&g.mf[k]);
+      } else {
+        const float mhk = LDG(&g.mh[k]);
+        if (k == 1) advz = -fzhi * g.rdz * mhk;
+        else if (k == nk) advz = +fzlo * g.rdz * mhk;
+        else advz = -(fzhi - fzlo) * g.rdz * mhk;
+      }
+      const long o = (long)k * plane + oc;
+      if (STAG == 2) {
+        ten[o] = t1 + (((advx + advy) + advz) + ac * 0.5f * (dv0 + dv1)) * LDG(&g.rr0[k]);
+      } else if (STAG == 3) {
+        ten[o] = t1 + (((advx + advy) + advz) + ac * 0.5f * (dv0 + dv1)) * LDG(&g.rr0[k]);
+      } else {
+        float t = t1 + (((advx + advy) + advz) + ac * (c2k * dv0 + c1k * dv1)) * LDG(&g.rrf0[k]);
+        if (th3d) t = t + (c1k * buoy_v(g, b0, b2, qv != nullptr, k - 1) + c2k * buoy_v(g, b1, b3, qv != nullptr, k));
+        ten[o] = t;
+      }
+#pragma unroll
+      for (int d = 0; d < 5; d++) wv[d] = wv[d + 1];
+      wv[5] = pwtop;            // top of the window of level k+1 (fetched above)
+      fzlo = fzhi;
+    }
+  }
+}
+
+static const int MOM_TX = 32, MOM_TY = 8, MOM_KC = 16;
+
 void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w,
                          const float *uten1, const float *vten1, const float *wten1,
                          float *uten, float *vten, float *wten, const float *th3d, const float *qv,
-                         cudaStream_t st, int64_t *nl) {
+                         float *divx, cudaStream_t st, int64_t *nl) {
   Vel q{u, v, w};
-  const int bx = 128;
   {
-    int i1 = g.ibw ? 2 : 1, i2 = g.ibe ? g.ni : g.ni + 1;
-    dim3 grid((i2 - i1 + 1 + bx - 1) / bx, g.nj, g.nk);
-    { ProfScope _ps("k_advu", st); k_advu<<<grid, bx, 0, st>>>(g, q, uten1, uten); }
+    dim3 grid((g.ni + 2 + 127) / 128, g.nj + 2, g.nk);
+    ProfScope _ps("k_mom_divx", st);
+    k_mom_divx<<<grid, 128, 0, st>>>(g, q, divx);
+  }
+  dim3 blk(MOM_TX, MOM_TY);
+  const int kch = (g.nk + MOM_KC - 1) / MOM_KC, kchw = (g.nk - 1 + MOM_KC - 1) / MOM_KC;
+  {
+    dim3 grid((g.ni + 1 + MOM_TX - 1) / MOM_TX, (g.nj + MOM_TY - 1) / MOM_TY, kch);
+    ProfScope _ps("k_advu", st);
+    k_mom_tile<MOM_TX, MOM_TY, MOM_KC, 2><<<grid, blk, 0, st>>>(g, q, divx, uten1, uten, nullptr, nullptr);
   }
   {
-    int j1 = g.ibs ? 2 : 1, j2 = g.ibn ? g.nj : g.nj + 1;
-    dim3 grid((g.ni + bx - 1) / bx, j2 - j1 + 1, g.nk);
-    { ProfScope _ps("k_advv", st); k_advv<<<grid, bx, 0, st>>>(g, q, vten1, vten); }
+    dim3 grid((g.ni + MOM_TX - 1) / MOM_TX, (g.nj + 1 + MOM_TY - 1) / MOM_TY, kch);
+    ProfScope _ps("k_advv", st);
+    k_mom_tile<MOM_TX, MOM_TY, MOM_KC, 3><<<grid, blk, 0, st>>>(g, q, divx, vten1, vten, nullptr, nullptr);
   }
   {
-    dim3 grid((g.ni + bx - 1) / bx, g.nj, g.nk - 1);
-    { ProfScope _ps("k_advw", st); k_advw<<<grid, bx, 0, st>>>(g, q, wten1, wten, th3d, qv); }
+    dim3 grid((g.ni + MOM_TX - 1) / MOM_TX, (g.nj + MOM_TY - 1) / MOM_TY, kchw);
+    ProfScope _ps("k_advw", st);
+    k_mom_tile<MOM_TX, MOM_TY, MOM_KC, 4><<<grid, blk, 0, st>>>(g, q, divx, wten1, wten, th3d, qv);
   }
-  if (nl) *nl += 3;
+  if (nl) *nl += 4;
 }
 
 // ---------------------------------------------------------------------
@@ -752,29 +1127,50 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
     fzlo = zflux_win(g, w0, fwlo, kc0, WENO, pdefweno, weps);
   }
 
+  // Every global read of a level (the staged plane, the face velocities, the
+  // cell's inputs and the next top of the column window) is issued one level
+  // ahead, so it is in flight while the previous level computes.  None of
+  // these arrays is written by this kernel.
+  float pst[NST], pru[2], prv[2], pwhi = 0.0f, pe0 = 0.0f, pe1 = 0.0f, pe2 = 0.0f, pwtop = 0.0f;
+  auto fetch = [&](int kf) {
+    const float *sk = a.s + (long)kf * planeS;
+#pragma unroll
+    for (int q = 0; q < NST; q++) pst[q] = (soff[q] >= 0) ? LDG(&sk[soff[q]]) : 0.0f;
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      pru[q] = (fxo[q] >= 0) ? LDG(&a.rru[(long)kf * planeU + fxo[q]]) : 0.0f;
+      prv[q] = (fyo[q] >= 0) ? LDG(&a.rrv[(long)kf * planeV + fyo[q]]) : 0.0f;
+    }
+    if (active) {
+      const long o = (long)kf * planeS + oc;
+      pwhi = WRAW(kf + 1);
+      if (MODE == MODE_UPDATE) {
+        pe0 = out.sten_in[o];
+        pe1 = LDG(&out.sbase[o]);
+        if (a.thterm) pe2 = LDG(&a.thterm[o]);
+      } else {
+        pe0 = LDG(&a.s0[o]);
+      }
+      pwtop = (kf + 3 <= nk + 1) ? SV(kf + 3) : 0.0f;   // top of the window of level kf
+    }
+  };
+  fetch(kc0);
+
   for (int k = kc0; k <= kc1; k++) {
     const float r0k = LDG(&g.rho0[k]);
     const float th0m = a.sadd ? (LDG(&g.th0[k]) - 300.0f) : 0.0f;
-    // ---- stage the level with its halo; fetch the raw face velocities
-    const float *sk = a.s + (long)k * planeS;
+    // ---- stage the level with its halo; take the raw face velocities
 #pragma unroll
     for (int q = 0; q < NST; q++) {
       if (sidx[q] >= 0) {
-        float v = 0.0f;
-        if (soff[q] >= 0) {
-          v = LDG(&sk[soff[q]]);
-          if (a.sadd) v = th0m + v;
-        }
+        float v = pst[q];
+        if (soff[q] >= 0 && a.sadd) v = th0m + v;
         ss[sidx[q]] = v;
       }
     }
-    float ru[2], rv[2];
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-      ru[q] = (fxo[q] >= 0) ? LDG(&a.rru[(long)k * planeU + fxo[q]]) : 0.0f;
-      rv[q] = (fyo[q] >= 0) ? LDG(&a.rrv[(long)k * planeV + fyo[q]]) : 0.0f;
-    }
-    const float whi = active ? WRAW(k + 1) : 0.0f;
+    const float ru[2] = {pru[0], pru[1]}, rv[2] = {prv[0], prv[1]};
+    const float whi = pwhi, e0 = pe0, e1 = pe1, e2 = pe2;
+    if (k < kc1) fetch(k + 1);
     __syncthreads();
     // ---- face values: each x/y face once, each upper z face once per column
 #pragma unroll
@@ -824,20 +1220,20 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
       float div = ((fu1 - fu0) * g.rdx * uh_i + (fv1 - fv0) * g.rdy * vh_j) + (fwhi - fwlo) * g.rdz * mhk;
       if (fabsf(div) < g.smeps) div = 0.0f;
       if (MODE == MODE_UPDATE) {
-        float ten = out.sten_in[o];
+        float ten = e0;
         if (a.thterm) {   // getdiv of the averaged velocities (misclibs.F:127-136)
           float rd = ((u1r - u0r) * g.rdx * uh_i + (v1r - v0r) * g.rdy * vh_j) + (whi - wlo) * g.rdz * mhk;
           if (fabsf(rd) < g.smeps) rd = 0.0f;
-          ten = ten - rd * LDG(&a.thterm[o]);
+          ten = ten - rd * e2;
         }
         ten = ten + (((advx + advy) + advz) + sc * div) * LDG(&g.rr0[k]);
-        float v = LDG(&out.sbase[o]) + dt * ten;
+        float v = e1 + dt * ten;
         if (flush && fabsf(v) < g.smeps) v = 0.0f;
         out.snew[o] = v;
       } else {
         // pdefx1 / pdefy1 / pdefz provisional masses (pdef.F:35-102, 289-340, 478-496)
         out.advx[o] = advx; out.advy[o] = advy; out.advz[o] = advz;
-        const float s0 = LDG(&a.s0[o]);
+        const float s0 = e0;
         float dx = r0k * s0 + dt * (advx + sc * (fu1 - fu0) * g.rdx * uh_i);
         if (doitw && i == 1 && fu0 >= 0.0f) dx = r0k * s0;
         if (doite && i == ni && fu1 <= 0.0f) dx = r0k * s0;
@@ -850,8 +1246,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
       // slide the column window and carry the upper face to the next level
 #pragma unroll
       for (int d = 0; d < 5; d++) wv[d] = wv[d + 1];
-      const int kn = k + 4;     // s(k+4) is the new top of the window for level k+1
-      wv[5] = (kn <= nk + 1) ? SV(kn) : 0.0f;
+      wv[5] = pwtop;            // s(k+4), the new top of the window for level k+1
       fzlo = fzhi;
       fwlo = fwhi;
       wlo = whi;
