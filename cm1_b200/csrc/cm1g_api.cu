@@ -52,8 +52,8 @@ void launch_cfl(const DGrid &g, const float *u, const float *v, const float *w, 
 void launch_pdefq(const DGrid &g, float rmax, const float *rho, float *q, double *bud, double *asq,
                   cudaStream_t st, int64_t *nl);
 void launch_ppx_update(const DGrid &g, const float *pp3d, float *ppx, cudaStream_t st, int64_t *nl);
-void launch_copy_range(const DGrid &g, int stag, int ilo, int ihi, int jlo, int jhi, const float *src, float *dst,
-                       cudaStream_t st, int64_t *nl);
+void launch_copy_batch(const DGrid &g, const float *const *src, float *const *dst, const int *stag, const int *ilo,
+                       const int *ihi, const int *jlo, const int *jhi, int n, cudaStream_t st, int64_t *nl);
 void launch_level_mass(const DGrid &g, const float *rho, double *lev, cudaStream_t st, int64_t *nl);
 void launch_maxmin(const DGrid &g, const float *a, int stag, unsigned long long *om, cudaStream_t st, int64_t *nl);
 }  // namespace cm1g
@@ -544,13 +544,24 @@ static void run_solve3(cm1g_ctx *c, const cm1g_state_t *d) {
   launch_ppx_update(g, d->pp3d, d->ppx, st, nl);
   launch_bc(g, d->ppx, 2, 0, st, nl);
   // solve3.F:546-640 rollover
-  launch_copy_range(g, 2, 0, ni + 2, 0, nj + 2, d->u3d, d->ua, st, nl);
-  launch_copy_range(g, 3, 0, ni + 2, 0, nj + 2, d->v3d, d->va, st, nl);
-  launch_copy_range(g, 4, 0, ni + 2, 0, nj + 2, d->w3d, d->wa, st, nl);
-  for (int n = 0; n < npt; n++) launch_copy_range(g, 1, 0, ni + 1, 0, nj + 1, d->pt3d + n * ns, d->pta + n * ns, st, nl);
-  launch_copy_range(g, 1, 0, ni + 1, 0, nj + 1, d->pp3d, d->ppi, st, nl);
-  launch_copy_range(g, 1, 0, ni + 1, 0, nj + 1, d->th3d, d->tha, st, nl);
-  for (int n = 0; n < numq; n++) launch_copy_range(g, 1, 0, ni + 1, 0, nj + 1, d->q3d + n * ns, d->qa + n * ns, st, nl);
+  {
+    std::vector<const float *> src;
+    std::vector<float *> dst;
+    std::vector<int> stag, ihi, jhi;
+    auto add = [&](const float *a, float *b, int sg, int ih, int jh) {
+      src.push_back(a); dst.push_back(b); stag.push_back(sg); ihi.push_back(ih); jhi.push_back(jh);
+    };
+    add(d->u3d, d->ua, 2, ni + 2, nj + 2);
+    add(d->v3d, d->va, 3, ni + 2, nj + 2);
+    add(d->w3d, d->wa, 4, ni + 2, nj + 2);
+    for (int n = 0; n < npt; n++) add(d->pt3d + n * ns, d->pta + n * ns, 1, ni + 1, nj + 1);
+    add(d->pp3d, d->ppi, 1, ni + 1, nj + 1);
+    add(d->th3d, d->tha, 1, ni + 1, nj + 1);
+    for (int n = 0; n < numq; n++) add(d->q3d + n * ns, d->qa + n * ns, 1, ni + 1, nj + 1);
+    std::vector<int> lo(src.size(), 0);
+    launch_copy_batch(g, src.data(), dst.data(), stag.data(), lo.data(), ihi.data(), lo.data(), jhi.data(),
+                      (int)src.size(), st, nl);
+  }
 }
 
 static void run_step(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass1) {

@@ -312,8 +312,8 @@ __device__ __forceinline__ float zflux_uv(const DGrid &g, const float *wv, float
   const int nk = g.nk;
   auto A = [&](int d) { return wv[d + 3]; };
   if (kk >= 4 && kk <= nk - 2) {
-    if (wbar >= 0.0f) return wbar * flx5(A(-3), A(-2), A(-1), A(0), A(1));
-    return wbar * flx5(A(2), A(1), A(0), A(-1), A(-2));
+    const bool up = (wbar >= 0.0f);
+    return wbar * flx5(up ? A(-3) : A(2), up ? A(-2) : A(1), up ? A(-1) : A(0), up ? A(0) : A(-1), up ? A(1) : A(-2));
   }
   const float c2k = LDG(&g.c2[kk]);
   if (kk == 2) {
@@ -337,8 +337,8 @@ __device__ __forceinline__ float zflux_w(const DGrid &g, const float *wv, float 
   const int nk = g.nk;
   auto A = [&](int d) { return wv[d + 2]; };
   if (kk >= 3 && kk <= nk - 2) {
-    if (wbar >= 0.0f) return wbar * flx5(A(-2), A(-1), A(0), A(1), A(2));
-    return wbar * flx5(A(3), A(2), A(1), A(0), A(-1));
+    const bool up = (wbar >= 0.0f);
+    return wbar * flx5(up ? A(-2) : A(3), up ? A(-1) : A(2), up ? A(0) : A(1), up ? A(1) : A(0), up ? A(2) : A(-1));
   }
   if (kk == 1) {
     if (wbar >= 0.0f) return wbar * 0.5f * (A(0) + A(1));
@@ -357,8 +357,9 @@ __device__ __forceinline__ float zflux_w(const DGrid &g, const float *wv, float 
 }
 
 __device__ __forceinline__ float hflux_mom(float r, const float *p, int stride) {
-  if (r >= 0.0f) return r * flx5(p[0], p[stride], p[2 * stride], p[3 * stride], p[4 * stride]);
-  return r * flx5(p[5 * stride], p[4 * stride], p[3 * stride], p[2 * stride], p[stride]);
+  const float a0 = p[0], a1 = p[stride], a2 = p[2 * stride], a3 = p[3 * stride], a4 = p[4 * stride], a5 = p[5 * stride];
+  const bool up = (r >= 0.0f);
+  return r * flx5(up ? a0 : a5, up ? a1 : a4, up ? a2 : a3, up ? a3 : a2, up ? a4 : a1);
 }
 
 template <int TX, int TY, int KC, int STAG>
@@ -976,8 +977,8 @@ __device__ __forceinline__ float zflux_win(const DGrid &g, const float *wv, floa
   const float c1k = LDG(&g.c1[kk]), c2k = LDG(&g.c2[kk]);
   if (!weno) {
     if (kk >= 4 && kk <= nk - 2) {
-      if (r >= 0.0f) return r * flx5(A(-3), A(-2), A(-1), A(0), A(1));
-      return r * flx5(A(2), A(1), A(0), A(-1), A(-2));
+      const bool up = (r >= 0.0f);
+      return r * flx5(up ? A(-3) : A(2), up ? A(-2) : A(1), up ? A(-1) : A(0), up ? A(0) : A(-1), up ? A(1) : A(-2));
     }
     if (kk == 2) {
       if (r >= 0.0f) return r * (c1k * A(-1) + c2k * A(0));
@@ -1011,8 +1012,10 @@ __device__ __forceinline__ float zflux_win(const DGrid &g, const float *wv, floa
     return (absmax5(s1, s2, s3, s4, s5) > (float)weps) ? r * weno5(s1, s2, s3, s4, s5, weps) : 0.0f;
   }
   if (kk >= 4 && kk <= nk - 2) {
-    if (r >= 0.0f) return r * weno5(A(-3), A(-2), A(-1), A(0), A(1), weps);
-    return r * weno5(A(2), A(1), A(0), A(-1), A(-2), weps);
+    // upwind-ordered stencil first, so a warp with both signs evaluates one WENO
+    const bool up = (r >= 0.0f);
+    return r * weno5(up ? A(-3) : A(2), up ? A(-2) : A(1), up ? A(-1) : A(0), up ? A(0) : A(-1), up ? A(1) : A(-2),
+                     weps);
   }
   if (kk == 3) {
     if (r >= 0.0f) return r * upstrpd(A(-2), A(-1), A(0), weps);

@@ -338,8 +338,31 @@ __global__ void k_ppx_update(DGrid g, const float *__restrict__ pp3d, float *ppx
   ppx[o] = LDG(&pp3d[o]) + ppx[o];
 }
 
-// copy dst = src over i=lo..hi, j=lo..hij, k=1..nk of an array with
-// x-extent `pitch` and rows `nrow` (stag 1/2/3/4 layouts)
+// Rollover copies dst = src over i = ilo..ihi, j = jlo..jhi, k = 1..nk
+// (solve3.F:546-640) for up to CP_MAXB arrays in one launch: blockIdx.y
+// picks the array, each warp copies one row segment (coalesced along i).
+static const int CP_MAXB = 16;
+struct CopyItem {
+  const float *src;
+  float *dst;
+  long pitch, plane;
+  int ilo, ihi, jlo, jhi;
+};
+struct CopyBatch {
+  CopyItem it[CP_MAXB];
+  int n, nk, ib, jb;
+};
+
+__global__ void k_copy_batch(CopyBatch b) {
+  const CopyItem c = b.it[blockIdx.y];
+  const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = (int)(threadIdx.x & 31);
+  const int nrow = c.jhi - c.jlo + 1;
+  if (warp >= nrow * b.nk) return;
+  const int k = 1 + warp / nrow, j = c.jlo + warp % nrow;
+  const long base = (long)(j - b.jb) * c.pitch + (long)k * c.plane - b.ib;
+  for (int i = c.ilo + lane; i <= c.ihi; i += 32) c.dst[base + i] = LDG(&c.src[base + i]);
+}
+
 __global__ void k_copy_range(long pitch, long plane, int ib, int jb, int ilo, int ihi, int jlo, int jhi, int nk,
                              const float *__restrict__ src, float *__restrict__ dst) {
   const int i = ilo + (int)(blockIdx.x * blockDim.x + threadIdx.x);
@@ -355,13 +378,25 @@ void launch_ppx_update(const DGrid &g, const float *pp3d, float *ppx, cudaStream
   if (nl) *nl += 1;
 }
 
-void launch_copy_range(const DGrid &g, int stag, int ilo, int ihi, int jlo, int jhi, const float *src, float *dst,
-                       cudaStream_t st, int64_t *nl) {
-  long pitch = (stag == 2) ? g.NI + 1 : g.NI;
-  long rows = (stag == 3) ? g.NJ + 1 : g.NJ;
-  dim3 grid((ihi - ilo + 1 + 127) / 128, jhi - jlo + 1, g.nk);
-  { ProfScope _ps("k_copy_range", st); k_copy_range<<<grid, 128, 0, st>>>(pitch, pitch * rows, g.ib, g.jb, ilo, ihi, jlo, jhi, g.nk, src, dst); }
-  if (nl) *nl += 1;
+// stag: 1 s, 2 u, 3 v, 4 w layout of each array
+void launch_copy_batch(const DGrid &g, const float *const *src, float *const *dst, const int *stag, const int *ilo,
+                       const int *ihi, const int *jlo, const int *jhi, int n, cudaStream_t st, int64_t *nl) {
+  for (int base = 0; base < n; base += CP_MAXB) {
+    CopyBatch b{};
+    b.n = (n - base < CP_MAXB) ? n - base : CP_MAXB;
+    b.nk = g.nk; b.ib = g.ib; b.jb = g.jb;
+    int maxrows = 0;
+    for (int q = 0; q < b.n; q++) {
+      const int t = base + q;
+      const long pitch = (stag[t] == 2) ? g.NI + 1 : g.NI, rows = (stag[t] == 3) ? g.NJ + 1 : g.NJ;
+      b.it[q] = CopyItem{src[t], dst[t], pitch, pitch * rows, ilo[t], ihi[t], jlo[t], jhi[t]};
+      const int r = (jhi[t] - jlo[t] + 1) * g.nk;
+      if (r > maxrows) maxrows = r;
+    }
+    dim3 grid((maxrows + 7) / 8, b.n);
+    { ProfScope _ps("k_copy_batch", st); k_copy_batch<<<grid, 256, 0, st>>>(b); }
+    if (nl) *nl += 1;
+  }
 }
 
 // ---------------------------------------------------------------------
