@@ -26,13 +26,16 @@ class CM1GError(RuntimeError):
 
 
 def lib():
-    """Load libcm1g.so (raises if it has not been built)."""
+    """Load libcm1g.so (raises if it has not been built).  CM1G_LIB names
+    another build of the same library (e.g. one compiled with different
+    tile parameters) to load instead."""
     global _lib
     if _lib is not None:
         return _lib
-    if not os.path.exists(LIB_PATH):
-        raise RuntimeError("libcm1g.so not built: run `python -m cm1_b200.build` (no CPU fallback exists)")
-    L = C.CDLL(LIB_PATH)
+    path = os.environ.get("CM1G_LIB", LIB_PATH)
+    if not os.path.exists(path):
+        raise RuntimeError("%s not built: run `python -m cm1_b200.build` (no CPU fallback exists)" % path)
+    L = C.CDLL(path)
     ctxp = C.c_void_p
     cfgp, grp, stp = C.POINTER(Config), C.POINTER(Grid), C.POINTER(State)
     L.cm1g_last_error.restype = C.c_char_p

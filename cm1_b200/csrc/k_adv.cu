@@ -953,6 +953,122 @@ __global__ void k_advs_pdef2(DGrid g, SAdv a, const float *__restrict__ advx, co
   }
 }
 
+// Tiled form of pass 2: a block owns TX x TY columns and marches upward;
+// each level's dumx (with its +-2 halo in x) and dumy (+-2 in y) are staged
+// in shared memory (double-buffered, one barrier per level), dumz comes
+// from a per-column register window, and every read of a level is issued
+// one level ahead.  Same arithmetic as k_advs_pdef2.
+template <int TX, int TY, int KC>
+__global__ void __launch_bounds__(TX * TY) k_advs_pdef2_tile(DGrid g, SAdv a, const float *__restrict__ advx,
+                                                             const float *__restrict__ advy, const float *__restrict__ advz,
+                                                             const float *__restrict__ dumx, const float *__restrict__ dumy,
+                                                             const float *__restrict__ dumz, const float *__restrict__ sten_in,
+                                                             float *__restrict__ snew, const float *__restrict__ sbase,
+                                                             float dt, int flush) {
+  constexpr int NT = TX * TY;
+  constexpr int XW = TX + 4, YH = TY + 4;
+  constexpr int NSX = (XW * TY + NT - 1) / NT, NSY = (TX * YH + NT - 1) / NT;
+  __shared__ float sx[2][TY * XW], sy[2][YH * TX];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
+  const int i0 = 1 + (int)blockIdx.x * TX, j0 = 1 + (int)blockIdx.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int ni = g.ni, nj = g.nj, nk = g.nk, NI = g.NI, NJ = g.NJ;
+  const bool active = (i <= ni && j <= nj);
+  const long planeS = (long)NI * NJ, planeU = (long)(NI + 1) * NJ, planeV = (long)NI * (NJ + 1);
+  const float smeps = g.smeps, rdt = 1.0f / dt;
+  const float uh_i = active ? LDG(&g.uh[i - g.ib]) : 0.0f, vh_j = active ? LDG(&g.vh[j - g.jb]) : 0.0f;
+  const int oc = active ? (i - g.ib) + NI * (j - g.jb) : 0;
+  const int ocu = active ? (i - g.ib) + (NI + 1) * (j - g.jb) : 0;
+  int xo[NSX], xs[NSX], yo[NSY], ys[NSY];   // staging: source offset in the plane (-1: none), slot
+#pragma unroll
+  for (int q = 0; q < NSX; q++) {
+    const int t = tid + q * NT;
+    xo[q] = -1; xs[q] = 0;
+    if (t < XW * TY) {
+      const int yy = t / XW, xx = t - yy * XW, ii = i0 - 2 + xx, jj = j0 + yy;
+      if (ii <= ni + 2 && jj <= nj) { xo[q] = (ii - g.ib) + NI * (jj - g.jb); xs[q] = t; }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < NSY; q++) {
+    const int t = tid + q * NT;
+    yo[q] = -1; ys[q] = 0;
+    if (t < TX * YH) {
+      const int yy = t / TX, xx = t - yy * TX, ii = i0 + xx, jj = j0 - 2 + yy;
+      if (ii <= ni && jj <= nj + 2) { yo[q] = (ii - g.ib) + NI * (jj - g.jb); ys[q] = t; }
+    }
+  }
+  const int kc0 = 1 + (int)blockIdx.z * KC, kc1 = min(nk, kc0 + KC - 1);
+  auto DZ = [&](int kk) { return (kk < 1 || kk > nk) ? 0.0f : LDG(&dumz[(long)kk * planeS + oc]); };
+  auto WR = [&](int kk) { return (kk <= 1 || kk >= nk + 1) ? 0.0f : LDG(&a.rrw[(long)kk * planeS + oc]); };
+  float zw[5];                                  // dumz(k-2 .. k+2)
+#pragma unroll
+  for (int d = 0; d < 5; d++) zw[d] = active ? DZ(kc0 - 2 + d) : 0.0f;
+  float wlo = active ? WR(kc0) : 0.0f;          // raw averaged w through the bottom face
+
+  float psx[NSX], psy[NSY], pax = 0.f, pay = 0.f, paz = 0.f, ps = 0.f, ps0 = 0.f, pt = 0.f, pb = 0.f;
+  float pu0 = 0.f, pu1 = 0.f, pv0 = 0.f, pv1 = 0.f, pwhi = 0.f, pztop = 0.f;
+  auto fetch = [&](int kf) {
+#pragma unroll
+    for (int q = 0; q < NSX; q++) psx[q] = (xo[q] >= 0) ? LDG(&dumx[(long)kf * planeS + xo[q]]) : 0.0f;
+#pragma unroll
+    for (int q = 0; q < NSY; q++) psy[q] = (yo[q] >= 0) ? LDG(&dumy[(long)kf * planeS + yo[q]]) : 0.0f;
+    if (active) {
+      const long o = (long)kf * planeS + oc, ou = (long)kf * planeU + ocu, ov = (long)kf * planeV + oc;
+      pax = LDG(&advx[o]); pay = LDG(&advy[o]); paz = LDG(&advz[o]);
+      ps = LDG(&a.s[o]);
+      if (a.sadd) ps = (LDG(&g.th0[kf]) - 300.0f) + ps;
+      ps0 = LDG(&a.s0[o]); pt = sten_in[o]; pb = LDG(&sbase[o]);
+      pu0 = LDG(&a.rru[ou]); pu1 = LDG(&a.rru[ou + 1]);
+      pv0 = LDG(&a.rrv[ov]); pv1 = LDG(&a.rrv[ov + NI]);
+      pwhi = WR(kf + 1);
+      pztop = DZ(kf + 2);                       // top of the dumz window of level kf
+    }
+  };
+  fetch(kc0);
+  for (int k = kc0; k <= kc1; k++) {
+    const int b = k & 1;
+#pragma unroll
+    for (int q = 0; q < NSX; q++) if (xo[q] >= 0) sx[b][xs[q]] = psx[q];
+#pragma unroll
+    for (int q = 0; q < NSY; q++) if (yo[q] >= 0) sy[b][ys[q]] = psy[q];
+    const float ax0 = pax, ay0 = pay, az0 = paz, s = ps, s0 = ps0, t1 = pt, base = pb;
+    const float u0r = pu0, u1r = pu1, v0r = pv0, v1r = pv1, whi = pwhi;
+    if (k < kc1) fetch(k + 1);
+    __syncthreads();
+    if (active) {
+      const float r0k = LDG(&g.rho0[k]), mhk = LDG(&g.mh[k]);
+      const float fu0 = u0r * r0k, fu1 = u1r * r0k, fv0 = v0r * r0k, fv1 = v1r * r0k;
+      const float fwlo = wlo * LDG(&g.rf0[k]), fwhi = whi * LDG(&g.rf0[k + 1]);
+      float m; bool f;
+      // z (pdefz): dum(0)=dum(nk+1)=0
+      float az = az0;
+      pdef_gather(zw[0], zw[1], zw[2], zw[3], zw[4], smeps, &m, &f);
+      if (f) az = (zw[2] + m - r0k * s0) * rdt - s * (fwhi - fwlo) * g.rdz * mhk;
+      // x (pdefx2)
+      const float *px = &sx[b][ty * XW + tx];
+      float ax = ax0;
+      pdef_gather(px[0], px[1], px[2], px[3], px[4], smeps, &m, &f);
+      if (f) ax = (px[2] + m - r0k * s0) * rdt - s * (fu1 - fu0) * g.rdx * uh_i;
+      // y (pdefy2)
+      const float *py = &sy[b][ty * TX + tx];
+      float ay = ay0;
+      pdef_gather(py[0], py[TX], py[2 * TX], py[3 * TX], py[4 * TX], smeps, &m, &f);
+      if (f) ay = (py[2 * TX] + m - r0k * s0) * rdt - s * (fv1 - fv0) * g.rdy * vh_j;
+      float div = ((fu1 - fu0) * g.rdx * uh_i + (fv1 - fv0) * g.rdy * vh_j) + (fwhi - fwlo) * g.rdz * mhk;
+      if (fabsf(div) < g.smeps) div = 0.0f;
+      const float ten = t1 + (((ax + ay) + az) + s * div) * LDG(&g.rr0[k]);
+      float v = base + dt * ten;
+      if (flush && fabsf(v) < g.smeps) v = 0.0f;
+      snew[(long)k * planeS + oc] = v;
+#pragma unroll
+      for (int d = 0; d < 4; d++) zw[d] = zw[d + 1];
+      zw[4] = pztop;            // dumz(k+3), fetched with level k+1 above
+      wlo = whi;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------
 // Tiled scalar advection (the production path of advs).
 //
@@ -1296,9 +1412,11 @@ void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const
     const int which[2] = {1, 1};
     launch_bc_batch(g, arr, which, nullptr, 2, st, nl);
   }
-  const int bx = 128;
-  dim3 g2((g.ni + bx - 1) / bx, g.nj, g.nk);
-  { ProfScope _ps("k_advs_pdef2", st); k_advs_pdef2<<<g2, bx, 0, st>>>(g, a, o.advx, o.advy, o.advz, o.dumx, o.dumy, o.dumz, ten1, nullptr, snew, s0, dt, flush); }
+  {
+    ProfScope _ps("k_advs_pdef2", st);
+    k_advs_pdef2_tile<ADV_TX, ADV_TY, ADV_KC><<<grid, blk, 0, st>>>(g, a, o.advx, o.advy, o.advz, o.dumx, o.dumy,
+                                                                  o.dumz, ten1, snew, s0, dt, flush);
+  }
   if (nl) *nl += 2;
 }
 

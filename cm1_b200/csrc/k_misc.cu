@@ -55,54 +55,64 @@ void launch_stage_prep(const DGrid &g, const float *th3d, const float *pp3d, con
 // ---------------------------------------------------------------------
 // radbcew4 / radbcns4 (bc.F:2054-2178): column-averaged phase speeds
 // ---------------------------------------------------------------------
+// One warp per boundary column: the lanes form the phase speeds of the
+// column's levels in parallel, then lane 0 adds them in the reference's
+// order k = 1..nk, and the lanes write the column average back.
 __global__ void k_radbc4(DGrid g, const float *__restrict__ ua, const float *__restrict__ u3d,
                          const float *__restrict__ va, const float *__restrict__ v3d,
                          float *radbcw, float *radbce, float *radbcs, float *radbcn, float dt) {
-  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int side = (int)blockIdx.y;   // 0 w, 1 e, 2 s, 3 n
+  __shared__ float cbs[4][130];
+  const int wib = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
+  const int t = (int)blockIdx.x * 4 + wib;     // column along the side
+  const int side = (int)blockIdx.y;            // 0 w, 1 e, 2 s, 3 n
   const int ni = g.ni, nj = g.nj, nk = g.nk;
-  const float umax = 350.0f;          // csmax, constants.F:45
-  if (side <= 1) {
+  const float umax = 350.0f;                   // csmax, constants.F:45
+  const bool ew = side <= 1;
+  const int n = ew ? nj : ni;
+  bool on = (1 + t <= n);
+  if (side == 0) on = on && g.ibw && g.wbc == 2;
+  if (side == 1) on = on && g.ibe && g.ebc == 2;
+  if (side == 2) on = on && g.ibs && g.sbc == 2;
+  if (side == 3) on = on && g.ibn && g.nbc == 2;
+  if (!on) return;                             // whole warp leaves together
+  float *cb = cbs[wib];
+  if (ew) {
     const int j = 1 + t;
-    if (j > nj) return;
-    if (side == 0 && !(g.ibw && g.wbc == 2)) return;
-    if (side == 1 && !(g.ibe && g.ebc == 2)) return;
     const int ia = (side == 0) ? 2 : ni, ib2 = (side == 0) ? 3 : ni - 1;
     const float ruf = LDG(&g.ruf[ia - g.ib]);
-    float avg = 0.0f;
-    for (int k = 1; k <= nk; k++) {
+    for (int k = 1 + lane; k <= nk; k += 32) {
       float foo = (side == 0) ? (ua[iU(g, ib2, j, k)] - ua[iU(g, ia, j, k)]) : (ua[iU(g, ia, j, k)] - ua[iU(g, ib2, j, k)]);
-      float cb = g.dx * ruf * (ua[iU(g, ia, j, k)] - u3d[iU(g, ia, j, k)]) / (dt * (copysignf(1.e-10f, foo) + foo));
-      cb = (side == 0) ? fmaxf(fminf(cb, 0.0f), -umax) : fminf(fmaxf(cb, 0.0f), umax);
-      avg = avg + cb;
+      float c = g.dx * ruf * (ua[iU(g, ia, j, k)] - u3d[iU(g, ia, j, k)]) / (dt * (copysignf(1.e-10f, foo) + foo));
+      cb[k] = (side == 0) ? fmaxf(fminf(c, 0.0f), -umax) : fminf(fmaxf(c, 0.0f), umax);
     }
-    avg = avg / (float)nk;
-    float *r = (side == 0) ? radbcw : radbce;
-    for (int k = 1; k <= nk; k++) r[(j - g.jb) + (long)g.NJ * k] = avg;
   } else {
     const int i = 1 + t;
-    if (i > ni) return;
-    if (side == 2 && !(g.ibs && g.sbc == 2)) return;
-    if (side == 3 && !(g.ibn && g.nbc == 2)) return;
     const int ja = (side == 2) ? 2 : nj, jb2 = (side == 2) ? 3 : nj - 1;
     const float rvf = LDG(&g.rvf[ja - g.jb]);
-    float avg = 0.0f;
-    for (int k = 1; k <= nk; k++) {
+    for (int k = 1 + lane; k <= nk; k += 32) {
       float foo = (side == 2) ? (va[iV(g, i, jb2, k)] - va[iV(g, i, ja, k)]) : (va[iV(g, i, ja, k)] - va[iV(g, i, jb2, k)]);
-      float cb = g.dy * rvf * (va[iV(g, i, ja, k)] - v3d[iV(g, i, ja, k)]) / (dt * (copysignf(1.e-10f, foo) + foo));
-      cb = (side == 2) ? fmaxf(fminf(cb, 0.0f), -umax) : fminf(fmaxf(cb, 0.0f), umax);
-      avg = avg + cb;
+      float c = g.dy * rvf * (va[iV(g, i, ja, k)] - v3d[iV(g, i, ja, k)]) / (dt * (copysignf(1.e-10f, foo) + foo));
+      cb[k] = (side == 2) ? fmaxf(fminf(c, 0.0f), -umax) : fminf(fmaxf(c, 0.0f), umax);
     }
+  }
+  __syncwarp();
+  float avg = 0.0f;
+  if (lane == 0) {
+    for (int k = 1; k <= nk; k++) avg = avg + cb[k];
     avg = avg / (float)nk;
-    float *r = (side == 2) ? radbcs : radbcn;
-    for (int k = 1; k <= nk; k++) r[(i - g.ib) + (long)g.NI * k] = avg;
+  }
+  avg = __shfl_sync(0xffffffffu, avg, 0);
+  float *r = (side == 0) ? radbcw : (side == 1) ? radbce : (side == 2) ? radbcs : radbcn;
+  for (int k = 1 + lane; k <= nk; k += 32) {
+    if (ew) r[(1 + t - g.jb) + (long)g.NJ * k] = avg;
+    else r[(1 + t - g.ib) + (long)g.NI * k] = avg;
   }
 }
 
 void launch_radbc4(const DGrid &g, const float *ua, const float *u3d, const float *va, const float *v3d,
                    float *rw, float *re, float *rs, float *rn, float dt, cudaStream_t st, int64_t *nl) {
   int n = g.ni > g.nj ? g.ni : g.nj;
-  dim3 grid((n + 127) / 128, 4);
+  dim3 grid((n + 3) / 4, 4);
   { ProfScope _ps("k_radbc4", st); k_radbc4<<<grid, 128, 0, st>>>(g, ua, u3d, va, v3d, rw, re, rs, rn, dt); }
   if (nl) *nl += 1;
 }
@@ -223,27 +233,37 @@ void launch_masscon(const DGrid &g, float *pp3d, const float *th3d, const float 
 // calccflquick (misclibs.F:2726-2814): max Courant number, stored as the
 // bits of a non-negative float so atomicMax on int orders it correctly.
 // ---------------------------------------------------------------------
+// Each block walks all levels of a 128-column strip of one row and reduces
+// in registers, shuffles and shared memory, so one atomic per block
+// (instead of one per warp) reaches the result.
 __global__ void k_cfl(DGrid g, const float *__restrict__ u, const float *__restrict__ v, const float *__restrict__ w,
                       float dt, int *out) {
+  __shared__ float red[4];
   const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int j = 1 + (int)blockIdx.y, k = 1 + (int)blockIdx.z;
-  float wsp = 0.0f;
+  const int j = 1 + (int)blockIdx.y;
+  float wmax = 0.0f;
   if (i <= g.ni) {
     const float dtdx = 0.5f * dt * g.rdx, dtdy = 0.5f * dt * g.rdy, dtdz = 0.5f * dt * g.rdz;
-    float a1 = (LDG(&u[iU(g, i, j, k)]) + LDG(&u[iU(g, i + 1, j, k)])) * dtdx * LDG(&g.uh[i - g.ib]);
-    float a2 = (LDG(&v[iV(g, i, j, k)]) + LDG(&v[iV(g, i, j + 1, k)])) * dtdy * LDG(&g.vh[j - g.jb]);
-    float a3 = (LDG(&w[iW(g, i, j, k)]) + LDG(&w[iW(g, i, j, k + 1)])) * dtdz * LDG(&g.mh[k]);
-    wsp = sqrtf((a1 * a1 + a2 * a2) + a3 * a3);
-    if (!(wsp <= 3.0e38f)) wsp = INFINITY;   // NaN/Inf velocity: reported as an error by the host
+    const float uh = LDG(&g.uh[i - g.ib]), vh = LDG(&g.vh[j - g.jb]);
+    for (int k = 1; k <= g.nk; k++) {
+      float a1 = (LDG(&u[iU(g, i, j, k)]) + LDG(&u[iU(g, i + 1, j, k)])) * dtdx * uh;
+      float a2 = (LDG(&v[iV(g, i, j, k)]) + LDG(&v[iV(g, i, j + 1, k)])) * dtdy * vh;
+      float a3 = (LDG(&w[iW(g, i, j, k)]) + LDG(&w[iW(g, i, j, k + 1)])) * dtdz * LDG(&g.mh[k]);
+      float wsp = sqrtf((a1 * a1 + a2 * a2) + a3 * a3);
+      if (!(wsp <= 3.0e38f)) wsp = INFINITY;   // NaN/Inf velocity: reported as an error by the host
+      wmax = fmaxf(wmax, wsp);
+    }
   }
-  for (int s = 16; s > 0; s >>= 1) wsp = fmaxf(wsp, __shfl_xor_sync(0xffffffffu, wsp, s));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_int(wsp));
+  for (int s = 16; s > 0; s >>= 1) wmax = fmaxf(wmax, __shfl_xor_sync(0xffffffffu, wmax, s));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = wmax;
+  __syncthreads();
+  if (threadIdx.x == 0) atomicMax(out, __float_as_int(fmaxf(fmaxf(red[0], red[1]), fmaxf(red[2], red[3]))));
 }
 
 void launch_cfl(const DGrid &g, const float *u, const float *v, const float *w, float dt, int *out,
                 cudaStream_t st, int64_t *nl) {
   cudaMemsetAsync(out, 0, sizeof(int), st);
-  dim3 grid((g.ni + 127) / 128, g.nj, g.nk);
+  dim3 grid((g.ni + 127) / 128, g.nj);
   { ProfScope _ps("k_cfl", st); k_cfl<<<grid, 128, 0, st>>>(g, u, v, w, dt, out); }
   if (nl) *nl += 1;
 }

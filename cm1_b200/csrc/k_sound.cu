@@ -73,8 +73,16 @@ static const int SND_TX = 32;     // columns per tile (one warp wide)
 static const int SND_NW = 8;      // warps per block
 static const int SND_KPT = 16;    // max levels per thread: nk <= SND_NW*SND_KPT
 
+#ifndef CM1G_SND_MINB
+#define CM1G_SND_MINB 3      // resident blocks per SM the tile kernel is compiled for
+#endif
+#ifndef CM1G_SND_UNROLL
+#define CM1G_SND_UNROLL 1    // phase-1 levels a warp keeps in flight
+#endif
+constexpr int kSndUnroll = CM1G_SND_UNROLL;
+
 template <int TX, int NW, int KPT>
-__global__ void __launch_bounds__(TX * NW, 3) k_sound_tile(DGrid g, SoundIO io, SoundStep p) {
+__global__ void __launch_bounds__(TX * NW, CM1G_SND_MINB) k_sound_tile(DGrid g, SoundIO io, SoundStep p) {
   extern __shared__ float sm[];
   const int lane = threadIdx.x, w = threadIdx.y;
   const int i = 1 + (int)blockIdx.x * TX + lane;
@@ -108,7 +116,7 @@ __global__ void __launch_bounds__(TX * NW, 3) k_sound_tile(DGrid g, SoundIO io, 
     // block's warps work on adjacent levels and share their vertical
     // neighbours through L1
     const long plane = (long)g.NI * g.NJ;
-#pragma unroll 1
+#pragma unroll kSndUnroll
     for (int m = 0; m < KPT; m++) {
       const int k = 1 + w + m * NW;
       if (k > nk) break;
