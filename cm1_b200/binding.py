@@ -61,6 +61,10 @@ def lib():
     L.cm1g_profile.argtypes = [ctxp, C.c_int32]
     L.cm1g_profile_read.argtypes = [ctxp, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(C.c_int64),
                                     C.POINTER(C.c_double)]
+    L.cm1g_calcener.argtypes = [ctxp] + [_P] * 11 + [C.POINTER(C.c_double)]
+    L.cm1g_dtsmall.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, C.c_int32,
+                               C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int32)]
+    L.cm1g_tendency_init.argtypes = [ctxp, C.c_int32, C.c_float] + [_P] * 16
     L.cm1g_pdefq_noalloc.argtypes = [cfgp, C.c_float, C.POINTER(C.c_double), _P, _P, _P, _P, _P, C.c_void_p]
     _lib = L
     return L
@@ -176,6 +180,19 @@ class Context:
         check(lib().cm1g_maxmin(self.h, ptr(a), stag, C.byref(mx), C.byref(mn), loc))
         return mx.value, mn.value, tuple(loc)
 
+    def calcener(self, zh, rho, ua, va, wa, ppi, tha, qv=None, ql=None, qi=None, vr=None):
+        """(ek, ei, ep, le, et) of calcener, FP64."""
+        out = (C.c_double * 5)()
+        check(lib().cm1g_calcener(self.h, ptr(zh), ptr(rho), ptr(ua), ptr(va), ptr(wa), ptr(ppi), ptr(tha),
+                                  ptr(qv), ptr(ql), ptr(qi), ptr(vr), out))
+        return tuple(out)
+
+    def tendency_init(self, irdamp, rdalpha, uten1, vten1, wten1, thten1, qten=None, ptten=None, tauh=None,
+                      taus=None, tauf=None, uavg=None, vavg=None, thavg=None, ua=None, va=None, wa=None, tha=None):
+        check(lib().cm1g_tendency_init(self.h, irdamp, rdalpha, ptr(tauh), ptr(taus), ptr(tauf), ptr(uavg), ptr(vavg),
+                                       ptr(thavg), ptr(ua), ptr(va), ptr(wa), ptr(tha), ptr(uten1), ptr(vten1),
+                                       ptr(wten1), ptr(thten1), ptr(qten), ptr(ptten)))
+
     def profile(self, enable):
         check(lib().cm1g_profile(self.h, 1 if enable else 0))
 
@@ -190,6 +207,14 @@ class Context:
             out[buf.value.decode()] = (n.value, ms.value)
             i += 1
         return out
+
+
+def dtsmall(psolver, nx, ny, min_dx, min_dy, min_dz, dt, adapt_dt=0):
+    """nsound (and dt, dbldt, changed only by adapt_dt) as dtsmall computes them."""
+    fdt, ddt, ns = C.c_float(dt), C.c_double(dt), C.c_int32()
+    check(lib().cm1g_dtsmall(psolver, nx, ny, min_dx, min_dy, min_dz, adapt_dt, C.byref(fdt), C.byref(ddt),
+                             C.byref(ns)))
+    return ns.value, fdt.value, ddt.value
 
 
 def to_device(arrays, device="cuda"):

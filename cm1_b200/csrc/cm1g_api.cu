@@ -19,6 +19,9 @@ namespace cm1g {
 void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, int64_t *nlaunch);
 void launch_bc_batch(const DGrid &g, float *const *arrays, const int *which, const int *wflag, int n,
                      cudaStream_t st, int64_t *nlaunch);
+void launch_tend_init(const DGrid &g, const TendIn &t, cudaStream_t st, int64_t *nl);
+int ener_chunks(const DGrid &g);
+void launch_calcener(const DGrid &g, const EnerIn &e, double *part, double *out, cudaStream_t st, int64_t *nl);
 void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w, const float *uten1,
                          const float *vten1, const float *wten1, float *uten, float *vten, float *wten,
                          const float *th3d, const float *qv, float *divx, cudaStream_t st, int64_t *nl);
@@ -137,6 +140,7 @@ struct cm1g_ctx {
   float *pdefscr = nullptr;                   // 6 s-arrays
   float *mdivx = nullptr;                     // divx of the momentum pass
   double *part3 = nullptr, *part4 = nullptr, *dscal = nullptr, *bud = nullptr, *lev = nullptr;
+  double *ener = nullptr;                     // calcener chunk sums (4 x nk x chunks) and results
   float *fscal = nullptr;
   int *cflbits = nullptr;
   unsigned long long *mm = nullptr;
@@ -309,6 +313,16 @@ extern "C" int cm1g_init(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_c
   bool pdef_needed = cfg->imoist || (cfg->iptra && cfg->pdtra);
   c->pdefscr = (float *)dalloc(c, (pdef_needed ? 6 : 6) * bS);
   c->mdivx = (float *)dalloc(c, bS);
+  c->ener = (double *)dalloc(c, ((size_t)4 * g.nk * ener_chunks(g) + 8) * sizeof(double));
+  // base-state winds (full u/v arrays) for the Rayleigh damping of cm1g_tendency_init
+  if (gr->u0 && gr->v0) {
+    float *du0 = (float *)dalloc(c, bU), *dv0 = (float *)dalloc(c, bV);
+    if (du0 && dv0) {
+      cudaMemcpy(du0, gr->u0, bU, cudaMemcpyHostToDevice);
+      cudaMemcpy(dv0, gr->v0, bV, cudaMemcpyHostToDevice);
+      g.u0 = du0; g.v0 = dv0;
+    }
+  }
   int nchunk = prs_nchunk(g);
   c->part3 = (double *)dalloc(c, (size_t)(g.nk + 2) * nchunk * sizeof(double));
   c->part4 = (double *)dalloc(c, (size_t)(g.nk + 2) * nchunk * sizeof(double));
@@ -771,6 +785,105 @@ extern "C" int cm1g_calcmass(cm1g_ctx_t *c, const float *rho, double *tmass) {
   double tm = 0.0;
   for (int k = 1; k <= c->g.nk; k++) tm = tm + lev[k];
   *tmass = tm * (double)(c->g.dx * c->g.dy * c->g.dz);
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_dtsmall(int32_t psolver, int32_t nx, int32_t ny, float min_dx, float min_dy, float min_dz,
+                            int32_t adapt_dt, float *dt, double *dbldt, int32_t *nsound) {
+  if (!dt || !dbldt || !nsound) return set_err(CM1G_ERR_ARG, "null argument");
+  const int max_nsound = 192;
+  float dtsm;
+  if (psolver == 1 || psolver == 4 || psolver == 5) { *nsound = 1; return CM1G_OK; }
+  if (psolver == 2) {
+    if (ny == 1) dtsm = 0.60f * fminf(min_dx, min_dz) / 360.0f;
+    else if (nx == 1) dtsm = 0.60f * fminf(min_dy, min_dz) / 360.0f;
+    else dtsm = 0.50f * fminf(fminf(min_dx, min_dy), min_dz) / 360.0f;
+  } else if (psolver == 3) {
+    if (ny == 1) dtsm = 0.60f * min_dx / 360.0f;
+    else if (nx == 1) dtsm = 0.60f * min_dy / 360.0f;
+    else dtsm = 0.60f * fminf(min_dx, min_dy) / 360.0f;
+  } else {
+    return set_err(CM1G_ERR_UNSUPPORTED, "dtsmall: psolver=%d is not built", psolver);
+  }
+  const double x = *dbldt / (double)dtsm;
+  int ns = (int)(x >= 0.0 ? floor(x + 0.5) : ceil(x - 0.5));   // Fortran nint
+  if (ns < 4) ns = 4;
+  if (ns % 2 != 0) ns = ns + 1;
+  if (*dbldt / (double)(float)ns > (double)dtsm) ns = ns + 2;
+  if (ns > max_nsound) {
+    if (adapt_dt != 1)
+      return set_err(CM1G_ERR_ARG, "limit for number of small steps exceeded: nsound=%d > %d; dtl needs to be smaller",
+                     ns, max_nsound);
+    ns = max_nsound;
+    *dbldt = (double)((float)ns * dtsm);
+    *dt = (float)*dbldt;
+  }
+  *nsound = ns;
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_tendency_init(cm1g_ctx_t *c, int32_t irdamp, float rdalpha, const float *tauh, const float *taus,
+                                  const float *tauf, const float *uavg, const float *vavg, const float *thavg,
+                                  const float *ua, const float *va, const float *wa, const float *tha, float *uten1,
+                                  float *vten1, float *wten1, float *thten1, float *qten, float *ptten) {
+  if (!c || !uten1 || !vten1 || !wten1 || !thten1) return set_err(CM1G_ERR_ARG, "null argument");
+  if (irdamp < 0 || irdamp > 2) return set_err(CM1G_ERR_ARG, "irdamp must be 0, 1 or 2");
+  const DGrid &g = c->g;
+  const int numq = c->cfg.imoist ? c->cfg.numq : 0, npt = c->cfg.iptra ? c->cfg.npt : 0;
+  if ((numq && !qten) || (npt && !ptten)) return set_err(CM1G_ERR_ARG, "qten/ptten missing");
+  if (irdamp && (!tauh || !taus || !tauf || !ua || !va || !wa || !tha))
+    return set_err(CM1G_ERR_ARG, "Rayleigh damping needs tauh, taus, tauf, ua, va, wa, tha");
+  if (irdamp == 1 && (!g.u0 || !g.v0)) return set_err(CM1G_ERR_ARG, "grid u0/v0 were not given to cm1g_init");
+  if (irdamp == 2 && (!uavg || !vavg || !thavg)) return set_err(CM1G_ERR_ARG, "irdamp=2 needs uavg, vavg, thavg");
+  ProfActive pa(c);
+  Stager S(c);
+  const size_t ns = nS(g), nk2 = (size_t)g.NK;
+  TendIn t{};
+  t.irdamp = irdamp; t.rdalpha = rdalpha;
+  if (irdamp) {
+    t.tauh = S.in(tauh, ns, false); t.taus = S.in(taus, ns, false); t.tauf = S.in(tauf, nW(g), false);
+    t.ua = S.in(ua, nU(g), false); t.va = S.in(va, nV(g), false); t.wa = S.in(wa, nW(g), false);
+    t.tha = S.in(tha, ns, false);
+    if (irdamp == 2) { t.uavg = S.in(uavg, nk2, false); t.vavg = S.in(vavg, nk2, false); t.thavg = S.in(thavg, nk2, false); }
+  }
+  t.uten1 = S.in(uten1, nU(g), true); t.vten1 = S.in(vten1, nV(g), true);
+  t.wten1 = S.in(wten1, nW(g), true); t.thten1 = S.in(thten1, ns, true);
+  t.qten = numq ? S.in(qten, numq * ns, true) : nullptr;
+  t.ptten = npt ? S.in(ptten, npt * ns, true) : nullptr;
+  t.numq = numq; t.nq = numq + npt;
+  launch_tend_init(g, t, c->stream, &c->nlaunch);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
+  return S.finish();
+}
+
+extern "C" int cm1g_calcener(cm1g_ctx_t *c, const float *zh, const float *rho, const float *ua, const float *va,
+                             const float *wa, const float *ppi, const float *tha, const float *qv, const float *ql,
+                             const float *qi, const float *vr, double energy[5]) {
+  if (!c || !zh || !rho || !ua || !va || !wa || !ppi || !tha || !energy) return set_err(CM1G_ERR_ARG, "null argument");
+  ProfActive pa(c);
+  Stager S(c);
+  const DGrid &g = c->g;
+  const size_t ns = nS(g);
+  EnerIn e{};
+  e.zh = S.in(zh, ns, false); e.rho = S.in(rho, ns, false); e.ua = S.in(ua, nU(g), false);
+  e.va = S.in(va, nV(g), false); e.wa = S.in(wa, nW(g), false); e.ppi = S.in(ppi, ns, false);
+  e.tha = S.in(tha, ns, false);
+  e.qv = qv ? S.in(qv, ns, false) : nullptr; e.ql = ql ? S.in(ql, ns, false) : nullptr;
+  e.qi = qi ? S.in(qi, ns, false) : nullptr; e.vr = vr ? S.in(vr, ns, false) : nullptr;
+  // constants.F:85-150: latent heats at the reference temperature to = 273.15
+  const int tc = c->cfg.testcase;
+  const float xlv = tc == 4 ? 2.47e6f : tc == 5 ? 2.50e6f : 2501000.0f, xls = 2834000.0f, to = 273.15f;
+  e.lv1 = xlv + (g.c.cpl - g.c.cpv) * to;
+  e.ls1 = xls + (g.c.cpi - g.c.cpv) * to;
+  double *part = c->ener + 8;
+  launch_calcener(g, e, part, c->ener, c->stream, &c->nlaunch);
+  double h[4];
+  CUCHK(cudaMemcpyAsync(h, c->ener, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  int rc = S.finish();
+  if (rc) return rc;
+  for (int q = 0; q < 4; q++) energy[q] = h[q];
+  energy[4] = ((h[0] + h[1]) + h[2]) + h[3];
   return CM1G_OK;
 }
 

@@ -31,6 +31,7 @@ struct DGrid {
   // horizontal metrics (index i-ib / j-jb)
   const float *uh, *ruh, *uf, *ruf, *vh, *rvh, *vf, *rvf;
   const float *dtu0, *dtv0;   // (ib:ie, jb:je)
+  const float *u0, *v0;       // base-state winds, full u-/v-arrays (Rayleigh damping)
 };
 
 // Fortran-layout offsets.  s and w arrays share the plane (NI*NJ); u arrays
@@ -117,6 +118,20 @@ __device__ __forceinline__ float upstrpd(float s1, float s2, float s3, double we
 __device__ __forceinline__ float absmax5(float a, float b, float c, float d, float e) {
   return fmaxf(fmaxf(fmaxf(fmaxf(fabsf(a), fabsf(b)), fabsf(c)), fabsf(d)), fabsf(e));
 }
+
+// Inputs of the solve1 tendency initialisation and of calcener (k_misc.cu).
+struct TendIn {
+  int irdamp;
+  float rdalpha;
+  const float *tauh, *taus, *tauf, *uavg, *vavg, *thavg, *ua, *va, *wa, *tha;
+  float *uten1, *vten1, *wten1, *thten1, *qten, *ptten;
+  int nq;     // moisture + tracer arrays to zero (qten first, then ptten)
+  int numq;
+};
+struct EnerIn {
+  const float *zh, *rho, *ua, *va, *wa, *ppi, *tha, *qv, *ql, *qi, *vr;
+  float lv1, ls1;
+};
 
 // Records a message for cm1g_last_error() and returns code (C++ linkage,
 // not part of the C-ABI).

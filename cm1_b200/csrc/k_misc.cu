@@ -420,6 +420,118 @@ void launch_copy_batch(const DGrid &g, const float *const *src, float *const *ds
 }
 
 // ---------------------------------------------------------------------
+// pre-RK tendencies of solve1 (solve1.F:414-486): Rayleigh damping of u, v,
+// w, theta (irdamp=1: toward the base state; irdamp=2: toward the mean
+// profiles uavg/vavg/thavg), else zero, on i = 1..ni+1, j = 1..nj+1,
+// k = 1..nk; the moisture and tracer tendencies are zeroed on the interior.
+// ---------------------------------------------------------------------
+
+__global__ void k_tend_init(DGrid g, TendIn t) {
+  const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = 1 + (int)blockIdx.y, k = 1 + (int)blockIdx.z;
+  if (i > g.ni + 1) return;
+  const long o = iS(g, i, j, k), ou = iU(g, i, j, k), ov = iV(g, i, j, k);
+  const float ra = t.rdalpha;
+  if (t.irdamp == 1 || t.irdamp == 2) {
+    const float tu = LDG(&t.tauh[o - 1]) + LDG(&t.tauh[o]);
+    const float tv = LDG(&t.tauh[o - g.NI]) + LDG(&t.tauh[o]);
+    const float ur = (t.irdamp == 1) ? LDG(&g.u0[ou]) : LDG(&t.uavg[k]);
+    const float vr = (t.irdamp == 1) ? LDG(&g.v0[ov]) : LDG(&t.vavg[k]);
+    t.uten1[ou] = -(ra * 0.5f * tu * (LDG(&t.ua[ou]) - ur));
+    t.vten1[ov] = -(ra * 0.5f * tv * (LDG(&t.va[ov]) - vr));
+    t.wten1[o] = -(ra * LDG(&t.tauf[o]) * LDG(&t.wa[o]));
+    const float th = (t.irdamp == 1) ? LDG(&t.tha[o]) : (LDG(&g.th0[k]) - LDG(&t.thavg[k])) + LDG(&t.tha[o]);
+    t.thten1[o] = -(ra * LDG(&t.taus[o]) * th);
+  } else {
+    t.uten1[ou] = 0.0f; t.vten1[ov] = 0.0f; t.wten1[o] = 0.0f; t.thten1[o] = 0.0f;
+  }
+  if (i <= g.ni && j <= g.nj)
+    for (int n = 0; n < t.nq; n++) {
+      float *q = (n < t.numq) ? t.qten + (long)n * nS(g) : t.ptten + (long)(n - t.numq) * nS(g);
+      q[o] = 0.0f;
+    }
+}
+
+void launch_tend_init(const DGrid &g, const TendIn &t, cudaStream_t st, int64_t *nl) {
+  dim3 grid((g.ni + 1 + 127) / 128, g.nj + 1, g.nk);
+  { ProfScope _ps("k_tend_init", st); k_tend_init<<<grid, 128, 0, st>>>(g, t); }
+  if (nl) *nl += 1;
+}
+
+// ---------------------------------------------------------------------
+// calcener (misclibs.F:3343-3454, umove = vmove = 0): FP64 kinetic,
+// internal, potential and latent energy.  Per-cell terms keep the
+// reference's operand kinds (binary32 factors promoted where a binary64
+// operand meets them); block (x, k) adds its chunk of level k, and
+// k_ener_finish adds the chunks and then the levels in a fixed order.
+// ---------------------------------------------------------------------
+static const int EN_NT = 256, EN_PER = 8;
+
+__global__ void __launch_bounds__(EN_NT) k_ener_part(DGrid g, EnerIn e, double *part, int nchunk) {
+  __shared__ double red[EN_NT];
+  const int k = 1 + (int)blockIdx.y;
+  const long npl = (long)g.ni * g.nj;
+  const long base = (long)blockIdx.x * EN_NT * EN_PER;
+  const Consts &c = g.c;
+  double f1 = 0.0, f2 = 0.0, f3 = 0.0, f4 = 0.0;
+  for (int r = 0; r < EN_PER; r++) {
+    const long t = base + (long)r * EN_NT + threadIdx.x;
+    if (t >= npl) break;
+    const int i = 1 + (int)(t % g.ni), j = 1 + (int)(t / g.ni);
+    const long o = iS(g, i, j, k), ou = iU(g, i, j, k), ov = iV(g, i, j, k);
+    const double tem = (double)(LDG(&g.ruh[i - g.ib]) * LDG(&g.rvh[j - g.jb]) * LDG(&g.rmh[k]));
+    const float u1 = LDG(&e.ua[ou]), u2 = LDG(&e.ua[ou + 1]), v1 = LDG(&e.va[ov]), v2 = LDG(&e.va[ov + g.NI]);
+    const float w1 = LDG(&e.wa[o]), w2 = LDG(&e.wa[o + (long)g.NI * g.NJ]);
+    const double ww = (double)(0.5f * (w1 + w2));
+    const float q_v = e.qv ? LDG(&e.qv[o]) : 0.0f, q_l = e.ql ? LDG(&e.ql[o]) : 0.0f;
+    const float q_i = e.qi ? LDG(&e.qi[o]) : 0.0f, v_r = e.vr ? LDG(&e.vr[o]) : 0.0f;
+    const double qtot = (double)((q_v + q_l) + q_i);
+    const float rr = LDG(&e.rho[o]);
+    const float ke = (0.5f * (u1 * u1 + u2 * u2) + 0.5f * (v1 * v1 + v2 * v2)) + 0.5f * (w1 * w1 + w2 * w2);
+    f1 = (f1 + (double)rr * tem * (1.0 + qtot) * 0.5 * (double)ke) +
+         (double)(q_l * rr) * tem * 0.5 * ((double)(v_r * v_r) - 2.0 * ww * (double)v_r);
+    const double tmp = (double)((LDG(&g.th0[k]) + LDG(&e.tha[o])) * (LDG(&g.pi0[k]) + LDG(&e.ppi[o])));
+    f2 = f2 + (double)rr * tem * (double)(c.cv + c.cvv * q_v) * tmp;
+    f3 = f3 + (double)rr * tem * (1.0 + qtot) * (double)c.g * (double)LDG(&e.zh[o]);
+    f4 = (f4 + (double)rr * tem * (double)q_l * ((double)c.cpl * tmp - (double)e.lv1)) +
+         (double)rr * tem * (double)q_i * ((double)c.cpi * tmp - (double)e.ls1);
+  }
+  double s[4] = {f1, f2, f3, f4};
+  for (int q = 0; q < 4; q++) {
+    red[threadIdx.x] = s[q];
+    __syncthreads();
+    for (int h = EN_NT / 2; h > 0; h >>= 1) {
+      if ((int)threadIdx.x < h) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + h];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) part[((long)q * g.nk + (k - 1)) * nchunk + blockIdx.x] = red[0];
+    __syncthreads();
+  }
+}
+
+__global__ void k_ener_finish(DGrid g, const double *part, int nchunk, double *out) {
+  const int q = (int)threadIdx.x;   // 0 ek, 1 ei, 2 ep, 3 le
+  if (q >= 4) return;
+  double tot = 0.0;
+  for (int k = 0; k < g.nk; k++) {
+    double f = 0.0;
+    for (int c = 0; c < nchunk; c++) f = f + part[((long)q * g.nk + k) * nchunk + c];
+    tot = tot + f;
+  }
+  out[q] = tot * (double)(g.dx * g.dy * g.dz);
+}
+
+int ener_chunks(const DGrid &g) { return (int)(((long)g.ni * g.nj + EN_NT * EN_PER - 1) / (EN_NT * EN_PER)); }
+
+void launch_calcener(const DGrid &g, const EnerIn &e, double *part, double *out, cudaStream_t st, int64_t *nl) {
+  const int nchunk = ener_chunks(g);
+  dim3 grid(nchunk, g.nk);
+  { ProfScope _ps("k_ener_part", st); k_ener_part<<<grid, EN_NT, 0, st>>>(g, e, part, nchunk); }
+  { ProfScope _ps("k_ener_finish", st); k_ener_finish<<<1, 32, 0, st>>>(g, part, nchunk, out); }
+  if (nl) *nl += 2;
+}
+
+// ---------------------------------------------------------------------
 // calcmass (misclibs.F:3134-3191) and maxmin (maxmin.F:5-119)
 // ---------------------------------------------------------------------
 __global__ void k_level_mass(DGrid g, const float *__restrict__ rho, double *lev) {

@@ -24,6 +24,7 @@ module cm1g_iso
   public :: cm1g_config_t, cm1g_grid_t, cm1g_state_t
   public :: cm1g_init, cm1g_finalize, cm1g_step, cm1g_solve2, cm1g_solve3, cm1g_pdefq
   public :: cm1g_bcs, cm1g_bcp, cm1g_bcu, cm1g_bcv, cm1g_bcw, cm1g_last_error_f
+  public :: cm1g_calcmass, cm1g_calcener, cm1g_dtsmall, cm1g_tendency_init
   public :: cm1g_setup, cm1g_large_step
 
   integer(c_int32_t), parameter :: CM1G_MAXQ = 8
@@ -132,6 +133,40 @@ module cm1g_iso
       type(c_ptr), value :: ctx
       real(c_float), intent(inout) :: w(*)
       integer(c_int32_t), value :: flag
+    end function
+    ! calcmass (misclibs.F:3134) and calcener (misclibs.F:3343): FP64 budgets
+    integer(c_int) function cm1g_calcmass(ctx, rho, tmass) bind(C, name="cm1g_calcmass")
+      import :: c_int, c_float, c_double, c_ptr
+      type(c_ptr), value :: ctx
+      real(c_float), intent(in) :: rho(*)
+      real(c_double), intent(out) :: tmass
+    end function
+    integer(c_int) function cm1g_calcener(ctx, zh, rho, ua, va, wa, ppi, tha, qv, ql, qi, vr, energy) &
+        bind(C, name="cm1g_calcener")
+      import :: c_int, c_float, c_double, c_ptr
+      type(c_ptr), value :: ctx
+      real(c_float), intent(in) :: zh(*), rho(*), ua(*), va(*), wa(*), ppi(*), tha(*), qv(*), ql(*), qi(*), vr(*)
+      real(c_double), intent(out) :: energy(5)
+    end function
+    ! dtsmall (misclibs.F:817): the module values it reads are arguments here
+    integer(c_int) function cm1g_dtsmall(psolver, nx, ny, min_dx, min_dy, min_dz, adapt_dt, dt, dbldt, nsound) &
+        bind(C, name="cm1g_dtsmall")
+      import :: c_int, c_int32_t, c_float, c_double
+      integer(c_int32_t), value :: psolver, nx, ny, adapt_dt
+      real(c_float), value :: min_dx, min_dy, min_dz
+      real(c_float), intent(inout) :: dt
+      real(c_double), intent(inout) :: dbldt
+      integer(c_int32_t), intent(out) :: nsound
+    end function
+    ! Rayleigh damping / zeroing of the pre-RK tendencies (solve1.F:414-486)
+    integer(c_int) function cm1g_tendency_init(ctx, irdamp, rdalpha, tauh, taus, tauf, uavg, vavg, thavg, &
+        ua, va, wa, tha, uten1, vten1, wten1, thten1, qten, ptten) bind(C, name="cm1g_tendency_init")
+      import :: c_int, c_int32_t, c_float, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: irdamp
+      real(c_float), value :: rdalpha
+      real(c_float), intent(in) :: tauh(*), taus(*), tauf(*), uavg(*), vavg(*), thavg(*), ua(*), va(*), wa(*), tha(*)
+      real(c_float), intent(inout) :: uten1(*), vten1(*), wten1(*), thten1(*), qten(*), ptten(*)
     end function
     type(c_ptr) function cm1g_last_error() bind(C, name="cm1g_last_error")
       import :: c_ptr

@@ -198,6 +198,32 @@ int cm1g_sound(cm1g_ctx_t *ctx, int32_t nrk, float dt, float dttmp,
  * (src/misclibs.F:3134-3191).  tmass = sum(rho*dV). */
 int cm1g_calcmass(cm1g_ctx_t *ctx, const float *rho, double *tmass);
 
+/* Energy budget, FP64 accumulation: replaces calcener
+ * (src/misclibs.F:3343-3454, argument order of its arrays, umove = vmove = 0).
+ * energy receives ek, ei, ep, le and their total et.  zh is the s-level
+ * height array; qv, ql, qi, vr may be NULL (zero). */
+int cm1g_calcener(cm1g_ctx_t *ctx, const float *zh, const float *rho, const float *ua, const float *va,
+                  const float *wa, const float *ppi, const float *tha, const float *qv, const float *ql,
+                  const float *qi, const float *vr, double energy[5]);
+
+/* Number of small steps per large step: replaces dtsmall
+ * (src/misclibs.F:817-915) with the module values it reads passed in
+ * (psolver, nx, ny, min_dx, min_dy, min_dz, adapt_dt).  Host-only, no
+ * context.  Where the reference stops the model (nsound > 192 without
+ * adapt_dt) it returns CM1G_ERR_ARG; psolver 6/7 return UNSUPPORTED. */
+int cm1g_dtsmall(int32_t psolver, int32_t nx, int32_t ny, float min_dx, float min_dy, float min_dz,
+                 int32_t adapt_dt, float *dt, double *dbldt, int32_t *nsound);
+
+/* Pre-RK tendencies of solve1 (src/solve1.F:414-486): irdamp 1 damps u, v,
+ * w, theta toward the base state (u0/v0 of cm1g_init, as hrdamp=1 does),
+ * irdamp 2 toward the horizontal-mean profiles uavg/vavg/thavg(kb:ke), 0
+ * zeroes them; qten/ptten are zeroed.  tauh/taus are s-arrays, tauf a
+ * w-array (param.F:8650-8680). */
+int cm1g_tendency_init(cm1g_ctx_t *ctx, int32_t irdamp, float rdalpha, const float *tauh, const float *taus,
+                       const float *tauf, const float *uavg, const float *vavg, const float *thavg,
+                       const float *ua, const float *va, const float *wa, const float *tha,
+                       float *uten1, float *vten1, float *wten1, float *thten1, float *qten, float *ptten);
+
 /* Domain extrema over the physical cells of an s/u/v/w array: replaces
  * maxmin (src/maxmin.F:5-119).  stag: 1 s, 2 u, 3 v, 4 w.  loc receives
  * 1-based (i,j,k) of the max (loc[0..2]) and of the min (loc[3..5]). */

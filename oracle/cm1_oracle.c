@@ -1759,6 +1759,128 @@ int oracle_maxmin(const cm1g_config_t *cfg, const float *a, int stag, float *ama
   return 0;
 }
 
+/* dtsmall: misclibs.F:817-915, the number of small steps per large step.
+   psolver 1/4/5 -> 1; 2 and 3 from the grid spacing.  The reference stops
+   the model when nsound exceeds 192 without adapt_dt; here that returns -2.
+   psolver 6/7 (which need csound) return -1. */
+static int nint_d(double x) { return (int)(x >= 0.0 ? floor(x + 0.5) : ceil(x - 0.5)); }
+int oracle_dtsmall(int psolver, int nx, int ny, float min_dx, float min_dy, float min_dz, int adapt_dt,
+                   float *dt, double *dbldt, int *nsound) {
+  const int max_nsound = 192;
+  float dtsm;
+  if (psolver == 1 || psolver == 4 || psolver == 5) { *nsound = 1; return 0; }
+  if (psolver == 2) {
+    if (ny == 1) dtsm = 0.60f * fminf(min_dx, min_dz) / 360.0f;
+    else if (nx == 1) dtsm = 0.60f * fminf(min_dy, min_dz) / 360.0f;
+    else dtsm = 0.50f * fminf(fminf(min_dx, min_dy), min_dz) / 360.0f;
+  } else if (psolver == 3) {
+    if (ny == 1) dtsm = 0.60f * min_dx / 360.0f;
+    else if (nx == 1) dtsm = 0.60f * min_dy / 360.0f;
+    else dtsm = 0.60f * fminf(min_dx, min_dy) / 360.0f;
+  } else {
+    return -1;
+  }
+  int ns = nint_d(*dbldt / (double)dtsm);
+  if (ns < 4) ns = 4;
+  if (ns % 2 != 0) ns = ns + 1;
+  if (*dbldt / (double)(float)ns > (double)dtsm) ns = ns + 2;
+  if (ns > max_nsound) {
+    if (adapt_dt != 1) return -2;
+    ns = max_nsound;
+    *dbldt = (double)((float)ns * dtsm);
+    *dt = (float)*dbldt;
+  }
+  *nsound = ns;
+  return 0;
+}
+
+/* Pre-RK tendencies of solve1 (solve1.F:414-486): Rayleigh damping of u, v,
+   w, theta toward the base state (irdamp=1, or hrdamp=1) or toward the
+   horizontal-mean profiles uavg/vavg/thavg (irdamp=2), else zero; the
+   moisture and tracer tendencies are zeroed.  tauh/taus are s-arrays, tauf
+   a w-array (param.F:8650-8680). */
+int oracle_tendency_init(const cm1g_config_t *cfg, const cm1g_grid_t *gr, int irdamp, float rdalpha,
+                         const float *tauh, const float *taus, const float *tauf, const float *uavg,
+                         const float *vavg, const float *thavg, const float *ua, const float *va, const float *wa,
+                         const float *tha, float *uten1, float *vten1, float *wten1, float *thten1, float *qten,
+                         float *ptten) {
+  OG G, *g = &G;
+  if (og_setup(g, cfg, gr)) return -1;
+  F3 th = mkS(g, tauh), ts = mkS(g, taus), tf = mkW(g, tauf);
+  F3 u = mkU(g, ua), v = mkV(g, va), w = mkW(g, wa), t = mkS(g, tha);
+  F3 ut = mkU(g, uten1), vt = mkV(g, vten1), wt = mkW(g, wten1), tt = mkS(g, thten1);
+  for (int k = 1; k <= g->nk; k++)
+    for (int j = 1; j <= g->nj + 1; j++)
+      for (int i = 1; i <= g->ni + 1; i++) {
+        if (irdamp == 1) {
+          A3(ut, i, j, k) = -(rdalpha * 0.5f * (A3(th, i - 1, j, k) + A3(th, i, j, k)) * (A3(u, i, j, k) - A3(g->u0, i, j, k)));
+          A3(vt, i, j, k) = -(rdalpha * 0.5f * (A3(th, i, j - 1, k) + A3(th, i, j, k)) * (A3(v, i, j, k) - A3(g->v0, i, j, k)));
+          A3(wt, i, j, k) = -(rdalpha * A3(tf, i, j, k) * A3(w, i, j, k));
+          A3(tt, i, j, k) = -(rdalpha * A3(ts, i, j, k) * A3(t, i, j, k));
+        } else if (irdamp == 2) {
+          A3(ut, i, j, k) = -(rdalpha * 0.5f * (A3(th, i - 1, j, k) + A3(th, i, j, k)) * (A3(u, i, j, k) - uavg[k]));
+          A3(vt, i, j, k) = -(rdalpha * 0.5f * (A3(th, i, j - 1, k) + A3(th, i, j, k)) * (A3(v, i, j, k) - vavg[k]));
+          A3(wt, i, j, k) = -(rdalpha * A3(tf, i, j, k) * A3(w, i, j, k));
+          A3(tt, i, j, k) = -(rdalpha * A3(ts, i, j, k) * ((A3(g->th0, i, j, k) - thavg[k]) + A3(t, i, j, k)));
+        } else {
+          A3(ut, i, j, k) = 0.0f; A3(vt, i, j, k) = 0.0f; A3(wt, i, j, k) = 0.0f; A3(tt, i, j, k) = 0.0f;
+        }
+      }
+  const int numq = cfg->imoist ? cfg->numq : 0, npt = cfg->iptra ? cfg->npt : 0;
+  for (int n = 0; n < numq + npt; n++) {
+    F3 q = mkS(g, (n < numq ? qten : ptten) + (long)(n < numq ? n : n - numq) * nS(g));
+    for (int k = 1; k <= g->nk; k++) for (int j = 1; j <= g->nj; j++) for (int i = 1; i <= g->ni; i++)
+      A3(q, i, j, k) = 0.0f;
+  }
+  return 0;
+}
+
+/* calcener: misclibs.F:3343-3454 (umove = vmove = 0).  Kinetic, internal,
+   potential and latent energy and their total, each an FP64 sum over the
+   physical cells.  Operands keep the reference's kinds: the per-cell
+   factors are binary32 expressions promoted where a binary64 operand meets
+   them.  ql, qi, vr may be NULL (zero); qv may be NULL for a dry run. */
+int oracle_calcener(const cm1g_config_t *cfg, const cm1g_grid_t *gr, const float *zh, const float *rho,
+                    const float *ua, const float *va, const float *wa, const float *ppi, const float *tha,
+                    const float *qv, const float *ql, const float *qi, const float *vr, double out[5]) {
+  OG G, *g = &G;
+  if (og_setup(g, cfg, gr)) return -1;
+  const Consts c = g->c;
+  const float xlv = cfg->testcase == 4 ? 2.47e6f : cfg->testcase == 5 ? 2.50e6f : 2501000.0f;
+  const float xls = 2834000.0f, to = 273.15f;
+  const float lv1 = xlv + (c.cpl - c.cpv) * to, ls1 = xls + (c.cpi - c.cpv) * to;
+  F3 z = mkS(g, zh), r = mkS(g, rho), u = mkU(g, ua), v = mkV(g, va), w = mkW(g, wa), p = mkS(g, ppi), t = mkS(g, tha);
+  F3 fv = mkS(g, qv), fl = mkS(g, ql), fi = mkS(g, qi), fr = mkS(g, vr);
+  double ek = 0.0, ei = 0.0, ep = 0.0, le = 0.0;
+  for (int k = 1; k <= g->nk; k++) {
+    double f1 = 0.0, f2 = 0.0, f3 = 0.0, f4 = 0.0;
+    for (int j = 1; j <= g->nj; j++)
+      for (int i = 1; i <= g->ni; i++) {
+        const double tem = (double)(RUH(i) * RVH(j) * A3(g->rmh, i, j, k));
+        const float u1 = A3(u, i, j, k), u2 = A3(u, i + 1, j, k), v1 = A3(v, i, j, k), v2 = A3(v, i, j + 1, k);
+        const float w1 = A3(w, i, j, k), w2 = A3(w, i, j, k + 1);
+        const double ww = (double)(0.5f * (w1 + w2));
+        const float q_v = qv ? A3(fv, i, j, k) : 0.0f, q_l = ql ? A3(fl, i, j, k) : 0.0f;
+        const float q_i = qi ? A3(fi, i, j, k) : 0.0f, v_r = vr ? A3(fr, i, j, k) : 0.0f;
+        const double qtot = (double)((q_v + q_l) + q_i);
+        const float rr = A3(r, i, j, k);
+        const float ke = (0.5f * (u1 * u1 + u2 * u2) + 0.5f * (v1 * v1 + v2 * v2)) + 0.5f * (w1 * w1 + w2 * w2);
+        f1 = (f1 + (double)rr * tem * (1.0 + qtot) * 0.5 * (double)ke) +
+             (double)(q_l * rr) * tem * 0.5 * ((double)(v_r * v_r) - 2.0 * ww * (double)v_r);
+        const double tmp = (double)((A3(g->th0, i, j, k) + A3(t, i, j, k)) * (A3(g->pi0, i, j, k) + A3(p, i, j, k)));
+        f2 = f2 + (double)rr * tem * (double)(c.cv + c.cvv * q_v) * tmp;
+        f3 = f3 + (double)rr * tem * (1.0 + qtot) * (double)c.g * (double)A3(z, i, j, k);
+        f4 = (f4 + (double)rr * tem * (double)q_l * ((double)c.cpl * tmp - (double)lv1)) +
+             (double)rr * tem * (double)q_i * ((double)c.cpi * tmp - (double)ls1);
+      }
+    ek = ek + f1; ei = ei + f2; ep = ep + f3; le = le + f4;
+  }
+  const double vol = (double)(g->dx * g->dy * g->dz);
+  out[0] = ek * vol; out[1] = ei * vol; out[2] = ep * vol; out[3] = le * vol;
+  out[4] = ((out[0] + out[1]) + out[2]) + out[3];
+  return 0;
+}
+
 /* Exposed face-value functions for known-answer tests. */
 float oracle_flx5(float s1, float s2, float s3, float s4, float s5) { return flx5(s1, s2, s3, s4, s5); }
 float oracle_flx3(float s1, float s2, float s3) { return flx3(s1, s2, s3); }

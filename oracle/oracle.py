@@ -50,6 +50,10 @@ def lib():
         L.oracle_upstrpd.argtypes = [C.c_float] * 3 + [C.c_double]
         L.oracle_upstrpd.restype = C.c_float
         L.oracle_last_error.restype = C.c_char_p
+        L.oracle_dtsmall.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_int,
+                                     C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        L.oracle_tendency_init.argtypes = [cfgp, grp, C.c_int, C.c_float] + [P] * 16
+        L.oracle_calcener.argtypes = [cfgp, grp] + [P] * 11 + [C.POINTER(C.c_double)]
         L.oracle_threads.restype = C.c_int
         _lib = L
     return _lib

@@ -191,3 +191,37 @@ def test_golden_fixture_regression(oracle_lib):
             continue
         assert np.array_equal(st[k], fx[k]), k
     assert m2 == float(fx["mass2"]) and cfl == float(fx["cflmax"])
+
+
+def _dtsmall(L, psolver, dx, dy, dz, dt, adapt=0, nx=64, ny=64):
+    fdt, ddt, ns = C.c_float(dt), C.c_double(dt), C.c_int()
+    rc = L.oracle_dtsmall(psolver, nx, ny, dx, dy, dz, adapt, C.byref(fdt), C.byref(ddt), C.byref(ns))
+    return rc, ns.value, fdt.value, ddt.value
+
+
+def test_dtsmall_known_answers(oracle_lib):
+    """misclibs.F:817-915 for the three workloads' grids: dtsm = 0.6 min(dx,dy)/360."""
+    L = oracle_lib.lib()
+    assert _dtsmall(L, 3, 1000.0, 1000.0, 250.0, 6.0)[:2] == (0, 4)     # 64x64x40 bubble: 6/1.667 -> 4
+    assert _dtsmall(L, 3, 500.0, 500.0, 250.0, 3.0)[:2] == (0, 4)       # supercell: 3/0.833 -> 4
+    assert _dtsmall(L, 3, 50.0, 50.0, 20.0, 0.5)[:2] == (0, 6)          # CBL: 0.5/0.0833 -> 6
+    assert _dtsmall(L, 3, 500.0, 500.0, 250.0, 3.4)[:2] == (0, 6)       # 4.08 -> 4, 3.4/4 > dtsm -> 6
+    assert _dtsmall(L, 3, 500.0, 500.0, 250.0, 0.5)[:2] == (0, 4)       # at least 4
+    assert _dtsmall(L, 1, 500.0, 500.0, 250.0, 3.0)[:2] == (0, 1)
+    assert _dtsmall(L, 3, 50.0, 50.0, 20.0, 20.0)[0] == -2              # 240 > 192 small steps: stop
+    rc, ns, fdt, ddt = _dtsmall(L, 3, 50.0, 50.0, 20.0, 20.0, adapt=1)  # adapt_dt: cap and shorten dt
+    assert rc == 0 and ns == 192 and abs(ddt - 192 * (0.6 * 50 / 360)) < 1e-4 and fdt == np.float32(ddt)
+
+
+def test_dtsmall_library_matches_oracle(oracle_lib, cm1g):
+    """The C-ABI's dtsmall (host code, no GPU) against the oracle over a sweep."""
+    L = oracle_lib.lib()
+    for dx in (50.0, 125.0, 500.0, 1000.0, 2000.0):
+        for dt in (0.5, 1.0, 3.0, 6.0, 10.0, 12.5):
+            for psolver in (2, 3):
+                rc, ns, _, _ = _dtsmall(L, psolver, dx, dx, 0.5 * dx, dt)
+                if rc == 0:
+                    assert cm1g.dtsmall(psolver, 64, 64, dx, dx, 0.5 * dx, dt)[0] == ns, (dx, dt, psolver)
+                else:
+                    with pytest.raises(cm1g.CM1GError):
+                        cm1g.dtsmall(psolver, 64, 64, dx, dx, 0.5 * dx, dt)
