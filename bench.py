@@ -148,6 +148,72 @@ def workload_config(case, args):
             "parallelism": "replicas" if args.gpus > 1 else "single"}
 
 
+def run_ensemble(args):
+    """The uneven 64-member warm-bubble ensemble: one graph launch per large
+    step for all members (cm1g_ensemble_step) against looping the members'
+    own graph-replayed steps one after another.  Both legs are timed on the
+    host around `steps` synchronised steps (each call returns after its
+    results are read back)."""
+    import torch
+    from cm1_b200.cases import make_ensemble
+    from cm1_b200 import binding
+    members = make_ensemble(64)
+    cells = sum(c.cfg.ni * c.cfg.nj * c.cfg.nk for c in members)
+    ctxs = [binding.Context(c.cfg, c.grid) for c in members]
+    dev = [binding.to_device(c.state) for c in members]
+    ens = binding.Ensemble(ctxs)
+    dts, m1 = [c.dt for c in members], [c.mass1 for c in members]
+    for _ in range(args.warmup):
+        ens.step(dev, dts, m1, use_graph=True)
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ens.step(dev, dts, m1, use_graph=True)
+        sec = time.perf_counter() - t0
+    # looping the members: each its own captured step, one after another
+    for ctx, st, c in zip(ctxs, dev, members):
+        for _ in range(args.warmup):
+            ctx.step(st, c.dt, c.mass1, use_graph=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for ctx, st, c in zip(ctxs, dev, members):
+            ctx.step(st, c.dt, c.mass1, use_graph=True)
+    sec_loop = time.perf_counter() - t0
+    # and looping them with eager launches (no graphs): the plain per-member kernels
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for ctx, st, c in zip(ctxs, dev, members):
+            ctx.step(st, c.dt, c.mass1, use_graph=False)
+    sec_eager = time.perf_counter() - t0
+    hbm, peak_kind = peaks()
+    B = algorithmic_bytes_per_cell(members[0].cfg)
+    value = cells * args.steps / sec
+    loop_value = cells * args.steps / sec_loop
+    line = {"metric": "cell-updates/s per RK3 large step", "value": value, "unit": "cell-updates/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded, generated in-repo)",
+            "config": {"workload": "ensemble", "members": len(members), "total_cells": cells,
+                       "grids": sorted({(c.cfg.ni, c.cfg.nj, c.cfg.nk) for c in members}),
+                       "dt_s": members[0].dt, "nsound": members[0].cfg.nsound, "advwenos": 1,
+                       "timing": "host clock around synchronised steps",
+                       "l2": "all members together exceed L2 (no flush needed)"},
+            "step_roofline": {"algorithmic_bytes_per_cell": B, "achieved_gbs": B * value / 1e9,
+                              "frac": B * value / 1e9 / hbm, "peak": hbm, "peak_kind": peak_kind},
+            "looping_members": {"value": loop_value, "ms_per_step": 1e3 * sec_loop / args.steps},
+            "speedup_vs_looping": value / loop_value,
+            "looping_members_eager": {"value": cells * args.steps / sec_eager, "ms_per_step": 1e3 * sec_eager / args.steps},
+            "speedup_vs_looping_eager": sec_eager / sec,
+            "gpu_launches": ens.kernels_per_step() * args.steps, "clocks": clk.summary()}
+    print(json.dumps(line))
+    ens.close()
+    for c in ctxs:
+        c.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -161,6 +227,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "ensemble":
+        return run_ensemble(args)
 
     import torch
     from cm1_b200.cases import make_case

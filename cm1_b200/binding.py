@@ -65,6 +65,11 @@ def lib():
     L.cm1g_dtsmall.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, C.c_int32,
                                C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int32)]
     L.cm1g_tendency_init.argtypes = [ctxp, C.c_int32, C.c_float] + [_P] * 16
+    L.cm1g_ensemble_create.argtypes = [C.POINTER(ctxp), C.c_int32, C.POINTER(ctxp)]
+    L.cm1g_ensemble_step.argtypes = [ctxp, stp, C.POINTER(C.c_float), C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), C.POINTER(C.c_float), C.c_int32]
+    L.cm1g_ensemble_launch_count.argtypes = [ctxp, C.POINTER(C.c_int64)]
+    L.cm1g_ensemble_destroy.argtypes = [ctxp]
     L.cm1g_pdefq_noalloc.argtypes = [cfgp, C.c_float, C.POINTER(C.c_double), _P, _P, _P, _P, _P, C.c_void_p]
     _lib = L
     return L
@@ -207,6 +212,45 @@ class Context:
             out[buf.value.decode()] = (n.value, ms.value)
             i += 1
         return out
+
+
+class Ensemble:
+    """cm1g_ensemble_*: members advanced side by side, one graph per step.
+
+    contexts: list of Context (one per member); states: list of dicts of
+    CUDA tensors in the members' layouts."""
+
+    def __init__(self, contexts):
+        self.contexts = list(contexts)
+        arr = (C.c_void_p * len(self.contexts))(*[c.h for c in self.contexts])
+        h = C.c_void_p()
+        check(lib().cm1g_ensemble_create(arr, len(self.contexts), C.byref(h)))
+        self.h = h
+
+    def step(self, states, dt, mass1, use_graph=True):
+        n = len(self.contexts)
+        self._structs = (State * n)(*[Context.state_struct(s) for s in states])
+        dts = (C.c_float * n)(*dt)
+        m1 = (C.c_double * n)(*mass1)
+        m2, cfl = (C.c_double * n)(), (C.c_float * n)()
+        check(lib().cm1g_ensemble_step(self.h, self._structs, dts, m1, m2, cfl, 1 if use_graph else 0))
+        return list(m2), list(cfl)
+
+    def kernels_per_step(self):
+        n = C.c_int64()
+        check(lib().cm1g_ensemble_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cm1g_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def dtsmall(psolver, nx, ny, min_dx, min_dy, min_dz, dt, adapt_dt=0):

@@ -406,3 +406,24 @@ def make_case(name, seed=1234, **over):
     mass1 = float(rr.sum(dtype=np.float64))
     return Case(name=name, lay=lay, cfg=cfg, grid=gr, state=st, dt=float(w["dt"]),
                 mass1=mass1, nsteps=int(w["nsteps"]))
+
+
+ENSEMBLE_SIZES = tuple(range(48, 193, 16))   # nx, ny in {48 .. 192}
+
+
+def make_ensemble(n=64, seed=2024, sizes=ENSEMBLE_SIZES, levels=(40, 60, 80)):
+    """Uneven ensemble of warm-bubble members (dx = dy = 1 km, dz = 250 m, WENO5
+    scalars, periodic, dt = 6 s, nsound = 6): per member nx, ny drawn from
+    `sizes`, nz from `levels`, a bubble of 1-3 K and 3-6 km horizontal radius,
+    and a uniform background wind in +-10 m/s, all from `seed`."""
+    rng = np.random.default_rng(seed)
+    members = []
+    for m in range(n):
+        ni, nj = int(rng.choice(sizes)), int(rng.choice(sizes))
+        nk = int(rng.choice(levels))
+        amp, xr = float(rng.uniform(1.0, 3.0)), float(rng.uniform(3000.0, 6000.0))
+        u, v = (float(x) for x in rng.uniform(-10.0, 10.0, 2))
+        members.append(make_case("dry_bubble", seed=seed + 1 + m, ni=ni, nj=nj, nk=nk, advwenos=1,
+                                 bubble=dict(amp=amp, xr=xr, zr=1400.0, zc=1400.0),
+                                 wind=("uniform", dict(u=u, v=v))))
+    return members

@@ -663,6 +663,146 @@ extern "C" int cm1g_step(cm1g_ctx_t *c, int32_t nstep, float dt, double mtime, d
   return solve_common(c, dt, mass1, mass2, cflmax, st, 3, use_graph);
 }
 
+// ---------------------------------------------------------------------
+// Ensembles of independent members (uneven grids).  Each member keeps its
+// own context and stream; one ensemble step forks from the ensemble's
+// stream onto every member's stream, runs each member's large step there,
+// and joins back, so the members' kernels run side by side and the small
+// grids fill the GPU together.  With use_graph the whole fork/join is
+// captured once into one CUDA graph (cached on the member states, dt and
+// mass1) and replayed with a single launch per step.
+// ---------------------------------------------------------------------
+struct cm1g_ens {
+  std::vector<cm1g_ctx *> m;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<cm1g_state_t> gstate;
+  std::vector<float> gdt;
+  std::vector<double> gmass1;
+  int64_t graph_nodes = 0;
+};
+
+static void ens_drop_graph(cm1g_ens *e) {
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  e->exec = nullptr; e->graph = nullptr;
+}
+
+extern "C" int cm1g_ensemble_create(cm1g_ctx_t **members, int32_t n, cm1g_ens_t **out) {
+  if (!members || n < 1 || !out) return set_err(CM1G_ERR_ARG, "null argument or empty ensemble");
+  int dev0 = members[0] ? members[0]->device : -1;
+  for (int q = 0; q < n; q++) {
+    if (!members[q]) return set_err(CM1G_ERR_ARG, "member %d is null", q);
+    if (members[q]->device != dev0) return set_err(CM1G_ERR_ARG, "members must share one device");
+    for (int r = 0; r < q; r++)
+      if (members[r] == members[q] || members[r]->stream == members[q]->stream)
+        return set_err(CM1G_ERR_ARG, "members %d and %d share a context or stream", r, q);
+  }
+  cm1g_ens *e = new cm1g_ens();
+  e->m.assign(members, members + n);
+  e->join.resize(n);
+  bool ok = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) == cudaSuccess;
+  for (int q = 0; q < n && ok; q++) ok = cudaEventCreateWithFlags(&e->join[q], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) { cm1g_ensemble_destroy(e); return set_err(CM1G_ERR_CUDA, "ensemble stream/event creation failed"); }
+  *out = e;
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_ensemble_destroy(cm1g_ens_t *e) {
+  if (!e) return CM1G_OK;
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  ens_drop_graph(e);
+  for (cudaEvent_t ev : e->join) if (ev) cudaEventDestroy(ev);
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+  return CM1G_OK;
+}
+
+// fork onto the members' streams, one large step each, join
+static void ens_enqueue(cm1g_ens *e, const cm1g_state_t *st, const float *dt, const double *mass1) {
+  cudaEventRecord(e->fork, e->stream);
+  for (size_t q = 0; q < e->m.size(); q++) {
+    cm1g_ctx *c = e->m[q];
+    cudaStreamWaitEvent(c->stream, e->fork, 0);
+    run_step(c, &st[q], dt[q], mass1[q]);
+    cudaEventRecord(e->join[q], c->stream);
+    cudaStreamWaitEvent(e->stream, e->join[q], 0);
+  }
+}
+
+extern "C" int cm1g_ensemble_step(cm1g_ens_t *e, cm1g_state_t *states, const float *dt, const double *mass1,
+                                  double *mass2, float *cflmax, int32_t use_graph) {
+  if (!e || !states || !dt || !mass1) return set_err(CM1G_ERR_ARG, "null argument");
+  const size_t n = e->m.size();
+  for (size_t q = 0; q < n; q++) {
+    cm1g_ctx *c = e->m[q];
+    int rc = check_state(c, &states[q]);
+    if (rc) return rc;
+    if (!(dt[q] > 0.0f) || !std::isfinite(dt[q])) return set_err(CM1G_ERR_ARG, "member %zu: dt must be positive", q);
+    if (c->cfg.apmasscon == 1 && !(mass1[q] > 0.0)) return set_err(CM1G_ERR_ARG, "member %zu: mass1 must be positive", q);
+    const float *req[] = {states[q].ua, states[q].u3d, states[q].va, states[q].v3d, states[q].wa, states[q].w3d,
+                          states[q].pp3d, states[q].th3d, states[q].rho};
+    for (const float *p : req)
+      if (p && !is_device_ptr(p)) return set_err(CM1G_ERR_ARG, "member %zu: ensemble states must be device arrays", q);
+  }
+  if (use_graph) {
+    bool same = e->exec && e->gstate.size() == n &&
+                memcmp(e->gstate.data(), states, n * sizeof(cm1g_state_t)) == 0 &&
+                memcmp(e->gdt.data(), dt, n * sizeof(float)) == 0 && memcmp(e->gmass1.data(), mass1, n * sizeof(double)) == 0;
+    if (!same) {
+      ens_drop_graph(e);
+      int64_t before = 0;
+      for (cm1g_ctx *c : e->m) before += c->nlaunch;
+      CUCHK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+      ens_enqueue(e, states, dt, mass1);
+      cudaGraph_t gr;
+      CUCHK(cudaStreamEndCapture(e->stream, &gr));
+      e->graph = gr;
+      CUCHK(cudaGraphInstantiate(&e->exec, gr, 0));
+      int64_t after = 0;
+      for (cm1g_ctx *c : e->m) after += c->nlaunch;
+      e->graph_nodes = after - before;
+      e->gstate.assign(states, states + n);
+      e->gdt.assign(dt, dt + n);
+      e->gmass1.assign(mass1, mass1 + n);
+    }
+    CUCHK(cudaGraphLaunch(e->exec, e->stream));
+  } else {
+    ens_enqueue(e, states, dt, mass1);
+  }
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return set_err(CM1G_ERR_CUDA, "ensemble launch: %s", cudaGetErrorString(err));
+  // the members' mass sums and CFL maxima, read back in one synchronisation
+  std::vector<double> dv(2 * n);
+  std::vector<int> bits(n);
+  for (size_t q = 0; q < n; q++) {
+    CUCHK(cudaMemcpyAsync(&dv[2 * q], e->m[q]->dscal, 2 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    CUCHK(cudaMemcpyAsync(&bits[q], e->m[q]->cflbits, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  }
+  CUCHK(cudaStreamSynchronize(e->stream));
+  int rc = CM1G_OK;
+  for (size_t q = 0; q < n; q++) {
+    float f;
+    memcpy(&f, &bits[q], 4);
+    if (mass2) mass2[q] = e->m[q]->cfg.apmasscon == 1 ? dv[2 * q] : 0.0;
+    if (cflmax) cflmax[q] = f;
+    if (!std::isfinite(f) && rc == CM1G_OK)
+      rc = set_err(CM1G_ERR_NONFINITE, "member %zu: non-finite velocity after the large step", q);
+  }
+  return rc;
+}
+
+extern "C" int cm1g_ensemble_launch_count(cm1g_ens_t *e, int64_t *count) {
+  if (!e || !count) return set_err(CM1G_ERR_ARG, "null argument");
+  *count = e->graph_nodes;
+  return CM1G_OK;
+}
+
 extern "C" int cm1g_pdefq(cm1g_ctx_t *c, float rmax, double *asq, const float *rho, float *q3d) {
   if (!c || !rho || !q3d) return set_err(CM1G_ERR_ARG, "null argument");
   ProfActive pa(c);

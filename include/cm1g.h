@@ -120,6 +120,7 @@ typedef struct cm1g_state {
 } cm1g_state_t;
 
 typedef struct cm1g_ctx cm1g_ctx_t;
+typedef struct cm1g_ens cm1g_ens_t;
 
 const char *cm1g_last_error(void);
 int cm1g_version(int32_t *major, int32_t *minor);
@@ -237,6 +238,20 @@ int cm1g_maxmin(cm1g_ctx_t *ctx, const float *a, int32_t stag,
 int cm1g_profile(cm1g_ctx_t *ctx, int32_t enable);
 int cm1g_profile_read(cm1g_ctx_t *ctx, int32_t index, char *name, int32_t name_len,
                       int64_t *launches, double *total_ms);
+
+/* Ensembles of independent members with uneven grids (no counterpart in the
+ * reference, which runs one domain per executable).  Each member is a context
+ * from cm1g_init with its own stream; cm1g_ensemble_step advances every member
+ * by one large step (solve2 + pdefq + solve3, as cm1g_step), forking the
+ * members onto their own streams so that their kernels run concurrently, and
+ * with use_graph replays the whole ensemble step as one CUDA graph launch.
+ * states, dt, mass1, mass2 and cflmax hold one entry per member; the states
+ * must be device arrays.  The ensemble does not own the member contexts. */
+int cm1g_ensemble_create(cm1g_ctx_t **members, int32_t n, cm1g_ens_t **ens);
+int cm1g_ensemble_step(cm1g_ens_t *ens, cm1g_state_t *states, const float *dt, const double *mass1,
+                       double *mass2, float *cflmax, int32_t use_graph);
+int cm1g_ensemble_launch_count(cm1g_ens_t *ens, int64_t *kernels_per_step);
+int cm1g_ensemble_destroy(cm1g_ens_t *ens);
 
 /* Largest ni*nj that cm1g_pdefq_noalloc accepts: its scratch array holds one
  * FP64 budget per column, 8 MiB of device memory at this size. */
