@@ -70,6 +70,17 @@ def lib():
                                      C.POINTER(C.c_double), C.POINTER(C.c_float), C.c_int32]
     L.cm1g_ensemble_launch_count.argtypes = [ctxp, C.POINTER(C.c_int64)]
     L.cm1g_ensemble_destroy.argtypes = [ctxp]
+    L.cm1g_mlp_param_count.restype = C.c_int32
+    L.cm1g_mlp_param_count.argtypes = []
+    L.cm1g_mlp_forward.argtypes = [_P, C.c_int32, _P, _P, _P, _P, _P, C.c_void_p]
+    L.cm1g_mlp_backward.argtypes = [_P, C.c_int32, _P, _P, _P, _P, _P, C.c_void_p]
+    L.cm1g_closure_loss.argtypes = [C.c_int32, _P, _P, _P, _P, _P, _P, _P, C.c_void_p, C.c_void_p]
+    L.cm1g_adam.argtypes = [C.c_int32, _P, _P, _P, _P, C.c_int32, C.c_float, C.c_float, C.c_void_p]
+    L.cm1g_face_features.argtypes = [C.c_int32] * 5 + [_P, _P, C.c_int32, _P, C.c_float, _P, _P, _P, _P,
+                                                         C.c_void_p]
+    L.cm1g_face_phi.argtypes = [C.c_int64, _P, _P, _P, _P, _P, C.c_void_p]
+    L.cm1g_closure_set.argtypes = [ctxp, _P, C.c_int32]
+    L.cm1g_capture_fluxes.argtypes = [ctxp, _P, _P, _P, _P]
     L.cm1g_pdefq_noalloc.argtypes = [cfgp, C.c_float, C.POINTER(C.c_double), _P, _P, _P, _P, _P, C.c_void_p]
     _lib = L
     return L
@@ -197,6 +208,13 @@ class Context:
         check(lib().cm1g_tendency_init(self.h, irdamp, rdalpha, ptr(tauh), ptr(taus), ptr(tauf), ptr(uavg), ptr(vavg),
                                        ptr(thavg), ptr(ua), ptr(va), ptr(wa), ptr(tha), ptr(uten1), ptr(vten1),
                                        ptr(wten1), ptr(thten1), ptr(qten), ptr(ptten)))
+
+    def closure(self, params, enable=True):
+        """Learned closure of theta's horizontal faces on/off (params: FP32 array)."""
+        check(lib().cm1g_closure_set(self.h, ptr(params), 1 if enable else 0))
+
+    def capture_fluxes(self, fx=None, fy=None, rx=None, ry=None):
+        check(lib().cm1g_capture_fluxes(self.h, ptr(fx), ptr(fy), ptr(rx), ptr(ry)))
 
     def profile(self, enable):
         check(lib().cm1g_profile(self.h, 1 if enable else 0))

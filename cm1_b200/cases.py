@@ -129,6 +129,10 @@ def _hodograph(kind, z, **kw):
         return np.zeros_like(z), np.zeros_like(z)
     if kind == "uniform":
         return np.full_like(z, kw.get("u", 0.0)), np.full_like(z, kw.get("v", 0.0))
+    if kind == "shear":
+        # u grows linearly from 0 to `du` over the lowest `depth` metres, constant above
+        du, depth = kw.get("du", 10.0), kw.get("depth", 6000.0)
+        return du * np.clip(z / depth, 0.0, 1.0), np.zeros_like(z)
     if kind == "curved":
         # quarter circle of radius 10 m/s below 2 km, straight to U at 6 km,
         # constant above; shifted so the storm is roughly stationary.

@@ -20,6 +20,13 @@ void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, 
 void launch_bc_batch(const DGrid &g, float *const *arrays, const int *which, const int *wflag, int n,
                      cudaStream_t st, int64_t *nlaunch);
 void launch_tend_init(const DGrid &g, const TendIn &t, cudaStream_t st, int64_t *nl);
+void launch_mlp_forward(const float *params, int n, const float *x, float *y, float *c, float *z1, float *z2,
+                        cudaStream_t st);
+void launch_face_features(int ni, int nj, int nk, int ngxy, int dir, const float *s, const float *th0, int sadd,
+                          const float *vel, float dtdx, float *x, float *m, float *d, float *u, cudaStream_t st);
+void launch_face_phi(long nf, const float *x, const float *c, const float *m, const float *d, float *phi,
+                     cudaStream_t st);
+int mlp_param_count();
 int ener_chunks(const DGrid &g);
 void launch_calcener(const DGrid &g, const EnerIn &e, double *part, double *out, cudaStream_t st, int64_t *nl);
 void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w, const float *uten1,
@@ -32,7 +39,7 @@ void launch_advs(const DGrid &g, const float *rru, const float *rrv, const float
 void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const float *rrw, const float *s,
                        const float *s0, int sadd, const float *ten1, const float *thterm, float *snew, int weno,
                        int pdef, int pdefweno, double weps, float dt, int flush, float *scratch, cudaStream_t st,
-                       int64_t *nl);
+                       int64_t *nl, const TileExtras *ex = nullptr);
 void launch_sound(const DGrid &g, int nsound, int nrk, float dt, const float *ua, float *u3d, const float *uten,
                   const float *va, float *v3d, const float *vten, const float *wa, float *w3d, const float *wten,
                   const float *ppi, float *pp3d, const float *piadv, const float *ppten, float *ppx,
@@ -139,6 +146,13 @@ struct cm1g_ctx {
   float *sx[2 * (1 + 2 * CM1G_MAXQ)] = {};   // per-scalar stage buffers
   float *pdefscr = nullptr;                   // 6 s-arrays
   float *mdivx = nullptr;                     // divx of the momentum pass
+  // learned closure of theta's horizontal faces (cm1g_closure_set)
+  bool cl_on = false;
+  float *cl_params = nullptr;
+  float *cl_x[2] = {}, *cl_m[2] = {}, *cl_d[2] = {}, *cl_u[2] = {}, *cl_c[2] = {}, *cl_phi[2] = {};
+  long cl_nf[2] = {0, 0};
+  // capture of theta's final-stage face fluxes (cm1g_capture_fluxes)
+  float *cap_fx = nullptr, *cap_fy = nullptr, *cap_rx = nullptr, *cap_ry = nullptr;
   double *part3 = nullptr, *part4 = nullptr, *dscal = nullptr, *bud = nullptr, *lev = nullptr;
   double *ener = nullptr;                     // calcener chunk sums (4 x nk x chunks) and results
   float *fscal = nullptr;
@@ -451,6 +465,19 @@ static int check_state(const cm1g_ctx *c, const cm1g_state_t *st) {
 // ---------------------------------------------------------------------
 // solve2 on device arrays (solve2.F:296-2075)
 // ---------------------------------------------------------------------
+// learned face values of theta's horizontal faces for one RK stage: features
+// of every x- and y-face, the MLP, and the bounded face value (NaN: WENO5)
+static void closure_phi(cm1g_ctx *c, const float *th, float dt, cudaStream_t st, int64_t *nl) {
+  const DGrid &g = c->g;
+  for (int dir = 0; dir < 2; dir++) {
+    launch_face_features(g.ni, g.nj, g.nk, g.ngxy, dir, th, g.th0, 1, dir ? c->rrv : c->rru,
+                         dt * (dir ? g.rdy : g.rdx), c->cl_x[dir], c->cl_m[dir], c->cl_d[dir], c->cl_u[dir], st);
+    launch_mlp_forward(c->cl_params, (int)c->cl_nf[dir], c->cl_x[dir], nullptr, c->cl_c[dir], nullptr, nullptr, st);
+    launch_face_phi(c->cl_nf[dir], c->cl_x[dir], c->cl_c[dir], c->cl_m[dir], c->cl_d[dir], c->cl_phi[dir], st);
+    if (nl) *nl += 3;
+  }
+}
+
 static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass1) {
   const DGrid &g = c->g;
   const cm1g_config_t &cf = c->cfg;
@@ -486,9 +513,18 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
     if (openrad) launch_radbc4(g, d->ua, d->u3d, d->va, d->v3d, d->radbcw, d->radbce, d->radbcs, d->radbcn, dttmp, st, nl);
     const int weno = (cf.advwenos == 1 || (cf.advwenos == 2 && nrk == 3)) ? 1 : 0;
     // theta (solve2.F:1320-1425)
+    TileExtras ex;
+    const TileExtras *exp = nullptr;
+    if (c->cl_on) {
+      closure_phi(c, th_in, dt, st, nl);
+      ex.phix = c->cl_phi[0]; ex.phiy = c->cl_phi[1]; exp = &ex;
+    }
+    if (nrk == 3 && c->cap_fx) {
+      ex.capfx = c->cap_fx; ex.capfy = c->cap_fy; ex.caprx = c->cap_rx; ex.capry = c->cap_ry; exp = &ex;
+    }
     launch_advs_tiled(g, c->rru, c->rrv, c->rrw, th_in, d->tha, 1, d->thten1,
                       (cf.imoist && cf.eqtset == 2) ? c->thterm : nullptr, buf_out(0, nrk), weno, 0, 0,
-                      (double)(10.0f * 1.0e-18f), dttmp, 1, c->pdefscr, st, nl);
+                      (double)(10.0f * 1.0e-18f), dttmp, 1, c->pdefscr, st, nl, exp);
     // moisture (solve2.F:1431-1530)
     for (int n = 0; n < numq; n++) {
       const int s = 1 + n;
@@ -800,6 +836,46 @@ extern "C" int cm1g_ensemble_step(cm1g_ens_t *e, cm1g_state_t *states, const flo
 extern "C" int cm1g_ensemble_launch_count(cm1g_ens_t *e, int64_t *count) {
   if (!e || !count) return set_err(CM1G_ERR_ARG, "null argument");
   *count = e->graph_nodes;
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_closure_set(cm1g_ctx_t *c, const float *params, int32_t enable) {
+  if (!c) return set_err(CM1G_ERR_STATE, "null context");
+  drop_graph(c);
+  if (!enable) { c->cl_on = false; return CM1G_OK; }
+  if (!params) return set_err(CM1G_ERR_ARG, "null parameters");
+  const DGrid &g = c->g;
+  if (!c->cl_params) {
+    c->cl_params = (float *)dalloc(c, (size_t)mlp_param_count() * sizeof(float));
+    for (int dir = 0; dir < 2; dir++) {
+      const long nf = (long)(dir ? g.ni : g.ni + 1) * (dir ? g.nj + 1 : g.nj) * g.nk;
+      c->cl_nf[dir] = nf;
+      c->cl_x[dir] = (float *)dalloc(c, nf * 8 * sizeof(float));
+      c->cl_c[dir] = (float *)dalloc(c, nf * 6 * sizeof(float));
+      c->cl_m[dir] = (float *)dalloc(c, nf * sizeof(float));
+      c->cl_d[dir] = (float *)dalloc(c, nf * sizeof(float));
+      c->cl_u[dir] = (float *)dalloc(c, nf * sizeof(float));
+      c->cl_phi[dir] = (float *)dalloc(c, nf * sizeof(float));
+      if (!c->cl_x[dir] || !c->cl_c[dir] || !c->cl_m[dir] || !c->cl_d[dir] || !c->cl_u[dir] || !c->cl_phi[dir])
+        return set_err(CM1G_ERR_NOMEM, "closure buffers");
+    }
+    if (!c->cl_params) return set_err(CM1G_ERR_NOMEM, "closure parameters");
+  }
+  CUCHK(cudaMemcpyAsync(c->cl_params, params, (size_t)mlp_param_count() * sizeof(float), cudaMemcpyDefault,
+                        c->stream));
+  CUCHK(cudaStreamSynchronize(c->stream));
+  c->cl_on = true;
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_capture_fluxes(cm1g_ctx_t *c, float *fx, float *fy, float *rx, float *ry) {
+  if (!c) return set_err(CM1G_ERR_STATE, "null context");
+  drop_graph(c);
+  if (!fx && !fy && !rx && !ry) { c->cap_fx = c->cap_fy = c->cap_rx = c->cap_ry = nullptr; return CM1G_OK; }
+  if (!fx || !fy || !rx || !ry) return set_err(CM1G_ERR_ARG, "give all four capture arrays or none");
+  for (const float *p : {fx, fy, rx, ry})
+    if (!is_device_ptr(p)) return set_err(CM1G_ERR_ARG, "capture arrays must be device arrays");
+  c->cap_fx = fx; c->cap_fy = fy; c->cap_rx = rx; c->cap_ry = ry;
   return CM1G_OK;
 }
 

@@ -119,6 +119,17 @@ __device__ __forceinline__ float absmax5(float a, float b, float c, float d, flo
   return fmaxf(fmaxf(fmaxf(fmaxf(fabsf(a), fabsf(b)), fabsf(c)), fabsf(d)), fabsf(e));
 }
 
+// Optional extras of the scalar tile (k_advs_tile, update mode):
+//  phix/phiy  learned face values of the horizontal faces (NaN: use WENO5),
+//             indexed f = (k-1)*nfx*nfy + (j-1)*nfx + (i-1) with
+//             nfx x nfy = (ni+1) x nj for x-faces and ni x (nj+1) for y-faces;
+//  cap*       capture of the x/y face fluxes and face mass fluxes the
+//             kernel used (u-/v-array layout), for building training targets.
+struct TileExtras {
+  const float *phix = nullptr, *phiy = nullptr;
+  float *capfx = nullptr, *capfy = nullptr, *caprx = nullptr, *capry = nullptr;
+};
+
 // Inputs of the solve1 tendency initialisation and of calcener (k_misc.cu).
 struct TendIn {
   int irdamp;

@@ -1157,6 +1157,7 @@ struct STileOut {
   const float *sbase;         // RK base value (tha, qa, pta)
   float *snew;                // MODE_UPDATE output
   float *advx, *advy, *advz, *dumx, *dumy, *dumz;   // MODE_PDEF1 outputs
+  TileExtras ex;              // learned face values / flux capture (update mode)
 };
 
 // The (TX+1)*TY x-faces and TX*(TY+1) y-faces of a
@@ -1200,19 +1201,26 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
     }
   }
   int fxo[2], fxs[2], fyo[2], fys[2];   // face offsets (-1: no face) and stencil starts in ss
+  int fxl[2], fyl[2];                   // in-level index of the face in the learned-value arrays
 #pragma unroll
   for (int q = 0; q < 2; q++) {
     const int f = tid + q * NT;
-    fxo[q] = -1; fxs[q] = 0; fyo[q] = -1; fys[q] = 0;
+    fxo[q] = -1; fxs[q] = 0; fyo[q] = -1; fys[q] = 0; fxl[q] = 0; fyl[q] = 0;
     if (f < NFX) {
       const int row = f / (TX + 1), col = f - row * (TX + 1);
       const int ii = i0 + col, jj = j0 + row;
-      if (ii <= ni + 1 && jj <= nj) { fxo[q] = (ii - g.ib) + (NI + 1) * (jj - g.jb); fxs[q] = (row + 3) * SP + col; }
+      if (ii <= ni + 1 && jj <= nj) {
+        fxo[q] = (ii - g.ib) + (NI + 1) * (jj - g.jb); fxs[q] = (row + 3) * SP + col;
+        fxl[q] = (jj - 1) * (ni + 1) + (ii - 1);
+      }
     }
     if (f < NFY) {
       const int row = f / TX, col = f - row * TX;
       const int ii = i0 + col, jj = j0 + row;
-      if (ii <= ni && jj <= nj + 1) { fyo[q] = (ii - g.ib) + NI * (jj - g.jb); fys[q] = row * SP + col + 3; }
+      if (ii <= ni && jj <= nj + 1) {
+        fyo[q] = (ii - g.ib) + NI * (jj - g.jb); fys[q] = row * SP + col + 3;
+        fyl[q] = (jj - 1) * ni + (ii - 1);
+      }
     }
   }
 
@@ -1297,13 +1305,30 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
       const int f = tid + q * NT;
       if (fxo[q] >= 0) {
         const float *p = &ss[fxs[q]];
-        fx[f] = hflux5(ru[q] * r0k, p[0], p[1], p[2], p[3], p[4], p[5], WENO, pdef, weps);
+        const float r = ru[q] * r0k;
+        float ph = __int_as_float(0x7fc00000);
+        if (MODE == MODE_UPDATE && out.ex.phix) ph = out.ex.phix[(long)(k - 1) * (ni + 1) * nj + fxl[q]];
+        const float fl = (ph == ph) ? r * ph : hflux5(r, p[0], p[1], p[2], p[3], p[4], p[5], WENO, pdef, weps);
+        fx[f] = fl;
         ux[f] = ru[q];
+        if (MODE == MODE_UPDATE && out.ex.capfx) {
+          out.ex.capfx[(long)k * planeU + fxo[q]] = fl;
+          out.ex.caprx[(long)k * planeU + fxo[q]] = r;
+        }
       }
       if (fyo[q] >= 0) {
         const float *p = &ss[fys[q]];
-        fy[f] = hflux5(rv[q] * r0k, p[0], p[SP], p[2 * SP], p[3 * SP], p[4 * SP], p[5 * SP], WENO, pdef, weps);
+        const float r = rv[q] * r0k;
+        float ph = __int_as_float(0x7fc00000);
+        if (MODE == MODE_UPDATE && out.ex.phiy) ph = out.ex.phiy[(long)(k - 1) * ni * (nj + 1) + fyl[q]];
+        const float fl = (ph == ph) ? r * ph
+                                    : hflux5(r, p[0], p[SP], p[2 * SP], p[3 * SP], p[4 * SP], p[5 * SP], WENO, pdef, weps);
+        fy[f] = fl;
         vy[f] = rv[q];
+        if (MODE == MODE_UPDATE && out.ex.capfy) {
+          out.ex.capfy[(long)k * planeV + fyo[q]] = fl;
+          out.ex.capry[(long)k * planeV + fyo[q]] = r;
+        }
       }
     }
     const float fwhi = whi * LDG(&g.rf0[k + 1]);
@@ -1386,12 +1411,13 @@ static const int ADV_TX = 32, ADV_TY = 8, ADV_KC = 16;
 void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const float *rrw, const float *s,
                        const float *s0, int sadd, const float *ten1, const float *thterm, float *snew, int weno,
                        int pdef, int pdefweno, double weps, float dt, int flush, float *scratch, cudaStream_t st,
-                       int64_t *nl) {
+                       int64_t *nl, const TileExtras *ex) {
   SAdv a{rru, rrv, rrw, s, s0, nullptr, thterm, 1, sadd};
   dim3 blk(ADV_TX, ADV_TY),
       grid((g.ni + ADV_TX - 1) / ADV_TX, (g.nj + ADV_TY - 1) / ADV_TY, (g.nk + ADV_KC - 1) / ADV_KC);
   STileOut o{};
   o.sten_in = ten1; o.sbase = s0; o.snew = snew;
+  if (ex) o.ex = *ex;
   if (!pdef) {
     ProfScope _ps("k_advs_tile", st);
     if (weno) k_advs_tile<ADV_TX, ADV_TY, ADV_KC, MODE_UPDATE, 1><<<grid, blk, 0, st>>>(g, a, o, 0, pdefweno, weps, dt, flush);

@@ -253,6 +253,45 @@ int cm1g_ensemble_step(cm1g_ens_t *ens, cm1g_state_t *states, const float *dt, c
 int cm1g_ensemble_launch_count(cm1g_ens_t *ens, int64_t *kernels_per_step);
 int cm1g_ensemble_destroy(cm1g_ens_t *ens);
 
+/* Learned coarse-grid advection closure (no counterpart in the reference).
+ * A 7 -> 64 -> 64 -> 6 GELU MLP with BF16 weights and FP32 accumulation
+ * predicts the six coefficients (projected to sum to 1) of the face value
+ * of theta's horizontal faces from the face's upwind-ordered six-point
+ * stencil (normalised) and its Courant number; where the face value leaves
+ * the range of the two cells sharing the face, WENO5 is used.  params is an
+ * FP32 array of cm1g_mlp_param_count() values: W1[8][64], b1[64],
+ * W2[64][64], b2[64], W3[64][8], b3[8].  The building blocks below take
+ * device pointers and the caller's stream:
+ *   face_features: x[f][8] (6 stencil values, Courant number, 0), mean m[f],
+ *     scale d[f], face velocity u[f] of the x-faces (dir 0: (ni+1) x nj x nk)
+ *     or y-faces (dir 1: ni x (nj+1) x nk), f = ((k-1)*nfy + j-1)*nfx + i-1;
+ *   mlp_forward: y[n][8] outputs before the projection, c[n][6]
+ *     coefficients, z1/z2[n][64] pre-activations (each may be NULL);
+ *   mlp_backward: grad += d loss / d params from dy = d loss / d y;
+ *   closure_loss: *loss += sum_f w (phi_f - target_f)^2, dy of it;
+ *   adam: one Adam step on params with grad * grad_scale;
+ *   face_phi: phi[f] = m + d sum_k c_k x_k, or NaN outside the bounds.
+ * cm1g_closure_set turns the closure on (enable=1) for theta in the
+ * context's large step; cm1g_capture_fluxes records theta's final-stage
+ * x/y face fluxes and face mass fluxes (u-/v-array layout, device arrays;
+ * all NULL stops) for building training targets from fine-grid runs. */
+int32_t cm1g_mlp_param_count(void);
+int cm1g_mlp_forward(const float *params, int32_t n, const float *x, float *y, float *c, float *z1, float *z2,
+                     void *stream);
+int cm1g_mlp_backward(const float *params, int32_t n, const float *x, const float *z1, const float *z2,
+                      const float *dy, float *grad, void *stream);
+int cm1g_closure_loss(int32_t n, const float *x, const float *y, const float *m, const float *d,
+                      const float *target, const float *w, float *dy, double *loss, void *stream);
+int cm1g_adam(int32_t np, float *params, const float *grad, float *m1, float *m2, int32_t step, float lr,
+              float grad_scale, void *stream);
+int cm1g_face_features(int32_t ni, int32_t nj, int32_t nk, int32_t ngxy, int32_t dir, const float *s,
+                       const float *th0, int32_t sadd, const float *vel, float dtdx, float *x, float *m, float *d,
+                       float *u, void *stream);
+int cm1g_face_phi(int64_t nf, const float *x, const float *c, const float *m, const float *d, float *phi,
+                  void *stream);
+int cm1g_closure_set(cm1g_ctx_t *ctx, const float *params, int32_t enable);
+int cm1g_capture_fluxes(cm1g_ctx_t *ctx, float *fx, float *fy, float *rx, float *ry);
+
 /* Largest ni*nj that cm1g_pdefq_noalloc accepts: its scratch array holds one
  * FP64 budget per column, 8 MiB of device memory at this size. */
 #define CM1G_PDEFQ_NOALLOC_MAX_COLUMNS (1024 * 1024)

@@ -1,0 +1,154 @@
+"""Learned closure kernels (k_learned.cu) against the CPU reference of the MLP
+(oracle/mlp_ref.py): tensor-core forward, backward gradients, loss, Adam,
+face features, and the closure inside the large step."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from cm1_b200.cases import make_case
+from oracle import mlp_ref as R
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _p(t):
+    return C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_float)) if t is not None else C.cast(None, C.POINTER(C.c_float))
+
+
+def _data(n, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(0, 0.3, (n, R.IN)).astype(np.float32)
+    x[:, 6] = rng.uniform(0, 1, n)
+    x[:, 7] = 0
+    return x, rng
+
+
+def test_forward_and_backward_match_reference(cm1g):
+    torch = _torch()
+    L = cm1g.lib()
+    assert L.cm1g_mlp_param_count() == R.P_TOTAL
+    n = 1000                                          # not a multiple of 16: partial tiles
+    x, rng = _data(n, 1)
+    p = R.init_params(2)
+    p[R.P_W3:R.P_B3] = rng.normal(0, 0.2, R.H * R.OUT).astype(np.float32)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+    P, X = dev(p), dev(x)
+    Y, Cc = torch.zeros(n, 8, device="cuda"), torch.zeros(n, 6, device="cuda")
+    Z1, Z2 = torch.zeros(n, 64, device="cuda"), torch.zeros(n, 64, device="cuda")
+    cm1g.check(L.cm1g_mlp_forward(_p(P), n, _p(X), _p(Y), _p(Cc), _p(Z1), _p(Z2), None))
+    torch.cuda.synchronize()
+    z1g, z2g = Z1.cpu().numpy().astype(np.float64), Z2.cpu().numpy().astype(np.float64)
+    _, _, z1r, _ = R.forward(p, x)
+    assert np.abs(z1g - z1r).max() <= 1e-5 * max(1.0, np.abs(z1r).max())
+    # later layers from the GPU's pre-activations (same BF16 rounding points)
+    yr, cr, _, z2r = R.forward(p, x, z1=z1g)
+    assert np.abs(z2g - z2r).max() <= 1e-5 * max(1.0, np.abs(z2r).max())
+    yr, cr, _, _ = R.forward(p, x, z1=z1g, z2=z2g)
+    # the GPU's float32 GELU and the reference's float64 GELU can land on
+    # opposite sides of a BF16 rounding tie (one BF16 ulp of an activation)
+    assert np.abs(Y.cpu().numpy() - yr).max() <= 1e-3 * max(1.0, np.abs(yr).max())
+    assert np.abs(Cc.cpu().numpy() - cr).max() <= 1e-3 * max(1.0, np.abs(cr).max())
+    assert np.allclose(Cc.cpu().numpy().sum(1), 1.0, atol=1e-5)
+
+    # loss and dy
+    m = rng.normal(0, 1, n).astype(np.float32)
+    d = rng.uniform(0.1, 2, n).astype(np.float32)
+    tgt = (m + rng.normal(0, 0.1, n)).astype(np.float32)
+    w = rng.uniform(0.5, 2, n).astype(np.float32)
+    DY = torch.zeros(n, 8, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+    Md, Dd, Td, Wd = dev(m), dev(d), dev(tgt), dev(w)          # keep the device copies alive
+    cm1g.check(L.cm1g_closure_loss(n, _p(X), _p(Y), _p(Md), _p(Dd), _p(Td), _p(Wd), _p(DY),
+                                   C.c_void_p(loss.data_ptr()), None))
+    torch.cuda.synchronize()
+    lr_, dyr = R.loss_and_dy(x, Y.cpu().numpy().astype(np.float64), m, d, tgt, w)
+    assert abs(loss.item() - lr_) <= 1e-5 * abs(lr_)
+    assert np.abs(DY.cpu().numpy() - dyr).max() <= 1e-4 * max(1e-6, np.abs(dyr).max())
+
+    # backward
+    G = torch.zeros(R.P_TOTAL, device="cuda")
+    cm1g.check(L.cm1g_mlp_backward(_p(P), n, _p(X), _p(Z1), _p(Z2), _p(DY), _p(G), None))
+    torch.cuda.synchronize()
+    gr = R.backward(p, x, z1g, z2g, DY.cpu().numpy().astype(np.float64))
+    gg = G.cpu().numpy()
+    for a, b in ((R.P_W1, R.P_B1), (R.P_B1, R.P_W2), (R.P_W2, R.P_B2), (R.P_B2, R.P_W3), (R.P_W3, R.P_B3),
+                 (R.P_B3, R.P_TOTAL)):
+        scale = max(1e-12, np.abs(gr[a:b]).max())
+        assert np.abs(gg[a:b] - gr[a:b]).max() <= 2e-3 * scale, (a, b)
+
+    # Adam
+    M1, M2 = torch.zeros(R.P_TOTAL, device="cuda"), torch.zeros(R.P_TOTAL, device="cuda")
+    cm1g.check(L.cm1g_adam(R.P_TOTAL, _p(P), _p(G), _p(M1), _p(M2), 1, 1e-3, 0.5, None))
+    torch.cuda.synchronize()
+    pr, _, _ = R.adam(p.astype(np.float64), gg.astype(np.float64), 0.0, 0.0, 1, 1e-3, 0.5)
+    assert np.abs(P.cpu().numpy() - pr).max() <= 1e-6
+
+
+def test_face_features_match_numpy(cm1g):
+    torch = _torch()
+    L = cm1g.lib()
+    case = make_case("dry_bubble", ni=20, nj=12, nk=10)
+    lay, st, gr = case.lay, case.state, case.grid
+    rng = np.random.default_rng(3)
+    th = (st["th3d"] + rng.normal(0, 0.5, lay.shape(1))).astype(np.float32)
+    u = rng.normal(0, 5, lay.shape(2)).astype(np.float32)
+    th0 = gr["th0"][:, 3, 3].copy()
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+    nf = (lay.ni + 1) * lay.nj * lay.nk
+    X, M, D, U = (torch.zeros(nf, 8, device="cuda"), torch.zeros(nf, device="cuda"), torch.zeros(nf, device="cuda"),
+                  torch.zeros(nf, device="cuda"))
+    TH, TH0, UU = dev(th), dev(th0), dev(u)                  # keep the device copies alive
+    cm1g.check(L.cm1g_face_features(lay.ni, lay.nj, lay.nk, 3, 0, _p(TH), _p(TH0), 1, _p(UU), 0.3,
+                                    _p(X), _p(M), _p(D), _p(U), None))
+    torch.cuda.synchronize()
+    X, M, D, U = X.cpu().numpy(), M.cpu().numpy(), D.cpu().numpy(), U.cpu().numpy()
+    s = (th0[:, None, None] - np.float32(300.0)) + th       # (NK, NJ, NI), the advected value
+    f = 0
+    for k in range(1, lay.nk + 1):
+        for j in range(1, lay.nj + 1):
+            for i in range(1, lay.ni + 2):
+                uu = u[lay.kx(k), lay.jx(j), lay.ix(i)]
+                offs = range(-3, 3) if uu >= 0 else range(2, -4, -1)
+                v = np.array([s[lay.kx(k), lay.jx(j), lay.ix(i + o)] for o in offs], np.float32)
+                mean = v.sum(dtype=np.float32) / np.float32(6)
+                sc = (v.max() - v.min()) + np.float32(1e-6)
+                assert abs(M[f] - mean) <= 1e-6 * max(1.0, abs(mean)) and abs(D[f] - sc) <= 1e-6 * sc
+                assert np.abs(X[f, :6] - (v - mean) / sc).max() <= 1e-5
+                assert abs(X[f, 6] - abs(uu) * 0.3) <= 1e-6 * max(1.0, abs(uu)) and X[f, 7] == 0 and U[f] == uu
+                f += 1
+
+
+def test_closure_in_the_step(cm1g):
+    """With the closure on, theta's horizontal faces come from the MLP where
+    they stay inside the bounds of the two neighbouring cells; the step stays
+    finite and close to the plain step; turning it off restores the plain step
+    bit for bit."""
+    torch = _torch()
+    case = make_case("dry_bubble", ni=40, nj=32, nk=24, advwenos=1)
+    ctx = cm1g.Context(case.cfg, case.grid)
+    plain = cm1g.to_device(case.state)
+    learned = cm1g.to_device(case.state)
+    again = cm1g.to_device(case.state)
+    ctx.step(plain, case.dt, case.mass1)
+    p = R.init_params(0)
+    ctx.closure(torch.from_numpy(p).cuda())
+    m2, cfl = ctx.step(learned, case.dt, case.mass1)
+    assert np.isfinite(m2) and np.isfinite(cfl)
+    ctx.closure(None, enable=False)
+    ctx.step(again, case.dt, case.mass1)
+    torch.cuda.synchronize()
+    for k in plain:
+        assert torch.equal(plain[k], again[k]), k
+    th_p, th_l = plain["th3d"].cpu().numpy(), learned["th3d"].cpu().numpy()
+    sl = case.lay.interior(1)
+    rng_ = float(th_p[sl].max() - th_p[sl].min())
+    diff = float(np.abs(th_l[sl] - th_p[sl]).max())
+    assert 0.0 < diff <= 0.05 * rng_
