@@ -140,12 +140,31 @@ def run_reference(args):
     return 0
 
 
+def _shapes(tune, binding):
+    """The launch shapes used (autotuner's choice, or the defaults)."""
+    if tune is None:
+        return {"autotuned": False}
+    tab = binding.tile_shapes()
+    forms = {0: "tile 32 columns x 8 warps", 1: "tile 32 columns x 4 warps", 2: "column sweep 32x4",
+             3: "column sweep 32x2"}
+    return {"autotuned": True, "scalar_tile_xyz": tab[tune["adv_shape"]], "momentum_tile_xyz": tab[tune["mom_shape"]],
+            "acoustic": forms.get(tune["sound_form"], tune["sound_form"]), "tuned_step_ms": tune["step_ms"]}
+
+
 def workload_config(case, args):
     c = case.cfg
     return {"workload": args.workload, "grid": [c.ni, c.nj, c.nk], "dx_m": c.dx, "dz_m": c.dz, "dt_s": case.dt,
             "nsound": c.nsound, "advwenos": c.advwenos, "moist": bool(c.imoist), "passive_tracers": c.npt if c.iptra else 0,
             "lateral_bc": {1: "periodic", 2: "open-radiative"}[c.wbc], "l2": "inputs larger than L2 (no flush needed)",
             "parallelism": "replicas" if args.gpus > 1 else "single"}
+
+
+def _tally(tunes):
+    out = {}
+    for t in tunes:
+        k = (t["adv_shape"], t["mom_shape"], t["sound_form"])
+        out[k] = out.get(k, 0) + 1
+    return out
 
 
 def run_ensemble(args):
@@ -161,6 +180,12 @@ def run_ensemble(args):
     cells = sum(c.cfg.ni * c.cfg.nj * c.cfg.nk for c in members)
     ctxs = [binding.Context(c.cfg, c.grid) for c in members]
     dev = [binding.to_device(c.state) for c in members]
+    # launch shapes per member grid from the autotuner (each member timed
+    # alone; members of the same grid share the cached choice)
+    tunes = []
+    if not args.no_tune:
+        for ctx, st, c in zip(ctxs, dev, members):
+            tunes.append(ctx.autotune(st, c.dt, c.mass1, reps=3))
     ens = binding.Ensemble(ctxs)
     dts, m1 = [c.dt for c in members], [c.mass1 for c in members]
     for _ in range(args.warmup):
@@ -199,6 +224,8 @@ def run_ensemble(args):
                        "grids": sorted({(c.cfg.ni, c.cfg.nj, c.cfg.nk) for c in members}),
                        "dt_s": members[0].dt, "nsound": members[0].cfg.nsound, "advwenos": 1,
                        "timing": "host clock around synchronised steps",
+                       "tuned_members": len(tunes),
+                       "tune_choices": {str(k): v for k, v in _tally(tunes).items()},
                        "l2": "all members together exceed L2 (no flush needed)"},
             "step_roofline": {"algorithmic_bytes_per_cell": B, "achieved_gbs": B * value / 1e9,
                               "frac": B * value / 1e9 / hbm, "peak": hbm, "peak_kind": peak_kind},
@@ -224,6 +251,7 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=3)
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of the autotuner's")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -252,6 +280,8 @@ def main():
     ctx.set_stream(stream.cuda_stream)
     dev = binding.to_device(case.state)
     torch.cuda.synchronize()
+    # ---- launch shapes for this grid (timed on a copy of the state, untimed here)
+    tune = None if args.no_tune else ctx.autotune(dev, case.dt, case.mass1, reps=3)
 
     # ---- device-resident throughput (graph replay)
     with torch.cuda.stream(stream):
@@ -337,7 +367,8 @@ def main():
         line = {"metric": "cell-updates/s per RK3 large step", "value": value, "unit": "cell-updates/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic (seeded, generated in-repo)", "config": workload_config(case, args),
+                "data": "synthetic (seeded, generated in-repo)",
+                "config": dict(workload_config(case, args), launch_shapes=_shapes(tune, binding)),
                 "roofline": {"bound": "hbm", "kernel": "k_sound_step", "achieved": achieved, "peak": hbm,
                              "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                              "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": per_launch_ms,

@@ -57,6 +57,12 @@ STATE_FIELDS = ["ua", "u3d", "uten1", "va", "v3d", "vten1", "wa", "w3d", "wten1"
                 "radbcw", "radbce", "radbcs", "radbcn"]
 
 
+class Tune(C.Structure):
+    """cm1g_tune_t: launch shapes of the large step."""
+    _fields_ = [("adv_shape", C.c_int32), ("mom_shape", C.c_int32), ("sound_form", C.c_int32),
+                ("step_ms", C.c_float)]
+
+
 class State(C.Structure):
     """cm1g_state_t: prognostic state and pre-RK tendencies."""
     _fields_ = [(n, _P) for n in STATE_FIELDS]

@@ -10,7 +10,7 @@ import os
 
 import numpy as np
 
-from .abi import Config, Grid, State, STATE_FIELDS, fptr, CM1G_OK
+from .abi import Config, Grid, State, Tune, STATE_FIELDS, fptr, CM1G_OK
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libcm1g.so")
@@ -79,9 +79,15 @@ def lib():
     L.cm1g_face_features.argtypes = [C.c_int32] * 5 + [_P, _P, C.c_int32, _P, C.c_float, _P, _P, _P, _P,
                                                          C.c_void_p]
     L.cm1g_face_phi.argtypes = [C.c_int64, _P, _P, _P, _P, _P, C.c_void_p]
+    L.cm1g_closure_faces.argtypes = [C.c_int32] * 5 + [_P, _P, C.c_int32, _P, C.c_float, _P, _P, C.c_void_p]
     L.cm1g_closure_set.argtypes = [ctxp, _P, C.c_int32]
     L.cm1g_capture_fluxes.argtypes = [ctxp, _P, _P, _P, _P]
     L.cm1g_pdefq_noalloc.argtypes = [cfgp, C.c_float, C.POINTER(C.c_double), _P, _P, _P, _P, _P, C.c_void_p]
+    tunep = C.POINTER(Tune)
+    L.cm1g_tile_shape.argtypes = [C.c_int32, C.POINTER(C.c_int32)]
+    L.cm1g_set_tune.argtypes = [ctxp, tunep]
+    L.cm1g_get_tune.argtypes = [ctxp, tunep]
+    L.cm1g_autotune.argtypes = [ctxp, C.c_float, C.c_double, stp, C.c_int32, C.c_char_p, tunep]
     _lib = L
     return L
 
@@ -216,6 +222,26 @@ class Context:
     def capture_fluxes(self, fx=None, fy=None, rx=None, ry=None):
         check(lib().cm1g_capture_fluxes(self.h, ptr(fx), ptr(fy), ptr(rx), ptr(ry)))
 
+    def get_tune(self):
+        """The context's launch shapes: dict of adv_shape, mom_shape, sound_form, step_ms."""
+        t = Tune()
+        check(lib().cm1g_get_tune(self.h, C.byref(t)))
+        return {n: getattr(t, n) for n, _ in Tune._fields_}
+
+    def set_tune(self, adv_shape=0, mom_shape=0, sound_form=-1, step_ms=0.0):
+        t = Tune(adv_shape, mom_shape, sound_form, step_ms)
+        check(lib().cm1g_set_tune(self.h, C.byref(t)))
+
+    def autotune(self, state, dt, mass1, reps=3, cache=None):
+        """Times the candidate launch shapes on a copy of `state` and keeps
+        the fastest (cm1g_autotune); `cache` names a text file of results
+        per grid shape.  Returns get_tune()."""
+        s = state if isinstance(state, State) else self.state_struct(state)
+        t = Tune()
+        check(lib().cm1g_autotune(self.h, dt, mass1, C.byref(s), reps,
+                                  None if cache is None else os.fsencode(cache), C.byref(t)))
+        return {n: getattr(t, n) for n, _ in Tune._fields_}
+
     def profile(self, enable):
         check(lib().cm1g_profile(self.h, 1 if enable else 0))
 
@@ -269,6 +295,16 @@ class Ensemble:
             self.close()
         except Exception:
             pass
+
+
+def tile_shapes():
+    """The tile-shape table of the scalar and momentum passes: list of (x, y, levels)."""
+    out, i = [], 0
+    a = (C.c_int32 * 3)()
+    while lib().cm1g_tile_shape(i, a) == CM1G_OK:
+        out.append(tuple(a))
+        i += 1
+    return out
 
 
 def dtsmall(psolver, nx, ny, min_dx, min_dy, min_dz, dt, adapt_dt=0):

@@ -20,15 +20,30 @@ def nvcc():
 
 
 def build(verbose=False, extra=()):
+    """Compiles each source to an object in parallel (in _build/ beside the
+    sources), then links libcm1g.so."""
     srcs = [os.path.join(HERE, "csrc", s) for s in SRC]
     newest = max(os.path.getmtime(s) for s in srcs + [os.path.join(HERE, "csrc", "cm1g_common.cuh"),
                                                        os.path.join(HERE, "..", "include", "cm1g.h")])
     if os.path.exists(LIB) and os.path.getmtime(LIB) >= newest and not extra:
         return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + list(extra) + ["-o", LIB] + srcs
     host = "/usr/bin/g++"
-    if os.path.exists(host):
-        cmd[1:1] = ["-ccbin", host]
+    base = [nvcc()] + (["-ccbin", host] if os.path.exists(host) else [])
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"] + list(extra)
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs, procs = [], []
+    for src in srcs:
+        obj = os.path.join(objdir, os.path.splitext(os.path.basename(src))[0] + ".o")
+        cmd = base + compile_flags + ["-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd))
+        procs.append((src, subprocess.Popen(cmd)))
+        objs.append(obj)
+    failed = [src for src, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, "nvcc " + " ".join(os.path.basename(f) for f in failed))
+    cmd = base + ["-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB] + objs
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

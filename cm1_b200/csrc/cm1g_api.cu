@@ -12,6 +12,8 @@
 #include <cmath>
 #include <vector>
 #include <string>
+#include <map>
+#include <mutex>
 #include "cm1g_common.cuh"
 #include "../../include/cm1g.h"
 
@@ -20,12 +22,8 @@ void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, 
 void launch_bc_batch(const DGrid &g, float *const *arrays, const int *which, const int *wflag, int n,
                      cudaStream_t st, int64_t *nlaunch);
 void launch_tend_init(const DGrid &g, const TendIn &t, cudaStream_t st, int64_t *nl);
-void launch_mlp_forward(const float *params, int n, const float *x, float *y, float *c, float *z1, float *z2,
-                        cudaStream_t st);
-void launch_face_features(int ni, int nj, int nk, int ngxy, int dir, const float *s, const float *th0, int sadd,
-                          const float *vel, float dtdx, float *x, float *m, float *d, float *u, cudaStream_t st);
-void launch_face_phi(long nf, const float *x, const float *c, const float *m, const float *d, float *phi,
-                     cudaStream_t st);
+void launch_closure_faces(int ni, int nj, int nk, int ngxy, int dir, const float *s, const float *th0, int sadd,
+                          const float *vel, float dtdx, const float *params, float *phi, cudaStream_t st);
 int mlp_param_count();
 int ener_chunks(const DGrid &g);
 void launch_calcener(const DGrid &g, const EnerIn &e, double *part, double *out, cudaStream_t st, int64_t *nl);
@@ -149,7 +147,7 @@ struct cm1g_ctx {
   // learned closure of theta's horizontal faces (cm1g_closure_set)
   bool cl_on = false;
   float *cl_params = nullptr;
-  float *cl_x[2] = {}, *cl_m[2] = {}, *cl_d[2] = {}, *cl_u[2] = {}, *cl_c[2] = {}, *cl_phi[2] = {};
+  float *cl_phi[2] = {};
   long cl_nf[2] = {0, 0};
   // capture of theta's final-stage face fluxes (cm1g_capture_fluxes)
   float *cap_fx = nullptr, *cap_fy = nullptr, *cap_rx = nullptr, *cap_ry = nullptr;
@@ -169,6 +167,8 @@ struct cm1g_ctx {
   float gdt = 0.f;
   double gmass1 = 0.0;
   int64_t graph_nodes = 0;
+  uint64_t gen = 0;                           // bumped when launch shapes or the closure change
+  float tuned_ms = 0.0f;                      // measured step time of the launch shapes (autotune)
   Profile *prof = nullptr;
 };
 
@@ -279,6 +279,7 @@ extern "C" int cm1g_init(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_c
   g.wbc = cfg->wbc; g.ebc = cfg->ebc; g.sbc = cfg->sbc; g.nbc = cfg->nbc;
   g.ibw = cfg->wbc != 1; g.ibe = cfg->ebc != 1; g.ibs = cfg->sbc != 1; g.ibn = cfg->nbc != 1;
   g.smeps = cfg->smeps; g.alph = cfg->alph; g.kdiv = cfg->kdiv;
+  g.tile_adv = 0; g.tile_mom = 0; g.sound_cfg = -1;
   set_constants_(cfg->testcase, &g.c);
 
   // vertical profiles from the 3-D base state
@@ -470,11 +471,10 @@ static int check_state(const cm1g_ctx *c, const cm1g_state_t *st) {
 static void closure_phi(cm1g_ctx *c, const float *th, float dt, cudaStream_t st, int64_t *nl) {
   const DGrid &g = c->g;
   for (int dir = 0; dir < 2; dir++) {
-    launch_face_features(g.ni, g.nj, g.nk, g.ngxy, dir, th, g.th0, 1, dir ? c->rrv : c->rru,
-                         dt * (dir ? g.rdy : g.rdx), c->cl_x[dir], c->cl_m[dir], c->cl_d[dir], c->cl_u[dir], st);
-    launch_mlp_forward(c->cl_params, (int)c->cl_nf[dir], c->cl_x[dir], nullptr, c->cl_c[dir], nullptr, nullptr, st);
-    launch_face_phi(c->cl_nf[dir], c->cl_x[dir], c->cl_c[dir], c->cl_m[dir], c->cl_d[dir], c->cl_phi[dir], st);
-    if (nl) *nl += 3;
+    ProfScope _ps("k_closure_faces", st);
+    launch_closure_faces(g.ni, g.nj, g.nk, g.ngxy, dir, th, g.th0, 1, dir ? c->rrv : c->rru,
+                         dt * (dir ? g.rdy : g.rdx), c->cl_params, c->cl_phi[dir], st);
+    if (nl) *nl += 1;
   }
 }
 
@@ -638,6 +638,28 @@ static int fetch_scalars(cm1g_ctx *c, double *mass2, float *cflmax) {
   return CM1G_OK;
 }
 
+// One large step as a CUDA graph: captured on first use (and again when the
+// state arrays, dt or mass1 change), then replayed with one launch.
+static int graph_step(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass1) {
+  bool same = c->gexec && memcmp(&c->gstate, d, sizeof *d) == 0 && c->gdt == dt && c->gmass1 == mass1;
+  if (!same) {
+    drop_graph(c);
+    int64_t before = c->nlaunch;
+    CUCHK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    run_step(c, d, dt, mass1);
+    cudaGraph_t gr;
+    CUCHK(cudaStreamEndCapture(c->stream, &gr));
+    c->graph = gr;
+    CUCHK(cudaGraphInstantiate(&c->gexec, gr, 0));
+    c->graph_nodes = c->nlaunch - before;
+    c->nlaunch = before;
+    c->gstate = *d; c->gdt = dt; c->gmass1 = mass1;
+  }
+  CUCHK(cudaGraphLaunch(c->gexec, c->stream));
+  c->nlaunch += c->graph_nodes;
+  return CM1G_OK;
+}
+
 static int solve_common(cm1g_ctx_t *c, float dt, double mass1, double *mass2, float *cflmax, cm1g_state_t *st,
                         int which, int use_graph) {
   if (!c) return set_err(CM1G_ERR_STATE, "null context");
@@ -653,22 +675,8 @@ static int solve_common(cm1g_ctx_t *c, float dt, double mass1, double *mass2, fl
   bool all_device = S.items.empty();
   ProfActive pa(c);
   if (use_graph && all_device && which == 3 && !c->prof) {
-    bool same = c->gexec && memcmp(&c->gstate, &d, sizeof d) == 0 && c->gdt == dt && c->gmass1 == mass1;
-    if (!same) {
-      drop_graph(c);
-      int64_t before = c->nlaunch;
-      CUCHK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      run_step(c, &d, dt, mass1);
-      cudaGraph_t gr;
-      CUCHK(cudaStreamEndCapture(c->stream, &gr));
-      c->graph = gr;
-      CUCHK(cudaGraphInstantiate(&c->gexec, gr, 0));
-      c->graph_nodes = c->nlaunch - before;
-      c->nlaunch = before;
-      c->gstate = d; c->gdt = dt; c->gmass1 = mass1;
-    }
-    CUCHK(cudaGraphLaunch(c->gexec, c->stream));
-    c->nlaunch += c->graph_nodes;
+    rc = graph_step(c, &d, dt, mass1);
+    if (rc) return rc;
   } else {
     if (which == 1) run_solve2(c, &d, dt, mass1);
     else if (which == 2) run_solve3(c, &d);
@@ -700,6 +708,224 @@ extern "C" int cm1g_step(cm1g_ctx_t *c, int32_t nstep, float dt, double mtime, d
 }
 
 // ---------------------------------------------------------------------
+// Launch shapes and the autotuner.  The choices live on the context's
+// DGrid (tile_adv, tile_mom, sound_cfg) and are read by the launchers when
+// a step is enqueued, so a change drops the captured graph.
+// ---------------------------------------------------------------------
+extern "C" int cm1g_tile_shape(int32_t index, int32_t shape[3]) {
+  if (!shape || index < 0 || index >= kNumTileShapes) return set_err(CM1G_ERR_ARG, "no tile shape %d", index);
+  for (int q = 0; q < 3; q++) shape[q] = kTileShapes[index][q];
+  return CM1G_OK;
+}
+
+static int apply_tune(cm1g_ctx *c, const cm1g_tune_t *t) {
+  if (t->adv_shape < 0 || t->adv_shape >= kNumTileShapes || t->mom_shape < 0 || t->mom_shape >= kNumTileShapes ||
+      t->sound_form < -1 || t->sound_form >= kNumSoundCfgs)
+    return set_err(CM1G_ERR_ARG, "launch shape out of range (%d %d %d)", t->adv_shape, t->mom_shape, t->sound_form);
+  if (c->g.tile_adv != t->adv_shape || c->g.tile_mom != t->mom_shape || c->g.sound_cfg != t->sound_form) {
+    drop_graph(c);
+    c->gen++;
+  }
+  c->g.tile_adv = t->adv_shape; c->g.tile_mom = t->mom_shape; c->g.sound_cfg = t->sound_form;
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_set_tune(cm1g_ctx_t *c, const cm1g_tune_t *t) {
+  if (!c || !t) return set_err(CM1G_ERR_ARG, "null argument");
+  int rc = apply_tune(c, t);
+  if (rc == CM1G_OK) c->tuned_ms = t->step_ms;
+  return rc;
+}
+
+extern "C" int cm1g_get_tune(cm1g_ctx_t *c, cm1g_tune_t *t) {
+  if (!c || !t) return set_err(CM1G_ERR_ARG, "null argument");
+  t->adv_shape = c->g.tile_adv; t->mom_shape = c->g.tile_mom; t->sound_form = c->g.sound_cfg;
+  t->step_ms = c->tuned_ms;
+  return CM1G_OK;
+}
+
+// The cache key: device, grid shape and the options that change which
+// kernels run (no spaces, so that a cache file line splits on blanks).
+static std::string tune_key(const cm1g_ctx *c) {
+  cudaDeviceProp prop;
+  char name[256] = "gpu";
+  int sms = 0;
+  if (cudaGetDeviceProperties(&prop, c->device) == cudaSuccess) {
+    snprintf(name, sizeof name, "%s", prop.name);
+    sms = prop.multiProcessorCount;
+  } else {
+    cudaGetLastError();
+  }
+  for (char *p = name; *p; p++) if (*p == ' ' || *p == '\t') *p = '_';
+  const cm1g_config_t &f = c->cfg;
+  char key[512];
+  snprintf(key, sizeof key, "%s/sm%d/%dx%dx%d/h%d/q%d/t%d/w%d/pd%d/ns%d/bc%d%d%d%d", name,
+           sms, f.ni, f.nj, f.nk, f.ngxy, f.imoist ? f.numq : 0,
+           f.iptra ? f.npt : 0, f.advwenos, f.pdtra, f.nsound, f.wbc, f.ebc, f.sbc, f.nbc);
+  return key;
+}
+
+static std::mutex g_tune_mu;
+static std::map<std::string, cm1g_tune_t> g_tune_cache;
+
+static bool tune_file_lookup(const char *path, const std::string &key, cm1g_tune_t *t) {
+  FILE *f = fopen(path, "r");
+  if (!f) return false;
+  char line[1024], k[600];
+  bool hit = false;
+  while (fgets(line, sizeof line, f)) {
+    cm1g_tune_t e{};
+    if (sscanf(line, "%599s %d %d %d %f", k, &e.adv_shape, &e.mom_shape, &e.sound_form, &e.step_ms) == 5 &&
+        key == k) {
+      *t = e;          // the last entry of a key wins
+      hit = true;
+    }
+  }
+  fclose(f);
+  return hit;
+}
+
+static void tune_file_append(const char *path, const std::string &key, const cm1g_tune_t &t) {
+  FILE *f = fopen(path, "a");
+  if (!f) return;
+  fprintf(f, "%s %d %d %d %.6f\n", key.c_str(), t.adv_shape, t.mom_shape, t.sound_form, t.step_ms);
+  fclose(f);
+}
+
+// Average time of `reps` graph replays of the large step on d with the
+// context's current launch shapes (after one untimed replay).
+static int time_steps(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass1, int reps, float *ms) {
+  drop_graph(c);
+  int rc = graph_step(c, d, dt, mass1);
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  CUCHK(cudaEventCreate(&e0));
+  CUCHK(cudaEventCreate(&e1));
+  cudaEventRecord(e0, c->stream);
+  for (int r = 0; r < reps; r++) {
+    cudaGraphLaunch(c->gexec, c->stream);
+    c->nlaunch += c->graph_nodes;
+  }
+  cudaEventRecord(e1, c->stream);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float t = 0.0f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "autotune timing: %s", cudaGetErrorString(e));
+  *ms = t / (float)reps;
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_autotune(cm1g_ctx_t *c, float dt, double mass1, const cm1g_state_t *st, int32_t reps,
+                             const char *cache_path, cm1g_tune_t *out) {
+  if (!c || !st) return set_err(CM1G_ERR_ARG, "null argument");
+  int rc = check_state(c, st);
+  if (rc) return rc;
+  if (!(dt > 0.0f) || !std::isfinite(dt)) return set_err(CM1G_ERR_ARG, "dt must be positive");
+  if (c->cfg.apmasscon == 1 && !(mass1 > 0.0)) return set_err(CM1G_ERR_ARG, "mass1 must be positive");
+  if (reps < 1) return set_err(CM1G_ERR_ARG, "reps must be at least 1");
+  const std::string key = tune_key(c);
+  cm1g_tune_t best{};
+  bool hit = false;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) { best = it->second; hit = true; }
+  }
+  if (!hit && cache_path) hit = tune_file_lookup(cache_path, key, &best);
+  if (hit) {
+    rc = apply_tune(c, &best);
+    if (rc) return rc;
+    c->tuned_ms = best.step_ms;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = best;
+    if (out) *out = best;
+    return CM1G_OK;
+  }
+
+  // scratch copy of the state (device or host source), so that the timed
+  // steps leave the caller's arrays as they were
+  const DGrid &g = c->g;
+  const size_t ns = nS(g), nu = nU(g), nv = nV(g), nw = nW(g);
+  const size_t nq = (c->cfg.imoist ? c->cfg.numq : 0) * ns, npt = (c->cfg.iptra ? c->cfg.npt : 0) * ns;
+  const size_t nrw = (size_t)g.NJ * g.NK, nrs = (size_t)g.NI * g.NK;
+  cm1g_state_t d = *st;
+  struct F { float **dst; size_t n; } fields[] = {
+      {&d.ua, nu}, {&d.u3d, nu}, {&d.uten1, nu}, {&d.va, nv}, {&d.v3d, nv}, {&d.vten1, nv},
+      {&d.wa, nw}, {&d.w3d, nw}, {&d.wten1, nw}, {&d.ppi, ns}, {&d.pp3d, ns}, {&d.ppx, ns}, {&d.ppten, ns},
+      {&d.tha, ns}, {&d.th3d, ns}, {&d.thten1, ns}, {&d.rho, ns}, {&d.prs, ns}, {&d.qa, nq}, {&d.q3d, nq},
+      {&d.qten, nq}, {&d.pta, npt}, {&d.pt3d, npt}, {&d.ptten, npt}, {&d.radbcw, nrw}, {&d.radbce, nrw},
+      {&d.radbcs, nrs}, {&d.radbcn, nrs}};
+  std::vector<void *> scratch;
+  auto release = [&]() {
+    cudaStreamSynchronize(c->stream);
+    for (void *p : scratch) cudaFree(p);
+  };
+  for (auto &f : fields) {
+    if (!*f.dst || f.n == 0) { *f.dst = nullptr; continue; }
+    void *p = nullptr;
+    if (cudaMalloc(&p, f.n * sizeof(float)) != cudaSuccess) {
+      cudaGetLastError();
+      release();
+      return set_err(CM1G_ERR_NOMEM, "autotune scratch state");
+    }
+    scratch.push_back(p);
+    if (cudaMemcpyAsync(p, *f.dst, f.n * sizeof(float), cudaMemcpyDefault, c->stream) != cudaSuccess) {
+      release();
+      return set_err(CM1G_ERR_CUDA, "autotune state copy: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    *f.dst = (float *)p;
+  }
+
+  const cm1g_tune_t saved{c->g.tile_adv, c->g.tile_mom, c->g.sound_cfg, c->tuned_ms};
+  cm1g_tune_t cur{0, 0, -1, 0.0f};
+  float best_ms = 0.0f;
+  auto trial = [&](const cm1g_tune_t &t, float *ms) -> int {
+    int r = apply_tune(c, &t);
+    if (r) return r;
+    return time_steps(c, &d, dt, mass1, reps, ms);
+  };
+  // acoustic form first (the largest single kernel), then the scalar tile,
+  // then the momentum tile, each with the others held at the best so far
+  const int ncand[3] = {kNumSoundCfgs, kNumTileShapes, kNumTileShapes};
+  for (int knob = 0; knob < 3 && rc == CM1G_OK; knob++) {
+    int best_v = knob == 0 ? 0 : knob == 1 ? cur.adv_shape : cur.mom_shape;
+    float knob_best = 0.0f;
+    for (int v = 0; v < ncand[knob] && rc == CM1G_OK; v++) {
+      cm1g_tune_t t = cur;
+      if (knob == 0) t.sound_form = v;
+      else if (knob == 1) t.adv_shape = v;
+      else t.mom_shape = v;
+      float ms = 0.0f;
+      rc = trial(t, &ms);
+      if (rc == CM1G_OK && (v == 0 || ms < knob_best)) { knob_best = ms; best_v = v; }
+    }
+    if (knob == 0) cur.sound_form = best_v;
+    else if (knob == 1) cur.adv_shape = best_v;
+    else cur.mom_shape = best_v;
+    best_ms = knob_best;
+  }
+  drop_graph(c);
+  release();
+  if (rc) {
+    apply_tune(c, &saved);
+    return rc;
+  }
+  cur.step_ms = best_ms;
+  rc = apply_tune(c, &cur);
+  if (rc) return rc;
+  c->tuned_ms = best_ms;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = cur;
+  }
+  if (cache_path) tune_file_append(cache_path, key, cur);
+  if (out) *out = cur;
+  return CM1G_OK;
+}
+
+// ---------------------------------------------------------------------
 // Ensembles of independent members (uneven grids).  Each member keeps its
 // own context and stream; one ensemble step forks from the ensemble's
 // stream onto every member's stream, runs each member's large step there,
@@ -718,6 +944,7 @@ struct cm1g_ens {
   std::vector<cm1g_state_t> gstate;
   std::vector<float> gdt;
   std::vector<double> gmass1;
+  std::vector<uint64_t> ggen;                 // the members' gen at capture
   int64_t graph_nodes = 0;
 };
 
@@ -790,6 +1017,7 @@ extern "C" int cm1g_ensemble_step(cm1g_ens_t *e, cm1g_state_t *states, const flo
     bool same = e->exec && e->gstate.size() == n &&
                 memcmp(e->gstate.data(), states, n * sizeof(cm1g_state_t)) == 0 &&
                 memcmp(e->gdt.data(), dt, n * sizeof(float)) == 0 && memcmp(e->gmass1.data(), mass1, n * sizeof(double)) == 0;
+    for (size_t q = 0; same && q < n; q++) same = e->ggen[q] == e->m[q]->gen;
     if (!same) {
       ens_drop_graph(e);
       int64_t before = 0;
@@ -806,6 +1034,8 @@ extern "C" int cm1g_ensemble_step(cm1g_ens_t *e, cm1g_state_t *states, const flo
       e->gstate.assign(states, states + n);
       e->gdt.assign(dt, dt + n);
       e->gmass1.assign(mass1, mass1 + n);
+      e->ggen.resize(n);
+      for (size_t q = 0; q < n; q++) e->ggen[q] = e->m[q]->gen;
     }
     CUCHK(cudaGraphLaunch(e->exec, e->stream));
   } else {
@@ -842,6 +1072,7 @@ extern "C" int cm1g_ensemble_launch_count(cm1g_ens_t *e, int64_t *count) {
 extern "C" int cm1g_closure_set(cm1g_ctx_t *c, const float *params, int32_t enable) {
   if (!c) return set_err(CM1G_ERR_STATE, "null context");
   drop_graph(c);
+  c->gen++;
   if (!enable) { c->cl_on = false; return CM1G_OK; }
   if (!params) return set_err(CM1G_ERR_ARG, "null parameters");
   const DGrid &g = c->g;
@@ -850,14 +1081,8 @@ extern "C" int cm1g_closure_set(cm1g_ctx_t *c, const float *params, int32_t enab
     for (int dir = 0; dir < 2; dir++) {
       const long nf = (long)(dir ? g.ni : g.ni + 1) * (dir ? g.nj + 1 : g.nj) * g.nk;
       c->cl_nf[dir] = nf;
-      c->cl_x[dir] = (float *)dalloc(c, nf * 8 * sizeof(float));
-      c->cl_c[dir] = (float *)dalloc(c, nf * 6 * sizeof(float));
-      c->cl_m[dir] = (float *)dalloc(c, nf * sizeof(float));
-      c->cl_d[dir] = (float *)dalloc(c, nf * sizeof(float));
-      c->cl_u[dir] = (float *)dalloc(c, nf * sizeof(float));
       c->cl_phi[dir] = (float *)dalloc(c, nf * sizeof(float));
-      if (!c->cl_x[dir] || !c->cl_c[dir] || !c->cl_m[dir] || !c->cl_d[dir] || !c->cl_u[dir] || !c->cl_phi[dir])
-        return set_err(CM1G_ERR_NOMEM, "closure buffers");
+      if (!c->cl_phi[dir]) return set_err(CM1G_ERR_NOMEM, "closure buffers");
     }
     if (!c->cl_params) return set_err(CM1G_ERR_NOMEM, "closure parameters");
   }
@@ -871,6 +1096,7 @@ extern "C" int cm1g_closure_set(cm1g_ctx_t *c, const float *params, int32_t enab
 extern "C" int cm1g_capture_fluxes(cm1g_ctx_t *c, float *fx, float *fy, float *rx, float *ry) {
   if (!c) return set_err(CM1G_ERR_STATE, "null context");
   drop_graph(c);
+  c->gen++;
   if (!fx && !fy && !rx && !ry) { c->cap_fx = c->cap_fy = c->cap_rx = c->cap_ry = nullptr; return CM1G_OK; }
   if (!fx || !fy || !rx || !ry) return set_err(CM1G_ERR_ARG, "give all four capture arrays or none");
   for (const float *p : {fx, fy, rx, ry})

@@ -32,7 +32,21 @@ struct DGrid {
   const float *uh, *ruh, *uf, *ruf, *vh, *rvh, *vf, *rvf;
   const float *dtu0, *dtv0;   // (ib:ie, jb:je)
   const float *u0, *v0;       // base-state winds, full u-/v-arrays (Rayleigh damping)
+  // launch shapes (cm1g_set_tune / cm1g_autotune): index into the tile-shape
+  // table of the scalar and momentum passes, and the acoustic kernel's form
+  // (-1: chosen by the number of columns)
+  int tile_adv, tile_mom, sound_cfg;
 };
+
+// Tile shapes of the scalar and momentum passes: x and y extent of a block
+// (threads) and the levels one block marches through (z).  Entry 0 is the
+// default; the others are the autotuner's candidates.
+constexpr int kNumTileShapes = 5;
+constexpr int kTileShapes[kNumTileShapes][3] = {{32, 8, 16}, {32, 8, 8}, {32, 4, 16}, {64, 4, 16}, {32, 8, 32}};
+// Forms of the acoustic kernel: 0 tile (32 columns x 8 warps over the
+// levels), 1 tile with 4 warps, 2 column sweep 32 x 4 columns, 3 column
+// sweep 32 x 2 columns.
+constexpr int kNumSoundCfgs = 4;
 
 // Fortran-layout offsets.  s and w arrays share the plane (NI*NJ); u arrays
 // have NI+1 points in x, v arrays NJ+1 rows.

@@ -642,7 +642,28 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
   }
 }
 
-static const int MOM_TX = 32, MOM_TY = 8, MOM_KC = 16;
+template <int TX, int TY, int KC>
+static void mom_tiles_shape(const DGrid &g, const Vel &q, const float *uten1, const float *vten1,
+                            const float *wten1, float *uten, float *vten, float *wten, const float *th3d,
+                            const float *qv, const float *divx, cudaStream_t st) {
+  dim3 blk(TX, TY);
+  const int kch = (g.nk + KC - 1) / KC, kchw = (g.nk - 1 + KC - 1) / KC;
+  {
+    dim3 grid((g.ni + 1 + TX - 1) / TX, (g.nj + TY - 1) / TY, kch);
+    ProfScope _ps("k_advu", st);
+    k_mom_tile<TX, TY, KC, 2><<<grid, blk, 0, st>>>(g, q, divx, uten1, uten, nullptr, nullptr);
+  }
+  {
+    dim3 grid((g.ni + TX - 1) / TX, (g.nj + 1 + TY - 1) / TY, kch);
+    ProfScope _ps("k_advv", st);
+    k_mom_tile<TX, TY, KC, 3><<<grid, blk, 0, st>>>(g, q, divx, vten1, vten, nullptr, nullptr);
+  }
+  {
+    dim3 grid((g.ni + TX - 1) / TX, (g.nj + TY - 1) / TY, kchw);
+    ProfScope _ps("k_advw", st);
+    k_mom_tile<TX, TY, KC, 4><<<grid, blk, 0, st>>>(g, q, divx, wten1, wten, th3d, qv);
+  }
+}
 
 void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w,
                          const float *uten1, const float *vten1, const float *wten1,
@@ -654,23 +675,19 @@ void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const f
     ProfScope _ps("k_mom_divx", st);
     k_mom_divx<<<grid, 128, 0, st>>>(g, q, divx);
   }
-  dim3 blk(MOM_TX, MOM_TY);
-  const int kch = (g.nk + MOM_KC - 1) / MOM_KC, kchw = (g.nk - 1 + MOM_KC - 1) / MOM_KC;
-  {
-    dim3 grid((g.ni + 1 + MOM_TX - 1) / MOM_TX, (g.nj + MOM_TY - 1) / MOM_TY, kch);
-    ProfScope _ps("k_advu", st);
-    k_mom_tile<MOM_TX, MOM_TY, MOM_KC, 2><<<grid, blk, 0, st>>>(g, q, divx, uten1, uten, nullptr, nullptr);
+#define CM1G_MOM_SHAPE(n)                                                                                     \
+  case n:                                                                                                     \
+    mom_tiles_shape<kTileShapes[n][0], kTileShapes[n][1], kTileShapes[n][2]>(g, q, uten1, vten1, wten1, uten, \
+                                                                             vten, wten, th3d, qv, divx, st); \
+    break;
+  switch (g.tile_mom) {
+    CM1G_MOM_SHAPE(1)
+    CM1G_MOM_SHAPE(2)
+    CM1G_MOM_SHAPE(3)
+    CM1G_MOM_SHAPE(4)
+    default: CM1G_MOM_SHAPE(0)
   }
-  {
-    dim3 grid((g.ni + MOM_TX - 1) / MOM_TX, (g.nj + 1 + MOM_TY - 1) / MOM_TY, kch);
-    ProfScope _ps("k_advv", st);
-    k_mom_tile<MOM_TX, MOM_TY, MOM_KC, 3><<<grid, blk, 0, st>>>(g, q, divx, vten1, vten, nullptr, nullptr);
-  }
-  {
-    dim3 grid((g.ni + MOM_TX - 1) / MOM_TX, (g.nj + MOM_TY - 1) / MOM_TY, kchw);
-    ProfScope _ps("k_advw", st);
-    k_mom_tile<MOM_TX, MOM_TY, MOM_KC, 4><<<grid, blk, 0, st>>>(g, q, divx, wten1, wten, th3d, qv);
-  }
+#undef CM1G_MOM_SHAPE
   if (nl) *nl += 4;
 }
 
@@ -1405,23 +1422,16 @@ void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, 
 void launch_bc_batch(const DGrid &g, float *const *arrays, const int *which, const int *wflag, int n,
                      cudaStream_t st, int64_t *nlaunch);
 
-static const int ADV_TX = 32, ADV_TY = 8, ADV_KC = 16;
-
-// Production scalar pass (MODE_UPDATE, or the pdef two-pass form).
-void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const float *rrw, const float *s,
-                       const float *s0, int sadd, const float *ten1, const float *thterm, float *snew, int weno,
-                       int pdef, int pdefweno, double weps, float dt, int flush, float *scratch, cudaStream_t st,
-                       int64_t *nl, const TileExtras *ex) {
-  SAdv a{rru, rrv, rrw, s, s0, nullptr, thterm, 1, sadd};
-  dim3 blk(ADV_TX, ADV_TY),
-      grid((g.ni + ADV_TX - 1) / ADV_TX, (g.nj + ADV_TY - 1) / ADV_TY, (g.nk + ADV_KC - 1) / ADV_KC);
-  STileOut o{};
-  o.sten_in = ten1; o.sbase = s0; o.snew = snew;
-  if (ex) o.ex = *ex;
+// Production scalar pass (MODE_UPDATE, or the pdef two-pass form) with the
+// tile shape TX x TY x KC.
+template <int TX, int TY, int KC>
+static void advs_tiled_shape(const DGrid &g, const SAdv &a, STileOut o, int weno, int pdef, int pdefweno,
+                             double weps, float dt, int flush, float *scratch, cudaStream_t st, int64_t *nl) {
+  dim3 blk(TX, TY), grid((g.ni + TX - 1) / TX, (g.nj + TY - 1) / TY, (g.nk + KC - 1) / KC);
   if (!pdef) {
     ProfScope _ps("k_advs_tile", st);
-    if (weno) k_advs_tile<ADV_TX, ADV_TY, ADV_KC, MODE_UPDATE, 1><<<grid, blk, 0, st>>>(g, a, o, 0, pdefweno, weps, dt, flush);
-    else k_advs_tile<ADV_TX, ADV_TY, ADV_KC, MODE_UPDATE, 0><<<grid, blk, 0, st>>>(g, a, o, 0, pdefweno, weps, dt, flush);
+    if (weno) k_advs_tile<TX, TY, KC, MODE_UPDATE, 1><<<grid, blk, 0, st>>>(g, a, o, 0, pdefweno, weps, dt, flush);
+    else k_advs_tile<TX, TY, KC, MODE_UPDATE, 0><<<grid, blk, 0, st>>>(g, a, o, 0, pdefweno, weps, dt, flush);
     if (nl) *nl += 1;
     return;
   }
@@ -1430,8 +1440,8 @@ void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const
   o.dumx = scratch + 3 * n; o.dumy = scratch + 4 * n; o.dumz = scratch + 5 * n;
   {
     ProfScope _ps("k_advs_tile_pdef1", st);
-    if (weno) k_advs_tile<ADV_TX, ADV_TY, ADV_KC, MODE_PDEF1, 1><<<grid, blk, 0, st>>>(g, a, o, 1, pdefweno, weps, dt, flush);
-    else k_advs_tile<ADV_TX, ADV_TY, ADV_KC, MODE_PDEF1, 0><<<grid, blk, 0, st>>>(g, a, o, 1, pdefweno, weps, dt, flush);
+    if (weno) k_advs_tile<TX, TY, KC, MODE_PDEF1, 1><<<grid, blk, 0, st>>>(g, a, o, 1, pdefweno, weps, dt, flush);
+    else k_advs_tile<TX, TY, KC, MODE_PDEF1, 0><<<grid, blk, 0, st>>>(g, a, o, 1, pdefweno, weps, dt, flush);
   }
   {
     float *arr[2] = {o.dumx, o.dumy};
@@ -1440,10 +1450,34 @@ void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const
   }
   {
     ProfScope _ps("k_advs_pdef2", st);
-    k_advs_pdef2_tile<ADV_TX, ADV_TY, ADV_KC><<<grid, blk, 0, st>>>(g, a, o.advx, o.advy, o.advz, o.dumx, o.dumy,
-                                                                  o.dumz, ten1, snew, s0, dt, flush);
+    k_advs_pdef2_tile<TX, TY, KC><<<grid, blk, 0, st>>>(g, a, o.advx, o.advy, o.advz, o.dumx, o.dumy, o.dumz,
+                                                       o.sten_in, o.snew, o.sbase, dt, flush);
   }
   if (nl) *nl += 2;
+}
+
+void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const float *rrw, const float *s,
+                       const float *s0, int sadd, const float *ten1, const float *thterm, float *snew, int weno,
+                       int pdef, int pdefweno, double weps, float dt, int flush, float *scratch, cudaStream_t st,
+                       int64_t *nl, const TileExtras *ex) {
+  SAdv a{rru, rrv, rrw, s, s0, nullptr, thterm, 1, sadd};
+  STileOut o{};
+  o.sten_in = ten1; o.sbase = s0; o.snew = snew;
+  if (ex) o.ex = *ex;
+  static_assert(kNumTileShapes == 5, "one case per tile shape");
+#define CM1G_ADVS_SHAPE(n)                                                                                      \
+  case n:                                                                                                      \
+    advs_tiled_shape<kTileShapes[n][0], kTileShapes[n][1], kTileShapes[n][2]>(g, a, o, weno, pdef, pdefweno,    \
+                                                                              weps, dt, flush, scratch, st, nl); \
+    break;
+  switch (g.tile_adv) {
+    CM1G_ADVS_SHAPE(1)
+    CM1G_ADVS_SHAPE(2)
+    CM1G_ADVS_SHAPE(3)
+    CM1G_ADVS_SHAPE(4)
+    default: CM1G_ADVS_SHAPE(0)
+  }
+#undef CM1G_ADVS_SHAPE
 }
 
 // One advs call + RK update.  s = field (full halo), s0 = RK base,

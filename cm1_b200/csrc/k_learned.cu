@@ -1,12 +1,14 @@
 // k_learned.cu -- learned coarse-grid advection closure.
 //
-// A small MLP (7 inputs -> 64 -> 64 -> 6, GELU, BF16 weights, FP32
+// A small MLP (7 inputs -> 64 -> 64 -> 6, ReLU, BF16 weights, FP32
 // accumulation) predicts, for one horizontal face of a coarse grid, the six
 // coefficients of a linear reconstruction of the advected scalar from the
 // face's six-point upwind-ordered stencil.  The coefficients are projected
 // to sum to 1, so the face value phi = sum_k c_k s_k reproduces constants;
-// where phi leaves the range of the two cells that share the face, the
-// scalar kernel falls back to the WENO5 face value.
+// where phi leaves the range of the four stencil cells nearest the face
+// (two on each side), the scalar kernel falls back to the WENO5 face value:
+// the face value then creates no new extremum in its neighbourhood, and a
+// positive field stays positive.
 //
 // Features of a face (k_face_features): the stencil s_1..s_6 ordered from
 // the far upwind cell to the far downwind cell, normalised as
@@ -21,6 +23,7 @@
 // the three layers as warp-level tensor-core MMAs (mma.sync m16n8k16,
 // BF16 x BF16 -> FP32); the backward kernel uses the same BF16-rounded
 // operands so its gradient is the gradient of the computed forward.
+#include <algorithm>
 #include <cstdint>
 #include <cuda_bf16.h>
 #include "cm1g_common.cuh"
@@ -31,11 +34,10 @@ constexpr int MLP_IN = 8, MLP_H = 64, MLP_OUT = 8, MLP_NC = 6;
 constexpr int P_W1 = 0, P_B1 = P_W1 + MLP_IN * MLP_H, P_W2 = P_B1 + MLP_H, P_B2 = P_W2 + MLP_H * MLP_H;
 constexpr int P_W3 = P_B2 + MLP_H, P_B3 = P_W3 + MLP_H * MLP_OUT, P_TOTAL = P_B3 + MLP_OUT;
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678f)); }
-__device__ __forceinline__ float gelu_grad(float z) {
-  // d/dz [0.5 z (1 + erf(z/sqrt2))] = 0.5 (1 + erf(z/sqrt2)) + z * exp(-z^2/2) / sqrt(2 pi)
-  return 0.5f * (1.0f + erff(z * 0.70710678f)) + z * expf(-0.5f * z * z) * 0.39894228f;
-}
+// ReLU: one instruction per activation, exact on the host and the device
+// (a GELU's erf cost more than the three MMA layers together)
+__device__ __forceinline__ float act(float z) { return fmaxf(z, 0.0f); }
+__device__ __forceinline__ float act_grad(float z) { return z > 0.0f ? 1.0f : 0.0f; }
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
@@ -86,6 +88,85 @@ __device__ __forceinline__ void bfrag(const __nv_bfloat16 (*wt)[KS], int n0, int
   b1 = *reinterpret_cast<const uint32_t *>(&wt[n0 + g][k0 + 2 * t + 8]);
 }
 
+// The three layers for the 16 rows of one warp.  a: the layer-1 A
+// fragment (rows g and g+8 of the tile, inputs 2t, 2t+1).  On return d holds
+// the outputs before the projection (row g: columns 2t, 2t+1 in d[0..1];
+// row g+8 in d[2..3]; zero for t = 3, the unused columns 6 and 7) and ca/cb
+// the projection's shift (1 - sum y)/6 of rows g and g+8.  z1/z2 (may be
+// null) receive the pre-activations of rows ra, rb (< n).
+__device__ __forceinline__ void mlp_tile(const MlpSmem &S, const uint32_t a[4], int ra, int rb, int n, float *z1,
+                                         float *z2, float d[4], float &ca, float &cb) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  (void)g;
+  float h[8][4];
+#pragma unroll
+  for (int nt = 0; nt < 8; nt++) {
+    float e[4] = {0.f, 0.f, 0.f, 0.f};
+    uint32_t b0, b1;
+    bfrag<16>(S.w1t, nt * 8, 0, lane >> 2, t, b0, b1);
+    mma_bf16(e, a, b0, b1);
+    const int c0 = nt * 8 + 2 * t;
+    e[0] += S.b1[c0]; e[1] += S.b1[c0 + 1]; e[2] += S.b1[c0]; e[3] += S.b1[c0 + 1];
+    if (z1) {
+      if (ra < n) { z1[(long)ra * MLP_H + c0] = e[0]; z1[(long)ra * MLP_H + c0 + 1] = e[1]; }
+      if (rb < n) { z1[(long)rb * MLP_H + c0] = e[2]; z1[(long)rb * MLP_H + c0 + 1] = e[3]; }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) h[nt][q] = act(e[q]);
+  }
+  // layer 2: the accumulator tiles of layer 1 are the A fragments of layer 2
+  uint32_t A[4][4];
+#pragma unroll
+  for (int kt = 0; kt < 4; kt++) {
+    A[kt][0] = pack_bf16(h[2 * kt][0], h[2 * kt][1]);
+    A[kt][1] = pack_bf16(h[2 * kt][2], h[2 * kt][3]);
+    A[kt][2] = pack_bf16(h[2 * kt + 1][0], h[2 * kt + 1][1]);
+    A[kt][3] = pack_bf16(h[2 * kt + 1][2], h[2 * kt + 1][3]);
+  }
+#pragma unroll
+  for (int nt = 0; nt < 8; nt++) {
+    float e[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int kt = 0; kt < 4; kt++) {
+      uint32_t b0, b1;
+      bfrag<MLP_H>(S.w2t, nt * 8, kt * 16, lane >> 2, t, b0, b1);
+      mma_bf16(e, A[kt], b0, b1);
+    }
+    const int c0 = nt * 8 + 2 * t;
+    e[0] += S.b2[c0]; e[1] += S.b2[c0 + 1]; e[2] += S.b2[c0]; e[3] += S.b2[c0 + 1];
+    if (z2) {
+      if (ra < n) { z2[(long)ra * MLP_H + c0] = e[0]; z2[(long)ra * MLP_H + c0 + 1] = e[1]; }
+      if (rb < n) { z2[(long)rb * MLP_H + c0] = e[2]; z2[(long)rb * MLP_H + c0 + 1] = e[3]; }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) h[nt][q] = act(e[q]);
+  }
+#pragma unroll
+  for (int kt = 0; kt < 4; kt++) {
+    A[kt][0] = pack_bf16(h[2 * kt][0], h[2 * kt][1]);
+    A[kt][1] = pack_bf16(h[2 * kt][2], h[2 * kt][3]);
+    A[kt][2] = pack_bf16(h[2 * kt + 1][0], h[2 * kt + 1][1]);
+    A[kt][3] = pack_bf16(h[2 * kt + 1][2], h[2 * kt + 1][3]);
+  }
+  // layer 3 (N = 8, columns 6 and 7 unused)
+  d[0] = d[1] = d[2] = d[3] = 0.f;
+#pragma unroll
+  for (int kt = 0; kt < 4; kt++) {
+    uint32_t b0, b1;
+    bfrag<MLP_H>(S.w3t, 0, kt * 16, lane >> 2, t, b0, b1);
+    mma_bf16(d, A[kt], b0, b1);
+  }
+  const int c0 = 2 * t;
+  d[0] += S.b3[c0]; d[1] += S.b3[c0 + 1]; d[2] += S.b3[c0]; d[3] += S.b3[c0 + 1];
+  if (t == 3) { d[0] = d[1] = d[2] = d[3] = 0.0f; }   // columns 6, 7
+  // projection onto sum(c) = 1: the quad of lanes with the same g holds a row
+  float sa = d[0] + d[1], sb = d[2] + d[3];
+  sa += __shfl_xor_sync(0xffffffffu, sa, 1); sa += __shfl_xor_sync(0xffffffffu, sa, 2);
+  sb += __shfl_xor_sync(0xffffffffu, sb, 1); sb += __shfl_xor_sync(0xffffffffu, sb, 2);
+  ca = (1.0f - sa) * (1.0f / 6.0f);
+  cb = (1.0f - sb) * (1.0f / 6.0f);
+}
+
 // One warp, 16 rows starting at r0: x [n][8] -> y [n][8] (pre-projection),
 // c [n][6] (projected coefficients); z1, z2 [n][64] pre-activations if given.
 __device__ void mlp_rows(const MlpSmem &S, int r0, int n, const float *__restrict__ x, float *y, float *c, float *z1,
@@ -99,72 +180,9 @@ __device__ void mlp_rows(const MlpSmem &S, int r0, int n, const float *__restric
     const float x2 = rb < n ? x[(long)rb * MLP_IN + 2 * t] : 0.0f, x3 = rb < n ? x[(long)rb * MLP_IN + 2 * t + 1] : 0.0f;
     a[0] = pack_bf16(x0, x1); a[1] = pack_bf16(x2, x3); a[2] = 0u; a[3] = 0u;
   }
-  float h[8][4];
-#pragma unroll
-  for (int nt = 0; nt < 8; nt++) {
-    float d[4] = {0.f, 0.f, 0.f, 0.f};
-    uint32_t b0, b1;
-    bfrag<16>(S.w1t, nt * 8, 0, g, t, b0, b1);
-    mma_bf16(d, a, b0, b1);
-    const int c0 = nt * 8 + 2 * t;
-    d[0] += S.b1[c0]; d[1] += S.b1[c0 + 1]; d[2] += S.b1[c0]; d[3] += S.b1[c0 + 1];
-    if (z1) {
-      if (ra < n) { z1[(long)ra * MLP_H + c0] = d[0]; z1[(long)ra * MLP_H + c0 + 1] = d[1]; }
-      if (rb < n) { z1[(long)rb * MLP_H + c0] = d[2]; z1[(long)rb * MLP_H + c0 + 1] = d[3]; }
-    }
-#pragma unroll
-    for (int q = 0; q < 4; q++) h[nt][q] = gelu(d[q]);
-  }
-  // layer 2: the accumulator tiles of layer 1 are the A fragments of layer 2
-  uint32_t A[4][4];
-#pragma unroll
-  for (int kt = 0; kt < 4; kt++) {
-    A[kt][0] = pack_bf16(h[2 * kt][0], h[2 * kt][1]);
-    A[kt][1] = pack_bf16(h[2 * kt][2], h[2 * kt][3]);
-    A[kt][2] = pack_bf16(h[2 * kt + 1][0], h[2 * kt + 1][1]);
-    A[kt][3] = pack_bf16(h[2 * kt + 1][2], h[2 * kt + 1][3]);
-  }
-#pragma unroll
-  for (int nt = 0; nt < 8; nt++) {
-    float d[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-    for (int kt = 0; kt < 4; kt++) {
-      uint32_t b0, b1;
-      bfrag<MLP_H>(S.w2t, nt * 8, kt * 16, g, t, b0, b1);
-      mma_bf16(d, A[kt], b0, b1);
-    }
-    const int c0 = nt * 8 + 2 * t;
-    d[0] += S.b2[c0]; d[1] += S.b2[c0 + 1]; d[2] += S.b2[c0]; d[3] += S.b2[c0 + 1];
-    if (z2) {
-      if (ra < n) { z2[(long)ra * MLP_H + c0] = d[0]; z2[(long)ra * MLP_H + c0 + 1] = d[1]; }
-      if (rb < n) { z2[(long)rb * MLP_H + c0] = d[2]; z2[(long)rb * MLP_H + c0 + 1] = d[3]; }
-    }
-#pragma unroll
-    for (int q = 0; q < 4; q++) h[nt][q] = gelu(d[q]);
-  }
-#pragma unroll
-  for (int kt = 0; kt < 4; kt++) {
-    A[kt][0] = pack_bf16(h[2 * kt][0], h[2 * kt][1]);
-    A[kt][1] = pack_bf16(h[2 * kt][2], h[2 * kt][3]);
-    A[kt][2] = pack_bf16(h[2 * kt + 1][0], h[2 * kt + 1][1]);
-    A[kt][3] = pack_bf16(h[2 * kt + 1][2], h[2 * kt + 1][3]);
-  }
-  // layer 3 (N = 8, columns 6 and 7 unused)
-  float d[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-  for (int kt = 0; kt < 4; kt++) {
-    uint32_t b0, b1;
-    bfrag<MLP_H>(S.w3t, 0, kt * 16, g, t, b0, b1);
-    mma_bf16(d, A[kt], b0, b1);
-  }
+  float d[4], ca, cb;
+  mlp_tile(S, a, ra, rb, n, z1, z2, d, ca, cb);
   const int c0 = 2 * t;
-  d[0] += S.b3[c0]; d[1] += S.b3[c0 + 1]; d[2] += S.b3[c0]; d[3] += S.b3[c0 + 1];
-  if (t == 3) { d[0] = d[1] = d[2] = d[3] = 0.0f; }   // columns 6, 7
-  // projection onto sum(c) = 1: the quad of lanes with the same g holds a row
-  float sa = d[0] + d[1], sb = d[2] + d[3];
-  sa += __shfl_xor_sync(0xffffffffu, sa, 1); sa += __shfl_xor_sync(0xffffffffu, sa, 2);
-  sb += __shfl_xor_sync(0xffffffffu, sb, 1); sb += __shfl_xor_sync(0xffffffffu, sb, 2);
-  const float ca = (1.0f - sa) * (1.0f / 6.0f), cb = (1.0f - sb) * (1.0f / 6.0f);
   if (y) {
     if (ra < n) { y[(long)ra * MLP_OUT + c0] = d[0]; y[(long)ra * MLP_OUT + c0 + 1] = d[1]; }
     if (rb < n) { y[(long)rb * MLP_OUT + c0] = d[2]; y[(long)rb * MLP_OUT + c0 + 1] = d[3]; }
@@ -209,8 +227,8 @@ __global__ void __launch_bounds__(BW_NT) k_mlp_backward(const float *__restrict_
   const int r_begin = (int)blockIdx.x * BW_ROWS, r_end = min(n, r_begin + BW_ROWS);
   for (int r = r_begin; r < r_end; r++) {
     const float a1 = z1[(long)r * MLP_H + i], a2 = z2[(long)r * MLP_H + i];
-    h1s[i] = bf16r(gelu(a1));                // the BF16 operands the forward multiplied
-    h2s[i] = bf16r(gelu(a2));
+    h1s[i] = bf16r(act(a1));                // the BF16 operands the forward multiplied
+    h2s[i] = bf16r(act(a2));
     if (i < MLP_IN) xs[i] = bf16r(i < 7 ? x[(long)r * MLP_IN + i] : 0.0f);
     if (i < MLP_OUT) dys[i] = (i < MLP_NC) ? dy[(long)r * MLP_OUT + i] : 0.0f;
     __syncthreads();
@@ -219,7 +237,7 @@ __global__ void __launch_bounds__(BW_NT) k_mlp_backward(const float *__restrict_
 #pragma unroll
     for (int o = 0; o < MLP_OUT; o++) { gw3[o] += h2s[i] * dys[o]; dh2 += dys[o] * w3[i][o]; }
     if (i < MLP_OUT) gb3 += dys[i];
-    const float dz2 = dh2 * gelu_grad(a2);
+    const float dz2 = dh2 * act_grad(a2);
     dz2s[i] = dz2;
     gb2 += dz2;
     __syncthreads();
@@ -227,7 +245,7 @@ __global__ void __launch_bounds__(BW_NT) k_mlp_backward(const float *__restrict_
     float dh1 = 0.f;
 #pragma unroll
     for (int j = 0; j < MLP_H; j++) { gw2[j] += h1s[i] * dz2s[j]; dh1 += dz2s[j] * w2[i][j]; }
-    const float dz1 = dh1 * gelu_grad(a1);
+    const float dz1 = dh1 * act_grad(a1);
     gb1 += dz1;
 #pragma unroll
     for (int k = 0; k < MLP_IN; k++) gw1[k] += xs[k] * dz1;
@@ -332,8 +350,22 @@ __global__ void k_face_features(int ni, int nj, int nk, int ngxy, int dir, const
   m[f] = mean; dsc[f] = sc; uf[f] = u;
 }
 
-// Face value from the coefficients, or NaN where it leaves the range of the
-// two cells that share the face (there the WENO5 value is used instead).
+// p where it lies within the range of the stencil cells 2..5 (the two
+// cells on each side of the face; tolerance 1e-6 of the stencil's scale),
+// else NaN (the scalar kernel then takes the WENO5 value).
+__device__ __forceinline__ float bounded_face(float p, float m, float d, const float *x) {
+  float lo = m + d * x[1], hi = lo;
+#pragma unroll
+  for (int q = 2; q <= 4; q++) {
+    const float v = m + d * x[q];
+    lo = fminf(lo, v);
+    hi = fmaxf(hi, v);
+  }
+  const float tol = 1e-6f * d;
+  return (p >= lo - tol && p <= hi + tol) ? p : __int_as_float(0x7fc00000);
+}
+
+// Face value from the coefficients, bounded as above.
 __global__ void k_face_phi(long nf, const float *__restrict__ x, const float *__restrict__ c, const float *__restrict__ m,
                            const float *__restrict__ dsc, float *phi) {
   const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -342,10 +374,101 @@ __global__ void k_face_phi(long nf, const float *__restrict__ x, const float *__
 #pragma unroll
   for (int q = 0; q < MLP_NC; q++) acc += c[f * MLP_NC + q] * x[f * MLP_IN + q];
   const float p = m[f] + dsc[f] * acc;
-  // the two cells adjacent to the face are stencil points 3 and 4
-  const float a = m[f] + dsc[f] * x[f * MLP_IN + 2], b = m[f] + dsc[f] * x[f * MLP_IN + 3];
-  const float lo = fminf(a, b), hi = fmaxf(a, b), tol = 1e-6f * dsc[f];
-  phi[f] = (p >= lo - tol && p <= hi + tol) ? p : __int_as_float(0x7fc00000);
+  phi[f] = bounded_face(p, m[f], dsc[f], x + f * MLP_IN);
+}
+
+// The closure's face values in one pass: for 32 faces per warp, the
+// features (the arithmetic of k_face_features) go to shared memory, the
+// MLP runs on the tensor cores (two 16-row tiles), and the bounded face
+// value is formed as k_face_phi forms it, with the six coefficients gathered
+// to the first lane of each row's quad so that the sum runs in the same
+// order.  The result equals features -> forward -> face_phi bit for bit,
+// without the 31 floats per face those passes write and read back.
+constexpr int CF_WARPS = 4;
+struct FaceTile {
+  float x[32][MLP_IN + 1];     // pitch 9: the A-fragment reads of a quad fall in different banks
+  float m[32], d[32];
+};
+
+__global__ void __launch_bounds__(CF_WARPS * 32) k_closure_faces(int ni, int nj, int nk, int ngxy, int dir,
+                                                                const float *__restrict__ s,
+                                                                const float *__restrict__ th0, int sadd,
+                                                                const float *__restrict__ vel, float dtdx,
+                                                                const float *__restrict__ params, float *phi) {
+  __shared__ MlpSmem S;
+  __shared__ FaceTile T[CF_WARPS];
+  load_weights(S, params);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  FaceTile &F = T[wib];
+  const int NI = ni + 2 * ngxy, NJ = nj + 2 * ngxy, ib = 1 - ngxy;
+  const int nfx = (dir == 0) ? ni + 1 : ni, nfy = (dir == 0) ? nj : nj + 1;
+  const long nf = (long)nfx * nfy * nk, plane = (long)NI * NJ;
+  const long nw = (long)gridDim.x * CF_WARPS;
+  for (long f0 = ((long)blockIdx.x * CF_WARPS + wib) * 32; f0 < nf; f0 += nw * 32) {
+    const long f = f0 + lane;
+    if (f < nf) {
+      const int i = 1 + (int)(f % nfx), j = 1 + (int)((f / nfx) % nfy), k = 1 + (int)(f / ((long)nfx * nfy));
+      const float u = (dir == 0) ? vel[(long)(i - ib) + (long)(NI + 1) * ((j - ib) + (long)NJ * k)]
+                                 : vel[(long)(i - ib) + (long)NI * ((j - ib) + (long)(NJ + 1) * k)];
+      const float add = sadd ? (th0[k] - 300.0f) : 0.0f;
+      float v[6];
+#pragma unroll
+      for (int q = 0; q < 6; q++) {
+        const int off = (u >= 0.0f) ? (q - 3) : (2 - q);
+        const int ii = (dir == 0) ? i + off : i, jj = (dir == 0) ? j : j + off;
+        const float r = s[(long)(ii - ib) + (long)NI * (jj - ib) + plane * k];
+        v[q] = sadd ? add + r : r;
+      }
+      float mn = v[0], mx = v[0], sum = 0.f;
+#pragma unroll
+      for (int q = 0; q < 6; q++) { mn = fminf(mn, v[q]); mx = fmaxf(mx, v[q]); sum += v[q]; }
+      const float mean = sum * (1.0f / 6.0f), sc = (mx - mn) + 1e-6f;
+#pragma unroll
+      for (int q = 0; q < 6; q++) F.x[lane][q] = (v[q] - mean) / sc;
+      F.x[lane][6] = fabsf(u) * dtdx;
+      F.x[lane][7] = 0.0f;
+      F.m[lane] = mean; F.d[lane] = sc;
+    } else {
+#pragma unroll
+      for (int q = 0; q < MLP_IN; q++) F.x[lane][q] = 0.0f;
+      F.m[lane] = 0.0f; F.d[lane] = 1.0f;
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int h = 0; h < 2; h++) {
+      const int ra = 16 * h + g, rb = ra + 8;
+      uint32_t a[4];
+      a[0] = pack_bf16(F.x[ra][2 * t], F.x[ra][2 * t + 1]);
+      a[1] = pack_bf16(F.x[rb][2 * t], F.x[rb][2 * t + 1]);
+      a[2] = 0u; a[3] = 0u;
+      float d[4], ca, cb;
+      mlp_tile(S, a, 0, 0, 0, nullptr, nullptr, d, ca, cb);
+      // this lane's coefficients (columns 2t, 2t+1) of rows ra and rb
+      const float a0 = d[0] + ca, a1 = d[1] + ca, b0 = d[2] + cb, b1 = d[3] + cb;
+      const float a2 = __shfl_down_sync(0xffffffffu, a0, 1), a3 = __shfl_down_sync(0xffffffffu, a1, 1);
+      const float a4 = __shfl_down_sync(0xffffffffu, a0, 2), a5 = __shfl_down_sync(0xffffffffu, a1, 2);
+      const float b2 = __shfl_down_sync(0xffffffffu, b0, 1), b3 = __shfl_down_sync(0xffffffffu, b1, 1);
+      const float b4 = __shfl_down_sync(0xffffffffu, b0, 2), b5 = __shfl_down_sync(0xffffffffu, b1, 2);
+      if (t == 0) {
+        const float ca6[6] = {a0, a1, a2, a3, a4, a5}, cb6[6] = {b0, b1, b2, b3, b4, b5};
+#pragma unroll
+        for (int rr = 0; rr < 2; rr++) {
+          const int row = rr ? rb : ra;
+          const long fr = f0 + row;
+          if (fr >= nf) continue;
+          const float *cc = rr ? cb6 : ca6;
+          float acc = 0.f;
+#pragma unroll
+          for (int q = 0; q < MLP_NC; q++) acc += cc[q] * F.x[row][q];
+          const float mr = F.m[row], dr = F.d[row];
+          const float p = mr + dr * acc;
+          phi[fr] = bounded_face(p, mr, dr, F.x[row]);
+        }
+      }
+    }
+    __syncwarp();
+  }
 }
 
 // ---- launchers ----
@@ -377,6 +500,15 @@ void launch_face_phi(long nf, const float *x, const float *c, const float *m, co
                      cudaStream_t st) {
   k_face_phi<<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(nf, x, c, m, d, phi);
 }
+void launch_closure_faces(int ni, int nj, int nk, int ngxy, int dir, const float *s, const float *th0, int sadd,
+                          const float *vel, float dtdx, const float *params, float *phi, cudaStream_t st) {
+  const long nf = (long)((dir == 0) ? ni + 1 : ni) * ((dir == 0) ? nj : nj + 1) * nk;
+  const long tiles = (nf + 31) / 32;
+  const long blocks = std::min<long>((tiles + CF_WARPS - 1) / CF_WARPS, 148L * 8);
+  if (blocks > 0)
+    k_closure_faces<<<(unsigned)blocks, CF_WARPS * 32, 0, st>>>(ni, nj, nk, ngxy, dir, s, th0, sadd, vel, dtdx, params,
+                                                                 phi);
+}
 int mlp_param_count() { return P_TOTAL; }
 
 }  // namespace cm1g
@@ -396,6 +528,16 @@ int after_launch() {
 }  // namespace
 
 extern "C" int32_t cm1g_mlp_param_count(void) { return cm1g::P_TOTAL; }
+
+extern "C" int cm1g_closure_faces(int32_t ni, int32_t nj, int32_t nk, int32_t ngxy, int32_t dir, const float *s,
+                                  const float *th0, int32_t sadd, const float *vel, float dtdx, const float *params,
+                                  float *phi, void *stream) {
+  if (!s || !vel || !params || !phi || (sadd && !th0) || (dir != 0 && dir != 1) || ni < 1 || nj < 1 || nk < 1 ||
+      ngxy < 3)
+    return bad("cm1g_closure_faces: bad argument");
+  cm1g::launch_closure_faces(ni, nj, nk, ngxy, dir, s, th0, sadd, vel, dtdx, params, phi, (cudaStream_t)stream);
+  return after_launch();
+}
 
 extern "C" int cm1g_mlp_forward(const float *params, int32_t n, const float *x, float *y, float *c, float *z1,
                                 float *z2, void *stream) {

@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(TX * NW, CM1G_SND_MINB) k_sound_tile(DGrid g, 
 // pk1+qk and pk2-qk are recomputed on the way down from the same inputs.
 // The arithmetic and its order are those of the tile form.
 // ---------------------------------------------------------------------
-static const int SNC_TX = 32, SNC_TY = 4;
+static const int SNC_TX = 32;
 // grids with at least this many columns (ni*nj) use the column-sweep form
 #ifndef CM1G_SOUND_COL_MIN_COLUMNS
 #define CM1G_SOUND_COL_MIN_COLUMNS (1L << 20)
@@ -496,7 +496,6 @@ __global__ void __launch_bounds__(TX * TY, 4) k_sound_col(DGrid g, SoundIO io, S
   }
 }
 
-size_t sound_col_smem_bytes(const DGrid &g) { return (size_t)(g.nk + 2) * SNC_TX * SNC_TY * sizeof(float); }
 
 void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, int64_t *nlaunch);
 
@@ -523,6 +522,30 @@ void sound_nloop(int nsound, int nrk, float dt, int *nloop_out, float *dts_out) 
 size_t sound_smem_bytes(const DGrid &g) { return (size_t)5 * (g.nk + 2) * SND_TX * sizeof(float); }
 int sound_max_nk() { return SND_NW * SND_KPT; }
 
+// The acoustic kernel's forms (kNumSoundCfgs): the tile form with 8 or 4
+// warps over the levels of 32 columns, and the column sweep with 32 x 4 or
+// 32 x 2 columns per block.  Both tile forms cover SND_NW * SND_KPT levels.
+static_assert(SND_NW * SND_KPT == (SND_NW / 2) * (SND_KPT * 2), "both tile forms cover the same levels");
+template <int TY>
+static size_t sound_col_smem(const DGrid &g) { return (size_t)(g.nk + 2) * SNC_TX * TY * sizeof(float); }
+
+static void sound_set_attributes() {
+  static bool done = false;
+  if (done) return;
+  cudaFuncSetAttribute(k_sound_col<SNC_TX, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_sound_col<SNC_TX, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW, SND_KPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       200 * 1024);
+  cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW / 2, SND_KPT * 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       200 * 1024);
+  // three blocks of 5 column arrays each; the rest of the unified L1 stays
+  // cache for the neighbour reads of phase 1
+  cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW, SND_KPT>, cudaFuncAttributePreferredSharedMemoryCarveout, 70);
+  cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW / 2, SND_KPT * 2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       70);
+  done = true;
+}
+
 // One RK stage of acoustic steps.  At the first stage the reference starts
 // from the current u3d/v3d/w3d/pp3d (sound.F:192-208); at later stages it
 // first resets them to the start-of-step ua/va/wa/ppi (sound.F:212-230).
@@ -540,27 +563,22 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
   sound_nloop(nsound, nrk, dt, &nloop, &dts);
   // The column-sweep form keeps one thread per column, so it needs many
   // columns to fill the GPU; smaller grids use the tile form, whose warps
-  // split the levels of a column.
-  // CM1G_SOUND_FORM=col|tile overrides the choice (read at each call).
-  bool col = (long)g.ni * g.nj >= (long)CM1G_SOUND_COL_MIN_COLUMNS;
+  // split the levels of a column.  g.sound_cfg (set by the autotuner or
+  // cm1g_set_tune) overrides the choice, and CM1G_SOUND_FORM=col|tile
+  // (read at each call) overrides both.
+  int cfg = g.sound_cfg;
+  if (cfg < 0 || cfg >= kNumSoundCfgs) cfg = ((long)g.ni * g.nj >= (long)CM1G_SOUND_COL_MIN_COLUMNS) ? 2 : 0;
   if (const char *f = getenv("CM1G_SOUND_FORM")) {
-    if (!strcmp(f, "col")) col = true;
-    else if (!strcmp(f, "tile")) col = false;
+    if (!strcmp(f, "col")) cfg = 2;
+    else if (!strcmp(f, "tile")) cfg = 0;
   }
-  dim3 blk = col ? dim3(SNC_TX, SNC_TY) : dim3(SND_TX, SND_NW);
-  dim3 grid = col ? dim3((g.ni + SNC_TX - 1) / SNC_TX, (g.nj + SNC_TY - 1) / SNC_TY)
+  const int cty = (cfg == 3) ? 2 : 4, nw = (cfg == 1) ? SND_NW / 2 : SND_NW;
+  const bool col = cfg >= 2;
+  dim3 blk = col ? dim3(SNC_TX, cty) : dim3(SND_TX, nw);
+  dim3 grid = col ? dim3((g.ni + SNC_TX - 1) / SNC_TX, (g.nj + cty - 1) / cty)
                   : dim3((g.ni + SND_TX - 1) / SND_TX, g.nj);
-  size_t smem = col ? sound_col_smem_bytes(g) : sound_smem_bytes(g);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_sound_col<SNC_TX, SNC_TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW, SND_KPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
-    // three blocks of 5 column arrays each; the rest of the unified L1 stays
-    // cache for the neighbour reads of phase 1
-    cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW, SND_KPT>, cudaFuncAttributePreferredSharedMemoryCarveout, 70);
-    attr_set = true;
-  }
+  size_t smem = col ? (cty == 2 ? sound_col_smem<2>(g) : sound_col_smem<4>(g)) : sound_smem_bytes(g);
+  sound_set_attributes();
   const float *uin = (nrk == 1) ? u3d : ua, *vin = (nrk == 1) ? v3d : va, *ppdin = ppx;
   for (int n = 1; n <= nloop; n++) {
     SoundIO io;
@@ -582,8 +600,12 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
     sp.ppd_mapped = (n > 1);
     {
       ProfScope _ps("k_sound_step", st);
-      if (col) k_sound_col<SNC_TX, SNC_TY><<<grid, blk, smem, st>>>(g, io, sp);
-      else k_sound_tile<SND_TX, SND_NW, SND_KPT><<<grid, blk, smem, st>>>(g, io, sp);
+      switch (cfg) {
+        case 1: k_sound_tile<SND_TX, SND_NW / 2, SND_KPT * 2><<<grid, blk, smem, st>>>(g, io, sp); break;
+        case 2: k_sound_col<SNC_TX, 4><<<grid, blk, smem, st>>>(g, io, sp); break;
+        case 3: k_sound_col<SNC_TX, 2><<<grid, blk, smem, st>>>(g, io, sp); break;
+        default: k_sound_tile<SND_TX, SND_NW, SND_KPT><<<grid, blk, smem, st>>>(g, io, sp); break;
+      }
     }
     if (nl) *nl += 1;
     uin = io.u_out; vin = io.v_out; ppdin = io.ppd_out;

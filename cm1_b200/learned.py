@@ -19,7 +19,7 @@ runs with plain WENO5 and with the closure, and a plain run at twice the
 coarse resolution, are compared with the coarsened fine run after the same
 simulated time (L2 of theta'), together with each run's GPU time.
 
-    python -m cm1_b200.learned [--runs 8] [--outputs 16] [--epochs 40] [--minutes 30]
+    python -m cm1_b200.learned [--runs 8] [--outputs 16] [--epochs 40] [--keep 1.0] [--minutes 30]
 """
 import argparse
 import ctypes as C
@@ -48,10 +48,10 @@ def init_params(seed=0):
     rng = np.random.default_rng(seed)
     p = np.zeros(N_PARAMS, np.float32)
     o = 0
-    w1 = rng.normal(0, 1 / math.sqrt(7), (8, 64)).astype(np.float32)
+    w1 = rng.normal(0, math.sqrt(2.0 / 7), (8, 64)).astype(np.float32)      # He initialisation (ReLU)
     w1[7] = 0
     p[o:o + 512] = w1.ravel(); o += 512 + 64
-    p[o:o + 4096] = rng.normal(0, 1 / 8.0, 4096); o += 4096 + 64
+    p[o:o + 4096] = rng.normal(0, math.sqrt(2.0 / 64), 4096); o += 4096 + 64
     w3 = rng.normal(0, 0.01, (64, 8)).astype(np.float32)
     w3[:, 6:] = 0
     p[o:o + 512] = w3.ravel(); o += 512
@@ -180,8 +180,10 @@ def coarse_mass(ccase, dev):
 
 
 # ---------------------------------------------------------------- data
-def face_samples(ccase, cdev, fx_sum, fy_sum, rx_sum, ry_sum, dt_c, keep_quiet, rng):
-    """Features and targets of the coarse x- and y-faces for one coarse step."""
+def face_samples(ccase, cdev, fx_sum, fy_sum, rx_sum, ry_sum, dt_c, keep_quiet, keep_active=1.0):
+    """Features and targets of the coarse x- and y-faces for one coarse step:
+    a random `keep_active` of the faces whose stencil varies by more than
+    1e-3 K, and `keep_quiet` of the others."""
     import torch
     b = _lib()
     L = b.lib()
@@ -199,16 +201,18 @@ def face_samples(ccase, cdev, fx_sum, fy_sum, rx_sum, ry_sum, dt_c, keep_quiet, 
         wgt = (rsum * rsum).reshape(-1)
         ok = (rsum.abs().reshape(-1) > 1e-6) & torch.isfinite(phi)
         active = d > 1e-3
-        sel = ok & (active | (torch.rand(nf, device="cuda", generator=None) < keep_quiet))
+        draw_ = torch.rand(nf, device="cuda")
+        sel = ok & torch.where(active, draw_ < keep_active, draw_ < keep_quiet)
         out.append((x[sel], m[sel], d[sel], phi[sel], wgt[sel]))
     return out
 
 
-def generate(runs, outputs, spacing, seed=11, log=print):
+def generate(runs, outputs, spacing, seed=11, keep_active=1.0, log=print):
     """Training samples from `runs` fine-grid runs, `outputs` coarse steps each."""
     import torch
     b = _lib()
     rng = np.random.default_rng(seed)
+    torch.manual_seed(seed)
     chunks = []
     t_gpu = 0.0
     for r in range(runs):
@@ -234,7 +238,8 @@ def generate(runs, outputs, spacing, seed=11, log=print):
                 sums[0] += sum_uface(fl, cap[0]); sums[1] += sum_vface(fl, cap[1])
                 sums[2] += sum_uface(fl, cap[2]); sums[3] += sum_vface(fl, cap[3])
             fctx.capture_fluxes()
-            chunks.extend(face_samples(ccase, cdev, sums[0], sums[1], sums[2], sums[3], ccase.dt, 0.05, rng))
+            chunks.extend(face_samples(ccase, cdev, sums[0], sums[1], sums[2], sums[3], ccase.dt, 0.05 * keep_active,
+                                       keep_active))
         torch.cuda.synchronize()
         t_gpu += time.perf_counter() - t0
         log("run %d %s: %d samples so far" % (r, prm, sum(c[0].shape[0] for c in chunks)))
@@ -245,9 +250,30 @@ def generate(runs, outputs, spacing, seed=11, log=print):
 
 
 # ---------------------------------------------------------------- training
-def train(data, epochs, batch=65536, lr=2e-3, lr_end=5e-5, seed=5, log=print):
+def _loss_of(P, data, chunk=1 << 22):
+    """Mean weighted face loss of parameters P over a data set (library kernels)."""
+    import torch
+    b = _lib()
+    L = b.lib()
+    x, m, d, tgt, w = data
+    n = x.shape[0]
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+    y = torch.empty(min(n, chunk), 8, device="cuda")
+    dy = torch.empty(min(n, chunk), 8, device="cuda")
+    for s0 in range(0, n, chunk):
+        k = min(chunk, n - s0)
+        xs, ms, ds, ts, ws = (a[s0:s0 + k].contiguous() for a in (x, m, d, tgt, w))
+        b.check(L.cm1g_mlp_forward(_fp(P), k, _fp(xs), _fp(y), None, None, None, None))
+        b.check(L.cm1g_closure_loss(k, _fp(xs), _fp(y), _fp(ms), _fp(ds), _fp(ts), _fp(ws), _fp(dy),
+                                    C.c_void_p(loss.data_ptr()), None))
+    return float(loss.item()) / max(1, n)
+
+
+def train(data, epochs, batch=65536, lr=2e-3, lr_end=5e-5, seed=5, val=None, log=print):
     """Adam over shuffled mini-batches, all on the library's kernels; the step
-    size follows a cosine from lr to lr_end over the whole run."""
+    size follows a cosine from lr to lr_end over the whole run.  With a
+    validation set (samples of other runs), the parameters of the epoch with
+    the lowest validation loss are returned."""
     import torch
     b = _lib()
     L = b.lib()
@@ -263,7 +289,8 @@ def train(data, epochs, batch=65536, lr=2e-3, lr_end=5e-5, seed=5, log=print):
     loss = torch.zeros(1, dtype=torch.float64, device="cuda")
     gen = torch.Generator(device="cuda")
     gen.manual_seed(seed)
-    step, hist = 0, []
+    step, hist, vhist = 0, [], []
+    best, best_P = None, None
     t0 = time.perf_counter()
     for ep in range(epochs):
         perm = torch.randperm(n, device="cuda", generator=gen)
@@ -283,10 +310,17 @@ def train(data, epochs, batch=65536, lr=2e-3, lr_end=5e-5, seed=5, log=print):
         torch.cuda.synchronize()
         nb = max(1, n // batch)
         hist.append(loss.item() / (nb * batch))
+        if val is not None:
+            vhist.append(_loss_of(P, val))
+            if best is None or vhist[-1] < best:
+                best, best_P = vhist[-1], P.clone()
         if ep % 5 == 0 or ep == epochs - 1:
-            log("epoch %d loss %.4e" % (ep, hist[-1]))
+            log("epoch %d loss %.4e%s" % (ep, hist[-1], " validation %.4e" % vhist[-1] if vhist else ""))
     torch.cuda.synchronize()
-    return P, hist, time.perf_counter() - t0
+    t = time.perf_counter() - t0
+    if best_P is not None:
+        P = best_P
+    return P, {"train": hist, "validation": vhist}, t
 
 
 def baseline_loss(data):
@@ -299,21 +333,102 @@ def baseline_loss(data):
 
 
 # ---------------------------------------------------------------- evaluation
-def _timed_run(ctx, dev, case, nsteps, mass1=None):
+def weno5_faces(v, weps=1e-17):
+    """WENO5 face values with the Borges et al. (2008) weights (the plain
+    method of the scalar pass), float64, from the upwind-ordered stencil
+    values v[:, 0..4] (v[:, 2] and v[:, 3] are the cells beside the face)."""
+    s1, s2, s3, s4, s5 = (v[:, q] for q in range(5))
+    b1 = 13.0 / 12.0 * (s1 - 2 * s2 + s3) ** 2 + 0.25 * (s1 - 4 * s2 + 3 * s3) ** 2
+    b2 = 13.0 / 12.0 * (s2 - 2 * s3 + s4) ** 2 + 0.25 * (s2 - s4) ** 2
+    b3 = 13.0 / 12.0 * (s3 - 2 * s4 + s5) ** 2 + 0.25 * (3 * s3 - 4 * s4 + s5) ** 2
+    q1 = (2 * s1 - 7 * s2 + 11 * s3) / 6.0
+    q2 = (-s2 + 5 * s3 + 2 * s4) / 6.0
+    q3 = (2 * s3 + 5 * s4 - s5) / 6.0
+    tau = (b1 - b3).abs()
+    a1 = 0.1 * (1 + (tau / (b1 + weps)) ** 2)
+    a2 = 0.6 * (1 + (tau / (b2 + weps)) ** 2)
+    a3 = 0.3 * (1 + (tau / (b3 + weps)) ** 2)
+    return (a1 * q1 + a2 * q2 + a3 * q3) / (a1 + a2 + a3)
+
+
+def face_errors(P, data, chunk=1 << 22):
+    """Weighted mean squared error of the coarse face values against the
+    fine-run targets, for the 5th-order upwind weights, WENO5, the network,
+    and the network with the WENO5 fallback outside the neighbour bounds (the
+    form the large step uses)."""
     import torch
-    mass1 = case.mass1 if mass1 is None else mass1
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ctx.step(dev, case.dt, mass1, use_graph=True)             # capture the graph (untimed)
+    b = _lib()
+    L = b.lib()
+    x, m, d, tgt, w = data
+    n = x.shape[0]
+    c = torch.empty(n, 6, device="cuda")
+    y = torch.empty(min(n, chunk), 8, device="cuda")
+    for s0 in range(0, n, chunk):
+        k = min(chunk, n - s0)
+        xs = x[s0:s0 + k].contiguous()
+        cs = torch.empty(k, 6, device="cuda")
+        b.check(L.cm1g_mlp_forward(_fp(P), k, _fp(xs), _fp(y), _fp(cs), None, None, None))
+        c[s0:s0 + k] = cs
     torch.cuda.synchronize()
-    e0.record()
-    for _ in range(nsteps - 1):
-        ctx.step(dev, case.dt, mass1, use_graph=True)
-    e1.record()
-    torch.cuda.synchronize()
-    return e0.elapsed_time(e1) * nsteps / max(1, nsteps - 1) / 1e3
+    xd, md, dd, td, wd = x[:, :6].double(), m.double(), d.double(), tgt.double(), w.double()
+    v = md[:, None] + dd[:, None] * xd
+    c5 = torch.tensor([2, -13, 47, 27, -3, 0], dtype=torch.float64, device="cuda") / 60.0
+    phi5 = md + dd * (xd @ c5)
+    phiw = weno5_faces(v)
+    phil = md + dd * (c.double() * xd).sum(1)
+    lo, hi = v[:, 1:5].min(1).values, v[:, 1:5].max(1).values
+    tol = 1e-6 * dd
+    inside = lambda phi: (phi >= lo - tol) & (phi <= hi + tol)
+    ins = inside(phil)
+    phib = torch.where(ins, phil, phiw)
+    err = lambda phi: float((wd * (phi - td) ** 2).sum().item() / n)
+    frac_out = lambda phi: float(1.0 - inside(phi).double().mean().item())
+    return {"samples": int(n), "upwind5": err(phi5), "weno5": err(phiw), "learned": err(phil),
+            "learned_with_fallback": err(phib), "fallback_fraction": frac_out(phil),
+            "upwind5_outside_bounds": frac_out(phi5), "target_outside_bounds": frac_out(td)}
 
 
-def evaluate(P, tests, minutes, seed=77, log=print):
+class _Run:
+    """A run advanced in segments; its GPU time is the sum of CUDA-event
+    times of the replayed step graphs.  The first step of the run captures
+    the graph (host work) and is not timed; the run's time is scaled by
+    steps / timed steps."""
+
+    def __init__(self, ctx, dev, case, mass1):
+        self.ctx, self.dev, self.case, self.mass1 = ctx, dev, case, mass1
+        self.steps = self.timed = 0
+        self.ms = 0.0
+
+    def advance(self, n):
+        import torch
+        if n <= 0:
+            return
+        if self.steps == 0:
+            self.ctx.step(self.dev, self.case.dt, self.mass1, use_graph=True)
+            self.steps += 1
+            n -= 1
+            torch.cuda.synchronize()
+        if n <= 0:
+            return
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            self.ctx.step(self.dev, self.case.dt, self.mass1, use_graph=True)
+        e1.record()
+        torch.cuda.synchronize()
+        self.ms += e0.elapsed_time(e1)
+        self.steps += n
+        self.timed += n
+
+    def gpu_seconds(self):
+        return self.ms / 1e3 * self.steps / max(1, self.timed)
+
+
+def evaluate(P, tests, minutes, seed=77, horizons=(2, 10, 50), log=print):
+    """Held-out runs: L2 of theta' against the coarsened fine run after
+    `horizons` coarse steps and after `minutes`, for the coarse grid without
+    and with the closure and for the plain method at twice the coarse
+    resolution, with each run's GPU time to that point."""
     import torch
     b = _lib()
     rng = np.random.default_rng(seed)
@@ -323,38 +438,39 @@ def evaluate(P, tests, minutes, seed=77, log=print):
         fcase = member(FINE, seed + 100 * t, **prm)
         ccase = member(COARSE, seed + 100 * t + 1, **prm)
         mcase = member(MID, seed + 100 * t + 2, **prm)
-        fctx, cctx, mctx = (b.Context(c.cfg, c.grid) for c in (fcase, ccase, mcase))
+        fctx, pctx, lctx, mctx = (b.Context(c.cfg, c.grid) for c in (fcase, ccase, ccase, mcase))
+        lctx.closure(P)
         fdev = b.to_device(fcase.state)
         # initial coarse/mid states from the fine initial state (same bubble, same shear)
-        c_plain = coarse_state(fcase, fdev, ccase, cctx)
+        c_plain = coarse_state(fcase, fdev, ccase, pctx)
         c_learn = {k: v.clone() for k, v in c_plain.items()}
         mdev = coarse_state(fcase, fdev, mcase, mctx, (2, 2, 2))
-        steps_f = int(round(minutes * 60 / fcase.dt))
-        steps_c = int(round(minutes * 60 / ccase.dt))
-        steps_m = int(round(minutes * 60 / mcase.dt))
-        t_fine = _timed_run(fctx, fdev, fcase, steps_f)
         m1c = coarse_mass(ccase, c_plain)
-        t_plain = _timed_run(cctx, c_plain, ccase, steps_c, m1c)
-        cctx.closure(P)
-        t_learn = _timed_run(cctx, c_learn, ccase, steps_c, m1c)
-        cctx.closure(None, enable=False)
-        t_mid = _timed_run(mctx, mdev, mcase, steps_m, coarse_mass(mcase, mdev))
-        truth = coarse_state(fcase, fdev, ccase, cctx)
-        cl = ccase.lay
+        runs = {"fine_plain_250m": _Run(fctx, fdev, fcase, fcase.mass1),
+                "coarse_plain": _Run(pctx, c_plain, ccase, m1c),
+                "coarse_learned": _Run(lctx, c_learn, ccase, m1c),
+                "plain_500m": _Run(mctx, mdev, mcase, coarse_mass(mcase, mdev))}
+        ratio = {"fine_plain_250m": FX, "coarse_plain": 1, "coarse_learned": 1, "plain_500m": 2}
+        total = int(round(minutes * 60 / ccase.dt))
+        cl, ml = ccase.lay, mcase.lay
         ci = (slice(cl.kx(1), cl.kx(cl.nk) + 1), slice(cl.jx(1), cl.jx(cl.nj) + 1), slice(cl.ix(1), cl.ix(cl.ni) + 1))
-        ref = truth["th3d"][ci]
-        l2 = lambda a: float(torch.sqrt(((a - ref) ** 2).mean()).item())
-        # the 500 m plain run, averaged onto the coarse grid (2 x 2 horizontally, same levels)
-        ml = mcase.lay
-        mth = mdev["th3d"][ml.kx(1):ml.kx(ml.nk) + 1, ml.jx(1):ml.jx(ml.nj) + 1, ml.ix(1):ml.ix(ml.ni) + 1]
-        mth = mth.reshape(ml.nk, ml.nj // 2, 2, ml.ni // 2, 2).mean(dim=(2, 4))
-        r = {"params": prm, "minutes": minutes, "l2_theta": {"coarse_plain": l2(c_plain["th3d"][ci]),
-             "coarse_learned": l2(c_learn["th3d"][ci]), "plain_500m": l2(mth), "no_change": l2(torch.zeros_like(ref))},
-             "gpu_seconds": {"fine_plain_250m": t_fine, "coarse_plain": t_plain, "coarse_learned": t_learn,
-                             "plain_500m": t_mid}}
-        log(json.dumps(r))
-        res.append(r)
-        for c in (fctx, cctx, mctx):
+        done, rows = 0, []
+        for hz in sorted(set([h for h in horizons if h < total] + [total])):
+            for name, r in runs.items():
+                r.advance((hz - done) * ratio[name])
+            done = hz
+            ref = coarse_state(fcase, fdev, ccase, pctx)["th3d"][ci]
+            l2 = lambda a: float(torch.sqrt(((a - ref) ** 2).mean()).item())
+            mth = mdev["th3d"][ml.kx(1):ml.kx(ml.nk) + 1, ml.jx(1):ml.jx(ml.nj) + 1, ml.ix(1):ml.ix(ml.ni) + 1]
+            mth = mth.reshape(ml.nk, ml.nj // 2, 2, ml.ni // 2, 2).mean(dim=(2, 4))
+            row = {"coarse_steps": hz, "seconds": hz * ccase.dt,
+                   "l2_theta": {"coarse_plain": l2(c_plain["th3d"][ci]), "coarse_learned": l2(c_learn["th3d"][ci]),
+                                "plain_500m": l2(mth), "no_change": l2(torch.zeros_like(ref))},
+                   "gpu_seconds": {k: r.gpu_seconds() for k, r in runs.items()}}
+            log(json.dumps(row))
+            rows.append(row)
+        res.append({"params": prm, "horizons": rows})
+        for c in (fctx, pctx, lctx, mctx):
             c.close()
     return res
 
@@ -365,6 +481,9 @@ def main(argv=None):
     ap.add_argument("--outputs", type=int, default=16)
     ap.add_argument("--spacing", type=int, default=40, help="fine steps between samples (>= 4)")
     ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--keep", type=float, default=1.0, help="fraction of the active faces kept per output")
+    ap.add_argument("--val-runs", type=int, default=2, help="runs of the validation / held-out face set")
     ap.add_argument("--tests", type=int, default=2)
     ap.add_argument("--minutes", type=float, default=30.0)
     ap.add_argument("--out", default="gpurun_out/closure")
@@ -384,15 +503,27 @@ def main(argv=None):
         logf.write(s + "\n")
         logf.flush()
 
-    data, t_gen = generate(args.runs, args.outputs, args.spacing, log=log)
+    data, t_gen = generate(args.runs, args.outputs, args.spacing, keep_active=args.keep, log=log)
+    # samples of other runs: validation for the choice of epoch, and the
+    # held-out face errors reported below
+    held, _ = generate(args.val_runs, args.outputs, args.spacing, seed=907, keep_active=args.keep, log=log)
     base = baseline_loss(data)
-    P, hist, t_train = train(data, args.epochs, log=log)
+    P, hist, t_train = train(data, args.epochs, lr=args.lr, val=held, log=log)
     np.save(os.path.join(args.out, "params.npy"), P.cpu().numpy())
+    n_samples = int(data[0].shape[0])
+    faces_train = face_errors(P, [a[: min(a.shape[0], 1 << 24)] for a in data])
+    del data
+    torch.cuda.empty_cache()
+    faces = face_errors(P, held)
+    log(json.dumps({"held_out_face_errors": faces, "training_face_errors": faces_train}))
+    del held
+    torch.cuda.empty_cache()
     ev = evaluate(P, args.tests, args.minutes, log=log)
-    rep = {"samples": int(data[0].shape[0]), "data_gpu_seconds": t_gen, "train_gpu_seconds": t_train,
-           "loss_5th_order_start": base, "loss_final": hist[-1], "loss_history": hist,
+    rep = {"samples": n_samples, "data_gpu_seconds": t_gen, "train_gpu_seconds": t_train,
+           "loss_5th_order_start": base, "loss_final": hist["train"][-1], "loss_history": hist,
+           "held_out_face_errors": faces, "training_face_errors": faces_train,
            "grids": {"fine": FINE, "coarse": COARSE, "plain_2x": MID}, "runs": args.runs,
-           "outputs_per_run": args.outputs, "evaluation": ev}
+           "outputs_per_run": args.outputs, "epochs": args.epochs, "evaluation": ev}
     json.dump(rep, open(os.path.join(args.out, "report.json"), "w"), indent=1)
     log(json.dumps({k: v for k, v in rep.items() if k != "loss_history"}))
     return 0

@@ -254,11 +254,11 @@ int cm1g_ensemble_launch_count(cm1g_ens_t *ens, int64_t *kernels_per_step);
 int cm1g_ensemble_destroy(cm1g_ens_t *ens);
 
 /* Learned coarse-grid advection closure (no counterpart in the reference).
- * A 7 -> 64 -> 64 -> 6 GELU MLP with BF16 weights and FP32 accumulation
+ * A 7 -> 64 -> 64 -> 6 ReLU MLP with BF16 weights and FP32 accumulation
  * predicts the six coefficients (projected to sum to 1) of the face value
  * of theta's horizontal faces from the face's upwind-ordered six-point
  * stencil (normalised) and its Courant number; where the face value leaves
- * the range of the two cells sharing the face, WENO5 is used.  params is an
+ * the range of the four stencil cells nearest the face, WENO5 is used.  params is an
  * FP32 array of cm1g_mlp_param_count() values: W1[8][64], b1[64],
  * W2[64][64], b2[64], W3[64][8], b3[8].  The building blocks below take
  * device pointers and the caller's stream:
@@ -270,7 +270,10 @@ int cm1g_ensemble_destroy(cm1g_ens_t *ens);
  *   mlp_backward: grad += d loss / d params from dy = d loss / d y;
  *   closure_loss: *loss += sum_f w (phi_f - target_f)^2, dy of it;
  *   adam: one Adam step on params with grad * grad_scale;
- *   face_phi: phi[f] = m + d sum_k c_k x_k, or NaN outside the bounds.
+ *   face_phi: phi[f] = m + d sum_k c_k x_k, or NaN outside the range of
+ *     stencil cells 2..5 (two on each side of the face);
+ *   closure_faces: features -> forward -> face_phi in one kernel, the same
+ *     phi[f] bit for bit (the form the large step runs).
  * cm1g_closure_set turns the closure on (enable=1) for theta in the
  * context's large step; cm1g_capture_fluxes records theta's final-stage
  * x/y face fluxes and face mass fluxes (u-/v-array layout, device arrays;
@@ -289,6 +292,9 @@ int cm1g_face_features(int32_t ni, int32_t nj, int32_t nk, int32_t ngxy, int32_t
                        float *u, void *stream);
 int cm1g_face_phi(int64_t nf, const float *x, const float *c, const float *m, const float *d, float *phi,
                   void *stream);
+int cm1g_closure_faces(int32_t ni, int32_t nj, int32_t nk, int32_t ngxy, int32_t dir, const float *s,
+                       const float *th0, int32_t sadd, const float *vel, float dtdx, const float *params,
+                       float *phi, void *stream);
 int cm1g_closure_set(cm1g_ctx_t *ctx, const float *params, int32_t enable);
 int cm1g_capture_fluxes(cm1g_ctx_t *ctx, float *fx, float *fy, float *rx, float *ry);
 
@@ -313,6 +319,37 @@ int cm1g_capture_fluxes(cm1g_ctx_t *ctx, float *fx, float *fy, float *rx, float 
 int cm1g_pdefq_noalloc(const cm1g_config_t *cfg, float rmax, double *asq,
                        const float *ruh, const float *rvh, const float *rmh,
                        const float *rho, float *q3d, void *stream);
+
+/* Launch shapes of the large step.  This has no counterpart in the
+ * reference (its loops have no launch shapes).  adv_shape and mom_shape
+ * index the tile-shape table of the scalar and momentum passes
+ * (cm1g_tile_shape: x and y threads of a block, levels per block);
+ * sound_form selects the acoustic kernel: -1 automatic (by the number of
+ * columns), 0 tile form with 8 warps over the levels of 32 columns, 1 the
+ * same with 4 warps, 2 column sweep with 32 x 4 columns per block, 3 column
+ * sweep with 32 x 2.  step_ms is the measured large-step time of the
+ * configuration (cm1g_autotune; 0 when not measured). */
+typedef struct cm1g_tune {
+  int32_t adv_shape, mom_shape, sound_form;
+  float step_ms;
+} cm1g_tune_t;
+
+/* shape[0..2] = x threads, y threads, levels per block of tile shape
+ * `index`; CM1G_ERR_ARG past the end of the table. */
+int cm1g_tile_shape(int32_t index, int32_t shape[3]);
+int cm1g_set_tune(cm1g_ctx_t *ctx, const cm1g_tune_t *tune);
+int cm1g_get_tune(cm1g_ctx_t *ctx, cm1g_tune_t *tune);
+
+/* Autotuner: times the candidate launch shapes of this grid on a scratch
+ * copy of st (st itself is left unchanged; device or host pointers), each
+ * as `reps` replays of the captured large step after one untimed replay,
+ * one choice at a time (acoustic form, then scalar tile, then momentum
+ * tile), and keeps the fastest on the context.  Results are cached per
+ * device, grid shape and configuration: in the process, and, when
+ * cache_path is not NULL, in that text file (one line per entry); a cached
+ * entry is applied without timing.  out (may be NULL) receives the choice. */
+int cm1g_autotune(cm1g_ctx_t *ctx, float dt, double mass1, const cm1g_state_t *st, int32_t reps,
+                  const char *cache_path, cm1g_tune_t *out);
 
 #ifdef __cplusplus
 }

@@ -17,7 +17,6 @@ P_B2 = P_W2 + H * H
 P_W3 = P_B2 + H
 P_B3 = P_W3 + H * OUT
 P_TOTAL = P_B3 + OUT
-SQRT1_2 = 0.70710678
 
 
 def bf16(a):
@@ -40,26 +39,20 @@ def unpack_f64(p):
             p[P_W3:P_B3].reshape(H, OUT), p[P_B3:P_TOTAL])
 
 
-def _erf(x):
-    from math import erf
-    return np.vectorize(erf)(x)
+def act(z):
+    """ReLU, the hidden activation."""
+    return np.maximum(np.asarray(z, np.float64), 0.0)
 
 
-def gelu(z):
-    z = np.asarray(z, np.float64)
-    return 0.5 * z * (1.0 + _erf(z * SQRT1_2))
-
-
-def gelu_grad(z):
-    z = np.asarray(z, np.float64)
-    return 0.5 * (1.0 + _erf(z * SQRT1_2)) + z * np.exp(-0.5 * z * z) * 0.39894228
+def act_grad(z):
+    return (np.asarray(z, np.float64) > 0.0).astype(np.float64)
 
 
 def init_params(seed=0):
     rng = np.random.default_rng(seed)
     p = np.zeros(P_TOTAL, np.float32)
-    p[P_W1:P_B1] = (rng.normal(0, 1 / np.sqrt(7), (IN, H)) * (np.arange(IN) < 7)[:, None]).ravel()
-    p[P_W2:P_B2] = rng.normal(0, 1 / np.sqrt(H), H * H)
+    p[P_W1:P_B1] = (rng.normal(0, np.sqrt(2.0 / 7), (IN, H)) * (np.arange(IN) < 7)[:, None]).ravel()
+    p[P_W2:P_B2] = rng.normal(0, np.sqrt(2.0 / H), H * H)
     w3 = rng.normal(0, 0.01, (H, OUT))
     w3[:, NC:] = 0
     p[P_W3:P_B3] = w3.ravel()
@@ -86,10 +79,10 @@ def forward(p, x, z1=None, z2=None, rounding=True):
     xb = _rnd(x, rounding)
     if z1 is None:
         z1 = xb @ _rnd(W1, rounding) + b1
-    h1 = _rnd(gelu(z1), rounding)
+    h1 = _rnd(act(z1), rounding)
     if z2 is None:
         z2 = h1 @ _rnd(W2, rounding) + b2
-    h2 = _rnd(gelu(z2), rounding)
+    h2 = _rnd(act(z2), rounding)
     y = h2 @ _rnd(W3, rounding) + b3
     y[:, NC:] = 0.0
     c = y[:, :NC] + (1.0 - y[:, :NC].sum(1, keepdims=True)) / 6.0
@@ -115,17 +108,17 @@ def backward(p, x, z1, z2, dy, rounding=True):
     x = np.asarray(x, np.float64).copy()
     x[:, 7] = 0.0
     xb = _rnd(x, rounding)
-    h1 = _rnd(gelu(z1), rounding)
-    h2 = _rnd(gelu(z2), rounding)
+    h1 = _rnd(act(z1), rounding)
+    h2 = _rnd(act(z2), rounding)
     dy = np.asarray(dy, np.float64).copy()
     dy[:, NC:] = 0.0
     g = np.zeros(P_TOTAL, np.float64)
     g[P_W3:P_B3] = (h2.T @ dy).ravel()
     g[P_B3:P_TOTAL] = dy.sum(0)
-    dz2 = (dy @ _rnd(W3, rounding).T) * gelu_grad(z2)
+    dz2 = (dy @ _rnd(W3, rounding).T) * act_grad(z2)
     g[P_W2:P_B2] = (h1.T @ dz2).ravel()
     g[P_B2:P_W3] = dz2.sum(0)
-    dz1 = (dz2 @ _rnd(W2, rounding).T) * gelu_grad(z1)
+    dz1 = (dz2 @ _rnd(W2, rounding).T) * act_grad(z1)
     g[P_W1:P_B1] = (xb.T @ dz1).ravel()
     g[P_B1:P_W2] = dz1.sum(0)
     return g

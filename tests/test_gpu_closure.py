@@ -52,10 +52,10 @@ def test_forward_and_backward_match_reference(cm1g):
     yr, cr, _, z2r = R.forward(p, x, z1=z1g)
     assert np.abs(z2g - z2r).max() <= 1e-5 * max(1.0, np.abs(z2r).max())
     yr, cr, _, _ = R.forward(p, x, z1=z1g, z2=z2g)
-    # the GPU's float32 GELU and the reference's float64 GELU can land on
-    # opposite sides of a BF16 rounding tie (one BF16 ulp of an activation)
-    assert np.abs(Y.cpu().numpy() - yr).max() <= 1e-3 * max(1.0, np.abs(yr).max())
-    assert np.abs(Cc.cpu().numpy() - cr).max() <= 1e-3 * max(1.0, np.abs(cr).max())
+    # ReLU is exact on both sides; what remains is the FP32 accumulation
+    # order of the tensor-core products against the float64 reference
+    assert np.abs(Y.cpu().numpy() - yr).max() <= 1e-5 * max(1.0, np.abs(yr).max())
+    assert np.abs(Cc.cpu().numpy() - cr).max() <= 1e-5 * max(1.0, np.abs(cr).max())
     assert np.allclose(Cc.cpu().numpy().sum(1), 1.0, atol=1e-5)
 
     # loss and dy
@@ -126,9 +126,45 @@ def test_face_features_match_numpy(cm1g):
                 f += 1
 
 
+def test_fused_faces_equal_the_three_passes(cm1g):
+    """cm1g_closure_faces (features, MLP and bounded face value in one
+    kernel) gives the same phi as face_features -> mlp_forward -> face_phi,
+    NaN (WENO5 fallback) at the same faces."""
+    torch = _torch()
+    L = cm1g.lib()
+    case = make_case("dry_bubble", ni=37, nj=29, nk=11)
+    lay, st, gr = case.lay, case.state, case.grid
+    rng = np.random.default_rng(9)
+    th = (st["th3d"] + rng.normal(0, 0.5, lay.shape(1))).astype(np.float32)
+    p = R.init_params(4)
+    p[R.P_W3:R.P_B3] = rng.normal(0, 0.05, R.H * R.OUT).astype(np.float32)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+    TH, TH0, P = dev(th), dev(gr["th0"][:, 3, 3].copy()), dev(p)
+    for dir_ in (0, 1):
+        vel = rng.normal(0, 5, lay.shape(2 if dir_ == 0 else 3)).astype(np.float32)
+        VEL = dev(vel)
+        nf = (lay.ni + 1) * lay.nj * lay.nk if dir_ == 0 else lay.ni * (lay.nj + 1) * lay.nk
+        X, M, D, U = (torch.zeros(nf, 8, device="cuda"), torch.zeros(nf, device="cuda"),
+                      torch.zeros(nf, device="cuda"), torch.zeros(nf, device="cuda"))
+        Y, Cc = torch.zeros(nf, 8, device="cuda"), torch.zeros(nf, 6, device="cuda")
+        PHI3, PHI1 = torch.zeros(nf, device="cuda"), torch.full((nf,), 7.0, device="cuda")
+        cm1g.check(L.cm1g_face_features(lay.ni, lay.nj, lay.nk, 3, dir_, _p(TH), _p(TH0), 1, _p(VEL), 0.2,
+                                        _p(X), _p(M), _p(D), _p(U), None))
+        cm1g.check(L.cm1g_mlp_forward(_p(P), nf, _p(X), _p(Y), _p(Cc), None, None, None))
+        cm1g.check(L.cm1g_face_phi(nf, _p(X), _p(Cc), _p(M), _p(D), _p(PHI3), None))
+        cm1g.check(L.cm1g_closure_faces(lay.ni, lay.nj, lay.nk, 3, dir_, _p(TH), _p(TH0), 1, _p(VEL), 0.2,
+                                        _p(P), _p(PHI1), None))
+        torch.cuda.synchronize()
+        a, b = PHI3.cpu().numpy(), PHI1.cpu().numpy()
+        assert np.array_equal(np.isnan(a), np.isnan(b))
+        ok = ~np.isnan(a)
+        assert ok.mean() > 0.3 and (~ok).any()       # both outcomes occur
+        assert np.array_equal(a[ok], b[ok])
+
+
 def test_closure_in_the_step(cm1g):
     """With the closure on, theta's horizontal faces come from the MLP where
-    they stay inside the bounds of the two neighbouring cells; the step stays
+    they stay inside the range of the four nearest stencil cells; the step stays
     finite and close to the plain step; turning it off restores the plain step
     bit for bit."""
     torch = _torch()
