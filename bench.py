@@ -185,7 +185,7 @@ def run_ensemble(args):
     tunes = []
     if not args.no_tune:
         for ctx, st, c in zip(ctxs, dev, members):
-            tunes.append(ctx.autotune(st, c.dt, c.mass1, reps=3))
+            tunes.append(ctx.autotune(st, c.dt, c.mass1, reps=3, cache=args.tune_cache))
     ens = binding.Ensemble(ctxs)
     dts, m1 = [c.dt for c in members], [c.mass1 for c in members]
     for _ in range(args.warmup):
@@ -252,6 +252,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of the autotuner's")
+    ap.add_argument("--tune-cache", default=None,
+                    help="text file of autotuner results per grid (read if present, appended otherwise)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -281,7 +283,7 @@ def main():
     dev = binding.to_device(case.state)
     torch.cuda.synchronize()
     # ---- launch shapes for this grid (timed on a copy of the state, untimed here)
-    tune = None if args.no_tune else ctx.autotune(dev, case.dt, case.mass1, reps=3)
+    tune = None if args.no_tune else ctx.autotune(dev, case.dt, case.mass1, reps=3, cache=args.tune_cache)
 
     # ---- device-resident throughput (graph replay)
     with torch.cuda.stream(stream):

@@ -78,8 +78,10 @@ def lib():
     L.cm1g_adam.argtypes = [C.c_int32, _P, _P, _P, _P, C.c_int32, C.c_float, C.c_float, C.c_void_p]
     L.cm1g_face_features.argtypes = [C.c_int32] * 5 + [_P, _P, C.c_int32, _P, C.c_float, _P, _P, _P, _P,
                                                          C.c_void_p]
-    L.cm1g_face_phi.argtypes = [C.c_int64, _P, _P, _P, _P, _P, C.c_void_p]
-    L.cm1g_closure_faces.argtypes = [C.c_int32] * 5 + [_P, _P, C.c_int32, _P, C.c_float, _P, _P, C.c_void_p]
+    L.cm1g_face_phi.argtypes = [C.c_int64, _P, _P, _P, _P, C.c_float, _P, C.c_void_p]
+    L.cm1g_closure_faces.argtypes = [C.c_int32] * 5 + [_P, _P, C.c_int32, _P, C.c_float, _P, C.c_float, _P,
+                                                       C.c_void_p]
+    L.cm1g_closure_bounds.argtypes = [ctxp, C.c_float]
     L.cm1g_closure_set.argtypes = [ctxp, _P, C.c_int32]
     L.cm1g_capture_fluxes.argtypes = [ctxp, _P, _P, _P, _P]
     L.cm1g_pdefq_noalloc.argtypes = [cfgp, C.c_float, C.POINTER(C.c_double), _P, _P, _P, _P, _P, C.c_void_p]
@@ -215,9 +217,12 @@ class Context:
                                        ptr(thavg), ptr(ua), ptr(va), ptr(wa), ptr(tha), ptr(uten1), ptr(vten1),
                                        ptr(wten1), ptr(thten1), ptr(qten), ptr(ptten)))
 
-    def closure(self, params, enable=True):
-        """Learned closure of theta's horizontal faces on/off (params: FP32 array)."""
+    def closure(self, params, enable=True, widen=None):
+        """Learned closure of theta's horizontal faces on/off (params: FP32
+        array); widen sets the bounds of the face values (cm1g_closure_bounds)."""
         check(lib().cm1g_closure_set(self.h, ptr(params), 1 if enable else 0))
+        if widen is not None:
+            check(lib().cm1g_closure_bounds(self.h, widen))
 
     def capture_fluxes(self, fx=None, fy=None, rx=None, ry=None):
         check(lib().cm1g_capture_fluxes(self.h, ptr(fx), ptr(fy), ptr(rx), ptr(ry)))

@@ -23,7 +23,7 @@ void launch_bc_batch(const DGrid &g, float *const *arrays, const int *which, con
                      cudaStream_t st, int64_t *nlaunch);
 void launch_tend_init(const DGrid &g, const TendIn &t, cudaStream_t st, int64_t *nl);
 void launch_closure_faces(int ni, int nj, int nk, int ngxy, int dir, const float *s, const float *th0, int sadd,
-                          const float *vel, float dtdx, const float *params, float *phi, cudaStream_t st);
+                          const float *vel, float dtdx, const float *params, float widen, float *phi, cudaStream_t st);
 int mlp_param_count();
 int ener_chunks(const DGrid &g);
 void launch_calcener(const DGrid &g, const EnerIn &e, double *part, double *out, cudaStream_t st, int64_t *nl);
@@ -148,6 +148,7 @@ struct cm1g_ctx {
   bool cl_on = false;
   float *cl_params = nullptr;
   float *cl_phi[2] = {};
+  float cl_widen = 0.0f;                      // widening of the face-value bounds (cm1g_closure_bounds)
   long cl_nf[2] = {0, 0};
   // capture of theta's final-stage face fluxes (cm1g_capture_fluxes)
   float *cap_fx = nullptr, *cap_fy = nullptr, *cap_rx = nullptr, *cap_ry = nullptr;
@@ -473,7 +474,7 @@ static void closure_phi(cm1g_ctx *c, const float *th, float dt, cudaStream_t st,
   for (int dir = 0; dir < 2; dir++) {
     ProfScope _ps("k_closure_faces", st);
     launch_closure_faces(g.ni, g.nj, g.nk, g.ngxy, dir, th, g.th0, 1, dir ? c->rrv : c->rru,
-                         dt * (dir ? g.rdy : g.rdx), c->cl_params, c->cl_phi[dir], st);
+                         dt * (dir ? g.rdy : g.rdx), c->cl_params, c->cl_widen, c->cl_phi[dir], st);
     if (nl) *nl += 1;
   }
 }
@@ -1090,6 +1091,17 @@ extern "C" int cm1g_closure_set(cm1g_ctx_t *c, const float *params, int32_t enab
                         c->stream));
   CUCHK(cudaStreamSynchronize(c->stream));
   c->cl_on = true;
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_closure_bounds(cm1g_ctx_t *c, float widen) {
+  if (!c) return set_err(CM1G_ERR_STATE, "null context");
+  if (!(widen >= 0.0f) || !std::isfinite(widen)) return set_err(CM1G_ERR_ARG, "widen must be finite and >= 0");
+  if (widen != c->cl_widen) {
+    drop_graph(c);
+    c->gen++;
+  }
+  c->cl_widen = widen;
   return CM1G_OK;
 }
 

@@ -351,9 +351,10 @@ __global__ void k_face_features(int ni, int nj, int nk, int ngxy, int dir, const
 }
 
 // p where it lies within the range of the stencil cells 2..5 (the two
-// cells on each side of the face; tolerance 1e-6 of the stencil's scale),
-// else NaN (the scalar kernel then takes the WENO5 value).
-__device__ __forceinline__ float bounded_face(float p, float m, float d, const float *x) {
+// cells on each side of the face), widened on both sides by `widen` times
+// the stencil's scale d (plus a tolerance of 1e-6 d), else NaN (the scalar
+// kernel then takes the WENO5 value).  widen = 0 is the strict check.
+__device__ __forceinline__ float bounded_face(float p, float m, float d, const float *x, float widen) {
   float lo = m + d * x[1], hi = lo;
 #pragma unroll
   for (int q = 2; q <= 4; q++) {
@@ -361,20 +362,20 @@ __device__ __forceinline__ float bounded_face(float p, float m, float d, const f
     lo = fminf(lo, v);
     hi = fmaxf(hi, v);
   }
-  const float tol = 1e-6f * d;
+  const float tol = (1e-6f + widen) * d;
   return (p >= lo - tol && p <= hi + tol) ? p : __int_as_float(0x7fc00000);
 }
 
 // Face value from the coefficients, bounded as above.
 __global__ void k_face_phi(long nf, const float *__restrict__ x, const float *__restrict__ c, const float *__restrict__ m,
-                           const float *__restrict__ dsc, float *phi) {
+                           const float *__restrict__ dsc, float widen, float *phi) {
   const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= nf) return;
   float acc = 0.f;
 #pragma unroll
   for (int q = 0; q < MLP_NC; q++) acc += c[f * MLP_NC + q] * x[f * MLP_IN + q];
   const float p = m[f] + dsc[f] * acc;
-  phi[f] = bounded_face(p, m[f], dsc[f], x + f * MLP_IN);
+  phi[f] = bounded_face(p, m[f], dsc[f], x + f * MLP_IN, widen);
 }
 
 // The closure's face values in one pass: for 32 faces per warp, the
@@ -394,7 +395,8 @@ __global__ void __launch_bounds__(CF_WARPS * 32) k_closure_faces(int ni, int nj,
                                                                 const float *__restrict__ s,
                                                                 const float *__restrict__ th0, int sadd,
                                                                 const float *__restrict__ vel, float dtdx,
-                                                                const float *__restrict__ params, float *phi) {
+                                                                const float *__restrict__ params, float widen,
+                                                                float *phi) {
   __shared__ MlpSmem S;
   __shared__ FaceTile T[CF_WARPS];
   load_weights(S, params);
@@ -463,7 +465,7 @@ __global__ void __launch_bounds__(CF_WARPS * 32) k_closure_faces(int ni, int nj,
           for (int q = 0; q < MLP_NC; q++) acc += cc[q] * F.x[row][q];
           const float mr = F.m[row], dr = F.d[row];
           const float p = mr + dr * acc;
-          phi[fr] = bounded_face(p, mr, dr, F.x[row]);
+          phi[fr] = bounded_face(p, mr, dr, F.x[row], widen);
         }
       }
     }
@@ -496,18 +498,18 @@ void launch_face_features(int ni, int nj, int nk, int ngxy, int dir, const float
   k_face_features<<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(ni, nj, nk, ngxy, dir, s, th0, sadd, vel, dtdx, x, m,
                                                                  d, u);
 }
-void launch_face_phi(long nf, const float *x, const float *c, const float *m, const float *d, float *phi,
+void launch_face_phi(long nf, const float *x, const float *c, const float *m, const float *d, float widen, float *phi,
                      cudaStream_t st) {
-  k_face_phi<<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(nf, x, c, m, d, phi);
+  k_face_phi<<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(nf, x, c, m, d, widen, phi);
 }
 void launch_closure_faces(int ni, int nj, int nk, int ngxy, int dir, const float *s, const float *th0, int sadd,
-                          const float *vel, float dtdx, const float *params, float *phi, cudaStream_t st) {
+                          const float *vel, float dtdx, const float *params, float widen, float *phi, cudaStream_t st) {
   const long nf = (long)((dir == 0) ? ni + 1 : ni) * ((dir == 0) ? nj : nj + 1) * nk;
   const long tiles = (nf + 31) / 32;
   const long blocks = std::min<long>((tiles + CF_WARPS - 1) / CF_WARPS, 148L * 8);
   if (blocks > 0)
     k_closure_faces<<<(unsigned)blocks, CF_WARPS * 32, 0, st>>>(ni, nj, nk, ngxy, dir, s, th0, sadd, vel, dtdx, params,
-                                                                 phi);
+                                                                 widen, phi);
 }
 int mlp_param_count() { return P_TOTAL; }
 
@@ -531,11 +533,11 @@ extern "C" int32_t cm1g_mlp_param_count(void) { return cm1g::P_TOTAL; }
 
 extern "C" int cm1g_closure_faces(int32_t ni, int32_t nj, int32_t nk, int32_t ngxy, int32_t dir, const float *s,
                                   const float *th0, int32_t sadd, const float *vel, float dtdx, const float *params,
-                                  float *phi, void *stream) {
+                                  float widen, float *phi, void *stream) {
   if (!s || !vel || !params || !phi || (sadd && !th0) || (dir != 0 && dir != 1) || ni < 1 || nj < 1 || nk < 1 ||
-      ngxy < 3)
+      ngxy < 3 || !(widen >= 0.0f))
     return bad("cm1g_closure_faces: bad argument");
-  cm1g::launch_closure_faces(ni, nj, nk, ngxy, dir, s, th0, sadd, vel, dtdx, params, phi, (cudaStream_t)stream);
+  cm1g::launch_closure_faces(ni, nj, nk, ngxy, dir, s, th0, sadd, vel, dtdx, params, widen, phi, (cudaStream_t)stream);
   return after_launch();
 }
 
@@ -576,9 +578,9 @@ extern "C" int cm1g_face_features(int32_t ni, int32_t nj, int32_t nk, int32_t ng
   return after_launch();
 }
 
-extern "C" int cm1g_face_phi(int64_t nf, const float *x, const float *c, const float *m, const float *d, float *phi,
-                             void *stream) {
-  if (!x || !c || !m || !d || !phi || nf < 0) return bad("cm1g_face_phi: null argument");
-  if (nf) cm1g::launch_face_phi((long)nf, x, c, m, d, phi, (cudaStream_t)stream);
+extern "C" int cm1g_face_phi(int64_t nf, const float *x, const float *c, const float *m, const float *d, float widen,
+                             float *phi, void *stream) {
+  if (!x || !c || !m || !d || !phi || nf < 0 || !(widen >= 0.0f)) return bad("cm1g_face_phi: bad argument");
+  if (nf) cm1g::launch_face_phi((long)nf, x, c, m, d, widen, phi, (cudaStream_t)stream);
   return after_launch();
 }

@@ -351,7 +351,7 @@ def weno5_faces(v, weps=1e-17):
     return (a1 * q1 + a2 * q2 + a3 * q3) / (a1 + a2 + a3)
 
 
-def face_errors(P, data, chunk=1 << 22):
+def face_errors(P, data, widens=(0.0, 1.0), chunk=1 << 22):
     """Weighted mean squared error of the coarse face values against the
     fine-run targets, for the 5th-order upwind weights, WENO5, the network,
     and the network with the WENO5 fallback outside the neighbour bounds (the
@@ -377,15 +377,16 @@ def face_errors(P, data, chunk=1 << 22):
     phiw = weno5_faces(v)
     phil = md + dd * (c.double() * xd).sum(1)
     lo, hi = v[:, 1:5].min(1).values, v[:, 1:5].max(1).values
-    tol = 1e-6 * dd
-    inside = lambda phi: (phi >= lo - tol) & (phi <= hi + tol)
-    ins = inside(phil)
-    phib = torch.where(ins, phil, phiw)
     err = lambda phi: float((wd * (phi - td) ** 2).sum().item() / n)
-    frac_out = lambda phi: float(1.0 - inside(phi).double().mean().item())
-    return {"samples": int(n), "upwind5": err(phi5), "weno5": err(phiw), "learned": err(phil),
-            "learned_with_fallback": err(phib), "fallback_fraction": frac_out(phil),
-            "upwind5_outside_bounds": frac_out(phi5), "target_outside_bounds": frac_out(td)}
+    out = {"samples": int(n), "upwind5": err(phi5), "weno5": err(phiw), "learned": err(phil)}
+    for widen in widens:
+        tol = (1e-6 + widen) * dd
+        inside = lambda phi: (phi >= lo - tol) & (phi <= hi + tol)
+        frac_out = lambda phi: float(1.0 - inside(phi).double().mean().item())
+        out["widen_%g" % widen] = {"learned_with_fallback": err(torch.where(inside(phil), phil, phiw)),
+                                   "fallback_fraction": frac_out(phil), "upwind5_outside": frac_out(phi5),
+                                   "target_outside": frac_out(td)}
+    return out
 
 
 class _Run:
@@ -424,7 +425,7 @@ class _Run:
         return self.ms / 1e3 * self.steps / max(1, self.timed)
 
 
-def evaluate(P, tests, minutes, seed=77, horizons=(2, 10, 50), log=print):
+def evaluate(P, tests, minutes, seed=77, horizons=(2, 10, 50), widens=(0.0, 1.0), log=print):
     """Held-out runs: L2 of theta' against the coarsened fine run after
     `horizons` coarse steps and after `minutes`, for the coarse grid without
     and with the closure and for the plain method at twice the coarse
@@ -438,19 +439,23 @@ def evaluate(P, tests, minutes, seed=77, horizons=(2, 10, 50), log=print):
         fcase = member(FINE, seed + 100 * t, **prm)
         ccase = member(COARSE, seed + 100 * t + 1, **prm)
         mcase = member(MID, seed + 100 * t + 2, **prm)
-        fctx, pctx, lctx, mctx = (b.Context(c.cfg, c.grid) for c in (fcase, ccase, ccase, mcase))
-        lctx.closure(P)
+        fctx, pctx, mctx = (b.Context(c.cfg, c.grid) for c in (fcase, ccase, mcase))
+        lctx = {w: b.Context(ccase.cfg, ccase.grid) for w in widens}
+        for w, c in lctx.items():
+            c.closure(P, widen=w)
         fdev = b.to_device(fcase.state)
         # initial coarse/mid states from the fine initial state (same bubble, same shear)
         c_plain = coarse_state(fcase, fdev, ccase, pctx)
-        c_learn = {k: v.clone() for k, v in c_plain.items()}
+        c_learn = {w: {k: v.clone() for k, v in c_plain.items()} for w in widens}
         mdev = coarse_state(fcase, fdev, mcase, mctx, (2, 2, 2))
         m1c = coarse_mass(ccase, c_plain)
         runs = {"fine_plain_250m": _Run(fctx, fdev, fcase, fcase.mass1),
                 "coarse_plain": _Run(pctx, c_plain, ccase, m1c),
-                "coarse_learned": _Run(lctx, c_learn, ccase, m1c),
                 "plain_500m": _Run(mctx, mdev, mcase, coarse_mass(mcase, mdev))}
-        ratio = {"fine_plain_250m": FX, "coarse_plain": 1, "coarse_learned": 1, "plain_500m": 2}
+        ratio = {"fine_plain_250m": FX, "coarse_plain": 1, "plain_500m": 2}
+        for w in widens:
+            runs["coarse_learned_widen_%g" % w] = _Run(lctx[w], c_learn[w], ccase, m1c)
+            ratio["coarse_learned_widen_%g" % w] = 1
         total = int(round(minutes * 60 / ccase.dt))
         cl, ml = ccase.lay, mcase.lay
         ci = (slice(cl.kx(1), cl.kx(cl.nk) + 1), slice(cl.jx(1), cl.jx(cl.nj) + 1), slice(cl.ix(1), cl.ix(cl.ni) + 1))
@@ -463,14 +468,15 @@ def evaluate(P, tests, minutes, seed=77, horizons=(2, 10, 50), log=print):
             l2 = lambda a: float(torch.sqrt(((a - ref) ** 2).mean()).item())
             mth = mdev["th3d"][ml.kx(1):ml.kx(ml.nk) + 1, ml.jx(1):ml.jx(ml.nj) + 1, ml.ix(1):ml.ix(ml.ni) + 1]
             mth = mth.reshape(ml.nk, ml.nj // 2, 2, ml.ni // 2, 2).mean(dim=(2, 4))
-            row = {"coarse_steps": hz, "seconds": hz * ccase.dt,
-                   "l2_theta": {"coarse_plain": l2(c_plain["th3d"][ci]), "coarse_learned": l2(c_learn["th3d"][ci]),
-                                "plain_500m": l2(mth), "no_change": l2(torch.zeros_like(ref))},
+            l2s = {"coarse_plain": l2(c_plain["th3d"][ci]), "plain_500m": l2(mth), "no_change": l2(torch.zeros_like(ref))}
+            for w in widens:
+                l2s["coarse_learned_widen_%g" % w] = l2(c_learn[w]["th3d"][ci])
+            row = {"coarse_steps": hz, "seconds": hz * ccase.dt, "l2_theta": l2s,
                    "gpu_seconds": {k: r.gpu_seconds() for k, r in runs.items()}}
             log(json.dumps(row))
             rows.append(row)
         res.append({"params": prm, "horizons": rows})
-        for c in (fctx, pctx, lctx, mctx):
+        for c in [fctx, pctx, mctx] + list(lctx.values()):
             c.close()
     return res
 
@@ -484,6 +490,8 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--keep", type=float, default=1.0, help="fraction of the active faces kept per output")
     ap.add_argument("--val-runs", type=int, default=2, help="runs of the validation / held-out face set")
+    ap.add_argument("--params", default=None, help="evaluate these parameters (.npy) instead of training")
+    ap.add_argument("--widens", default="0,1", help="bound widenings of the face values to evaluate")
     ap.add_argument("--tests", type=int, default=2)
     ap.add_argument("--minutes", type=float, default=30.0)
     ap.add_argument("--out", default="gpurun_out/closure")
@@ -503,22 +511,29 @@ def main(argv=None):
         logf.write(s + "\n")
         logf.flush()
 
-    data, t_gen = generate(args.runs, args.outputs, args.spacing, keep_active=args.keep, log=log)
+    widens = tuple(float(w) for w in args.widens.split(","))
     # samples of other runs: validation for the choice of epoch, and the
     # held-out face errors reported below
     held, _ = generate(args.val_runs, args.outputs, args.spacing, seed=907, keep_active=args.keep, log=log)
-    base = baseline_loss(data)
-    P, hist, t_train = train(data, args.epochs, lr=args.lr, val=held, log=log)
+    if args.params:
+        # evaluate given parameters (no data generation, no training)
+        P = torch.from_numpy(np.load(args.params).astype(np.float32)).cuda()
+        t_gen = t_train = 0.0
+        base, hist, n_samples, faces_train = None, {"train": [None], "validation": []}, 0, None
+    else:
+        data, t_gen = generate(args.runs, args.outputs, args.spacing, keep_active=args.keep, log=log)
+        base = baseline_loss(data)
+        P, hist, t_train = train(data, args.epochs, lr=args.lr, val=held, log=log)
+        n_samples = int(data[0].shape[0])
+        faces_train = face_errors(P, [a[: min(a.shape[0], 1 << 24)] for a in data], widens)
+        del data
+        torch.cuda.empty_cache()
     np.save(os.path.join(args.out, "params.npy"), P.cpu().numpy())
-    n_samples = int(data[0].shape[0])
-    faces_train = face_errors(P, [a[: min(a.shape[0], 1 << 24)] for a in data])
-    del data
-    torch.cuda.empty_cache()
-    faces = face_errors(P, held)
+    faces = face_errors(P, held, widens)
     log(json.dumps({"held_out_face_errors": faces, "training_face_errors": faces_train}))
     del held
     torch.cuda.empty_cache()
-    ev = evaluate(P, args.tests, args.minutes, log=log)
+    ev = evaluate(P, args.tests, args.minutes, widens=widens, log=log)
     rep = {"samples": n_samples, "data_gpu_seconds": t_gen, "train_gpu_seconds": t_train,
            "loss_5th_order_start": base, "loss_final": hist["train"][-1], "loss_history": hist,
            "held_out_face_errors": faces, "training_face_errors": faces_train,

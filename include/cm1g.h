@@ -271,7 +271,8 @@ int cm1g_ensemble_destroy(cm1g_ens_t *ens);
  *   closure_loss: *loss += sum_f w (phi_f - target_f)^2, dy of it;
  *   adam: one Adam step on params with grad * grad_scale;
  *   face_phi: phi[f] = m + d sum_k c_k x_k, or NaN outside the range of
- *     stencil cells 2..5 (two on each side of the face);
+ *     stencil cells 2..5 (two on each side of the face) widened by
+ *     widen * d on each side (widen = 0: the strict range);
  *   closure_faces: features -> forward -> face_phi in one kernel, the same
  *     phi[f] bit for bit (the form the large step runs).
  * cm1g_closure_set turns the closure on (enable=1) for theta in the
@@ -290,12 +291,16 @@ int cm1g_adam(int32_t np, float *params, const float *grad, float *m1, float *m2
 int cm1g_face_features(int32_t ni, int32_t nj, int32_t nk, int32_t ngxy, int32_t dir, const float *s,
                        const float *th0, int32_t sadd, const float *vel, float dtdx, float *x, float *m, float *d,
                        float *u, void *stream);
-int cm1g_face_phi(int64_t nf, const float *x, const float *c, const float *m, const float *d, float *phi,
-                  void *stream);
+int cm1g_face_phi(int64_t nf, const float *x, const float *c, const float *m, const float *d, float widen,
+                  float *phi, void *stream);
 int cm1g_closure_faces(int32_t ni, int32_t nj, int32_t nk, int32_t ngxy, int32_t dir, const float *s,
                        const float *th0, int32_t sadd, const float *vel, float dtdx, const float *params,
-                       float *phi, void *stream);
+                       float widen, float *phi, void *stream);
 int cm1g_closure_set(cm1g_ctx_t *ctx, const float *params, int32_t enable);
+/* Bound of the closure's face values in the large step: the range of the
+ * four nearest stencil cells widened by widen * (stencil max - min) on each
+ * side (default 0). */
+int cm1g_closure_bounds(cm1g_ctx_t *ctx, float widen);
 int cm1g_capture_fluxes(cm1g_ctx_t *ctx, float *fx, float *fy, float *rx, float *ry);
 
 /* Largest ni*nj that cm1g_pdefq_noalloc accepts: its scratch array holds one

@@ -151,15 +151,22 @@ def test_fused_faces_equal_the_three_passes(cm1g):
         cm1g.check(L.cm1g_face_features(lay.ni, lay.nj, lay.nk, 3, dir_, _p(TH), _p(TH0), 1, _p(VEL), 0.2,
                                         _p(X), _p(M), _p(D), _p(U), None))
         cm1g.check(L.cm1g_mlp_forward(_p(P), nf, _p(X), _p(Y), _p(Cc), None, None, None))
-        cm1g.check(L.cm1g_face_phi(nf, _p(X), _p(Cc), _p(M), _p(D), _p(PHI3), None))
-        cm1g.check(L.cm1g_closure_faces(lay.ni, lay.nj, lay.nk, 3, dir_, _p(TH), _p(TH0), 1, _p(VEL), 0.2,
-                                        _p(P), _p(PHI1), None))
-        torch.cuda.synchronize()
-        a, b = PHI3.cpu().numpy(), PHI1.cpu().numpy()
-        assert np.array_equal(np.isnan(a), np.isnan(b))
-        ok = ~np.isnan(a)
-        assert ok.mean() > 0.3 and (~ok).any()       # both outcomes occur
-        assert np.array_equal(a[ok], b[ok])
+        for widen in (0.0, 0.5):
+            cm1g.check(L.cm1g_face_phi(nf, _p(X), _p(Cc), _p(M), _p(D), widen, _p(PHI3), None))
+            cm1g.check(L.cm1g_closure_faces(lay.ni, lay.nj, lay.nk, 3, dir_, _p(TH), _p(TH0), 1, _p(VEL), 0.2,
+                                            _p(P), widen, _p(PHI1), None))
+            torch.cuda.synchronize()
+            a, b = PHI3.cpu().numpy(), PHI1.cpu().numpy()
+            assert np.array_equal(np.isnan(a), np.isnan(b))
+            ok = ~np.isnan(a)
+            assert ok.mean() > 0.3 and (~ok).any()       # both outcomes occur
+            assert np.array_equal(a[ok], b[ok])
+            # the bound itself, from the features: within the widened range of stencil cells 2..5
+            x, m, d = X.cpu().numpy(), M.cpu().numpy(), D.cpu().numpy()
+            v = m[:, None].astype(np.float64) + d[:, None] * x[:, 1:5]
+            lo = v.min(1) - (1e-6 + widen) * d
+            hi = v.max(1) + (1e-6 + widen) * d
+            assert np.all((a[ok] >= lo[ok] - 1e-5 * d[ok]) & (a[ok] <= hi[ok] + 1e-5 * d[ok]))
 
 
 def test_closure_in_the_step(cm1g):
