@@ -37,6 +37,7 @@ class Config(C.Structure):
         ("testcase", C.c_int32), ("psolver", C.c_int32), ("terrain_flag", C.c_int32),
         ("axisymm", C.c_int32), ("icor", C.c_int32),
         ("qmag", C.c_float * CM1G_MAXQ),
+        ("idiff", C.c_int32), ("difforder", C.c_int32), ("mdiff", C.c_int32), ("kdiff6", C.c_float),
     ]
 
 

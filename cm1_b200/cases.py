@@ -221,7 +221,8 @@ WORKLOADS = {
 
 def make_case(name, seed=1234, **over):
     """Build a seeded workload.  `over` may override ni, nj, nk, dx, dz, dt,
-    nsound, advwenos, npt, bc, moist (for small parity cases)."""
+    nsound, advwenos, npt, bc, moist (for small parity cases), and add diff6
+    (kdiff6 of the 6th-order diffusion) and mdiff."""
     w = dict(WORKLOADS[name])
     w.update(over)
     ni, nj, nk = int(w["ni"]), int(w["nj"]), int(w["nk"])
@@ -246,6 +247,12 @@ def make_case(name, seed=1234, **over):
     cfg.testcase, cfg.psolver, cfg.terrain_flag, cfg.axisymm, cfg.icor = 0, 3, 0, 0, 0
     for q in range(CM1G_MAXQ):
         cfg.qmag[q] = 1.0e-2
+    # 6th-order horizontal diffusion inside advection (idiff=1, difforder=6):
+    # off unless `diff6` gives kdiff6 (the mdiff limiter with `mdiff`)
+    kd = w.get("diff6")
+    cfg.idiff, cfg.difforder = (1, 6) if kd is not None else (0, 6)
+    cfg.kdiff6 = float(kd) if kd is not None else 0.0
+    cfg.mdiff = int(w.get("mdiff", 0))
 
     # ---- grid metrics (uniform grid: param.F:7077-7081, 7459-7463, 7793-7802)
     f32 = np.float32

@@ -26,10 +26,12 @@ void launch_closure_faces(int ni, int nj, int nk, int ngxy, int dir, const float
                           const float *vel, float dtdx, const float *params, float widen, float *phi, cudaStream_t st);
 int mlp_param_count();
 int ener_chunks(const DGrid &g);
+void launch_recip_rho(const DGrid &g, const float *rho, float *rr, cudaStream_t st, int64_t *nl);
 void launch_calcener(const DGrid &g, const EnerIn &e, double *part, double *out, cudaStream_t st, int64_t *nl);
 void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w, const float *uten1,
                          const float *vten1, const float *wten1, float *uten, float *vten, float *wten,
-                         const float *th3d, const float *qv, float *divx, cudaStream_t st, int64_t *nl);
+                         const float *th3d, const float *qv, float *divx, cudaStream_t st, int64_t *nl,
+                         const Diff6 *diff = nullptr);
 void launch_advs(const DGrid &g, const float *rru, const float *rrv, const float *rrw, int weighted,
                  const float *divx, const float *s, const float *s0, int sadd, const float *ten1,
                  const float *thterm, float *sten_out, float *snew, int weno, int pdef, int pdefweno,
@@ -37,7 +39,7 @@ void launch_advs(const DGrid &g, const float *rru, const float *rrv, const float
 void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const float *rrw, const float *s,
                        const float *s0, int sadd, const float *ten1, const float *thterm, float *snew, int weno,
                        int pdef, int pdefweno, double weps, float dt, int flush, float *scratch, cudaStream_t st,
-                       int64_t *nl, const TileExtras *ex = nullptr);
+                       int64_t *nl, const TileExtras *ex = nullptr, const Diff6 *diff = nullptr);
 void launch_sound(const DGrid &g, int nsound, int nrk, float dt, const float *ua, float *u3d, const float *uten,
                   const float *va, float *v3d, const float *vten, const float *wa, float *w3d, const float *wten,
                   const float *ppi, float *pp3d, const float *piadv, const float *ppten, float *ppx,
@@ -144,6 +146,7 @@ struct cm1g_ctx {
   float *sx[2 * (1 + 2 * CM1G_MAXQ)] = {};   // per-scalar stage buffers
   float *pdefscr = nullptr;                   // 6 s-arrays
   float *mdivx = nullptr;                     // divx of the momentum pass
+  float *rr = nullptr;                        // 1/rho as solve2 keeps it (6th-order diffusion)
   // learned closure of theta's horizontal faces (cm1g_closure_set)
   bool cl_on = false;
   float *cl_params = nullptr;
@@ -236,6 +239,10 @@ static int check_config(const cm1g_config_t *c) {
     return set_err(CM1G_ERR_UNSUPPORTED, "moisture: water vapour only (numq=1, nqv=1)");
   if (c->iptra && (c->npt < 0 || c->npt > CM1G_MAXQ)) return set_err(CM1G_ERR_ARG, "npt out of range");
   if (c->roflux != 0) return set_err(CM1G_ERR_UNSUPPORTED, "roflux=1 is not built");
+  if (c->idiff != 0 && c->difforder != 6)
+    return set_err(CM1G_ERR_UNSUPPORTED, "diffusion: only the 6th-order form (difforder=6) is built");
+  if (c->idiff < 0 || c->idiff > 1) return set_err(CM1G_ERR_UNSUPPORTED, "idiff must be 0 or 1");
+  if (c->idiff && !(c->kdiff6 >= 0.0f)) return set_err(CM1G_ERR_ARG, "kdiff6 must be >= 0");
   bool open = c->wbc == 2 || c->ebc == 2 || c->sbc == 2 || c->nbc == 2;
   if (open && c->irbc != 4) return set_err(CM1G_ERR_UNSUPPORTED, "open boundaries need irbc=4");
   for (int b : {c->wbc, c->ebc, c->sbc, c->nbc})
@@ -329,6 +336,7 @@ extern "C" int cm1g_init(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_c
   bool pdef_needed = cfg->imoist || (cfg->iptra && cfg->pdtra);
   c->pdefscr = (float *)dalloc(c, (pdef_needed ? 6 : 6) * bS);
   c->mdivx = (float *)dalloc(c, bS);
+  if (cfg->idiff == 1) c->rr = (float *)dalloc(c, bS);
   c->ener = (double *)dalloc(c, ((size_t)4 * g.nk * ener_chunks(g) + 8) * sizeof(double));
   // base-state winds (full u/v arrays) for the Rayleigh damping of cm1g_tendency_init
   if (gr->u0 && gr->v0) {
@@ -498,6 +506,14 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
   auto buf_in = [&](int s, int nrk) -> float * { return nrk == 1 ? s3d[s] : c->sx[2 * s + (nrk - 2)]; };
   auto buf_out = [&](int s, int nrk) -> float * { return nrk == 3 ? s3d[s] : c->sx[2 * s + (nrk - 1)]; };
   const int iqv = cf.nqv;  // scalar index of qv
+  // 6th-order diffusion (solve2.F:1393, 1475, 1847, 1940): rho at the start of
+  // every stage, rr = 1/rho as solve3 left it, updated after stages 1 and 2
+  const bool diffit = cf.idiff == 1 && cf.difforder == 6;
+  Diff6 df;
+  if (diffit) {
+    df.rho = d->rho; df.ri = c->rr; df.mdiff = cf.mdiff;
+    launch_recip_rho(g, d->rho, c->rr, st, nl);
+  }
 
   for (int nrk = 1; nrk <= 3; nrk++) {
     const float dttmp = dt / (float)(3 + 1 - nrk);
@@ -505,8 +521,9 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
     const float *qv_in = cf.imoist ? buf_in(iqv, nrk) : nullptr;
     launch_stage_prep(g, th_in, d->pp3d, qv_in, cf.imoist, cf.eqtset, c->t11, c->t22, c->thterm, c->piadv, st, nl);
     launch_bc(g, c->t11, 2, 0, st, nl);
+    if (diffit) df.coef = cf.kdiff6 / 64.0f / dttmp;   // adv.F:80-82, 962-964
     launch_adv_momentum(g, d->u3d, d->v3d, d->w3d, d->uten1, d->vten1, d->wten1, c->uten, c->vten, c->wten,
-                        th_in, qv_in, c->mdivx, st, nl);
+                        th_in, qv_in, c->mdivx, st, nl, diffit ? &df : nullptr);
     launch_sound(g, cf.nsound, nrk, dt, d->ua, d->u3d, c->uten, d->va, d->v3d, c->vten, d->wa, d->w3d, c->wten,
                  d->ppi, d->pp3d, c->piadv, d->ppten, d->ppx, c->t11, c->t22, c->rru, c->rrv, c->rrw,
                  d->radbcw, d->radbce, d->radbcs, d->radbcn, c->su, c->sv, c->su2, c->sv2, c->d1, c->d2, st, nl);
@@ -525,25 +542,31 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
     }
     launch_advs_tiled(g, c->rru, c->rrv, c->rrw, th_in, d->tha, 1, d->thten1,
                       (cf.imoist && cf.eqtset == 2) ? c->thterm : nullptr, buf_out(0, nrk), weno, 0, 0,
-                      (double)(10.0f * 1.0e-18f), dttmp, 1, c->pdefscr, st, nl, exp);
+                      (double)(10.0f * 1.0e-18f), dttmp, 1, c->pdefscr, st, nl, exp, diffit ? &df : nullptr);
     // moisture (solve2.F:1431-1530)
     for (int n = 0; n < numq; n++) {
       const int s = 1 + n;
       launch_advs_tiled(g, c->rru, c->rrv, c->rrw, buf_in(s, nrk), base[s], 0, ten1[s], nullptr, buf_out(s, nrk),
                         weno, nrk == 3 ? 1 : 0, (n + 1 == cf.nqv) ? 0 : 1, (double)(cf.qmag[n] * 1.0e-18f), dttmp, 1,
-                        c->pdefscr, st, nl);
+                        c->pdefscr, st, nl, nullptr, diffit ? &df : nullptr);
     }
-    // pressure, density, mass sums (solve2.F:1536-1656)
-    if (nrk == 3)
-      launch_prs_rho(g, d->pp3d, buf_out(0, 3), cf.imoist ? buf_out(iqv, 3) : nullptr, cf.imoist, d->prs, d->rho,
-                     c->part3, c->part4, cf.apmasscon == 1, st, nl);
+    // pressure, density, mass sums (solve2.F:1536-1656; every stage with the
+    // 6th-order diffusion, solve2.F:1582, 1599)
+    if (nrk == 3 || diffit)
+      launch_prs_rho(g, d->pp3d, buf_out(0, nrk), cf.imoist ? buf_out(iqv, nrk) : nullptr, cf.imoist, d->prs, d->rho,
+                     c->part3, c->part4, nrk == 3 && cf.apmasscon == 1, st, nl);
+    // the tracers below read rho's halo through the diffusion: fill it where
+    // the reference does, before them (solve2.F:1681-1684)
+    if (diffit && nrk < 3) launch_bc(g, d->rho, 2, 0, st, nl);
     // passive tracers (solve2.F:1880-1970)
     for (int n = 0; n < npt; n++) {
       const int s = 1 + numq + n;
       const int pdef = (nrk == 3 && cf.pdtra == 1) ? 1 : 0;
       launch_advs_tiled(g, c->rru, c->rrv, c->rrw, buf_in(s, nrk), base[s], 0, ten1[s], nullptr, buf_out(s, nrk),
-                        weno, pdef, 1, (double)(1.0f * 1.0e-18f), dttmp, 0, c->pdefscr, st, nl);
+                        weno, pdef, 1, (double)(1.0f * 1.0e-18f), dttmp, 0, c->pdefscr, st, nl, nullptr,
+                        diffit ? &df : nullptr);
     }
+    if (diffit && nrk < 3) launch_recip_rho(g, d->rho, c->rr, st, nl);   // solve2.F:2036-2046
     // halo fills of the stage (solve2.F:1663-1707 and the tracers' bcs of
     // solve2.F:1959-1961), batched into one two-phase launch: every array is
     // distinct and nothing between their reference positions and here reads
@@ -552,7 +575,7 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
       std::vector<float *> arr{d->u3d, d->v3d, d->w3d};
       std::vector<int> which{3, 4, 5}, flag{0, 0, 1};
       if (nrk < 3) {
-        arr.push_back(d->rho); which.push_back(2); flag.push_back(0);
+        if (!diffit) { arr.push_back(d->rho); which.push_back(2); flag.push_back(0); }
         arr.push_back(d->pp3d); which.push_back(2); flag.push_back(0);
         for (int s = 0; s < nsc; s++) { arr.push_back(buf_out(s, nrk)); which.push_back(1); flag.push_back(0); }
       }

@@ -144,6 +144,26 @@ struct TileExtras {
   float *capfx = nullptr, *capfy = nullptr, *caprx = nullptr, *capry = nullptr;
 };
 
+// 6th-order horizontal diffusion inside the advection passes (idiff=1,
+// difforder=6; adv.F:342-406, 1177-1236, 2115-2174, 3109-3170).  rho null:
+// no diffusion.  ri is 1/rho as the scalar form uses it (rr of solve2; it
+// may lag rho by one stage), coef = kdiff6/64/dt, mdiff the limiter.
+struct Diff6 {
+  const float *rho = nullptr, *ri = nullptr;
+  float coef = 0.0f;
+  int mdiff = 0;
+};
+
+// The difference stencil of a face between a(-1) and a(0), as the Fortran
+// evaluates it: (10 (a0 - am1) - 5 (ap1 - am2)) + (ap2 - am3).
+__device__ __forceinline__ float diff6_stencil(float am3, float am2, float am1, float a0, float ap1, float ap2) {
+  return (10.0f * (a0 - am1) - 5.0f * (ap1 - am2)) + (ap2 - am3);
+}
+// the mdiff limiter: no flux against the local gradient
+__device__ __forceinline__ float diff6_limit(float f, float a0, float am1, int mdiff) {
+  return (mdiff == 1 && f * (a0 - am1) <= 0.0f) ? 0.0f : f;
+}
+
 // Inputs of the solve1 tendency initialisation and of calcener (k_misc.cu).
 struct TendIn {
   int irdamp;

@@ -365,13 +365,15 @@ __device__ __forceinline__ float hflux_mom(float r, const float *p, int stride) 
 template <int TX, int TY, int KC, int STAG>
 __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const float *__restrict__ divx,
                                                       const float *ten1, float *ten,
-                                                      const float *__restrict__ th3d, const float *__restrict__ qv) {
+                                                      const float *__restrict__ th3d, const float *__restrict__ qv,
+                                                      Diff6 df) {
   constexpr int NT = TX * TY;
   constexpr int SW = TX + 6, SH = TY + 6, SP = SW + 1;
   constexpr int NST = (SW * SH + NT - 1) / NT;
   constexpr int NFX = (TX + 1) * TY, NFY = TX * (TY + 1);
   __shared__ float ss[SH * SP];
   __shared__ float fx[NFX], fxv[NFX], fy[NFY], fyv[NFY];
+  __shared__ float dfx[NFX], dfy[NFY];     // 6th-order diffusion fluxes
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
   const int i0 = 1 + (int)blockIdx.x * TX, j0 = 1 + (int)blockIdx.y * TY;
   const int i = i0 + tx, j = j0 + ty;
@@ -535,6 +537,23 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
         if (STAG == 2) r = 0.5f * (r0k * p[2] + r0k * p[3]);
         fx[f] = hflux_mom(r, p, 1);
         fxv[f] = r;
+        if (df.rho) {
+          // the face between p[2] and p[3]: s-point fxi (u: adv.F:1190-1193),
+          // u-point fxi (v: adv.F:2128-2132; w: adv.F:3124-3130)
+          const int ii = fxi[s], jj = fxj[s];
+          const float d = diff6_stencil(p[0], p[1], p[2], p[3], p[4], p[5]);
+          float fd;
+          if (STAG == 2) {
+            fd = d * LDG(&df.rho[iS(g, ii, jj, k)]);
+          } else if (STAG == 3) {
+            fd = d * 0.25f * ((LDG(&df.rho[iS(g, ii - 1, jj - 1, k)]) + LDG(&df.rho[iS(g, ii, jj, k)])) +
+                              (LDG(&df.rho[iS(g, ii - 1, jj, k)]) + LDG(&df.rho[iS(g, ii, jj - 1, k)])));
+          } else {
+            fd = d * 0.5f * (cc2 * (LDG(&df.rho[iS(g, ii - 1, jj, k)]) + LDG(&df.rho[iS(g, ii, jj, k)])) +
+                             cc1 * (LDG(&df.rho[iS(g, ii - 1, jj, k - 1)]) + LDG(&df.rho[iS(g, ii, jj, k - 1)])));
+          }
+          dfx[f] = diff6_limit(fd, p[3], p[2], df.mdiff);
+        }
       }
       if (fyi[s] >= 0) {
         const int row = f / TX, col = f - row * TX;
@@ -543,6 +562,23 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
         if (STAG == 3) r = 0.5f * (r0k * p[2 * SP] + r0k * p[3 * SP]);
         fy[f] = hflux_mom(r, p, SP);
         fyv[f] = r;
+        if (df.rho) {
+          // the face between p[2 SP] and p[3 SP]: v-point fyj (u: adv.F:1210-1215;
+          // w: adv.F:3146-3152), s-point fyj (v: adv.F:2151-2153)
+          const int ii = fyi[s], jj = fyj[s];
+          const float d = diff6_stencil(p[0], p[SP], p[2 * SP], p[3 * SP], p[4 * SP], p[5 * SP]);
+          float fd;
+          if (STAG == 2) {
+            fd = d * 0.25f * ((LDG(&df.rho[iS(g, ii - 1, jj - 1, k)]) + LDG(&df.rho[iS(g, ii, jj, k)])) +
+                              (LDG(&df.rho[iS(g, ii - 1, jj, k)]) + LDG(&df.rho[iS(g, ii, jj - 1, k)])));
+          } else if (STAG == 3) {
+            fd = d * LDG(&df.rho[iS(g, ii, jj, k)]);
+          } else {
+            fd = d * 0.5f * (cc2 * (LDG(&df.rho[iS(g, ii, jj - 1, k)]) + LDG(&df.rho[iS(g, ii, jj, k)])) +
+                             cc1 * (LDG(&df.rho[iS(g, ii, jj - 1, k - 1)]) + LDG(&df.rho[iS(g, ii, jj, k - 1)])));
+          }
+          dfy[f] = diff6_limit(fd, p[3 * SP], p[2 * SP], df.mdiff);
+        }
       }
     }
     const int ku = (STAG == 4) ? k : k + 1;
@@ -616,6 +652,23 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
           advy = advy - ww * (c1k * (RRVk(nj + 1, k - 1) - RRVk(nj, k - 1)) + c2k * (RRVk(nj + 1, k) - RRVk(nj, k))) *
                             g.rdy * LDG(&g.vh[nj - g.jb]);
       }
+      if (df.rho) {   // adv.F:1199-1201, 1220-1222; 2139-2141, 2160-2162; 3135-3137, 3160-3162
+        const float ddx = df.coef * (dfx[xi + 1] - dfx[xi]), ddy = df.coef * (dfy[yi + TX] - dfy[yi]);
+        if (STAG == 2) {
+          const float rs = LDG(&df.rho[iS(g, i - 1, j, k)]) + LDG(&df.rho[iS(g, i, j, k)]);
+          advx = advx + ddx * (r0k + r0k) / rs;
+          advy = advy + ddy * (r0k + r0k) / rs;
+        } else if (STAG == 3) {
+          const float rs = LDG(&df.rho[iS(g, i, j - 1, k)]) + LDG(&df.rho[iS(g, i, j, k)]);
+          advx = advx + ddx * (r0k + r0k) / rs;
+          advy = advy + ddy * (r0k + r0k) / rs;
+        } else {
+          const float rf = LDG(&g.rf0[k]);
+          const float rs = 0.5f * (LDG(&df.rho[iS(g, i, j, k - 1)]) + LDG(&df.rho[iS(g, i, j, k)]));
+          advx = advx + ddx * rf / rs;
+          advy = advy + ddy * rf / rs;
+        }
+      }
       if (STAG == 4) {
         advz = -(fzhi - fzlo) * g.rdz * LDG(&g.mf[k]);
       } else {
@@ -645,31 +698,32 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
 template <int TX, int TY, int KC>
 static void mom_tiles_shape(const DGrid &g, const Vel &q, const float *uten1, const float *vten1,
                             const float *wten1, float *uten, float *vten, float *wten, const float *th3d,
-                            const float *qv, const float *divx, cudaStream_t st) {
+                            const float *qv, const float *divx, const Diff6 &df, cudaStream_t st) {
   dim3 blk(TX, TY);
   const int kch = (g.nk + KC - 1) / KC, kchw = (g.nk - 1 + KC - 1) / KC;
   {
     dim3 grid((g.ni + 1 + TX - 1) / TX, (g.nj + TY - 1) / TY, kch);
     ProfScope _ps("k_advu", st);
-    k_mom_tile<TX, TY, KC, 2><<<grid, blk, 0, st>>>(g, q, divx, uten1, uten, nullptr, nullptr);
+    k_mom_tile<TX, TY, KC, 2><<<grid, blk, 0, st>>>(g, q, divx, uten1, uten, nullptr, nullptr, df);
   }
   {
     dim3 grid((g.ni + TX - 1) / TX, (g.nj + 1 + TY - 1) / TY, kch);
     ProfScope _ps("k_advv", st);
-    k_mom_tile<TX, TY, KC, 3><<<grid, blk, 0, st>>>(g, q, divx, vten1, vten, nullptr, nullptr);
+    k_mom_tile<TX, TY, KC, 3><<<grid, blk, 0, st>>>(g, q, divx, vten1, vten, nullptr, nullptr, df);
   }
   {
     dim3 grid((g.ni + TX - 1) / TX, (g.nj + TY - 1) / TY, kchw);
     ProfScope _ps("k_advw", st);
-    k_mom_tile<TX, TY, KC, 4><<<grid, blk, 0, st>>>(g, q, divx, wten1, wten, th3d, qv);
+    k_mom_tile<TX, TY, KC, 4><<<grid, blk, 0, st>>>(g, q, divx, wten1, wten, th3d, qv, df);
   }
 }
 
 void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w,
                          const float *uten1, const float *vten1, const float *wten1,
                          float *uten, float *vten, float *wten, const float *th3d, const float *qv,
-                         float *divx, cudaStream_t st, int64_t *nl) {
+                         float *divx, cudaStream_t st, int64_t *nl, const Diff6 *diff) {
   Vel q{u, v, w};
+  const Diff6 df = diff ? *diff : Diff6{};
   {
     dim3 grid((g.ni + 2 + 127) / 128, g.nj + 2, g.nk);
     ProfScope _ps("k_mom_divx", st);
@@ -678,7 +732,7 @@ void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const f
 #define CM1G_MOM_SHAPE(n)                                                                                     \
   case n:                                                                                                     \
     mom_tiles_shape<kTileShapes[n][0], kTileShapes[n][1], kTileShapes[n][2]>(g, q, uten1, vten1, wten1, uten, \
-                                                                             vten, wten, th3d, qv, divx, st); \
+                                                                             vten, wten, th3d, qv, divx, df, st); \
     break;
   switch (g.tile_mom) {
     CM1G_MOM_SHAPE(1)
@@ -707,6 +761,7 @@ struct SAdv {
   const float *__restrict__ thterm; // moist theta: thten -= div(u_avg)*thterm (solve2.F:1320-1329)
   int weighted;                     // 1: rru/rrv/rrw are velocities to be weighted here
   int sadd;                         // add th0(k)-th0r to s (theta)
+  Diff6 df{};                       // 6th-order diffusion (df.rho null: none)
 };
 
 __device__ __forceinline__ float sval(const DGrid &g, const SAdv &a, int i, int j, int k) {
@@ -1193,6 +1248,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
   constexpr int NFX = (TX + 1) * TY, NFY = TX * (TY + 1);   // faces of one level
   __shared__ float ss[SH * SP];
   __shared__ float fx[NFX], ux[NFX], fy[NFY], vy[NFY];
+  __shared__ float dfx[NFX], dfy[NFY];     // 6th-order diffusion fluxes (adv.F:356-395)
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
   const int i0 = 1 + (int)blockIdx.x * TX, j0 = 1 + (int)blockIdx.y * TY;
   const int i = i0 + tx, j = j0 + ty;
@@ -1219,16 +1275,18 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
   }
   int fxo[2], fxs[2], fyo[2], fys[2];   // face offsets (-1: no face) and stencil starts in ss
   int fxl[2], fyl[2];                   // in-level index of the face in the learned-value arrays
+  int fxr[2];                           // s-plane offset of the cell (i, j) right of an x-face
 #pragma unroll
   for (int q = 0; q < 2; q++) {
     const int f = tid + q * NT;
-    fxo[q] = -1; fxs[q] = 0; fyo[q] = -1; fys[q] = 0; fxl[q] = 0; fyl[q] = 0;
+    fxo[q] = -1; fxs[q] = 0; fyo[q] = -1; fys[q] = 0; fxl[q] = 0; fyl[q] = 0; fxr[q] = 0;
     if (f < NFX) {
       const int row = f / (TX + 1), col = f - row * (TX + 1);
       const int ii = i0 + col, jj = j0 + row;
       if (ii <= ni + 1 && jj <= nj) {
         fxo[q] = (ii - g.ib) + (NI + 1) * (jj - g.jb); fxs[q] = (row + 3) * SP + col;
         fxl[q] = (jj - 1) * (ni + 1) + (ii - 1);
+        fxr[q] = (ii - g.ib) + NI * (jj - g.jb);
       }
     }
     if (f < NFY) {
@@ -1328,6 +1386,12 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
         const float fl = (ph == ph) ? r * ph : hflux5(r, p[0], p[1], p[2], p[3], p[4], p[5], WENO, pdef, weps);
         fx[f] = fl;
         ux[f] = ru[q];
+        if (a.df.rho) {   // face between s(i-1) and s(i): p[2], p[3]
+          const long ro = (long)k * planeS + fxr[q];                           // rho(i,j)
+          const float fd = diff6_stencil(p[0], p[1], p[2], p[3], p[4], p[5]) * 0.5f *
+                           (LDG(&a.df.rho[ro - 1]) + LDG(&a.df.rho[ro]));
+          dfx[f] = diff6_limit(fd, p[3], p[2], a.df.mdiff);
+        }
         if (MODE == MODE_UPDATE && out.ex.capfx) {
           out.ex.capfx[(long)k * planeU + fxo[q]] = fl;
           out.ex.caprx[(long)k * planeU + fxo[q]] = r;
@@ -1342,6 +1406,12 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
                                     : hflux5(r, p[0], p[SP], p[2 * SP], p[3 * SP], p[4 * SP], p[5 * SP], WENO, pdef, weps);
         fy[f] = fl;
         vy[f] = rv[q];
+        if (a.df.rho) {   // face between s(j-1) and s(j): p[2 SP], p[3 SP]
+          const long ro = (long)k * planeS + fyo[q];                           // rho(i,j)
+          const float fd = diff6_stencil(p[0], p[SP], p[2 * SP], p[3 * SP], p[4 * SP], p[5 * SP]) * 0.5f *
+                           (LDG(&a.df.rho[ro - NI]) + LDG(&a.df.rho[ro]));
+          dfy[f] = diff6_limit(fd, p[3 * SP], p[2 * SP], a.df.mdiff);
+        }
         if (MODE == MODE_UPDATE && out.ex.capfy) {
           out.ex.capfy[(long)k * planeV + fyo[q]] = fl;
           out.ex.capry[(long)k * planeV + fyo[q]] = r;
@@ -1373,6 +1443,11 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
       if (doite && i == ni && fu1 <= 0.0f) advx = advx - sc * (fu1 - fu0) * g.rdx * uh_i;
       if (doits && j == 1 && fv0 >= 0.0f) advy = advy - sc * (fv1 - fv0) * g.rdy * vh_j;
       if (doitn && j == nj && fv1 <= 0.0f) advy = advy - sc * (fv1 - fv0) * g.rdy * vh_j;
+      if (a.df.rho) {   // adv.F:375-378, 397-400
+        const float ri = LDG(&a.df.ri[o]);
+        advx = advx + a.df.coef * (dfx[xi + 1] - dfx[xi]) * ri * r0k;
+        advy = advy + a.df.coef * (dfy[yi + TX] - dfy[yi]) * ri * r0k;
+      }
       const float mhk = LDG(&g.mh[k]);
       float advz;
       if (k == 1) advz = -fzhi * g.rdz * mhk;
@@ -1459,8 +1534,9 @@ static void advs_tiled_shape(const DGrid &g, const SAdv &a, STileOut o, int weno
 void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const float *rrw, const float *s,
                        const float *s0, int sadd, const float *ten1, const float *thterm, float *snew, int weno,
                        int pdef, int pdefweno, double weps, float dt, int flush, float *scratch, cudaStream_t st,
-                       int64_t *nl, const TileExtras *ex) {
+                       int64_t *nl, const TileExtras *ex, const Diff6 *diff) {
   SAdv a{rru, rrv, rrw, s, s0, nullptr, thterm, 1, sadd};
+  if (diff) a.df = *diff;
   STileOut o{};
   o.sten_in = ten1; o.sbase = s0; o.snew = snew;
   if (ex) o.ex = *ex;

@@ -210,6 +210,22 @@ __global__ void k_masscon_apply(DGrid g, float *pp3d, const float *__restrict__ 
   prs_rho(g, pp, LDG(&th3d[o]), qv, o, k, imoist, prs, rho);
 }
 
+// rr = 1/rho over the physical cells and one halo cell (solve3.F:660-675,
+// solve2.F:2036-2046): the reciprocal the scalar form of the 6th-order
+// diffusion multiplies by.
+__global__ void k_recip_rho(DGrid g, const float *__restrict__ rho, float *rr) {
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x), j = (int)blockIdx.y, k = 1 + (int)blockIdx.z;
+  if (i > g.ni + 1) return;
+  const long o = iS(g, i, j, k);
+  rr[o] = 1.0f / LDG(&rho[o]);
+}
+
+void launch_recip_rho(const DGrid &g, const float *rho, float *rr, cudaStream_t st, int64_t *nl) {
+  dim3 grid((g.ni + 2 + 127) / 128, g.nj + 2, g.nk);
+  { ProfScope _ps("k_recip_rho", st); k_recip_rho<<<grid, 128, 0, st>>>(g, rho, rr); }
+  if (nl) *nl += 1;
+}
+
 int prs_nchunk(const DGrid &g) { return (int)(((long)g.ni * g.nj + PR_NT * PR_PER - 1) / (PR_NT * PR_PER)); }
 
 void launch_prs_rho(const DGrid &g, const float *pp3d, const float *th3d, const float *qv, int imoist,

@@ -46,6 +46,8 @@ module cm1g_iso
     real(c_float)      :: smeps
     integer(c_int32_t) :: testcase, psolver, terrain_flag, axisymm, icor
     real(c_float)      :: qmag(CM1G_MAXQ)
+    integer(c_int32_t) :: idiff, difforder, mdiff
+    real(c_float)      :: kdiff6
   end type
 
   type, bind(C) :: cm1g_grid_t
@@ -218,6 +220,7 @@ contains
     cfg%apmasscon = apmasscon; cfg%irbc = irbc; cfg%cstar = cstar; cfg%roflux = roflux
     cfg%smeps = smeps; cfg%testcase = testcase; cfg%psolver = psolver
     cfg%terrain_flag = merge(1, 0, terrain_flag); cfg%axisymm = axisymm; cfg%icor = icor
+    cfg%idiff = idiff; cfg%difforder = difforder; cfg%mdiff = mdiff; cfg%kdiff6 = kdiff6
     cfg%qmag = 0.0
     do n = 1, min(size(qmag), int(CM1G_MAXQ))
       cfg%qmag(n) = qmag(n)

@@ -399,11 +399,18 @@ class _Run:
         self.ctx, self.dev, self.case, self.mass1 = ctx, dev, case, mass1
         self.steps = self.timed = 0
         self.ms = 0.0
+        self.failed = None          # the library's error if the run went unstable
 
     def advance(self, n):
-        import torch
-        if n <= 0:
+        if n <= 0 or self.failed:
             return
+        try:
+            self._advance(n)
+        except Exception as e:      # a non-finite velocity ends this run only
+            self.failed = "step %d: %s" % (self.steps, e)
+
+    def _advance(self, n):
+        import torch
         if self.steps == 0:
             self.ctx.step(self.dev, self.case.dt, self.mass1, use_graph=True)
             self.steps += 1
@@ -470,8 +477,10 @@ def evaluate(P, tests, minutes, seed=77, horizons=(2, 10, 50), widens=(0.0, 1.0)
             mth = mth.reshape(ml.nk, ml.nj // 2, 2, ml.ni // 2, 2).mean(dim=(2, 4))
             l2s = {"coarse_plain": l2(c_plain["th3d"][ci]), "plain_500m": l2(mth), "no_change": l2(torch.zeros_like(ref))}
             for w in widens:
-                l2s["coarse_learned_widen_%g" % w] = l2(c_learn[w]["th3d"][ci])
+                r = runs["coarse_learned_widen_%g" % w]
+                l2s["coarse_learned_widen_%g" % w] = None if r.failed else l2(c_learn[w]["th3d"][ci])
             row = {"coarse_steps": hz, "seconds": hz * ccase.dt, "l2_theta": l2s,
+                   "unstable": {k: r.failed for k, r in runs.items() if r.failed},
                    "gpu_seconds": {k: r.gpu_seconds() for k, r in runs.items()}}
             log(json.dumps(row))
             rows.append(row)

@@ -82,6 +82,10 @@ typedef struct cm1g_config {
   int32_t axisymm;             /* 0 only                                          */
   int32_t icor;                /* 0 only                                          */
   float   qmag[CM1G_MAXQ];     /* magnitude of each q (param.F), for WENO eps     */
+  int32_t idiff;               /* 1: horizontal diffusion inside advection        */
+  int32_t difforder;           /* 6 (the advection-embedded 6th-order form) only  */
+  int32_t mdiff;               /* 1: monotonic limiter of the 6th-order fluxes    */
+  float   kdiff6;              /* 6th-order coefficient: kdiff6/64/dt per step    */
 } cm1g_config_t;
 
 /*
@@ -166,7 +170,8 @@ int cm1g_bcv(cm1g_ctx_t *ctx, float *v);
 int cm1g_bcw(cm1g_ctx_t *ctx, float *w, int32_t flag);
 
 /* Scalar advection tendency: replaces advs (src/adv.F:14-903) for
- * hadvorder=vadvorder=5 / WENO5, no budgets, no diffusion.  Argument
+ * hadvorder=vadvorder=5 / WENO5, no budgets, and diffit=0 (the 6th-order
+ * diffusion of idiff=1 runs inside cm1g_solve2 / cm1g_step only).  Argument
  * meaning follows adv.F:14-19: rru/rrv/rrw are the rho0-weighted fluxes,
  * divx their divergence, s0 the RK base value, s the advected field,
  * sten is incremented by the advective tendency (times rr0).  pdef selects
@@ -179,7 +184,9 @@ int cm1g_advs(cm1g_ctx_t *ctx, int32_t nrk, int32_t wflag,
 
 /* Momentum advection tendencies: replaces advu, advv, advw (src/adv.F:911,
  * 1847, 2778) with hadvordrv=vadvordrv=5: uten/vten/wten are incremented by
- * the flux-form advection of u3d/v3d/w3d by rho0*(u,v,w). */
+ * the flux-form advection of u3d/v3d/w3d by rho0*(u,v,w).  Advection only:
+ * the 6th-order diffusion of idiff=1 (which needs rho and dt) runs inside
+ * cm1g_solve2 / cm1g_step. */
 int cm1g_advuvw(cm1g_ctx_t *ctx, int32_t nrk, const float *u3d, const float *v3d,
                 const float *w3d, float *uten, float *vten, float *wten);
 

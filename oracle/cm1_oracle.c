@@ -779,6 +779,19 @@ static void pdefz(const OG *g, F3 rrw, F3 advz, F3 dum, F3 mass, B3 flag, F3 s0,
 
 typedef struct { F3 advx, advy, advz, dumx, dumy, dumz, mass; B3 flag; } Scratch;
 
+/* 6th-order horizontal diffusion (idiff=1, difforder=6), adv.F:342-406 and
+ * the advu/advv/advw forms (adv.F:1177-1236, 2115-2174, 3109-3170): the
+ * difference stencil of a face between a(-1) and a(0), evaluated as
+ * (10 (a0 - am1) - 5 (ap1 - am2)) + (ap2 - am3) like the Fortran. */
+static inline float d6(float am3, float am2, float am1, float a0, float ap1, float ap2) {
+  return (10.0f * (a0 - am1) - 5.0f * (ap1 - am2)) + (ap2 - am3);
+}
+/* the mdiff limiter: no flux against the local gradient (adv.F:366-373) */
+static inline float d6lim(const OG *g, float f, float a0, float am1) {
+  return (g->cfg->mdiff == 1 && f * (a0 - am1) <= 0.0f) ? 0.0f : f;
+}
+static inline int diff6_on(const OG *g) { return g->cfg->idiff == 1 && g->cfg->difforder == 6; }
+
 static int scratch_alloc(const OG *g, Scratch *w) {
   long n = nS(g);
   float *b = (float *)calloc((size_t)n * 7, sizeof(float));
@@ -793,7 +806,7 @@ static void scratch_free(Scratch *w) { free(w->advx.p); free(w->flag.p); }
 
 /* advs: adv.F:14-903 (Cartesian, no terrain, no diffusion, no budgets) */
 static void advs_g(const OG *g, Scratch *w, int nrk, int wflag, F3 rru, F3 rrv, F3 rrw, F3 divx,
-                   F3 s0, F3 s, F3 sten, int pdef, int pdefweno, float dt, double weps) {
+                   F3 s0, F3 s, F3 sten, int pdef, int pdefweno, float dt, double weps, F3 rho, F3 ri, int diffit) {
   int ni = g->ni, nj = g->nj, nk = g->nk;
   const cm1g_config_t *cfg = g->cfg;
   int doweno = (wflag == 1) && (cfg->advwenos == 1 || (cfg->advwenos == 2 && nrk == 3));
@@ -830,6 +843,27 @@ static void advs_g(const OG *g, Scratch *w, int nrk, int wflag, F3 rru, F3 rrv, 
   if (doitn) for (int k = 1; k <= nk; k++) for (int i = 1; i <= ni; i++)
     if (A3(rrv, i, nj + 1, k) <= 0.0f)
       A3(advy, i, nj, k) = A3(advy, i, nj, k) - A3(s, i, nj, k) * (A3(rrv, i, nj + 1, k) - A3(rrv, i, nj, k)) * g->rdy * VH(nj);
+  /* adv.F:342-406: 6th-order diffusion */
+  if (diffit == 1) {
+    float coef = g->cfg->kdiff6 / 64.0f / dt;   /* adv.F:80-82 */
+#pragma omp parallel for
+    for (int k = 1; k <= nk; k++) {
+      for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni + 1; i++) {
+        float f = d6(A3(s, i - 3, j, k), A3(s, i - 2, j, k), A3(s, i - 1, j, k), A3(s, i, j, k), A3(s, i + 1, j, k),
+                     A3(s, i + 2, j, k)) * 0.5f * (A3(rho, i - 1, j, k) + A3(rho, i, j, k));
+        A3(dumx, i, j, k) = d6lim(g, f, A3(s, i, j, k), A3(s, i - 1, j, k));
+      }
+      for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++)
+        A3(advx, i, j, k) = A3(advx, i, j, k) + coef * (A3(dumx, i + 1, j, k) - A3(dumx, i, j, k)) * A3(ri, i, j, k) * A3(g->rho0, i, j, k);
+      for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni; i++) {
+        float f = d6(A3(s, i, j - 3, k), A3(s, i, j - 2, k), A3(s, i, j - 1, k), A3(s, i, j, k), A3(s, i, j + 1, k),
+                     A3(s, i, j + 2, k)) * 0.5f * (A3(rho, i, j - 1, k) + A3(rho, i, j, k));
+        A3(dumy, i, j, k) = d6lim(g, f, A3(s, i, j, k), A3(s, i, j - 1, k));
+      }
+      for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++)
+        A3(advy, i, j, k) = A3(advy, i, j, k) + coef * (A3(dumy, i, j + 1, k) - A3(dumy, i, j, k)) * A3(ri, i, j, k) * A3(g->rho0, i, j, k);
+    }
+  }
   /* adv.F:426-446 */
   if (pdef == 1) pdefx1(g, rru, advx, dumx, s0, s, dt);
   if (pdef == 1) pdefy1(g, rrv, advy, dumy, s0, s, dt);
@@ -856,7 +890,7 @@ static void advs_g(const OG *g, Scratch *w, int nrk, int wflag, F3 rru, F3 rrv, 
 }
 
 /* advu: adv.F:911-1839 (hadvordrv=vadvordrv=5, no WENO) */
-static void advu_g(const OG *g, Scratch *w, F3 divx, F3 rru, F3 u3d, F3 uten, F3 rrv, F3 rrw) {
+static void advu_g(const OG *g, Scratch *w, F3 divx, F3 rru, F3 u3d, F3 uten, F3 rrv, F3 rrw, F3 rho, float dt) {
   int ni = g->ni, nj = g->nj, nk = g->nk;
   int i1 = g->ibw ? 2 : 1, i2 = g->ibe ? ni : ni + 1;
   int doits = (g->sbc == 2 && g->ibs), doitn = (g->nbc == 2 && g->ibn);
@@ -879,6 +913,31 @@ static void advu_g(const OG *g, Scratch *w, F3 divx, F3 rru, F3 u3d, F3 uten, F3
     if ((A3(rrv, i, nj + 1, k) + A3(rrv, i - 1, nj + 1, k)) <= 0.0f)
       A3(advy, i, nj, k) = A3(advy, i, nj, k) - A3(u3d, i, nj, k) * 0.5f *
           ((A3(rrv, i - 1, nj + 1, k) - A3(rrv, i - 1, nj, k)) + (A3(rrv, i, nj + 1, k) - A3(rrv, i, nj, k))) * g->rdy * VH(nj);
+  /* adv.F:1177-1236: 6th-order diffusion */
+  if (diff6_on(g)) {
+    float coef = g->cfg->kdiff6 / 64.0f / dt;
+#pragma omp parallel for
+    for (int k = 1; k <= nk; k++) {
+      float r0 = A3(g->rho0, 1, 1, k);
+      for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni + 2; i++) {
+        float f = d6(A3(u3d, i - 3, j, k), A3(u3d, i - 2, j, k), A3(u3d, i - 1, j, k), A3(u3d, i, j, k),
+                     A3(u3d, i + 1, j, k), A3(u3d, i + 2, j, k)) * A3(rho, i - 1, j, k);
+        A3(dumx, i, j, k) = d6lim(g, f, A3(u3d, i, j, k), A3(u3d, i - 1, j, k));
+      }
+      for (int j = 1; j <= nj; j++) for (int i = i1; i <= i2; i++)
+        A3(advx, i, j, k) = A3(advx, i, j, k) + coef * (A3(dumx, i + 1, j, k) - A3(dumx, i, j, k)) * (r0 + r0) /
+                                                    (A3(rho, i - 1, j, k) + A3(rho, i, j, k));
+      for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni + 1; i++) {
+        float f = d6(A3(u3d, i, j - 3, k), A3(u3d, i, j - 2, k), A3(u3d, i, j - 1, k), A3(u3d, i, j, k),
+                     A3(u3d, i, j + 1, k), A3(u3d, i, j + 2, k)) * 0.25f *
+                  ((A3(rho, i - 1, j - 1, k) + A3(rho, i, j, k)) + (A3(rho, i - 1, j, k) + A3(rho, i, j - 1, k)));
+        A3(dumy, i, j, k) = d6lim(g, f, A3(u3d, i, j, k), A3(u3d, i, j - 1, k));
+      }
+      for (int j = 1; j <= nj; j++) for (int i = i1; i <= i2; i++)
+        A3(advy, i, j, k) = A3(advy, i, j, k) + coef * (A3(dumy, i, j + 1, k) - A3(dumy, i, j, k)) * (r0 + r0) /
+                                                    (A3(rho, i - 1, j, k) + A3(rho, i, j, k));
+    }
+  }
   vadv5_uv(g, 2, rrw, dumz, u3d);
 #pragma omp parallel for
   for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = i1; i <= i2; i++) {
@@ -892,7 +951,7 @@ static void advu_g(const OG *g, Scratch *w, F3 divx, F3 rru, F3 u3d, F3 uten, F3
 }
 
 /* advv: adv.F:1847-2770 */
-static void advv_g(const OG *g, Scratch *w, F3 divx, F3 rru, F3 rrv, F3 v3d, F3 vten, F3 rrw) {
+static void advv_g(const OG *g, Scratch *w, F3 divx, F3 rru, F3 rrv, F3 v3d, F3 vten, F3 rrw, F3 rho, float dt) {
   int ni = g->ni, nj = g->nj, nk = g->nk;
   int j1 = g->ibs ? 2 : 1, j2 = g->ibn ? nj : nj + 1;
   int doitw = (g->wbc == 2 && g->ibw), doite = (g->ebc == 2 && g->ibe);
@@ -915,6 +974,31 @@ static void advv_g(const OG *g, Scratch *w, F3 divx, F3 rru, F3 rrv, F3 v3d, F3 
     if ((A3(rru, ni + 1, j, k) + A3(rru, ni + 1, j - 1, k)) <= 0.0f)
       A3(advx, ni, j, k) = A3(advx, ni, j, k) - A3(v3d, ni, j, k) * 0.5f *
           ((A3(rru, ni + 1, j - 1, k) - A3(rru, ni, j - 1, k)) + (A3(rru, ni + 1, j, k) - A3(rru, ni, j, k))) * g->rdx * UH(ni);
+  /* adv.F:2115-2174: 6th-order diffusion */
+  if (diff6_on(g)) {
+    float coef = g->cfg->kdiff6 / 64.0f / dt;
+#pragma omp parallel for
+    for (int k = 1; k <= nk; k++) {
+      float r0 = A3(g->rho0, 1, 1, k);
+      for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni + 1; i++) {
+        float f = d6(A3(v3d, i - 3, j, k), A3(v3d, i - 2, j, k), A3(v3d, i - 1, j, k), A3(v3d, i, j, k),
+                     A3(v3d, i + 1, j, k), A3(v3d, i + 2, j, k)) * 0.25f *
+                  ((A3(rho, i - 1, j - 1, k) + A3(rho, i, j, k)) + (A3(rho, i - 1, j, k) + A3(rho, i, j - 1, k)));
+        A3(dumx, i, j, k) = d6lim(g, f, A3(v3d, i, j, k), A3(v3d, i - 1, j, k));
+      }
+      for (int j = j1; j <= j2; j++) for (int i = 1; i <= ni; i++)
+        A3(advx, i, j, k) = A3(advx, i, j, k) + coef * (A3(dumx, i + 1, j, k) - A3(dumx, i, j, k)) * (r0 + r0) /
+                                                    (A3(rho, i, j - 1, k) + A3(rho, i, j, k));
+      for (int j = 1; j <= nj + 2; j++) for (int i = 1; i <= ni; i++) {
+        float f = d6(A3(v3d, i, j - 3, k), A3(v3d, i, j - 2, k), A3(v3d, i, j - 1, k), A3(v3d, i, j, k),
+                     A3(v3d, i, j + 1, k), A3(v3d, i, j + 2, k)) * A3(rho, i, j - 1, k);
+        A3(dumy, i, j, k) = d6lim(g, f, A3(v3d, i, j, k), A3(v3d, i, j - 1, k));
+      }
+      for (int j = j1; j <= j2; j++) for (int i = 1; i <= ni; i++)
+        A3(advy, i, j, k) = A3(advy, i, j, k) + coef * (A3(dumy, i, j + 1, k) - A3(dumy, i, j, k)) * (r0 + r0) /
+                                                    (A3(rho, i, j - 1, k) + A3(rho, i, j, k));
+    }
+  }
   vadv5_uv(g, 3, rrw, dumz, v3d);
 #pragma omp parallel for
   for (int k = 1; k <= nk; k++) for (int j = j1; j <= j2; j++) for (int i = 1; i <= ni; i++) {
@@ -928,7 +1012,7 @@ static void advv_g(const OG *g, Scratch *w, F3 divx, F3 rru, F3 rrv, F3 v3d, F3 
 }
 
 /* advw: adv.F:2778-3610 */
-static void advw_g(const OG *g, Scratch *w, F3 divx, F3 rru, F3 rrv, F3 rrw, F3 w3d, F3 wten) {
+static void advw_g(const OG *g, Scratch *w, F3 divx, F3 rru, F3 rrv, F3 rrw, F3 w3d, F3 wten, F3 rho, float dt) {
   int ni = g->ni, nj = g->nj, nk = g->nk;
   int doitw = (g->wbc == 2 && g->ibw), doite = (g->ebc == 2 && g->ibe);
   int doits = (g->sbc == 2 && g->ibs), doitn = (g->nbc == 2 && g->ibn);
@@ -987,6 +1071,34 @@ static void advw_g(const OG *g, Scratch *w, F3 divx, F3 rru, F3 rrv, F3 rrw, F3 
     if (vbar <= 0.0f)
       A3(advy, i, nj, k) = A3(advy, i, nj, k) - A3(w3d, i, nj, k) *
           (A3(c1, i, nj, k) * (A3(rrv, i, nj + 1, k - 1) - A3(rrv, i, nj, k - 1)) + A3(c2, i, nj, k) * (A3(rrv, i, nj + 1, k) - A3(rrv, i, nj, k))) * g->rdy * VH(nj);
+  }
+  /* adv.F:3109-3170: 6th-order diffusion */
+  if (diff6_on(g)) {
+    float coef = g->cfg->kdiff6 / 64.0f / dt;
+#pragma omp parallel for
+    for (int k = 2; k <= nk; k++) {
+      float rf = A3(g->rf0, 1, 1, k);
+      for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni + 1; i++) {
+        float cc2 = 0.5f * (A3(c2, i - 1, j, k) + A3(c2, i, j, k)), cc1 = 1.0f - cc2;
+        float f = d6(A3(w3d, i - 3, j, k), A3(w3d, i - 2, j, k), A3(w3d, i - 1, j, k), A3(w3d, i, j, k),
+                     A3(w3d, i + 1, j, k), A3(w3d, i + 2, j, k)) * 0.5f *
+                  (cc2 * (A3(rho, i - 1, j, k) + A3(rho, i, j, k)) + cc1 * (A3(rho, i - 1, j, k - 1) + A3(rho, i, j, k - 1)));
+        A3(dumx, i, j, k) = d6lim(g, f, A3(w3d, i, j, k), A3(w3d, i - 1, j, k));
+      }
+      for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++)
+        A3(advx, i, j, k) = A3(advx, i, j, k) + coef * (A3(dumx, i + 1, j, k) - A3(dumx, i, j, k)) * rf /
+                                                    (0.5f * (A3(rho, i, j, k - 1) + A3(rho, i, j, k)));
+      for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni; i++) {
+        float cc2 = 0.5f * (A3(c2, i, j - 1, k) + A3(c2, i, j, k)), cc1 = 1.0f - cc2;
+        float f = d6(A3(w3d, i, j - 3, k), A3(w3d, i, j - 2, k), A3(w3d, i, j - 1, k), A3(w3d, i, j, k),
+                     A3(w3d, i, j + 1, k), A3(w3d, i, j + 2, k)) * 0.5f *
+                  (cc2 * (A3(rho, i, j - 1, k) + A3(rho, i, j, k)) + cc1 * (A3(rho, i, j - 1, k - 1) + A3(rho, i, j, k - 1)));
+        A3(dumy, i, j, k) = d6lim(g, f, A3(w3d, i, j, k), A3(w3d, i, j - 1, k));
+      }
+      for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++)
+        A3(advy, i, j, k) = A3(advy, i, j, k) + coef * (A3(dumy, i, j + 1, k) - A3(dumy, i, j, k)) * rf /
+                                                    (0.5f * (A3(rho, i, j, k - 1) + A3(rho, i, j, k)));
+    }
   }
   vadv5_w(g, rrw, dumz, w3d);
 #pragma omp parallel for
@@ -1392,6 +1504,14 @@ int oracle_solve2(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_state_t 
   double mass2 = 0.0;
   float cflmax = 0.0f;
   int numq = cfg->imoist ? cfg->numq : 0, npt = cfg->iptra ? cfg->npt : 0;
+  /* 6th-order diffusion: rr = 1/rho as solve3 (solve3.F:660-675) left it at
+   * the end of the previous step, then updated after stages 1 and 2 */
+  const int diffit = diff6_on(g);
+  float *rrbuf = (float *)calloc((size_t)ns, sizeof(float));
+  F3 rr = mkS(g, rrbuf);
+  if (diffit)
+    for (int k = 1; k <= nk; k++) for (int j = 0; j <= nj + 1; j++) for (int i = 0; i <= ni + 1; i++)
+      A3(rr, i, j, k) = 1.0f / A3(s.rho, i, j, k);
 
   for (int nrk = 1; nrk <= 3; nrk++) {
     float dttmp = dt / (float)(3 + 1 - nrk);
@@ -1450,9 +1570,9 @@ int oracle_solve2(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_state_t 
       A3(divx, i, j, k) = d;
     }
     /* solve2.F:884-893 */
-    advu_g(g, &w, divx, rru, s.u3d, uten, rrv, rrw);
-    advv_g(g, &w, divx, rru, rrv, s.v3d, vten, rrw);
-    advw_g(g, &w, divx, rru, rrv, rrw, s.w3d, wten);
+    advu_g(g, &w, divx, rru, s.u3d, uten, rrv, rrw, s.rho, dttmp);
+    advv_g(g, &w, divx, rru, rrv, s.v3d, vten, rrw, s.rho, dttmp);
+    advw_g(g, &w, divx, rru, rrv, rrw, s.w3d, wten, s.rho, dttmp);
     /* solve2.F:899-907 */
 #pragma omp parallel for
     for (int k = 2; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++)
@@ -1488,7 +1608,8 @@ int oracle_solve2(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_state_t 
     for (int k = 1; k <= nk; k++) { float tem = A3(g->th0, 1, 1, k) - TH0R;
       for (int j = g->jb; j <= g->je; j++) for (int i = g->ib; i <= g->ie; i++) A3(sadv, i, j, k) = tem + A3(s.th3d, i, j, k); }
     /* solve2.F:1391-1399 */
-    advs_g(g, &w, nrk, 1, rru, rrv, rrw, divx, s.tha, sadv, thten, 0, 0, dttmp, (double)(10.0f * EPSILON_ADV));
+    advs_g(g, &w, nrk, 1, rru, rrv, rrw, divx, s.tha, sadv, thten, 0, 0, dttmp, (double)(10.0f * EPSILON_ADV),
+           s.rho, rr, diffit);
     /* solve2.F:1419-1425 */
 #pragma omp parallel for
     for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++) {
@@ -1502,7 +1623,7 @@ int oracle_solve2(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_state_t 
       int pdef = (nrk == 3);
       double weps = (double)(cfg->qmag[n] * EPSILON_ADV);
       int pdefweno = (n + 1 == cfg->nqv) ? 0 : 1;
-      advs_g(g, &w, nrk, 1, rru, rrv, rrw, divx, s.qa[n], s.q3d[n], sten, pdef, pdefweno, dttmp, weps);
+      advs_g(g, &w, nrk, 1, rru, rrv, rrw, divx, s.qa[n], s.q3d[n], sten, pdef, pdefweno, dttmp, weps, s.rho, rr, diffit);
 #pragma omp parallel for
       for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++) {
         float v = A3(s.qa[n], i, j, k) + dttmp * A3(sten, i, j, k);
@@ -1512,7 +1633,7 @@ int oracle_solve2(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_state_t 
     }
     /* solve2.F:1556-1656 */
     int dopf = 0;
-    if (nrk == 3) {
+    if (nrk == 3 || diffit) {   /* solve2.F:1582, 1599 */
 #pragma omp parallel for
       for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++) {
         float pi = A3(g->pi0, i, j, k) + A3(s.pp3d, i, j, k);
@@ -1523,7 +1644,7 @@ int oracle_solve2(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_state_t 
         else
           A3(s.rho, i, j, k) = pr / (c.rd * (A3(g->th0, i, j, k) + A3(s.th3d, i, j, k)) * pi);
       }
-      if (cfg->apmasscon == 1) {
+      if (cfg->apmasscon == 1 && nrk == 3) {
 #pragma omp parallel for
         for (int k = 1; k <= nk; k++) {
           double d3 = 0.0, d4 = 0.0;
@@ -1551,13 +1672,18 @@ int oracle_solve2(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_state_t 
       int pdef = (nrk == 3 && cfg->pdtra == 1);
       for (int n = 0; n < npt; n++) {
         for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++) A3(sten, i, j, k) = A3(s.ptten[n], i, j, k);
-        advs_g(g, &w, nrk, 1, rru, rrv, rrw, divx, s.pta[n], s.pt3d[n], sten, pdef, 1, dttmp, (double)(1.0f * EPSILON_ADV));
+        advs_g(g, &w, nrk, 1, rru, rrv, rrw, divx, s.pta[n], s.pt3d[n], sten, pdef, 1, dttmp, (double)(1.0f * EPSILON_ADV),
+               s.rho, rr, diffit);
 #pragma omp parallel for
         for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++)
           A3(s.pt3d[n], i, j, k) = A3(s.pta[n], i, j, k) + dttmp * A3(sten, i, j, k);
         if (nrk <= 2) oracle_bcs_g(g, s.pt3d[n]);
       }
     }
+    /* solve2.F:2036-2046 */
+    if (diffit && nrk < 3)
+      for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++)
+        A3(rr, i, j, k) = 1.0f / A3(s.rho, i, j, k);
     /* solve2.F:1976-2033 */
     if (dopf) {
       __float128 temq1 = 0, temq2 = 0;
@@ -1585,7 +1711,7 @@ int oracle_solve2(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_state_t 
   }
   if (mass2_out) *mass2_out = mass2;
   if (cflmax_out) *cflmax_out = cflmax;
-  free(dumk3); free(dumk4); free(tb); scratch_free(&w);
+  free(dumk3); free(dumk4); free(tb); free(rrbuf); scratch_free(&w);
   return 0;
 }
 
@@ -1672,13 +1798,18 @@ int oracle_advs(const cm1g_config_t *cfg, const cm1g_grid_t *gr, int nrk, int wf
   /* pdef routines write into the halos of dumx/dumy via bcs, the flux arrays
    * are scratch; s, rru, rrv, rrw, divx are read only. */
   advs_g(g, &w, nrk, wflag, mkU(g, rru), mkV(g, rrv), mkW(g, rrw), mkS(g, divx), mkS(g, s0), mkS(g, s), mkS(g, sten),
-         pdef, pdefweno, dt, weps);
+         pdef, pdefweno, dt, weps, mkS(g, s), mkS(g, s), 0);
   scratch_free(&w);
   return 0;
 }
 
-int oracle_advuvw(const cm1g_config_t *cfg, const cm1g_grid_t *gr, const float *u3d, const float *v3d,
+int oracle_advuvw(const cm1g_config_t *cfg_in, const cm1g_grid_t *gr, const float *u3d, const float *v3d,
                   const float *w3d, float *uten, float *vten, float *wten) {
+  /* advection alone: the 6th-order diffusion needs rho, which this entry
+   * point does not take */
+  cm1g_config_t cfgv = *cfg_in;
+  const cm1g_config_t *cfg = &cfgv;
+  cfgv.idiff = 0;
   OG G, *g = &G;
   if (og_setup(g, cfg, gr)) return -1;
   int ni = g->ni, nj = g->nj, nk = g->nk;
@@ -1700,9 +1831,9 @@ int oracle_advuvw(const cm1g_config_t *cfg, const cm1g_grid_t *gr, const float *
     if (fabsf(d) < cfg->smeps) d = 0.0f;
     A3(divx, i, j, k) = d;
   }
-  advu_g(g, &w, divx, rru, u, mkU(g, uten), rrv, rrw);
-  advv_g(g, &w, divx, rru, rrv, v, mkV(g, vten), rrw);
-  advw_g(g, &w, divx, rru, rrv, rrw, ww, mkW(g, wten));
+  advu_g(g, &w, divx, rru, u, mkU(g, uten), rrv, rrw, u, 1.0f);
+  advv_g(g, &w, divx, rru, rrv, v, mkV(g, vten), rrw, v, 1.0f);
+  advw_g(g, &w, divx, rru, rrv, rrw, ww, mkW(g, wten), ww, 1.0f);
   free(tb); scratch_free(&w);
   return 0;
 }

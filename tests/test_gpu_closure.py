@@ -159,7 +159,8 @@ def test_fused_faces_equal_the_three_passes(cm1g):
             a, b = PHI3.cpu().numpy(), PHI1.cpu().numpy()
             assert np.array_equal(np.isnan(a), np.isnan(b))
             ok = ~np.isnan(a)
-            assert ok.mean() > 0.3 and (~ok).any()       # both outcomes occur
+            if widen == 0.0:
+                assert ok.mean() > 0.3 and (~ok).any()   # both outcomes occur
             assert np.array_equal(a[ok], b[ok])
             # the bound itself, from the features: within the widened range of stencil cells 2..5
             x, m, d = X.cpu().numpy(), M.cpu().numpy(), D.cpu().numpy()

@@ -50,6 +50,9 @@ CASES = [
     ("supercell", dict(ni=40, nj=36, nk=40)),
     ("supercell", dict(ni=40, nj=36, nk=40, advwenos=2)),
     ("cbl", dict(ni=48, nj=40, nk=40)),
+    # 6th-order horizontal diffusion (idiff=1, difforder=6), with and without the mdiff limiter
+    ("dry_bubble", dict(diff6=0.04)),
+    ("supercell", dict(ni=40, nj=36, nk=40, diff6=0.04, mdiff=1)),
 ]
 
 

@@ -82,6 +82,30 @@ def test_resting_atmosphere_stays_at_rest(oracle_lib):
     assert cfl == 0.0
 
 
+def test_diffusion_keeps_rest_and_damps_noise(oracle_lib):
+    """6th-order diffusion (adv.F:342-406 and the advu/v/w forms): a resting
+    atmosphere stays at rest with it on; on a noisy field it only removes
+    variance; the mdiff limiter changes the result."""
+    case = _no_perturbation_case(diff6=0.04)
+    case.cfg.apmasscon = 0
+    st, _, _ = oracle_lib.step(case)
+    for f in ("u3d", "v3d", "w3d", "th3d", "pp3d"):
+        assert np.abs(st[f]).max() == 0.0, f
+    runs = {}
+    for label, over in (("plain", {}), ("diff", dict(diff6=0.04)), ("mdiff", dict(diff6=0.04, mdiff=1))):
+        c = make_case("dry_bubble", ni=24, nj=20, nk=20, noise=dict(amp=0.5, zmax=None), **over)
+        runs[label] = (c, oracle_lib.step(c)[0])
+    c, plain = runs["plain"]
+    lay = c.lay
+    th = {k: v[1]["th3d"][lay.interior(1)] for k, v in runs.items()}
+    # the 2-dx content of theta' (second differences in x) is damped
+    d2 = {k: float(np.abs(v[:, :, 2:] - 2 * v[:, :, 1:-1] + v[:, :, :-2]).mean()) for k, v in th.items()}
+    assert d2["diff"] < d2["plain"] and d2["mdiff"] < d2["plain"]
+    assert not np.array_equal(th["diff"], th["mdiff"])
+    for f, stag in (("u3d", 2), ("v3d", 3), ("w3d", 4)):
+        assert not np.array_equal(runs["diff"][1][f][lay.interior(stag)], plain[f][lay.interior(stag)]), f
+
+
 def test_constant_tracer_in_uniform_flow(oracle_lib):
     # flux-form advection of a constant by a non-divergent flow: the s*divx
     # term cancels the flux divergence (adv.F:650-659)
