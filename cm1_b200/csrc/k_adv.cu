@@ -362,7 +362,7 @@ __device__ __forceinline__ float hflux_mom(float r, const float *p, int stride) 
   return r * flx5(up ? a0 : a5, up ? a1 : a4, up ? a2 : a3, up ? a3 : a2, up ? a4 : a1);
 }
 
-template <int TX, int TY, int KC, int STAG>
+template <int TX, int TY, int KC, int STAG, int DIFF>
 __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const float *__restrict__ divx,
                                                       const float *ten1, float *ten,
                                                       const float *__restrict__ th3d, const float *__restrict__ qv,
@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
         if (STAG == 2) r = 0.5f * (r0k * p[2] + r0k * p[3]);
         fx[f] = hflux_mom(r, p, 1);
         fxv[f] = r;
-        if (df.rho) {
+        if (DIFF) {
           // the face between p[2] and p[3]: s-point fxi (u: adv.F:1190-1193),
           // u-point fxi (v: adv.F:2128-2132; w: adv.F:3124-3130)
           const int ii = fxi[s], jj = fxj[s];
@@ -562,7 +562,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
         if (STAG == 3) r = 0.5f * (r0k * p[2 * SP] + r0k * p[3 * SP]);
         fy[f] = hflux_mom(r, p, SP);
         fyv[f] = r;
-        if (df.rho) {
+        if (DIFF) {
           // the face between p[2 SP] and p[3 SP]: v-point fyj (u: adv.F:1210-1215;
           // w: adv.F:3146-3152), s-point fyj (v: adv.F:2151-2153)
           const int ii = fyi[s], jj = fyj[s];
@@ -652,7 +652,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
           advy = advy - ww * (c1k * (RRVk(nj + 1, k - 1) - RRVk(nj, k - 1)) + c2k * (RRVk(nj + 1, k) - RRVk(nj, k))) *
                             g.rdy * LDG(&g.vh[nj - g.jb]);
       }
-      if (df.rho) {   // adv.F:1199-1201, 1220-1222; 2139-2141, 2160-2162; 3135-3137, 3160-3162
+      if (DIFF) {   // adv.F:1199-1201, 1220-1222; 2139-2141, 2160-2162; 3135-3137, 3160-3162
         const float ddx = df.coef * (dfx[xi + 1] - dfx[xi]), ddy = df.coef * (dfy[yi + TX] - dfy[yi]);
         if (STAG == 2) {
           const float rs = LDG(&df.rho[iS(g, i - 1, j, k)]) + LDG(&df.rho[iS(g, i, j, k)]);
@@ -704,17 +704,20 @@ static void mom_tiles_shape(const DGrid &g, const Vel &q, const float *uten1, co
   {
     dim3 grid((g.ni + 1 + TX - 1) / TX, (g.nj + TY - 1) / TY, kch);
     ProfScope _ps("k_advu", st);
-    k_mom_tile<TX, TY, KC, 2><<<grid, blk, 0, st>>>(g, q, divx, uten1, uten, nullptr, nullptr, df);
+    if (df.rho) k_mom_tile<TX, TY, KC, 2, 1><<<grid, blk, 0, st>>>(g, q, divx, uten1, uten, nullptr, nullptr, df);
+    else k_mom_tile<TX, TY, KC, 2, 0><<<grid, blk, 0, st>>>(g, q, divx, uten1, uten, nullptr, nullptr, df);
   }
   {
     dim3 grid((g.ni + TX - 1) / TX, (g.nj + 1 + TY - 1) / TY, kch);
     ProfScope _ps("k_advv", st);
-    k_mom_tile<TX, TY, KC, 3><<<grid, blk, 0, st>>>(g, q, divx, vten1, vten, nullptr, nullptr, df);
+    if (df.rho) k_mom_tile<TX, TY, KC, 3, 1><<<grid, blk, 0, st>>>(g, q, divx, vten1, vten, nullptr, nullptr, df);
+    else k_mom_tile<TX, TY, KC, 3, 0><<<grid, blk, 0, st>>>(g, q, divx, vten1, vten, nullptr, nullptr, df);
   }
   {
     dim3 grid((g.ni + TX - 1) / TX, (g.nj + TY - 1) / TY, kchw);
     ProfScope _ps("k_advw", st);
-    k_mom_tile<TX, TY, KC, 4><<<grid, blk, 0, st>>>(g, q, divx, wten1, wten, th3d, qv, df);
+    if (df.rho) k_mom_tile<TX, TY, KC, 4, 1><<<grid, blk, 0, st>>>(g, q, divx, wten1, wten, th3d, qv, df);
+    else k_mom_tile<TX, TY, KC, 4, 0><<<grid, blk, 0, st>>>(g, q, divx, wten1, wten, th3d, qv, df);
   }
 }
 
@@ -1239,7 +1242,7 @@ struct STileOut {
 // computed once per block; the raw averaged velocities of the faces are kept
 // in shared memory for the divergence terms of the cell owners.  All
 // arrays must have fewer than 2^31 points per horizontal plane.
-template <int TX, int TY, int KC, int MODE, int WENO>
+template <int TX, int TY, int KC, int MODE, int WENO, int DIFF>
 __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STileOut out, int pdef, int pdefweno,
                                                        double weps, float dt, int flush) {
   constexpr int NT = TX * TY;
@@ -1386,7 +1389,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
         const float fl = (ph == ph) ? r * ph : hflux5(r, p[0], p[1], p[2], p[3], p[4], p[5], WENO, pdef, weps);
         fx[f] = fl;
         ux[f] = ru[q];
-        if (a.df.rho) {   // face between s(i-1) and s(i): p[2], p[3]
+        if (DIFF) {   // face between s(i-1) and s(i): p[2], p[3]
           const long ro = (long)k * planeS + fxr[q];                           // rho(i,j)
           const float fd = diff6_stencil(p[0], p[1], p[2], p[3], p[4], p[5]) * 0.5f *
                            (LDG(&a.df.rho[ro - 1]) + LDG(&a.df.rho[ro]));
@@ -1406,7 +1409,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
                                     : hflux5(r, p[0], p[SP], p[2 * SP], p[3 * SP], p[4 * SP], p[5 * SP], WENO, pdef, weps);
         fy[f] = fl;
         vy[f] = rv[q];
-        if (a.df.rho) {   // face between s(j-1) and s(j): p[2 SP], p[3 SP]
+        if (DIFF) {   // face between s(j-1) and s(j): p[2 SP], p[3 SP]
           const long ro = (long)k * planeS + fyo[q];                           // rho(i,j)
           const float fd = diff6_stencil(p[0], p[SP], p[2 * SP], p[3 * SP], p[4 * SP], p[5 * SP]) * 0.5f *
                            (LDG(&a.df.rho[ro - NI]) + LDG(&a.df.rho[ro]));
@@ -1443,7 +1446,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
       if (doite && i == ni && fu1 <= 0.0f) advx = advx - sc * (fu1 - fu0) * g.rdx * uh_i;
       if (doits && j == 1 && fv0 >= 0.0f) advy = advy - sc * (fv1 - fv0) * g.rdy * vh_j;
       if (doitn && j == nj && fv1 <= 0.0f) advy = advy - sc * (fv1 - fv0) * g.rdy * vh_j;
-      if (a.df.rho) {   // adv.F:375-378, 397-400
+      if (DIFF) {   // adv.F:375-378, 397-400
         const float ri = LDG(&a.df.ri[o]);
         advx = advx + a.df.coef * (dfx[xi + 1] - dfx[xi]) * ri * r0k;
         advy = advy + a.df.coef * (dfy[yi + TX] - dfy[yi]) * ri * r0k;
@@ -1497,6 +1500,20 @@ void launch_bc(const DGrid &g, float *a, int which, int wflag, cudaStream_t st, 
 void launch_bc_batch(const DGrid &g, float *const *arrays, const int *which, const int *wflag, int n,
                      cudaStream_t st, int64_t *nlaunch);
 
+// One k_advs_tile launch: WENO and the 6th-order diffusion (a.df.rho set)
+// select compile-time variants, so the plain pass carries no diffusion code.
+template <int TX, int TY, int KC, int MODE>
+static void advs_tile_launch(dim3 grid, dim3 blk, cudaStream_t st, int weno, const DGrid &g, const SAdv &a,
+                             const STileOut &o, int pdef, int pdefweno, double weps, float dt, int flush) {
+  if (a.df.rho) {
+    if (weno) k_advs_tile<TX, TY, KC, MODE, 1, 1><<<grid, blk, 0, st>>>(g, a, o, pdef, pdefweno, weps, dt, flush);
+    else k_advs_tile<TX, TY, KC, MODE, 0, 1><<<grid, blk, 0, st>>>(g, a, o, pdef, pdefweno, weps, dt, flush);
+  } else {
+    if (weno) k_advs_tile<TX, TY, KC, MODE, 1, 0><<<grid, blk, 0, st>>>(g, a, o, pdef, pdefweno, weps, dt, flush);
+    else k_advs_tile<TX, TY, KC, MODE, 0, 0><<<grid, blk, 0, st>>>(g, a, o, pdef, pdefweno, weps, dt, flush);
+  }
+}
+
 // Production scalar pass (MODE_UPDATE, or the pdef two-pass form) with the
 // tile shape TX x TY x KC.
 template <int TX, int TY, int KC>
@@ -1505,8 +1522,7 @@ static void advs_tiled_shape(const DGrid &g, const SAdv &a, STileOut o, int weno
   dim3 blk(TX, TY), grid((g.ni + TX - 1) / TX, (g.nj + TY - 1) / TY, (g.nk + KC - 1) / KC);
   if (!pdef) {
     ProfScope _ps("k_advs_tile", st);
-    if (weno) k_advs_tile<TX, TY, KC, MODE_UPDATE, 1><<<grid, blk, 0, st>>>(g, a, o, 0, pdefweno, weps, dt, flush);
-    else k_advs_tile<TX, TY, KC, MODE_UPDATE, 0><<<grid, blk, 0, st>>>(g, a, o, 0, pdefweno, weps, dt, flush);
+    advs_tile_launch<TX, TY, KC, MODE_UPDATE>(grid, blk, st, weno, g, a, o, 0, pdefweno, weps, dt, flush);
     if (nl) *nl += 1;
     return;
   }
@@ -1515,8 +1531,7 @@ static void advs_tiled_shape(const DGrid &g, const SAdv &a, STileOut o, int weno
   o.dumx = scratch + 3 * n; o.dumy = scratch + 4 * n; o.dumz = scratch + 5 * n;
   {
     ProfScope _ps("k_advs_tile_pdef1", st);
-    if (weno) k_advs_tile<TX, TY, KC, MODE_PDEF1, 1><<<grid, blk, 0, st>>>(g, a, o, 1, pdefweno, weps, dt, flush);
-    else k_advs_tile<TX, TY, KC, MODE_PDEF1, 0><<<grid, blk, 0, st>>>(g, a, o, 1, pdefweno, weps, dt, flush);
+    advs_tile_launch<TX, TY, KC, MODE_PDEF1>(grid, blk, st, weno, g, a, o, 1, pdefweno, weps, dt, flush);
   }
   {
     float *arr[2] = {o.dumx, o.dumy};

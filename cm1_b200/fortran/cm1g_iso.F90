@@ -26,6 +26,7 @@ module cm1g_iso
   public :: cm1g_bcs, cm1g_bcp, cm1g_bcu, cm1g_bcv, cm1g_bcw, cm1g_last_error_f
   public :: cm1g_calcmass, cm1g_calcener, cm1g_dtsmall, cm1g_tendency_init
   public :: cm1g_setup, cm1g_large_step
+  public :: cm1g_tune_t, cm1g_set_tune, cm1g_get_tune, cm1g_autotune
 
   integer(c_int32_t), parameter :: CM1G_MAXQ = 8
 
@@ -62,6 +63,12 @@ module cm1g_iso
     type(c_ptr) :: ppi, pp3d, ppx, ppten, tha, th3d, thten1, rho, prs
     type(c_ptr) :: qa, q3d, qten, pta, pt3d, ptten
     type(c_ptr) :: radbcw, radbce, radbcs, radbcn
+  end type
+
+  ! launch shapes of the large step (cm1g_set_tune / cm1g_autotune)
+  type, bind(C) :: cm1g_tune_t
+    integer(c_int32_t) :: adv_shape, mom_shape, sound_form
+    real(c_float)      :: step_ms
   end type
 
   interface
@@ -172,6 +179,28 @@ module cm1g_iso
     end function
     type(c_ptr) function cm1g_last_error() bind(C, name="cm1g_last_error")
       import :: c_ptr
+    end function
+    integer(c_int) function cm1g_set_tune(ctx, tune) bind(C, name="cm1g_set_tune")
+      import :: c_int, c_ptr, cm1g_tune_t
+      type(c_ptr), value :: ctx
+      type(cm1g_tune_t), intent(in) :: tune
+    end function
+    integer(c_int) function cm1g_get_tune(ctx, tune) bind(C, name="cm1g_get_tune")
+      import :: c_int, c_ptr, cm1g_tune_t
+      type(c_ptr), value :: ctx
+      type(cm1g_tune_t), intent(out) :: tune
+    end function
+    ! times the candidate launch shapes on a copy of st; cache_path: a
+    ! NUL-terminated file name (c_loc of a character array) or c_null_ptr
+    integer(c_int) function cm1g_autotune(ctx, dt, mass1, st, reps, cache_path, tune) bind(C, name="cm1g_autotune")
+      import :: c_int, c_int32_t, c_float, c_double, c_ptr, cm1g_state_t, cm1g_tune_t
+      type(c_ptr), value :: ctx
+      real(c_float), value :: dt
+      real(c_double), value :: mass1
+      type(cm1g_state_t), intent(in) :: st
+      integer(c_int32_t), value :: reps
+      type(c_ptr), value :: cache_path
+      type(cm1g_tune_t), intent(out) :: tune
     end function
   end interface
 
