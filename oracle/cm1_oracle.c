@@ -126,6 +126,13 @@ static long nW(const OG *g) { return (long)g->NI * g->NJ * (g->NK + 1); }
 static char g_err[256];
 const char *oracle_last_error(void) { return g_err; }
 
+/* Arrays that cross the C-ABI structs (cm1g_grid_t, cm1g_state_t) are typed
+ * float there.  RP/RPC view them as this file's real type, so that the FP64
+ * build (oracle/make_r8.py turns every binary32 type, literal and function
+ * of this file into binary64) reads the double arrays its caller passes. */
+#define RP(p) ((float *)(void *)(p))
+#define RPC(p) ((const float *)(const void *)(p))
+
 static int og_setup(OG *g, const cm1g_config_t *cfg, const cm1g_grid_t *gr) {
   memset(g, 0, sizeof(*g));
   g->cfg = cfg;
@@ -151,16 +158,16 @@ static int og_setup(OG *g, const cm1g_config_t *cfg, const cm1g_grid_t *gr) {
     return -1;
   }
   if (gr) {
-    g->uh = gr->uh; g->ruh = gr->ruh; g->uf = gr->uf; g->ruf = gr->ruf;
-    g->vh = gr->vh; g->rvh = gr->rvh; g->vf = gr->vf; g->rvf = gr->rvf;
-    g->mh = mkS(g, gr->mh); g->rmh = mkS(g, gr->rmh); g->c1 = mkS(g, gr->c1); g->c2 = mkS(g, gr->c2);
-    g->mf = mkW(g, gr->mf);
-    g->pi0 = mkS(g, gr->pi0); g->rho0 = mkS(g, gr->rho0); g->rr0 = mkS(g, gr->rr0);
-    g->rf0 = mkS(g, gr->rf0); g->rrf0 = mkS(g, gr->rrf0); g->th0 = mkS(g, gr->th0);
-    g->rth0 = mkS(g, gr->rth0); g->qv0 = mkS(g, gr->qv0); g->qc0 = mkS(g, gr->qc0);
-    g->qi0 = mkS(g, gr->qi0); g->prs0 = mkS(g, gr->prs0);
-    g->u0 = mkU(g, gr->u0); g->v0 = mkV(g, gr->v0);
-    g->dtu0 = mk2(g, gr->dtu0); g->dtv0 = mk2(g, gr->dtv0);
+    g->uh = RPC(gr->uh); g->ruh = RPC(gr->ruh); g->uf = RPC(gr->uf); g->ruf = RPC(gr->ruf);
+    g->vh = RPC(gr->vh); g->rvh = RPC(gr->rvh); g->vf = RPC(gr->vf); g->rvf = RPC(gr->rvf);
+    g->mh = mkS(g, RPC(gr->mh)); g->rmh = mkS(g, RPC(gr->rmh)); g->c1 = mkS(g, RPC(gr->c1)); g->c2 = mkS(g, RPC(gr->c2));
+    g->mf = mkW(g, RPC(gr->mf));
+    g->pi0 = mkS(g, RPC(gr->pi0)); g->rho0 = mkS(g, RPC(gr->rho0)); g->rr0 = mkS(g, RPC(gr->rr0));
+    g->rf0 = mkS(g, RPC(gr->rf0)); g->rrf0 = mkS(g, RPC(gr->rrf0)); g->th0 = mkS(g, RPC(gr->th0));
+    g->rth0 = mkS(g, RPC(gr->rth0)); g->qv0 = mkS(g, RPC(gr->qv0)); g->qc0 = mkS(g, RPC(gr->qc0));
+    g->qi0 = mkS(g, RPC(gr->qi0)); g->prs0 = mkS(g, RPC(gr->prs0));
+    g->u0 = mkU(g, RPC(gr->u0)); g->v0 = mkV(g, RPC(gr->v0));
+    g->dtu0 = mk2(g, RPC(gr->dtu0)); g->dtv0 = mk2(g, RPC(gr->dtv0));
   }
   return 0;
 }
@@ -1391,7 +1398,7 @@ static void getdivx_g(const OG *g, F3 rru, F3 rrv, F3 rrw, F3 divx) {
 static float calccflquick_g(const OG *g, float dt, F3 ua, F3 va, F3 wa) {
   int ni = g->ni, nj = g->nj, nk = g->nk;
   float dtdx = 0.5f * dt * g->rdx, dtdy = 0.5f * dt * g->rdy, dtdz = 0.5f * dt * g->rdz;
-  float fmax = -99999999.0f;
+  float cflmx = -99999999.0f;
   for (int k = 1; k <= nk; k++) {
     float cfl = 0.0f;
     for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++) {
@@ -1401,9 +1408,9 @@ static float calccflquick_g(const OG *g, float dt, F3 ua, F3 va, F3 wa) {
       float wsp = sqrtf((a1 * a1 + a2 * a2) + a3 * a3);
       cfl = fmaxf(cfl, wsp);
     }
-    fmax = fmaxf(fmax, cfl);
+    cflmx = fmaxf(cflmx, cfl);
   }
-  return fmax;
+  return cflmx;
 }
 
 /* pdefq: misclibs.F:1037-1117 (pdscheme=1).  Returns the budget change. */
@@ -1448,17 +1455,17 @@ typedef struct {
 } St;
 
 static void st_view(const OG *g, const cm1g_state_t *s, St *t) {
-  t->ua = mkU(g, s->ua); t->u3d = mkU(g, s->u3d); t->uten1 = mkU(g, s->uten1);
-  t->va = mkV(g, s->va); t->v3d = mkV(g, s->v3d); t->vten1 = mkV(g, s->vten1);
-  t->wa = mkW(g, s->wa); t->w3d = mkW(g, s->w3d); t->wten1 = mkW(g, s->wten1);
-  t->ppi = mkS(g, s->ppi); t->pp3d = mkS(g, s->pp3d); t->ppx = mkS(g, s->ppx); t->ppten = mkS(g, s->ppten);
-  t->tha = mkS(g, s->tha); t->th3d = mkS(g, s->th3d); t->thten1 = mkS(g, s->thten1);
-  t->rho = mkS(g, s->rho); t->prs = mkS(g, s->prs);
+  t->ua = mkU(g, RP(s->ua)); t->u3d = mkU(g, RP(s->u3d)); t->uten1 = mkU(g, RP(s->uten1));
+  t->va = mkV(g, RP(s->va)); t->v3d = mkV(g, RP(s->v3d)); t->vten1 = mkV(g, RP(s->vten1));
+  t->wa = mkW(g, RP(s->wa)); t->w3d = mkW(g, RP(s->w3d)); t->wten1 = mkW(g, RP(s->wten1));
+  t->ppi = mkS(g, RP(s->ppi)); t->pp3d = mkS(g, RP(s->pp3d)); t->ppx = mkS(g, RP(s->ppx)); t->ppten = mkS(g, RP(s->ppten));
+  t->tha = mkS(g, RP(s->tha)); t->th3d = mkS(g, RP(s->th3d)); t->thten1 = mkS(g, RP(s->thten1));
+  t->rho = mkS(g, RP(s->rho)); t->prs = mkS(g, RP(s->prs));
   long n = nS(g);
   int numq = g->cfg->imoist ? g->cfg->numq : 0, npt = g->cfg->iptra ? g->cfg->npt : 0;
-  for (int q = 0; q < numq; q++) { t->qa[q] = mkS(g, s->qa + q * n); t->q3d[q] = mkS(g, s->q3d + q * n); t->qten[q] = mkS(g, s->qten + q * n); }
-  for (int q = 0; q < npt; q++) { t->pta[q] = mkS(g, s->pta + q * n); t->pt3d[q] = mkS(g, s->pt3d + q * n); t->ptten[q] = mkS(g, s->ptten + q * n); }
-  t->radbcw = s->radbcw; t->radbce = s->radbce; t->radbcs = s->radbcs; t->radbcn = s->radbcn;
+  for (int q = 0; q < numq; q++) { t->qa[q] = mkS(g, RP(s->qa) + q * n); t->q3d[q] = mkS(g, RP(s->q3d) + q * n); t->qten[q] = mkS(g, RP(s->qten) + q * n); }
+  for (int q = 0; q < npt; q++) { t->pta[q] = mkS(g, RP(s->pta) + q * n); t->pt3d[q] = mkS(g, RP(s->pt3d) + q * n); t->ptten[q] = mkS(g, RP(s->ptten) + q * n); }
+  t->radbcw = RP(s->radbcw); t->radbce = RP(s->radbce); t->radbcs = RP(s->radbcs); t->radbcn = RP(s->radbcn);
 }
 
 static int check_cfg(const cm1g_config_t *cfg) {
@@ -1764,7 +1771,7 @@ int oracle_step(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_state_t *s
   if (cfg->imoist) {
     double asq = 0.0;
     long n = (long)(cfg->ni + 2 * cfg->ngxy) * (cfg->nj + 2 * cfg->ngxy) * (cfg->nk + 2);
-    rc = oracle_pdefq(cfg, gr, 0.0f, &asq, state->rho, state->q3d + (long)(cfg->nqv - 1) * n);
+    rc = oracle_pdefq(cfg, gr, 0.0f, &asq, RPC(state->rho), RP(state->q3d) + (long)(cfg->nqv - 1) * n);
     if (rc) return rc;
   }
   return oracle_solve3(cfg, gr, state);

@@ -78,5 +78,51 @@ def step(case, state=None, solve2_only=False, mtime=0.0):
     return st, m2.value, cfl.value
 
 
+_LIB_R8 = os.path.join(_HERE, "_r8", "liboracle_r8.so")
+_lib_r8 = None
+
+
+def lib_r8():
+    """The FP64 (-r8) build of the oracle (oracle/make_r8.py)."""
+    global _lib_r8
+    if _lib_r8 is None:
+        if not os.path.exists(_LIB_R8):
+            build()
+        L = C.CDLL(_LIB_R8)
+        cfgp, grp, stp = C.POINTER(Config), C.POINTER(Grid), C.POINTER(State)
+        # every binary32 argument of the FP32 build is binary64 here
+        L.oracle_step.argtypes = [cfgp, grp, stp, C.c_int, C.c_double, C.c_double, C.c_double,
+                                  C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.oracle_last_error.restype = C.c_char_p
+        _lib_r8 = L
+    return _lib_r8
+
+
+def step_r8(case, state=None, nsteps=1):
+    """`nsteps` large steps of the FP64 build from the same (binary32) inputs
+    promoted to float64; returns the float64 state dict."""
+    import numpy as np
+    from cm1_b200.abi import GRID_FIELDS, STATE_FIELDS
+    L = lib_r8()
+    src = case.state if state is None else state
+    st = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in src.items()}
+    grid = {k: np.ascontiguousarray(case.grid[k], dtype=np.float64) for k in GRID_FIELDS}
+    P = C.POINTER(C.c_float)
+    g = Grid()
+    for n in GRID_FIELDS:
+        setattr(g, n, C.cast(C.c_void_p(grid[n].ctypes.data), P))
+    s = State()
+    for n in STATE_FIELDS:
+        a = st.get(n)
+        setattr(s, n, C.cast(C.c_void_p(a.ctypes.data), P) if a is not None and a.size else C.cast(None, P))
+    m2, cfl = C.c_double(0.0), C.c_double(0.0)
+    for _ in range(nsteps):
+        rc = L.oracle_step(C.byref(case.cfg), C.byref(g), C.byref(s), 1, case.dt, 0.0, case.mass1, C.byref(m2),
+                           C.byref(cfl))
+        if rc != 0:
+            raise RuntimeError("FP64 oracle failed: %s" % L.oracle_last_error().decode())
+    return st
+
+
 def threads():
     return lib().oracle_threads()

@@ -76,6 +76,28 @@ def test_one_large_step(name, over, cm1g, oracle_lib):
     assert ctx.launches() > 0
 
 
+@pytest.mark.parametrize("name,over", CASES)
+def test_error_against_fp64_build(name, over, cm1g, oracle_lib):
+    """The error of one large step against the FP64 (-r8) build of the
+    oracle (oracle/make_r8.py), from the same inputs: the CUDA path's FP32
+    result must be as close to it as the FP32 restatement's is (within 2x
+    per field, or 1e-6 of the range)."""
+    torch = _torch()
+    case = make_case(name, **over)
+    ref32, _, _ = oracle_lib.step(case)
+    ref64 = oracle_lib.step_r8(case)
+    ctx = cm1g.Context(case.cfg, case.grid)
+    dev = cm1g.to_device(case.state)
+    ctx.step(dev, case.dt, case.mass1)
+    torch.cuda.synchronize()
+    got = cm1g.to_host(dev)
+    e_gpu, e_ref = field_errors(case, got, ref64), field_errors(case, ref32, ref64)
+    worst = max(e_gpu, key=e_gpu.get)
+    print("%s %s vs FP64: GPU worst %s %.3e, FP32 oracle %.3e" % (name, over, worst, e_gpu[worst], e_ref[worst]))
+    for f in e_gpu:
+        assert e_gpu[f] <= 2.0 * e_ref[f] + 1e-6, (f, e_gpu[f], e_ref[f])
+
+
 @pytest.mark.parametrize("name,over", [CASES[1], CASES[3]])
 def test_one_large_step_column_sweep_sound(name, over, cm1g, oracle_lib, monkeypatch):
     """The same step with the column-sweep acoustic kernel (the form large grids use)."""

@@ -106,6 +106,23 @@ def test_diffusion_keeps_rest_and_damps_noise(oracle_lib):
         assert not np.array_equal(runs["diff"][1][f][lay.interior(stag)], plain[f][lay.interior(stag)]), f
 
 
+def test_fp64_build_agrees_with_fp32(oracle_lib):
+    """The FP64 (-r8) build of the restatement (oracle/make_r8.py) runs the
+    same step from the same inputs; one step apart the two agree to the
+    binary32 rounding of the fields (well inside 1e-3 of each range)."""
+    for name, over in (("dry_bubble", {}), ("supercell", dict(ni=24, nj=20, nk=24))):
+        case = make_case(name, **over)
+        r32, _, _ = oracle_lib.step(case)
+        r64 = oracle_lib.step_r8(case)
+        lay = case.lay
+        for f, stag in (("u3d", 2), ("v3d", 3), ("w3d", 4), ("th3d", 1), ("pp3d", 1), ("rho", 1)):
+            a, b = r32[f][lay.interior(stag)].astype(np.float64), r64[f][lay.interior(stag)]
+            assert b.dtype == np.float64
+            rng = float(b.max() - b.min()) or 1.0
+            err = float(np.abs(a - b).max()) / rng
+            assert 0.0 < err <= 1e-3, (name, f, err)
+
+
 def test_constant_tracer_in_uniform_flow(oracle_lib):
     # flux-form advection of a constant by a non-divergent flow: the s*divx
     # term cancels the flux divergence (adv.F:650-659)
