@@ -105,14 +105,23 @@ def test_one_large_step_column_sweep_sound(name, over, cm1g, oracle_lib, monkeyp
     test_one_large_step(name, over, cm1g, oracle_lib)
 
 
-def test_many_steps_budgets(cm1g, oracle_lib):
-    """Extrema and budgets after 20 steps of the dry bubble (c0 sizes)."""
+@pytest.mark.parametrize("name,over", [("dry_bubble", {}), ("supercell", dict(ni=40, nj=36, nk=40, bc=1))])
+def test_many_steps_budgets(name, over, cm1g, oracle_lib):
+    """Domain max w, min pi', max theta', and the mass and theta budgets
+    after 100 large steps (the dry bubble at c0 sizes; a reduced moist
+    supercell with tracers, periodic), against the oracle; the distance of
+    both from the FP64 build after the same 100 steps is printed.  The open
+    radiative boundaries are left out of this test: with them the restated
+    scheme itself separates a 1e-7 perturbation of theta into 1e-3 of pi''s
+    range within 20 steps (inflow/outflow switches at the boundary), so a
+    1e-3 bar after 100 steps holds for no pair of builds."""
     torch = _torch()
-    case = make_case("dry_bubble")
+    case = make_case(name, **over)
     ref = case.copy_state()
     ctx = cm1g.Context(case.cfg, case.grid)
     dev = cm1g.to_device(case.state)
-    for n in range(20):
+    nsteps = 100
+    for n in range(nsteps):
         ref, m2r, _ = oracle_lib.step(case, ref)
         m2, _ = ctx.step(dev, case.dt, case.mass1, use_graph=(n > 0))
     torch.cuda.synchronize()
@@ -128,6 +137,10 @@ def test_many_steps_budgets(cm1g, oracle_lib):
     th_r = (interior(case, ref["rho"], 1).astype(np.float64) * interior(case, ref["th3d"], 1)).sum()
     assert abs(th_g - th_r) <= TOL_BUDGET * abs(th_r)
     assert abs(m2 - m2r) <= 1e-7 * abs(m2r)
+    r64 = oracle_lib.step_r8(case, nsteps=nsteps)
+    for f, stag, red in [("w3d", 4, np.max), ("pp3d", 1, np.min)]:
+        a, b, c = red(interior(case, got[f], stag)), red(interior(case, ref[f], stag)), red(interior(case, r64[f], stag))
+        print("%s %d steps %s: CUDA %.6e, FP32 oracle %.6e, FP64 %.6e" % (name, nsteps, f, a, b, c))
     del lay
 
 
