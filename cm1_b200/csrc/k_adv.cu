@@ -1,11 +1,13 @@
 // k_adv.cu -- flux-form advection tendencies (adv.F, adv_routines.F).
 //
-// One thread per output point.  Face fluxes are evaluated where they are
-// needed (the two faces of a cell in each direction) instead of being stored
-// in dumx/dumy/dumz, and the rho0-weighted fluxes rru/rrv/rrw and their
-// divergence divx are formed on the fly from the velocities, so a momentum
-// pass reads u, v, w (and theta/qv for buoyancy) and writes only the three
-// tendencies.  Every expression keeps the reference's operand order.
+// The production passes are k-marching tiles (k_mom_tile for u, v, w;
+// k_advs_tile for the scalars): each face flux is evaluated once, from a
+// level staged in shared memory with its 3-point halo, instead of being
+// stored in dumx/dumy/dumz; the rho0-weighted fluxes rru/rrv/rrw and their
+// divergence are formed on the fly, so a momentum pass reads u, v, w (and
+// theta/qv for buoyancy) and writes only the tendency.  The per-point
+// scalar kernels (k_advs, k_advs_pdef1/2) serve the per-routine entry
+// cm1g_advs.  Every expression keeps the reference's operand order.
 #include "cm1g_common.cuh"
 
 namespace cm1g {
@@ -36,208 +38,7 @@ __device__ __forceinline__ float DIVX(const DGrid &g, const Vel &q, int i, int j
   return d;
 }
 
-// ---------------------------------------------------------------------
-// advu: adv.F:911-1839 with hadv_flx5/vadv_flx5 stag=2
-// ---------------------------------------------------------------------
-__device__ __forceinline__ float advu_dumx(const DGrid &g, const Vel &q, int i, int j, int k) {
-  // hadv_flx5 stag=2 at s-point i (adv_routines.F:1388-1397)
-  const float *u = q.u;
-  float ubar = 0.5f * (RRU(g, q, i, j, k) + RRU(g, q, i + 1, j, k));
-  if (ubar >= 0.0f)
-    return ubar * flx5(LDG(&u[iU(g, i - 2, j, k)]), LDG(&u[iU(g, i - 1, j, k)]), LDG(&u[iU(g, i, j, k)]),
-                       LDG(&u[iU(g, i + 1, j, k)]), LDG(&u[iU(g, i + 2, j, k)]));
-  return ubar * flx5(LDG(&u[iU(g, i + 3, j, k)]), LDG(&u[iU(g, i + 2, j, k)]), LDG(&u[iU(g, i + 1, j, k)]),
-                     LDG(&u[iU(g, i, j, k)]), LDG(&u[iU(g, i - 1, j, k)]));
-}
-__device__ __forceinline__ float advu_dumy(const DGrid &g, const Vel &q, int i, int j, int k) {
-  const float *u = q.u;
-  float vbar = 0.5f * (RRV(g, q, i, j, k) + RRV(g, q, i - 1, j, k));
-  if (vbar >= 0.0f)
-    return vbar * flx5(LDG(&u[iU(g, i, j - 3, k)]), LDG(&u[iU(g, i, j - 2, k)]), LDG(&u[iU(g, i, j - 1, k)]),
-                       LDG(&u[iU(g, i, j, k)]), LDG(&u[iU(g, i, j + 1, k)]));
-  return vbar * flx5(LDG(&u[iU(g, i, j + 2, k)]), LDG(&u[iU(g, i, j + 1, k)]), LDG(&u[iU(g, i, j, k)]),
-                     LDG(&u[iU(g, i, j - 1, k)]), LDG(&u[iU(g, i, j - 2, k)]));
-}
-
-// vertical flux of a u- (stag 2) or v- (stag 3) column at w-level kk,
-// vadv_flx5 (adv_routines.F:3299-3364) + vadv_lwr_flx_23/_35.
-template <int STAG>
-__device__ __forceinline__ float vflux_uv(const DGrid &g, const Vel &q, const float *__restrict__ a, int i, int j, int kk) {
-  const int nk = g.nk;
-  auto A = [&](int k) { return LDG(&a[STAG == 2 ? iU(g, i, j, k) : iV(g, i, j, k)]); };
-  float wbar = (STAG == 2) ? 0.5f * (RRW(g, q, i, j, kk) + RRW(g, q, i - 1, j, kk))
-                           : 0.5f * (RRW(g, q, i, j, kk) + RRW(g, q, i, j - 1, kk));
-  if (kk >= 4 && kk <= nk - 2) {
-    if (wbar >= 0.0f) return wbar * flx5(A(kk - 3), A(kk - 2), A(kk - 1), A(kk), A(kk + 1));
-    return wbar * flx5(A(kk + 2), A(kk + 1), A(kk), A(kk - 1), A(kk - 2));
-  }
-  float c2k = LDG(&g.c2[kk]);
-  if (kk == 2) {
-    if (wbar >= 0.0f) { float cc2 = 0.5f * (c2k + c2k), cc1 = 1.0f - cc2; return wbar * (cc1 * A(kk - 1) + cc2 * A(kk)); }
-    return wbar * flx3(A(kk + 1), A(kk), A(kk - 1));
-  }
-  if (kk == nk) {
-    if (wbar >= 0.0f) return wbar * flx3(A(kk - 2), A(kk - 1), A(kk));
-    float cc2 = 0.5f * (c2k + c2k), cc1 = 1.0f - cc2; return wbar * (cc1 * A(kk - 1) + cc2 * A(kk));
-  }
-  if (kk == 3) {
-    if (wbar >= 0.0f) return wbar * flx3(A(kk - 2), A(kk - 1), A(kk));
-    return wbar * flx5(A(kk + 2), A(kk + 1), A(kk), A(kk - 1), A(kk - 2));
-  }
-  // kk == nk-1
-  if (wbar >= 0.0f) return wbar * flx5(A(kk - 3), A(kk - 2), A(kk - 1), A(kk), A(kk + 1));
-  return wbar * flx3(A(kk + 1), A(kk), A(kk - 1));
-}
-
-template <int STAG>
-__device__ __forceinline__ float advz_uv(const DGrid &g, const Vel &q, const float *a, int i, int j, int k) {
-  const float mhk = LDG(&g.mh[k]);
-  if (k == 1) return -vflux_uv<STAG>(g, q, a, i, j, 2) * g.rdz * mhk;
-  if (k == g.nk) return +vflux_uv<STAG>(g, q, a, i, j, g.nk) * g.rdz * mhk;
-  return -(vflux_uv<STAG>(g, q, a, i, j, k + 1) - vflux_uv<STAG>(g, q, a, i, j, k)) * g.rdz * mhk;
-}
-
-__global__ void k_advu(DGrid g, Vel q, const float *uten1, float *uten) {
-  const int i1 = g.ibw ? 2 : 1, i2 = g.ibe ? g.ni : g.ni + 1;
-  const int i = i1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int j = 1 + (int)blockIdx.y, k = 1 + (int)blockIdx.z;
-  if (i > i2) return;
-  const int nj = g.nj;
-  const bool doits = (g.sbc == 2 && g.ibs), doitn = (g.nbc == 2 && g.ibn);
-  float advx = -(advu_dumx(g, q, i, j, k) - advu_dumx(g, q, i - 1, j, k)) * g.rdx * LDG(&g.uf[i - g.ib]);
-  float dyp = advu_dumy(g, q, i, j + 1, k), dy0 = advu_dumy(g, q, i, j, k);
-  if (doits && j == 1 && (RRV(g, q, i, 1, k) + RRV(g, q, i - 1, 1, k)) >= 0.0f) dy0 = advu_dumy(g, q, i, 2, k);
-  if (doitn && j == nj && (RRV(g, q, i, nj + 1, k) + RRV(g, q, i - 1, nj + 1, k)) <= 0.0f) dyp = dy0;
-  float advy = -(dyp - dy0) * g.rdy * LDG(&g.vh[j - g.jb]);
-  if (doits && j == 1 && (RRV(g, q, i, 1, k) + RRV(g, q, i - 1, 1, k)) >= 0.0f)
-    advy = advy - LDG(&q.u[iU(g, i, 1, k)]) * 0.5f *
-                      ((RRV(g, q, i - 1, 2, k) - RRV(g, q, i - 1, 1, k)) + (RRV(g, q, i, 2, k) - RRV(g, q, i, 1, k))) *
-                      g.rdy * LDG(&g.vh[1 - g.jb]);
-  if (doitn && j == nj && (RRV(g, q, i, nj + 1, k) + RRV(g, q, i - 1, nj + 1, k)) <= 0.0f)
-    advy = advy - LDG(&q.u[iU(g, i, nj, k)]) * 0.5f *
-                      ((RRV(g, q, i - 1, nj + 1, k) - RRV(g, q, i - 1, nj, k)) + (RRV(g, q, i, nj + 1, k) - RRV(g, q, i, nj, k))) *
-                      g.rdy * LDG(&g.vh[nj - g.jb]);
-  float advz = advz_uv<2>(g, q, q.u, i, j, k);
-  long o = iU(g, i, j, k);
-  float uu = LDG(&q.u[o]);
-  uten[o] = uten1[o] + (((advx + advy) + advz) + uu * 0.5f * (DIVX(g, q, i, j, k) + DIVX(g, q, i - 1, j, k))) * LDG(&g.rr0[k]);
-}
-
-// ---------------------------------------------------------------------
-// advv: adv.F:1847-2770 with hadv_flx5/vadv_flx5 stag=3
-// ---------------------------------------------------------------------
-__device__ __forceinline__ float advv_dumx(const DGrid &g, const Vel &q, int i, int j, int k) {
-  const float *v = q.v;
-  float ubar = 0.5f * (RRU(g, q, i, j, k) + RRU(g, q, i, j - 1, k));
-  if (ubar >= 0.0f)
-    return ubar * flx5(LDG(&v[iV(g, i - 3, j, k)]), LDG(&v[iV(g, i - 2, j, k)]), LDG(&v[iV(g, i - 1, j, k)]),
-                       LDG(&v[iV(g, i, j, k)]), LDG(&v[iV(g, i + 1, j, k)]));
-  return ubar * flx5(LDG(&v[iV(g, i + 2, j, k)]), LDG(&v[iV(g, i + 1, j, k)]), LDG(&v[iV(g, i, j, k)]),
-                     LDG(&v[iV(g, i - 1, j, k)]), LDG(&v[iV(g, i - 2, j, k)]));
-}
-__device__ __forceinline__ float advv_dumy(const DGrid &g, const Vel &q, int i, int j, int k) {
-  const float *v = q.v;
-  float vbar = 0.5f * (RRV(g, q, i, j, k) + RRV(g, q, i, j + 1, k));
-  if (vbar >= 0.0f)
-    return vbar * flx5(LDG(&v[iV(g, i, j - 2, k)]), LDG(&v[iV(g, i, j - 1, k)]), LDG(&v[iV(g, i, j, k)]),
-                       LDG(&v[iV(g, i, j + 1, k)]), LDG(&v[iV(g, i, j + 2, k)]));
-  return vbar * flx5(LDG(&v[iV(g, i, j + 3, k)]), LDG(&v[iV(g, i, j + 2, k)]), LDG(&v[iV(g, i, j + 1, k)]),
-                     LDG(&v[iV(g, i, j, k)]), LDG(&v[iV(g, i, j - 1, k)]));
-}
-
-__global__ void k_advv(DGrid g, Vel q, const float *vten1, float *vten) {
-  const int j1 = g.ibs ? 2 : 1, j2 = g.ibn ? g.nj : g.nj + 1;
-  const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int j = j1 + (int)blockIdx.y, k = 1 + (int)blockIdx.z;
-  if (i > g.ni || j > j2) return;
-  const int ni = g.ni;
-  const bool doitw = (g.wbc == 2 && g.ibw), doite = (g.ebc == 2 && g.ibe);
-  float dx0 = advv_dumx(g, q, i, j, k), dxp = advv_dumx(g, q, i + 1, j, k);
-  if (doitw && i == 1 && (RRU(g, q, 1, j, k) + RRU(g, q, 1, j - 1, k)) >= 0.0f) dx0 = advv_dumx(g, q, 2, j, k);
-  if (doite && i == ni && (RRU(g, q, ni + 1, j, k) + RRU(g, q, ni + 1, j - 1, k)) <= 0.0f) dxp = dx0;
-  float advx = -(dxp - dx0) * g.rdx * LDG(&g.uh[i - g.ib]);
-  float advy = -(advv_dumy(g, q, i, j, k) - advv_dumy(g, q, i, j - 1, k)) * g.rdy * LDG(&g.vf[j - g.jb]);
-  if (doitw && i == 1 && (RRU(g, q, 1, j, k) + RRU(g, q, 1, j - 1, k)) >= 0.0f)
-    advx = advx - LDG(&q.v[iV(g, 1, j, k)]) * 0.5f *
-                      ((RRU(g, q, 2, j - 1, k) - RRU(g, q, 1, j - 1, k)) + (RRU(g, q, 2, j, k) - RRU(g, q, 1, j, k))) *
-                      g.rdx * LDG(&g.uh[1 - g.ib]);
-  if (doite && i == ni && (RRU(g, q, ni + 1, j, k) + RRU(g, q, ni + 1, j - 1, k)) <= 0.0f)
-    advx = advx - LDG(&q.v[iV(g, ni, j, k)]) * 0.5f *
-                      ((RRU(g, q, ni + 1, j - 1, k) - RRU(g, q, ni, j - 1, k)) + (RRU(g, q, ni + 1, j, k) - RRU(g, q, ni, j, k))) *
-                      g.rdx * LDG(&g.uh[ni - g.ib]);
-  float advz = advz_uv<3>(g, q, q.v, i, j, k);
-  long o = iV(g, i, j, k);
-  float vv = LDG(&q.v[o]);
-  vten[o] = vten1[o] + (((advx + advy) + advz) + vv * 0.5f * (DIVX(g, q, i, j, k) + DIVX(g, q, i, j - 1, k))) * LDG(&g.rr0[k]);
-}
-
-// ---------------------------------------------------------------------
-// advw: adv.F:2778-3610 with hadv_flx5/vadv_flx5 stag=4, plus the
-// buoyancy term of solve2.F:899-907 when th3d is given.
-// ---------------------------------------------------------------------
-__device__ __forceinline__ float advw_dumx(const DGrid &g, const Vel &q, int i, int j, int k, float *ubar_out) {
-  const float *w = q.w;
-  float c2k = LDG(&g.c2[k]);
-  float cc2 = 0.5f * (c2k + c2k), cc1 = 1.0f - cc2;
-  float ubar = cc2 * RRU(g, q, i, j, k) + cc1 * RRU(g, q, i, j, k - 1);
-  if (ubar_out) *ubar_out = ubar;
-  if (ubar >= 0.0f)
-    return ubar * flx5(LDG(&w[iW(g, i - 3, j, k)]), LDG(&w[iW(g, i - 2, j, k)]), LDG(&w[iW(g, i - 1, j, k)]),
-                       LDG(&w[iW(g, i, j, k)]), LDG(&w[iW(g, i + 1, j, k)]));
-  return ubar * flx5(LDG(&w[iW(g, i + 2, j, k)]), LDG(&w[iW(g, i + 1, j, k)]), LDG(&w[iW(g, i, j, k)]),
-                     LDG(&w[iW(g, i - 1, j, k)]), LDG(&w[iW(g, i - 2, j, k)]));
-}
-__device__ __forceinline__ float advw_dumy(const DGrid &g, const Vel &q, int i, int j, int k, float *vbar_out) {
-  const float *w = q.w;
-  float c2k = LDG(&g.c2[k]);
-  float cc2 = 0.5f * (c2k + c2k), cc1 = 1.0f - cc2;
-  float vbar = cc2 * RRV(g, q, i, j, k) + cc1 * RRV(g, q, i, j, k - 1);
-  if (vbar_out) *vbar_out = vbar;
-  if (vbar >= 0.0f)
-    return vbar * flx5(LDG(&w[iW(g, i, j - 3, k)]), LDG(&w[iW(g, i, j - 2, k)]), LDG(&w[iW(g, i, j - 1, k)]),
-                       LDG(&w[iW(g, i, j, k)]), LDG(&w[iW(g, i, j + 1, k)]));
-  return vbar * flx5(LDG(&w[iW(g, i, j + 2, k)]), LDG(&w[iW(g, i, j + 1, k)]), LDG(&w[iW(g, i, j, k)]),
-                     LDG(&w[iW(g, i, j - 1, k)]), LDG(&w[iW(g, i, j - 2, k)]));
-}
-// vadv_flx5 stag=4 at s-level kk (adv_routines.F:3366-3384, 4979-5000, 5148-5172)
-__device__ __forceinline__ float vflux_w(const DGrid &g, const Vel &q, int i, int j, int kk) {
-  const int nk = g.nk;
-  const float *w = q.w;
-  auto A = [&](int k) { return LDG(&w[iW(g, i, j, k)]); };
-  float wbar = 0.5f * (RRW(g, q, i, j, kk) + RRW(g, q, i, j, kk + 1));
-  if (kk >= 3 && kk <= nk - 2) {
-    if (wbar >= 0.0f) return wbar * flx5(A(kk - 2), A(kk - 1), A(kk), A(kk + 1), A(kk + 2));
-    return wbar * flx5(A(kk + 3), A(kk + 2), A(kk + 1), A(kk), A(kk - 1));
-  }
-  if (kk == 1) {
-    if (wbar >= 0.0f) return wbar * 0.5f * (A(kk) + A(kk + 1));
-    return wbar * flx3(A(kk + 2), A(kk + 1), A(kk));
-  }
-  if (kk == nk) {
-    if (wbar >= 0.0f) return wbar * flx3(A(kk - 1), A(kk), A(kk + 1));
-    return wbar * 0.5f * (A(kk) + A(kk + 1));
-  }
-  if (kk == 2) {
-    if (wbar >= 0.0f) return wbar * flx3(A(kk - 1), A(kk), A(kk + 1));
-    return wbar * flx5(A(kk + 3), A(kk + 2), A(kk + 1), A(kk), A(kk - 1));
-  }
-  // kk == nk-1
-  if (wbar >= 0.0f) return wbar * flx5(A(kk - 2), A(kk - 1), A(kk), A(kk + 1), A(kk + 2));
-  return wbar * flx3(A(kk + 2), A(kk + 1), A(kk));
-}
-
-// buoyancy at s-points (solve2.F:313-440)
-__device__ __forceinline__ float buoy(const DGrid &g, const float *th3d, const float *qv, int i, int j, int k) {
-  float th3 = LDG(&th3d[iS(g, i, j, k)]);
-  if (qv) {
-    float q = fmaxf(LDG(&qv[iS(g, i, j, k)]), 0.0f);
-    float qli = fmaxf(0.0f, 0.0f + 0.0f);
-    return g.c.g * ((th3 * LDG(&g.rth0[k]) + g.c.repsm1 * (q - LDG(&g.qv0[k]))) - ((qli - LDG(&g.qc0[k])) - LDG(&g.qi0[k])));
-  }
-  return g.c.g * th3 * LDG(&g.rth0[k]);
-}
-
-// buoy() from values already loaded: th = th3d(i,j,kk), q = qv(i,j,kk)
+// buoyancy of a w level from th3d(i,j,kk) and qv(i,j,kk) (solve2.F:313-446, dum8 of the moist and dry forms)
 __device__ __forceinline__ float buoy_v(const DGrid &g, float th3, float qvv, bool moist, int kk) {
   if (moist) {
     float q = fmaxf(qvv, 0.0f);
@@ -247,43 +48,6 @@ __device__ __forceinline__ float buoy_v(const DGrid &g, float th3, float qvv, bo
   return g.c.g * th3 * LDG(&g.rth0[kk]);
 }
 
-__global__ void k_advw(DGrid g, Vel q, const float *wten1, float *wten,
-                       const float *__restrict__ th3d, const float *__restrict__ qv) {
-  const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int j = 1 + (int)blockIdx.y, k = 2 + (int)blockIdx.z;
-  if (i > g.ni) return;
-  const int ni = g.ni, nj = g.nj;
-  const bool doitw = (g.wbc == 2 && g.ibw), doite = (g.ebc == 2 && g.ibe);
-  const bool doits = (g.sbc == 2 && g.ibs), doitn = (g.nbc == 2 && g.ibn);
-  float ub0, ubp, vb0, vbp;
-  float dx0 = advw_dumx(g, q, i, j, k, &ub0), dxp = advw_dumx(g, q, i + 1, j, k, &ubp);
-  if (doitw && i == 1 && ub0 >= 0.0f) dx0 = advw_dumx(g, q, 2, j, k, nullptr);
-  if (doite && i == ni && ubp <= 0.0f) dxp = dx0;
-  float dy0 = advw_dumy(g, q, i, j, k, &vb0), dyp = advw_dumy(g, q, i, j + 1, k, &vbp);
-  if (doits && j == 1 && vb0 >= 0.0f) dy0 = advw_dumy(g, q, i, 2, k, nullptr);
-  if (doitn && j == nj && vbp <= 0.0f) dyp = dy0;
-  float advx = -(dxp - dx0) * g.rdx * LDG(&g.uh[i - g.ib]);
-  float advy = -(dyp - dy0) * g.rdy * LDG(&g.vh[j - g.jb]);
-  const float c1k = LDG(&g.c1[k]), c2k = LDG(&g.c2[k]);
-  long o = iW(g, i, j, k);
-  const float ww = LDG(&q.w[o]);
-  if (doitw && i == 1 && ub0 >= 0.0f)
-    advx = advx - ww * (c1k * (RRU(g, q, 2, j, k - 1) - RRU(g, q, 1, j, k - 1)) + c2k * (RRU(g, q, 2, j, k) - RRU(g, q, 1, j, k))) *
-                      g.rdx * LDG(&g.uh[1 - g.ib]);
-  if (doite && i == ni && ubp <= 0.0f)
-    advx = advx - ww * (c1k * (RRU(g, q, ni + 1, j, k - 1) - RRU(g, q, ni, j, k - 1)) + c2k * (RRU(g, q, ni + 1, j, k) - RRU(g, q, ni, j, k))) *
-                      g.rdx * LDG(&g.uh[ni - g.ib]);
-  if (doits && j == 1 && vb0 >= 0.0f)
-    advy = advy - ww * (c1k * (RRV(g, q, i, 2, k - 1) - RRV(g, q, i, 1, k - 1)) + c2k * (RRV(g, q, i, 2, k) - RRV(g, q, i, 1, k))) *
-                      g.rdy * LDG(&g.vh[1 - g.jb]);
-  if (doitn && j == nj && vbp <= 0.0f)
-    advy = advy - ww * (c1k * (RRV(g, q, i, nj + 1, k - 1) - RRV(g, q, i, nj, k - 1)) + c2k * (RRV(g, q, i, nj + 1, k) - RRV(g, q, i, nj, k))) *
-                      g.rdy * LDG(&g.vh[nj - g.jb]);
-  float advz = -(vflux_w(g, q, i, j, k) - vflux_w(g, q, i, j, k - 1)) * g.rdz * LDG(&g.mf[k]);
-  float t = wten1[o] + (((advx + advy) + advz) + ww * (c2k * DIVX(g, q, i, j, k) + c1k * DIVX(g, q, i, j, k - 1))) * LDG(&g.rrf0[k]);
-  if (th3d) t = t + (c1k * buoy(g, th3d, qv, i, j, k - 1) + c2k * buoy(g, th3d, qv, i, j, k));
-  wten[o] = t;
-}
 
 // ---------------------------------------------------------------------
 // Tiled momentum advection (the production path of advu/advv/advw).

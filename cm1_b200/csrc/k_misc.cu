@@ -399,15 +399,6 @@ __global__ void k_copy_batch(CopyBatch b) {
   for (int i = c.ilo + lane; i <= c.ihi; i += 32) c.dst[base + i] = LDG(&c.src[base + i]);
 }
 
-__global__ void k_copy_range(long pitch, long plane, int ib, int jb, int ilo, int ihi, int jlo, int jhi, int nk,
-                             const float *__restrict__ src, float *__restrict__ dst) {
-  const int i = ilo + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int j = jlo + (int)blockIdx.y, k = 1 + (int)blockIdx.z;
-  if (i > ihi || j > jhi || k > nk) return;
-  const long o = (long)(i - ib) + pitch * (long)(j - jb) + plane * (long)k;
-  dst[o] = LDG(&src[o]);
-}
-
 void launch_ppx_update(const DGrid &g, const float *pp3d, float *ppx, cudaStream_t st, int64_t *nl) {
   dim3 grid((g.ni + 127) / 128, g.nj, g.nk);
   { ProfScope _ps("k_ppx_update", st); k_ppx_update<<<grid, 128, 0, st>>>(g, pp3d, ppx); }
