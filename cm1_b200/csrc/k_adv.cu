@@ -29,6 +29,25 @@ __device__ __forceinline__ float RRW(const DGrid &g, const Vel &q, int i, int j,
   if (k <= 1 || k >= g.nk + 1) return 0.0f;                       // solve2.F:509-511
   return LDG(&g.rf0[k]) * LDG(&q.w[iW(g, i, j, k)]);              // solve2.F:516
 }
+// Face loop of the tiles: each thread owns face `tid` of each direction,
+// and the faces past one per thread (NFX - NT x-faces, NFY - NT y-faces)
+// go to the threads from warp 1 (x) and the warps after those (y), so that
+// the second pass of the loop is spread over other warps than the first.
+template <int NT, int NFX, int NFY>
+struct FaceSlots {
+  static constexpr int X1 = 32;
+  static constexpr int Y1 = 32 * (1 + (NFX - NT + 31) / 32);
+  static_assert(NFX >= NT && NFY >= NT, "at least one face per thread");
+  static_assert(X1 + (NFX - NT) <= NT && Y1 + (NFY - NT) <= NT, "the extra faces fit the block");
+  // face index of slot q (0 or 1) of thread tid; >= NFX / NFY: none
+  __device__ static __forceinline__ int x(int tid, int q) {
+    return q == 0 ? tid : ((tid >= X1 && tid < X1 + NFX - NT) ? NT + tid - X1 : NFX);
+  }
+  __device__ static __forceinline__ int y(int tid, int q) {
+    return q == 0 ? tid : ((tid >= Y1 && tid < Y1 + NFY - NT) ? NT + tid - Y1 : NFY);
+  }
+};
+
 // divx of the momentum pass (solve2.F:590-596)
 __device__ __forceinline__ float DIVX(const DGrid &g, const Vel &q, int i, int j, int k) {
   float d = ((RRU(g, q, i + 1, j, k) - RRU(g, q, i, j, k)) * g.rdx * LDG(&g.uh[i - g.ib]) +
@@ -167,18 +186,19 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
     }
   }
   // faces owned by this thread: index-space position (-1 in fxi: none)
+  using FS = FaceSlots<NT, NFX, NFY>;
   int fxi[2], fxj[2], fyi[2], fyj[2];
 #pragma unroll
   for (int s = 0; s < 2; s++) {
-    const int f = tid + s * NT;
     fxi[s] = -1; fxj[s] = 0; fyi[s] = -1; fyj[s] = 0;
+    const int f = FS::x(tid, s), fy_ = FS::y(tid, s);
     if (f < NFX) {
       const int row = f / (TX + 1), col = f - row * (TX + 1);
       const int ii = (STAG == 2) ? i0 - 1 + col : i0 + col, jj = j0 + row;   // s-point (u) or u-point (v, w)
       if (ii >= 0 && ii <= ni + 1 && jj <= nj + 1) { fxi[s] = ii; fxj[s] = jj; }
     }
-    if (f < NFY) {
-      const int row = f / TX, col = f - row * TX;
+    if (fy_ < NFY) {
+      const int row = fy_ / TX, col = fy_ - row * TX;
       const int ii = i0 + col, jj = (STAG == 3) ? j0 - 1 + row : j0 + row;    // s-point (v) or v-point (u, w)
       if (jj >= 0 && jj <= nj + 1 && ii <= ni + 1) { fyi[s] = ii; fyj[s] = jj; }
     }
@@ -293,7 +313,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
     __syncthreads();
 #pragma unroll
     for (int s = 0; s < 2; s++) {
-      const int f = tid + s * NT;
+      const int f = FS::x(tid, s);
       if (fxi[s] >= 0) {
         const int row = f / (TX + 1), col = f - row * (TX + 1);
         const float *p = &ss[(row + 3) * SP + col];
@@ -320,12 +340,13 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
         }
       }
       if (fyi[s] >= 0) {
-        const int row = f / TX, col = f - row * TX;
+        const int fy_ = FS::y(tid, s);
+        const int row = fy_ / TX, col = fy_ - row * TX;
         const float *p = &ss[row * SP + col + 3];
         float r = vbar[s];
         if (STAG == 3) r = 0.5f * (r0k * p[2 * SP] + r0k * p[3 * SP]);
-        fy[f] = hflux_mom(r, p, SP);
-        fyv[f] = r;
+        fy[fy_] = hflux_mom(r, p, SP);
+        fyv[fy_] = r;
         if (DIFF) {
           // the face between p[2 SP] and p[3 SP]: v-point fyj (u: adv.F:1210-1215;
           // w: adv.F:3146-3152), s-point fyj (v: adv.F:2151-2153)
@@ -341,7 +362,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
             fd = d * 0.5f * (cc2 * (LDG(&df.rho[iS(g, ii, jj - 1, k)]) + LDG(&df.rho[iS(g, ii, jj, k)])) +
                              cc1 * (LDG(&df.rho[iS(g, ii, jj - 1, k - 1)]) + LDG(&df.rho[iS(g, ii, jj, k - 1)])));
           }
-          dfy[f] = diff6_limit(fd, p[3 * SP], p[2 * SP], df.mdiff);
+          dfy[fy_] = diff6_limit(fd, p[3 * SP], p[2 * SP], df.mdiff);
         }
       }
     }
@@ -1043,9 +1064,10 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
   int fxo[2], fxs[2], fyo[2], fys[2];   // face offsets (-1: no face) and stencil starts in ss
   int fxl[2], fyl[2];                   // in-level index of the face in the learned-value arrays
   int fxr[2];                           // s-plane offset of the cell (i, j) right of an x-face
+  using FS = FaceSlots<NT, NFX, NFY>;
 #pragma unroll
   for (int q = 0; q < 2; q++) {
-    const int f = tid + q * NT;
+    const int f = FS::x(tid, q), fy_ = FS::y(tid, q);
     fxo[q] = -1; fxs[q] = 0; fyo[q] = -1; fys[q] = 0; fxl[q] = 0; fyl[q] = 0; fxr[q] = 0;
     if (f < NFX) {
       const int row = f / (TX + 1), col = f - row * (TX + 1);
@@ -1056,8 +1078,8 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
         fxr[q] = (ii - g.ib) + NI * (jj - g.jb);
       }
     }
-    if (f < NFY) {
-      const int row = f / TX, col = f - row * TX;
+    if (fy_ < NFY) {
+      const int row = fy_ / TX, col = fy_ - row * TX;
       const int ii = i0 + col, jj = j0 + row;
       if (ii <= ni && jj <= nj + 1) {
         fyo[q] = (ii - g.ib) + NI * (jj - g.jb); fys[q] = row * SP + col + 3;
@@ -1144,7 +1166,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
     // ---- face values: each x/y face once, each upper z face once per column
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-      const int f = tid + q * NT;
+      const int f = FS::x(tid, q), fy_ = FS::y(tid, q);
       if (fxo[q] >= 0) {
         const float *p = &ss[fxs[q]];
         const float r = ru[q] * r0k;
@@ -1171,13 +1193,13 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
         if (MODE == MODE_UPDATE && out.ex.phiy) ph = out.ex.phiy[(long)(k - 1) * ni * (nj + 1) + fyl[q]];
         const float fl = (ph == ph) ? r * ph
                                     : hflux5(r, p[0], p[SP], p[2 * SP], p[3 * SP], p[4 * SP], p[5 * SP], WENO, pdef, weps);
-        fy[f] = fl;
-        vy[f] = rv[q];
+        fy[fy_] = fl;
+        vy[fy_] = rv[q];
         if (DIFF) {   // face between s(j-1) and s(j): p[2 SP], p[3 SP]
           const long ro = (long)k * planeS + fyo[q];                           // rho(i,j)
           const float fd = diff6_stencil(p[0], p[SP], p[2 * SP], p[3 * SP], p[4 * SP], p[5 * SP]) * 0.5f *
                            (LDG(&a.df.rho[ro - NI]) + LDG(&a.df.rho[ro]));
-          dfy[f] = diff6_limit(fd, p[3 * SP], p[2 * SP], a.df.mdiff);
+          dfy[fy_] = diff6_limit(fd, p[3 * SP], p[2 * SP], a.df.mdiff);
         }
         if (MODE == MODE_UPDATE && out.ex.capfy) {
           out.ex.capfy[(long)k * planeV + fyo[q]] = fl;
