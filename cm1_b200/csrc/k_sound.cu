@@ -213,33 +213,46 @@ __global__ void __launch_bounds__(TX * NW, CM1G_SND_MINB) k_sound_tile(DGrid g, 
   __syncthreads();
 
   // ---------------- phase 2: Thomas solve for w, k = 2..nk ----------------
+  // The first and last levels are peeled off so that the loop body has no
+  // branches and its shared-memory reads (independent of the recurrence)
+  // can be issued ahead of the dependent chain; nk >= 6 (cm1g_init).
   if (w == 0 && active) {
-    float d1p = 0.0f, d2p = 0.0f;
-    for (int k = 2; k <= nk; k++) {
+    float d1p, d2p;
+    {
+      const int k = 2;
       const float mm = S(MM, k);
       const float bb = 1.0f - asq * (+mm * (-S(P1, k) + S(P2, k - 1)));
       const float dd = S(DD, k) + alph * (-mm * (S(PF, k) - S(PF, k - 1)));
+      const float cc = -asq * (-mm * S(P2, k));
       // __frcp_rn is the correctly rounded 1/x, the same value as 1.0f/x
-      if (k == 2) {
-        const float cc = -asq * (-mm * S(P2, k));
-        const float rr = __frcp_rn(bb);
-        d1p = -cc * rr;
-        d2p = dd * rr;
-        S(MM, k) = d1p; S(DD, k) = d2p;
-      } else {
-        const float aa = -asq * (+mm * S(P1, k - 1));
-        const float rr = __frcp_rn(aa * d1p + bb);
-        if (k < nk) {
-          const float cc = -asq * (-mm * S(P2, k));
-          d1p = -cc * rr;
-          d2p = (dd - aa * d2p) * rr;
-          S(MM, k) = d1p; S(DD, k) = d2p;
-        } else {
-          S(DD, k) = (dd - aa * d2p) * rr;   // w(nk)
-        }
-      }
+      const float rr = __frcp_rn(bb);
+      d1p = -cc * rr;
+      d2p = dd * rr;
+      S(MM, k) = d1p; S(DD, k) = d2p;
+    }
+#pragma unroll 4
+    for (int k = 3; k < nk; k++) {
+      const float mm = S(MM, k);
+      const float bb = 1.0f - asq * (+mm * (-S(P1, k) + S(P2, k - 1)));
+      const float dd = S(DD, k) + alph * (-mm * (S(PF, k) - S(PF, k - 1)));
+      const float aa = -asq * (+mm * S(P1, k - 1));
+      const float cc = -asq * (-mm * S(P2, k));
+      const float rr = __frcp_rn(aa * d1p + bb);
+      d1p = -cc * rr;
+      d2p = (dd - aa * d2p) * rr;
+      S(MM, k) = d1p; S(DD, k) = d2p;
+    }
+    {
+      const int k = nk;
+      const float mm = S(MM, k);
+      const float bb = 1.0f - asq * (+mm * (-S(P1, k) + S(P2, k - 1)));
+      const float dd = S(DD, k) + alph * (-mm * (S(PF, k) - S(PF, k - 1)));
+      const float aa = -asq * (+mm * S(P1, k - 1));
+      const float rr = __frcp_rn(aa * d1p + bb);
+      S(DD, k) = (dd - aa * d2p) * rr;   // w(nk)
     }
     float wup = S(DD, nk);
+#pragma unroll 4
     for (int k = nk - 1; k >= 2; k--) {
       wup = S(MM, k) * wup + S(DD, k);
       S(DD, k) = wup;
