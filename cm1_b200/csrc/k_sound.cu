@@ -212,6 +212,23 @@ __global__ void __launch_bounds__(TX * NW, CM1G_SND_MINB) k_sound_tile(DGrid g, 
   }
   __syncthreads();
 
+  // phase 3's global inputs of this warp's levels (pi' before the step and
+  // the running sum of w; the column's own points), loaded now so that they
+  // arrive while warp 0 runs the Thomas solve
+  float ppo[KPT], acs[KPT];
+  if (active) {
+#pragma unroll
+    for (int m = 0; m < KPT; m++) {
+      const int k = 1 + w + m * NW;
+      ppo[m] = 0.0f; acs[m] = 0.0f;
+      if (k <= nk) {
+        const long o = iS(g, i, j, k);
+        ppo[m] = io.pp_in[o];
+        acs[m] = p.first ? LDG(&io.wa[o]) * beta : io.rrw[o];
+      }
+    }
+  }
+
   // ---------------- phase 2: Thomas solve for w, k = 2..nk ----------------
   // The first and last levels are peeled off so that the loop body has no
   // branches and its shared-memory reads (independent of the recurrence)
@@ -262,7 +279,7 @@ __global__ void __launch_bounds__(TX * NW, CM1G_SND_MINB) k_sound_tile(DGrid g, 
 
   // ---------------- phase 3 ----------------
   if (active) {
-#pragma unroll 1
+#pragma unroll
     for (int m = 0; m < KPT; m++) {
       const int k = 1 + w + m * NW;
       if (k > nk) break;
@@ -271,10 +288,8 @@ __global__ void __launch_bounds__(TX * NW, CM1G_SND_MINB) k_sound_tile(DGrid g, 
       const float wkp = (k < nk) ? S(DD, k + 1) : 0.0f;
       float pn = S(PF, k) + alph * (wk * S(P1, k) + wkp * S(P2, k));
       if (fabsf(pn) < g.smeps) pn = 0.0f;
-      // pi' before the step and the running sum of w are re-read here (the
-      // column's own points, still in L2 from phase 1)
-      const float d1 = g.kdiv * (pn - io.pp_in[o]);
-      const float ac = p.first ? LDG(&io.wa[o]) * beta : io.rrw[o];
+      const float d1 = g.kdiv * (pn - ppo[m]);
+      const float ac = acs[m];
       io.pp_out[o] = pn;
       io.ppd_out[o] = pn + d1;
       if (p.write_ppx) io.ppx[o] = d1;
