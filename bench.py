@@ -264,9 +264,8 @@ def main():
     from cm1_b200.cases import make_case
     from cm1_b200 import binding
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from cm1_b200.replicas import rank_env, replica_seed, max_over_ranks, job_value
+    world, rank, local = rank_env()
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -274,7 +273,7 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    case = make_case(args.workload, seed=1234 + rank)
+    case = make_case(args.workload, seed=replica_seed(rank))
     cfg = case.cfg
     cells = cfg.ni * cfg.nj * cfg.nk
     ctx = binding.Context(cfg, case.grid)
@@ -303,13 +302,11 @@ def main():
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
     launches = ctx.launches() - n0
+    ms = max_over_ranks(ms, dist, device="cuda")
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     ms_step = ms / args.steps
-    value = world * cells * args.steps / (ms * 1e-3)
+    value = job_value(world, cells, args.steps, ms)
 
     # ---- per-kernel device times (profiled pass, eager launches)
     ctx.profile(True)
@@ -351,11 +348,8 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-    e2e_value = world * cells * e2e_steps / (ms_e2e * 1e-3)
+    ms_e2e = max_over_ranks(ms_e2e, dist, device="cuda")
+    e2e_value = job_value(world, cells, e2e_steps, ms_e2e)
 
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
