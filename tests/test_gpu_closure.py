@@ -196,3 +196,25 @@ def test_closure_in_the_step(cm1g):
     rng_ = float(th_p[sl].max() - th_p[sl].min())
     diff = float(np.abs(th_l[sl] - th_p[sl]).max())
     assert 0.0 < diff <= 0.05 * rng_
+
+
+def test_trained_network_beats_weno5_on_held_out_faces(cm1g, monkeypatch):
+    """What training gains, at the face level: on quarter-size grids, fine
+    runs of the plain method give the training faces (4 runs) and held-out
+    faces (1 further run); the network trained by the library's kernels
+    (forward, loss, backward, Adam; validation-selected epoch) reproduces the
+    held-out target face values better than both the 5th-order upwind
+    weights it starts from and WENO5, the plain method."""
+    _torch()
+    from cm1_b200 import learned as Lm
+    monkeypatch.setattr(Lm, "FINE", dict(ni=128, nj=128, nk=40, dx=250.0, dz=125.0, dt=1.5))
+    monkeypatch.setattr(Lm, "COARSE", dict(ni=32, nj=32, nk=20, dx=1000.0, dz=250.0, dt=6.0))
+    quiet = lambda s: None
+    data, _ = Lm.generate(4, 8, 12, seed=11, log=quiet)
+    held, _ = Lm.generate(1, 8, 12, seed=907, log=quiet)
+    P, hist, _ = Lm.train(data, 20, batch=8192, val=held, log=quiet)
+    fe = Lm.face_errors(P, held)
+    print("held-out face errors: upwind5 %.3e, WENO5 %.3e, network %.3e" % (fe["upwind5"], fe["weno5"], fe["learned"]))
+    assert fe["learned"] < 0.95 * fe["upwind5"]
+    assert fe["learned"] < 0.95 * fe["weno5"]
+    assert min(hist["validation"]) < Lm.baseline_loss(held)
