@@ -64,6 +64,22 @@ class Tune(C.Structure):
                 ("step_ms", C.c_float)]
 
 
+STAT_SWITCHES = ["stat_w", "stat_wlevs", "stat_u", "stat_v", "stat_rmw", "stat_pipert", "stat_prspert",
+                 "stat_thpert", "stat_q", "stat_tke", "stat_km", "stat_kh", "stat_div", "stat_rh", "stat_rhi",
+                 "stat_the", "stat_cloud", "stat_sfcprs", "stat_wsp", "stat_cfl", "stat_vort", "stat_tmass",
+                 "stat_tmois", "stat_qmass", "stat_tenerg", "stat_mo", "stat_tmf", "stat_pcn", "stat_qsrc"]
+
+
+class StatOpts(C.Structure):
+    """cm1g_stat_opts_t: switches and host values of the statistics package."""
+    _fields_ = ([(n, C.c_int32) for n in STAT_SWITCHES] +
+                [("adapt_dt", C.c_int32), ("bbc", C.c_int32), ("ptype", C.c_int32), ("iice", C.c_int32),
+                 ("nql1", C.c_int32), ("nql2", C.c_int32), ("cloudvar", C.c_int32 * CM1G_MAXQ),
+                 ("nbudget", C.c_int32), ("maxz", C.c_float), ("cgs1", C.c_float), ("cgs2", C.c_float),
+                 ("cgs3", C.c_float), ("zh", _P), ("zf", _P), ("qname", (C.c_char * 4) * CM1G_MAXQ),
+                 ("budname", C.c_char_p)])
+
+
 class State(C.Structure):
     """cm1g_state_t: prognostic state and pre-RK tendencies."""
     _fields_ = [(n, _P) for n in STATE_FIELDS]

@@ -10,7 +10,7 @@ import os
 
 import numpy as np
 
-from .abi import Config, Grid, State, Tune, STATE_FIELDS, fptr, CM1G_OK
+from .abi import Config, Grid, State, StatOpts, Tune, STATE_FIELDS, fptr, CM1G_OK
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libcm1g.so")
@@ -62,6 +62,11 @@ def lib():
     L.cm1g_profile_read.argtypes = [ctxp, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(C.c_int64),
                                     C.POINTER(C.c_double)]
     L.cm1g_calcener.argtypes = [ctxp] + [_P] * 11 + [C.POINTER(C.c_double)]
+    L.cm1g_stat_setup.argtypes = [ctxp, C.POINTER(StatOpts), C.POINTER(C.c_int32)]
+    L.cm1g_stat_name.argtypes = [ctxp, C.c_int32, C.c_char_p, C.c_int32]
+    L.cm1g_statpack.argtypes = ([ctxp, C.c_double, C.c_float] + [_P] * 10 +
+                                [C.POINTER(C.c_double)] * 3 + [_P])
+    L.cm1g_stat_write.argtypes = [C.c_char_p, C.c_int32, _P, C.c_int32]
     L.cm1g_dtsmall.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, C.c_int32,
                                C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int32)]
     L.cm1g_tendency_init.argtypes = [ctxp, C.c_int32, C.c_float] + [_P] * 16
@@ -107,6 +112,12 @@ def ptr(a):
     if isinstance(a, np.ndarray):
         return a.ctypes.data_as(_P)
     return fptr(a.data_ptr())
+
+
+def stat_write(path, nrec, rstat):
+    """cm1g_stat_write: rstat as record nrec (1-based) of a GrADS stats file."""
+    a = np.ascontiguousarray(rstat, np.float32)
+    check(lib().cm1g_stat_write(str(path).encode(), int(nrec), a.ctypes.data_as(_P), a.size))
 
 
 class Context:
@@ -210,6 +221,35 @@ class Context:
         check(lib().cm1g_calcener(self.h, ptr(zh), ptr(rho), ptr(ua), ptr(va), ptr(wa), ptr(ppi), ptr(tha),
                                   ptr(qv), ptr(ql), ptr(qi), ptr(vr), out))
         return tuple(out)
+
+    def stat_setup(self, opts):
+        """cm1g_stat_setup: builds the statistics list; returns the statistic names."""
+        n = C.c_int32()
+        check(lib().cm1g_stat_setup(self.h, C.byref(opts), C.byref(n)))
+        buf = C.create_string_buffer(64)
+        names = []
+        for i in range(1, n.value + 1):
+            check(lib().cm1g_stat_name(self.h, i, buf, 64))
+            names.append(buf.value.decode())
+        self._nstat = n.value
+        return names
+
+    def statpack(self, mtime, dt, ua, va, wa, ppi, tha, prs, rho, qa=None, pta=None, prate=None,
+                 qbudget=None, asq=None, bsq=None):
+        """cm1g_statpack: the statistics of the fields (host or device arrays) as a float32 array."""
+        out = np.zeros(self._nstat, np.float32)
+
+        def dp(a):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, np.float64)
+            return a.ctypes.data_as(C.POINTER(C.c_double)), a
+        qb, ab, bb = dp(qbudget), dp(asq), dp(bsq)
+        check(lib().cm1g_statpack(self.h, float(mtime), float(dt), ptr(ua), ptr(va), ptr(wa), ptr(ppi), ptr(tha),
+                                  ptr(prs), ptr(rho), ptr(qa), ptr(pta), ptr(prate),
+                                  qb[0] if qb else None, ab[0] if ab else None, bb[0] if bb else None,
+                                  out.ctypes.data_as(_P)))
+        return out
 
     def tendency_init(self, irdamp, rdalpha, uten1, vten1, wten1, thten1, qten=None, ptten=None, tauh=None,
                       taus=None, tauf=None, uavg=None, vavg=None, thavg=None, ua=None, va=None, wa=None, tha=None):

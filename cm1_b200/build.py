@@ -5,7 +5,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = ["cm1g_api.cu", "k_adv.cu", "k_sound.cu", "k_bc.cu", "k_misc.cu", "k_pdefq_noalloc.cu", "k_learned.cu"]
+SRC = ["cm1g_api.cu", "k_adv.cu", "k_sound.cu", "k_bc.cu", "k_misc.cu", "k_pdefq_noalloc.cu", "k_learned.cu", "k_stat.cu"]
 LIB = os.path.join(HERE, "libcm1g.so")
 
 # --fmad=false: keep every binary32 product and sum rounded separately, as
@@ -23,8 +23,8 @@ def build(verbose=False, extra=()):
     """Compiles each source to an object in parallel (in _build/ beside the
     sources), then links libcm1g.so."""
     srcs = [os.path.join(HERE, "csrc", s) for s in SRC]
-    newest = max(os.path.getmtime(s) for s in srcs + [os.path.join(HERE, "csrc", "cm1g_common.cuh"),
-                                                       os.path.join(HERE, "..", "include", "cm1g.h")])
+    heads = [os.path.join(HERE, "csrc", h) for h in os.listdir(os.path.join(HERE, "csrc")) if h.endswith(".cuh")]
+    newest = max(os.path.getmtime(s) for s in srcs + heads + [os.path.join(HERE, "..", "include", "cm1g.h")])
     if os.path.exists(LIB) and os.path.getmtime(LIB) >= newest and not extra:
         return LIB
     host = "/usr/bin/g++"

@@ -23,7 +23,7 @@ import math
 
 import numpy as np
 
-from .abi import Config, Grid, State, GRID_FIELDS, STATE_FIELDS, fptr, CM1G_MAXQ
+from .abi import Config, Grid, State, StatOpts, STAT_SWITCHES, GRID_FIELDS, STATE_FIELDS, fptr, CM1G_MAXQ
 
 G = 9.81
 RD = 287.04
@@ -417,6 +417,39 @@ def make_case(name, seed=1234, **over):
     mass1 = float(rr.sum(dtype=np.float64))
     return Case(name=name, lay=lay, cfg=cfg, grid=gr, state=st, dt=float(w["dt"]),
                 mass1=mass1, nsteps=int(w["nsteps"]))
+
+
+# statistics this library does not build (turbulence, ice, axisymmetric runs)
+_STAT_OFF = ("stat_rmw", "stat_tke", "stat_km", "stat_kh", "stat_rhi")
+
+
+def stat_opts(case, off=(), qnames=("qv",), nql=(0, 0), cloud=(), budnames=()):
+    """cm1g_stat_opts_t for a case: every statistic this library builds is on
+    except those in `off`; level heights of the uniform grid, the surface
+    extrapolation weights from zh(1..3) to z = 0 (Lagrange, as param.F's
+    delta gives them), model top nk*dz.  Returns (opts, arrays to keep alive)."""
+    cfg = case.cfg
+    nk, dz = cfg.nk, cfg.dz
+    o = StatOpts()
+    for n in STAT_SWITCHES:
+        setattr(o, n, 0 if (n in _STAT_OFF or n in off) else 1)
+    o.adapt_dt, o.bbc, o.ptype, o.iice = 0, 1, 0, 0
+    o.nql1, o.nql2 = nql
+    for q in cloud:
+        o.cloudvar[q] = 1
+    zh = ((np.arange(nk + 2) - 0.5) * dz).astype(np.float32)
+    zf = ((np.arange(nk + 3) - 1.0) * dz).astype(np.float32)
+    z = zh[1:4].astype(np.float64)
+    w = [np.prod([(0.0 - z[m]) / (z[l] - z[m]) for m in range(3) if m != l]) for l in range(3)]
+    o.cgs1, o.cgs2, o.cgs3 = (float(np.float32(x)) for x in w)
+    o.maxz = float(np.float32(nk * dz))
+    o.zh, o.zf = fptr(zh.ctypes.data), fptr(zf.ctypes.data)
+    for q, nm in enumerate(qnames[:CM1G_MAXQ]):
+        o.qname[q].value = nm.encode()
+    bud = b"".join(b.encode().ljust(6)[:6] for b in budnames)
+    o.nbudget = len(budnames)
+    o.budname = bud if budnames else None
+    return o, [zh, zf, bud]
 
 
 ENSEMBLE_SIZES = tuple(range(48, 193, 16))   # nx, ny in {48 .. 192}

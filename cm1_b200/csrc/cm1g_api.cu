@@ -11,10 +11,12 @@
 #include <cstdarg>
 #include <cmath>
 #include <vector>
+#include <algorithm>
 #include <string>
 #include <map>
 #include <mutex>
 #include "cm1g_common.cuh"
+#include "k_stat.cuh"
 #include "../../include/cm1g.h"
 
 namespace cm1g {
@@ -174,6 +176,17 @@ struct cm1g_ctx {
   uint64_t gen = 0;                           // bumped when launch shapes or the closure change
   float tuned_ms = 0.0f;                      // measured step time of the launch shapes (autotune)
   Profile *prof = nullptr;
+  // statistics package (cm1g_stat_setup / cm1g_statpack)
+  bool st_ready = false;
+  cm1g_stat_opts_t st_opts{};
+  std::vector<StatJob> st_jobs;
+  std::vector<StatOp> st_ops;
+  std::vector<std::string> st_names;
+  StatJob *d_st_jobs = nullptr;
+  StatOp *d_st_ops = nullptr;
+  StatLev *d_st_lev = nullptr;
+  float *d_rstat = nullptr, *d_st_zh = nullptr, *d_st_zf = nullptr;
+  int st_cap_jobs = 0, st_cap_ops = 0, st_nch = 1;
 };
 
 // Makes the context's profile (if any) the active one for the calling thread.
@@ -382,6 +395,9 @@ extern "C" int cm1g_finalize(cm1g_ctx_t *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->prof) { c->prof->drain(); delete c->prof; }
   for (void *p : c->allocs) if (p) cudaFree(p);
+  for (void *p : {(void *)c->d_st_jobs, (void *)c->d_st_ops, (void *)c->d_st_lev, (void *)c->d_rstat,
+                  (void *)c->d_st_zh, (void *)c->d_st_zf})
+    if (p) cudaFree(p);
   for (auto &b : c->stage_pool) cudaFree(b.first);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -1351,7 +1367,7 @@ extern "C" int cm1g_calcener(cm1g_ctx_t *c, const float *zh, const float *rho, c
   // constants.F:85-150: latent heats at the reference temperature to = 273.15
   const int tc = c->cfg.testcase;
   const float xlv = tc == 4 ? 2.47e6f : tc == 5 ? 2.50e6f : 2501000.0f, xls = 2834000.0f, to = 273.15f;
-  e.lv1 = xlv + (g.c.cpl - g.c.cpv) * to;
+  e.lv1 = (tc == 4 || tc == 5) ? xlv : xlv + (g.c.cpl - g.c.cpv) * to;   // constants.F:156-159
   e.ls1 = xls + (g.c.cpi - g.c.cpv) * to;
   double *part = c->ener + 8;
   launch_calcener(g, e, part, c->ener, c->stream, &c->nlaunch);
@@ -1387,6 +1403,340 @@ extern "C" int cm1g_maxmin(cm1g_ctx_t *c, const float *a, int32_t stag, float *a
   loc[0] = 1 + (int)(imax % ie); loc[1] = 1 + (int)((imax / ie) % je); loc[2] = 1 + (int)(imax / ((unsigned)ie * je));
   loc[3] = 1 + (int)(imin % ie); loc[4] = 1 + (int)((imin / ie) % je); loc[5] = 1 + (int)(imin / ((unsigned)ie * je));
   return CM1G_OK;
+}
+
+// ---------------------------------------------------------------------
+// Statistics package (statpack.F:10-658).  cm1g_stat_setup turns the
+// switches into a job list (one per reduced quantity) and an output program
+// (one operation per rstat entry) in the order of setup_stat_vars
+// (statpack.F:666-1458) and statpack (statpack.F:122-600); cm1g_statpack
+// launches k_stat_levels and k_stat_finish and copies rstat back once.
+// ---------------------------------------------------------------------
+namespace {
+enum HostSlot { HS_MTIME = 0, HS_QBUDGET, HS_ASQ, HS_BSQ };
+
+std::string trim_name(const char *p, int n) {
+  std::string t(p, strnlen(p, n));
+  while (!t.empty() && t.back() == ' ') t.pop_back();
+  while (!t.empty() && t.front() == ' ') t.erase(t.begin());
+  return t;
+}
+}  // namespace
+
+extern "C" int cm1g_stat_setup(cm1g_ctx_t *c, const cm1g_stat_opts_t *o, int32_t *stat_out) {
+  if (!c || !o || !stat_out) return set_err(CM1G_ERR_ARG, "null argument");
+  const DGrid &g = c->g;
+  const cm1g_config_t &cf = c->cfg;
+  const bool moist = cf.imoist == 1;
+  if (o->adapt_dt) return set_err(CM1G_ERR_UNSUPPORTED, "statpack: adapt_dt is not built");
+  if (o->stat_rmw) return set_err(CM1G_ERR_UNSUPPORTED, "statpack: stat_rmw (axisymmetric runs) is not built");
+  if (o->stat_km || o->stat_kh)
+    return set_err(CM1G_ERR_UNSUPPORTED, "statpack: stat_km/stat_kh need the subgrid turbulence, not built");
+  if (moist && (o->stat_rhi || o->iice))
+    return set_err(CM1G_ERR_UNSUPPORTED, "statpack: ice species (iice, stat_rhi) are not built");
+  if (o->bbc == 3) return set_err(CM1G_ERR_UNSUPPORTED, "statpack: bbc=3 (surface layer) is not built");
+  if (!o->zh || !o->zf) return set_err(CM1G_ERR_ARG, "statpack: zh and zf are required");
+  const int numq = moist ? cf.numq : 0, npt = cf.iptra ? cf.npt : 0, nk = g.nk, ni = g.ni, nj = g.nj;
+  if (moist && (o->nql1 < 0 || o->nql2 > numq || (o->nql1 > 0 && o->nql2 < o->nql1)))
+    return set_err(CM1G_ERR_ARG, "statpack: nql1..nql2 outside 1..numq");
+  if (moist && o->stat_pcn && (o->nbudget < 0 || (o->nbudget > 0 && !o->budname)))
+    return set_err(CM1G_ERR_ARG, "statpack: stat_pcn needs nbudget names");
+  const float *zh = o->zh - 0, *zf = o->zf;   // index k = 0 .. nk+1 (nk+2 for zf)
+
+  std::vector<StatJob> jobs;
+  std::vector<StatOp> ops;
+  std::vector<std::string> names;
+  auto job = [&](int kind, int src, int stag, int klo, int nlev, int ie, int je) {
+    StatJob j{};
+    j.kind = kind; j.src = src; j.stag = stag; j.qn = 0; j.klo = klo; j.nlev = nlev;
+    j.i0 = 1; j.ie = ie; j.j0 = 1; j.je = je; j.k0 = 0; j.r1 = j.r2 = 0.0f;
+    jobs.push_back(j);
+    return (int)jobs.size() - 1;
+  };
+  auto op = [&](int kind, int jx, int k, int arg, const std::string &name) {
+    ops.push_back(StatOp{kind, jx, k, arg});
+    names.push_back(name);
+  };
+  auto mm = [&](int jx, const std::string &a, const std::string &b) {   // maxmin
+    op(SO_MAX, jx, 0, 0, a); op(SO_MIN, jx, 0, 0, b);
+  };
+  auto mm1 = [&](int jx, const std::string &a, const std::string &b) {  // maxmin2d of level 1
+    op(SO_LEVMAX, jx, 1, 0, a); op(SO_LEVMIN, jx, 1, 0, b);
+  };
+  auto qn = [&](int n) { return trim_name(o->qname[n], 4); };
+
+  op(SO_HOST, -1, 0, HS_MTIME, "mtime");
+  if (o->stat_w) {
+    int w = job(SK_FIELD, SF_W, 4, 1, nk + 1, ni, nj);
+    mm(w, "wmax", "wmin");
+    op(SO_ZF_KMAX, w, 0, 0, "zwmax"); op(SO_ZF_KMIN, w, 0, 0, "zwmin");
+  }
+  if (o->stat_wlevs && o->maxz >= 10000.0f) {   // statpack.F:146-212
+    const float zl[5] = {500.0f, 1000.0f, 2500.0f, 5000.0f, 10000.0f};
+    const char *nm[5] = {"500", "1000", "2500", "5000", "10k"};
+    for (int n = 0; n < 5; n++) {
+      if (zl[n] < zf[nk + 1]) {
+        int nkm = nk + 1;
+        while (zf[nkm] > zl[n] && nkm > 1) nkm--;
+        const float r2 = (zl[n] - zf[nkm]) / (zf[nkm + 1] - zf[nkm]);
+        int jx = job(SK_WLEV, 0, 1, 1, 1, ni, nj);
+        jobs[jx].k0 = nkm; jobs[jx].r1 = 1.0f - r2; jobs[jx].r2 = r2;
+        mm1(jx, std::string("wmax") + nm[n], std::string("wmin") + nm[n]);
+      } else {
+        op(SO_ZERO, -1, 0, 0, std::string("wmax") + nm[n]);
+        op(SO_ZERO, -1, 0, 0, std::string("wmin") + nm[n]);
+      }
+    }
+  }
+  if (o->stat_u) {
+    int u = job(SK_FIELD, SF_U, 2, 1, nk, ni + 1, nj);
+    mm(u, "umax", "umin"); mm1(u, "sumax", "sumin");
+  }
+  if (o->stat_v) {
+    int v = job(SK_FIELD, SF_V, 3, 1, nk, ni, nj + 1);
+    mm(v, "vmax", "vmin"); mm1(v, "svmax", "svmin");
+  }
+  if (o->stat_pipert) mm(job(SK_FIELD, SF_PPI, 1, 1, nk, ni, nj), "ppimax", "ppimin");
+  if (o->stat_prspert) mm(job(SK_PP, 0, 1, 1, nk, ni, nj), "ppmax", "ppmin");
+  if (o->stat_thpert) {
+    int t = job(SK_FIELD, SF_THA, 1, 1, nk, ni, nj);
+    mm(t, "thpmax", "thpmin"); mm1(t, "sthpmax", "sthpmin");
+  }
+  if (moist && o->stat_q) {
+    for (int n = 0; n < numq; n++) {
+      int q = job(SK_FIELD, SF_Q, 1, 1, nk, ni, nj);
+      jobs[q].qn = n;
+      mm(q, "max" + qn(n), "min" + qn(n));
+    }
+    mm1(job(SK_PRATE, 0, 1, 1, 1, ni, nj), "pratemax", "pratemin");
+  }
+  if (o->stat_div) mm(job(SK_DIV, 0, 1, 1, nk, ni, nj), "divmax", "divmin");
+  if (moist && o->stat_rh) mm(job(SK_RH, 0, 1, 1, nk, ni, nj), "rhmax", "rhmin");
+  for (int n = 0; n < npt; n++) {
+    int p = job(SK_FIELD, SF_PT, 1, 1, nk, ni, nj);
+    jobs[p].qn = n;
+    mm(p, "maxpt" + std::to_string(n + 1), "minpt" + std::to_string(n + 1));
+  }
+  if (moist && o->stat_the) {
+    // calcthe copies the level below above 10 km: those levels repeat values
+    int nl = 0;
+    while (nl < nk && zh[nl + 1] <= 10000.0f) nl++;
+    if (nl < 1) nl = 1;
+    int t = job(SK_THE, 0, 1, 1, nl, ni, nj);
+    mm(t, "themax", "themin"); mm1(t, "sthemax", "sthemin");
+  }
+  if (moist && o->stat_cloud) {
+    int cl = job(SK_CLOUD, 0, 1, 1, nk, ni, nj);
+    op(SO_QCTOP, cl, 0, 0, "qctop"); op(SO_QCBOT, cl, 0, 0, "qcbot");
+  }
+  if (o->stat_sfcprs) {
+    mm1(job(SK_FIELD, SF_PRS, 1, 1, 1, ni, nj), "sprsmax", "sprsmin");
+    mm1(job(SK_PSFC, 0, 1, 1, 1, ni, nj), "psfcmax", "psfcmin");
+  }
+  if (o->stat_wsp) {
+    int w = job(SK_WSP, 0, 1, 1, nk, ni, nj);
+    mm(w, "wspmax", "wspmin");
+    op(SO_ZH_KMAX, w, 0, 0, "zwspmax"); op(SO_ZH_KMIN, w, 0, 0, "zwspmin");
+    mm1(w, "swspmax", "swspmin");
+  }
+  if (o->stat_cfl) op(SO_CFL, job(SK_CFL, 0, 1, 1, nk, ni, nj), 0, 0, "cflmax");
+  if (o->stat_vort) {   // vertvort: levels of 1-5 km from zh (misclibs.F:2455-2466)
+    int kv[6] = {1, nk + 1, nk + 1, nk + 1, nk + 1, nk + 1};
+    for (int k = nk; k >= 1; k--)
+      for (int n = 1; n <= 5; n++)
+        if (zh[k] >= 1000.0f * n) kv[n] = k;
+    const char *nm[6] = {"vortsfc", "vort1km", "vort2km", "vort3km", "vort4km", "vort5km"};
+    for (int n = 0; n < 6; n++) {
+      if (kv[n] <= nk) {
+        int v = job(SK_VORT, 0, 1, 1, 1, ni + 1 - g.ibe, nj + 1 - g.ibn);
+        jobs[v].i0 = 1 + g.ibw; jobs[v].j0 = 1 + g.ibs; jobs[v].k0 = kv[n];
+        op(SO_VORT, v, kv[n], 0, nm[n]);
+      } else {
+        op(SO_ZERO, -1, 0, 0, nm[n]);
+      }
+    }
+  }
+  if (o->stat_tmass) op(SO_SUM, job(SK_MASS, 0, 1, 1, nk, ni, nj), 0, 1, "tmass");
+  if (moist && o->stat_tmois) op(SO_SUM, job(SK_TMOIS, 0, 1, 1, nk, ni, nj), 0, 1, "tmois");
+  if (moist && o->stat_qmass)
+    for (int n = 0; n < numq; n++) {
+      const bool liq = o->nql1 > 0 && n + 1 >= o->nql1 && n + 1 <= o->nql2;
+      if (n + 1 == cf.nqv || liq) {
+        int q = job(SK_QMAS, 0, 1, 1, nk, ni, nj);
+        jobs[q].qn = n;
+        op(SO_SUM, q, 0, 1, "mass" + qn(n));
+      }
+    }
+  if (o->stat_tenerg) {
+    int e = job(SK_ENER, 0, 1, 1, nk, ni, nj);
+    op(SO_SUM, e, 0, 1, "ek"); op(SO_SUM, e, 1, 1, "ei"); op(SO_SUM, e, 2, 1, "ep"); op(SO_SUM, e, 3, 1, "le");
+    op(SO_ENER_TOTAL, e, 0, 0, "et");
+  }
+  if (o->stat_mo) {
+    int m = job(SK_MOE, 0, 1, 1, nk, ni, nj);
+    op(SO_SUM, m, 0, 1, "tmu"); op(SO_SUM, m, 1, 1, "tmv"); op(SO_SUM, m, 2, 1, "tmw");
+  }
+  if (o->stat_tmf) {
+    int m = job(SK_TMF, 0, 1, 1, nk, ni, nj);
+    op(SO_SUM, m, 0, 2, "tmfu"); op(SO_SUM, m, 1, 2, "tmfd");
+  }
+  if (moist && o->stat_pcn)
+    for (int n = 0; n < o->nbudget; n++) {
+      ops.push_back(StatOp{SO_HOST, -1, n, HS_QBUDGET});
+      names.push_back(trim_name(o->budname + 6 * n, 6));
+    }
+  if (moist && o->stat_qsrc) {
+    for (int n = 0; n < numq; n++) { ops.push_back(StatOp{SO_HOST, -1, n, HS_ASQ}); names.push_back("as" + qn(n)); }
+    for (int n = 0; n < numq; n++) { ops.push_back(StatOp{SO_HOST, -1, n, HS_BSQ}); names.push_back("bs" + qn(n)); }
+  }
+  if (jobs.empty()) job(SK_MASS, 0, 1, 1, 0, ni, nj);   // keeps the job table non-empty (no levels)
+
+  // device tables (grown, never shrunk); chunk records [job][level][chunk]
+  const int maxlev = nk + 1;
+  int npl = 1;
+  for (const StatJob &j : jobs) npl = std::max(npl, (j.ie - j.i0 + 1) * (j.je - j.j0 + 1));
+  const int nch = stat_chunks(npl);
+  if ((int)jobs.size() > c->st_cap_jobs) {
+    if (c->d_st_jobs) { cudaFree(c->d_st_jobs); cudaFree(c->d_st_lev); c->d_st_jobs = nullptr; c->d_st_lev = nullptr; }
+    c->st_cap_jobs = (int)jobs.size() + 16;
+    CUCHK(cudaMalloc(&c->d_st_jobs, c->st_cap_jobs * sizeof(StatJob)));
+    CUCHK(cudaMalloc(&c->d_st_lev, (size_t)c->st_cap_jobs * maxlev * stat_chunks((g.ni + 1) * (g.nj + 1)) *
+                                       sizeof(StatLev)));
+  }
+  if ((int)ops.size() > c->st_cap_ops) {
+    if (c->d_st_ops) { cudaFree(c->d_st_ops); cudaFree(c->d_rstat); c->d_st_ops = nullptr; c->d_rstat = nullptr; }
+    c->st_cap_ops = (int)ops.size() + 32;
+    CUCHK(cudaMalloc(&c->d_st_ops, c->st_cap_ops * sizeof(StatOp)));
+    CUCHK(cudaMalloc(&c->d_rstat, c->st_cap_ops * sizeof(float)));
+  }
+  if (!c->d_st_zh) {
+    CUCHK(cudaMalloc(&c->d_st_zh, (size_t)(nk + 2) * sizeof(float)));
+    CUCHK(cudaMalloc(&c->d_st_zf, (size_t)(nk + 3) * sizeof(float)));
+  }
+  CUCHK(cudaMemcpyAsync(c->d_st_jobs, jobs.data(), jobs.size() * sizeof(StatJob), cudaMemcpyHostToDevice, c->stream));
+  CUCHK(cudaMemcpyAsync(c->d_st_ops, ops.data(), ops.size() * sizeof(StatOp), cudaMemcpyHostToDevice, c->stream));
+  CUCHK(cudaMemcpyAsync(c->d_st_zh, zh, (size_t)(nk + 2) * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  CUCHK(cudaMemcpyAsync(c->d_st_zf, zf, (size_t)(nk + 3) * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  CUCHK(cudaStreamSynchronize(c->stream));
+  c->st_opts = *o;
+  c->st_opts.zh = c->st_opts.zf = nullptr;
+  c->st_opts.budname = nullptr;
+  c->st_jobs = jobs; c->st_ops = ops; c->st_names = names;
+  c->st_nch = nch;
+  c->st_ready = true;
+  *stat_out = (int32_t)ops.size();
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_stat_name(cm1g_ctx_t *c, int32_t n, char *name, int32_t len) {
+  if (!c || !name || len < 1) return set_err(CM1G_ERR_ARG, "null argument");
+  if (!c->st_ready) return set_err(CM1G_ERR_STATE, "cm1g_stat_setup has not been called");
+  if (n < 1 || n > (int)c->st_names.size()) return set_err(CM1G_ERR_ARG, "statistic %d out of range", n);
+  snprintf(name, (size_t)len, "%s", c->st_names[n - 1].c_str());
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_statpack(cm1g_ctx_t *c, double mtime, float dt, const float *ua, const float *va,
+                             const float *wa, const float *ppi, const float *tha, const float *prs, const float *rho,
+                             const float *qa, const float *pta, const float *prate, const double *qbudget,
+                             const double *asq, const double *bsq, float *rstat) {
+  if (!c || !rstat) return set_err(CM1G_ERR_ARG, "null argument");
+  if (!c->st_ready) return set_err(CM1G_ERR_STATE, "cm1g_stat_setup has not been called");
+  const DGrid &g = c->g;
+  const cm1g_config_t &cf = c->cfg;
+  const bool moist = cf.imoist == 1;
+  const int numq = moist ? cf.numq : 0, npt = cf.iptra ? cf.npt : 0;
+  // the fields the job list reads
+  bool need_u = false, need_v = false, need_w = false, need_ppi = false, need_tha = false, need_prs = false;
+  bool need_rho = false, need_q = false, need_pt = false;
+  for (const StatJob &j : c->st_jobs) {
+    if (j.nlev == 0) continue;
+    switch (j.kind) {
+      case SK_FIELD:
+        need_u |= j.src == SF_U; need_v |= j.src == SF_V; need_w |= j.src == SF_W; need_ppi |= j.src == SF_PPI;
+        need_tha |= j.src == SF_THA; need_prs |= j.src == SF_PRS; need_q |= j.src == SF_Q; need_pt |= j.src == SF_PT;
+        break;
+      case SK_PP: case SK_PSFC: need_prs = true; break;
+      case SK_DIV: case SK_CFL: need_u = need_v = need_w = true; break;
+      case SK_RH: case SK_THE: need_prs = need_tha = need_ppi = need_q = true; break;
+      case SK_WSP: case SK_VORT: need_u = need_v = true; break;
+      case SK_WLEV: need_w = true; break;
+      case SK_CLOUD: need_q = true; break;
+      case SK_MASS: need_rho = true; break;
+      case SK_TMOIS: case SK_QMAS: need_rho = need_q = true; break;
+      case SK_TMF: need_rho = need_w = true; break;
+      case SK_MOE: need_rho = need_u = need_v = need_w = true; need_q |= moist; break;
+      case SK_ENER: need_rho = need_u = need_v = need_w = need_ppi = need_tha = true; need_q |= moist; break;
+      default: break;
+    }
+  }
+  if ((need_u && !ua) || (need_v && !va) || (need_w && !wa) || (need_ppi && !ppi) || (need_tha && !tha) ||
+      (need_prs && !prs) || (need_rho && !rho) || (need_q && numq && !qa) || (need_pt && npt && !pta))
+    return set_err(CM1G_ERR_ARG, "statpack: a field the statistics need is NULL");
+  for (const StatOp &p : c->st_ops) {
+    if (p.op != SO_HOST) continue;
+    if ((p.arg == HS_QBUDGET && !qbudget) || (p.arg == HS_ASQ && !asq) || (p.arg == HS_BSQ && !bsq))
+      return set_err(CM1G_ERR_ARG, "statpack: qbudget/asq/bsq are needed by stat_pcn/stat_qsrc");
+  }
+  ProfActive pa(c);
+  Stager S(c);
+  const size_t ns = nS(g);
+  StatFields f{};
+  f.ua = need_u ? S.in(ua, nU(g), false) : nullptr;
+  f.va = need_v ? S.in(va, nV(g), false) : nullptr;
+  f.wa = need_w ? S.in(wa, nW(g), false) : nullptr;
+  f.ppi = need_ppi ? S.in(ppi, ns, false) : nullptr;
+  f.tha = need_tha ? S.in(tha, ns, false) : nullptr;
+  f.prs = need_prs ? S.in(prs, ns, false) : nullptr;
+  f.rho = need_rho ? S.in(rho, ns, false) : nullptr;
+  f.qa = (need_q && numq) ? S.in(qa, (size_t)numq * ns, false) : nullptr;
+  f.pta = (need_pt && npt) ? S.in(pta, (size_t)npt * ns, false) : nullptr;
+  f.prate = prate ? S.in(prate, (size_t)g.NI * g.NJ, false) : nullptr;
+  f.qstride = (long)ns;
+  const cm1g_stat_opts_t &o = c->st_opts;
+  StatConsts k{};
+  const Consts &cc = g.c;
+  k.p00 = 1.0e5f; k.eps = cc.rd / cc.rv; k.reps = cc.reps; k.rd = cc.rd; k.rv = cc.rv; k.cp = cc.cp;
+  k.cv = cc.cv; k.cvv = cc.cvv; k.cpl = cc.cpl; k.cpi = cc.cpi; k.cpdrd = cc.cpdrd; k.g = cc.g;
+  // constants.F:85-160: latent heats at to = 273.15 (testcases 4 and 5 use lv1 = xlv)
+  const int tc = cf.testcase;
+  const float xlv = tc == 4 ? 2.47e6f : tc == 5 ? 2.50e6f : 2501000.0f, xls = 2834000.0f, to = 273.15f;
+  k.lv1 = (tc == 4 || tc == 5) ? xlv : xlv + (cc.cpl - cc.cpv) * to;
+  k.ls1 = xls + (cc.cpi - cc.cpv) * to;
+  k.dtdx = 0.5f * dt * g.rdx; k.dtdy = 0.5f * dt * g.rdy; k.dtdz = 0.5f * dt * g.rdz;
+  k.cgs1 = o.cgs1; k.cgs2 = o.cgs2; k.cgs3 = o.cgs3; k.maxz = o.maxz;
+  k.ptype = o.ptype; k.imoist = moist; k.numq = numq; k.nqv = moist ? cf.nqv - 1 : 0;
+  k.nql1 = o.nql1 > 0 ? o.nql1 - 1 : -1; k.nql2 = o.nql1 > 0 ? o.nql2 - 1 : -1;
+  k.nx = g.ni; k.ny = g.nj;
+  k.cloudmask = 0;
+  for (int n = 0; n < numq && n < CM1G_MAXQ; n++) if (o.cloudvar[n]) k.cloudmask |= 1u << n;
+  k.zh = c->d_st_zh; k.zf = c->d_st_zf;
+  const int nops = (int)c->st_ops.size();
+  launch_stat(g, f, k, c->d_st_jobs, (int)c->st_jobs.size(), c->d_st_lev, g.nk + 1, c->st_nch, c->d_st_ops, nops,
+              c->d_rstat, c->stream, &c->nlaunch);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
+  CUCHK(cudaMemcpyAsync(rstat, c->d_rstat, (size_t)nops * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  int rc = S.finish();
+  if (rc) return rc;
+  for (int p = 0; p < nops; p++) {
+    const StatOp &q = c->st_ops[p];
+    if (q.op != SO_HOST) continue;
+    rstat[p] = q.arg == HS_MTIME ? (float)mtime : q.arg == HS_QBUDGET ? (float)qbudget[q.k]
+             : q.arg == HS_ASQ ? (float)asq[q.k] : (float)bsq[q.k];
+  }
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_stat_write(const char *path, int32_t nrec, const float *rstat, int32_t nstat) {
+  if (!path || !rstat || nrec < 1 || nstat < 1) return set_err(CM1G_ERR_ARG, "bad argument");
+  FILE *fp = fopen(path, "r+b");
+  if (!fp) fp = fopen(path, "w+b");
+  if (!fp) return set_err(CM1G_ERR_ARG, "cannot open %s", path);
+  const long off = (long)(nrec - 1) * 4L * nstat;
+  int ok = fseek(fp, off, SEEK_SET) == 0 && fwrite(rstat, sizeof(float), (size_t)nstat, fp) == (size_t)nstat;
+  ok = (fclose(fp) == 0) && ok;
+  return ok ? CM1G_OK : set_err(CM1G_ERR_ARG, "write to %s failed", path);
 }
 
 extern "C" int cm1g_profile(cm1g_ctx_t *c, int32_t enable) {

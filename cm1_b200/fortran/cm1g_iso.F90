@@ -71,6 +71,23 @@ module cm1g_iso
     real(c_float)      :: step_ms
   end type
 
+  ! switches of namelist param9 and host values of the statistics package
+  ! (cm1g_stat_setup); fill from module input after param
+  type, bind(C) :: cm1g_stat_opts_t
+    integer(c_int32_t) :: stat_w, stat_wlevs, stat_u, stat_v, stat_rmw, stat_pipert, stat_prspert, &
+                          stat_thpert, stat_q, stat_tke, stat_km, stat_kh, stat_div, stat_rh, stat_rhi, &
+                          stat_the, stat_cloud, stat_sfcprs, stat_wsp, stat_cfl, stat_vort, stat_tmass, &
+                          stat_tmois, stat_qmass, stat_tenerg, stat_mo, stat_tmf, stat_pcn, stat_qsrc
+    integer(c_int32_t) :: adapt_dt, bbc, ptype, iice
+    integer(c_int32_t) :: nql1, nql2
+    integer(c_int32_t) :: cloudvar(CM1G_MAXQ)
+    integer(c_int32_t) :: nbudget
+    real(c_float)      :: maxz, cgs1, cgs2, cgs3
+    type(c_ptr)        :: zh, zf
+    character(kind=c_char) :: qname(4, CM1G_MAXQ)
+    type(c_ptr)        :: budname
+  end type
+
   interface
     integer(c_int) function cm1g_init(cfg, grid, ctx) bind(C, name="cm1g_init")
       import :: c_int, c_ptr, cm1g_config_t, cm1g_grid_t
@@ -179,6 +196,28 @@ module cm1g_iso
     end function
     type(c_ptr) function cm1g_last_error() bind(C, name="cm1g_last_error")
       import :: c_ptr
+    end function
+    ! statpack (statpack.F:10-658): set-up once, then one call per statfrq
+    integer(c_int) function cm1g_stat_setup(ctx, opts, stat_out) bind(C, name="cm1g_stat_setup")
+      import :: c_int, c_int32_t, c_ptr, cm1g_stat_opts_t
+      type(c_ptr), value :: ctx
+      type(cm1g_stat_opts_t), intent(in) :: opts
+      integer(c_int32_t), intent(out) :: stat_out
+    end function
+    integer(c_int) function cm1g_statpack(ctx, mtime, dt, ua, va, wa, ppi, tha, prs, rho, qa, pta, prate, &
+                                          qbudget, asq, bsq, rstat) bind(C, name="cm1g_statpack")
+      import :: c_int, c_float, c_double, c_ptr
+      type(c_ptr), value :: ctx
+      real(c_double), value :: mtime
+      real(c_float), value :: dt
+      type(c_ptr), value :: ua, va, wa, ppi, tha, prs, rho, qa, pta, prate, qbudget, asq, bsq
+      real(c_float), intent(out) :: rstat(*)
+    end function
+    integer(c_int) function cm1g_stat_write(path, nrec, rstat, nstat) bind(C, name="cm1g_stat_write")
+      import :: c_int, c_int32_t, c_float, c_char
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int32_t), value :: nrec, nstat
+      real(c_float), intent(in) :: rstat(*)
     end function
     integer(c_int) function cm1g_set_tune(ctx, tune) bind(C, name="cm1g_set_tune")
       import :: c_int, c_ptr, cm1g_tune_t

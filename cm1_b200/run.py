@@ -3,11 +3,15 @@ diagnostics (the in-process counterpart of running cm1.exe through the
 reference's cm1/run.py).
 
     python -m cm1_b200.run --workload supercell --steps 10 [--ni 128 --nj 128 --nk 80] [--graph]
-                           [--time] [--profile]
+                           [--time] [--profile] [--stats N] [--stats-file cm1out_stats.dat]
 
 --time reports the device time per large step (CUDA events around the steps,
 after one untimed step); --profile reports per-kernel device time per step,
-the counterpart of the reference's timestats table.
+the counterpart of the reference's timestats table.  --stats N runs the statistics package
+(cm1g_statpack: every statistic this library builds) after the steps, N+1
+times, and reports the device-resident time per call (CUDA events, the
+first call untimed, rstat copied to the host each call) with the values;
+--stats-file appends them as a record of the GrADS stats file.
 """
 import argparse
 import json
@@ -27,6 +31,8 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--time", action="store_true")
     ap.add_argument("--profile", action="store_true")
+    ap.add_argument("--stats", type=int, default=0)
+    ap.add_argument("--stats-file")
     args = ap.parse_args(argv)
 
     import torch
@@ -72,6 +78,27 @@ def main(argv=None):
            "mass1": case.mass1, "mass2": mass2, "cflmax": cfl, "kernels": ctx.launches(),
            "theta_max": float(dev["th3d"][lay.interior(1)].max().item())}
     out.update(timing)
+    if args.stats > 0:
+        from .cases import stat_opts
+        opts, keep = stat_opts(case)
+        names = ctx.stat_setup(opts)
+        fields = [dev[n] for n in ("ua", "va", "wa", "ppi", "tha", "prs", "rho")]
+        extra = dict(qa=dev.get("qa") if case.cfg.imoist else None, pta=dev.get("pta") if case.cfg.iptra else None)
+        if case.cfg.imoist:   # no moisture budgets are kept: their entries are zero
+            extra.update(asq=np.zeros(case.cfg.numq), bsq=np.zeros(case.cfg.numq))
+        mtime = case.dt * args.steps
+        rstat = ctx.statpack(mtime, case.dt, *fields, **extra)   # untimed
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(args.stats):
+            rstat = ctx.statpack(mtime, case.dt, *fields, **extra)
+        t1.record()
+        torch.cuda.synchronize()
+        out["statpack_ms"] = t0.elapsed_time(t1) / args.stats
+        out["stats"] = {n: float(v) for n, v in zip(names, rstat)}
+        if args.stats_file:
+            binding.stat_write(args.stats_file, 1, rstat)
     print(json.dumps(out))
     ctx.close()
     return 0 if np.isfinite(out["max_w"]) else 1

@@ -238,6 +238,57 @@ int cm1g_tendency_init(cm1g_ctx_t *ctx, int32_t irdamp, float rdalpha, const flo
 int cm1g_maxmin(cm1g_ctx_t *ctx, const float *a, int32_t stag,
                 float *amax, float *amin, int32_t loc[6]);
 
+/* Statistics package: replaces statpack (src/statpack.F:10-658) for the
+ * fields of the dynamical core.  The switches are those of namelist param9
+ * after param's checks (src/param.F:6140-6205); the statistics are the
+ * reference's, in its order (setup_stat_vars, statpack.F:666-1458).  Not
+ * built: adapt_dt's mean time step, stat_rmw (axisymmetric runs), stat_rhi
+ * (ice), stat_km/stat_kh (subgrid turbulence), and bbc=3 (surface layer):
+ * a non-zero switch for any of them returns CM1G_ERR_UNSUPPORTED (stat_tke
+ * adds nothing without turbulence and is accepted).  umove = vmove = 0.
+ *   nql1..nql2   1-based q indices of the liquid species (0 0: none);
+ *   cloudvar[n]  1: q n+1 counts as cloud for qctop/qcbot;
+ *   zh, zf       host arrays (kb:ke) and (kb:ke+1): heights of the s- and
+ *                w-levels (sigma and sigmaf without terrain);
+ *   maxz         model top; cgs1..cgs3 the surface extrapolation weights
+ *                (param.F:9038-9040);
+ *   qname        short names of the q arrays ("qv"), budname nbudget names
+ *                of 6 characters each (stat_pcn), used by cm1g_stat_name. */
+typedef struct cm1g_stat_opts {
+  int32_t stat_w, stat_wlevs, stat_u, stat_v, stat_rmw, stat_pipert, stat_prspert, stat_thpert,
+          stat_q, stat_tke, stat_km, stat_kh, stat_div, stat_rh, stat_rhi, stat_the, stat_cloud,
+          stat_sfcprs, stat_wsp, stat_cfl, stat_vort, stat_tmass, stat_tmois, stat_qmass,
+          stat_tenerg, stat_mo, stat_tmf, stat_pcn, stat_qsrc;
+  int32_t adapt_dt, bbc, ptype, iice;
+  int32_t nql1, nql2;
+  int32_t cloudvar[CM1G_MAXQ];
+  int32_t nbudget;
+  float maxz, cgs1, cgs2, cgs3;
+  const float *zh, *zf;
+  char qname[CM1G_MAXQ][4];
+  const char *budname;
+} cm1g_stat_opts_t;
+
+/* Builds the statistics list of opts on the context (once per run, like
+ * setup_stat_vars); stat_out receives the number of statistics. */
+int cm1g_stat_setup(cm1g_ctx_t *ctx, const cm1g_stat_opts_t *opts, int32_t *stat_out);
+/* Name of statistic n (1-based), as setup_stat_vars names it. */
+int cm1g_stat_name(cm1g_ctx_t *ctx, int32_t n, char *name, int32_t len);
+/* One call of statpack: rstat (host, stat_out floats) receives the
+ * statistics, computed on the device with one device-to-host copy of rstat.
+ * Fields may be host or device arrays; qa holds numq q arrays and pta npt
+ * tracers (NULL when absent); prate (ib:ie,jb:je) may be NULL (zero).
+ * qbudget (nbudget), asq and bsq (numq) are copied into their entries when
+ * stat_pcn / stat_qsrc are on; dt is the time step calccfl uses. */
+int cm1g_statpack(cm1g_ctx_t *ctx, double mtime, float dt, const float *ua, const float *va, const float *wa,
+                  const float *ppi, const float *tha, const float *prs, const float *rho, const float *qa,
+                  const float *pta, const float *prate, const double *qbudget, const double *asq,
+                  const double *bsq, float *rstat);
+/* Writes rstat as record nrec (1-based) of the GrADS stats file
+ * (cm1out_stats.dat: direct access, record length 4*nstat bytes,
+ * statpack.F:620-632). */
+int cm1g_stat_write(const char *path, int32_t nrec, const float *rstat, int32_t nstat);
+
 /* Per-kernel device timing, the counterpart of the reference's timestats
  * (src/input.F:359-387, cm1.F:4597-4689).  While enabled, every kernel launch
  * is bracketed by CUDA events (graph replay is bypassed); entries are read

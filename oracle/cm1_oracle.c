@@ -1986,7 +1986,9 @@ int oracle_calcener(const cm1g_config_t *cfg, const cm1g_grid_t *gr, const float
   const Consts c = g->c;
   const float xlv = cfg->testcase == 4 ? 2.47e6f : cfg->testcase == 5 ? 2.50e6f : 2501000.0f;
   const float xls = 2834000.0f, to = 273.15f;
-  const float lv1 = xlv + (c.cpl - c.cpv) * to, ls1 = xls + (c.cpi - c.cpv) * to;
+  /* constants.F:148-159: testcases 4 and 5 take lv1 = xlv */
+  const float lv1 = (cfg->testcase == 4 || cfg->testcase == 5) ? xlv : xlv + (c.cpl - c.cpv) * to;
+  const float ls1 = xls + (c.cpi - c.cpv) * to;
   F3 z = mkS(g, zh), r = mkS(g, rho), u = mkU(g, ua), v = mkV(g, va), w = mkW(g, wa), p = mkS(g, ppi), t = mkS(g, tha);
   F3 fv = mkS(g, qv), fl = mkS(g, ql), fi = mkS(g, qi), fr = mkS(g, vr);
   double ek = 0.0, ei = 0.0, ep = 0.0, le = 0.0;

@@ -9,7 +9,7 @@ import ctypes as C
 import os
 import subprocess
 
-from cm1_b200.abi import Config, Grid, State
+from cm1_b200.abi import Config, Grid, State, StatOpts
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "liboracle.so")
@@ -55,6 +55,8 @@ def lib():
         L.oracle_tendency_init.argtypes = [cfgp, grp, C.c_int, C.c_float] + [P] * 16
         L.oracle_calcener.argtypes = [cfgp, grp] + [P] * 11 + [C.POINTER(C.c_double)]
         L.oracle_threads.restype = C.c_int
+        L.oracle_statpack.argtypes = ([cfgp, grp, C.POINTER(StatOpts), C.c_double, C.c_float] + [P] * 10 +
+                                      [C.POINTER(C.c_double)] * 3 + [P, C.POINTER(C.c_int)])
         _lib = L
     return _lib
 
@@ -126,3 +128,30 @@ def step_r8(case, state=None, nsteps=1):
 
 def threads():
     return lib().oracle_threads()
+
+
+def statpack(case, opts, st, mtime=0.0, prate=None, qbudget=None, asq=None, bsq=None, nmax=512):
+    """The statistics of state dict `st` (numpy arrays) as the statpack
+    restatement computes them; returns a float32 array."""
+    import numpy as np
+    L = lib()
+    out = np.zeros(nmax, np.float32)
+    n = C.c_int(0)
+
+    def f(name):
+        a = st.get(name)
+        return _fp(a) if a is not None and a.size else None
+
+    def d(a):
+        if a is None:
+            return None, None
+        a = np.ascontiguousarray(a, np.float64)
+        return a.ctypes.data_as(C.POINTER(C.c_double)), a
+    qb, ab, bb = d(qbudget), d(asq), d(bsq)
+    g = case.grid_struct()
+    rc = L.oracle_statpack(C.byref(case.cfg), C.byref(g), C.byref(opts), mtime, case.dt, f("ua"), f("va"), f("wa"),
+                           f("ppi"), f("tha"), f("prs"), f("rho"), f("qa"), f("pta"),
+                           _fp(prate) if prate is not None else None, qb[0], ab[0], bb[0], _fp(out), C.byref(n))
+    if rc != 0:
+        raise RuntimeError("oracle statpack failed")
+    return out[:n.value].copy()
