@@ -38,6 +38,8 @@ class Config(C.Structure):
         ("axisymm", C.c_int32), ("icor", C.c_int32),
         ("qmag", C.c_float * CM1G_MAXQ),
         ("idiff", C.c_int32), ("difforder", C.c_int32), ("mdiff", C.c_int32), ("kdiff6", C.c_float),
+        ("ptype", C.c_int32), ("nql1", C.c_int32), ("nql2", C.c_int32), ("efall", C.c_int32),
+        ("tsmall", C.c_float), ("qsmall", C.c_float),
     ]
 
 
@@ -55,7 +57,7 @@ class Grid(C.Structure):
 STATE_FIELDS = ["ua", "u3d", "uten1", "va", "v3d", "vten1", "wa", "w3d", "wten1",
                 "ppi", "pp3d", "ppx", "ppten", "tha", "th3d", "thten1", "rho", "prs",
                 "qa", "q3d", "qten", "pta", "pt3d", "ptten",
-                "radbcw", "radbce", "radbcs", "radbcn"]
+                "radbcw", "radbce", "radbcs", "radbcn", "rain", "prate"]
 
 
 class Tune(C.Structure):

@@ -48,6 +48,8 @@ def lib():
                               C.POINTER(C.c_float), stp]
     L.cm1g_step.argtypes = L.cm1g_solve2.argtypes + [C.c_int32]
     L.cm1g_solve3.argtypes = [ctxp, stp]
+    L.cm1g_mp_driver.argtypes = [ctxp, C.c_float, stp]
+    L.cm1g_mp_budget.argtypes = [ctxp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int32]
     L.cm1g_pdefq.argtypes = [ctxp, C.c_float, C.POINTER(C.c_double), _P, _P]
     for n in ("cm1g_bcs", "cm1g_bcp", "cm1g_bcu", "cm1g_bcv"):
         getattr(L, n).argtypes = [ctxp, _P]
@@ -174,6 +176,17 @@ class Context:
             check(L.cm1g_step(self.h, nstep, dt, mtime, mass1, C.byref(m2), C.byref(cfl), C.byref(s),
                               1 if use_graph else 0))
         return m2.value, cfl.value
+
+    def mp_driver(self, state, dt):
+        """cm1g_mp_driver: the Kessler branch of mp_driver on `state` (ptype=1)."""
+        s = state if isinstance(state, State) else self.state_struct(state)
+        check(lib().cm1g_mp_driver(self.h, dt, C.byref(s)))
+
+    def mp_budget(self, reset=False):
+        """(qbudget(1..7), asq(1..3)) accumulated by the microphysics (FP64)."""
+        qb, asq = (C.c_double * 7)(), (C.c_double * 3)()
+        check(lib().cm1g_mp_budget(self.h, qb, asq, 1 if reset else 0))
+        return list(qb), list(asq)
 
     def solve3(self, state):
         s = state if isinstance(state, State) else self.state_struct(state)

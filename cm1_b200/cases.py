@@ -213,6 +213,14 @@ WORKLOADS = {
                       sounding="weisman_klemp", wind="curved", bc=2, moist=True, npt=5,
                       advwenos=1, bubble=dict(amp=3.0, xr=10000.0, zr=1400.0, zc=1400.0),
                       noise=dict(amp=0.1, zmax=None)),
+    # the supercell with Kessler warm-rain microphysics (ptype=1: qv, qc, qr)
+    # and seeded cloud and rain in the bubble, so that every process of the
+    # scheme (condensation, autoconversion, accretion, evaporation, fallout)
+    # acts from the first step
+    "kessler": dict(ni=256, nj=256, nk=80, dx=500.0, dz=250.0, dt=3.0, nsound=8, nsteps=60,
+                    sounding="weisman_klemp", wind="curved", bc=2, moist=True, npt=0, ptype=1,
+                    advwenos=1, bubble=dict(amp=3.0, xr=10000.0, zr=1400.0, zc=1400.0),
+                    noise=dict(amp=0.1, zmax=None)),
     "cbl": dict(ni=1024, nj=1024, nk=128, dx=50.0, dz=20.0, dt=0.5, nsound=6, nsteps=200,
                 sounding="cbl", wind=("uniform", dict(u=5.0, v=0.0)), bc=1, moist=False, npt=2,
                 advwenos=1, bubble=None, noise=dict(amp=0.1, zmax=400.0)),
@@ -221,8 +229,8 @@ WORKLOADS = {
 
 def make_case(name, seed=1234, **over):
     """Build a seeded workload.  `over` may override ni, nj, nk, dx, dz, dt,
-    nsound, advwenos, npt, bc, moist (for small parity cases), and add diff6
-    (kdiff6 of the 6th-order diffusion) and mdiff."""
+    nsound, advwenos, npt, bc, moist, ptype (for small parity cases), eqtset,
+    and add diff6 (kdiff6 of the 6th-order diffusion) and mdiff."""
     w = dict(WORKLOADS[name])
     w.update(over)
     ni, nj, nk = int(w["ni"]), int(w["nj"]), int(w["nk"])
@@ -238,8 +246,13 @@ def make_case(name, seed=1234, **over):
     cfg.hadvordrs = cfg.vadvordrs = cfg.hadvordrv = cfg.vadvordrv = 5
     cfg.advwenos, cfg.advwenov, cfg.weno_order = int(w["advwenos"]), 0, 5
     cfg.nsound, cfg.alph, cfg.kdiv = int(w["nsound"]), 0.60, 0.10
-    cfg.imoist, cfg.eqtset = (1 if moist else 0), 2
-    cfg.numq, cfg.nqv = (1, 1) if moist else (0, 1)
+    ptype = int(w.get("ptype", 0)) if moist else 0
+    cfg.imoist, cfg.eqtset = (1 if moist else 0), int(w.get("eqtset", 2))
+    cfg.numq, cfg.nqv = ((3 if ptype == 1 else 1), 1) if moist else (0, 1)
+    # microphysics (cm1.F:311-319, param.F:3169-3175)
+    cfg.ptype, cfg.efall = ptype, 0
+    cfg.nql1, cfg.nql2 = (2, 3) if ptype == 1 else (0, 0)
+    cfg.tsmall, cfg.qsmall = 1.0e-4, 1.0e-14
     cfg.iptra, cfg.npt, cfg.pdtra = (1 if npt > 0 else 0), npt, 1
     cfg.apmasscon = 1
     cfg.irbc, cfg.cstar, cfg.roflux = 4, 30.0, 0
@@ -372,8 +385,18 @@ def make_case(name, seed=1234, **over):
     st["uten1"], st["vten1"], st["wten1"] = lay.zeros(2), lay.zeros(3), lay.zeros(4)
 
     if moist:
-        q = np.empty((1,) + lay.shape(1), f32)
+        q = np.zeros((cfg.numq,) + lay.shape(1), f32)
         q[0] = gr["qv0"]
+        if ptype == 1 and b:
+            # seeded cloud in the bubble, rain in a wider shell around it, and
+            # a 3 % supersaturation of the bubble's core
+            qc = np.where(beta < 1.0, 1.5e-3 * np.cos(0.5 * np.pi * beta) ** 2, 0.0)
+            qr = np.where(beta < 1.6, 2.0e-3 * np.cos(0.5 * np.pi * beta / 1.6) ** 2, 0.0)
+            q[1][kin] = qc
+            q[2][kin] = qr
+            q[0][kin] *= np.where(beta < 0.5, 1.03, 1.0)
+            for n in range(3):
+                _fill_lateral(lay, q[n], bc)
         st["qa"], st["q3d"], st["qten"] = q.copy(), q.copy(), np.zeros_like(q)
     else:
         st["qa"] = st["q3d"] = st["qten"] = np.zeros((0,) + lay.shape(1), f32)
@@ -408,6 +431,9 @@ def make_case(name, seed=1234, **over):
     st["radbce"] = np.zeros((lay.NK, lay.NJ), f32)
     st["radbcs"] = np.zeros((lay.NK, lay.NI), f32)
     st["radbcn"] = np.zeros((lay.NK, lay.NI), f32)
+    if ptype == 1:
+        st["rain"] = np.zeros((lay.NJ, lay.NI), f32)
+        st["prate"] = np.zeros((lay.NJ, lay.NI), f32)
     for k in st:
         st[k] = np.ascontiguousarray(st[k], dtype=f32)
 

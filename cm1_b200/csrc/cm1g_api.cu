@@ -17,6 +17,7 @@
 #include <mutex>
 #include "cm1g_common.cuh"
 #include "k_stat.cuh"
+#include "k_micro.cuh"
 #include "../../include/cm1g.h"
 
 namespace cm1g {
@@ -33,7 +34,7 @@ void launch_calcener(const DGrid &g, const EnerIn &e, double *part, double *out,
 void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w, const float *uten1,
                          const float *vten1, const float *wten1, float *uten, float *vten, float *wten,
                          const float *th3d, const float *qv, float *divx, cudaStream_t st, int64_t *nl,
-                         const Diff6 *diff = nullptr);
+                         const Diff6 *diff = nullptr, const float *b8 = nullptr);
 void launch_advs(const DGrid &g, const float *rru, const float *rrv, const float *rrw, int weighted,
                  const float *divx, const float *s, const float *s0, int sadd, const float *ten1,
                  const float *thterm, float *sten_out, float *snew, int weno, int pdef, int pdefweno,
@@ -49,8 +50,9 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt, const float *ua
                   const float *radbce, const float *radbcs, const float *radbcn, float *su, float *sv, float *su2,
                   float *sv2, float *d1, float *d2, cudaStream_t st, int64_t *nl);
 int sound_max_nk();
-void launch_stage_prep(const DGrid &g, const float *th3d, const float *pp3d, const float *qv, int imoist, int eqtset,
-                       float *t11, float *t22, float *thterm, float *piadv, cudaStream_t st, int64_t *nl);
+void launch_stage_prep(const DGrid &g, const float *th3d, const float *pp3d, const float *qv, const LiquidIn &liq,
+                       int imoist, int eqtset, float *t11, float *t22, float *thterm, float *piadv, cudaStream_t st,
+                       int64_t *nl);
 void launch_radbc4(const DGrid &g, const float *ua, const float *u3d, const float *va, const float *v3d,
                    float *rw, float *re, float *rs, float *rn, float dt, cudaStream_t st, int64_t *nl);
 int prs_nchunk(const DGrid &g);
@@ -187,6 +189,11 @@ struct cm1g_ctx {
   StatLev *d_st_lev = nullptr;
   float *d_rstat = nullptr, *d_st_zh = nullptr, *d_st_zf = nullptr;
   int st_cap_jobs = 0, st_cap_ops = 0, st_nch = 1;
+  // Kessler microphysics (ptype=1)
+  float *b8 = nullptr, *vr = nullptr;         // buoyancy of the stage set-up; rain fall speed
+  double *mp_part = nullptr, *mp_colbud = nullptr;
+  double *mp_qbud = nullptr;                  // qbudget(1..7) and asq(1..3), accumulated on the device
+  int *mp_err = nullptr;
 };
 
 // Makes the context's profile (if any) the active one for the calling thread.
@@ -248,8 +255,16 @@ static int check_config(const cm1g_config_t *c) {
   if (c->advwenov != 0) return set_err(CM1G_ERR_UNSUPPORTED, "momentum WENO is not built");
   if (c->advwenos && c->weno_order != 5) return set_err(CM1G_ERR_UNSUPPORTED, "only WENO5 is built");
   if (c->nsound < 2 || (c->nsound % 2)) return set_err(CM1G_ERR_ARG, "nsound must be even and >= 2");
-  if (c->imoist && (c->numq != 1 || c->nqv != 1))
-    return set_err(CM1G_ERR_UNSUPPORTED, "moisture: water vapour only (numq=1, nqv=1)");
+  if (c->ptype != 0 && c->ptype != 1)
+    return set_err(CM1G_ERR_UNSUPPORTED, "microphysics: ptype=%d is not built (0 water vapour, 1 Kessler)", c->ptype);
+  if (c->imoist && c->ptype == 0 && (c->numq != 1 || c->nqv != 1))
+    return set_err(CM1G_ERR_UNSUPPORTED, "moisture: ptype=0 is water vapour only (numq=1, nqv=1)");
+  if (c->ptype == 1) {   // param.F:3169-3175
+    if (!c->imoist || c->numq != 3 || c->nqv != 1 || c->nql1 != 2 || c->nql2 != 3)
+      return set_err(CM1G_ERR_ARG, "Kessler needs imoist=1, numq=3, nqv=1, nql1=2, nql2=3");
+    if (c->efall != 0) return set_err(CM1G_ERR_UNSUPPORTED, "efall=1 is not built");
+    if (!(c->tsmall > 0.0f) || !(c->qsmall >= 0.0f)) return set_err(CM1G_ERR_ARG, "tsmall/qsmall not set");
+  }
   if (c->iptra && (c->npt < 0 || c->npt > CM1G_MAXQ)) return set_err(CM1G_ERR_ARG, "npt out of range");
   if (c->roflux != 0) return set_err(CM1G_ERR_UNSUPPORTED, "roflux=1 is not built");
   if (c->idiff != 0 && c->difforder != 6)
@@ -369,6 +384,14 @@ extern "C" int cm1g_init(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_c
   c->fscal = (float *)dalloc(c, 16 * sizeof(float));
   c->cflbits = (int *)dalloc(c, 16 * sizeof(int));
   c->mm = (unsigned long long *)dalloc(c, 4 * sizeof(unsigned long long));
+  if (cfg->ptype == 1) {
+    c->b8 = (float *)dalloc(c, bS);
+    c->vr = (float *)dalloc(c, bS);
+    c->mp_part = (double *)dalloc(c, (size_t)5 * g.nk * mp_chunks(g) * sizeof(double));
+    c->mp_colbud = (double *)dalloc(c, (size_t)2 * g.ni * g.nj * sizeof(double));
+    c->mp_qbud = (double *)dalloc(c, 16 * sizeof(double));
+    c->mp_err = (int *)dalloc(c, 4 * sizeof(int));
+  }
   for (void *p : c->allocs)
     if (!p) { cm1g_finalize(c); return set_err(CM1G_ERR_NOMEM, "scratch alloc"); }
   if (!c->mm) { cm1g_finalize(c); return set_err(CM1G_ERR_NOMEM, "scratch alloc"); }
@@ -473,6 +496,11 @@ static int stage_state(cm1g_ctx *c, Stager &S, const cm1g_state_t *st, cm1g_stat
   d->pta = S.in(st->pta, npt, true); d->pt3d = S.in(st->pt3d, npt, true); d->ptten = S.in(st->ptten, npt, false);
   d->radbcw = S.in(st->radbcw, nrw, true); d->radbce = S.in(st->radbce, nrw, true);
   d->radbcs = S.in(st->radbcs, nrs, true); d->radbcn = S.in(st->radbcn, nrs, true);
+  if (c->cfg.ptype == 1) {
+    d->rain = S.in(st->rain, (size_t)g.NI * g.NJ, true); d->prate = S.in(st->prate, (size_t)g.NI * g.NJ, true);
+  } else {
+    d->rain = d->prate = nullptr;
+  }
   if (S.err) return set_err(CM1G_ERR_NOMEM, "staging alloc");
   return CM1G_OK;
 }
@@ -483,6 +511,7 @@ static int check_state(const cm1g_ctx *c, const cm1g_state_t *st) {
                         st->radbcw, st->radbce, st->radbcs, st->radbcn};
   for (const float *p : req) if (!p) return set_err(CM1G_ERR_ARG, "state array missing");
   if (c->cfg.imoist && (!st->qa || !st->q3d || !st->qten)) return set_err(CM1G_ERR_ARG, "moisture arrays missing");
+  if (c->cfg.ptype == 1 && (!st->rain || !st->prate)) return set_err(CM1G_ERR_ARG, "Kessler needs rain and prate");
   if (c->cfg.iptra && c->cfg.npt > 0 && (!st->pta || !st->pt3d || !st->ptten))
     return set_err(CM1G_ERR_ARG, "tracer arrays missing");
   return CM1G_OK;
@@ -535,11 +564,17 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
     const float dttmp = dt / (float)(3 + 1 - nrk);
     const float *th_in = buf_in(0, nrk);
     const float *qv_in = cf.imoist ? buf_in(iqv, nrk) : nullptr;
-    launch_stage_prep(g, th_in, d->pp3d, qv_in, cf.imoist, cf.eqtset, c->t11, c->t22, c->thterm, c->piadv, st, nl);
+    LiquidIn liq;
+    if (cf.imoist && cf.nql1 > 0) {   // liquid species of this stage's input (solve2.F:315-345)
+      for (int n = cf.nql1; n <= cf.nql2 && liq.n < 2; n++) liq.q[liq.n++] = buf_in(n, nrk);
+      liq.b8 = c->b8;
+    }
+    launch_stage_prep(g, th_in, d->pp3d, qv_in, liq, cf.imoist, cf.eqtset, c->t11, c->t22, c->thterm, c->piadv, st,
+                      nl);
     launch_bc(g, c->t11, 2, 0, st, nl);
     if (diffit) df.coef = cf.kdiff6 / 64.0f / dttmp;   // adv.F:80-82, 962-964
     launch_adv_momentum(g, d->u3d, d->v3d, d->w3d, d->uten1, d->vten1, d->wten1, c->uten, c->vten, c->wten,
-                        th_in, qv_in, c->mdivx, st, nl, diffit ? &df : nullptr);
+                        th_in, qv_in, c->mdivx, st, nl, diffit ? &df : nullptr, liq.b8);
     launch_sound(g, cf.nsound, nrk, dt, d->ua, d->u3d, c->uten, d->va, d->v3d, c->vten, d->wa, d->w3d, c->wten,
                  d->ppi, d->pp3d, c->piadv, d->ppten, d->ppx, c->t11, c->t22, c->rru, c->rrv, c->rrw,
                  d->radbcw, d->radbce, d->radbcs, d->radbcn, c->su, c->sv, c->su2, c->sv2, c->d1, c->d2, st, nl);
@@ -654,9 +689,40 @@ static void run_solve3(cm1g_ctx *c, const cm1g_state_t *d) {
   }
 }
 
+// mp_driver's Kessler branch (mp_driver.F:189-233): pdefq of qv, qc, qr,
+// then fall speeds, geterain and fallout (k_mp_fall), kessler and satadj
+// (k_mp_point), and the FP64 budgets.
+static void run_kessler(cm1g_ctx *c, const cm1g_state_t *d, float dt) {
+  const DGrid &g = c->g;
+  const cm1g_config_t &cf = c->cfg;
+  const long ns = nS(g);
+  float *qv = d->q3d, *qc = d->q3d + ns, *qr = d->q3d + 2 * ns;
+  launch_pdefq(g, 0.0f, d->rho, qv, c->bud, c->mp_qbud + 8, c->stream, &c->nlaunch);
+  launch_pdefq(g, cf.qsmall, d->rho, qc, c->bud, c->mp_qbud + 9, c->stream, &c->nlaunch);
+  launch_pdefq(g, cf.qsmall, d->rho, qr, c->bud, c->mp_qbud + 10, c->stream, &c->nlaunch);
+  MicroArgs a{};
+  a.th3d = d->th3d; a.pp3d = d->pp3d; a.prs = d->prs; a.rho = d->rho;
+  a.qv = qv; a.qc = qc; a.qr = qr; a.vr = c->vr; a.rain = d->rain; a.prate = d->prate; a.err = c->mp_err;
+  a.dt = dt; a.converge = 2.0f * cf.tsmall; a.eqtset = cf.eqtset;
+  // constants.F:115-159
+  const Consts &k = g.c;
+  const int tc = cf.testcase;
+  const float xlv = tc == 4 ? 2.47e6f : tc == 5 ? 2.50e6f : 2501000.0f, to = 273.15f;
+  MicroConsts &m = a.c;
+  m.eps = k.rd / k.rv; m.reps = k.reps; m.rd = k.rd; m.rv = k.rv; m.cp = k.cp; m.cv = k.cv; m.cpv = k.cpv;
+  m.cvv = k.cvv; m.cpl = k.cpl; m.cpi = k.cpi;
+  m.lv1 = (tc == 4 || tc == 5) ? xlv : xlv + (k.cpl - k.cpv) * to;
+  m.lv2 = (tc == 4 || tc == 5) ? 0.0f : k.cpl - k.cpv;
+  m.cpdcv = k.cp / k.cv; m.rovcp = k.rovcp; m.rddcv = k.rddcv; m.cpdrd = k.cpdrd;
+  m.p00 = 1.0e5f; m.rp00 = 1.0f / 1.0e5f;
+  launch_kessler(g, a, c->mp_part, c->mp_colbud, c->mp_qbud, c->stream, &c->nlaunch);
+}
+
 static void run_step(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass1) {
   run_solve2(c, d, dt, mass1);
-  if (c->cfg.imoist)   // cm1.F:3410-3415 (ptype=0)
+  if (c->cfg.imoist && c->cfg.ptype == 1)   // cm1.F:3421-3431 (mp_driver)
+    run_kessler(c, d, dt);
+  else if (c->cfg.imoist)                   // cm1.F:3410-3415 (ptype=0)
     launch_pdefq(c->g, 0.0f, d->rho, d->q3d + (long)(c->cfg.nqv - 1) * nS(c->g), nullptr, nullptr, c->stream,
                  &c->nlaunch);
   run_solve3(c, d);
@@ -675,6 +741,14 @@ static int fetch_scalars(cm1g_ctx *c, double *mass2, float *cflmax) {
   // the reference stops the model when the step goes unstable (solve2.F:2082);
   // here a non-finite velocity is returned as an error code instead
   if (!std::isfinite(f)) return set_err(CM1G_ERR_NONFINITE, "non-finite velocity after the large step");
+  if (c->mp_err) {   // satadj without convergence (kessler.F:412-426 stops the model)
+    int err = 0;
+    CUCHK(cudaMemcpy(&err, c->mp_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) {
+      cudaMemset(c->mp_err, 0, sizeof(int));
+      return set_err(CM1G_ERR_NONFINITE, "satadj: convergence cannot be reached (unstable step?)");
+    }
+  }
   return CM1G_OK;
 }
 
@@ -720,11 +794,21 @@ static int solve_common(cm1g_ctx_t *c, float dt, double mass1, double *mass2, fl
   } else {
     if (which == 1) run_solve2(c, &d, dt, mass1);
     else if (which == 2) run_solve3(c, &d);
+    else if (which == 4) run_kessler(c, &d, dt);
     else run_step(c, &d, dt, mass1);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
-  if (which != 2) {
+  if (which == 4) {   // satadj's convergence flag only
+    int err = 0;
+    CUCHK(cudaMemcpyAsync(&err, c->mp_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CUCHK(cudaStreamSynchronize(c->stream));
+    if (err) {
+      cudaMemset(c->mp_err, 0, sizeof(int));
+      S.finish();
+      return set_err(CM1G_ERR_NONFINITE, "satadj: convergence cannot be reached (unstable step?)");
+    }
+  } else if (which != 2) {
     rc = fetch_scalars(c, mass2, cflmax);
     if (rc) return rc;
   }
@@ -739,6 +823,27 @@ extern "C" int cm1g_solve2(cm1g_ctx_t *c, int32_t nstep, float dt, double mtime,
 
 extern "C" int cm1g_solve3(cm1g_ctx_t *c, cm1g_state_t *st) {
   return solve_common(c, 1.0f, 1.0, nullptr, nullptr, st, 2, 0);
+}
+
+extern "C" int cm1g_mp_driver(cm1g_ctx_t *c, float dt, cm1g_state_t *st) {
+  if (!c) return set_err(CM1G_ERR_STATE, "null context");
+  if (c->cfg.ptype != 1 || !c->cfg.imoist) return set_err(CM1G_ERR_ARG, "cm1g_mp_driver needs ptype=1 (Kessler)");
+  return solve_common(c, dt, 1.0, nullptr, nullptr, st, 4, 0);
+}
+
+extern "C" int cm1g_mp_budget(cm1g_ctx_t *c, double qbudget[7], double asq[3], int32_t reset) {
+  if (!c) return set_err(CM1G_ERR_STATE, "null context");
+  if (!c->mp_qbud) return set_err(CM1G_ERR_ARG, "no microphysics budgets (ptype=0)");
+  double h[16];
+  CUCHK(cudaMemcpyAsync(h, c->mp_qbud, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  CUCHK(cudaStreamSynchronize(c->stream));
+  if (qbudget) for (int q = 0; q < 7; q++) qbudget[q] = h[q];
+  if (asq) for (int q = 0; q < 3; q++) asq[q] = h[8 + q];
+  if (reset) {
+    CUCHK(cudaMemsetAsync(c->mp_qbud, 0, 16 * sizeof(double), c->stream));
+    CUCHK(cudaStreamSynchronize(c->stream));
+  }
+  return CM1G_OK;
 }
 
 extern "C" int cm1g_step(cm1g_ctx_t *c, int32_t nstep, float dt, double mtime, double mass1, double *mass2,

@@ -164,6 +164,15 @@ __device__ __forceinline__ float diff6_limit(float f, float a0, float am1, int m
   return (mdiff == 1 && f * (a0 - am1) <= 0.0f) ? 0.0f : f;
 }
 
+// Liquid water of the stage set-up (ptype=1): the RK-stage input of each
+// liquid species (at most two: Kessler's qc, qr) and the buoyancy array
+// that the stage set-up writes for the w tendency (null without liquid).
+struct LiquidIn {
+  const float *q[2] = {nullptr, nullptr};
+  int n = 0;
+  float *b8 = nullptr;
+};
+
 // Inputs of the solve1 tendency initialisation and of calcener (k_misc.cu).
 struct TendIn {
   int irdamp;

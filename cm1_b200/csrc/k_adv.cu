@@ -149,7 +149,7 @@ template <int TX, int TY, int KC, int STAG, int DIFF>
 __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const float *__restrict__ divx,
                                                       const float *ten1, float *ten,
                                                       const float *__restrict__ th3d, const float *__restrict__ qv,
-                                                      Diff6 df) {
+                                                      const float *__restrict__ b8, Diff6 df) {
   constexpr int NT = TX * TY;
   constexpr int SW = TX + 6, SH = TY + 6, SP = SW + 1;
   constexpr int NST = (SW * SH + NT - 1) / NT;
@@ -273,7 +273,9 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
       pt1 = ten1[(long)kf * plane + oc];
       pd0 = LDG(&divx[oS]);
       pd1 = LDG(&divx[oS - ((STAG == 2) ? 1L : (STAG == 3) ? (long)g.NI : (long)g.NI * g.NJ)]);
-      if (STAG == 4 && th3d) {
+      if (STAG == 4 && b8) {          // buoyancy of the stage set-up (liquid water present)
+        pb0 = LDG(&b8[oS - (long)g.NI * g.NJ]); pb1 = LDG(&b8[oS]);
+      } else if (STAG == 4 && th3d) {
         pb0 = LDG(&th3d[oS - (long)g.NI * g.NJ]); pb1 = LDG(&th3d[oS]);
         if (qv) { pb2 = LDG(&qv[oS - (long)g.NI * g.NJ]); pb3 = LDG(&qv[oS]); }
       }
@@ -469,7 +471,8 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
         ten[o] = t1 + (((advx + advy) + advz) + ac * 0.5f * (dv0 + dv1)) * LDG(&g.rr0[k]);
       } else {
         float t = t1 + (((advx + advy) + advz) + ac * (c2k * dv0 + c1k * dv1)) * LDG(&g.rrf0[k]);
-        if (th3d) t = t + (c1k * buoy_v(g, b0, b2, qv != nullptr, k - 1) + c2k * buoy_v(g, b1, b3, qv != nullptr, k));
+        if (b8) t = t + (c1k * b0 + c2k * b1);
+        else if (th3d) t = t + (c1k * buoy_v(g, b0, b2, qv != nullptr, k - 1) + c2k * buoy_v(g, b1, b3, qv != nullptr, k));
         ten[o] = t;
       }
 #pragma unroll
@@ -483,33 +486,34 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
 template <int TX, int TY, int KC>
 static void mom_tiles_shape(const DGrid &g, const Vel &q, const float *uten1, const float *vten1,
                             const float *wten1, float *uten, float *vten, float *wten, const float *th3d,
-                            const float *qv, const float *divx, const Diff6 &df, cudaStream_t st) {
+                            const float *qv, const float *b8, const float *divx, const Diff6 &df,
+                            cudaStream_t st) {
   dim3 blk(TX, TY);
   const int kch = (g.nk + KC - 1) / KC, kchw = (g.nk - 1 + KC - 1) / KC;
   {
     dim3 grid((g.ni + 1 + TX - 1) / TX, (g.nj + TY - 1) / TY, kch);
     ProfScope _ps("k_advu", st);
-    if (df.rho) k_mom_tile<TX, TY, KC, 2, 1><<<grid, blk, 0, st>>>(g, q, divx, uten1, uten, nullptr, nullptr, df);
-    else k_mom_tile<TX, TY, KC, 2, 0><<<grid, blk, 0, st>>>(g, q, divx, uten1, uten, nullptr, nullptr, df);
+    if (df.rho) k_mom_tile<TX, TY, KC, 2, 1><<<grid, blk, 0, st>>>(g, q, divx, uten1, uten, nullptr, nullptr, nullptr, df);
+    else k_mom_tile<TX, TY, KC, 2, 0><<<grid, blk, 0, st>>>(g, q, divx, uten1, uten, nullptr, nullptr, nullptr, df);
   }
   {
     dim3 grid((g.ni + TX - 1) / TX, (g.nj + 1 + TY - 1) / TY, kch);
     ProfScope _ps("k_advv", st);
-    if (df.rho) k_mom_tile<TX, TY, KC, 3, 1><<<grid, blk, 0, st>>>(g, q, divx, vten1, vten, nullptr, nullptr, df);
-    else k_mom_tile<TX, TY, KC, 3, 0><<<grid, blk, 0, st>>>(g, q, divx, vten1, vten, nullptr, nullptr, df);
+    if (df.rho) k_mom_tile<TX, TY, KC, 3, 1><<<grid, blk, 0, st>>>(g, q, divx, vten1, vten, nullptr, nullptr, nullptr, df);
+    else k_mom_tile<TX, TY, KC, 3, 0><<<grid, blk, 0, st>>>(g, q, divx, vten1, vten, nullptr, nullptr, nullptr, df);
   }
   {
     dim3 grid((g.ni + TX - 1) / TX, (g.nj + TY - 1) / TY, kchw);
     ProfScope _ps("k_advw", st);
-    if (df.rho) k_mom_tile<TX, TY, KC, 4, 1><<<grid, blk, 0, st>>>(g, q, divx, wten1, wten, th3d, qv, df);
-    else k_mom_tile<TX, TY, KC, 4, 0><<<grid, blk, 0, st>>>(g, q, divx, wten1, wten, th3d, qv, df);
+    if (df.rho) k_mom_tile<TX, TY, KC, 4, 1><<<grid, blk, 0, st>>>(g, q, divx, wten1, wten, th3d, qv, b8, df);
+    else k_mom_tile<TX, TY, KC, 4, 0><<<grid, blk, 0, st>>>(g, q, divx, wten1, wten, th3d, qv, b8, df);
   }
 }
 
 void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w,
                          const float *uten1, const float *vten1, const float *wten1,
                          float *uten, float *vten, float *wten, const float *th3d, const float *qv,
-                         float *divx, cudaStream_t st, int64_t *nl, const Diff6 *diff) {
+                         float *divx, cudaStream_t st, int64_t *nl, const Diff6 *diff, const float *b8) {
   Vel q{u, v, w};
   const Diff6 df = diff ? *diff : Diff6{};
   {
@@ -520,7 +524,7 @@ void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const f
 #define CM1G_MOM_SHAPE(n)                                                                                     \
   case n:                                                                                                     \
     mom_tiles_shape<kTileShapes[n][0], kTileShapes[n][1], kTileShapes[n][2]>(g, q, uten1, vten1, wten1, uten, \
-                                                                             vten, wten, th3d, qv, divx, df, st); \
+                                                                             vten, wten, th3d, qv, b8, divx, df, st); \
     break;
   switch (g.tile_mom) {
     CM1G_MOM_SHAPE(1)

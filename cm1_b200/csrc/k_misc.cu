@@ -11,7 +11,7 @@ namespace cm1g {
 // on the interior and piadv = pi0+pp' on 0..ni+1 x 0..nj+1 (solve2.F:1027-1038)
 // ---------------------------------------------------------------------
 __global__ void k_stage_prep(DGrid g, const float *__restrict__ th3d, const float *__restrict__ pp3d,
-                             const float *__restrict__ qv, int imoist, int eqtset,
+                             const float *__restrict__ qv, LiquidIn liq, int imoist, int eqtset,
                              float *__restrict__ t11, float *__restrict__ t22, float *__restrict__ thterm,
                              float *__restrict__ piadv) {
   const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);       // 0..ni+1
@@ -26,8 +26,19 @@ __global__ void k_stage_prep(DGrid g, const float *__restrict__ th3d, const floa
   const float th3 = LDG(&th3d[o]), th0 = LDG(&g.th0[k]), pi0 = LDG(&g.pi0[k]);
   if (imoist) {
     const float q = fmaxf(LDG(&qv[o]), 0.0f);
-    const float d2 = 0.0f, d3 = 0.0f;   // water vapour only: no liquid or ice arrays
+    // dum2: the liquid species in index order (solve2.F:315-345); no ice
+    float d2 = 0.0f;
+    if (liq.n > 0) {
+      d2 = LDG(&liq.q[0][o]);
+      for (int n = 1; n < liq.n; n++) d2 = d2 + LDG(&liq.q[n][o]);
+    }
+    const float d3 = 0.0f;
     const float qli = fmaxf(0.0f, d2 + d3);
+    // buoyancy dum8 at s-points (solve2.F:395-396) when liquid is present;
+    // without it k_mom_tile forms the same expression from theta and qv
+    if (liq.b8)
+      liq.b8[o] = c.g * ((th3 * LDG(&g.rth0[k]) + c.repsm1 * (q - LDG(&g.qv0[k]))) -
+                         ((qli - LDG(&g.qc0[k])) - LDG(&g.qi0[k])));
     t11[o] = (th0 + th3) * (1.0f + c.reps * q) / ((1.0f + q) + qli);
     if (eqtset == 2) {
       const float cpli = c.cpl * fmaxf(0.0f, d2) + c.cpi * fmaxf(0.0f, d3);
@@ -44,11 +55,12 @@ __global__ void k_stage_prep(DGrid g, const float *__restrict__ th3d, const floa
   }
 }
 
-void launch_stage_prep(const DGrid &g, const float *th3d, const float *pp3d, const float *qv, int imoist, int eqtset,
-                       float *t11, float *t22, float *thterm, float *piadv, cudaStream_t st, int64_t *nl) {
+void launch_stage_prep(const DGrid &g, const float *th3d, const float *pp3d, const float *qv, const LiquidIn &liq,
+                       int imoist, int eqtset, float *t11, float *t22, float *thterm, float *piadv, cudaStream_t st,
+                       int64_t *nl) {
   dim3 grid((g.ni + 2 + 127) / 128, g.nj + 2, g.nk);
   // j index offset: blockIdx.y = j directly (0..nj+1)
-  { ProfScope _ps("k_stage_prep", st); k_stage_prep<<<grid, 128, 0, st>>>(g, th3d, pp3d, qv, imoist, eqtset, t11, t22, thterm, piadv); }
+  { ProfScope _ps("k_stage_prep", st); k_stage_prep<<<grid, 128, 0, st>>>(g, th3d, pp3d, qv, liq, imoist, eqtset, t11, t22, thterm, piadv); }
   if (nl) *nl += 1;
 }
 

@@ -6,12 +6,12 @@
 !    use cm1g_iso
 !    ...  (once, after param/base/init3d)
 !    call cm1g_setup( cm1g_ctx )
-!    ...  (in the time loop, instead of solve2 + pdefq + solve3)
+!    ...  (in the time loop, instead of solve2 + pdefq or mp_driver + solve3)
 !    call cm1g_large_step( cm1g_ctx, nstep, dt, mtime, mass1, mass2, cflmax, &
 !                          ua,u3d,uten1, va,v3d,vten1, wa,w3d,wten1,       &
 !                          ppi,pp3d,ppx,ppten, tha,th3d,thten1, rho,prs,   &
 !                          qa,q3d,qten, pta,pt3d,ptten,                    &
-!                          radbcw,radbce,radbcs,radbcn )
+!                          radbcw,radbce,radbcs,radbcn, rain,prate )
 !
 !  The arrays are the model's own (ib:ie,jb:je,kb:ke ...) arrays; the
 !  library copies them to the GPU and back each call.  Fortran `real` is
@@ -49,6 +49,8 @@ module cm1g_iso
     real(c_float)      :: qmag(CM1G_MAXQ)
     integer(c_int32_t) :: idiff, difforder, mdiff
     real(c_float)      :: kdiff6
+    integer(c_int32_t) :: ptype, nql1, nql2, efall
+    real(c_float)      :: tsmall, qsmall
   end type
 
   type, bind(C) :: cm1g_grid_t
@@ -63,6 +65,7 @@ module cm1g_iso
     type(c_ptr) :: ppi, pp3d, ppx, ppten, tha, th3d, thten1, rho, prs
     type(c_ptr) :: qa, q3d, qten, pta, pt3d, ptten
     type(c_ptr) :: radbcw, radbce, radbcs, radbcn
+    type(c_ptr) :: rain, prate
   end type
 
   ! launch shapes of the large step (cm1g_set_tune / cm1g_autotune)
@@ -289,6 +292,8 @@ contains
     cfg%smeps = smeps; cfg%testcase = testcase; cfg%psolver = psolver
     cfg%terrain_flag = merge(1, 0, terrain_flag); cfg%axisymm = axisymm; cfg%icor = icor
     cfg%idiff = idiff; cfg%difforder = difforder; cfg%mdiff = mdiff; cfg%kdiff6 = kdiff6
+    cfg%ptype = ptype; cfg%nql1 = nql1; cfg%nql2 = nql2; cfg%efall = efall
+    cfg%tsmall = tsmall; cfg%qsmall = qsmall
     cfg%qmag = 0.0
     do n = 1, min(size(qmag), int(CM1G_MAXQ))
       cfg%qmag(n) = qmag(n)
@@ -308,11 +313,13 @@ contains
     endif
   end subroutine
 
-  ! One large step (solve2 + pdefq for qv + solve3's dynamical-core part).
+  ! One large step (solve2, then pdefq for qv (ptype=0) or mp_driver's
+  ! Kessler branch (ptype=1), then solve3's dynamical-core part).
   subroutine cm1g_large_step(ctx, nstep, dt, mtime, mass1, mass2, cflmax, &
                              ua,u3d,uten1, va,v3d,vten1, wa,w3d,wten1,   &
                              ppi,pp3d,ppx,ppten, tha,th3d,thten1, rho,prs, &
-                             qa,q3d,qten, pta,pt3d,ptten, radbcw,radbce,radbcs,radbcn)
+                             qa,q3d,qten, pta,pt3d,ptten, radbcw,radbce,radbcs,radbcn, &
+                             rain,prate)
     type(c_ptr), intent(in) :: ctx
     integer, intent(in) :: nstep
     real, intent(in) :: dt
@@ -323,6 +330,7 @@ contains
     real, target, intent(inout) :: ppi(*),pp3d(*),ppx(*),ppten(*),tha(*),th3d(*),thten1(*),rho(*),prs(*)
     real, target, intent(inout) :: qa(*),q3d(*),qten(*),pta(*),pt3d(*),ptten(*)
     real, target, intent(inout) :: radbcw(*),radbce(*),radbcs(*),radbcn(*)
+    real, target, intent(inout) :: rain(*),prate(*)
     type(cm1g_state_t) :: s
     integer :: rc
     s%ua = c_loc(ua); s%u3d = c_loc(u3d); s%uten1 = c_loc(uten1)
@@ -334,6 +342,7 @@ contains
     s%qa = c_loc(qa); s%q3d = c_loc(q3d); s%qten = c_loc(qten)
     s%pta = c_loc(pta); s%pt3d = c_loc(pt3d); s%ptten = c_loc(ptten)
     s%radbcw = c_loc(radbcw); s%radbce = c_loc(radbce); s%radbcs = c_loc(radbcs); s%radbcn = c_loc(radbcn)
+    s%rain = c_loc(rain); s%prate = c_loc(prate)
     rc = cm1g_step(ctx, int(nstep, c_int32_t), dt, mtime, mass1, mass2, cflmax, s, 0_c_int32_t)
     if (rc /= 0) then
       print *, ' cm1g_step failed: ', trim(cm1g_last_error_f())

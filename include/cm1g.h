@@ -86,6 +86,13 @@ typedef struct cm1g_config {
   int32_t difforder;           /* 6 (the advection-embedded 6th-order form) only  */
   int32_t mdiff;               /* 1: monotonic limiter of the 6th-order fluxes    */
   float   kdiff6;              /* 6th-order coefficient: kdiff6/64/dt per step    */
+  int32_t ptype;               /* microphysics: 0 water vapour only (pdefq after  */
+                               /* solve2), 1 Kessler (numq=3: qv, qc, qr)         */
+  int32_t nql1, nql2;          /* 1-based q indices of the liquid species (0 0:   */
+                               /* none; Kessler 2 3), param.F:3169-3175           */
+  int32_t efall;               /* energy fallout correction of mp_driver: 0 only  */
+  float   tsmall, qsmall;      /* cm1.F:311-319 (1e-4, 1e-14): satadj's           */
+                               /* convergence 2*tsmall, pdefq floor of qc, qr     */
 } cm1g_config_t;
 
 /*
@@ -121,6 +128,8 @@ typedef struct cm1g_state {
   float *pta, *pt3d, *ptten;         /* npt  s-point arrays */
   float *radbcw, *radbce;            /* (jb:je,kb:ke) */
   float *radbcs, *radbcn;            /* (ib:ie,kb:ke) */
+  float *rain, *prate;               /* (ib:ie,jb:je): accumulated surface rain (cm) and
+                                        the surface precipitation rate (ptype=1; nrain=1) */
 } cm1g_state_t;
 
 typedef struct cm1g_ctx cm1g_ctx_t;
@@ -154,12 +163,28 @@ int cm1g_pdefq(cm1g_ctx_t *ctx, float rmax, double *asq, const float *rho, float
 int cm1g_solve3(cm1g_ctx_t *ctx, cm1g_state_t *st);
 
 /* One complete large step as the reference's time loop runs it
- * (cm1.F:3357 solve2, cm1.F:3414 pdefq for qv-only moisture, cm1.F:3432
- * solve3).  With use_graph != 0 the step is captured once in a CUDA graph
- * and replayed (device pointers only). */
+ * (cm1.F:3357 solve2; cm1.F:3414 pdefq for qv-only moisture or mp_driver's
+ * Kessler branch for ptype=1; cm1.F:3432 solve3).  With use_graph != 0
+ * the step is captured once in a CUDA graph and replayed (device pointers
+ * only). */
 int cm1g_step(cm1g_ctx_t *ctx, int32_t nstep, float dt, double mtime,
               double mass1, double *mass2, float *cflmax, cm1g_state_t *st,
               int32_t use_graph);
+
+/* Kessler warm-rain microphysics (ptype=1): replaces the Kessler branch of
+ * mp_driver (src/mp_driver.F:189-233) that cm1.F:3421-3431 calls between
+ * solve2 and solve3: pdefq of qv, qc, qr; rain fall speeds (k_fallout),
+ * geterain, fallout (sedimentation, st->rain += rain, st->prate), kessler
+ * (autoconversion, accretion, evaporation) and satadj (saturation
+ * adjustment, nrk=4), kessler.F:10-558.  cm1g_step runs it itself when
+ * ptype=1.  Where satadj does not converge in 100 iterations the reference
+ * stops the model; here the call returns CM1G_ERR_NONFINITE.
+ * cm1g_mp_budget reads the FP64 budgets the context has accumulated:
+ * qbudget(1..7) (tcond, tevac, tauto, taccr, tevar, train, erain, the
+ * reference's qbudget entries 1-7) and asq(1..3) of the three pdefq calls;
+ * reset != 0 zeroes them afterwards. */
+int cm1g_mp_driver(cm1g_ctx_t *ctx, float dt, cm1g_state_t *st);
+int cm1g_mp_budget(cm1g_ctx_t *ctx, double qbudget[7], double asq[3], int32_t reset);
 
 /* Lateral boundary fills: replace bcs, bcp, bcu, bcv, bcw
  * (src/bc.F:180, 372, 528, 722, 942).  flag as in bcw (1: w=0 top/bottom). */

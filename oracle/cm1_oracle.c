@@ -1452,6 +1452,7 @@ typedef struct {
   F3 qa[CM1G_MAXQ], q3d[CM1G_MAXQ], qten[CM1G_MAXQ];
   F3 pta[CM1G_MAXQ], pt3d[CM1G_MAXQ], ptten[CM1G_MAXQ];
   float *radbcw, *radbce, *radbcs, *radbcn;
+  F3 rain, prate;   /* (ib:ie,jb:je), ptype=1 */
 } St;
 
 static void st_view(const OG *g, const cm1g_state_t *s, St *t) {
@@ -1466,10 +1467,14 @@ static void st_view(const OG *g, const cm1g_state_t *s, St *t) {
   for (int q = 0; q < numq; q++) { t->qa[q] = mkS(g, RP(s->qa) + q * n); t->q3d[q] = mkS(g, RP(s->q3d) + q * n); t->qten[q] = mkS(g, RP(s->qten) + q * n); }
   for (int q = 0; q < npt; q++) { t->pta[q] = mkS(g, RP(s->pta) + q * n); t->pt3d[q] = mkS(g, RP(s->pt3d) + q * n); t->ptten[q] = mkS(g, RP(s->ptten) + q * n); }
   t->radbcw = RP(s->radbcw); t->radbce = RP(s->radbce); t->radbcs = RP(s->radbcs); t->radbcn = RP(s->radbcn);
+  if (g->cfg->ptype == 1) { t->rain = mk2(g, RP(s->rain)); t->prate = mk2(g, RP(s->prate)); }
 }
 
 static int check_cfg(const cm1g_config_t *cfg) {
-  if (cfg->imoist && (cfg->numq < 1 || cfg->numq > CM1G_MAXQ || cfg->nqv != 1 || cfg->numq != 1)) return -1;
+  if (cfg->imoist && cfg->ptype == 0 && (cfg->nqv != 1 || cfg->numq != 1)) return -1;
+  if (cfg->ptype == 1 && (!cfg->imoist || cfg->numq != 3 || cfg->nqv != 1 || cfg->nql1 != 2 || cfg->nql2 != 3 ||
+                          cfg->efall != 0)) return -1;
+  if (cfg->ptype != 0 && cfg->ptype != 1) return -1;
   if (cfg->iptra && (cfg->npt < 0 || cfg->npt > CM1G_MAXQ)) return -1;
   if (cfg->roflux != 0) return -1;
   if ((cfg->wbc == 2 || cfg->ebc == 2 || cfg->sbc == 2 || cfg->nbc == 2) && cfg->irbc != 4) return -1;
@@ -1528,7 +1533,12 @@ int oracle_solve2(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_state_t 
       float th3 = A3(s.th3d, i, j, k), th0 = A3(g->th0, i, j, k), pi0 = A3(g->pi0, i, j, k);
       if (cfg->imoist) {
         float qv = fmaxf(A3(s.q3d[cfg->nqv - 1], i, j, k), 0.0f);
-        float d2 = 0.0f, d3 = 0.0f;  /* no liquid or ice species (ptype=0) */
+        /* dum2: the liquid species (solve2.F:315-345); no ice */
+        float d2 = 0.0f, d3 = 0.0f;
+        if (cfg->nql1 > 0) {
+          d2 = A3(s.q3d[cfg->nql1 - 1], i, j, k);
+          for (int n = cfg->nql1 + 1; n <= cfg->nql2; n++) d2 = d2 + A3(s.q3d[n - 1], i, j, k);
+        }
         float qli = fmaxf(0.0f, d2 + d3);
         A3(dum8, i, j, k) = c.g * ((th3 * A3(g->rth0, i, j, k) + c.repsm1 * (qv - A3(g->qv0, i, j, k))) -
                                    ((qli - A3(g->qc0, i, j, k)) - A3(g->qi0, i, j, k)));
@@ -1763,12 +1773,314 @@ int oracle_pdefq(const cm1g_config_t *cfg, const cm1g_grid_t *gr, float rmax, do
   return 0;
 }
 
-/* One time step as cm1.F runs it: solve2 (3357), pdefq for ptype=0 (3414), solve3 (3432). */
+/* ------------------------------------------------------------------ */
+/* Kessler microphysics (ptype=1): mp_driver.F:189-233, kessler.F      */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+  float eps, lv1, lv2, cpdcv, rp00;
+} KConsts;
+
+static KConsts kessler_consts(const OG *g) {
+  /* constants.F:115-159 */
+  const Consts c = g->c;
+  const int tc = g->cfg->testcase;
+  const float xlv = tc == 4 ? 2.47e6f : tc == 5 ? 2.50e6f : 2501000.0f, to = 273.15f;
+  KConsts k;
+  k.eps = c.rd / c.rv;
+  k.lv1 = (tc == 4 || tc == 5) ? xlv : xlv + (c.cpl - c.cpv) * to;
+  k.lv2 = (tc == 4 || tc == 5) ? 0.0f : c.cpl - c.cpv;
+  k.cpdcv = c.cp / c.cv;
+  k.rp00 = 1.0f / P00;
+  return k;
+}
+
+/* k_fallout (kessler.F:441-462) */
+static void k_fallout_g(const OG *g, F3 rho, F3 qr, F3 vr) {
+#pragma omp parallel for
+  for (int k = 1; k <= g->nk; k++) for (int j = 1; j <= g->nj; j++) for (int i = 1; i <= g->ni; i++) {
+    A3(vr, i, j, k) = 0.0f;
+    if (A3(qr, i, j, k) > 1.0e-12f)
+      A3(vr, i, j, k) = 14.34f * powf(A3(rho, i, j, k) * A3(qr, i, j, k), 0.1346f) * sqrtf(1.15f / A3(rho, i, j, k));
+  }
+}
+
+/* geterain (kessler.F:529-558) */
+static void geterain_g(const OG *g, float dt, float cpx, float lx1, double *erain, F3 t, F3 rr, F3 q, F3 vr) {
+  double *bud = (double *)calloc((size_t)g->nj + 1, sizeof(double));
+#pragma omp parallel for
+  for (int j = 1; j <= g->nj; j++) {
+    bud[j] = 0.0;
+    for (int i = 1; i <= g->ni; i++)
+      bud[j] = bud[j] + (double)(dt * A3(vr, i, j, 1) * A3(rr, i, j, 1) * A3(q, i, j, 1) * (cpx * A3(t, i, j, 1) - lx1) *
+                                 RUH(i) * RVH(j));
+  }
+  for (int j = 1; j <= g->nj; j++) *erain = *erain + bud[j] * (double)g->dx * (double)g->dy;
+  free(bud);
+}
+
+/* fallout (kessler.F:470-521), nrain = 1 */
+static void fallout_g(const OG *g, float dt, double *train, F3 rain, F3 prate, F3 rr, F3 rho, F3 q, F3 vq) {
+  const int ni = g->ni, nj = g->nj, nk = g->nk;
+  double *bud = (double *)calloc((size_t)nj + 1, sizeof(double));
+#pragma omp parallel for
+  for (int j = 1; j <= nj; j++) {
+    float *rq = (float *)calloc((size_t)nk + 5, sizeof(float));   /* rq(-1:nk+3) at rq[k+1] */
+    bud[j] = 0.0;
+    for (int i = 1; i <= ni; i++) {
+      float crmax = 0.0f;
+      for (int k = 1; k <= nk; k++) crmax = fmaxf(crmax, A3(vq, i, j, k) * dt * g->rdz * A3(g->mh, i, j, k));
+      int nfall = (int)(crmax + 1.0f);
+      if (nfall < 1) nfall = 1;
+      for (int k = nk - 1; k >= 1; k--)
+        if (A3(q, i, j, k) < 1.0e-8f) A3(vq, i, j, k) = A3(vq, i, j, k + 1);
+      float dtfall = dt / (float)nfall;
+      for (int n = 1; n <= nfall; n++) {
+        for (int k = 1; k <= nk; k++) rq[k + 1] = A3(rho, i, j, k) * A3(vq, i, j, k) * fmaxf(0.0f, A3(q, i, j, k));
+        rq[nk + 2] = 0.0f;
+        for (int k = 1; k <= nk; k++)
+          A3(q, i, j, k) = A3(q, i, j, k) + dtfall * (rq[k + 2] - rq[k + 1]) * g->rdz * A3(g->mh, i, j, k) /
+                                                A3(rho, i, j, k);
+        A3(rain, i, j, 0) = A3(rain, i, j, 0) + 0.1f * dtfall * rq[2];
+        A3(prate, i, j, 0) = rq[2];
+        bud[j] = bud[j] + (double)(dtfall * A3(rr, i, j, 1) * A3(vq, i, j, 1) * fmaxf(0.0f, A3(q, i, j, 1)) * RUH(i) *
+                                   RVH(j));
+      }
+    }
+    free(rq);
+  }
+  double tem = (double)(g->dx * g->dy);
+  for (int j = 1; j <= nj; j++) *train = *train + bud[j] * tem;
+  free(bud);
+}
+
+static float esl_of(float t, float p) {
+  float esl = 611.2f * expf(17.67f * (t - 273.15f) / (t - 29.65f));
+  return fminf(esl, p * 0.5f);
+}
+
+/* kessler (kessler.F:10-133) */
+static void kessler_g(const OG *g, float dt, double *tauto, double *taccr, double *tevar, F3 tmp, F3 rho, F3 rr,
+                      F3 pp3d, F3 th3d, F3 prs, F3 qv3d, F3 qc3d, F3 qr3d) {
+  const int ni = g->ni, nj = g->nj, nk = g->nk;
+  const Consts c = g->c;
+  const KConsts K = kessler_consts(g);
+  double *bud = (double *)calloc((size_t)3 * (nk + 1), sizeof(double));
+#pragma omp parallel for
+  for (int k = 1; k <= nk; k++) {
+    double b1 = 0.0, b2 = 0.0, b3 = 0.0;
+    for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++) {
+      const float th0 = A3(g->th0, i, j, k), pi0 = A3(g->pi0, i, j, k);
+      A3(tmp, i, j, k) = (th0 + A3(th3d, i, j, k)) * (pi0 + A3(pp3d, i, j, k));
+      float qvnew = A3(qv3d, i, j, k), qcnew = A3(qc3d, i, j, k), qrnew = A3(qr3d, i, j, k);
+      float ar = 0.0f, cr = 0.0f, er = 0.0f;
+      if (qcnew > 0.0f) {
+        ar = fmaxf(0.001f * (qcnew - 0.001f), 0.0f);
+        ar = ar * dt;
+      }
+      if (qcnew > 0.0f && qrnew > 0.0f) {
+        cr = 2.2f * qcnew * powf(qrnew, 0.875f);
+        cr = cr * dt;
+      }
+      if (qrnew > 0.0f) {
+        float esl = esl_of(A3(tmp, i, j, k), A3(prs, i, j, k));
+        float qvs = K.eps * esl / (A3(prs, i, j, k) - esl);
+        if (qvnew < qvs) {
+          float r = A3(rho, i, j, k);
+          er = (1.6f + 30.3922f * powf(r * qrnew, 0.2046f)) * (1.0f - (qvnew / qvs)) * powf(r * qrnew, 0.525f) /
+               ((2.03e4f + 9.584e6f / (qvs * A3(prs, i, j, k))) * r);
+          er = fminf(er * dt, qrnew);
+          if ((qvnew + er) > qvs) er = qvs - qvnew;
+        }
+      }
+      if ((ar + cr) > qcnew) {
+        float term1 = ar + cr;
+        ar = qcnew * ar / term1;
+        cr = qcnew * cr / term1;
+      }
+      qvnew = qvnew + er;
+      qcnew = qcnew - (ar + cr);
+      qrnew = qrnew + (ar + cr - er);
+      if (er > 1.0e-7f) {
+        if (g->cfg->eqtset == 2) {
+          float cpml = c.cp + c.cpv * qvnew + c.cpl * (qcnew + qrnew);
+          float cvml = c.cv + c.cvv * qvnew + c.cpl * (qcnew + qrnew);
+          float rm = c.rd + c.rv * qvnew;
+          A3(th3d, i, j, k) = A3(th3d, i, j, k) -
+              er * ((K.lv1 - K.lv2 * A3(tmp, i, j, k)) / (K.cpdcv * cvml * (pi0 + A3(pp3d, i, j, k))) -
+                    (th0 + A3(th3d, i, j, k)) * (c.rv / cvml) * (1.0f - c.rovcp * cpml / rm));
+          A3(pp3d, i, j, k) = powf(A3(rho, i, j, k) * rm * (th0 + A3(th3d, i, j, k)) * K.rp00, c.rddcv) - pi0;
+          A3(prs, i, j, k) = P00 * powf(pi0 + A3(pp3d, i, j, k), c.cpdrd);
+        } else {
+          A3(th3d, i, j, k) = A3(th3d, i, j, k) - er * ((K.lv1 - K.lv2 * A3(tmp, i, j, k)) / (c.cp * (pi0 + A3(pp3d, i, j, k))));
+          A3(rho, i, j, k) = A3(prs, i, j, k) /
+              (c.rd * (th0 + A3(th3d, i, j, k)) * (pi0 + A3(pp3d, i, j, k)) * (1.0f + qvnew * c.reps));
+        }
+      }
+      float tem = RUH(i) * RVH(j) * A3(g->rmh, i, j, k);
+      b1 = b1 + (double)(A3(rr, i, j, k) * ar * tem);
+      b2 = b2 + (double)(A3(rr, i, j, k) * cr * tem);
+      b3 = b3 + (double)(A3(rr, i, j, k) * er * tem);
+      A3(qv3d, i, j, k) = qvnew;
+      A3(qc3d, i, j, k) = qcnew;
+      A3(qr3d, i, j, k) = qrnew;
+    }
+    bud[3 * k] = b1; bud[3 * k + 1] = b2; bud[3 * k + 2] = b3;
+  }
+  double dum = (double)(g->dx * g->dy * g->dz);
+  for (int k = 1; k <= nk; k++) *tauto = *tauto + bud[3 * k] * dum;
+  for (int k = 1; k <= nk; k++) *taccr = *taccr + bud[3 * k + 1] * dum;
+  for (int k = 1; k <= nk; k++) *tevar = *tevar + bud[3 * k + 2] * dum;
+  free(bud);
+}
+
+/* satadj (kessler.F:142-432) with nrk = 4; returns 1 when an iteration did
+ * not converge (the reference stops the model) */
+static int satadj_g(const OG *g, float dt, double *tcond, double *tevac, F3 rho, F3 rr, F3 pp3d, F3 prs, F3 th3d,
+                    F3 *q3d) {
+  (void)dt;
+  const int ni = g->ni, nj = g->nj, nk = g->nk;
+  const Consts c = g->c;
+  const KConsts K = kessler_consts(g);
+  const cm1g_config_t *cfg = g->cfg;
+  const int nqv = cfg->nqv - 1, nqc = cfg->nql1 - 1;
+  double *bud = (double *)calloc((size_t)2 * (nk + 1), sizeof(double));
+  int iflag = 0;
+  if (cfg->eqtset == 2) {
+    const float converge = 2.0f * cfg->tsmall;
+#pragma omp parallel for reduction(|:iflag)
+    for (int k = 1; k <= nk; k++) {
+      double b1 = 0.0, b2 = 0.0;
+      for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++) {
+        const float th0 = A3(g->th0, i, j, k), pi0 = A3(g->pi0, i, j, k);
+        float tnew = (th0 + A3(th3d, i, j, k)) * (pi0 + A3(pp3d, i, j, k));
+        float esl = esl_of(tnew, A3(prs, i, j, k));
+        float qvs = K.eps * esl / (A3(prs, i, j, k) - esl);
+        if (A3(q3d[nqc], i, j, k) > 1.0e-12f || A3(q3d[nqv], i, j, k) > qvs) {
+          float qvnew = A3(q3d[nqv], i, j, k), qcnew = A3(q3d[nqc], i, j, k);
+          float ql = 0.0f, qi = 0.0f;
+          for (int n = cfg->nql1; n <= cfg->nql2; n++) ql = ql + A3(q3d[n - 1], i, j, k);
+          ql = fmaxf(0.0f, ql);
+          qi = fmaxf(0.0f, qi);
+          float cvml = c.cv + c.cvv * qvnew + c.cpl * ql + c.cpi * qi;
+          float lhv = K.lv1 - K.lv2 * tnew;
+          float t1 = (lhv - c.rv * tnew) / cvml;
+          float d1 = t1 * 17.67f * 243.5f;
+          int n = 0;
+          float tlast = tnew, pnew = 0.0f;
+          int doit = 1;
+          while (doit) {
+            n = n + 1;
+            float dqv = (qvs - qvnew) / (1.0f + d1 * qvs / ((tnew - 29.65f) * (tnew - 29.65f)));
+            dqv = fminf(dqv, qcnew);
+            if ((qvnew + dqv) < 1.0e-20f) dqv = 1.0e-20f - qvnew;
+            qvnew = qvnew + dqv;
+            qcnew = qcnew - dqv;
+            tnew = tnew - dqv * t1;
+            pnew = A3(rho, i, j, k) * (c.rd + c.rv * qvnew) * tnew;
+            doit = 0;
+            if (fabsf(tnew - tlast) > converge) {
+              tlast = tnew;
+              esl = esl_of(tnew, A3(prs, i, j, k));
+              qvs = K.eps * esl / (pnew - esl);
+              doit = 1;
+            }
+            if (n == 100) { iflag = 1; doit = 0; }
+          }
+          float tem = RUH(i) * RVH(j) * A3(g->rmh, i, j, k);
+          b1 = b1 + (double)(A3(rr, i, j, k) * fmaxf(qcnew - A3(q3d[nqc], i, j, k), 0.0f) * tem);
+          b2 = b2 + (double)(A3(rr, i, j, k) * fmaxf(qvnew - A3(q3d[nqv], i, j, k), 0.0f) * tem);
+          A3(prs, i, j, k) = pnew;
+          A3(pp3d, i, j, k) = powf(pnew * K.rp00, c.rovcp) - pi0;
+          A3(th3d, i, j, k) = tnew / (pi0 + A3(pp3d, i, j, k)) - th0;
+          A3(q3d[nqc], i, j, k) = qcnew;
+          A3(q3d[nqv], i, j, k) = qvnew;
+        }
+      }
+      bud[2 * k] = b1; bud[2 * k + 1] = b2;
+    }
+  } else {
+#pragma omp parallel for
+    for (int k = 1; k <= nk; k++) {
+      double b1 = 0.0, b2 = 0.0;
+      for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++) {
+        const float th0 = A3(g->th0, i, j, k), pi0 = A3(g->pi0, i, j, k);
+        float qvnew = A3(q3d[nqv], i, j, k), qcnew = A3(q3d[nqc], i, j, k);
+        float tnew = (th0 + A3(th3d, i, j, k)) * (pi0 + A3(pp3d, i, j, k));
+        float esl = esl_of(tnew, A3(prs, i, j, k));
+        float qvs = K.eps * esl / (A3(prs, i, j, k) - esl);
+        float lhv = K.lv1 - K.lv2 * tnew;
+        float dqv = (qvs - qvnew) / (1.0f + lhv * qvs * 17.67f * 243.5f / (c.cp * ((tnew - 29.65f) * (tnew - 29.65f))));
+        if ((qvnew + dqv) < 1.0e-20f) dqv = 1.0e-20f - qvnew;
+        dqv = fminf(dqv, fmaxf(0.0f, qcnew));
+        qvnew = qvnew + dqv;
+        qcnew = qcnew - dqv;
+        float tem = RUH(i) * RVH(j) * A3(g->rmh, i, j, k);
+        b1 = b1 + (double)(A3(rr, i, j, k) * fmaxf(qcnew - A3(q3d[nqc], i, j, k), 0.0f) * tem);
+        b2 = b2 + (double)(A3(rr, i, j, k) * fmaxf(qvnew - A3(q3d[nqv], i, j, k), 0.0f) * tem);
+        A3(th3d, i, j, k) = A3(th3d, i, j, k) - dqv * (lhv / (c.cp * (pi0 + A3(pp3d, i, j, k))));
+        A3(q3d[nqc], i, j, k) = qcnew;
+        A3(q3d[nqv], i, j, k) = qvnew;
+        A3(rho, i, j, k) = A3(prs, i, j, k) /
+            (c.rd * (th0 + A3(th3d, i, j, k)) * (pi0 + A3(pp3d, i, j, k)) * (1.0f + qvnew * c.reps));
+      }
+      bud[2 * k] = b1; bud[2 * k + 1] = b2;
+    }
+  }
+  double dum = (double)(g->dx * g->dy * g->dz);
+  for (int k = 1; k <= nk; k++) *tcond = *tcond + bud[2 * k] * dum;
+  for (int k = 1; k <= nk; k++) *tevac = *tevac + bud[2 * k + 1] * dum;
+  free(bud);
+  return iflag;
+}
+
+/* The Kessler branch of mp_driver (mp_driver.F:98-233, efall = 0):
+ * qbudget[0..6] = qbudget(1..7), asq[0..2] = asq(1..3). */
+static int mp_kessler_g(const OG *g, St *s, float dt, double *qbudget, double *asq) {
+  const long ns = nS(g);
+  const Consts c = g->c;
+  const KConsts K = kessler_consts(g);
+  float *buf = (float *)calloc((size_t)3 * ns, sizeof(float));
+  if (!buf) return -3;
+  F3 dum1 = mkS(g, buf), dum3 = mkS(g, buf + ns), vr = mkS(g, buf + 2 * ns);
+  for (int k = 1; k <= g->nk; k++) for (int j = 1; j <= g->nj; j++) for (int i = 1; i <= g->ni; i++) {
+    A3(dum1, i, j, k) = (A3(g->th0, i, j, k) + A3(s->th3d, i, j, k)) * (A3(g->pi0, i, j, k) + A3(s->pp3d, i, j, k));
+    A3(dum3, i, j, k) = A3(s->rho, i, j, k);
+  }
+  asq[0] += pdefq_g(g, 0.0f, s->rho, s->q3d[0]);
+  asq[1] += pdefq_g(g, g->cfg->qsmall, s->rho, s->q3d[1]);
+  asq[2] += pdefq_g(g, g->cfg->qsmall, s->rho, s->q3d[2]);
+  k_fallout_g(g, s->rho, s->q3d[2], vr);
+  geterain_g(g, dt, c.cpl, K.lv1, &qbudget[6], dum1, dum3, s->q3d[2], vr);
+  fallout_g(g, dt, &qbudget[5], s->rain, s->prate, dum3, s->rho, s->q3d[2], vr);
+  kessler_g(g, dt, &qbudget[2], &qbudget[3], &qbudget[4], dum1, s->rho, dum3, s->pp3d, s->th3d, s->prs, s->q3d[0],
+            s->q3d[1], s->q3d[2]);
+  int bad = satadj_g(g, dt, &qbudget[0], &qbudget[1], s->rho, dum3, s->pp3d, s->prs, s->th3d, s->q3d);
+  free(buf);
+  if (bad) { snprintf(g_err, sizeof g_err, "satadj: convergence cannot be reached"); return -4; }
+  return 0;
+}
+
+/* mp_driver alone (ptype=1), with the budgets it adds to */
+int oracle_mp_driver(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_state_t *state, float dt,
+                     double qbudget[7], double asq[3]) {
+  OG G, *g = &G;
+  if (og_setup(g, cfg, gr) || check_cfg(cfg) || cfg->ptype != 1) return -1;
+  St s; st_view(g, state, &s);
+  return mp_kessler_g(g, &s, dt, qbudget, asq);
+}
+
+/* One time step as cm1.F runs it: solve2 (3357), pdefq for ptype=0 (3414)
+ * or mp_driver for ptype=1 (3421-3431), solve3 (3432). */
 int oracle_step(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_state_t *state, int nstep, float dt,
                 double mtime, double mass1, double *mass2, float *cflmax) {
   int rc = oracle_solve2(cfg, gr, state, nstep, dt, mtime, mass1, mass2, cflmax);
   if (rc) return rc;
-  if (cfg->imoist) {
+  if (cfg->imoist && cfg->ptype == 1) {   /* cm1.F:3421-3431: mp_driver */
+    double qb[7] = {0, 0, 0, 0, 0, 0, 0}, asq[3] = {0, 0, 0};
+    rc = oracle_mp_driver(cfg, gr, state, dt, qb, asq);
+    if (rc) return rc;
+  } else if (cfg->imoist) {
     double asq = 0.0;
     long n = (long)(cfg->ni + 2 * cfg->ngxy) * (cfg->nj + 2 * cfg->ngxy) * (cfg->nk + 2);
     rc = oracle_pdefq(cfg, gr, 0.0f, &asq, RPC(state->rho), RP(state->q3d) + (long)(cfg->nqv - 1) * n);

@@ -55,6 +55,7 @@ def lib():
         L.oracle_tendency_init.argtypes = [cfgp, grp, C.c_int, C.c_float] + [P] * 16
         L.oracle_calcener.argtypes = [cfgp, grp] + [P] * 11 + [C.POINTER(C.c_double)]
         L.oracle_threads.restype = C.c_int
+        L.oracle_mp_driver.argtypes = [cfgp, grp, stp, C.c_float, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.oracle_statpack.argtypes = ([cfgp, grp, C.POINTER(StatOpts), C.c_double, C.c_float] + [P] * 10 +
                                       [C.POINTER(C.c_double)] * 3 + [P, C.POINTER(C.c_int)])
         _lib = L
@@ -155,3 +156,16 @@ def statpack(case, opts, st, mtime=0.0, prate=None, qbudget=None, asq=None, bsq=
     if rc != 0:
         raise RuntimeError("oracle statpack failed")
     return out[:n.value].copy()
+
+
+def mp_driver(case, st, dt=None):
+    """The Kessler branch of mp_driver on state dict `st` in place; returns
+    (qbudget(1..7), asq(1..3)) of this call."""
+    L = lib()
+    s = case.state_struct(st)
+    g = case.grid_struct()
+    qb, asq = (C.c_double * 7)(), (C.c_double * 3)()
+    rc = L.oracle_mp_driver(C.byref(case.cfg), C.byref(g), C.byref(s), case.dt if dt is None else dt, qb, asq)
+    if rc != 0:
+        raise RuntimeError("oracle mp_driver failed: %s" % L.oracle_last_error().decode())
+    return list(qb), list(asq)
