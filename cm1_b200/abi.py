@@ -82,6 +82,12 @@ class StatOpts(C.Structure):
                  ("budname", C.c_char_p)])
 
 
+class Restart(C.Structure):
+    """cm1g_restart_t: scalars of a restart file."""
+    _fields_ = [("nstep", C.c_int32), ("mtime", C.c_double), ("dt", C.c_float), ("dtlast", C.c_float),
+                ("mass1", C.c_double)]
+
+
 class State(C.Structure):
     """cm1g_state_t: prognostic state and pre-RK tendencies."""
     _fields_ = [(n, _P) for n in STATE_FIELDS]

@@ -10,7 +10,7 @@ import os
 
 import numpy as np
 
-from .abi import Config, Grid, State, StatOpts, Tune, STATE_FIELDS, fptr, CM1G_OK
+from .abi import Config, Grid, Restart, State, StatOpts, Tune, STATE_FIELDS, fptr, CM1G_OK
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libcm1g.so")
@@ -49,6 +49,12 @@ def lib():
     L.cm1g_step.argtypes = L.cm1g_solve2.argtypes + [C.c_int32]
     L.cm1g_solve3.argtypes = [ctxp, stp]
     L.cm1g_mp_driver.argtypes = [ctxp, C.c_float, stp]
+    i32p = C.POINTER(C.c_int32)
+    L.cm1g_records_size.argtypes = [ctxp, C.c_int32, i32p, i32p, i32p, C.POINTER(C.c_int64)]
+    L.cm1g_pack_records.argtypes = [ctxp, C.c_int32, C.POINTER(_P), i32p, i32p, i32p, _P]
+    L.cm1g_unpack_records.argtypes = [ctxp, C.c_int32, C.POINTER(_P), i32p, i32p, i32p, _P]
+    L.cm1g_restart_write.argtypes = [ctxp, C.c_char_p, C.POINTER(Restart), stp]
+    L.cm1g_restart_read.argtypes = [ctxp, C.c_char_p, C.POINTER(Restart), stp]
     L.cm1g_mp_budget.argtypes = [ctxp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int32]
     L.cm1g_pdefq.argtypes = [ctxp, C.c_float, C.POINTER(C.c_double), _P, _P]
     for n in ("cm1g_bcs", "cm1g_bcp", "cm1g_bcu", "cm1g_bcv"):
@@ -176,6 +182,44 @@ class Context:
             check(L.cm1g_step(self.h, nstep, dt, mtime, mass1, C.byref(m2), C.byref(cfl), C.byref(s),
                               1 if use_graph else 0))
         return m2.value, cfl.value
+
+    @staticmethod
+    def _rec_args(fields, stag, k1, k2):
+        n = len(fields)
+        a32 = lambda v: (C.c_int32 * n)(*v)
+        return n, (_P * n)(*[ptr(f) for f in fields]), a32(stag), a32(k1), a32(k2)
+
+    def records_size(self, stag, k1, k2):
+        n = len(stag)
+        out = C.c_int64()
+        check(lib().cm1g_records_size(self.h, n, (C.c_int32 * n)(*stag), (C.c_int32 * n)(*k1), (C.c_int32 * n)(*k2),
+                                      C.byref(out)))
+        return out.value
+
+    def pack_records(self, fields, stag, k1, k2, out=None):
+        """cm1g_pack_records: the fields' records (level by level, i fastest) as
+        one float32 array (numpy unless `out` is given)."""
+        n, fp, s, a, b = self._rec_args(fields, stag, k1, k2)
+        if out is None:
+            out = np.zeros(self.records_size(stag, k1, k2), np.float32)
+        check(lib().cm1g_pack_records(self.h, n, fp, s, a, b, ptr(out)))
+        return out
+
+    def unpack_records(self, fields, stag, k1, k2, buf):
+        n, fp, s, a, b = self._rec_args(fields, stag, k1, k2)
+        check(lib().cm1g_unpack_records(self.h, n, fp, s, a, b, ptr(buf)))
+
+    def restart_write(self, path, state, nstep=0, mtime=0.0, dt=0.0, dtlast=0.0, mass1=0.0):
+        s = state if isinstance(state, State) else self.state_struct(state)
+        h = Restart(nstep, mtime, dt, dtlast, mass1)
+        check(lib().cm1g_restart_write(self.h, str(path).encode(), C.byref(h), C.byref(s)))
+
+    def restart_read(self, path, state):
+        """cm1g_restart_read into `state`; returns the header as a dict."""
+        s = state if isinstance(state, State) else self.state_struct(state)
+        h = Restart()
+        check(lib().cm1g_restart_read(self.h, str(path).encode(), C.byref(h), C.byref(s)))
+        return {n: getattr(h, n) for n, _ in Restart._fields_}
 
     def mp_driver(self, state, dt):
         """cm1g_mp_driver: the Kessler branch of mp_driver on `state` (ptype=1)."""

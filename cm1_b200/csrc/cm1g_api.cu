@@ -30,6 +30,9 @@ void launch_closure_faces(int ni, int nj, int nk, int ngxy, int dir, const float
 int mlp_param_count();
 int ener_chunks(const DGrid &g);
 void launch_recip_rho(const DGrid &g, const float *rho, float *rr, cudaStream_t st, int64_t *nl);
+long record_count(const DGrid &g, int stag, int k1, int k2);
+void launch_pack_records(const DGrid &g, const float *a, int stag, int k1, int k2, float *out, bool unpack,
+                         cudaStream_t st, int64_t *nl);
 void launch_calcener(const DGrid &g, const EnerIn &e, double *part, double *out, cudaStream_t st, int64_t *nl);
 void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w, const float *uten1,
                          const float *vten1, const float *wten1, float *uten, float *vten, float *wten,
@@ -1842,6 +1845,272 @@ extern "C" int cm1g_stat_write(const char *path, int32_t nrec, const float *rsta
   int ok = fseek(fp, off, SEEK_SET) == 0 && fwrite(rstat, sizeof(float), (size_t)nstat, fp) == (size_t)nstat;
   ok = (fclose(fp) == 0) && ok;
   return ok ? CM1G_OK : set_err(CM1G_ERR_ARG, "write to %s failed", path);
+}
+
+// ---------------------------------------------------------------------
+// Records of output and restart files (k_io.cu) and the restart of the
+// state this library advances.
+// ---------------------------------------------------------------------
+extern "C" int cm1g_records_size(cm1g_ctx_t *c, int32_t n, const int32_t *stag, const int32_t *k1, const int32_t *k2,
+                                 int64_t *nvals) {
+  if (!c || !stag || !k1 || !k2 || !nvals || n < 0) return set_err(CM1G_ERR_ARG, "bad argument");
+  int64_t tot = 0;
+  for (int f = 0; f < n; f++) {
+    if (stag[f] < 1 || stag[f] > 4) return set_err(CM1G_ERR_ARG, "field %d: stag must be 1..4", f);
+    const int kmax = c->g.nk + 1 + (stag[f] == 4);
+    if (k1[f] < 0 || k2[f] > kmax || k2[f] < k1[f]) return set_err(CM1G_ERR_ARG, "field %d: levels out of range", f);
+    tot += record_count(c->g, stag[f], k1[f], k2[f]);
+  }
+  *nvals = tot;
+  return CM1G_OK;
+}
+
+// elements of a field up to level k2 (a 2-D array is levels 0..0)
+static size_t field_elems(const DGrid &g, int stag, int k2) {
+  const size_t plane = stag == 2 ? (size_t)(g.NI + 1) * g.NJ : stag == 3 ? (size_t)g.NI * (g.NJ + 1)
+                                                                         : (size_t)g.NI * g.NJ;
+  return plane * (size_t)(k2 + 1);
+}
+
+static int records_common(cm1g_ctx_t *c, int32_t n, float *const *fields, const int32_t *stag, const int32_t *k1,
+                          const int32_t *k2, float *buf, bool unpack) {
+  if (!c || !fields || !buf) return set_err(CM1G_ERR_ARG, "null argument");
+  int64_t tot = 0;
+  int rc = cm1g_records_size(c, n, stag, k1, k2, &tot);
+  if (rc) return rc;
+  for (int f = 0; f < n; f++) if (!fields[f]) return set_err(CM1G_ERR_ARG, "field %d is NULL", f);
+  ProfActive pa(c);
+  Stager S(c);
+  float *dbuf = S.in(buf, (size_t)tot, !unpack);
+  if (!dbuf) return set_err(CM1G_ERR_NOMEM, "staging alloc");
+  int64_t off = 0;
+  for (int f = 0; f < n; f++) {
+    float *d = S.in(fields[f], field_elems(c->g, stag[f], k2[f]), unpack);
+    if (!d) return set_err(CM1G_ERR_NOMEM, "staging alloc");
+    launch_pack_records(c->g, d, stag[f], k1[f], k2[f], dbuf + off, unpack, c->stream, &c->nlaunch);
+    off += record_count(c->g, stag[f], k1[f], k2[f]);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
+  return S.finish();
+}
+
+extern "C" int cm1g_pack_records(cm1g_ctx_t *c, int32_t n, const float *const *fields, const int32_t *stag,
+                                 const int32_t *k1, const int32_t *k2, float *out) {
+  return records_common(c, n, const_cast<float *const *>(fields), stag, k1, k2, out, false);
+}
+
+extern "C" int cm1g_unpack_records(cm1g_ctx_t *c, int32_t n, float *const *fields, const int32_t *stag,
+                                   const int32_t *k1, const int32_t *k2, const float *in) {
+  return records_common(c, n, fields, stag, k1, k2, const_cast<float *>(in), true);
+}
+
+namespace {
+struct RField { std::string name; float *a; int stag, k1, k2; };
+const char kRstMagic[8] = {'C', 'M', '1', 'G', 'R', 'S', 'T', '1'};
+
+// restart_write's order of the fields this library advances
+// (restart_write.F:692-839): rain, rho, prs, ua, va, wa, ppi, tha, ppx,
+// the q arrays, the tracers; the radiative boundary speeds follow
+std::vector<RField> restart_fields(cm1g_ctx *c, const cm1g_state_t *d) {
+  const DGrid &g = c->g;
+  const cm1g_config_t &cf = c->cfg;
+  const long ns = nS(g);
+  const int nk = g.nk, numq = cf.imoist ? cf.numq : 0, npt = cf.iptra ? cf.npt : 0;
+  std::vector<RField> f;
+  if (cf.ptype == 1) f.push_back({"rain", d->rain, 1, 0, 0});
+  f.push_back({"rho", d->rho, 1, 1, nk});
+  f.push_back({"prs", d->prs, 1, 1, nk});
+  f.push_back({"ua", d->ua, 2, 1, nk});
+  f.push_back({"va", d->va, 3, 1, nk});
+  f.push_back({"wa", d->wa, 4, 1, nk + 1});
+  f.push_back({"ppi", d->ppi, 1, 1, nk});
+  f.push_back({"tha", d->tha, 1, 1, nk});
+  f.push_back({"ppx", d->ppx, 1, 1, nk});
+  for (int q = 0; q < numq; q++) f.push_back({"q" + std::to_string(q + 1), d->qa + q * ns, 1, 1, nk});
+  for (int q = 0; q < npt; q++) f.push_back({"pt" + std::to_string(q + 1), d->pta + q * ns, 1, 1, nk});
+  return f;
+}
+
+template <class T> bool put(FILE *fp, const T &v) { return fwrite(&v, sizeof v, 1, fp) == 1; }
+template <class T> bool get(FILE *fp, T &v) { return fread(&v, sizeof v, 1, fp) == 1; }
+}  // namespace
+
+static int restart_check_state(cm1g_ctx *c, const cm1g_state_t *st) {
+  const cm1g_config_t &cf = c->cfg;
+  const float *req[] = {st->ua, st->va, st->wa, st->ppi, st->tha, st->ppx, st->rho, st->prs,
+                        st->radbcw, st->radbce, st->radbcs, st->radbcn};
+  for (const float *p : req) if (!p) return set_err(CM1G_ERR_ARG, "restart: state array missing");
+  if (cf.imoist && !st->qa) return set_err(CM1G_ERR_ARG, "restart: qa missing");
+  if (cf.iptra && cf.npt > 0 && !st->pta) return set_err(CM1G_ERR_ARG, "restart: pta missing");
+  if (cf.ptype == 1 && !st->rain) return set_err(CM1G_ERR_ARG, "restart: rain missing");
+  return CM1G_OK;
+}
+
+extern "C" int cm1g_restart_write(cm1g_ctx_t *c, const char *path, const cm1g_restart_t *hdr,
+                                  const cm1g_state_t *st) {
+  if (!c || !path || !hdr || !st) return set_err(CM1G_ERR_ARG, "null argument");
+  int rc = restart_check_state(c, st);
+  if (rc) return rc;
+  const DGrid &g = c->g;
+  const cm1g_config_t &cf = c->cfg;
+  const int numq = cf.imoist ? cf.numq : 0, npt = cf.iptra ? cf.npt : 0;
+  ProfActive pa(c);
+  Stager S(c);
+  cm1g_state_t d{};
+  const size_t ns = nS(g), n2 = (size_t)g.NI * g.NJ;
+  d.ua = S.in(st->ua, nU(g), false); d.va = S.in(st->va, nV(g), false); d.wa = S.in(st->wa, nW(g), false);
+  d.ppi = S.in(st->ppi, ns, false); d.tha = S.in(st->tha, ns, false); d.ppx = S.in(st->ppx, ns, false);
+  d.rho = S.in(st->rho, ns, false); d.prs = S.in(st->prs, ns, false);
+  d.qa = numq ? S.in(st->qa, numq * ns, false) : nullptr;
+  d.pta = npt ? S.in(st->pta, npt * ns, false) : nullptr;
+  d.rain = cf.ptype == 1 ? S.in(st->rain, n2, false) : nullptr;
+  std::vector<RField> flds = restart_fields(c, &d);
+  int64_t tot = 0;
+  for (auto &f : flds) tot += record_count(g, f.stag, f.k1, f.k2);
+  float *dbuf = S.dev_buffer((size_t)tot);
+  if (!dbuf || S.err) return set_err(CM1G_ERR_NOMEM, "staging alloc");
+  int64_t off = 0;
+  for (auto &f : flds) {
+    launch_pack_records(g, f.a, f.stag, f.k1, f.k2, dbuf + off, false, c->stream, &c->nlaunch);
+    off += record_count(g, f.stag, f.k1, f.k2);
+  }
+  std::vector<float> h((size_t)tot);
+  CUCHK(cudaMemcpyAsync(h.data(), dbuf, (size_t)tot * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  // radiative boundary speeds: (jb:je,kb:ke) and (ib:ie,kb:ke) arrays, their j (i) = 1..n, k = 1..nk
+  const size_t nrw = (size_t)g.NJ * g.NK, nrs = (size_t)g.NI * g.NK;
+  std::vector<float> rb[4] = {std::vector<float>(nrw), std::vector<float>(nrw), std::vector<float>(nrs),
+                              std::vector<float>(nrs)};
+  const float *rsrc[4] = {st->radbcw, st->radbce, st->radbcs, st->radbcn};
+  for (int s = 0; s < 4; s++)
+    CUCHK(cudaMemcpyAsync(rb[s].data(), rsrc[s], rb[s].size() * sizeof(float), cudaMemcpyDefault, c->stream));
+  rc = S.finish();
+  if (rc) return rc;
+  FILE *fp = fopen(path, "wb");
+  if (!fp) return set_err(CM1G_ERR_ARG, "cannot create %s", path);
+  bool ok = fwrite(kRstMagic, 1, 8, fp) == 8;
+  const int32_t ver = 1, nf = (int32_t)flds.size() + 4;
+  const int32_t dims[8] = {g.ni, g.nj, g.nk, g.ngxy, numq, npt, cf.ptype, nf};
+  ok = ok && put(fp, ver) && fwrite(dims, sizeof(int32_t), 8, fp) == 8;
+  ok = ok && put(fp, hdr->nstep) && put(fp, (int32_t)0) && put(fp, hdr->mtime) && put(fp, hdr->dt) &&
+       put(fp, hdr->dtlast) && put(fp, hdr->mass1);
+  auto put_desc = [&](const std::string &name, int stag, int k1, int k2) {
+    char nm[8] = {0};
+    memcpy(nm, name.c_str(), std::min<size_t>(8, name.size()));
+    const int32_t v[4] = {stag, k1, k2, 0};
+    return fwrite(nm, 1, 8, fp) == 8 && fwrite(v, sizeof(int32_t), 4, fp) == 4;
+  };
+  for (auto &f : flds) ok = ok && put_desc(f.name, f.stag, f.k1, f.k2);
+  const char *rbn[4] = {"radbcw", "radbce", "radbcs", "radbcn"};
+  for (int s = 0; s < 4; s++) ok = ok && put_desc(rbn[s], 0, 1, g.nk);
+  ok = ok && fwrite(h.data(), sizeof(float), h.size(), fp) == h.size();
+  for (int s = 0; s < 4; s++) {   // writerbcwe / writerbcsn (restart_write.F:2164-2286): per level, j (i) = 1..n
+    const bool we = s < 2;
+    const int n = we ? g.nj : g.ni, L = we ? g.NJ : g.NI, lb = we ? g.jb : g.ib;
+    for (int k = 1; k <= g.nk && ok; k++)
+      ok = fwrite(rb[s].data() + (size_t)k * L + (1 - lb), sizeof(float), (size_t)n, fp) == (size_t)n;
+  }
+  ok = (fclose(fp) == 0) && ok;
+  return ok ? CM1G_OK : set_err(CM1G_ERR_ARG, "write to %s failed", path);
+}
+
+extern "C" int cm1g_restart_read(cm1g_ctx_t *c, const char *path, cm1g_restart_t *hdr, cm1g_state_t *st) {
+  if (!c || !path || !hdr || !st) return set_err(CM1G_ERR_ARG, "null argument");
+  int rc = restart_check_state(c, st);
+  if (rc) return rc;
+  const DGrid &g = c->g;
+  const cm1g_config_t &cf = c->cfg;
+  const int numq = cf.imoist ? cf.numq : 0, npt = cf.iptra ? cf.npt : 0;
+  FILE *fp = fopen(path, "rb");
+  if (!fp) return set_err(CM1G_ERR_ARG, "cannot open %s", path);
+  struct Closer { FILE *f; ~Closer() { fclose(f); } } closer{fp};
+  char magic[8];
+  int32_t ver = 0, dims[8], pad;
+  cm1g_restart_t h{};
+  bool ok = fread(magic, 1, 8, fp) == 8 && memcmp(magic, kRstMagic, 8) == 0 && get(fp, ver) && ver == 1 &&
+            fread(dims, sizeof(int32_t), 8, fp) == 8;
+  if (!ok) return set_err(CM1G_ERR_ARG, "%s is not a restart file of this library", path);
+  if (dims[0] != g.ni || dims[1] != g.nj || dims[2] != g.nk || dims[3] != g.ngxy || dims[4] != numq ||
+      dims[5] != npt || dims[6] != cf.ptype)
+    return set_err(CM1G_ERR_ARG, "restart %s: grid or options differ from the context", path);
+  ok = get(fp, h.nstep) && get(fp, pad) && get(fp, h.mtime) && get(fp, h.dt) && get(fp, h.dtlast) && get(fp, h.mass1);
+  cm1g_state_t d{};
+  ProfActive pa(c);
+  Stager S(c);
+  const size_t ns = nS(g), n2 = (size_t)g.NI * g.NJ;
+  d.ua = S.in(st->ua, nU(g), true); d.va = S.in(st->va, nV(g), true); d.wa = S.in(st->wa, nW(g), true);
+  d.ppi = S.in(st->ppi, ns, true); d.tha = S.in(st->tha, ns, true); d.ppx = S.in(st->ppx, ns, true);
+  d.rho = S.in(st->rho, ns, true); d.prs = S.in(st->prs, ns, true);
+  d.qa = numq ? S.in(st->qa, numq * ns, true) : nullptr;
+  d.pta = npt ? S.in(st->pta, npt * ns, true) : nullptr;
+  d.rain = cf.ptype == 1 ? S.in(st->rain, n2, true) : nullptr;
+  d.u3d = st->u3d ? S.in(st->u3d, nU(g), true) : nullptr;
+  d.v3d = st->v3d ? S.in(st->v3d, nV(g), true) : nullptr;
+  d.w3d = st->w3d ? S.in(st->w3d, nW(g), true) : nullptr;
+  d.pp3d = st->pp3d ? S.in(st->pp3d, ns, true) : nullptr;
+  d.th3d = st->th3d ? S.in(st->th3d, ns, true) : nullptr;
+  d.q3d = (numq && st->q3d) ? S.in(st->q3d, numq * ns, true) : nullptr;
+  d.pt3d = (npt && st->pt3d) ? S.in(st->pt3d, npt * ns, true) : nullptr;
+  std::vector<RField> flds = restart_fields(c, &d);
+  if (dims[7] != (int32_t)flds.size() + 4) return set_err(CM1G_ERR_ARG, "restart %s: field list differs", path);
+  for (size_t q = 0; q < flds.size() + 4 && ok; q++) {
+    char nm[8];
+    int32_t v[4];
+    ok = fread(nm, 1, 8, fp) == 8 && fread(v, sizeof(int32_t), 4, fp) == 4;
+    if (ok && q < flds.size()) {
+      const RField &f = flds[q];
+      if (strncmp(nm, f.name.c_str(), 8) != 0 || v[0] != f.stag || v[1] != f.k1 || v[2] != f.k2)
+        return set_err(CM1G_ERR_ARG, "restart %s: field %zu is not %s", path, q, f.name.c_str());
+    }
+  }
+  int64_t tot = 0;
+  for (auto &f : flds) tot += record_count(g, f.stag, f.k1, f.k2);
+  std::vector<float> hbuf((size_t)tot);
+  ok = ok && fread(hbuf.data(), sizeof(float), hbuf.size(), fp) == hbuf.size();
+  const size_t nrw = (size_t)g.NJ * g.NK, nrs = (size_t)g.NI * g.NK;
+  float *rdst[4] = {st->radbcw, st->radbce, st->radbcs, st->radbcn};
+  std::vector<float> rb[4] = {std::vector<float>(nrw), std::vector<float>(nrw), std::vector<float>(nrs),
+                              std::vector<float>(nrs)};
+  for (int s = 0; s < 4 && ok; s++) {
+    CUCHK(cudaMemcpy(rb[s].data(), rdst[s], rb[s].size() * sizeof(float), cudaMemcpyDefault));
+    const bool we = s < 2;
+    const int n = we ? g.nj : g.ni, L = we ? g.NJ : g.NI, lb = we ? g.jb : g.ib;
+    for (int k = 1; k <= g.nk && ok; k++)
+      ok = fread(rb[s].data() + (size_t)k * L + (1 - lb), sizeof(float), (size_t)n, fp) == (size_t)n;
+  }
+  if (!ok) return set_err(CM1G_ERR_ARG, "restart %s: truncated", path);
+  float *dbuf = S.dev_buffer((size_t)tot);
+  if (!dbuf || S.err) return set_err(CM1G_ERR_NOMEM, "staging alloc");
+  CUCHK(cudaMemcpyAsync(dbuf, hbuf.data(), (size_t)tot * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  int64_t off = 0;
+  for (auto &f : flds) {
+    launch_pack_records(g, f.a, f.stag, f.k1, f.k2, dbuf + off, true, c->stream, &c->nlaunch);
+    off += record_count(g, f.stag, f.k1, f.k2);
+  }
+  for (int s = 0; s < 4; s++)
+    CUCHK(cudaMemcpyAsync(rdst[s], rb[s].data(), rb[s].size() * sizeof(float), cudaMemcpyDefault, c->stream));
+  // halos as the end of a step leaves them (the stage-3 fills of solve2 and
+  // solve3's fills), then the time-t+dt copies equal the time-t arrays
+  {
+    std::vector<float *> arr{d.ua, d.va, d.wa, d.ppi, d.tha, d.rho, d.ppx};
+    std::vector<int> which{3, 4, 5, 2, 1, 2, 2}, flag{0, 0, 1, 0, 0, 0, 0};
+    for (int q = 0; q < numq; q++) { arr.push_back(d.qa + q * ns); which.push_back(1); flag.push_back(0); }
+    for (int q = 0; q < npt; q++) { arr.push_back(d.pta + q * ns); which.push_back(1); flag.push_back(0); }
+    launch_bc_batch(g, arr.data(), which.data(), flag.data(), (int)arr.size(), c->stream, &c->nlaunch);
+  }
+  auto cp = [&](float *dst, const float *src, size_t n) {
+    if (dst && src) cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream);
+  };
+  cp(d.u3d, d.ua, nU(g)); cp(d.v3d, d.va, nV(g)); cp(d.w3d, d.wa, nW(g));
+  cp(d.pp3d, d.ppi, ns); cp(d.th3d, d.tha, ns);
+  if (numq) cp(d.q3d, d.qa, numq * ns);
+  if (npt) cp(d.pt3d, d.pta, npt * ns);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
+  rc = S.finish();
+  if (rc) return rc;
+  *hdr = h;
+  return CM1G_OK;
 }
 
 extern "C" int cm1g_profile(cm1g_ctx_t *c, int32_t enable) {

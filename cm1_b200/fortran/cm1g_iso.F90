@@ -91,6 +91,14 @@ module cm1g_iso
     type(c_ptr)        :: budname
   end type
 
+  ! scalars of a restart file (cm1g_restart_write / cm1g_restart_read)
+  type, bind(C) :: cm1g_restart_t
+    integer(c_int32_t) :: nstep
+    real(c_double)     :: mtime
+    real(c_float)      :: dt, dtlast
+    real(c_double)     :: mass1
+  end type
+
   interface
     integer(c_int) function cm1g_init(cfg, grid, ctx) bind(C, name="cm1g_init")
       import :: c_int, c_ptr, cm1g_config_t, cm1g_grid_t
@@ -199,6 +207,42 @@ module cm1g_iso
     end function
     type(c_ptr) function cm1g_last_error() bind(C, name="cm1g_last_error")
       import :: c_ptr
+    end function
+    ! mp_driver's Kessler branch alone (ptype=1) and its FP64 budgets
+    integer(c_int) function cm1g_mp_driver(ctx, dt, st) bind(C, name="cm1g_mp_driver")
+      import :: c_int, c_float, c_ptr, cm1g_state_t
+      type(c_ptr), value :: ctx
+      real(c_float), value :: dt
+      type(cm1g_state_t), intent(inout) :: st
+    end function
+    integer(c_int) function cm1g_mp_budget(ctx, qbudget, asq, reset) bind(C, name="cm1g_mp_budget")
+      import :: c_int, c_int32_t, c_double, c_ptr
+      type(c_ptr), value :: ctx
+      real(c_double), intent(out) :: qbudget(7), asq(3)
+      integer(c_int32_t), value :: reset
+    end function
+    ! records of output files (level by level, i fastest) and restart files
+    integer(c_int) function cm1g_pack_records(ctx, n, fields, stag, k1, k2, out) bind(C, name="cm1g_pack_records")
+      import :: c_int, c_int32_t, c_float, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: n
+      type(c_ptr), intent(in) :: fields(*)
+      integer(c_int32_t), intent(in) :: stag(*), k1(*), k2(*)
+      real(c_float), intent(out) :: out(*)
+    end function
+    integer(c_int) function cm1g_restart_write(ctx, path, hdr, st) bind(C, name="cm1g_restart_write")
+      import :: c_int, c_char, c_ptr, cm1g_restart_t, cm1g_state_t
+      type(c_ptr), value :: ctx
+      character(kind=c_char), intent(in) :: path(*)
+      type(cm1g_restart_t), intent(in) :: hdr
+      type(cm1g_state_t), intent(in) :: st
+    end function
+    integer(c_int) function cm1g_restart_read(ctx, path, hdr, st) bind(C, name="cm1g_restart_read")
+      import :: c_int, c_char, c_ptr, cm1g_restart_t, cm1g_state_t
+      type(c_ptr), value :: ctx
+      character(kind=c_char), intent(in) :: path(*)
+      type(cm1g_restart_t), intent(out) :: hdr
+      type(cm1g_state_t), intent(inout) :: st
     end function
     ! statpack (statpack.F:10-658): set-up once, then one call per statfrq
     integer(c_int) function cm1g_stat_setup(ctx, opts, stat_out) bind(C, name="cm1g_stat_setup")

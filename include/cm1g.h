@@ -314,6 +314,40 @@ int cm1g_statpack(cm1g_ctx_t *ctx, double mtime, float dt, const float *ua, cons
  * statpack.F:620-632). */
 int cm1g_stat_write(const char *path, int32_t nrec, const float *rstat, int32_t nstat);
 
+/* Records of output files: field n's physical points as one record per
+ * level k1[n]..k2[n], i fastest then j (the GrADS layout of writeout with
+ * output_format=1, writeout.F:8901-8995, and the records of restart_write's
+ * writer, restart_write.F:2422-2714), the fields one after another.  stag: 1
+ * s (a 2-D (ib:ie,jb:je) array is an s-array with k1 = k2 = 0), 2 u, 3 v,
+ * 4 w.  The fields leave the device in one gather and one copy; fields and
+ * the buffer may be host or device arrays.  cm1g_records_size gives the
+ * buffer's length in floats; cm1g_unpack_records is the inverse. */
+int cm1g_records_size(cm1g_ctx_t *ctx, int32_t n, const int32_t *stag, const int32_t *k1, const int32_t *k2,
+                      int64_t *nvals);
+int cm1g_pack_records(cm1g_ctx_t *ctx, int32_t n, const float *const *fields, const int32_t *stag,
+                      const int32_t *k1, const int32_t *k2, float *out);
+int cm1g_unpack_records(cm1g_ctx_t *ctx, int32_t n, float *const *fields, const int32_t *stag,
+                        const int32_t *k1, const int32_t *k2, const float *in);
+
+/* Restart of the state the library advances: the dynamical-core part of
+ * restart_write / restart_read (restart_write.F:10-2850, restart_read.F).
+ * The file holds a header (grid, options, nstep, mtime, dt, dtlast, mass1),
+ * a field table, then the fields' records in restart_write's order (rain
+ * when ptype=1, rho, prs, ua, va, wa, ppi, tha, ppx, each q, each tracer) and
+ * the radiative boundary speeds radbcw/e/s/n per level.  Reading checks the
+ * grid and options against the context, fills the halos as the end of a
+ * step leaves them and sets u3d, v3d, w3d, pp3d, th3d, q3d, pt3d (when
+ * given) equal to the time-t arrays, so that stepping on resumes bit for bit.
+ * The tendencies of solve1 and the diagnostics (prate) are not part of it. */
+typedef struct cm1g_restart {
+  int32_t nstep;
+  double mtime;
+  float dt, dtlast;
+  double mass1;
+} cm1g_restart_t;
+int cm1g_restart_write(cm1g_ctx_t *ctx, const char *path, const cm1g_restart_t *hdr, const cm1g_state_t *st);
+int cm1g_restart_read(cm1g_ctx_t *ctx, const char *path, cm1g_restart_t *hdr, cm1g_state_t *st);
+
 /* Per-kernel device timing, the counterpart of the reference's timestats
  * (src/input.F:359-387, cm1.F:4597-4689).  While enabled, every kernel launch
  * is bracketed by CUDA events (graph replay is bypassed); entries are read
