@@ -18,6 +18,7 @@
 #include "cm1g_common.cuh"
 #include "k_stat.cuh"
 #include "k_micro.cuh"
+#include "k_diff2.cuh"
 #include "../../include/cm1g.h"
 
 namespace cm1g {
@@ -197,6 +198,7 @@ struct cm1g_ctx {
   double *mp_part = nullptr, *mp_colbud = nullptr;
   double *mp_qbud = nullptr;                  // qbudget(1..7) and asq(1..3), accumulated on the device
   int *mp_err = nullptr;
+  float *d2s = nullptr;                       // scratch of the 2nd-order diffusion (cm1g_diff2)
 };
 
 // Makes the context's profile (if any) the active one for the calling thread.
@@ -2111,6 +2113,56 @@ extern "C" int cm1g_restart_read(cm1g_ctx_t *c, const char *path, cm1g_restart_t
   if (rc) return rc;
   *hdr = h;
   return CM1G_OK;
+}
+
+extern "C" int cm1g_diff2(cm1g_ctx_t *c, float kdiff2, int32_t idiff, int32_t bbc, int32_t tbc, const float cgs[3],
+                          const float cgt[3], const float *ua, const float *va, const float *wa, const float *rho,
+                          const float *tha, const float *qa, const float *pta, float *uten1, float *vten1,
+                          float *wten1, float *thten1, float *qten, float *ptten) {
+  if (!c || !cgs || !cgt || !ua || !va || !wa || !rho) return set_err(CM1G_ERR_ARG, "null argument");
+  if (idiff < 1) return CM1G_OK;                       // solve1.F:689: nothing to add
+  if (!(kdiff2 >= 0.0f)) return set_err(CM1G_ERR_ARG, "kdiff2 must be >= 0");
+  if ((bbc != 1 && bbc != 2) || (tbc != 1 && tbc != 2))
+    return set_err(CM1G_ERR_UNSUPPORTED, "diff2: bbc/tbc 1 (free slip) or 2 (no slip) only (bbc=3 needs the surface layer)");
+  if (!uten1 || !vten1 || !wten1) return set_err(CM1G_ERR_ARG, "uten1/vten1/wten1 missing");
+  const DGrid &g = c->g;
+  const cm1g_config_t &cf = c->cfg;
+  const int numq = cf.imoist ? cf.numq : 0, npt = cf.iptra ? cf.npt : 0;
+  const bool scal = idiff == 1;
+  if (scal && (!tha || !thten1 || (numq && (!qa || !qten)) || (npt && (!pta || !ptten))))
+    return set_err(CM1G_ERR_ARG, "diff2 with idiff=1 needs tha/thten1, qa/qten, pta/ptten");
+  if (!c->d2s) {
+    const size_t bS = nS(g) * sizeof(float), bW = nW(g) * sizeof(float);
+    c->d2s = (float *)dalloc(c, 6 * bS + 3 * bW);
+    if (!c->d2s) return set_err(CM1G_ERR_NOMEM, "diff2 scratch");
+  }
+  ProfActive pa(c);
+  Stager S(c);
+  const size_t ns = nS(g);
+  Diff2Args a{};
+  a.kdiff2 = kdiff2; a.bbc = bbc; a.tbc = tbc; a.momentum = 1;
+  a.cgs1 = cgs[0]; a.cgs2 = cgs[1]; a.cgs3 = cgs[2]; a.cgt1 = cgt[0]; a.cgt2 = cgt[1]; a.cgt3 = cgt[2];
+  a.ua = S.in(ua, nU(g), false); a.va = S.in(va, nV(g), false); a.wa = S.in(wa, nW(g), false);
+  a.rho = S.in(rho, ns, false);
+  a.uten = S.in(uten1, nU(g), true); a.vten = S.in(vten1, nV(g), true); a.wten = S.in(wten1, nW(g), true);
+  float *p = c->d2s;
+  a.rr = p; p += ns; a.divx = p; p += ns; a.t11 = p; p += ns; a.t22 = p; p += ns; a.t33 = p; p += ns;
+  a.t12 = p; p += ns; a.rf = p; p += nW(g); a.t13 = p; p += nW(g); a.t23 = p;
+  a.nsc = 0;
+  if (scal) {   // solve1.F:706-733: theta, every q, every tracer
+    a.s[a.nsc] = S.in(tha, ns, false); a.sten[a.nsc++] = S.in(thten1, ns, true);
+    const float *dq = numq ? S.in(qa, numq * ns, false) : nullptr;
+    float *dqt = numq ? S.in(qten, numq * ns, true) : nullptr;
+    for (int n = 0; n < numq; n++) { a.s[a.nsc] = dq + n * ns; a.sten[a.nsc++] = dqt + n * ns; }
+    const float *dp = npt ? S.in(pta, npt * ns, false) : nullptr;
+    float *dpt = npt ? S.in(ptten, npt * ns, true) : nullptr;
+    for (int n = 0; n < npt; n++) { a.s[a.nsc] = dp + n * ns; a.sten[a.nsc++] = dpt + n * ns; }
+  }
+  if (S.err) return set_err(CM1G_ERR_NOMEM, "staging alloc");
+  launch_diff2(g, a, c->stream, &c->nlaunch);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
+  return S.finish();
 }
 
 extern "C" int cm1g_profile(cm1g_ctx_t *c, int32_t enable) {

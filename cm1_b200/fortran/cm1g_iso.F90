@@ -208,6 +208,16 @@ module cm1g_iso
     type(c_ptr) function cm1g_last_error() bind(C, name="cm1g_last_error")
       import :: c_ptr
     end function
+    ! 2nd-order diffusion: diff2def + diff2u/v/w/s of solve1 (difforder=2)
+    integer(c_int) function cm1g_diff2(ctx, kdiff2, idiff, bbc, tbc, cgs, cgt, ua, va, wa, rho, tha, qa, pta, &
+                                       uten1, vten1, wten1, thten1, qten, ptten) bind(C, name="cm1g_diff2")
+      import :: c_int, c_int32_t, c_float, c_ptr
+      type(c_ptr), value :: ctx
+      real(c_float), value :: kdiff2
+      integer(c_int32_t), value :: idiff, bbc, tbc
+      real(c_float), intent(in) :: cgs(3), cgt(3)
+      type(c_ptr), value :: ua, va, wa, rho, tha, qa, pta, uten1, vten1, wten1, thten1, qten, ptten
+    end function
     ! mp_driver's Kessler branch alone (ptype=1) and its FP64 budgets
     integer(c_int) function cm1g_mp_driver(ctx, dt, st) bind(C, name="cm1g_mp_driver")
       import :: c_int, c_float, c_ptr, cm1g_state_t

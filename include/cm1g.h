@@ -257,6 +257,21 @@ int cm1g_tendency_init(cm1g_ctx_t *ctx, int32_t irdamp, float rdalpha, const flo
                        const float *ua, const float *va, const float *wa, const float *tha,
                        float *uten1, float *vten1, float *wten1, float *thten1, float *qten, float *ptten);
 
+/* 2nd-order diffusion with a fixed viscosity kdiff2 (difforder=2): the
+ * stress tensor of diff2def (src/diff2.F:743-1221) and the tendencies of
+ * diff2u/v/w (idiff >= 1) and diff2s for theta, each q and each tracer
+ * (idiff = 1), added to uten1 ... ptten as solve1 does (solve1.F:686-734),
+ * with rr = 1/rho and the w-level density rf of solve3.F:660-678 (cgs and cgt
+ * the extrapolation weights of rf to the bottom and top w-levels,
+ * param.F:9038-9060).  Cartesian grid, no terrain; bbc and tbc 1 (free slip)
+ * or 2 (no slip); lateral walls wbc..nbc = 3 (free slip) or 4 (no slip) are
+ * honoured.  ua/va/wa are the velocities diff2def is given (u3d, v3d, w3d
+ * after solve3); rho, tha, qa, pta need filled halos. */
+int cm1g_diff2(cm1g_ctx_t *ctx, float kdiff2, int32_t idiff, int32_t bbc, int32_t tbc, const float cgs[3],
+               const float cgt[3], const float *ua, const float *va, const float *wa, const float *rho,
+               const float *tha, const float *qa, const float *pta, float *uten1, float *vten1, float *wten1,
+               float *thten1, float *qten, float *ptten);
+
 /* Domain extrema over the physical cells of an s/u/v/w array: replaces
  * maxmin (src/maxmin.F:5-119).  stag: 1 s, 2 u, 3 v, 4 w.  loc receives
  * 1-based (i,j,k) of the max (loc[0..2]) and of the min (loc[3..5]). */

@@ -1774,6 +1774,166 @@ int oracle_pdefq(const cm1g_config_t *cfg, const cm1g_grid_t *gr, float rmax, do
 }
 
 /* ------------------------------------------------------------------ */
+/* 2nd-order diffusion (difforder=2): diff2def + diff2u/v/w/s          */
+/* ------------------------------------------------------------------ */
+
+/* rr, rf (solve3.F:660-678), divx and the stress tensor (diff2.F:743-989),
+ * then the tendencies (diff2.F:11-735), in solve1's order (solve1.F:686-734) */
+int oracle_diff2(const cm1g_config_t *cfg, const cm1g_grid_t *gr, float kdiff2, int idiff, int bbc, int tbc,
+                 const float *cgs, const float *cgt, const float *ua_, const float *va_, const float *wa_,
+                 const float *rho_, const float *tha_, const float *qa_, const float *pta_, float *uten_,
+                 float *vten_, float *wten_, float *thten_, float *qten_, float *ptten_) {
+  OG G, *g = &G;
+  if (og_setup(g, cfg, gr)) return -1;
+  if (idiff < 1) return 0;
+  const int ni = g->ni, nj = g->nj, nk = g->nk;
+  const long ns = nS(g);
+  F3 ua = mkU(g, ua_), va = mkV(g, va_), wa = mkW(g, wa_), rho = mkS(g, rho_);
+  F3 uten = mkU(g, uten_), vten = mkV(g, vten_), wten = mkW(g, wten_);
+  float *buf = (float *)calloc((size_t)(6 * ns + 3 * nW(g)), sizeof(float));
+  if (!buf) return -3;
+  float *p = buf;
+  F3 rr = mkS(g, p); p += ns;
+  F3 divx = mkS(g, p); p += ns;
+  F3 t11 = mkS(g, p); p += ns;
+  F3 t22 = mkS(g, p); p += ns;
+  F3 t33 = mkS(g, p); p += ns;
+  F3 t12 = mkS(g, p); p += ns;
+  F3 rf = mkW(g, p); p += nW(g);
+  F3 t13 = mkW(g, p); p += nW(g);
+  F3 t23 = mkW(g, p);
+  const float coef = kdiff2, twdth = 2.0f / 3.0f;
+  const float rdx = g->rdx, rdy = g->rdy, rdz = g->rdz;
+  const int wbc = cfg->wbc, ebc = cfg->ebc, sbc = cfg->sbc, nbc = cfg->nbc;
+  /* solve3.F:660-678 */
+  for (int k = 2; k <= nk; k++) for (int j = 0; j <= nj + 1; j++) for (int i = 0; i <= ni + 1; i++) {
+    A3(rr, i, j, k) = 1.0f / A3(rho, i, j, k);
+    A3(rf, i, j, k) = (A3(g->c1, i, j, k) * A3(rho, i, j, k - 1) + A3(g->c2, i, j, k) * A3(rho, i, j, k));
+  }
+  for (int j = 0; j <= nj + 1; j++) for (int i = 0; i <= ni + 1; i++) {
+    A3(rr, i, j, 1) = 1.0f / A3(rho, i, j, 1);
+    A3(rf, i, j, 1) = cgs[0] * A3(rho, i, j, 1) + cgs[1] * A3(rho, i, j, 2) + cgs[2] * A3(rho, i, j, 3);
+    A3(rf, i, j, nk + 1) = cgt[0] * A3(rho, i, j, nk) + cgt[1] * A3(rho, i, j, nk - 1) + cgt[2] * A3(rho, i, j, nk - 2);
+  }
+  /* diff2def (Cartesian) */
+  for (int k = 1; k <= nk; k++) {
+    for (int j = 0; j <= nj + 1; j++) for (int i = 0; i <= ni + 1; i++) {
+      float d = (A3(ua, i + 1, j, k) - A3(ua, i, j, k)) * rdx * UH(i) + (A3(va, i, j + 1, k) - A3(va, i, j, k)) * rdy * VH(j) +
+                (A3(wa, i, j, k + 1) - A3(wa, i, j, k)) * rdz * A3(g->mh, 1, 1, k);
+      if (fabsf(d) < cfg->smeps) d = 0.0f;
+      A3(divx, i, j, k) = d;
+    }
+    for (int j = 0; j <= nj + 1; j++) for (int i = 0; i <= ni + 1; i++) {
+      A3(t11, i, j, k) = coef * A3(rho, i, j, k) * (A3(ua, i + 1, j, k) - A3(ua, i, j, k)) * rdx * UH(i);
+      A3(t22, i, j, k) = coef * A3(rho, i, j, k) * (A3(va, i, j + 1, k) - A3(va, i, j, k)) * rdy * VH(j);
+      A3(t33, i, j, k) = coef * A3(rho, i, j, k) * (A3(wa, i, j, k + 1) - A3(wa, i, j, k)) * rdz * A3(g->mh, 1, 1, k);
+      A3(t12, i, j, k) = coef * ((A3(ua, i, j, k) - A3(ua, i, j - 1, k)) * rdy * VF(j) +
+                                 (A3(va, i, j, k) - A3(va, i - 1, j, k)) * rdx * UF(i)) * 0.25f *
+                         ((A3(rho, i - 1, j - 1, k) + A3(rho, i, j, k)) + (A3(rho, i - 1, j, k) + A3(rho, i, j - 1, k)));
+    }
+#define R4(i, j) ((A3(rho, (i) - 1, (j) - 1, k) + A3(rho, i, j, k)) + (A3(rho, (i) - 1, j, k) + A3(rho, i, (j) - 1, k)))
+    if (wbc == 3 && g->ibw) { for (int j = 1; j <= nj + 1; j++) A3(t12, 1, j, k) = A3(t12, 2, j, k); }
+    else if (wbc == 4 && g->ibw) { for (int j = 1; j <= nj + 1; j++) A3(t12, 1, j, k) = coef * 2.0f * A3(va, 1, j, k) * rdx * UF(1) * 0.25f * R4(1, j); }
+    if (ebc == 3 && g->ibe) { for (int j = 1; j <= nj + 1; j++) A3(t12, ni + 1, j, k) = A3(t12, ni, j, k); }
+    else if (ebc == 4 && g->ibe) { for (int j = 1; j <= nj + 1; j++) A3(t12, ni + 1, j, k) = -coef * 2.0f * A3(va, ni, j, k) * rdx * UF(ni + 1) * 0.25f * R4(ni + 1, j); }
+    if (sbc == 3 && g->ibs) { for (int i = 1; i <= ni + 1; i++) A3(t12, i, 1, k) = A3(t12, i, 2, k); }
+    else if (sbc == 4 && g->ibs) { for (int i = 1; i <= ni + 1; i++) A3(t12, i, 1, k) = coef * 2.0f * A3(ua, i, 1, k) * rdy * VF(1) * 0.25f * R4(i, 1); }
+    if (nbc == 3 && g->ibn) { for (int i = 1; i <= ni + 1; i++) A3(t12, i, nj + 1, k) = A3(t12, i, nj, k); }
+    else if (nbc == 4 && g->ibn) { for (int i = 1; i <= ni + 1; i++) A3(t12, i, nj + 1, k) = -coef * 2.0f * A3(ua, i, nj, k) * rdy * VF(nj + 1) * 0.25f * R4(i, nj + 1); }
+#undef R4
+    if (k != 1) {
+      for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni + 1; i++) {
+        A3(t13, i, j, k) = coef * ((A3(ua, i, j, k) - A3(ua, i, j, k - 1)) * rdz * A3(g->mf, 1, 1, k) +
+                                   (A3(wa, i, j, k) - A3(wa, i - 1, j, k)) * rdx * UF(i));
+        A3(t23, i, j, k) = coef * ((A3(va, i, j, k) - A3(va, i, j, k - 1)) * rdz * A3(g->mf, 1, 1, k) +
+                                   (A3(wa, i, j, k) - A3(wa, i, j - 1, k)) * rdy * VF(j));
+      }
+      if (wbc == 3 && g->ibw) { for (int j = 1; j <= nj; j++) A3(t13, 1, j, k) = A3(t13, 2, j, k); }
+      else if (wbc == 4 && g->ibw) { for (int j = 1; j <= nj; j++) A3(t13, 1, j, k) = coef * 2.0f * A3(wa, 1, j, k) * rdx * UF(1); }
+      if (ebc == 3 && g->ibe) { for (int j = 1; j <= nj; j++) A3(t13, ni + 1, j, k) = A3(t13, ni, j, k); }
+      else if (ebc == 4 && g->ibe) { for (int j = 1; j <= nj; j++) A3(t13, ni + 1, j, k) = -coef * 2.0f * A3(wa, ni, j, k) * rdx * UF(ni + 1); }
+      if (sbc == 3 && g->ibs) { for (int i = 1; i <= ni; i++) A3(t23, i, 1, k) = A3(t23, i, 2, k); }
+      else if (sbc == 4 && g->ibs) { for (int i = 1; i <= ni; i++) A3(t23, i, 1, k) = coef * 2.0f * A3(wa, i, 1, k) * rdy * VF(1); }
+      if (nbc == 3 && g->ibn) { for (int i = 1; i <= ni; i++) A3(t23, i, nj + 1, k) = A3(t23, i, nj, k); }
+      else if (nbc == 4 && g->ibn) { for (int i = 1; i <= ni; i++) A3(t23, i, nj + 1, k) = -coef * 2.0f * A3(wa, i, nj, k) * rdy * VF(nj + 1); }
+    }
+  }
+  if (bbc == 1) {
+    for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni + 1; i++) A3(t13, i, j, 1) = A3(t13, i, j, 2);
+    for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni; i++) A3(t23, i, j, 1) = A3(t23, i, j, 2);
+  } else if (bbc == 2) {
+    for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni + 1; i++)
+      A3(t13, i, j, 1) = coef * 2.0f * (A3(ua, i, j, 1) + 0.0f) * rdz * A3(g->mf, 1, 1, 1);
+    for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni; i++)
+      A3(t23, i, j, 1) = coef * 2.0f * (A3(va, i, j, 1) + 0.0f) * rdz * A3(g->mf, 1, 1, 1);
+  }
+  if (tbc == 1) {
+    for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni + 1; i++) A3(t13, i, j, nk + 1) = A3(t13, i, j, nk);
+    for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni; i++) A3(t23, i, j, nk + 1) = A3(t23, i, j, nk);
+  } else if (tbc == 2) {
+    for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni + 1; i++)
+      A3(t13, i, j, nk + 1) = -coef * 2.0f * A3(ua, i, j, nk) * rdz * A3(g->mf, 1, 1, nk + 1);
+    for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni; i++)
+      A3(t23, i, j, nk + 1) = -coef * 2.0f * A3(va, i, j, nk) * rdz * A3(g->mf, 1, 1, nk + 1);
+  }
+  for (int k = 1; k <= nk + 1; k++) for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni + 1; i++) {
+    A3(t13, i, j, k) = A3(t13, i, j, k) * 0.5f * (A3(rf, i - 1, j, k) + A3(rf, i, j, k));
+    A3(t23, i, j, k) = A3(t23, i, j, k) * 0.5f * (A3(rf, i, j - 1, k) + A3(rf, i, j, k));
+  }
+  /* diff2u */
+  for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni + 1; i++) {
+    float d0 = 2.0f * A3(t11, i, j, k) - A3(rho, i, j, k) * twdth * A3(divx, i, j, k);
+    float dm = 2.0f * A3(t11, i - 1, j, k) - A3(rho, i - 1, j, k) * twdth * A3(divx, i - 1, j, k);
+    float fx = (d0 - dm) * rdx * UF(i);
+    float fy = (A3(t12, i, j + 1, k) - A3(t12, i, j, k)) * rdy * VH(j);
+    float fz = (A3(t13, i, j, k + 1) - A3(t13, i, j, k)) * rdz * A3(g->mh, 1, 1, k);
+    A3(uten, i, j, k) = A3(uten, i, j, k) + ((fx + fy) + fz) / (0.5f * (A3(rho, i - 1, j, k) + A3(rho, i, j, k)));
+  }
+  /* diff2v */
+  for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni; i++) {
+    float fx = (A3(t12, i + 1, j, k) - A3(t12, i, j, k)) * rdx * UH(i);
+    float d0 = 2.0f * A3(t22, i, j, k) - A3(rho, i, j, k) * twdth * A3(divx, i, j, k);
+    float dm = 2.0f * A3(t22, i, j - 1, k) - A3(rho, i, j - 1, k) * twdth * A3(divx, i, j - 1, k);
+    float fy = (d0 - dm) * rdy * VF(j);
+    float fz = (A3(t23, i, j, k + 1) - A3(t23, i, j, k)) * rdz * A3(g->mh, 1, 1, k);
+    A3(vten, i, j, k) = A3(vten, i, j, k) + ((fx + fy) + fz) / (0.5f * (A3(rho, i, j - 1, k) + A3(rho, i, j, k)));
+  }
+  /* diff2w */
+  for (int k = 2; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++) {
+    float fx = (A3(t13, i + 1, j, k) - A3(t13, i, j, k)) * rdx * UH(i);
+    float fy = (A3(t23, i, j + 1, k) - A3(t23, i, j, k)) * rdy * VH(j);
+    float d0 = 2.0f * A3(t33, i, j, k) - A3(rho, i, j, k) * twdth * A3(divx, i, j, k);
+    float dm = 2.0f * A3(t33, i, j, k - 1) - A3(rho, i, j, k - 1) * twdth * A3(divx, i, j, k - 1);
+    float fz = (d0 - dm) * rdz * A3(g->mf, 1, 1, k);
+    A3(wten, i, j, k) = A3(wten, i, j, k) + ((fx + fy) + fz) / A3(rf, i, j, k);
+  }
+  /* diff2s: theta, each q, each tracer (idiff = 1) */
+  if (idiff == 1) {
+    int numq = cfg->imoist ? cfg->numq : 0, npt = cfg->iptra ? cfg->npt : 0;
+    int nsc = 1 + numq + npt;
+    for (int n = 0; n < nsc; n++) {
+      const float *sp = n == 0 ? tha_ : n <= numq ? qa_ + (n - 1) * ns : pta_ + (n - 1 - numq) * ns;
+      float *tp = n == 0 ? thten_ : n <= numq ? qten_ + (n - 1) * ns : ptten_ + (n - 1 - numq) * ns;
+      F3 s = mkS(g, sp), sten = mkS(g, tp);
+      for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++) {
+        float dxl = 0.5f * (A3(rho, i, j, k) + A3(rho, i - 1, j, k)) * (A3(s, i, j, k) - A3(s, i - 1, j, k)) * rdx * UF(i);
+        float dxr = 0.5f * (A3(rho, i + 1, j, k) + A3(rho, i, j, k)) * (A3(s, i + 1, j, k) - A3(s, i, j, k)) * rdx * UF(i + 1);
+        float fx = coef * (dxr - dxl) * rdx * UH(i);
+        float dyl = 0.5f * (A3(rho, i, j, k) + A3(rho, i, j - 1, k)) * (A3(s, i, j, k) - A3(s, i, j - 1, k)) * rdy * VF(j);
+        float dyr = 0.5f * (A3(rho, i, j + 1, k) + A3(rho, i, j, k)) * (A3(s, i, j + 1, k) - A3(s, i, j, k)) * rdy * VF(j + 1);
+        float fy = coef * (dyr - dyl) * rdy * VH(j);
+        float dzl = k == 1 ? 0.0f : (A3(s, i, j, k) - A3(s, i, j, k - 1)) * rdz * A3(g->mf, 1, 1, k);
+        float dzu = k == nk ? 0.0f : (A3(s, i, j, k + 1) - A3(s, i, j, k)) * rdz * A3(g->mf, 1, 1, k + 1);
+        float fz = coef * (A3(rf, i, j, k + 1) * dzu - A3(rf, i, j, k) * dzl) * rdz * A3(g->mh, 1, 1, k);
+        A3(sten, i, j, k) = A3(sten, i, j, k) + ((fx + fy) + fz) * A3(rr, i, j, k);
+      }
+    }
+  }
+  free(buf);
+  return 0;
+}
+
+/* ------------------------------------------------------------------ */
 /* Kessler microphysics (ptype=1): mp_driver.F:189-233, kessler.F      */
 /* ------------------------------------------------------------------ */
 
