@@ -4,6 +4,7 @@ reference's cm1/run.py).
 
     python -m cm1_b200.run --workload supercell --steps 10 [--ni 128 --nj 128 --nk 80] [--graph]
                            [--time] [--profile] [--stats N] [--stats-file cm1out_stats.dat]
+                           [--aux N] [--aux-dir DIR]
 
 --time reports the device time per large step (CUDA events around the steps,
 after one untimed step); --profile reports per-kernel device time per step,
@@ -11,7 +12,12 @@ the counterpart of the reference's timestats table.  --stats N runs the statisti
 (cm1g_statpack: every statistic this library builds) after the steps, N+1
 times, and reports the device-resident time per call (CUDA events, the
 first call untimed, rstat copied to the host each call) with the values;
---stats-file appends them as a record of the GrADS stats file.
+--stats-file appends them as a record of the GrADS stats file.  --aux N
+times, after the steps, N calls each of the other entry points of the path
+with device-resident arrays (CUDA events, one untimed call first): the
+2nd-order diffusion (kdiff2 = 75 m2/s), the records of the prognostic fields
+(one gather and one copy to pinned host memory), a restart write and read
+(files under --aux-dir), and for ptype=1 mp_driver.
 """
 import argparse
 import json
@@ -33,6 +39,8 @@ def main(argv=None):
     ap.add_argument("--profile", action="store_true")
     ap.add_argument("--stats", type=int, default=0)
     ap.add_argument("--stats-file")
+    ap.add_argument("--aux", type=int, default=0)
+    ap.add_argument("--aux-dir", default=".")
     args = ap.parse_args(argv)
 
     import torch
@@ -99,9 +107,63 @@ def main(argv=None):
         out["stats"] = {n: float(v) for n, v in zip(names, rstat)}
         if args.stats_file:
             binding.stat_write(args.stats_file, 1, rstat)
+    if args.aux > 0:
+        out["aux"] = _time_aux(ctx, case, dev, args.aux, args.aux_dir)
     print(json.dumps(out))
     ctx.close()
     return 0 if np.isfinite(out["max_w"]) else 1
+
+
+def _time_aux(ctx, case, dev, n, outdir):
+    """Device time per call (ms) of the path's other entry points."""
+    import os
+    import time
+    import torch
+    lay, cfg = case.lay, case.cfg
+    res = {}
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(reps):
+            fn()
+        t1.record()
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1) / reps
+
+    ten = {k: torch.zeros_like(dev[k]) for k in ("uten1", "vten1", "wten1", "thten1", "qten", "ptten")}
+    dz = cfg.dz
+    zs = np.array([0.5, 1.5, 2.5]) * dz
+    w = [float(np.prod([(0.0 - zs[m]) / (zs[l] - zs[m]) for m in range(3) if m != l])) for l in range(3)]
+    qa = dev["qa"] if cfg.imoist else None
+    pta = dev["pta"] if cfg.iptra else None
+    res["diff2_ms"] = timed(lambda: ctx.diff2(75.0, 1, 1, 1, w, w, dev["u3d"], dev["v3d"], dev["w3d"], dev["rho"],
+                                              dev["tha"], qa, pta, ten["uten1"], ten["vten1"], ten["wten1"],
+                                              ten["thten1"], ten["qten"] if qa is not None else None,
+                                              ten["ptten"] if pta is not None else None), n)
+    names = ["rho", "prs", "ua", "va", "wa", "ppi", "tha", "ppx"]
+    stag = [1, 1, 2, 3, 4, 1, 1, 1]
+    fields = [dev[k] for k in names]
+    k2 = [lay.nk, lay.nk, lay.nk, lay.nk, lay.nk + 1, lay.nk, lay.nk, lay.nk]
+    nv = ctx.records_size(stag, [1] * len(stag), k2)
+    host = torch.empty(nv, dtype=torch.float32).pin_memory()
+    res["records_ms"] = timed(lambda: ctx.pack_records(fields, stag, [1] * len(stag), k2, out=host), n)
+    res["records_bytes"] = nv * 4
+    path = os.path.join(outdir, "cm1g_restart.bin")
+    t0 = time.perf_counter()
+    for _ in range(n):
+        ctx.restart_write(path, dev, nstep=1, mtime=case.dt, dt=case.dt, dtlast=case.dt, mass1=case.mass1)
+    res["restart_write_ms_wall"] = (time.perf_counter() - t0) * 1e3 / n
+    res["restart_bytes"] = os.path.getsize(path)
+    t0 = time.perf_counter()
+    for _ in range(n):
+        ctx.restart_read(path, dev)
+    res["restart_read_ms_wall"] = (time.perf_counter() - t0) * 1e3 / n
+    if cfg.ptype == 1:
+        res["mp_driver_ms"] = timed(lambda: ctx.mp_driver(dev, case.dt), n)
+    return res
 
 
 if __name__ == "__main__":
