@@ -2073,8 +2073,12 @@ extern "C" int cm1g_restart_read(cm1g_ctx_t *c, const char *path, cm1g_restart_t
   float *rdst[4] = {st->radbcw, st->radbce, st->radbcs, st->radbcn};
   std::vector<float> rb[4] = {std::vector<float>(nrw), std::vector<float>(nrw), std::vector<float>(nrs),
                               std::vector<float>(nrs)};
+  // the arrays' halo values are kept: fetch them on the context's stream,
+  // after any work already queued there
+  for (int s = 0; s < 4; s++)
+    CUCHK(cudaMemcpyAsync(rb[s].data(), rdst[s], rb[s].size() * sizeof(float), cudaMemcpyDefault, c->stream));
+  CUCHK(cudaStreamSynchronize(c->stream));
   for (int s = 0; s < 4 && ok; s++) {
-    CUCHK(cudaMemcpy(rb[s].data(), rdst[s], rb[s].size() * sizeof(float), cudaMemcpyDefault));
     const bool we = s < 2;
     const int n = we ? g.nj : g.ni, L = we ? g.NJ : g.NI, lb = we ? g.jb : g.ib;
     for (int k = 1; k <= g.nk && ok; k++)

@@ -16,7 +16,8 @@ from cm1_b200.cases import make_case, stat_opts
 
 pytestmark = pytest.mark.gpu
 
-SUMS = {"tmass", "tmois", "massqv", "ek", "ei", "ep", "le", "et", "tmu", "tmv", "tmw", "tmfu", "tmfd"}
+SUMS = {"tmass", "tmois", "massqv", "massqc", "massqr", "ek", "ei", "ep", "le", "et", "tmu", "tmv", "tmw", "tmfu",
+        "tmfd"}
 MATHLIB = {"rhmax", "rhmin", "themax", "themin", "sthemax", "sthemin"}
 PP = {"ppmax", "ppmin"}
 
@@ -116,4 +117,33 @@ def test_statpack_switches_and_errors(cm1g, oracle_lib):
     ctx.stat_setup(o3)
     with pytest.raises(cm1g.CM1GError):
         ctx.statpack(0.0, case.dt, f[0], f[1], None, *f[3:], asq=np.zeros(1), bsq=np.zeros(1), **kw)
+    ctx.close()
+
+
+def test_statpack_with_kessler_liquid(cm1g, oracle_lib):
+    """Statistics of a Kessler state (qv, qc, qr): cloud top and base from qc,
+    the total moisture and the masses of the liquid species, and the energy
+    budget's liquid terms, against the oracle."""
+    torch = _torch()
+    case = make_case("kessler", ni=40, nj=36, nk=44)
+    st = case.copy_state()
+    for _ in range(2):
+        oracle_lib.step(case, st)
+    o, keep = stat_opts(case, qnames=("qv", "qc", "qr"), nql=(2, 3), cloud=(1,), budnames=("tcond", "tevac"))
+    I = case.lay.interior(1)
+    assert st["q3d"][1][I].max() > 1e-5
+    qb = np.array([1.5e6, 2.5e5])
+    asq, bsq = np.array([1.0, 2.0, 3.0]), np.array([-1.0, -2.0, -3.0])
+    ref = oracle_lib.statpack(case, o, st, mtime=6.0, prate=st["prate"], qbudget=qb, asq=asq, bsq=bsq)
+    ctx = cm1g.Context(case.cfg, case.grid)
+    names = ctx.stat_setup(o)
+    for n in ("maxqc", "minqr", "qctop", "qcbot", "tmois", "massqv", "massqc", "massqr", "le", "tcond", "asqr"):
+        assert n in names, n
+    dev = cm1g.to_device(st)
+    f, kw = _args(case, dev)
+    kw["prate"] = dev["prate"]
+    got = ctx.statpack(6.0, case.dt, *f, qbudget=qb, asq=asq, bsq=bsq, **kw)
+    _compare(names, got, ref)
+    v = dict(zip(names, got))
+    assert v["qctop"] > v["qcbot"] > 0.0 and v["le"] != 0.0 and v["pratemax"] > 0.0
     ctx.close()
