@@ -1006,7 +1006,8 @@ extern "C" int cm1g_autotune(cm1g_ctx_t *c, float dt, double mass1, const cm1g_s
       {&d.wa, nw}, {&d.w3d, nw}, {&d.wten1, nw}, {&d.ppi, ns}, {&d.pp3d, ns}, {&d.ppx, ns}, {&d.ppten, ns},
       {&d.tha, ns}, {&d.th3d, ns}, {&d.thten1, ns}, {&d.rho, ns}, {&d.prs, ns}, {&d.qa, nq}, {&d.q3d, nq},
       {&d.qten, nq}, {&d.pta, npt}, {&d.pt3d, npt}, {&d.ptten, npt}, {&d.radbcw, nrw}, {&d.radbce, nrw},
-      {&d.radbcs, nrs}, {&d.radbcn, nrs}};
+      {&d.radbcs, nrs}, {&d.radbcn, nrs},
+      {&d.rain, c->cfg.ptype == 1 ? (size_t)g.NI * g.NJ : 0}, {&d.prate, c->cfg.ptype == 1 ? (size_t)g.NI * g.NJ : 0}};
   std::vector<void *> scratch;
   auto release = [&]() {
     cudaStreamSynchronize(c->stream);

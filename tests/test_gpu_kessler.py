@@ -181,3 +181,19 @@ def test_config_checks(cm1g):
     case.cfg.numq = 2
     with pytest.raises(cm1g.CM1GError):
         cm1g.Context(case.cfg, case.grid)
+
+
+def test_autotune_leaves_the_kessler_state_unchanged(cm1g):
+    """The autotuner times steps on a copy of the state: the caller's arrays,
+    the accumulated rain included, are left as they were."""
+    torch = _torch()
+    case = make_case("kessler", ni=40, nj=36, nk=40)
+    ctx = cm1g.Context(case.cfg, case.grid)
+    dev = cm1g.to_device(case.state)
+    dev["rain"] += 0.5
+    before = {k: v.clone() for k, v in dev.items()}
+    ctx.autotune(dev, case.dt, case.mass1, reps=1)
+    torch.cuda.synchronize()
+    for k in dev:
+        assert torch.equal(dev[k], before[k]), k
+    ctx.close()
