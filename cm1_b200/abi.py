@@ -82,6 +82,16 @@ class StatOpts(C.Structure):
                  ("budname", C.c_char_p)])
 
 
+WRITEOUT_SWITCHES = ["output_rain", "output_prate", "output_th", "output_thpert", "output_prs", "output_prspert",
+                     "output_pi", "output_pipert", "output_rho", "output_rhopert", "output_qv", "output_qvpert",
+                     "output_q", "output_u", "output_upert", "output_v", "output_vpert", "output_w"]
+
+
+class WriteoutOpts(C.Structure):
+    """cm1g_writeout_opts_t: writeout's output switches for the advanced fields."""
+    _fields_ = [(n, C.c_int32) for n in WRITEOUT_SWITCHES] + [("qname", (C.c_char * 4) * CM1G_MAXQ)]
+
+
 class Restart(C.Structure):
     """cm1g_restart_t: scalars of a restart file."""
     _fields_ = [("nstep", C.c_int32), ("mtime", C.c_double), ("dt", C.c_float), ("dtlast", C.c_float),

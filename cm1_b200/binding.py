@@ -10,7 +10,7 @@ import os
 
 import numpy as np
 
-from .abi import Config, Grid, Restart, State, StatOpts, Tune, STATE_FIELDS, fptr, CM1G_OK
+from .abi import Config, Grid, Restart, State, StatOpts, Tune, WriteoutOpts, WRITEOUT_SWITCHES, STATE_FIELDS, fptr, CM1G_OK
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libcm1g.so")
@@ -55,6 +55,7 @@ def lib():
     L.cm1g_pack_records.argtypes = [ctxp, C.c_int32, C.POINTER(_P), i32p, i32p, i32p, _P]
     L.cm1g_unpack_records.argtypes = [ctxp, C.c_int32, C.POINTER(_P), i32p, i32p, i32p, _P]
     L.cm1g_restart_write.argtypes = [ctxp, C.c_char_p, C.POINTER(Restart), stp]
+    L.cm1g_writeout.argtypes = [ctxp, C.c_char_p, C.c_int32, C.c_double, C.POINTER(WriteoutOpts), stp]
     L.cm1g_restart_read.argtypes = [ctxp, C.c_char_p, C.POINTER(Restart), stp]
     L.cm1g_mp_budget.argtypes = [ctxp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int32]
     L.cm1g_pdefq.argtypes = [ctxp, C.c_float, C.POINTER(C.c_double), _P, _P]
@@ -209,6 +210,17 @@ class Context:
     def unpack_records(self, fields, stag, k1, k2, buf):
         n, fp, s, a, b = self._rec_args(fields, stag, k1, k2)
         check(lib().cm1g_unpack_records(self.h, n, fp, s, a, b, ptr(buf)))
+
+    def writeout(self, prefix, nwrite, state, mtime=0.0, switches=None, qnames=("qv", "qc", "qr")):
+        """cm1g_writeout: GrADS files <prefix>_s/_u/_v/_w.dat (+ .ctl) at time
+        nwrite; `switches` names the output_* switches that are on (all by default)."""
+        o = WriteoutOpts()
+        for n in WRITEOUT_SWITCHES:
+            setattr(o, n, 1 if switches is None or n in switches else 0)
+        for q, nm in enumerate(qnames[:8]):
+            o.qname[q].value = nm.encode()
+        s = state if isinstance(state, State) else self.state_struct(state)
+        check(lib().cm1g_writeout(self.h, str(prefix).encode(), nwrite, mtime, C.byref(o), C.byref(s)))
 
     def restart_write(self, path, state, nstep=0, mtime=0.0, dt=0.0, dtlast=0.0, mass1=0.0):
         s = state if isinstance(state, State) else self.state_struct(state)

@@ -33,7 +33,7 @@ int ener_chunks(const DGrid &g);
 void launch_recip_rho(const DGrid &g, const float *rho, float *rr, cudaStream_t st, int64_t *nl);
 long record_count(const DGrid &g, int stag, int k1, int k2);
 void launch_pack_records(const DGrid &g, const float *a, int stag, int k1, int k2, float *out, bool unpack,
-                         cudaStream_t st, int64_t *nl);
+                         cudaStream_t st, int64_t *nl, int mode = 0, const float *base = nullptr);
 void launch_calcener(const DGrid &g, const EnerIn &e, double *part, double *out, cudaStream_t st, int64_t *nl);
 void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w, const float *uten1,
                          const float *vten1, const float *wten1, float *uten, float *vten, float *wten,
@@ -341,6 +341,13 @@ extern "C" int cm1g_init(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_c
     if (!d) { cm1g_finalize(c); return set_err(CM1G_ERR_NOMEM, "profile alloc"); }
     cudaMemcpy(d, col.data(), col.size() * sizeof(float), cudaMemcpyHostToDevice);
     *p.dst = d;
+  }
+  if (gr->prs0 && column_of(gr->prs0, g, g.NK, col)) {   // optional: the output's pressure perturbation
+    col.resize(g.NK + 2, col.back());
+    float *d = (float *)dalloc(c, col.size() * sizeof(float));
+    if (!d) { cm1g_finalize(c); return set_err(CM1G_ERR_NOMEM, "profile alloc"); }
+    cudaMemcpy(d, col.data(), col.size() * sizeof(float), cudaMemcpyHostToDevice);
+    g.prs0 = d;
   }
   struct { const float *src; const float **dst; size_t n; } h1[] = {
       {gr->uh, &g.uh, (size_t)g.NI}, {gr->ruh, &g.ruh, (size_t)g.NI}, {gr->uf, &g.uf, (size_t)g.NI + 1},
@@ -2168,6 +2175,135 @@ extern "C" int cm1g_diff2(cm1g_ctx_t *c, float kdiff2, int32_t idiff, int32_t bb
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
   return S.finish();
+}
+
+// writeout (output_format=1): the GrADS records of the fields this library
+// advances, in writeout's order, and their descriptors.
+namespace {
+struct WVar { std::string name; const float *src; int stag, k1, k2, mode; const float *base; };
+}
+
+extern "C" int cm1g_writeout(cm1g_ctx_t *c, const char *prefix, int32_t nwrite, double mtime,
+                             const cm1g_writeout_opts_t *o, const cm1g_state_t *st) {
+  if (!c || !prefix || !o || !st || nwrite < 1) return set_err(CM1G_ERR_ARG, "bad argument");
+  const DGrid &g = c->g;
+  const cm1g_config_t &cf = c->cfg;
+  const int nk = g.nk, numq = cf.imoist ? cf.numq : 0;
+  enum { PLAIN = 0, ADDP, SUBP, SUBF, EXNER, EXNERP };
+  if ((o->output_prspert) && !g.prs0) return set_err(CM1G_ERR_ARG, "writeout: prspert needs the grid's prs0");
+  auto need = [&](const void *p, const char *what) -> int {
+    return p ? CM1G_OK : set_err(CM1G_ERR_ARG, "writeout: %s is NULL", what);
+  };
+  int rc = CM1G_OK;
+  if (o->output_th || o->output_thpert) rc = rc ? rc : need(st->tha, "tha");
+  if (o->output_prs || o->output_prspert || o->output_pi || o->output_pipert) rc = rc ? rc : need(st->prs, "prs");
+  if (o->output_rho || o->output_rhopert) rc = rc ? rc : need(st->rho, "rho");
+  if (numq && (o->output_qv || o->output_qvpert || o->output_q)) rc = rc ? rc : need(st->qa, "qa");
+  if (o->output_u || o->output_upert) rc = rc ? rc : need(st->ua, "ua");
+  if (o->output_v || o->output_vpert) rc = rc ? rc : need(st->va, "va");
+  if (o->output_w) rc = rc ? rc : need(st->wa, "wa");
+  if (cf.ptype == 1 && (o->output_rain || o->output_prate)) rc = rc ? rc : need(st->rain && st->prate ? st : nullptr, "rain/prate");
+  if (rc) return rc;
+  ProfActive pa(c);
+  Stager S(c);
+  const size_t ns = nS(g), n2 = (size_t)g.NI * g.NJ;
+  auto dv = [&](const float *p, size_t n) { return p ? (const float *)S.in(p, n, false) : nullptr; };
+  const float *tha = dv(st->tha, ns), *prs = dv(st->prs, ns), *rho = dv(st->rho, ns);
+  const float *qa = numq ? dv(st->qa, numq * ns) : nullptr;
+  const float *ua = dv(st->ua, nU(g)), *va = dv(st->va, nV(g)), *wa = dv(st->wa, nW(g));
+  const float *rain = cf.ptype == 1 ? dv(st->rain, n2) : nullptr, *prate = cf.ptype == 1 ? dv(st->prate, n2) : nullptr;
+  if (S.err) return set_err(CM1G_ERR_NOMEM, "staging alloc");
+  // writeout.F's order for these variables (writeout.F:2300-7000)
+  std::vector<WVar> fs, fu, fv, fw;
+  if (cf.ptype == 1 && o->output_rain) fs.push_back({"rain", rain, 1, 0, 0, PLAIN, nullptr});
+  if (cf.ptype == 1 && o->output_prate) fs.push_back({"prate", prate, 1, 0, 0, PLAIN, nullptr});
+  if (o->output_th) fs.push_back({"th", tha, 1, 1, nk, ADDP, g.th0});
+  if (o->output_thpert) fs.push_back({"thpert", tha, 1, 1, nk, PLAIN, nullptr});
+  if (o->output_prs) fs.push_back({"prs", prs, 1, 1, nk, PLAIN, nullptr});
+  if (o->output_prspert) fs.push_back({"prspert", prs, 1, 1, nk, SUBP, g.prs0});
+  if (o->output_pi) fs.push_back({"pi", prs, 1, 1, nk, EXNER, nullptr});
+  if (o->output_pipert) fs.push_back({"pipert", prs, 1, 1, nk, EXNERP, nullptr});
+  if (o->output_rho) fs.push_back({"rho", rho, 1, 1, nk, PLAIN, nullptr});
+  if (o->output_rhopert) fs.push_back({"rhopert", rho, 1, 1, nk, SUBP, g.rho0});
+  if (numq) {
+    const float *qv = qa + (long)(cf.nqv - 1) * ns;
+    if (o->output_qv) fs.push_back({"qv", qv, 1, 1, nk, PLAIN, nullptr});
+    if (o->output_qvpert) fs.push_back({"qvpert", qv, 1, 1, nk, SUBP, g.qv0});
+    if (o->output_q)
+      for (int n = 0; n < numq; n++)
+        if (n + 1 != cf.nqv) {
+          std::string nm(o->qname[n], strnlen(o->qname[n], 4));
+          while (!nm.empty() && nm.back() == ' ') nm.pop_back();
+          fs.push_back({nm.empty() ? "q" + std::to_string(n + 1) : nm, qa + (long)n * ns, 1, 1, nk, PLAIN, nullptr});
+        }
+  }
+  if (o->output_u) fu.push_back({"u", ua, 2, 1, nk, PLAIN, nullptr});
+  if (o->output_upert) fu.push_back({"upert", ua, 2, 1, nk, SUBF, g.u0});
+  if (o->output_v) fv.push_back({"v", va, 3, 1, nk, PLAIN, nullptr});
+  if (o->output_vpert) fv.push_back({"vpert", va, 3, 1, nk, SUBF, g.v0});
+  if (o->output_w) fw.push_back({"w", wa, 4, 1, nk + 1, PLAIN, nullptr});
+  if ((o->output_upert && !g.u0) || (o->output_vpert && !g.v0))
+    return set_err(CM1G_ERR_ARG, "writeout: upert/vpert need the grid's u0/v0");
+  // level heights for the descriptors (zf(1) = 0, dz/mh between w-levels)
+  std::vector<float> mh(g.NK + 2);
+  CUCHK(cudaMemcpyAsync(mh.data(), g.mh, mh.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  struct File { const char *tag; std::vector<WVar> *v; int stag; } files[] = {
+      {"s", &fs, 1}, {"u", &fu, 2}, {"v", &fv, 3}, {"w", &fw, 4}};
+  std::vector<std::vector<float>> host(4);
+  for (int f = 0; f < 4; f++) {
+    auto &vars = *files[f].v;
+    if (vars.empty()) continue;
+    int64_t tot = 0;
+    for (auto &w : vars) tot += record_count(g, w.stag, w.k1, w.k2);
+    float *dbuf = S.dev_buffer((size_t)tot);
+    if (!dbuf || S.err) return set_err(CM1G_ERR_NOMEM, "staging alloc");
+    int64_t off = 0;
+    for (auto &w : vars) {
+      launch_pack_records(g, w.src, w.stag, w.k1, w.k2, dbuf + off, false, c->stream, &c->nlaunch, w.mode, w.base);
+      off += record_count(g, w.stag, w.k1, w.k2);
+    }
+    host[f].resize((size_t)tot);
+    CUCHK(cudaMemcpyAsync(host[f].data(), dbuf, (size_t)tot * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
+  rc = S.finish();
+  if (rc) return rc;
+  std::vector<double> zf(nk + 2, 0.0), zh(nk + 1, 0.0);
+  for (int k = 1; k <= nk; k++) {
+    zf[k + 1] = zf[k] + (double)g.dz / (double)mh[k];
+    zh[k] = 0.5 * (zf[k] + zf[k + 1]);
+  }
+  for (int f = 0; f < 4; f++) {
+    auto &vars = *files[f].v;
+    if (vars.empty()) continue;
+    const std::string base = std::string(prefix) + "_" + files[f].tag;
+    const std::string dat = base + ".dat";
+    FILE *fp = fopen(dat.c_str(), "r+b");
+    if (!fp) fp = fopen(dat.c_str(), "w+b");
+    if (!fp) return set_err(CM1G_ERR_ARG, "cannot open %s", dat.c_str());
+    const long off = (long)(nwrite - 1) * (long)host[f].size() * 4L;
+    bool ok = fseek(fp, off, SEEK_SET) == 0 && fwrite(host[f].data(), 4, host[f].size(), fp) == host[f].size();
+    ok = (fclose(fp) == 0) && ok;
+    if (!ok) return set_err(CM1G_ERR_ARG, "write to %s failed", dat.c_str());
+    // GrADS descriptor of the file (kilometres; one time per call)
+    const int nx = g.ni + (files[f].stag == 2), ny = g.nj + (files[f].stag == 3);
+    const bool wlev = files[f].stag == 4;
+    FILE *cp = fopen((base + ".ctl").c_str(), "w");
+    if (!cp) return set_err(CM1G_ERR_ARG, "cannot create %s.ctl", base.c_str());
+    const char *slash = strrchr(dat.c_str(), '/');
+    fprintf(cp, "dset ^%s\n", slash ? slash + 1 : dat.c_str());
+    fprintf(cp, "title CM1 output (%s points), time %.6f s\nundef -999999.9\n", files[f].tag, mtime);
+    fprintf(cp, "xdef %d linear %.6f %.6f\n", nx, files[f].stag == 2 ? 0.0 : 0.5e-3 * g.dx, 1.0e-3 * g.dx);
+    fprintf(cp, "ydef %d linear %.6f %.6f\n", ny, files[f].stag == 3 ? 0.0 : 0.5e-3 * g.dy, 1.0e-3 * g.dy);
+    fprintf(cp, "zdef %d levels\n", wlev ? nk + 1 : nk);
+    for (int k = 1; k <= (wlev ? nk + 1 : nk); k++) fprintf(cp, "%.6f\n", 1.0e-3 * (wlev ? zf[k] : zh[k]));
+    fprintf(cp, "tdef %d linear 00:00Z03JUL0001 1YR\nvars %zu\n", nwrite, vars.size());
+    for (auto &w : vars) fprintf(cp, "%-8s %d 99 %s\n", w.name.c_str(), w.k2 == 0 ? 0 : w.k2 - w.k1 + 1, w.name.c_str());
+    fprintf(cp, "endvars\n");
+    fclose(cp);
+  }
+  return CM1G_OK;
 }
 
 extern "C" int cm1g_profile(cm1g_ctx_t *c, int32_t enable) {

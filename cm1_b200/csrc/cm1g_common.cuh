@@ -28,6 +28,7 @@ struct DGrid {
   Consts c;
   // vertical profiles (index k, k = 0..nk+1; w-profiles to nk+2)
   const float *mh, *rmh, *mf, *rho0, *rr0, *rf0, *rrf0, *c1, *c2, *pi0, *th0, *rth0, *qv0, *qc0, *qi0;
+  const float *prs0;          // base-state pressure profile (output only; null when not given)
   // horizontal metrics (index i-ib / j-jb)
   const float *uh, *ruh, *uf, *ruf, *vh, *rvh, *vf, *rvf;
   const float *dtu0, *dtv0;   // (ib:ie, jb:je)

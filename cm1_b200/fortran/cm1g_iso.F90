@@ -91,6 +91,14 @@ module cm1g_iso
     type(c_ptr)        :: budname
   end type
 
+  ! writeout's output switches for the fields the library advances
+  type, bind(C) :: cm1g_writeout_opts_t
+    integer(c_int32_t) :: output_rain, output_prate, output_th, output_thpert, output_prs, output_prspert, &
+                          output_pi, output_pipert, output_rho, output_rhopert, output_qv, output_qvpert, &
+                          output_q, output_u, output_upert, output_v, output_vpert, output_w
+    character(kind=c_char) :: qname(4, CM1G_MAXQ)
+  end type
+
   ! scalars of a restart file (cm1g_restart_write / cm1g_restart_read)
   type, bind(C) :: cm1g_restart_t
     integer(c_int32_t) :: nstep
@@ -239,6 +247,15 @@ module cm1g_iso
       type(c_ptr), intent(in) :: fields(*)
       integer(c_int32_t), intent(in) :: stag(*), k1(*), k2(*)
       real(c_float), intent(out) :: out(*)
+    end function
+    integer(c_int) function cm1g_writeout(ctx, prefix, nwrite, mtime, opts, st) bind(C, name="cm1g_writeout")
+      import :: c_int, c_int32_t, c_double, c_char, c_ptr, cm1g_writeout_opts_t, cm1g_state_t
+      type(c_ptr), value :: ctx
+      character(kind=c_char), intent(in) :: prefix(*)
+      integer(c_int32_t), value :: nwrite
+      real(c_double), value :: mtime
+      type(cm1g_writeout_opts_t), intent(in) :: opts
+      type(cm1g_state_t), intent(in) :: st
     end function
     integer(c_int) function cm1g_restart_write(ctx, path, hdr, st) bind(C, name="cm1g_restart_write")
       import :: c_int, c_char, c_ptr, cm1g_restart_t, cm1g_state_t

@@ -344,6 +344,25 @@ int cm1g_pack_records(cm1g_ctx_t *ctx, int32_t n, const float *const *fields, co
 int cm1g_unpack_records(cm1g_ctx_t *ctx, int32_t n, float *const *fields, const int32_t *stag,
                         const int32_t *k1, const int32_t *k2, const float *in);
 
+/* writeout with output_format=1 (writeout.F:20-8752) for the fields this
+ * library advances: the switches are writeout's output_* of namelist param6
+ * for those fields, the variables follow writeout's order and forms (th =
+ * th0+tha, prspert = prs-prs0, pi = (prs/p00)**(rd/cp), pipert = pi-pi0,
+ * rhopert = rho-rho0, qvpert = qv-qv0, the other q arrays by qname, upert =
+ * ua-u0, vpert = va-v0; rain and prate with ptype=1), gathered on the device
+ * and written as time nwrite (1-based) of <prefix>_s.dat, _u.dat, _v.dat and
+ * _w.dat (direct access, one record per level of nx*ny points), each with a
+ * GrADS descriptor <prefix>_?.ctl (its own layout; not byte-identical to the
+ * reference's write_ctl).  prspert needs the grid's prs0 at cm1g_init. */
+typedef struct cm1g_writeout_opts {
+  int32_t output_rain, output_prate, output_th, output_thpert, output_prs, output_prspert, output_pi,
+          output_pipert, output_rho, output_rhopert, output_qv, output_qvpert, output_q, output_u, output_upert,
+          output_v, output_vpert, output_w;
+  char qname[CM1G_MAXQ][4];
+} cm1g_writeout_opts_t;
+int cm1g_writeout(cm1g_ctx_t *ctx, const char *prefix, int32_t nwrite, double mtime,
+                  const cm1g_writeout_opts_t *opts, const cm1g_state_t *st);
+
 /* Restart of the state the library advances: the dynamical-core part of
  * restart_write / restart_read (restart_write.F:10-2850, restart_read.F).
  * The file holds a header (grid, options, nstep, mtime, dt, dtlast, mass1),

@@ -123,3 +123,52 @@ def test_restart_rejects_other_grid(tmp_path, cm1g):
         ctx.restart_read(bad, case.copy_state())
     ctx.close()
     ctx2.close()
+
+
+def test_writeout_grads_files(tmp_path, cm1g):
+    """writeout's GrADS files for a Kessler state: each variable's records
+    (one per level, i fastest) equal writeout's formula applied to the state
+    with numpy; two output times land as consecutive time blocks."""
+    torch = _torch()
+    case = make_case("kessler", ni=24, nj=20, nk=16)
+    lay, gr = case.lay, case.grid
+    ctx = cm1g.Context(case.cfg, case.grid)
+    dev = cm1g.to_device(case.state)
+    for _ in range(2):
+        ctx.step(dev, case.dt, case.mass1, use_graph=True)
+    prefix = tmp_path / "cm1out"
+    ctx.writeout(prefix, 1, dev, mtime=2 * case.dt)
+    h1 = cm1g.to_host(dev)
+    ctx.step(dev, case.dt, case.mass1, use_graph=True)
+    ctx.writeout(prefix, 2, dev, mtime=3 * case.dt)
+    h2 = cm1g.to_host(dev)
+    I, U, V, W = lay.interior(1), lay.interior(2), lay.interior(3), lay.interior(4)
+    f32 = np.float32
+
+    def s_vars(h):
+        pi = np.power((h["prs"][I] * f32(1.0 / 1.0e5)).astype(np.float64),
+                      float(np.float32(287.04) / np.float32(1005.7))).astype(f32)
+        sfc = (slice(lay.jx(1), lay.jx(lay.nj) + 1), slice(lay.ix(1), lay.ix(lay.ni) + 1))
+        return [h["rain"][sfc], h["prate"][sfc], gr["th0"][I] + h["tha"][I], h["tha"][I], h["prs"][I],
+                h["prs"][I] - gr["prs0"][I], pi, pi - gr["pi0"][I], h["rho"][I], h["rho"][I] - gr["rho0"][I],
+                h["qa"][0][I], h["qa"][0][I] - gr["qv0"][I], h["qa"][1][I], h["qa"][2][I]]
+
+    per_s = sum(v.size for v in s_vars(h1))
+    s = np.fromfile(str(prefix) + "_s.dat", dtype=f32)
+    assert s.size == 2 * per_s
+    for t, h in ((0, h1), (1, h2)):
+        off = t * per_s
+        for n, v in enumerate(s_vars(h)):
+            got = s[off:off + v.size].reshape(v.shape)
+            if n in (6, 7):    # pi and pipert: binary64 power rounded once on both sides
+                assert np.abs(got - v).max() <= 2 * np.spacing(f32(1.0)), n
+            else:
+                assert np.array_equal(got, v), n
+            off += v.size
+    u = np.fromfile(str(prefix) + "_u.dat", dtype=f32).reshape(2, 2, -1)
+    assert np.array_equal(u[1, 0], h2["ua"][U].ravel()) and np.array_equal(u[1, 1], (h2["ua"][U] - gr["u0"][U]).ravel())
+    w = np.fromfile(str(prefix) + "_w.dat", dtype=f32).reshape(2, -1)
+    assert np.array_equal(w[0], h1["wa"][W].ravel())
+    ctl = open(str(prefix) + "_s.ctl").read()
+    assert "vars 14" in ctl and "tdef 2" in ctl and "qc " in ctl
+    ctx.close()
