@@ -50,6 +50,7 @@ def lib():
     L.cm1g_solve3.argtypes = [ctxp, stp]
     L.cm1g_mp_driver.argtypes = [ctxp, C.c_float, stp]
     L.cm1g_diff2.argtypes = [ctxp, C.c_float, C.c_int32, C.c_int32, C.c_int32, _P, _P] + [_P] * 13
+    L.cm1g_turbsmag.argtypes = [ctxp, C.c_float] + [C.c_int32] * 4 + [_P, _P] + [_P] * 15
     i32p = C.POINTER(C.c_int32)
     L.cm1g_records_size.argtypes = [ctxp, C.c_int32, i32p, i32p, i32p, C.POINTER(C.c_int64)]
     L.cm1g_pack_records.argtypes = [ctxp, C.c_int32, C.POINTER(_P), i32p, i32p, i32p, _P]
@@ -241,6 +242,14 @@ class Context:
         check(lib().cm1g_diff2(self.h, kdiff2, idiff, bbc, tbc, f3(cgs), f3(cgt), ptr(ua), ptr(va), ptr(wa),
                                ptr(rho), ptr(tha), ptr(qa), ptr(pta), ptr(uten1), ptr(vten1), ptr(wten1),
                                ptr(thten1), ptr(qten), ptr(ptten)))
+
+    def turbsmag(self, csm, tconfig, bcturbs, bbc, tbc, cgs, cgt, ua, va, wa, rho, tha, pta=None, uten1=None,
+                 vten1=None, wten1=None, thten1=None, ptten=None, kmh=None, kmv=None):
+        """cm1g_turbsmag: Smagorinsky LES tendencies added to uten1 ... ptten."""
+        f3 = lambda v: (C.c_float * 3)(*[float(x) for x in v])
+        check(lib().cm1g_turbsmag(self.h, csm, tconfig, bcturbs, bbc, tbc, f3(cgs), f3(cgt), ptr(ua), ptr(va),
+                                  ptr(wa), ptr(rho), ptr(tha), None, ptr(pta), ptr(uten1), ptr(vten1), ptr(wten1),
+                                  ptr(thten1), None, ptr(ptten), ptr(kmh), ptr(kmv)))
 
     def mp_driver(self, state, dt):
         """cm1g_mp_driver: the Kessler branch of mp_driver on `state` (ptype=1)."""

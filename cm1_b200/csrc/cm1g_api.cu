@@ -19,6 +19,7 @@
 #include "k_stat.cuh"
 #include "k_micro.cuh"
 #include "k_diff2.cuh"
+#include "k_turb.cuh"
 #include "../../include/cm1g.h"
 
 namespace cm1g {
@@ -199,6 +200,7 @@ struct cm1g_ctx {
   double *mp_qbud = nullptr;                  // qbudget(1..7) and asq(1..3), accumulated on the device
   int *mp_err = nullptr;
   float *d2s = nullptr;                       // scratch of the 2nd-order diffusion (cm1g_diff2)
+  float *les = nullptr;                       // scratch of the Smagorinsky LES tendencies (cm1g_turbsmag)
 };
 
 // Makes the context's profile (if any) the active one for the calling thread.
@@ -2172,6 +2174,63 @@ extern "C" int cm1g_diff2(cm1g_ctx_t *c, float kdiff2, int32_t idiff, int32_t bb
   }
   if (S.err) return set_err(CM1G_ERR_NOMEM, "staging alloc");
   launch_diff2(g, a, c->stream, &c->nlaunch);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
+  return S.finish();
+}
+
+// Smagorinsky LES (sgsmodel=2): deformation, N^2, kmh/kmv, stresses and the
+// tendencies solve1 adds (turb.F:1327-1340, 1405-1415, 1629-1640; solve1.F:
+// 1113-1240).  kmh/kmv, when given, receive the eddy viscosities (w-arrays).
+extern "C" int cm1g_turbsmag(cm1g_ctx_t *c, float csm, int32_t tconfig, int32_t bcturbs, int32_t bbc, int32_t tbc,
+                             const float cgs[3], const float cgt[3], const float *ua, const float *va,
+                             const float *wa, const float *rho, const float *tha, const float *qa, const float *pta,
+                             float *uten1, float *vten1, float *wten1, float *thten1, float *qten, float *ptten,
+                             float *kmh, float *kmv) {
+  if (!c || !cgs || !cgt || !ua || !va || !wa || !rho || !tha) return set_err(CM1G_ERR_ARG, "null argument");
+  if (!uten1 || !vten1 || !wten1) return set_err(CM1G_ERR_ARG, "uten1/vten1/wten1 missing");
+  if (!(csm >= 0.0f)) return set_err(CM1G_ERR_ARG, "csm must be >= 0");
+  if (tconfig != 1 && tconfig != 2) return set_err(CM1G_ERR_ARG, "tconfig must be 1 or 2");
+  if (bcturbs != 1 && bcturbs != 2) return set_err(CM1G_ERR_ARG, "bcturbs must be 1 or 2");
+  if ((bbc != 1 && bbc != 2) || (tbc != 1 && tbc != 2))
+    return set_err(CM1G_ERR_UNSUPPORTED, "turbsmag: bbc/tbc 1 (free slip) or 2 (no slip) only (bbc=3 needs the surface layer)");
+  const DGrid &g = c->g;
+  const cm1g_config_t &cf = c->cfg;
+  if (g.wbc != 1 || g.ebc != 1 || g.sbc != 1 || g.nbc != 1)
+    return set_err(CM1G_ERR_UNSUPPORTED, "turbsmag: periodic lateral boundaries only");
+  if (cf.imoist) return set_err(CM1G_ERR_UNSUPPORTED, "turbsmag: the moist N^2 of calcnm is not built (imoist=0 only)");
+  const int npt = cf.iptra ? cf.npt : 0;
+  if (thten1 && npt && (!pta || !ptten)) return set_err(CM1G_ERR_ARG, "turbsmag with tracers needs pta/ptten");
+  const size_t ns = nS(g), nw = nW(g);
+  if (!c->les) {
+    c->les = (float *)dalloc(c, (4 * ns + 6 * nw) * sizeof(float));
+    if (!c->les) return set_err(CM1G_ERR_NOMEM, "turbsmag scratch");
+  }
+  ProfActive pa(c);
+  Stager S(c);
+  TurbArgs a{};
+  a.csm = csm;
+  const float prandtl = 1.0f / 3.00f;
+  a.prinv = 1.0f / prandtl;
+  a.cgs1 = cgs[0]; a.cgs2 = cgs[1]; a.cgs3 = cgs[2]; a.cgt1 = cgt[0]; a.cgt2 = cgt[1]; a.cgt3 = cgt[2];
+  a.tconfig = tconfig; a.bcturbs = bcturbs; a.bbc = bbc; a.tbc = tbc;
+  a.ua = S.in(ua, nU(g), false); a.va = S.in(va, nV(g), false); a.wa = S.in(wa, nW(g), false);
+  a.rho = S.in(rho, ns, false); a.tha = S.in(tha, ns, false);
+  a.uten = S.in(uten1, nU(g), true); a.vten = S.in(vten1, nV(g), true); a.wten = S.in(wten1, nW(g), true);
+  if (thten1) {
+    a.thten = S.in(thten1, ns, true);
+    a.numq = 0;
+    a.npt = npt;
+    a.pta = npt ? S.in(pta, npt * ns, false) : nullptr;
+    a.ptten = npt ? S.in(ptten, npt * ns, true) : nullptr;
+  }
+  float *p = c->les;
+  a.t11 = p; p += ns; a.t22 = p; p += ns; a.t33 = p; p += ns; a.t12 = p; p += ns;
+  a.s13 = p; p += nw; a.s23 = p; p += nw; a.t13 = p; p += nw; a.t23 = p; p += nw;
+  a.kmh = kmh ? S.in(kmh, nw, true) : p; p += nw;
+  a.kmv = kmv ? S.in(kmv, nw, true) : p;
+  if (S.err) return set_err(CM1G_ERR_NOMEM, "staging alloc");
+  launch_turbsmag(g, a, c->stream, &c->nlaunch);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
   return S.finish();

@@ -226,6 +226,17 @@ module cm1g_iso
       real(c_float), intent(in) :: cgs(3), cgt(3)
       type(c_ptr), value :: ua, va, wa, rho, tha, qa, pta, uten1, vten1, wten1, thten1, qten, ptten
     end function
+    ! Smagorinsky LES (sgsmodel=2): sfc_and_turb's closure + solve1's turb* tendencies
+    integer(c_int) function cm1g_turbsmag(ctx, csm, tconfig, bcturbs, bbc, tbc, cgs, cgt, ua, va, wa, rho, tha, &
+                                          qa, pta, uten1, vten1, wten1, thten1, qten, ptten, kmh, kmv) &
+                                          bind(C, name="cm1g_turbsmag")
+      import :: c_int, c_int32_t, c_float, c_ptr
+      type(c_ptr), value :: ctx
+      real(c_float), value :: csm
+      integer(c_int32_t), value :: tconfig, bcturbs, bbc, tbc
+      real(c_float), intent(in) :: cgs(3), cgt(3)
+      type(c_ptr), value :: ua, va, wa, rho, tha, qa, pta, uten1, vten1, wten1, thten1, qten, ptten, kmh, kmv
+    end function
     ! mp_driver's Kessler branch alone (ptype=1) and its FP64 budgets
     integer(c_int) function cm1g_mp_driver(ctx, dt, st) bind(C, name="cm1g_mp_driver")
       import :: c_int, c_float, c_ptr, cm1g_state_t

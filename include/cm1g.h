@@ -272,6 +272,25 @@ int cm1g_diff2(cm1g_ctx_t *ctx, float kdiff2, int32_t idiff, int32_t bbc, int32_
                const float *tha, const float *qa, const float *pta, float *uten1, float *vten1, float *wten1,
                float *thten1, float *qten, float *ptten);
 
+/* Smagorinsky subgrid turbulence of an LES (sgsmodel=2), dry, Cartesian
+ * without terrain, periodic lateral boundaries, explicit vertical mixing
+ * (doimpl=0): calcnm's dry N^2 and calcdef's deformation (src/turb.F:
+ * 1327-1340, 4711-5423, 5432-5480), turbsmag's kmh/kmv for tconfig 1 or 2
+ * with a uniform Smagorinsky constant csm (src/turb.F:3375-3621), gettau's
+ * stresses with sfcstress's free-slip (bbc=1) or no-slip (bbc=2) bottom and
+ * the free-slip/no-slip top (src/turb.F:4059-4582), and the tendencies of
+ * turbu/turbv/turbw and turbs for theta and each tracer that solve1 adds to
+ * uten1 ... ptten (src/turbtend.F; src/solve1.F:1113-1240), without surface
+ * fluxes.  cgs/cgt extrapolate rf to the bottom/top w-levels.  thten1 NULL
+ * skips the scalars.  kmh/kmv (w-arrays, may be NULL) receive the eddy
+ * viscosities including bcw's zero bottom/top rows and periodic halo.
+ * Replaces: the iturb/sgsmodel=2 branch of sfc_and_turb plus the doturb
+ * block of solve1 (src/solve1.F:1113). */
+int cm1g_turbsmag(cm1g_ctx_t *ctx, float csm, int32_t tconfig, int32_t bcturbs, int32_t bbc, int32_t tbc,
+                  const float cgs[3], const float cgt[3], const float *ua, const float *va, const float *wa,
+                  const float *rho, const float *tha, const float *qa, const float *pta, float *uten1,
+                  float *vten1, float *wten1, float *thten1, float *qten, float *ptten, float *kmh, float *kmv);
+
 /* Domain extrema over the physical cells of an s/u/v/w array: replaces
  * maxmin (src/maxmin.F:5-119).  stag: 1 s, 2 u, 3 v, 4 w.  loc receives
  * 1-based (i,j,k) of the max (loc[0..2]) and of the min (loc[3..5]). */

@@ -2505,3 +2505,227 @@ int oracle_threads(void) {
   return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------ */
+/* Smagorinsky LES (sgsmodel=2), dry, no terrain, periodic laterals    */
+/* ------------------------------------------------------------------ */
+
+/* calcnm (dry, turb.F:5458-5477), calcdef (turb.F:4772-4893, 5366-5390),
+ * turbsmag (turb.F:3415-3540) with bcw(kmh/kmv, 1) (bc.F:1126-1137 and the
+ * periodic fill), gettau (turb.F:4110-4135, 4190-4200) with sfcstress
+ * (turb.F:4537-4562) and the top rows (turb.F:4397-4420), then turbu, turbv,
+ * turbw (turbtend.F:1101-1104, 1290-1296, 1408-1416; 1860-1866, 2056-2060,
+ * 2170-2180; 2510-2515, 2540-2547, 2575-2580) and turbs/turbsz explicit
+ * (turbtend.F:66-104, 380-395, 480-545) in solve1's order
+ * (solve1.F:1113-1240).  Loops over the same index ranges as the Fortran;
+ * binary32 in its evaluation order; logf and powf from the C library. */
+int oracle_turbsmag(const cm1g_config_t *cfg, const cm1g_grid_t *gr, float csm, int tconfig, int bcturbs, int bbc,
+                    int tbc, const float *cgs, const float *cgt, const float *ua_, const float *va_, const float *wa_,
+                    const float *rho_, const float *tha_, const float *pta_, float *uten_, float *vten_, float *wten_,
+                    float *thten_, float *ptten_, float *kmh_out, float *kmv_out) {
+  OG G, *g = &G;
+  if (og_setup(g, cfg, gr)) return -1;
+  if (cfg->wbc != 1 || cfg->ebc != 1 || cfg->sbc != 1 || cfg->nbc != 1 || cfg->imoist) return -2;
+  const int ni = g->ni, nj = g->nj, nk = g->nk;
+  const int npt = cfg->iptra ? cfg->npt : 0;
+  const long ns = nS(g), nw = nW(g);
+  F3 ua = mkU(g, ua_), va = mkV(g, va_), wa = mkW(g, wa_), rho = mkS(g, rho_), tha = mkS(g, tha_);
+  F3 uten = mkU(g, uten_), vten = mkV(g, vten_), wten = mkW(g, wten_);
+  float *buf = (float *)calloc((size_t)(7 * ns + 9 * nw), sizeof(float));
+  if (!buf) return -3;
+  float *p = buf;
+  F3 rr = mkS(g, p); p += ns;
+  F3 t11 = mkS(g, p); p += ns;
+  F3 t22 = mkS(g, p); p += ns;
+  F3 t33 = mkS(g, p); p += ns;
+  F3 t12 = mkS(g, p); p += ns;
+  F3 sadv = mkS(g, p); p += ns;
+  F3 dumx = mkS(g, p); p += ns;
+  F3 rf = mkW(g, p); p += nw;
+  F3 t13 = mkW(g, p); p += nw;
+  F3 t23 = mkW(g, p); p += nw;
+  F3 nm = mkW(g, p); p += nw;
+  F3 defv = mkW(g, p); p += nw;
+  F3 defh = mkW(g, p); p += nw;
+  F3 kmh = mkW(g, p); p += nw;
+  F3 kmv = mkW(g, p); p += nw;
+  F3 dumz = mkW(g, p);
+  const float rdx = g->rdx, rdy = g->rdy, rdz = g->rdz, grav = g->c.g;
+  const float prandtl = 1.0f / 3.00f, prinv = 1.0f / prandtl, dmin = 1.0e-10f;
+  /* rr, rf (solve3.F:660-678) */
+  for (int k = 2; k <= nk; k++) for (int j = 0; j <= nj + 1; j++) for (int i = 0; i <= ni + 1; i++) {
+    A3(rr, i, j, k) = 1.0f / A3(rho, i, j, k);
+    A3(rf, i, j, k) = (A3(g->c1, i, j, k) * A3(rho, i, j, k - 1) + A3(g->c2, i, j, k) * A3(rho, i, j, k));
+  }
+  for (int j = 0; j <= nj + 1; j++) for (int i = 0; i <= ni + 1; i++) {
+    A3(rr, i, j, 1) = 1.0f / A3(rho, i, j, 1);
+    A3(rf, i, j, 1) = cgs[0] * A3(rho, i, j, 1) + cgs[1] * A3(rho, i, j, 2) + cgs[2] * A3(rho, i, j, 3);
+    A3(rf, i, j, nk + 1) = cgt[0] * A3(rho, i, j, nk) + cgt[1] * A3(rho, i, j, nk - 1) + cgt[2] * A3(rho, i, j, nk - 2);
+  }
+  /* calcnm, imoist = 0 */
+  for (int k = 2; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++)
+    A3(nm, i, j, k) = logf((A3(g->th0, i, j, k) + A3(tha, i, j, k)) / (A3(g->th0, i, j, k - 1) + A3(tha, i, j, k - 1))) *
+                      grav * rdz * A3(g->mf, i, j, k);
+  /* calcdef: rho * S_ij */
+  for (int k = 1; k <= nk; k++) {
+    const float temz = rdz * A3(g->mh, 1, 1, k);
+    for (int j = 0; j <= nj + 1; j++) for (int i = 0; i <= ni + 1; i++) {
+      A3(t11, i, j, k) = A3(rho, i, j, k) * (A3(ua, i + 1, j, k) - A3(ua, i, j, k)) * rdx * UH(i);
+      A3(t22, i, j, k) = A3(rho, i, j, k) * (A3(va, i, j + 1, k) - A3(va, i, j, k)) * rdy * VH(j);
+      A3(t33, i, j, k) = A3(rho, i, j, k) * (A3(wa, i, j, k + 1) - A3(wa, i, j, k)) * temz;
+      A3(t12, i, j, k) = 0.5f * ((A3(ua, i, j, k) - A3(ua, i, j - 1, k)) * rdy * VF(j) +
+                                 (A3(va, i, j, k) - A3(va, i - 1, j, k)) * rdx * UF(i)) * 0.25f *
+                         ((A3(rho, i - 1, j - 1, k) + A3(rho, i, j, k)) + (A3(rho, i - 1, j, k) + A3(rho, i, j - 1, k)));
+    }
+  }
+  for (int k = 2; k <= nk; k++) for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni + 1; i++) {
+    A3(t13, i, j, k) = 0.5f * ((A3(wa, i, j, k) - A3(wa, i - 1, j, k)) * rdx * UF(i) +
+                               (A3(ua, i, j, k) - A3(ua, i, j, k - 1)) * rdz * 0.5f * (A3(g->mf, i - 1, j, k) + A3(g->mf, i, j, k))) *
+                       0.5f * (A3(rf, i - 1, j, k) + A3(rf, i, j, k));
+    A3(t23, i, j, k) = 0.5f * ((A3(wa, i, j, k) - A3(wa, i, j - 1, k)) * rdy * VF(j) +
+                               (A3(va, i, j, k) - A3(va, i, j, k - 1)) * rdz * 0.5f * (A3(g->mf, i, j - 1, k) + A3(g->mf, i, j, k))) *
+                       0.5f * (A3(rf, i, j - 1, k) + A3(rf, i, j, k));
+  }
+#define SQ(x) ((x) * (x))
+  for (int k = 2; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++) {
+    const float c1 = A3(g->c1, i, j, k), c2 = A3(g->c2, i, j, k);
+    float tmp11 = (c1 * SQ(A3(t11, i, j, k - 1)) + c2 * SQ(A3(t11, i, j, k)));
+    float tmp22 = (c1 * SQ(A3(t22, i, j, k - 1)) + c2 * SQ(A3(t22, i, j, k)));
+    float tmp33 = (c1 * SQ(A3(t33, i, j, k - 1)) + c2 * SQ(A3(t33, i, j, k)));
+    float tmp12 = 0.25f * (c1 * ((SQ(A3(t12, i, j, k - 1)) + SQ(A3(t12, i + 1, j + 1, k - 1))) +
+                                 (SQ(A3(t12, i, j + 1, k - 1)) + SQ(A3(t12, i + 1, j, k - 1)))) +
+                           c2 * ((SQ(A3(t12, i, j, k)) + SQ(A3(t12, i + 1, j + 1, k))) +
+                                 (SQ(A3(t12, i, j + 1, k)) + SQ(A3(t12, i + 1, j, k)))));
+    float tmp13 = 0.5f * (SQ(A3(t13, i, j, k)) + SQ(A3(t13, i + 1, j, k)));
+    float tmp23 = 0.5f * (SQ(A3(t23, i, j, k)) + SQ(A3(t23, i, j + 1, k)));
+    float rrf = 1.0f / SQ(A3(rf, i, j, k));
+    A3(defv, i, j, k) = 4.0f * (tmp13 + tmp23) * rrf;
+    A3(defh, i, j, k) = (2.0f * ((tmp11 + tmp22) + tmp33) + 4.0f * tmp12) * rrf;
+  }
+  /* turbsmag */
+  for (int j = 1; j <= nj; j++) for (int k = 2; k <= nk; k++) for (int i = 1; i <= ni; i++) {
+    const float rmf = 1.0f / A3(g->mf, i, j, k);
+    if (tconfig == 1) {
+      float grdscl = powf(((g->dx * RUH(i)) * (g->dy * RVH(j))) * (g->dz * rmf), 0.33333333f);
+      A3(kmh, i, j, k) = SQ(csm * grdscl) * sqrtf(fmaxf(A3(defv, i, j, k) + A3(defh, i, j, k) - A3(nm, i, j, k) * prinv, dmin));
+      A3(kmv, i, j, k) = A3(kmh, i, j, k);
+    } else {
+      float lenh = sqrtf((g->dx * RUH(i)) * (g->dy * RVH(j)));
+      float grdscl = g->dz * rmf;
+      A3(kmh, i, j, k) = SQ(csm * lenh) * sqrtf(fmaxf(A3(defh, i, j, k), dmin));
+      A3(kmv, i, j, k) = SQ(csm * grdscl) * sqrtf(fmaxf(A3(defv, i, j, k) - A3(nm, i, j, k) * prinv, dmin));
+    }
+  }
+  /* bcw(kmh, 1), bcw(kmv, 1): periodic fill of the halo ring, zero bottom and top rows */
+  F3 km2[2] = {kmh, kmv};
+  for (int m = 0; m < 2; m++) {
+    F3 K = km2[m];
+    for (int k = 2; k <= nk; k++) {
+      for (int j = 1; j <= nj; j++) { A3(K, 0, j, k) = A3(K, ni, j, k); A3(K, ni + 1, j, k) = A3(K, 1, j, k); }
+      for (int i = 0; i <= ni + 1; i++) { A3(K, i, 0, k) = A3(K, i, nj, k); A3(K, i, nj + 1, k) = A3(K, i, 1, k); }
+    }
+    for (int j = 0; j <= nj + 1; j++) for (int i = 0; i <= ni + 1; i++) { A3(K, i, j, 1) = 0.0f; A3(K, i, j, nk + 1) = 0.0f; }
+  }
+  /* gettau */
+  for (int k = 1; k <= nk; k++) for (int j = 0; j <= nj + 1; j++) for (int i = 0; i <= ni + 1; i++) {
+    float tem = (A3(kmh, i, j, k) + A3(kmh, i, j, k + 1));
+    A3(t11, i, j, k) = A3(t11, i, j, k) * tem;
+    A3(t22, i, j, k) = A3(t22, i, j, k) * tem;
+    A3(t33, i, j, k) = A3(t33, i, j, k) * tem;
+    if (i >= 1 && j >= 1)   /* the Fortran's i=0/j=0 products are never read */
+      A3(t12, i, j, k) = A3(t12, i, j, k) * 0.25f *
+                         (((A3(kmh, i - 1, j - 1, k) + A3(kmh, i, j, k)) + (A3(kmh, i - 1, j, k) + A3(kmh, i, j - 1, k))) +
+                          ((A3(kmh, i - 1, j - 1, k + 1) + A3(kmh, i, j, k + 1)) + (A3(kmh, i - 1, j, k + 1) + A3(kmh, i, j - 1, k + 1))));
+  }
+  for (int k = 2; k <= nk; k++) for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni + 1; i++) {
+    A3(t13, i, j, k) = A3(t13, i, j, k) * (A3(kmv, i - 1, j, k) + A3(kmv, i, j, k));
+    A3(t23, i, j, k) = A3(t23, i, j, k) * (A3(kmv, i, j - 1, k) + A3(kmv, i, j, k));
+  }
+  for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni + 1; i++) {
+    if (bbc == 1) { A3(t13, i, j, 1) = A3(t13, i, j, 2); A3(t23, i, j, 1) = A3(t23, i, j, 2); }
+    else {
+      A3(t13, i, j, 1) = 2.0f * A3(ua, i, j, 1) * rdz * 0.5f * (A3(g->mf, i - 1, j, 1) + A3(g->mf, i, j, 1)) * 0.5f *
+                         (A3(rf, i - 1, j, 1) + A3(rf, i, j, 1)) * 0.5f * (A3(kmv, i - 1, j, 2) + A3(kmv, i, j, 2));
+      A3(t23, i, j, 1) = 2.0f * A3(va, i, j, 1) * rdz * 0.5f * (A3(g->mf, i, j - 1, 1) + A3(g->mf, i, j, 1)) * 0.5f *
+                         (A3(rf, i, j - 1, 1) + A3(rf, i, j, 1)) * 0.5f * (A3(kmv, i, j - 1, 2) + A3(kmv, i, j, 2));
+    }
+    if (tbc == 1) { A3(t13, i, j, nk + 1) = A3(t13, i, j, nk); A3(t23, i, j, nk + 1) = A3(t23, i, j, nk); }
+    else {
+      A3(t13, i, j, nk + 1) = -2.0f * A3(ua, i, j, nk) * rdz * 0.5f * (A3(g->mf, i - 1, j, nk + 1) + A3(g->mf, i, j, nk + 1)) *
+                              0.5f * (A3(rf, i - 1, j, nk + 1) + A3(rf, i, j, nk + 1)) * 0.5f *
+                              (A3(kmv, i - 1, j, nk) + A3(kmv, i, j, nk));
+      A3(t23, i, j, nk + 1) = -2.0f * A3(va, i, j, nk) * rdz * 0.5f * (A3(g->mf, i, j - 1, nk + 1) + A3(g->mf, i, j, nk + 1)) *
+                              0.5f * (A3(rf, i, j - 1, nk + 1) + A3(rf, i, j, nk + 1)) * 0.5f *
+                              (A3(kmv, i, j - 1, nk) + A3(kmv, i, j, nk));
+    }
+  }
+  /* turbu, turbv, turbw */
+  const float tem = rdz * 0.5f;
+  for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni + 1; i++) {
+    float tx = (A3(t11, i, j, k) - A3(t11, i - 1, j, k)) * rdx * UF(i);
+    float ty = (A3(t12, i, j + 1, k) - A3(t12, i, j, k)) * rdy * VH(j);
+    float tz = (A3(t13, i, j, k + 1) - A3(t13, i, j, k)) * tem * (A3(g->mh, i - 1, j, k) + A3(g->mh, i, j, k));
+    float rru0 = 1.0f / (0.5f * (A3(rho, i - 1, j, k) + A3(rho, i, j, k)));
+    A3(uten, i, j, k) = A3(uten, i, j, k) + ((tx + ty) + tz) * rru0;
+  }
+  for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni; i++) {
+    float tx = (A3(t12, i + 1, j, k) - A3(t12, i, j, k)) * rdx * UH(i);
+    float ty = (A3(t22, i, j, k) - A3(t22, i, j - 1, k)) * rdy * VF(j);
+    float tz = (A3(t23, i, j, k + 1) - A3(t23, i, j, k)) * tem * (A3(g->mh, i, j - 1, k) + A3(g->mh, i, j, k));
+    float rrv0 = 1.0f / (0.5f * (A3(rho, i, j - 1, k) + A3(rho, i, j, k)));
+    A3(vten, i, j, k) = A3(vten, i, j, k) + ((tx + ty) + tz) * rrv0;
+  }
+  for (int k = 2; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++) {
+    float tx = (A3(t13, i + 1, j, k) - A3(t13, i, j, k)) * rdx * UH(i);
+    float ty = (A3(t23, i, j + 1, k) - A3(t23, i, j, k)) * rdy * VH(j);
+    float tz = (A3(t33, i, j, k) - A3(t33, i, j, k - 1)) * rdz * A3(g->mf, i, j, k);
+    A3(wten, i, j, k) = A3(wten, i, j, k) + ((tx + ty) + tz) / A3(rf, i, j, k);
+  }
+  /* turbs: theta (s = th0 - th0r + tha), then each tracer */
+  if (thten_) {
+    for (int n = -1; n < npt; n++) {
+      F3 sten = n < 0 ? mkS(g, thten_) : mkS(g, ptten_ + (long)n * ns);
+      if (n < 0) {
+        for (int k = 1; k <= nk; k++) {
+          float t0 = A3(g->th0, 1, 1, k) - 300.0f;
+          for (int j = 0; j <= nj + 1; j++) for (int i = 0; i <= ni + 1; i++) A3(sadv, i, j, k) = t0 + A3(tha, i, j, k);
+        }
+      } else {
+        memcpy(sadv.p, pta_ + (long)n * ns, (size_t)ns * sizeof(float));
+      }
+      F3 s = sadv;
+      for (int k = 1; k <= nk; k++) {
+        for (int j = 1; j <= nj + 1; j++) for (int i = 1; i <= ni + 1; i++) {
+          A3(dumx, i, j, k) = -0.125f * (A3(rho, i, j, k) + A3(rho, i - 1, j, k)) *
+                              ((A3(kmh, i, j, k) * prinv + A3(kmh, i - 1, j, k) * prinv) +
+                               (A3(kmh, i, j, k + 1) * prinv + A3(kmh, i - 1, j, k + 1) * prinv)) *
+                              (A3(s, i, j, k) - A3(s, i - 1, j, k)) * rdx * UF(i);
+          A3(t13, i, j, k) = -0.125f * (A3(rho, i, j, k) + A3(rho, i, j - 1, k)) *    /* t13 reused as dumy */
+                             ((A3(kmh, i, j, k) * prinv + A3(kmh, i, j - 1, k) * prinv) +
+                              (A3(kmh, i, j, k + 1) * prinv + A3(kmh, i, j - 1, k + 1) * prinv)) *
+                             (A3(s, i, j, k) - A3(s, i, j - 1, k)) * rdy * VF(j);
+        }
+      }
+      for (int j = 1; j <= nj; j++) {
+        for (int k = 2; k <= nk; k++) for (int i = 1; i <= ni; i++)
+          A3(dumz, i, j, k) = -(A3(kmv, i, j, k) * prinv) * (A3(s, i, j, k) - A3(s, i, j, k - 1)) * rdz * A3(g->mf, i, j, k) *
+                              A3(rf, i, j, k);
+        for (int i = 1; i <= ni; i++) {
+          if (bcturbs == 1) { A3(dumz, i, j, 1) = 0.0f; A3(dumz, i, j, nk + 1) = 0.0f; }
+          else { A3(dumz, i, j, 1) = A3(dumz, i, j, 2); A3(dumz, i, j, nk + 1) = A3(dumz, i, j, nk); }
+        }
+      }
+      for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++) {
+        float tx = -(A3(dumx, i + 1, j, k) - A3(dumx, i, j, k)) * rdx * UH(i);
+        float ty = -(A3(t13, i, j + 1, k) - A3(t13, i, j, k)) * rdy * VH(j);
+        float tz = -(A3(dumz, i, j, k + 1) - A3(dumz, i, j, k)) * rdz * A3(g->mh, i, j, k);
+        A3(sten, i, j, k) = A3(sten, i, j, k) + ((tx + ty) + tz) * A3(rr, i, j, k);
+      }
+    }
+  }
+#undef SQ
+  if (kmh_out) memcpy(kmh_out, kmh.p, (size_t)nw * sizeof(float));
+  if (kmv_out) memcpy(kmv_out, kmv.p, (size_t)nw * sizeof(float));
+  free(buf);
+  return 0;
+}

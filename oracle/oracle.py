@@ -56,6 +56,7 @@ def lib():
         L.oracle_calcener.argtypes = [cfgp, grp] + [P] * 11 + [C.POINTER(C.c_double)]
         L.oracle_threads.restype = C.c_int
         L.oracle_diff2.argtypes = [cfgp, grp, C.c_float, C.c_int, C.c_int, C.c_int, P, P] + [P] * 13
+        L.oracle_turbsmag.argtypes = [cfgp, grp, C.c_float] + [C.c_int] * 4 + [P, P] + [P] * 13
         L.oracle_mp_driver.argtypes = [cfgp, grp, stp, C.c_float, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.oracle_statpack.argtypes = ([cfgp, grp, C.POINTER(StatOpts), C.c_double, C.c_float] + [P] * 10 +
                                       [C.POINTER(C.c_double)] * 3 + [P, C.POINTER(C.c_int)])
