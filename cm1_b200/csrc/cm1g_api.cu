@@ -2203,7 +2203,7 @@ extern "C" int cm1g_turbsmag(cm1g_ctx_t *c, float csm, int32_t tconfig, int32_t 
   if (thten1 && npt && (!pta || !ptten)) return set_err(CM1G_ERR_ARG, "turbsmag with tracers needs pta/ptten");
   const size_t ns = nS(g), nw = nW(g);
   if (!c->les) {
-    c->les = (float *)dalloc(c, (4 * ns + 6 * nw) * sizeof(float));
+    c->les = (float *)dalloc(c, (6 * ns + 6 * nw) * sizeof(float));
     if (!c->les) return set_err(CM1G_ERR_NOMEM, "turbsmag scratch");
   }
   ProfActive pa(c);
@@ -2226,6 +2226,7 @@ extern "C" int cm1g_turbsmag(cm1g_ctx_t *c, float csm, int32_t tconfig, int32_t 
   }
   float *p = c->les;
   a.t11 = p; p += ns; a.t22 = p; p += ns; a.t33 = p; p += ns; a.t12 = p; p += ns;
+  a.cx = p; p += ns; a.cy = p; p += ns;
   a.s13 = p; p += nw; a.s23 = p; p += nw; a.t13 = p; p += nw; a.t23 = p; p += nw;
   a.kmh = kmh ? S.in(kmh, nw, true) : p; p += nw;
   a.kmv = kmv ? S.in(kmv, nw, true) : p;

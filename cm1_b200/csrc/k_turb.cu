@@ -13,7 +13,8 @@
 //
 // Four launches: k_les_strain (rho*S_ij at every point), k_les_km (N^2, the
 // deformations and kmh/kmv, the halo ring evaluated at its periodic image),
-// k_les_stress (t_ij in place; t13/t23 with the bottom and top rows) and
+// k_les_stress (t_ij in place; t13/t23 with the bottom and top rows; the
+// scalar fluxes' face coefficients, shared by every scalar) and
 // k_les_tend (momentum and all scalars, blockIdx.z over levels and fields).
 // Binary32 in the Fortran's evaluation order (--fmad=false); the logarithm
 // of calcnm and the cube root of tconfig=1 are evaluated in binary64 and
@@ -136,6 +137,14 @@ __global__ void k_les_stress(DGrid g, TurbArgs a) {
   }
   if (i < 1 || j < 1) return;
   const long ox = iS(g, i - 1, j, k), oy = iS(g, i, j - 1, k);
+  if (k <= nk) {
+    // turbs' face coefficients (turbtend.F:68-77): khh = kmh * prinv at the
+    // four points, summed as the Fortran does, times -0.125 (rho + rho); the
+    // Fortran's left-to-right product forms this factor first
+    const float pr = a.prinv;
+    a.cx[o] = -0.125f * (a.rho[o] + a.rho[ox]) * ((kmh[o] * pr + kmh[ox] * pr) + (kmh[o + pl] * pr + kmh[ox + pl] * pr));
+    a.cy[o] = -0.125f * (a.rho[o] + a.rho[oy]) * ((kmh[o] * pr + kmh[oy] * pr) + (kmh[o + pl] * pr + kmh[oy + pl] * pr));
+  }
   if (k >= 2 && k <= nk) {
     a.t13[o] = a.s13[o] * (kmv[ox] + kmv[o]);
     a.t23[o] = a.s23[o] * (kmv[oy] + kmv[o]);
@@ -170,18 +179,15 @@ __device__ __forceinline__ float les_s(const DGrid &g, const float *s, bool th, 
   return th ? (LDG(&g.th0[k]) - 300.0f) + v : v;
 }
 
-// x/y flux dumx, dumy of turbs (turbtend.F:66-78)
+// x/y flux dumx, dumy of turbs (turbtend.F:66-78): the face coefficient
+// times the difference, rdx and the metric, in the Fortran's order
 __device__ __forceinline__ float les_sfx(const DGrid &g, const TurbArgs &a, const float *s, bool th, int i, int j, int k,
                                          bool ydir) {
-  const long pl = (long)g.NI * g.NJ;
   const int im = ydir ? i : i - 1, jm = ydir ? j - 1 : j;
-  const long o = iS(g, i, j, k), om = iS(g, im, jm, k);
-  const float kh = a.prinv;
-  // khh = kmh * prinv at each of the four points, summed as the Fortran does
-  const float khs = (a.kmh[o] * kh + a.kmh[om] * kh) + (a.kmh[o + pl] * kh + a.kmh[om + pl] * kh);
+  const long o = iS(g, i, j, k);
   const float met = ydir ? LDG(&g.vf[j - g.jb]) : LDG(&g.uf[i - g.ib]);
-  return -0.125f * (a.rho[o] + a.rho[om]) * khs * (les_s(g, s, th, i, j, k) - les_s(g, s, th, im, jm, k)) *
-         (ydir ? g.rdy : g.rdx) * met;
+  return (ydir ? a.cy[o] : a.cx[o]) * (les_s(g, s, th, i, j, k) - les_s(g, s, th, im, jm, k)) * (ydir ? g.rdy : g.rdx) *
+         met;
 }
 
 // vertical flux dumz of turbsz, explicit (turbtend.F:480-510)
@@ -251,6 +257,7 @@ __global__ void k_les_tend(DGrid g, TurbArgs a) {
 }
 
 void launch_turbsmag(const DGrid &g, const TurbArgs &a, cudaStream_t st, int64_t *nl) {
+  // one row of 128 points per block (32 x 8 blocks measured no faster)
   const int bx = 128;
   {
     dim3 grid((g.ni + 2 + bx - 1) / bx, g.nj + 2, g.nk);

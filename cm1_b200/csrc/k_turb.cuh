@@ -18,6 +18,9 @@ struct TurbArgs {
   // scratch: rho*S_ij, then the stresses (s-shaped t11, t22, t33, t12 in
   // place; w-shaped t13, t23 formed from s13, s23); kmh, kmv (w-shaped)
   float *t11, *t22, *t33, *t12, *s13, *s23, *t13, *t23, *kmh, *kmv;
+  // face coefficients of turbs' x/y fluxes, -0.125*(rho+rho)*(sum of khh)
+  // (s-shaped, faces i or j = 1 .. n+1), shared by every scalar
+  float *cx, *cy;
 };
 
 void launch_turbsmag(const DGrid &g, const TurbArgs &a, cudaStream_t st, int64_t *nl);
