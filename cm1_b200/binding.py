@@ -66,7 +66,9 @@ def lib():
     L.cm1g_advs.argtypes = [ctxp, C.c_int32, C.c_int32, _P, _P, _P, _P, _P, _P, _P, C.c_int32, C.c_int32,
                             C.c_float, C.c_double]
     L.cm1g_advuvw.argtypes = [ctxp, C.c_int32, _P, _P, _P, _P, _P, _P]
-    L.cm1g_sound.argtypes = [ctxp, C.c_int32, C.c_float, C.c_float] + [_P] * 23
+    for n in ("cm1g_advu", "cm1g_advv", "cm1g_advw"):
+        getattr(L, n).argtypes = [ctxp, C.c_int32, _P, _P, _P, _P]
+    L.cm1g_sound.argtypes = [ctxp, C.c_float] + [_P] * 23 + [C.c_int32, C.c_float]
     L.cm1g_calcmass.argtypes = [ctxp, _P, C.POINTER(C.c_double)]
     L.cm1g_maxmin.argtypes = [ctxp, _P, C.c_int32, _P, _P, C.POINTER(C.c_int32)]
     L.cm1g_profile.argtypes = [ctxp, C.c_int32]
@@ -274,17 +276,29 @@ class Context:
         else:
             check(f[which](self.h, ptr(a)))
 
-    def advs(self, nrk, wflag, rru, rrv, rrw, divx, s0, s, sten, pdef, pdefweno, dt, weps):
-        check(lib().cm1g_advs(self.h, nrk, wflag, ptr(rru), ptr(rrv), ptr(rrw), ptr(divx), ptr(s0), ptr(s),
+    def advs(self, nrk, wflag, divx, rru, rrv, rrw, s0, s, sten, pdef, pdefweno, dt, weps):
+        """advs (adv.F:14-19): the kept arguments in the reference's order."""
+        check(lib().cm1g_advs(self.h, nrk, wflag, ptr(divx), ptr(rru), ptr(rrv), ptr(rrw), ptr(s0), ptr(s),
                               ptr(sten), pdef, pdefweno, dt, weps))
 
     def advuvw(self, nrk, u, v, w, uten, vten, wten):
         check(lib().cm1g_advuvw(self.h, nrk, ptr(u), ptr(v), ptr(w), ptr(uten), ptr(vten), ptr(wten)))
 
+    def advu(self, nrk, u3d, uten, v3d, w3d):
+        check(lib().cm1g_advu(self.h, nrk, ptr(u3d), ptr(uten), ptr(v3d), ptr(w3d)))
+
+    def advv(self, nrk, v3d, vten, u3d, w3d):
+        check(lib().cm1g_advv(self.h, nrk, ptr(v3d), ptr(vten), ptr(u3d), ptr(w3d)))
+
+    def advw(self, nrk, w3d, wten, u3d, v3d):
+        check(lib().cm1g_advw(self.h, nrk, ptr(w3d), ptr(wten), ptr(u3d), ptr(v3d)))
+
+    SOUND_ARRAYS = ["radbcw", "radbce", "radbcs", "radbcn", "rru", "ua", "u3d", "uten", "rrv", "va", "v3d", "vten",
+                    "rrw", "wa", "w3d", "wten", "ppi", "pp3d", "piadv", "ppten", "ppx", "thv", "ppterm"]
+
     def sound(self, nrk, dt, dttmp, **a):
-        names = ["ua", "u3d", "uten", "va", "v3d", "vten", "wa", "w3d", "wten", "ppi", "pp3d", "piadv", "ppten",
-                 "ppx", "thv", "ppterm", "rru", "rrv", "rrw", "radbcw", "radbce", "radbcs", "radbcn"]
-        check(lib().cm1g_sound(self.h, nrk, dt, dttmp, *[ptr(a[n]) for n in names]))
+        """sound (sound.F:10-24): arrays by name, passed in the reference's order."""
+        check(lib().cm1g_sound(self.h, dt, *[ptr(a[n]) for n in self.SOUND_ARRAYS], nrk, dttmp))
 
     def pdefq(self, rmax, rho, q):
         asq = C.c_double(0.0)

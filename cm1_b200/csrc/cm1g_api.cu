@@ -39,7 +39,7 @@ void launch_calcener(const DGrid &g, const EnerIn &e, double *part, double *out,
 void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w, const float *uten1,
                          const float *vten1, const float *wten1, float *uten, float *vten, float *wten,
                          const float *th3d, const float *qv, float *divx, cudaStream_t st, int64_t *nl,
-                         const Diff6 *diff = nullptr, const float *b8 = nullptr);
+                         const Diff6 *diff = nullptr, const float *b8 = nullptr, int which = 7);
 void launch_advs(const DGrid &g, const float *rru, const float *rrv, const float *rrw, int weighted,
                  const float *divx, const float *s, const float *s0, int sadd, const float *ten1,
                  const float *thterm, float *sten_out, float *snew, int weno, int pdef, int pdefweno,
@@ -253,6 +253,8 @@ extern "C" int cm1g_version(int32_t *major, int32_t *minor) {
 static int check_config(const cm1g_config_t *c) {
   if (c->ni < 4 || c->nj < 4 || c->nk < 6) return set_err(CM1G_ERR_ARG, "grid too small (ni,nj>=4, nk>=6)");
   if (c->ngxy < 3) return set_err(CM1G_ERR_ARG, "ngxy must be >= 3 for 5th order");
+  // the per-point kernels index rows with a launch grid's y extent
+  if (c->nj + 2 * c->ngxy > 65535) return set_err(CM1G_ERR_UNSUPPORTED, "nj > %d rows is not built", 65535 - 2 * c->ngxy);
   if (c->nk > sound_max_nk()) return set_err(CM1G_ERR_UNSUPPORTED, "nk > %d levels is not built", sound_max_nk());
   if (c->psolver != 3) return set_err(CM1G_ERR_UNSUPPORTED, "psolver=%d: only 3 (sound.F) is built", c->psolver);
   if (c->terrain_flag || c->axisymm || c->icor)
@@ -1309,8 +1311,8 @@ extern "C" int cm1g_bcu(cm1g_ctx_t *c, float *u) { return bc_entry(c, u, 3, 0); 
 extern "C" int cm1g_bcv(cm1g_ctx_t *c, float *v) { return bc_entry(c, v, 4, 0); }
 extern "C" int cm1g_bcw(cm1g_ctx_t *c, float *w, int32_t flag) { return bc_entry(c, w, 5, flag); }
 
-extern "C" int cm1g_advs(cm1g_ctx_t *c, int32_t nrk, int32_t wflag, const float *rru, const float *rrv,
-                         const float *rrw, const float *divx, const float *s0, const float *s, float *sten,
+extern "C" int cm1g_advs(cm1g_ctx_t *c, int32_t nrk, int32_t wflag, const float *divx, const float *rru,
+                         const float *rrv, const float *rrw, const float *s0, const float *s, float *sten,
                          int32_t pdef, int32_t pdefweno, float dt, double weps) {
   if (!c || !rru || !rrv || !rrw || !divx || !s || !sten || (pdef && !s0)) return set_err(CM1G_ERR_ARG, "null argument");
   if (nrk < 1 || nrk > 3) return set_err(CM1G_ERR_ARG, "nrk must be 1..3");
@@ -1334,26 +1336,55 @@ extern "C" int cm1g_advs(cm1g_ctx_t *c, int32_t nrk, int32_t wflag, const float 
   return S.finish();
 }
 
-extern "C" int cm1g_advuvw(cm1g_ctx_t *c, int32_t nrk, const float *u3d, const float *v3d, const float *w3d,
-                           float *uten, float *vten, float *wten) {
-  (void)nrk;
-  if (!c || !u3d || !v3d || !w3d || !uten || !vten || !wten) return set_err(CM1G_ERR_ARG, "null argument");
+// Momentum advection of the components selected by `which` (bit 0 u, 1 v,
+// 2 w); null tendencies are allowed for the components not selected.
+static int adv_momentum_entry(cm1g_ctx_t *c, int which, const float *u3d, const float *v3d, const float *w3d,
+                              float *uten, float *vten, float *wten) {
+  if (!c || !u3d || !v3d || !w3d) return set_err(CM1G_ERR_ARG, "null argument");
+  if (((which & 1) && !uten) || ((which & 2) && !vten) || ((which & 4) && !wten))
+    return set_err(CM1G_ERR_ARG, "null argument");
   ProfActive pa(c);
   Stager S(c);
   const DGrid &g = c->g;
   const float *du = S.in(u3d, nU(g), false), *dv = S.in(v3d, nV(g), false), *dw = S.in(w3d, nW(g), false);
-  float *tu = S.in(uten, nU(g), true), *tv = S.in(vten, nV(g), true), *tw = S.in(wten, nW(g), true);
-  launch_adv_momentum(g, du, dv, dw, tu, tv, tw, tu, tv, tw, nullptr, nullptr, c->mdivx, c->stream, &c->nlaunch);
+  float *tu = (which & 1) ? S.in(uten, nU(g), true) : nullptr;
+  float *tv = (which & 2) ? S.in(vten, nV(g), true) : nullptr;
+  float *tw = (which & 4) ? S.in(wten, nW(g), true) : nullptr;
+  if (S.err) return set_err(CM1G_ERR_NOMEM, "staging");
+  launch_adv_momentum(g, du, dv, dw, tu, tv, tw, tu, tv, tw, nullptr, nullptr, c->mdivx, c->stream, &c->nlaunch,
+                      nullptr, nullptr, which);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));
   return S.finish();
 }
 
-extern "C" int cm1g_sound(cm1g_ctx_t *c, int32_t nrk, float dt, float dttmp, float *ua, float *u3d,
-                          const float *uten, float *va, float *v3d, const float *vten, float *wa, float *w3d,
-                          const float *wten, float *ppi, float *pp3d, const float *piadv, const float *ppten,
-                          float *ppx, const float *thv, const float *ppterm, float *rru, float *rrv, float *rrw,
-                          float *radbcw, float *radbce, float *radbcs, float *radbcn) {
+extern "C" int cm1g_advuvw(cm1g_ctx_t *c, int32_t nrk, const float *u3d, const float *v3d, const float *w3d,
+                           float *uten, float *vten, float *wten) {
+  (void)nrk;
+  return adv_momentum_entry(c, 7, u3d, v3d, w3d, uten, vten, wten);
+}
+extern "C" int cm1g_advu(cm1g_ctx_t *c, int32_t nrk, const float *u3d, float *uten, const float *v3d,
+                         const float *w3d) {
+  (void)nrk;
+  return adv_momentum_entry(c, 1, u3d, v3d, w3d, uten, nullptr, nullptr);
+}
+extern "C" int cm1g_advv(cm1g_ctx_t *c, int32_t nrk, const float *v3d, float *vten, const float *u3d,
+                         const float *w3d) {
+  (void)nrk;
+  return adv_momentum_entry(c, 2, u3d, v3d, w3d, nullptr, vten, nullptr);
+}
+extern "C" int cm1g_advw(cm1g_ctx_t *c, int32_t nrk, const float *w3d, float *wten, const float *u3d,
+                         const float *v3d) {
+  (void)nrk;
+  return adv_momentum_entry(c, 4, u3d, v3d, w3d, nullptr, nullptr, wten);
+}
+
+extern "C" int cm1g_sound(cm1g_ctx_t *c, float dt, float *radbcw, float *radbce, float *radbcs, float *radbcn,
+                          float *rru, float *ua, float *u3d, const float *uten,
+                          float *rrv, float *va, float *v3d, const float *vten,
+                          float *rrw, float *wa, float *w3d, const float *wten,
+                          float *ppi, float *pp3d, const float *piadv, const float *ppten, float *ppx,
+                          const float *thv, const float *ppterm, int32_t nrk, float dttmp) {
   (void)dttmp;
   if (!c) return set_err(CM1G_ERR_STATE, "null context");
   if (nrk < 1 || nrk > 3) return set_err(CM1G_ERR_ARG, "nrk must be 1..3");

@@ -487,22 +487,22 @@ template <int TX, int TY, int KC>
 static void mom_tiles_shape(const DGrid &g, const Vel &q, const float *uten1, const float *vten1,
                             const float *wten1, float *uten, float *vten, float *wten, const float *th3d,
                             const float *qv, const float *b8, const float *divx, const Diff6 &df,
-                            cudaStream_t st) {
+                            cudaStream_t st, int which) {
   dim3 blk(TX, TY);
   const int kch = (g.nk + KC - 1) / KC, kchw = (g.nk - 1 + KC - 1) / KC;
-  {
+  if (which & 1) {
     dim3 grid((g.ni + 1 + TX - 1) / TX, (g.nj + TY - 1) / TY, kch);
     ProfScope _ps("k_advu", st);
     if (df.rho) k_mom_tile<TX, TY, KC, 2, 1><<<grid, blk, 0, st>>>(g, q, divx, uten1, uten, nullptr, nullptr, nullptr, df);
     else k_mom_tile<TX, TY, KC, 2, 0><<<grid, blk, 0, st>>>(g, q, divx, uten1, uten, nullptr, nullptr, nullptr, df);
   }
-  {
+  if (which & 2) {
     dim3 grid((g.ni + TX - 1) / TX, (g.nj + 1 + TY - 1) / TY, kch);
     ProfScope _ps("k_advv", st);
     if (df.rho) k_mom_tile<TX, TY, KC, 3, 1><<<grid, blk, 0, st>>>(g, q, divx, vten1, vten, nullptr, nullptr, nullptr, df);
     else k_mom_tile<TX, TY, KC, 3, 0><<<grid, blk, 0, st>>>(g, q, divx, vten1, vten, nullptr, nullptr, nullptr, df);
   }
-  {
+  if (which & 4) {
     dim3 grid((g.ni + TX - 1) / TX, (g.nj + TY - 1) / TY, kchw);
     ProfScope _ps("k_advw", st);
     if (df.rho) k_mom_tile<TX, TY, KC, 4, 1><<<grid, blk, 0, st>>>(g, q, divx, wten1, wten, th3d, qv, b8, df);
@@ -513,7 +513,9 @@ static void mom_tiles_shape(const DGrid &g, const Vel &q, const float *uten1, co
 void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const float *w,
                          const float *uten1, const float *vten1, const float *wten1,
                          float *uten, float *vten, float *wten, const float *th3d, const float *qv,
-                         float *divx, cudaStream_t st, int64_t *nl, const Diff6 *diff, const float *b8) {
+                         float *divx, cudaStream_t st, int64_t *nl, const Diff6 *diff, const float *b8,
+                         int which) {
+  // which: bit 0 u (advu), bit 1 v (advv), bit 2 w (advw)
   Vel q{u, v, w};
   const Diff6 df = diff ? *diff : Diff6{};
   {
@@ -524,7 +526,8 @@ void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const f
 #define CM1G_MOM_SHAPE(n)                                                                                     \
   case n:                                                                                                     \
     mom_tiles_shape<kTileShapes[n][0], kTileShapes[n][1], kTileShapes[n][2]>(g, q, uten1, vten1, wten1, uten, \
-                                                                             vten, wten, th3d, qv, b8, divx, df, st); \
+                                                                             vten, wten, th3d, qv, b8, divx, df, st, \
+                                                                             which);                                \
     break;
   switch (g.tile_mom) {
     CM1G_MOM_SHAPE(1)
@@ -534,7 +537,7 @@ void launch_adv_momentum(const DGrid &g, const float *u, const float *v, const f
     default: CM1G_MOM_SHAPE(0)
   }
 #undef CM1G_MOM_SHAPE
-  if (nl) *nl += 4;
+  if (nl) *nl += 1 + ((which & 1) != 0) + ((which & 2) != 0) + ((which & 4) != 0);
 }
 
 // ---------------------------------------------------------------------

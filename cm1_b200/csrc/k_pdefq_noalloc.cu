@@ -17,8 +17,16 @@
 // it, so nothing has to start at zero.
 //
 // The device address of the array is looked up once per device, on the first
-// call made with that device current (cudaGetSymbolAddress); make that first
-// call outside any stream capture.
+// call made with that device current (cudaGetSymbolAddress).  Every call
+// copies asq's increment back and synchronizes the stream, so no call can be
+// made while the stream is being captured into a CUDA graph.
+//
+// The columns are spread over a one-dimensional grid (one thread per column,
+// at most CM1G_PDEFQ_NOALLOC_MAX_COLUMNS / 128 = 8192 blocks), so any ni x nj
+// within the limit launches, however the columns split between i and j.  The
+// budget sum walks each row of columns in order on one thread (the order of
+// the context-based entry point): a grid of a few very long rows (ni of
+// 10^5-10^6) spends about a millisecond there.
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -49,9 +57,9 @@ __device__ __forceinline__ long sidx(const Dims &d, int i, int j, int k) {
 // one thread per column: pdefq's loops over k (misclibs.F:1063-1081)
 __global__ void k_pdefq_na(Dims d, float rmax, const float *__restrict__ ruh, const float *__restrict__ rvh,
                            const float *__restrict__ rmh, const float *__restrict__ rho, float *q, double *bud) {
-  const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int j = 1 + (int)blockIdx.y;
-  if (i > d.ni) return;
+  const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (j-1)*ni + (i-1)
+  if (col >= (long)d.ni * d.nj) return;
+  const int j = 1 + (int)(col / d.ni), i = 1 + (int)(col - (long)(j - 1) * d.ni);
   const float ru = ruh[i - d.ib], rv = rvh[j - d.jb];
   double t1 = 0.0, t2 = 0.0, a1 = 0.0, a2 = 0.0;
   for (int k = 1; k <= d.nk; k++) {
@@ -132,11 +140,15 @@ extern "C" int cm1g_pdefq_noalloc(const cm1g_config_t *cfg, float rmax, double *
   cudaStream_t st = (cudaStream_t)stream;
   Dims d{cfg->ni, cfg->nj, cfg->nk, cfg->ni + 2 * cfg->ngxy, cfg->nj + 2 * cfg->ngxy, 1 - cfg->ngxy, 1 - cfg->ngxy};
   double *bud = scratch, *out = scratch + CM1G_PDEFQ_NOALLOC_MAX_COLUMNS;
-  dim3 grid((d.ni + 127) / 128, d.nj);
-  k_pdefq_na<<<grid, 128, 0, st>>>(d, rmax, ruh, rvh, rmh, rho, q3d, bud);
+  const long ncol = (long)d.ni * d.nj;
+  k_pdefq_na<<<(unsigned)((ncol + 127) / 128), 128, 0, st>>>(d, rmax, ruh, rvh, rmh, rho, q3d, bud);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(CM1G_ERR_CUDA, cudaGetErrorString(e));
   k_pdefq_na_sum<<<1, 128, 0, st>>>(d, (double)(cfg->dx * cfg->dy * cfg->dz), bud, out);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(CM1G_ERR_CUDA, cudaGetErrorString(e));
   double h = 0.0;
-  cudaError_t e = cudaMemcpyAsync(&h, out, sizeof(double), cudaMemcpyDeviceToHost, st);
+  e = cudaMemcpyAsync(&h, out, sizeof(double), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return fail(CM1G_ERR_CUDA, cudaGetErrorString(e));
   if (asq) *asq += h;

@@ -179,6 +179,62 @@ module cm1g_iso
       real(c_float), intent(inout) :: w(*)
       integer(c_int32_t), value :: flag
     end function
+    ! advs (adv.F:14-19): the arguments kept, in advs's order
+    integer(c_int) function cm1g_advs(ctx, nrk, wflag, divx, rru, rrv, rrw, s0, s, sten, pdef, pdefweno, &
+                                      dt, weps) bind(C, name="cm1g_advs")
+      import :: c_int, c_int32_t, c_float, c_double, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: nrk, wflag, pdef, pdefweno
+      real(c_float), intent(in) :: divx(*), rru(*), rrv(*), rrw(*), s0(*), s(*)
+      real(c_float), intent(inout) :: sten(*)
+      real(c_float), value :: dt
+      real(c_double), value :: weps
+    end function
+    ! advu, advv, advw (adv.F:911-912, 1847-1848, 2778-2781): the arguments
+    ! kept, in each routine's order; rru/rrv/rrw/divx are formed on the device
+    integer(c_int) function cm1g_advu(ctx, nrk, u3d, uten, v3d, w3d) bind(C, name="cm1g_advu")
+      import :: c_int, c_int32_t, c_float, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: nrk
+      real(c_float), intent(in) :: u3d(*), v3d(*), w3d(*)
+      real(c_float), intent(inout) :: uten(*)
+    end function
+    integer(c_int) function cm1g_advv(ctx, nrk, v3d, vten, u3d, w3d) bind(C, name="cm1g_advv")
+      import :: c_int, c_int32_t, c_float, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: nrk
+      real(c_float), intent(in) :: v3d(*), u3d(*), w3d(*)
+      real(c_float), intent(inout) :: vten(*)
+    end function
+    integer(c_int) function cm1g_advw(ctx, nrk, w3d, wten, u3d, v3d) bind(C, name="cm1g_advw")
+      import :: c_int, c_int32_t, c_float, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: nrk
+      real(c_float), intent(in) :: w3d(*), u3d(*), v3d(*)
+      real(c_float), intent(inout) :: wten(*)
+    end function
+    ! solve2.F:883-893's three calls in one
+    integer(c_int) function cm1g_advuvw(ctx, nrk, u3d, v3d, w3d, uten, vten, wten) bind(C, name="cm1g_advuvw")
+      import :: c_int, c_int32_t, c_float, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: nrk
+      real(c_float), intent(in) :: u3d(*), v3d(*), w3d(*)
+      real(c_float), intent(inout) :: uten(*), vten(*), wten(*)
+    end function
+    ! sound (sound.F:10-24): the arguments kept, in sound's order
+    integer(c_int) function cm1g_sound(ctx, dt, radbcw, radbce, radbcs, radbcn, &
+                                       rru, ua, u3d, uten, rrv, va, v3d, vten, rrw, wa, w3d, wten, &
+                                       ppi, pp3d, piadv, ppten, ppx, thv, ppterm, nrk, dttmp) &
+        bind(C, name="cm1g_sound")
+      import :: c_int, c_int32_t, c_float, c_ptr
+      type(c_ptr), value :: ctx
+      real(c_float), value :: dt, dttmp
+      real(c_float), intent(inout) :: radbcw(*), radbce(*), radbcs(*), radbcn(*)
+      real(c_float), intent(inout) :: rru(*), ua(*), u3d(*), rrv(*), va(*), v3d(*), rrw(*), wa(*), w3d(*)
+      real(c_float), intent(in) :: uten(*), vten(*), wten(*), piadv(*), ppten(*), thv(*), ppterm(*)
+      real(c_float), intent(inout) :: ppi(*), pp3d(*), ppx(*)
+      integer(c_int32_t), value :: nrk
+    end function
     ! calcmass (misclibs.F:3134) and calcener (misclibs.F:3343): FP64 budgets
     integer(c_int) function cm1g_calcmass(ctx, rho, tmass) bind(C, name="cm1g_calcmass")
       import :: c_int, c_float, c_double, c_ptr

@@ -503,7 +503,7 @@ def main(argv=None):
     ap.add_argument("--widens", default="0,1", help="bound widenings of the face values to evaluate")
     ap.add_argument("--tests", type=int, default=2)
     ap.add_argument("--minutes", type=float, default=30.0)
-    ap.add_argument("--out", default="gpurun_out/closure")
+    ap.add_argument("--out", default="closure_out")
     ap.add_argument("--small", action="store_true", help="quarter-size grids (a quick end-to-end check)")
     args = ap.parse_args(argv)
     import torch

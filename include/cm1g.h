@@ -201,31 +201,50 @@ int cm1g_bcw(cm1g_ctx_t *ctx, float *w, int32_t flag);
  * divx their divergence, s0 the RK base value, s the advected field,
  * sten is incremented by the advective tendency (times rr0).  pdef selects
  * the positive-definite limiter (pdef.F), pdefweno the pdef form of the
- * vertical WENO (adv_routines.F:2359-2433).  All arrays device or host. */
+ * vertical WENO (adv_routines.F:2359-2433).  All arrays device or host.
+ * The arguments kept are those of adv.F:14-19 in their order there (nrk,
+ * wflag, ..., divx, rru, rrv, rrw, s0, s, sten, pdef, pdefweno, dt, weps);
+ * grid metrics and scratch arrays come from the context. */
 int cm1g_advs(cm1g_ctx_t *ctx, int32_t nrk, int32_t wflag,
-              const float *rru, const float *rrv, const float *rrw,
-              const float *divx, const float *s0, const float *s, float *sten,
+              const float *divx, const float *rru, const float *rrv, const float *rrw,
+              const float *s0, const float *s, float *sten,
               int32_t pdef, int32_t pdefweno, float dt, double weps);
 
-/* Momentum advection tendencies: replaces advu, advv, advw (src/adv.F:911,
- * 1847, 2778) with hadvordrv=vadvordrv=5: uten/vten/wten are incremented by
- * the flux-form advection of u3d/v3d/w3d by rho0*(u,v,w).  Advection only:
+/* Momentum advection tendencies, one routine each: replace advu, advv and
+ * advw (src/adv.F:911-912, 1847-1848, 2778-2781) with hadvordrv=vadvordrv=5.
+ * The tendency of the routine's component is incremented by the flux-form
+ * advection of that component.  The arguments kept are the reference's, in
+ * its order (advu: nrk, ..., u3d, uten, ..., v3d, w3d; advv: nrk, ..., v3d,
+ * vten, ..., u3d, w3d; advw: nrk, ..., w3d, wten, ..., u3d, v3d).  The mass
+ * fluxes rru/rrv/rrw and their divergence divx, which solve2 forms from
+ * u3d/v3d/w3d just before these calls (solve2.F:490-628), are formed on the
+ * device from the same velocities, so they are not passed.  Advection only:
  * the 6th-order diffusion of idiff=1 (which needs rho and dt) runs inside
  * cm1g_solve2 / cm1g_step. */
+int cm1g_advu(cm1g_ctx_t *ctx, int32_t nrk, const float *u3d, float *uten,
+              const float *v3d, const float *w3d);
+int cm1g_advv(cm1g_ctx_t *ctx, int32_t nrk, const float *v3d, float *vten,
+              const float *u3d, const float *w3d);
+int cm1g_advw(cm1g_ctx_t *ctx, int32_t nrk, const float *w3d, float *wten,
+              const float *u3d, const float *v3d);
+/* The three calls of solve2.F:883-893 in one: advu, advv and advw of the
+ * same velocities (no single reference routine has this argument list). */
 int cm1g_advuvw(cm1g_ctx_t *ctx, int32_t nrk, const float *u3d, const float *v3d,
                 const float *w3d, float *uten, float *vten, float *wten);
 
 /* Acoustic substeps of one RK stage: replaces sound (src/sound.F:10-857)
  * with psolver=3.  thv = theta_rho (t11), ppterm (t22), piadv (pi0+pp').
- * On return rru/rrv/rrw hold the small-step-averaged velocities. */
-int cm1g_sound(cm1g_ctx_t *ctx, int32_t nrk, float dt, float dttmp,
-               float *ua, float *u3d, const float *uten,
-               float *va, float *v3d, const float *vten,
-               float *wa, float *w3d, const float *wten,
-               float *ppi, float *pp3d, const float *piadv, const float *ppten,
-               float *ppx, const float *thv, const float *ppterm,
-               float *rru, float *rrv, float *rrw,
-               float *radbcw, float *radbce, float *radbcs, float *radbcn);
+ * On return rru/rrv/rrw hold the small-step-averaged velocities.  The
+ * arguments kept are those of sound.F:10-24 in their order there; grid
+ * metrics, the base state and the work arrays (dum1..dum4, mm, ppd, fpk, qk,
+ * pk1, pk2) come from the context. */
+int cm1g_sound(cm1g_ctx_t *ctx, float dt,
+               float *radbcw, float *radbce, float *radbcs, float *radbcn,
+               float *rru, float *ua, float *u3d, const float *uten,
+               float *rrv, float *va, float *v3d, const float *vten,
+               float *rrw, float *wa, float *w3d, const float *wten,
+               float *ppi, float *pp3d, const float *piadv, const float *ppten, float *ppx,
+               const float *thv, const float *ppterm, int32_t nrk, float dttmp);
 
 /* Domain-integrated dry-air mass, FP64 accumulation: replaces calcmass
  * (src/misclibs.F:3134-3191).  tmass = sum(rho*dV). */
@@ -488,9 +507,12 @@ int cm1g_capture_fluxes(cm1g_ctx_t *ctx, float *fx, float *fy, float *rx, float 
  * lives in a fixed file-scope device array shared by every call in the
  * process: calls that may overlap on one GPU must be serialized by the
  * caller.  The first call with a given device current looks the array's
- * address up (cudaGetSymbolAddress); make that call before any stream capture.
- * ni*nj above CM1G_PDEFQ_NOALLOC_MAX_COLUMNS returns CM1G_ERR_ARG.  The call
- * synchronizes stream to read asq back. */
+ * address up (cudaGetSymbolAddress).  Every call synchronizes `stream` to
+ * read asq back, so it cannot be made while that stream is being captured
+ * into a CUDA graph.  Any ni x nj up to CM1G_PDEFQ_NOALLOC_MAX_COLUMNS
+ * columns is accepted (the columns are spread over a one-dimensional grid);
+ * more returns CM1G_ERR_ARG, and a failed launch returns CM1G_ERR_CUDA
+ * before asq is touched. */
 int cm1g_pdefq_noalloc(const cm1g_config_t *cfg, float rmax, double *asq,
                        const float *ruh, const float *rvh, const float *rmh,
                        const float *rho, float *q3d, void *stream);

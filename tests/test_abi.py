@@ -57,6 +57,75 @@ def test_version(cm1g):
     assert (a.value, b.value) == (0, 1)
 
 
+# Argument lists of the reference routines the per-routine entry points
+# replace, as declared (src/adv.F:14-19, 911-912, 1847-1848, 2778-2781;
+# src/sound.F:10-24; src/misclibs.F:1037).
+REFERENCE_ARGS = {
+    "advs": "nrk,wflag,bflag,bsq,xh,rxh,arh1,arh2,uh,ruh,xf,vh,rvh,gz,rgz,mh,rmh,rho0,rr0,rf0,rrf0,advx,advy,"
+            "advz,dumx,dumy,dumz,mass,subs,divx,rru,rrv,rrw,s0,s,sten,pdef,pdefweno,dt,weps,flag,sw31,sw32,se31,"
+            "se32,ss31,ss32,sn31,sn32,rdsf,c1,c2,rho,ri,diffit,dobud,ibd,ied,jbd,jed,kbd,ked,ndiag,diag,sd_hadv,"
+            "sd_vadv,sd_lsw,sd_hidiff,sd_vidiff,sd_hediff,wprof,dumk1,dumk2,hadvorder,vadvorder,kbdy,bndy,hflxw,"
+            "hflxe,hflxs,hflxn,out3d",
+    "advu": "nrk,arh1,arh2,uh,xf,rxf,arf1,arf2,uf,vh,gz,rgz,gzu,mh,rho0,rr0,rf0,rrf0,dumx,dumy,dumz,advx,advy,"
+            "advz,subs,divx,rru,u3d,uten,rrv,rrw,rdsf,c1,c2,rho,dt,doubud,udiag,wprof,bndy,kbdy,hflxw,hflxe,hflxs,"
+            "hflxn,vf,mf,v3d,w3d",
+    "advv": "nrk,xh,rxh,arh1,arh2,uh,xf,vh,vf,gz,rgz,gzv,mh,rho0,rr0,rf0,rrf0,dumx,dumy,dumz,advx,advy,advz,subs,"
+            "divx,rru,rrv,v3d,vten,rrw,rdsf,c1,c2,rho,dt,dovbud,vdiag,wprof,bndy,kbdy,hflxw,hflxe,hflxs,hflxn,uf,"
+            "mf,u3d,w3d",
+    "advw": "nrk,xh,rxh,arh1,arh2,uh,xf,vh,gz,rgz,mh,mf,rho0,rr0,rf0,rrf0,dumx,dumy,dumz,advx,advy,advz,subs,"
+            "divx,rru,rrv,rrw,w3d,wten,rds,rdsf,c1,c2,rho,dt,dowbud,wdiag,hadvorder,vadvorder,advweno,bndy,kbdy,uf,"
+            "vf,u3d,v3d,hflxw,hflxe,hflxs,hflxn,iamw",
+    "sound": "dt,xh,arh1,arh2,uh,ruh,xf,uf,yh,vh,rvh,yf,vf,rds,sigma,rdsf,sigmaf,zh,mh,rmh,c1,c2,mf,zf,pi0,rho0,"
+             "rr0,rf0,rrf0,th0,rth0,zs,gz,rgz,gzu,rgzu,gzv,rgzv,dzdx,dzdy,gx,gxu,gy,gyv,radbcw,radbce,radbcs,"
+             "radbcn,dtu,dtu0,dtv,dtv0,dum1,dum2,dum3,dum4,mm,bk,ppd,fpk,qk,pk1,pk2,wtens,u0,rru,ua,u3d,uten,v0,"
+             "rrv,va,v3d,vten,rrw,wa,w3d,wten,ppi,pp3d,piadv,ppten,ppx,thv,ppterm,nrk,dttmp,rtime,mtime,"
+             "get_time_avg,bndy,kbdy,pw1,pw2,pe1,pe2,ps1,ps2,pn1,pn2,reqs_p",
+    "pdefq": "rmax,asq,ruh,rvh,rmh,rho,q3d",
+}
+# C entry point -> the reference routine whose argument order it keeps
+ENTRY_ROUTINE = {"cm1g_advs": "advs", "cm1g_advu": "advu", "cm1g_advv": "advv", "cm1g_advw": "advw",
+                 "cm1g_sound": "sound", "cm1g_pdefq": "pdefq", "cm1g_pdefq_noalloc": "pdefq"}
+# arguments of the C entries that carry no reference argument
+NOT_REFERENCE = {"ctx", "cfg", "stream"}
+
+
+def c_arguments(name):
+    src = re.sub(r"/\*.*?\*/", " ", open(HEADER).read(), flags=re.S)
+    m = re.search(r"\bint\s+%s\s*\(([^;]*?)\)\s*;" % name, src, flags=re.S)
+    assert m, name
+    out = []
+    for a in m.group(1).split(","):
+        out.append(re.findall(r"[A-Za-z_][A-Za-z0-9_]*", a.split("[")[0])[-1])
+    return out
+
+
+def fortran_arguments(name):
+    src = open(os.path.join(ROOT, "cm1_b200", "fortran", "cm1g_iso.F90")).read().replace("&\n", " ")
+    m = re.search(r"function\s+%s\s*\(([^)]*)\)" % name, src)
+    assert m, name
+    return [a.strip() for a in m.group(1).split(",")]
+
+
+@pytest.mark.parametrize("entry", sorted(ENTRY_ROUTINE))
+def test_entry_keeps_reference_argument_order(entry):
+    """Every argument an entry point shares with its reference routine is a
+    reference argument, and they come in the reference's order."""
+    ref = REFERENCE_ARGS[ENTRY_ROUTINE[entry]].split(",")
+    kept = [a for a in c_arguments(entry) if a not in NOT_REFERENCE]
+    assert kept, entry
+    missing = [a for a in kept if a not in ref]
+    assert not missing, (entry, missing)
+    pos = [ref.index(a) for a in kept]
+    assert pos == sorted(pos), (entry, kept)
+
+
+@pytest.mark.parametrize("entry", ["cm1g_advs", "cm1g_advu", "cm1g_advv", "cm1g_advw", "cm1g_sound",
+                                   "cm1g_pdefq"])
+def test_fortran_interface_matches_header(entry):
+    """The ISO_C_BINDING interface lists the C arguments in the same order."""
+    assert fortran_arguments(entry) == c_arguments(entry)
+
+
 def test_oracle_header_and_threads(oracle_lib):
     assert oracle_lib.threads() >= 1
     assert "parity unpinned" in open(os.path.join(ROOT, "oracle", "cm1_oracle.c")).read().lower()

@@ -81,7 +81,7 @@ def test_advs(bc, weno, pdef, pdefweno, cm1g, oracle_lib):
     assert rc == 0
     ctx = cm1g.Context(case.cfg, case.grid)
     d = cm1g.to_device(dict(rru=rru, rrv=rrv, rrw=rrw, divx=divx, s0=s0, s=s, sten=sten))
-    ctx.advs(3, 1, d["rru"], d["rrv"], d["rrw"], d["divx"], d["s0"], d["s"], d["sten"], pdef, pdefweno, case.dt, weps)
+    ctx.advs(3, 1, d["divx"], d["rru"], d["rrv"], d["rrw"], d["s0"], d["s"], d["sten"], pdef, pdefweno, case.dt, weps)
     got = d["sten"].cpu().numpy()
     sl = case.lay.interior(1)
     e = relerr(got[sl], ref[sl])
@@ -116,6 +116,13 @@ def test_advuvw(bc, cm1g, oracle_lib):
     assert relerr(d["vt"].cpu().numpy()[sv], rvt[sv]) <= 1e-6
     sw = (slice(lay.kx(2), lay.kx(lay.nk) + 1), slice(lay.jx(1), lay.jx(lay.nj) + 1), slice(lay.ix(1), lay.ix(lay.ni) + 1))
     assert relerr(d["wt"].cpu().numpy()[sw], rwt[sw]) <= 1e-6
+    # the per-routine entries (advu, advv, advw) give the combined call's tendencies bit for bit
+    e = cm1g.to_device(dict(u=u, v=v, w=w, ut=ut, vt=vt, wt=wt))
+    ctx.advu(1, e["u"], e["ut"], e["v"], e["w"])
+    ctx.advv(1, e["v"], e["vt"], e["u"], e["w"])
+    ctx.advw(1, e["w"], e["wt"], e["u"], e["v"])
+    for n in ("ut", "vt", "wt"):
+        assert np.array_equal(e[n].cpu().numpy(), d[n].cpu().numpy()), n
 
 
 @pytest.mark.parametrize("form", ["tile", "col"])
