@@ -5,7 +5,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = ["cm1g_api.cu", "k_adv.cu", "k_sound.cu", "k_bc.cu", "k_misc.cu", "k_pdefq_noalloc.cu", "k_learned.cu", "k_stat.cu", "k_micro.cu", "k_io.cu", "k_diff2.cu", "k_turb.cu"]
+SRC = ["cm1g_api.cu", "k_adv.cu", "k_scal.cu", "k_sound.cu", "k_bc.cu", "k_misc.cu", "k_pdefq_noalloc.cu", "k_learned.cu", "k_stat.cu", "k_micro.cu", "k_io.cu", "k_diff2.cu", "k_turb.cu"]
 LIB = os.path.join(HERE, "libcm1g.so")
 
 # --fmad=false: keep every binary32 product and sum rounded separately, as

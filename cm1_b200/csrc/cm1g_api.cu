@@ -48,6 +48,9 @@ void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const
                        const float *s0, int sadd, const float *ten1, const float *thterm, float *snew, int weno,
                        int pdef, int pdefweno, double weps, float dt, int flush, float *scratch, cudaStream_t st,
                        int64_t *nl, const TileExtras *ex = nullptr, const Diff6 *diff = nullptr);
+void launch_scal_pass(const DGrid &g, const ScalField *f, int n, const float *rru, const float *rrv,
+                      const float *rrw, const float *thterm, int weno, float dt, int *err, cudaStream_t st,
+                      int64_t *nl);
 void launch_sound(const DGrid &g, int nsound, int nrk, float dt, const float *ua, float *u3d, const float *uten,
                   const float *va, float *v3d, const float *vten, const float *wa, float *w3d, const float *wten,
                   const float *ppi, float *pp3d, const float *piadv, const float *ppten, float *ppx,
@@ -164,6 +167,9 @@ struct cm1g_ctx {
   long cl_nf[2] = {0, 0};
   // capture of theta's final-stage face fluxes (cm1g_capture_fluxes)
   float *cap_fx = nullptr, *cap_fy = nullptr, *cap_rx = nullptr, *cap_ry = nullptr;
+  // the scalar fields of a stage in one fused launch (k_scal_tile); off: one
+  // k_advs_tile launch per field (CM1G_SCALAR_PASS=perfield, for comparisons)
+  bool scal_fused = true;
   double *part3 = nullptr, *part4 = nullptr, *dscal = nullptr, *bud = nullptr, *lev = nullptr;
   double *ener = nullptr;                     // calcener chunk sums (4 x nk x chunks) and results
   float *fscal = nullptr;
@@ -398,7 +404,11 @@ extern "C" int cm1g_init(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_c
   c->bud = (double *)dalloc(c, (size_t)g.ni * g.nj * sizeof(double));
   c->lev = (double *)dalloc(c, (size_t)(g.nk + 2) * sizeof(double));
   c->fscal = (float *)dalloc(c, 16 * sizeof(float));
-  c->cflbits = (int *)dalloc(c, 16 * sizeof(int));
+  c->cflbits = (int *)dalloc(c, 16 * sizeof(int));   // [0] max CFL bits, [1] staging-wait error of k_scal_tile
+  {
+    const char *sp = getenv("CM1G_SCALAR_PASS");
+    c->scal_fused = !(sp && strcmp(sp, "perfield") == 0);
+  }
   c->mm = (unsigned long long *)dalloc(c, 4 * sizeof(unsigned long long));
   if (cfg->ptype == 1) {
     c->b8 = (float *)dalloc(c, bS);
@@ -597,6 +607,30 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
     if (nrk == 3) launch_cfl(g, d->u3d, d->v3d, d->w3d, dt, c->cflbits, st, nl);
     if (openrad) launch_radbc4(g, d->ua, d->u3d, d->va, d->v3d, d->radbcw, d->radbce, d->radbcs, d->radbcn, dttmp, st, nl);
     const int weno = (cf.advwenos == 1 || (cf.advwenos == 2 && nrk == 3)) ? 1 : 0;
+    // Every field whose stage is a plain update (theta; moisture and tracers
+    // except at the final stage's positive-definite pass) in one fused launch;
+    // the fields are independent given rru/rrv/rrw, so this equals the
+    // reference's sequence of advs calls.  The 6th-order diffusion, the
+    // learned closure and the flux capture use the per-field tiles below.
+    const bool fused = c->scal_fused && !diffit && !c->cl_on && !(nrk == 3 && c->cap_fx);
+    std::vector<char> done(nsc, 0);
+    if (fused) {
+      std::vector<ScalField> fl;
+      auto add = [&](int s, int sadd, double weps, int flush, int pdefweno) {
+        ScalField f{};
+        f.s = buf_in(s, nrk); f.sbase = base[s]; f.ten1 = ten1[s]; f.snew = buf_out(s, nrk);
+        f.weps = weps; f.sadd = sadd; f.flush = flush; f.pdefweno = pdefweno;
+        fl.push_back(f);
+        done[s] = 1;
+      };
+      add(0, 1, (double)(10.0f * 1.0e-18f), 1, 0);
+      for (int n = 0; n < numq; n++)
+        if (nrk < 3) add(1 + n, 0, (double)(cf.qmag[n] * 1.0e-18f), 1, (n + 1 == cf.nqv) ? 0 : 1);
+      for (int n = 0; n < npt; n++)
+        if (!(nrk == 3 && cf.pdtra == 1)) add(1 + numq + n, 0, (double)(1.0f * 1.0e-18f), 0, 1);
+      launch_scal_pass(g, fl.data(), (int)fl.size(), c->rru, c->rrv, c->rrw,
+                       (cf.imoist && cf.eqtset == 2) ? c->thterm : nullptr, weno, dttmp, c->cflbits + 1, st, nl);
+    }
     // theta (solve2.F:1320-1425)
     TileExtras ex;
     const TileExtras *exp = nullptr;
@@ -607,12 +641,14 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
     if (nrk == 3 && c->cap_fx) {
       ex.capfx = c->cap_fx; ex.capfy = c->cap_fy; ex.caprx = c->cap_rx; ex.capry = c->cap_ry; exp = &ex;
     }
-    launch_advs_tiled(g, c->rru, c->rrv, c->rrw, th_in, d->tha, 1, d->thten1,
-                      (cf.imoist && cf.eqtset == 2) ? c->thterm : nullptr, buf_out(0, nrk), weno, 0, 0,
-                      (double)(10.0f * 1.0e-18f), dttmp, 1, c->pdefscr, st, nl, exp, diffit ? &df : nullptr);
+    if (!done[0])
+      launch_advs_tiled(g, c->rru, c->rrv, c->rrw, th_in, d->tha, 1, d->thten1,
+                        (cf.imoist && cf.eqtset == 2) ? c->thterm : nullptr, buf_out(0, nrk), weno, 0, 0,
+                        (double)(10.0f * 1.0e-18f), dttmp, 1, c->pdefscr, st, nl, exp, diffit ? &df : nullptr);
     // moisture (solve2.F:1431-1530)
     for (int n = 0; n < numq; n++) {
       const int s = 1 + n;
+      if (done[s]) continue;
       launch_advs_tiled(g, c->rru, c->rrv, c->rrw, buf_in(s, nrk), base[s], 0, ten1[s], nullptr, buf_out(s, nrk),
                         weno, nrk == 3 ? 1 : 0, (n + 1 == cf.nqv) ? 0 : 1, (double)(cf.qmag[n] * 1.0e-18f), dttmp, 1,
                         c->pdefscr, st, nl, nullptr, diffit ? &df : nullptr);
@@ -628,6 +664,7 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
     // passive tracers (solve2.F:1880-1970)
     for (int n = 0; n < npt; n++) {
       const int s = 1 + numq + n;
+      if (done[s]) continue;
       const int pdef = (nrk == 3 && cf.pdtra == 1) ? 1 : 0;
       launch_advs_tiled(g, c->rru, c->rrv, c->rrw, buf_in(s, nrk), base[s], 0, ten1[s], nullptr, buf_out(s, nrk),
                         weno, pdef, 1, (double)(1.0f * 1.0e-18f), dttmp, 0, c->pdefscr, st, nl, nullptr,
@@ -746,14 +783,18 @@ static void run_step(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass1)
 
 static int fetch_scalars(cm1g_ctx *c, double *mass2, float *cflmax) {
   double dv[2];
-  int bits = 0;
+  int fl[2] = {0, 0};
   CUCHK(cudaMemcpyAsync(dv, c->dscal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CUCHK(cudaMemcpyAsync(&bits, c->cflbits, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CUCHK(cudaMemcpyAsync(fl, c->cflbits, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CUCHK(cudaStreamSynchronize(c->stream));
   if (mass2) *mass2 = c->cfg.apmasscon == 1 ? dv[0] : 0.0;
   float f;
-  memcpy(&f, &bits, 4);
+  memcpy(&f, &fl[0], 4);
   if (cflmax) *cflmax = f;
+  if (fl[1]) {   // a block of the fused scalar pass gave up waiting for its staged planes
+    CUCHK(cudaMemsetAsync(c->cflbits + 1, 0, sizeof(int), c->stream));
+    return set_err(CM1G_ERR_CUDA, "scalar pass: staged data did not arrive (bulk-copy wait gave up)");
+  }
   // the reference stops the model when the step goes unstable (solve2.F:2082);
   // here a non-finite velocity is returned as an error code instead
   if (!std::isfinite(f)) return set_err(CM1G_ERR_NONFINITE, "non-finite velocity after the large step");
@@ -1207,18 +1248,22 @@ extern "C" int cm1g_ensemble_step(cm1g_ens_t *e, cm1g_state_t *states, const flo
   if (err != cudaSuccess) return set_err(CM1G_ERR_CUDA, "ensemble launch: %s", cudaGetErrorString(err));
   // the members' mass sums and CFL maxima, read back in one synchronisation
   std::vector<double> dv(2 * n);
-  std::vector<int> bits(n);
+  std::vector<int> bits(2 * n);
   for (size_t q = 0; q < n; q++) {
     CUCHK(cudaMemcpyAsync(&dv[2 * q], e->m[q]->dscal, 2 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
-    CUCHK(cudaMemcpyAsync(&bits[q], e->m[q]->cflbits, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+    CUCHK(cudaMemcpyAsync(&bits[2 * q], e->m[q]->cflbits, 2 * sizeof(int), cudaMemcpyDeviceToHost, e->stream));
   }
   CUCHK(cudaStreamSynchronize(e->stream));
   int rc = CM1G_OK;
   for (size_t q = 0; q < n; q++) {
     float f;
-    memcpy(&f, &bits[q], 4);
+    memcpy(&f, &bits[2 * q], 4);
     if (mass2) mass2[q] = e->m[q]->cfg.apmasscon == 1 ? dv[2 * q] : 0.0;
     if (cflmax) cflmax[q] = f;
+    if (bits[2 * q + 1] && rc == CM1G_OK) {
+      CUCHK(cudaMemsetAsync(e->m[q]->cflbits + 1, 0, sizeof(int), e->stream));
+      rc = set_err(CM1G_ERR_CUDA, "member %zu: scalar pass staged data did not arrive (bulk-copy wait gave up)", q);
+    }
     if (!std::isfinite(f) && rc == CM1G_OK)
       rc = set_err(CM1G_ERR_NONFINITE, "member %zu: non-finite velocity after the large step", q);
   }

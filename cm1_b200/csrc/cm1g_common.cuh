@@ -165,6 +165,18 @@ __device__ __forceinline__ float diff6_limit(float f, float a0, float am1, int m
   return (mdiff == 1 && f * (a0 - am1) <= 0.0f) ? 0.0f : f;
 }
 
+// One advected field of the fused scalar pass of an RK stage (k_scal.cu).
+struct ScalField {
+  const float *s;               // stage input (full halo)
+  const float *sbase;           // RK base value (tha, qa, pta)
+  const float *ten1;            // fixed tendency (thten1, qten, ptten)
+  float *snew;                  // stage output
+  double weps;                  // WENO epsilon of the field (solve2.F:1391, 1472-1514, 1941)
+  int sadd;                     // theta: advect th0(k) - 300 + s (solve2.F:1365-1372)
+  int flush;                    // |snew| < smeps -> 0 (theta and moisture)
+  int pdefweno;                 // pdef form of the vertical WENO (adv_routines.F:2386-2421)
+};
+
 // Liquid water of the stage set-up (ptype=1): the RK-stage input of each
 // liquid species (at most two: Kessler's qc, qr) and the buoyancy array
 // that the stage set-up writes for the w tendency (null without liquid).

@@ -9,6 +9,7 @@
 // scalar kernels (k_advs, k_advs_pdef1/2) serve the per-routine entry
 // cm1g_advs.  Every expression keeps the reference's operand order.
 #include "cm1g_common.cuh"
+#include "k_face.cuh"
 
 namespace cm1g {
 
@@ -29,25 +30,6 @@ __device__ __forceinline__ float RRW(const DGrid &g, const Vel &q, int i, int j,
   if (k <= 1 || k >= g.nk + 1) return 0.0f;                       // solve2.F:509-511
   return LDG(&g.rf0[k]) * LDG(&q.w[iW(g, i, j, k)]);              // solve2.F:516
 }
-// Face loop of the tiles: each thread owns face `tid` of each direction,
-// and the faces past one per thread (NFX - NT x-faces, NFY - NT y-faces)
-// go to the threads from warp 1 (x) and the warps after those (y), so that
-// the second pass of the loop is spread over other warps than the first.
-template <int NT, int NFX, int NFY>
-struct FaceSlots {
-  static constexpr int X1 = 32;
-  static constexpr int Y1 = 32 * (1 + (NFX - NT + 31) / 32);
-  static_assert(NFX >= NT && NFY >= NT, "at least one face per thread");
-  static_assert(X1 + (NFX - NT) <= NT && Y1 + (NFY - NT) <= NT, "the extra faces fit the block");
-  // face index of slot q (0 or 1) of thread tid; >= NFX / NFY: none
-  __device__ static __forceinline__ int x(int tid, int q) {
-    return q == 0 ? tid : ((tid >= X1 && tid < X1 + NFX - NT) ? NT + tid - X1 : NFX);
-  }
-  __device__ static __forceinline__ int y(int tid, int q) {
-    return q == 0 ? tid : ((tid >= Y1 && tid < Y1 + NFY - NT) ? NT + tid - Y1 : NFY);
-  }
-};
-
 // divx of the momentum pass (solve2.F:590-596)
 __device__ __forceinline__ float DIVX(const DGrid &g, const Vel &q, int i, int j, int k) {
   float d = ((RRU(g, q, i + 1, j, k) - RRU(g, q, i, j, k)) * g.rdx * LDG(&g.uh[i - g.ib]) +
@@ -951,73 +933,6 @@ __global__ void __launch_bounds__(TX * TY) k_advs_pdef2_tile(DGrid g, SAdv a, co
 // provisional masses of pdefx1/pdefy1/pdefz for the second pdef pass.
 // ---------------------------------------------------------------------
 enum { MODE_UPDATE = 0, MODE_PDEF1 = 1 };
-
-// vertical face flux at level kk from wv[d+3] = s(kk+d), d = -3..2
-__device__ __forceinline__ float zflux_win(const DGrid &g, const float *wv, float r, int kk, int weno, int pdefweno,
-                                           double weps) {
-  const int nk = g.nk;
-  auto A = [&](int d) { return wv[d + 3]; };
-  const float c1k = LDG(&g.c1[kk]), c2k = LDG(&g.c2[kk]);
-  if (!weno) {
-    if (kk >= 4 && kk <= nk - 2) {
-      const bool up = (r >= 0.0f);
-      return r * flx5(up ? A(-3) : A(2), up ? A(-2) : A(1), up ? A(-1) : A(0), up ? A(0) : A(-1), up ? A(1) : A(-2));
-    }
-    if (kk == 2) {
-      if (r >= 0.0f) return r * (c1k * A(-1) + c2k * A(0));
-      return r * flx3(A(1), A(0), A(-1));
-    }
-    if (kk == nk) {
-      if (r >= 0.0f) return r * flx3(A(-2), A(-1), A(0));
-      return r * (c1k * A(-1) + c2k * A(0));
-    }
-    if (kk == 3) {
-      if (r >= 0.0f) return r * flx3(A(-2), A(-1), A(0));
-      return r * flx5(A(2), A(1), A(0), A(-1), A(-2));
-    }
-    if (r >= 0.0f) return r * flx5(A(-3), A(-2), A(-1), A(0), A(1));
-    return r * flx3(A(1), A(0), A(-1));
-  }
-  if (kk == 2) {
-    if (r >= 0.0f) return r * (c1k * A(-1) + c2k * A(0));
-    return r * upstrpd(A(1), A(0), A(-1), weps);
-  }
-  if (kk == nk) {
-    if (r > 0.0f) return r * upstrpd(A(-2), A(-1), A(0), weps);
-    return r * (c1k * A(-1) + c2k * A(0));
-  }
-  if (pdefweno == 1) {
-    if (kk == 3 && r > 0.0f) return r * upstrpd(A(-2), A(-1), A(0), weps);
-    if (kk == nk - 1 && r < 0.0f) return r * upstrpd(A(1), A(0), A(-1), weps);
-    float s1, s2, s3, s4, s5;
-    if (r >= 0.0f) { s1 = A(-3); s2 = A(-2); s3 = A(-1); s4 = A(0); s5 = A(1); }
-    else { s1 = A(2); s2 = A(1); s3 = A(0); s4 = A(-1); s5 = A(-2); }
-    return (absmax5(s1, s2, s3, s4, s5) > (float)weps) ? r * weno5(s1, s2, s3, s4, s5, weps) : 0.0f;
-  }
-  if (kk >= 4 && kk <= nk - 2) {
-    // upwind-ordered stencil first, so a warp with both signs evaluates one WENO
-    const bool up = (r >= 0.0f);
-    return r * weno5(up ? A(-3) : A(2), up ? A(-2) : A(1), up ? A(-1) : A(0), up ? A(0) : A(-1), up ? A(1) : A(-2),
-                     weps);
-  }
-  if (kk == 3) {
-    if (r >= 0.0f) return r * upstrpd(A(-2), A(-1), A(0), weps);
-    return r * weno5(A(2), A(1), A(0), A(-1), A(-2), weps);
-  }
-  if (r >= 0.0f) return r * weno5(A(-3), A(-2), A(-1), A(0), A(1), weps);
-  return r * upstrpd(A(1), A(0), A(-1), weps);
-}
-
-// horizontal face flux from five upwind-ordered values
-__device__ __forceinline__ float hflux5(float r, float sm3, float sm2, float sm1, float s0, float sp1, float sp2,
-                                        int weno, int pdef, double weps) {
-  float s1, s2, s3, s4, s5;
-  if (r >= 0.0f) { s1 = sm3; s2 = sm2; s3 = sm1; s4 = s0; s5 = sp1; }
-  else { s1 = sp2; s2 = sp1; s3 = s0; s4 = sm1; s5 = sm2; }
-  if (!weno) return r * flx5(s1, s2, s3, s4, s5);
-  if (pdef == 1 && !(absmax5(s1, s2, s3, s4, s5) > (float)weps)) return 0.0f;
-  return r * weno5(s1, s2, s3, s4, s5, weps);
-}
 
 struct STileOut {
   const float *sten_in;       // fixed tendency (thten1, qten, ptten)
