@@ -86,10 +86,29 @@ __device__ __forceinline__ float flx5(float s1, float s2, float s3, float s4, fl
 
 // WENO5 with Borges et al. (2008) weights.  Smoothness indicators in
 // binary32 (as the Fortran evaluates them), weights and quotient in binary64.
-// The three weight divisions of the textbook form are folded into one
-// binary64 division over a common denominator d1^2 d2^2 d3^2, which agrees
-// with the per-weight form to binary64 rounding; the 1e30 clamp of the
-// reference (adv_routines.F:6186-6188) is honoured by the guard.
+//
+// The reference (adv_routines.F:6166-6205) forms each weight with its own
+// binary64 division, w_i = c_i (1 + min(1e30, tau/(b_i+weps))^2), and the
+// face value as (w1 q1 + w2 q2 + w3 q3)/(w1 + w2 + w3) rounded to binary32.
+// The fast path folds the three divisions into one over the common
+// denominator d1^2 d2^2 d3^2.  Both binary64 results lie within 17 units of
+// the last binary64 place, times max|q_i|, of the exact weighted average, so
+// they differ by less than 2^-46 max|q_i|; when the folded value is farther
+// than that from both ends of the rounding interval of its binary32 result,
+// the reference's value rounds to the same binary32 number.  Otherwise (about
+// one face in a million) the face is evaluated exactly as the reference
+// does, so the result is always the reference's binary32 value.
+static __device__ __noinline__ float weno5_ref(double b1, double b2, double b3, float q1, float q2, float q3,
+                                               double weps) {
+  const double tau = fabs(b1 - b3);
+  double r;
+  r = fmin(1.0e30, tau / (b1 + weps)); double w1 = (double)0.1f * (1.0 + r * r);
+  r = fmin(1.0e30, tau / (b2 + weps)); double w2 = (double)0.6f * (1.0 + r * r);
+  r = fmin(1.0e30, tau / (b3 + weps)); double w3 = (double)0.3f * (1.0 + r * r);
+  double num = (w1 * (double)q1 + w2 * (double)q2) + w3 * (double)q3;
+  double den = (w1 + w2) + w3;
+  return (float)(num / den);
+}
 __device__ __forceinline__ float weno5(float s1, float s2, float s3, float s4, float s5, double weps) {
   const float c1312 = 13.0f / 12.0f;
   float t, u;
@@ -112,15 +131,21 @@ __device__ __forceinline__ float weno5(float s1, float s2, float s3, float s4, f
     double a3 = (double)0.3f * (e3 + tt) * (e1 * e2);
     double num = (a1 * (double)q1 + a2 * (double)q2) + a3 * (double)q3;
     double den = (a1 + a2) + a3;
-    return (float)(num / den);
+    const double v = num / den;
+    const float f = (float)v;
+    const float qm = fmaxf(fmaxf(fabsf(q1), fabsf(q2)), fabsf(q3));
+    if (qm == 0.0f) return 0.0f;   // q1 = q2 = q3 = 0: both forms give exactly 0
+    // e = v - f is exact (Sterbenz); f's rounding interval reaches h = 2^(E-24)
+    // on each side (E = the binary exponent of f), h/2 toward zero when f is a
+    // power of two; v's binary32 rounding is safe when |e| + delta < h.
+    const double fd = (double)f;
+    const double e = v - fd;
+    double h = __hiloint2double(__double2hiint(fd) & 0x7ff00000, 0) * 5.9604644775390625e-08;   // 2^-24
+    if ((__float_as_int(f) & 0x7fffff) == 0) h = 0.5 * h;
+    const double delta = (double)qm * 1.4210854715202004e-14;   // 2^-46
+    if (fabs(e) + delta < h) return f;
   }
-  double r;
-  r = fmin(1.0e30, tau / d1); double w1 = (double)0.1f * (1.0 + r * r);
-  r = fmin(1.0e30, tau / d2); double w2 = (double)0.6f * (1.0 + r * r);
-  r = fmin(1.0e30, tau / d3); double w3 = (double)0.3f * (1.0 + r * r);
-  double num = (w1 * (double)q1 + w2 * (double)q2) + w3 * (double)q3;
-  double den = (w1 + w2) + w3;
-  return (float)(num / den);
+  return weno5_ref(b1, b2, b3, q1, q2, q3, weps);
 }
 
 __device__ __forceinline__ float upstrpd(float s1, float s2, float s3, double weps) {

@@ -139,7 +139,13 @@ __device__ __forceinline__ void prs_rho(const DGrid &g, float pp, float th3, con
                                         int imoist, float *prs, float *rho) {
   const Consts &c = g.c;
   const float pi = LDG(&g.pi0[k]) + pp;
-  const float pr = 1.0e5f * powf(pi, c.cpdrd);
+  // pi**(cp/rd) in binary64, rounded once: the correctly rounded binary32
+  // power, which is what the reference's powf (glibc) returns for all but
+  // rare inputs.  A last-place difference here moves rho, hence the FP64
+  // mass sum of apmasscon, hence the uniform pi' shift of the mass fix,
+  // which on near-uniform pressure fields (the CBL) is a visible fraction
+  // of pi''s range.
+  const float pr = 1.0e5f * (float)pow((double)pi, (double)c.cpdrd);
   prs[o] = pr;
   if (imoist) rho[o] = pr / ((LDG(&g.th0[k]) + th3) * pi * (c.rd + fmaxf(0.0f, LDG(&qv[o])) * c.rv));
   else rho[o] = pr / (c.rd * (LDG(&g.th0[k]) + th3) * pi);

@@ -72,6 +72,20 @@ static const float TH0R = 300.0f;           /* constants.F:15 */
 static const float P00 = 1.0e5f;            /* constants.F:17 */
 static const float CSMAX = 350.0f;          /* constants.F:45 */
 
+/* The binary32 powers of the pressure/density relations (solve2.F:1580-1606,
+ * 1976-2033) and of the Kessler scheme.  The reference, built with gfortran,
+ * evaluates real**real with the C library's powf; glibc's powf is not
+ * correctly rounded for about 0.1% of the arguments these relations see.
+ * Mode 0 (default) calls powf, as the reference build does; mode 1 evaluates
+ * the power in binary64 and rounds once (the correctly rounded result for all
+ * but vanishingly rare arguments), the choice of the CUDA path.  Comparing the
+ * two modes measures how much a last-place choice of the math library moves
+ * the model. */
+static int g_pow_mode = 0;
+void oracle_set_pow_mode(int mode) { g_pow_mode = mode; }
+int oracle_get_pow_mode(void) { return g_pow_mode; }
+static float opowf(float x, float y) { return g_pow_mode ? (float)pow((double)x, (double)y) : powf(x, y); }
+
 typedef struct {
   int ni, nj, nk, ngxy, ib, ie, jb, je, kb, ke, NI, NJ, NK;
   float dx, dy, dz, rdx, rdy, rdz;
@@ -1654,7 +1668,7 @@ int oracle_solve2(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_state_t 
 #pragma omp parallel for
       for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++) {
         float pi = A3(g->pi0, i, j, k) + A3(s.pp3d, i, j, k);
-        float pr = P00 * powf(pi, c.cpdrd);
+        float pr = P00 * opowf(pi, c.cpdrd);
         A3(s.prs, i, j, k) = pr;
         if (cfg->imoist)
           A3(s.rho, i, j, k) = pr / ((A3(g->th0, i, j, k) + A3(s.th3d, i, j, k)) * pi * (c.rd + fmaxf(0.0f, A3(s.q3d[cfg->nqv - 1], i, j, k)) * c.rv));
@@ -1712,7 +1726,7 @@ int oracle_solve2(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_state_t 
       for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj; j++) for (int i = 1; i <= ni; i++) {
         A3(s.pp3d, i, j, k) = A3(s.pp3d, i, j, k) + tem;
         float pi = A3(g->pi0, i, j, k) + A3(s.pp3d, i, j, k);
-        float pr = P00 * powf(pi, c.cpdrd);
+        float pr = P00 * opowf(pi, c.cpdrd);
         A3(s.prs, i, j, k) = pr;
         if (cfg->imoist)
           A3(s.rho, i, j, k) = pr / ((A3(g->th0, i, j, k) + A3(s.th3d, i, j, k)) * pi * (c.rd + fmaxf(0.0f, A3(s.q3d[cfg->nqv - 1], i, j, k)) * c.rv));
@@ -1961,7 +1975,7 @@ static void k_fallout_g(const OG *g, F3 rho, F3 qr, F3 vr) {
   for (int k = 1; k <= g->nk; k++) for (int j = 1; j <= g->nj; j++) for (int i = 1; i <= g->ni; i++) {
     A3(vr, i, j, k) = 0.0f;
     if (A3(qr, i, j, k) > 1.0e-12f)
-      A3(vr, i, j, k) = 14.34f * powf(A3(rho, i, j, k) * A3(qr, i, j, k), 0.1346f) * sqrtf(1.15f / A3(rho, i, j, k));
+      A3(vr, i, j, k) = 14.34f * opowf(A3(rho, i, j, k) * A3(qr, i, j, k), 0.1346f) * sqrtf(1.15f / A3(rho, i, j, k));
   }
 }
 
@@ -2039,7 +2053,7 @@ static void kessler_g(const OG *g, float dt, double *tauto, double *taccr, doubl
         ar = ar * dt;
       }
       if (qcnew > 0.0f && qrnew > 0.0f) {
-        cr = 2.2f * qcnew * powf(qrnew, 0.875f);
+        cr = 2.2f * qcnew * opowf(qrnew, 0.875f);
         cr = cr * dt;
       }
       if (qrnew > 0.0f) {
@@ -2047,7 +2061,7 @@ static void kessler_g(const OG *g, float dt, double *tauto, double *taccr, doubl
         float qvs = K.eps * esl / (A3(prs, i, j, k) - esl);
         if (qvnew < qvs) {
           float r = A3(rho, i, j, k);
-          er = (1.6f + 30.3922f * powf(r * qrnew, 0.2046f)) * (1.0f - (qvnew / qvs)) * powf(r * qrnew, 0.525f) /
+          er = (1.6f + 30.3922f * opowf(r * qrnew, 0.2046f)) * (1.0f - (qvnew / qvs)) * opowf(r * qrnew, 0.525f) /
                ((2.03e4f + 9.584e6f / (qvs * A3(prs, i, j, k))) * r);
           er = fminf(er * dt, qrnew);
           if ((qvnew + er) > qvs) er = qvs - qvnew;
@@ -2069,8 +2083,8 @@ static void kessler_g(const OG *g, float dt, double *tauto, double *taccr, doubl
           A3(th3d, i, j, k) = A3(th3d, i, j, k) -
               er * ((K.lv1 - K.lv2 * A3(tmp, i, j, k)) / (K.cpdcv * cvml * (pi0 + A3(pp3d, i, j, k))) -
                     (th0 + A3(th3d, i, j, k)) * (c.rv / cvml) * (1.0f - c.rovcp * cpml / rm));
-          A3(pp3d, i, j, k) = powf(A3(rho, i, j, k) * rm * (th0 + A3(th3d, i, j, k)) * K.rp00, c.rddcv) - pi0;
-          A3(prs, i, j, k) = P00 * powf(pi0 + A3(pp3d, i, j, k), c.cpdrd);
+          A3(pp3d, i, j, k) = opowf(A3(rho, i, j, k) * rm * (th0 + A3(th3d, i, j, k)) * K.rp00, c.rddcv) - pi0;
+          A3(prs, i, j, k) = P00 * opowf(pi0 + A3(pp3d, i, j, k), c.cpdrd);
         } else {
           A3(th3d, i, j, k) = A3(th3d, i, j, k) - er * ((K.lv1 - K.lv2 * A3(tmp, i, j, k)) / (c.cp * (pi0 + A3(pp3d, i, j, k))));
           A3(rho, i, j, k) = A3(prs, i, j, k) /
@@ -2151,7 +2165,7 @@ static int satadj_g(const OG *g, float dt, double *tcond, double *tevac, F3 rho,
           b1 = b1 + (double)(A3(rr, i, j, k) * fmaxf(qcnew - A3(q3d[nqc], i, j, k), 0.0f) * tem);
           b2 = b2 + (double)(A3(rr, i, j, k) * fmaxf(qvnew - A3(q3d[nqv], i, j, k), 0.0f) * tem);
           A3(prs, i, j, k) = pnew;
-          A3(pp3d, i, j, k) = powf(pnew * K.rp00, c.rovcp) - pi0;
+          A3(pp3d, i, j, k) = opowf(pnew * K.rp00, c.rovcp) - pi0;
           A3(th3d, i, j, k) = tnew / (pi0 + A3(pp3d, i, j, k)) - th0;
           A3(q3d[nqc], i, j, k) = qcnew;
           A3(q3d[nqv], i, j, k) = qvnew;
@@ -2606,7 +2620,7 @@ int oracle_turbsmag(const cm1g_config_t *cfg, const cm1g_grid_t *gr, float csm, 
   for (int j = 1; j <= nj; j++) for (int k = 2; k <= nk; k++) for (int i = 1; i <= ni; i++) {
     const float rmf = 1.0f / A3(g->mf, i, j, k);
     if (tconfig == 1) {
-      float grdscl = powf(((g->dx * RUH(i)) * (g->dy * RVH(j))) * (g->dz * rmf), 0.33333333f);
+      float grdscl = opowf(((g->dx * RUH(i)) * (g->dy * RVH(j))) * (g->dz * rmf), 0.33333333f);
       A3(kmh, i, j, k) = SQ(csm * grdscl) * sqrtf(fmaxf(A3(defv, i, j, k) + A3(defh, i, j, k) - A3(nm, i, j, k) * prinv, dmin));
       A3(kmv, i, j, k) = A3(kmh, i, j, k);
     } else {

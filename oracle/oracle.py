@@ -83,6 +83,26 @@ def step(case, state=None, solve2_only=False, mtime=0.0):
     return st, m2.value, cfl.value
 
 
+class pow_mode:
+    """Context manager selecting how the oracle evaluates the binary32
+    powers of the pressure/density relations and the Kessler scheme:
+    "libm" (the C library's powf, as the reference build does; the default)
+    or "binary64" (the power in binary64 rounded once, the CUDA path's
+    choice)."""
+
+    def __init__(self, mode):
+        self.mode = {"libm": 0, "binary64": 1}[mode]
+
+    def __enter__(self):
+        L = lib()
+        self.saved = L.oracle_get_pow_mode()
+        L.oracle_set_pow_mode(self.mode)
+        return self
+
+    def __exit__(self, *a):
+        lib().oracle_set_pow_mode(self.saved)
+
+
 _LIB_R8 = os.path.join(_HERE, "_r8", "liboracle_r8.so")
 _lib_r8 = None
 
