@@ -54,8 +54,8 @@ void launch_scal_pass(const DGrid &g, const ScalField *f, int n, const float *rr
 void launch_sound(const DGrid &g, int nsound, int nrk, float dt, const float *ua, float *u3d, const float *uten,
                   const float *va, float *v3d, const float *vten, const float *wa, float *w3d, const float *wten,
                   const float *ppi, float *pp3d, const float *piadv, const float *ppten, float *ppx,
-                  const float *thv, const float *ppterm, float *rru, float *rrv, float *rrw, const float *radbcw,
-                  const float *radbce, const float *radbcs, const float *radbcn, float *su, float *sv, float *su2,
+                  const float *thv, const float *ppterm, float *rru, float *rrv, float *rrw, float *radbcw,
+                  float *radbce, float *radbcs, float *radbcn, float *su, float *sv, float *su2,
                   float *sv2, float *d1, float *d2, cudaStream_t st, int64_t *nl);
 int sound_max_nk();
 void launch_stage_prep(const DGrid &g, const float *th3d, const float *pp3d, const float *qv, const LiquidIn &liq,
@@ -63,6 +63,8 @@ void launch_stage_prep(const DGrid &g, const float *th3d, const float *pp3d, con
                        int64_t *nl);
 void launch_radbc4(const DGrid &g, const float *ua, const float *u3d, const float *va, const float *v3d,
                    float *rw, float *re, float *rs, float *rn, float dt, cudaStream_t st, int64_t *nl);
+void launch_radbc_kw(const DGrid &g, const float *ua, const float *va, float *rw, float *re, float *rs, float *rn,
+                     cudaStream_t st, int64_t *nl);
 int prs_nchunk(const DGrid &g);
 void launch_prs_rho(const DGrid &g, const float *pp3d, const float *th3d, const float *qv, int imoist,
                     float *prs, float *rho, double *part3, double *part4, int do_sums, cudaStream_t st, int64_t *nl);
@@ -287,7 +289,8 @@ static int check_config(const cm1g_config_t *c) {
   if (c->idiff < 0 || c->idiff > 1) return set_err(CM1G_ERR_UNSUPPORTED, "idiff must be 0 or 1");
   if (c->idiff && !(c->kdiff6 >= 0.0f)) return set_err(CM1G_ERR_ARG, "kdiff6 must be >= 0");
   bool open = c->wbc == 2 || c->ebc == 2 || c->sbc == 2 || c->nbc == 2;
-  if (open && c->irbc != 4) return set_err(CM1G_ERR_UNSUPPORTED, "open boundaries need irbc=4");
+  if (open && !(c->irbc == 1 || c->irbc == 2 || c->irbc == 4))
+    return set_err(CM1G_ERR_UNSUPPORTED, "open boundaries: irbc=%d is not built (1, 2 and 4 are)", c->irbc);
   for (int b : {c->wbc, c->ebc, c->sbc, c->nbc})
     if (b < 1 || b > 4) return set_err(CM1G_ERR_ARG, "lateral bc must be 1..4");
   if ((c->wbc == 1) != (c->ebc == 1) || (c->sbc == 1) != (c->nbc == 1))
@@ -330,6 +333,7 @@ extern "C" int cm1g_init(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_c
   g.wbc = cfg->wbc; g.ebc = cfg->ebc; g.sbc = cfg->sbc; g.nbc = cfg->nbc;
   g.ibw = cfg->wbc != 1; g.ibe = cfg->ebc != 1; g.ibs = cfg->sbc != 1; g.ibn = cfg->nbc != 1;
   g.smeps = cfg->smeps; g.alph = cfg->alph; g.kdiv = cfg->kdiv;
+  g.irbc = cfg->irbc; g.cstar = cfg->cstar;
   g.tile_adv = 0; g.tile_mom = 0; g.sound_cfg = -1;
   set_constants_(cfg->testcase, &g.c);
 
@@ -586,6 +590,10 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
     launch_recip_rho(g, d->rho, c->rr, st, nl);
   }
 
+  // irbc = 1: the open boundaries' phase speeds of the step, from ua/va, as
+  // solve1 forms them before solve2 (solve1.F:403-409)
+  if (cf.irbc == 1 && open)
+    launch_radbc_kw(g, d->ua, d->va, d->radbcw, d->radbce, d->radbcs, d->radbcn, st, nl);
   for (int nrk = 1; nrk <= 3; nrk++) {
     const float dttmp = dt / (float)(3 + 1 - nrk);
     const float *th_in = buf_in(0, nrk);
@@ -1451,8 +1459,10 @@ extern "C" int cm1g_sound(cm1g_ctx_t *c, float dt, float *radbcw, float *radbce,
   float *dppx = S.in(ppx, ns, true);
   const float *dthv = S.in(thv, ns, false), *dppterm = S.in(ppterm, ns, false);
   float *dru = S.in(rru, nu, true), *drv = S.in(rrv, nv, true), *drw = S.in(rrw, nw, true);
-  float *rw = S.in(radbcw, nrw, false), *re = S.in(radbce, nrw, false), *rs = S.in(radbcs, nrs, false),
-        *rn = S.in(radbcn, nrs, false);
+  // irbc = 2 rewrites the phase speeds each small step (sound.F:261-267)
+  const bool rad_out = c->g.irbc == 2;
+  float *rw = S.in(radbcw, nrw, rad_out), *re = S.in(radbce, nrw, rad_out), *rs = S.in(radbcs, nrs, rad_out),
+        *rn = S.in(radbcn, nrs, rad_out);
   if (S.err) return set_err(CM1G_ERR_NOMEM, "staging");
   launch_sound(g, c->cfg.nsound, nrk, dt, dua, du3, dut, dva, dv3, dvt, dwa, dw3, dwt, dppi, dpp, dpia, dppt, dppx,
                dthv, dppterm, dru, drv, drw, rw, re, rs, rn, c->su, c->sv, c->su2, c->sv2, c->d1, c->d2, c->stream,

@@ -129,6 +129,35 @@ void launch_radbc4(const DGrid &g, const float *ua, const float *u3d, const floa
   if (nl) *nl += 1;
 }
 
+// radbcew / radbcns with irbc = 1 (bc.F:1948-2046, called by solve1.F:403-409
+// before the RK loop): the Klemp-Wilhelmson phase speeds of the step from ua
+// and va, u - cstar where negative (west, south), u + cstar where positive
+// (east, north), else 0.  One thread per boundary column and level.
+__global__ void k_radbc_kw(DGrid g, const float *__restrict__ ua, const float *__restrict__ va, float *rw, float *re,
+                           float *rs, float *rn) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x), k = 1 + (int)blockIdx.y;
+  if (t < g.nj) {
+    const int j = 1 + t;
+    const long o = (j - g.jb) + (long)g.NJ * k;
+    if (g.ibw && g.wbc == 2) { const float c = LDG(&ua[iU(g, 1, j, k)]) - g.cstar; rw[o] = (c < 0.0f) ? c : 0.0f; }
+    if (g.ibe && g.ebc == 2) { const float c = LDG(&ua[iU(g, g.ni + 1, j, k)]) + g.cstar; re[o] = (c > 0.0f) ? c : 0.0f; }
+  }
+  if (t < g.ni) {
+    const int i = 1 + t;
+    const long o = (i - g.ib) + (long)g.NI * k;
+    if (g.ibs && g.sbc == 2) { const float c = LDG(&va[iV(g, i, 1, k)]) - g.cstar; rs[o] = (c < 0.0f) ? c : 0.0f; }
+    if (g.ibn && g.nbc == 2) { const float c = LDG(&va[iV(g, i, g.nj + 1, k)]) + g.cstar; rn[o] = (c > 0.0f) ? c : 0.0f; }
+  }
+}
+
+void launch_radbc_kw(const DGrid &g, const float *ua, const float *va, float *rw, float *re, float *rs, float *rn,
+                     cudaStream_t st, int64_t *nl) {
+  const int n = g.ni > g.nj ? g.ni : g.nj;
+  dim3 grid((n + 127) / 128, g.nk);
+  { ProfScope _ps("k_radbc_kw", st); k_radbc_kw<<<grid, 128, 0, st>>>(g, ua, va, rw, re, rs, rn); }
+  if (nl) *nl += 1;
+}
+
 // ---------------------------------------------------------------------
 // pressure and density (solve2.F:1580-1606) with the per-level FP64
 // sums of apmasscon (solve2.F:1617-1648).  Block (x, k) covers a chunk of

@@ -39,7 +39,7 @@ struct SoundIO {
   const float *wa;                // start-of-stage w (first step: rrw = wa*beta)
   const float *uten, *vten, *wten, *ppten;
   const float *thv, *ppterm, *piadv;
-  const float *radbcw, *radbce, *radbcs, *radbcn;
+  float *radbcw, *radbce, *radbcs, *radbcn;   // phase speeds (irbc = 2: formed and stored here)
   float *ppx;                     // last step of the final stage: kdiv*(pi'_new - pi'_old)
 };
 
@@ -68,6 +68,28 @@ __device__ __forceinline__ PpdNbr ppd_nbr(const DGrid &g, int mapped, int i, int
 
 #define RJK(g, a, j, k) ((a)[((j) - (g).jb) + (long)(g).NJ * (k)])
 #define RIK(g, a, i, k) ((a)[((i) - (g).ib) + (long)(g).NI * (k)])
+
+// Phase speed of an open-boundary point for this small step.  With irbc = 2
+// the Klemp-Wilhelmson speed is formed from the current velocity at every
+// small step (sound.F:261-267; radbcew/radbcns, bc.F:1948-2046): u - cstar
+// where negative at the west and south boundaries, u + cstar where positive
+// at the east and north ones, else 0; it is stored for the state.  Otherwise
+// the stored speed (irbc = 4 from radbcew4/ns4, irbc = 1 from the start of
+// the step) is used.
+__device__ __forceinline__ float radbc_in(const DGrid &g, float &slot, float ub) {
+  if (g.irbc != 2) return slot;
+  const float c = ub - g.cstar;
+  const float r = (c < 0.0f) ? c : 0.0f;
+  slot = r;
+  return r;
+}
+__device__ __forceinline__ float radbc_out(const DGrid &g, float &slot, float ub) {
+  if (g.irbc != 2) return slot;
+  const float c = ub + g.cstar;
+  const float r = (c > 0.0f) ? c : 0.0f;
+  slot = r;
+  return r;
+}
 
 static const int SND_TX = 32;     // columns per tile (one warp wide)
 static const int SND_NW = 8;      // warps per block
@@ -148,16 +170,16 @@ __global__ void __launch_bounds__(TX * NW, CM1G_SND_MINB) k_sound_tile(DGrid g, 
       const float accv0 = p.first ? 0.0f : io.rrv[ov];
       // ---- u at faces i, i+1 and v at faces j, j+1
       float uo = u0v;
-      if (openw) uo = uo + dts * (-RJK(g, io.radbcw, j, k) * (u1v - u0v) * rdx * LDG(&g.uh[1 - g.ib]) + ut0);
+      if (openw) uo = uo + dts * (-radbc_in(g, RJK(g, io.radbcw, j, k), u0v) * (u1v - u0v) * rdx * LDG(&g.uh[1 - g.ib]) + ut0);
       const float un0 = uo + dtu_i * (ut0 - tem1pg * (ppc - ppw) * uf_i * (thc + thw));
       float uop = u1v;
-      if (opene) uop = uop + dts * (-RJK(g, io.radbce, j, k) * (u1v - u0v) * rdx * LDG(&g.uh[ni - g.ib]) + ut1);
+      if (opene) uop = uop + dts * (-radbc_out(g, RJK(g, io.radbce, j, k), u1v) * (u1v - u0v) * rdx * LDG(&g.uh[ni - g.ib]) + ut1);
       const float unp = uop + dtu_ip * (ut1 - tem1pg * (ppe - ppc) * uf_ip * (the + thc));
       float vo = v0v;
-      if (opens) vo = vo + dts * (-RIK(g, io.radbcs, i, k) * (v1v - v0v) * rdy * LDG(&g.vh[1 - g.jb]) + vt0);
+      if (opens) vo = vo + dts * (-radbc_in(g, RIK(g, io.radbcs, i, k), v0v) * (v1v - v0v) * rdy * LDG(&g.vh[1 - g.jb]) + vt0);
       const float vn0 = vo + dtv_j * (vt0 - tem2pg * (ppc - pps) * vf_j * (thc + ths));
       float vop = v1v;
-      if (openn) vop = vop + dts * (-RIK(g, io.radbcn, i, k) * (v1v - v0v) * rdy * LDG(&g.vh[nj - g.jb]) + vt1);
+      if (openn) vop = vop + dts * (-radbc_out(g, RIK(g, io.radbcn, i, k), v1v) * (v1v - v0v) * rdy * LDG(&g.vh[nj - g.jb]) + vt1);
       const float vnp = vop + dtv_jp * (vt1 - tem2pg * (ppn - ppc) * vf_jp * (thn + thc));
       io.u_out[ou] = un0;
       io.v_out[ov] = vn0;
@@ -413,16 +435,16 @@ __global__ void __launch_bounds__(TX * TY, 4) k_sound_col(DGrid g, SoundIO io, S
       const float accu0 = cur.accu0, accv0 = cur.accv0;
       // ---- u at faces i, i+1 and v at faces j, j+1 (sound.F:321-341, bc.F:2392-2686)
       float uo = u0v;
-      if (openw) uo = uo + dts * (-RJK(g, io.radbcw, j, k) * (u1v - u0v) * rdx * LDG(&g.uh[1 - g.ib]) + ut0);
+      if (openw) uo = uo + dts * (-radbc_in(g, RJK(g, io.radbcw, j, k), u0v) * (u1v - u0v) * rdx * LDG(&g.uh[1 - g.ib]) + ut0);
       const float un0 = uo + dtu_i * (ut0 - tem1pg * (ppc - ppw) * uf_i * (thc + thw));
       float uop = u1v;
-      if (opene) uop = uop + dts * (-RJK(g, io.radbce, j, k) * (u1v - u0v) * rdx * LDG(&g.uh[ni - g.ib]) + ut1);
+      if (opene) uop = uop + dts * (-radbc_out(g, RJK(g, io.radbce, j, k), u1v) * (u1v - u0v) * rdx * LDG(&g.uh[ni - g.ib]) + ut1);
       const float unp = uop + dtu_ip * (ut1 - tem1pg * (ppe - ppc) * uf_ip * (the + thc));
       float vo = v0v;
-      if (opens) vo = vo + dts * (-RIK(g, io.radbcs, i, k) * (v1v - v0v) * rdy * LDG(&g.vh[1 - g.jb]) + vt0);
+      if (opens) vo = vo + dts * (-radbc_in(g, RIK(g, io.radbcs, i, k), v0v) * (v1v - v0v) * rdy * LDG(&g.vh[1 - g.jb]) + vt0);
       const float vn0 = vo + dtv_j * (vt0 - tem2pg * (ppc - pps) * vf_j * (thc + ths));
       float vop = v1v;
-      if (openn) vop = vop + dts * (-RIK(g, io.radbcn, i, k) * (v1v - v0v) * rdy * LDG(&g.vh[nj - g.jb]) + vt1);
+      if (openn) vop = vop + dts * (-radbc_out(g, RIK(g, io.radbcn, i, k), v1v) * (v1v - v0v) * rdy * LDG(&g.vh[nj - g.jb]) + vt1);
       const float vnp = vop + dtv_jp * (vt1 - tem2pg * (ppn - ppc) * vf_jp * (thn + thc));
       io.u_out[ou] = un0;
       io.v_out[ov] = vn0;
@@ -583,8 +605,8 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
                   const float *ua, float *u3d, const float *uten, const float *va, float *v3d, const float *vten,
                   const float *wa, float *w3d, const float *wten, const float *ppi, float *pp3d,
                   const float *piadv, const float *ppten, float *ppx, const float *thv, const float *ppterm,
-                  float *rru, float *rrv, float *rrw, const float *radbcw, const float *radbce,
-                  const float *radbcs, const float *radbcn, float *su, float *sv, float *su2, float *sv2,
+                  float *rru, float *rrv, float *rrw, float *radbcw, float *radbce,
+                  float *radbcs, float *radbcn, float *su, float *sv, float *su2, float *sv2,
                   float *d1, float *d2, cudaStream_t st, int64_t *nl) {
   int nloop;
   float dts;

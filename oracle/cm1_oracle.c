@@ -1134,6 +1134,36 @@ static void advw_g(const OG *g, Scratch *w, F3 divx, F3 rru, F3 rrv, F3 rrw, F3 
 /* Open-radiative boundary pieces, bc.F                                 */
 /* ------------------------------------------------------------------ */
 
+/* radbcew / radbcns: bc.F:1948-2046, the Klemp-Wilhelmson phase speeds
+ * u -/+ cstar of irbc = 1 (from ua, solve1.F:403-409) and irbc = 2 (from
+ * u3d at every small step, sound.F:261-267) */
+static void radbcew_kw(const OG *g, float *radbcw, float *radbce, F3 ua) {
+  const float cstar = g->cfg->cstar;
+  if (g->ibw && g->wbc == 2)
+    for (int k = 1; k <= g->nk; k++) for (int j = 1; j <= g->nj; j++) {
+      float cbcw = A3(ua, 1, j, k) - cstar;
+      RJK(g, radbcw, j, k) = (cbcw < 0.0f) ? cbcw : 0.0f;
+    }
+  if (g->ibe && g->ebc == 2)
+    for (int k = 1; k <= g->nk; k++) for (int j = 1; j <= g->nj; j++) {
+      float cbce = A3(ua, g->ni + 1, j, k) + cstar;
+      RJK(g, radbce, j, k) = (cbce > 0.0f) ? cbce : 0.0f;
+    }
+}
+static void radbcns_kw(const OG *g, float *radbcs, float *radbcn, F3 va) {
+  const float cstar = g->cfg->cstar;
+  if (g->ibs && g->sbc == 2)
+    for (int k = 1; k <= g->nk; k++) for (int i = 1; i <= g->ni; i++) {
+      float cbcs = A3(va, i, 1, k) - cstar;
+      RIK(g, radbcs, i, k) = (cbcs < 0.0f) ? cbcs : 0.0f;
+    }
+  if (g->ibn && g->nbc == 2)
+    for (int k = 1; k <= g->nk; k++) for (int i = 1; i <= g->ni; i++) {
+      float cbcn = A3(va, i, g->nj + 1, k) + cstar;
+      RIK(g, radbcn, i, k) = (cbcn > 0.0f) ? cbcn : 0.0f;
+    }
+}
+
 /* radbcew4: bc.F:2054-2115 */
 static void radbcew4(const OG *g, float *radbcw, float *radbce, F3 u1, F3 u2, float dt) {
   int ni = g->ni, nj = g->nj, nk = g->nk;
@@ -1266,6 +1296,11 @@ static void sound_g(const OG *g, const SoundArgs *a, int nrk, float dt) {
   }
 
   for (int n = 1; n <= nloop; n++) {
+    /* sound.F:261-267 */
+    if (cfg->irbc == 2) {
+      if (g->ibw || g->ibe) radbcew_kw(g, a->radbcw, a->radbce, u3d);
+      if (g->ibs || g->ibn) radbcns_kw(g, a->radbcs, a->radbcn, v3d);
+    }
     /* sound.F:273-303 */
     if (cfg->wbc == 2 && g->ibw)
       for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj; j++)
@@ -1491,7 +1526,8 @@ static int check_cfg(const cm1g_config_t *cfg) {
   if (cfg->ptype != 0 && cfg->ptype != 1) return -1;
   if (cfg->iptra && (cfg->npt < 0 || cfg->npt > CM1G_MAXQ)) return -1;
   if (cfg->roflux != 0) return -1;
-  if ((cfg->wbc == 2 || cfg->ebc == 2 || cfg->sbc == 2 || cfg->nbc == 2) && cfg->irbc != 4) return -1;
+  if ((cfg->wbc == 2 || cfg->ebc == 2 || cfg->sbc == 2 || cfg->nbc == 2) &&
+      !(cfg->irbc == 1 || cfg->irbc == 2 || cfg->irbc == 4)) return -1;
   if (cfg->nsound < 2 || (cfg->nsound % 2)) return -1;
   return 0;
 }
@@ -1538,6 +1574,12 @@ int oracle_solve2(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_state_t 
   if (diffit)
     for (int k = 1; k <= nk; k++) for (int j = 0; j <= nj + 1; j++) for (int i = 0; i <= ni + 1; i++)
       A3(rr, i, j, k) = 1.0f / A3(s.rho, i, j, k);
+  /* irbc = 1: the phase speeds of the step, from ua, as solve1 forms them
+   * before solve2 (solve1.F:403-409) */
+  if (cfg->irbc == 1) {
+    if (g->ibw || g->ibe) radbcew_kw(g, s.radbcw, s.radbce, s.ua);
+    if (g->ibs || g->ibn) radbcns_kw(g, s.radbcs, s.radbcn, s.va);
+  }
 
   for (int nrk = 1; nrk <= 3; nrk++) {
     float dttmp = dt / (float)(3 + 1 - nrk);

@@ -53,6 +53,10 @@ CASES = [
     # 6th-order horizontal diffusion (idiff=1, difforder=6), with and without the mdiff limiter
     ("dry_bubble", dict(diff6=0.04)),
     ("supercell", dict(ni=40, nj=36, nk=40, diff6=0.04, mdiff=1)),
+    # open-boundary phase speeds of Klemp-Wilhelmson form: from ua once per
+    # large step (irbc=1) and from u3d at every small step (irbc=2)
+    ("supercell", dict(ni=40, nj=36, nk=40, irbc=1)),
+    ("supercell", dict(ni=40, nj=36, nk=40, irbc=2)),
 ]
 
 

@@ -132,3 +132,36 @@ def test_open_boundary_100_steps_within_oracle_sensitivity(cm1g, oracle_lib):
         print("%d steps, open boundaries, %s: oracle(powf) %.7e; oracle(binary64 powers) %.2e, oracle(theta'(1+1e-7)) "
               "%.2e, CUDA %.2e away" % (nsteps, k, sb[k], libm, pert, cuda))
         assert cuda <= max(libm, pert, 1e-3), (k, cuda, libm, pert)
+
+
+@pytest.mark.parametrize("irbc", [1, 2])
+def test_open_boundary_phase_speed_forms_30_steps(irbc, cm1g, oracle_lib):
+    """30 large steps of the reduced supercell with the Klemp-Wilhelmson phase
+    speeds (irbc=1: from ua once per step; irbc=2: from u3d at every small
+    step) against the oracle evaluating the pressure power as the CUDA path
+    does: every field within 1e-5 of its range, and the stored phase speeds
+    of the last small step equal to the oracle's."""
+    torch = _torch()
+    case = make_case("supercell", ni=40, nj=36, nk=40, irbc=irbc)
+    ref = case.copy_state()
+    ctx = cm1g.Context(case.cfg, case.grid)
+    dev = cm1g.to_device(case.state)
+    for n in range(30):
+        with oracle_lib.pow_mode("binary64"):
+            ref, _, _ = oracle_lib.step(case, ref)
+        ctx.step(dev, case.dt, case.mass1, use_graph=(n > 0))
+    torch.cuda.synchronize()
+    got = cm1g.to_host(dev)
+    errs = field_errors(case, got, ref)
+    worst = max(errs, key=errs.get)
+    print("irbc=%d, 30 steps: worst %s %.3e of range" % (irbc, worst, errs[worst]))
+    for f, e in errs.items():
+        assert e <= TOL_RANGE, (f, e)
+    lay = case.lay
+    K = slice(lay.kx(1), lay.kx(lay.nk) + 1)
+    for n, sl in (("radbcw", (K, slice(lay.jx(1), lay.jx(lay.nj) + 1))),
+                  ("radbce", (K, slice(lay.jx(1), lay.jx(lay.nj) + 1))),
+                  ("radbcs", (K, slice(lay.ix(1), lay.ix(lay.ni) + 1))),
+                  ("radbcn", (K, slice(lay.ix(1), lay.ix(lay.ni) + 1)))):
+        assert np.array_equal(got[n][sl], ref[n][sl]), n
+        assert (got[n][sl] != 0).any() or n in ("radbce", "radbcn"), n

@@ -126,13 +126,15 @@ def test_advuvw(bc, cm1g, oracle_lib):
 
 
 @pytest.mark.parametrize("form", ["tile", "col"])
-@pytest.mark.parametrize("bc", [1, 2])
+@pytest.mark.parametrize("bc,irbc", [(1, 4), (2, 4), (2, 2)])
 @pytest.mark.parametrize("nrk", [1, 2, 3])
-def test_sound_stage(bc, nrk, form, cm1g, oracle_lib, monkeypatch):
-    """Both forms of the acoustic kernel (3-phase tile, column sweep)."""
+def test_sound_stage(bc, irbc, nrk, form, cm1g, oracle_lib, monkeypatch):
+    """Both forms of the acoustic kernel (3-phase tile, column sweep); with
+    irbc=2 the routine forms the phase speeds at every small step and returns
+    the last ones in radbcw/e/s/n."""
     _torch()
     monkeypatch.setenv("CM1G_SOUND_FORM", form)
-    case = make_case("supercell", ni=24, nj=20, nk=24, bc=bc)
+    case = make_case("supercell", ni=24, nj=20, nk=24, bc=bc, irbc=irbc)
     lay, st, gr = case.lay, case.state, case.grid
     rng = np.random.default_rng(5 + nrk)
     A = {}
@@ -182,6 +184,9 @@ def test_sound_stage(bc, nrk, form, cm1g, oracle_lib, monkeypatch):
               ("rrw", (K,) + lay.interior(1)[1:])]
     if nrk == 3:
         checks.append(("ppx", lay.interior(1)))
+    if irbc == 2:
+        checks += [(n, (K, slice(lay.jx(1), lay.jx(nj) + 1))) for n in ("radbcw", "radbce")]
+        checks += [(n, (K, slice(lay.ix(1), lay.ix(ni) + 1))) for n in ("radbcs", "radbcn")]
     for n, sl in checks:
         e = relerr(G[n][sl], R[n][sl])
         assert e <= 1e-6, (n, e)
