@@ -36,6 +36,11 @@ namespace cm1g {
 
 constexpr int SC_MAX = 16;      // fields per launch
 
+// Tile shapes of the pass, indexed like kTileShapes: TX x TY cells and KC
+// levels per block; the block has one more row of TX threads than the tile
+// has cell rows (the row that evaluates the tile's north and east faces).
+constexpr int kScalShapes[kNumTileShapes][3] = {{32, 7, 16}, {32, 7, 8}, {32, 3, 16}, {64, 3, 16}, {32, 7, 32}};
+
 struct ScalPass {
   ScalField f[SC_MAX];
   int n;
@@ -87,8 +92,8 @@ __host__ __device__ __forceinline__ int scal_pitch(int NI) {
 }
 
 template <int TX, int TY, int KC, int WENO>
-__global__ void __launch_bounds__(TX * TY, 3) k_scal_tile(DGrid g, ScalPass P) {
-  constexpr int NT = TX * TY;
+__global__ void __launch_bounds__(TX * (TY + 1), 3) k_scal_tile(DGrid g, ScalPass P) {
+  constexpr int NT = TX * (TY + 1);
   constexpr int SW = TX + 6, SH = TY + 6;                  // staged columns and rows
   constexpr int RD = 4;                                     // ring of staged planes
   constexpr int PL = ((8 + (SH - 1) * (TX + 19) + TX + 12) + 3) / 4 * 4;   // floats per plane
@@ -101,10 +106,12 @@ __global__ void __launch_bounds__(TX * TY, 3) k_scal_tile(DGrid g, ScalPass P) {
   __shared__ __align__(8) uint64_t bars[RD];
 
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty, lane = tid & 31;
+  // the first warp of the extra row issues the staging copies
+  const bool stager = (tid >= TX * TY && tid < TX * TY + 32);
   const int i0 = 1 + (int)blockIdx.x * TX, j0 = 1 + (int)blockIdx.y * TY;
   const int i = i0 + tx, j = j0 + ty;
   const int ni = g.ni, nj = g.nj, nk = g.nk, NI = g.NI, NJ = g.NJ;
-  const bool active = (i <= ni && j <= nj);
+  const bool active = (ty < TY && i <= ni && j <= nj);
   const bool doitw = (g.wbc == 2 && g.ibw), doite = (g.ebc == 2 && g.ibe);
   const bool doits = (g.sbc == 2 && g.ibs), doitn = (g.nbc == 2 && g.ibn);
   // the open-boundary fix-ups of adv.F touch only the cells next to an open edge
@@ -121,21 +128,22 @@ __global__ void __launch_bounds__(TX * TY, 3) k_scal_tile(DGrid g, ScalPass P) {
   const int kb0 = kc0 - 3;                                     // level of prof[.][0]
   const float rdx = g.rdx, rdy = g.rdy, rdz = g.rdz, smeps = g.smeps, dt = P.dt;
 
-  // faces of this thread (FaceSlots spreads the few extra faces over other warps)
-  int fxo[2], fxs[2], fyo[2], fys[2], fxd[2], fyd[2];
-  using FS = FaceSlots<NT, NFX, NFY>;
-#pragma unroll
-  for (int q = 0; q < 2; q++) {
-    const int f = FS::x(tid, q), fy_ = FS::y(tid, q);
-    fxo[q] = -1; fxs[q] = 0; fyo[q] = -1; fys[q] = 0; fxd[q] = f; fyd[q] = fy_;
-    if (f < NFX) {
-      const int row = f / (TX + 1), col = f - row * (TX + 1), ii = i0 + col, jj = j0 + row;
-      if (ii <= ni + 1 && jj <= nj) { fxo[q] = (ii - g.ib) + (NI + 1) * (jj - g.jb); fxs[q] = (row + 3) * SP + col; }
+  // faces of this thread: a cell row's thread owns the x face on the west of
+  // its cell and the y face on its south; the extra row's threads own the y
+  // faces north of the tile and (the first TY of them) the x faces east of it,
+  // so that every cell thread evaluates three faces and no thread more
+  int fxo = -1, fxs = 0, fyo = -1, fys = 0, fxd = NFX, fyd;
+  {
+    int xrow = ty, xcol = tx;
+    if (ty == TY) { xrow = tx; xcol = TX; }
+    if (xrow < TY) {
+      fxd = xrow * (TX + 1) + xcol;
+      const int ii = i0 + xcol, jj = j0 + xrow;
+      if (ii <= ni + 1 && jj <= nj) { fxo = (ii - g.ib) + (NI + 1) * (jj - g.jb); fxs = (xrow + 3) * SP + xcol; }
     }
-    if (fy_ < NFY) {
-      const int row = fy_ / TX, col = fy_ - row * TX, ii = i0 + col, jj = j0 + row;
-      if (ii <= ni && jj <= nj + 1) { fyo[q] = (ii - g.ib) + NI * (jj - g.jb); fys[q] = row * SP + col + 3; }
-    }
+    fyd = ty * TX + tx;
+    const int ii = i0 + tx, jj = j0 + ty;
+    if (ii <= ni && jj <= nj + 1) { fyo = (ii - g.ib) + NI * (jj - g.jb); fys = ty * SP + tx + 3; }
   }
   const int csel = (ty + 3) * SP + tx + 3;   // the cell in a staged plane
   const int xi = ty * (TX + 1) + tx, yi = ty * TX + tx;
@@ -193,19 +201,16 @@ __global__ void __launch_bounds__(TX * TY, 3) k_scal_tile(DGrid g, ScalPass P) {
     it_++;
     if (++ik_ > kc1) { ik_ = kc0; in_++; }
   };
-  if (tid < 32)
+  if (stager)
     while (it_ < RD && it_ < nitem) issue_next();
 
   // ---- per-item global reads, issued one item ahead
-  float pru[2], prv[2], pwhi = 0.0f, pe0 = 0.0f, pe1 = 0.0f, pe2 = 0.0f, pwtop = 0.0f;
+  float pru = 0.0f, prv = 0.0f, pwhi = 0.0f, pe0 = 0.0f, pe1 = 0.0f, pe2 = 0.0f, pwtop = 0.0f;
   auto fetch = [&](int nf, int kf) {
     const ScalField &F = P.f[nf];
     const float *uk = P.rru + (size_t)kf * planeU, *vk = P.rrv + (size_t)kf * planeV;
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-      pru[q] = (fxo[q] >= 0) ? LDG(&uk[fxo[q]]) : 0.0f;
-      prv[q] = (fyo[q] >= 0) ? LDG(&vk[fyo[q]]) : 0.0f;
-    }
+    pru = (fxo >= 0) ? LDG(&uk[fxo]) : 0.0f;
+    prv = (fyo >= 0) ? LDG(&vk[fyo]) : 0.0f;
     if (active) {
       const size_t o = (size_t)kf * planeS + oc;
       pwhi = (kf + 1 >= nk + 1) ? 0.0f : LDG(&P.rrw[o + planeS]);
@@ -258,7 +263,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_scal_tile(DGrid g, ScalPass P) {
     }
     for (int k = kc0; k <= kc1; k++, t++) {
       const float r0k = PR0[k], th0m = sadd ? PTH[k] : 0.0f;
-      const float ru0 = pru[0], ru1 = pru[1], rv0 = prv[0], rv1 = prv[1];
+      const float ru0 = pru, rv0 = prv;
       const float whi = pwhi, e0 = pe0, e1 = pe1, e2 = pe2;
       if (k < kc1) fetch(n, k + 1);                 // pwtop becomes s(k+4): the next level's window top
       else if (n + 1 < P.n) fetch(n + 1, kc0);
@@ -267,24 +272,22 @@ __global__ void __launch_bounds__(TX * TY, 3) k_scal_tile(DGrid g, ScalPass P) {
       const bool ok = mbar_wait(bar0 + 8 * slot, (uint32_t)((t / RD) & 1));
       const float *pl = &ring[slot][(int)((((uintptr_t)(F.s + (size_t)k * planeS + orow0)) >> 2) & 3) + 4];
       // ---- face values: each x/y face once, the upper z face once per column
-      auto xface = [&](int q, float ru) {
-        const float *p = pl + fxs[q];
+      auto xface = [&](float ru) {
+        const float *p = pl + fxs;
         float s0 = p[0], s1 = p[1], s2 = p[2], s3 = p[3], s4 = p[4], s5 = p[5];
         if (sadd) { s0 = th0m + s0; s1 = th0m + s1; s2 = th0m + s2; s3 = th0m + s3; s4 = th0m + s4; s5 = th0m + s5; }
-        fx[b][fxd[q]] = hflux5(ru * r0k, s0, s1, s2, s3, s4, s5, WENO, 0, weps);
-        ux[b][fxd[q]] = ru;
+        fx[b][fxd] = hflux5(ru * r0k, s0, s1, s2, s3, s4, s5, WENO, 0, weps);
+        ux[b][fxd] = ru;
       };
-      auto yface = [&](int q, float rv) {
-        const float *p = pl + fys[q];
+      auto yface = [&](float rv) {
+        const float *p = pl + fys;
         float s0 = p[0], s1 = p[SP], s2 = p[2 * SP], s3 = p[3 * SP], s4 = p[4 * SP], s5 = p[5 * SP];
         if (sadd) { s0 = th0m + s0; s1 = th0m + s1; s2 = th0m + s2; s3 = th0m + s3; s4 = th0m + s4; s5 = th0m + s5; }
-        fy[b][fyd[q]] = hflux5(rv * r0k, s0, s1, s2, s3, s4, s5, WENO, 0, weps);
-        vy[b][fyd[q]] = rv;
+        fy[b][fyd] = hflux5(rv * r0k, s0, s1, s2, s3, s4, s5, WENO, 0, weps);
+        vy[b][fyd] = rv;
       };
-      if (fxo[0] >= 0) xface(0, ru0);
-      if (fyo[0] >= 0) yface(0, rv0);
-      if (fxo[1] >= 0) xface(1, ru1);
-      if (fyo[1] >= 0) yface(1, rv1);
+      if (fxo >= 0) xface(ru0);
+      if (fyo >= 0) yface(rv0);
       const float fwhi = whi * PRF[k + 1];
       float fzhi = 0.0f, sc = 0.0f;
       if (active) {
@@ -296,7 +299,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_scal_tile(DGrid g, ScalPass P) {
       }
       if (__syncthreads_or(!ok)) { tfail = t; break; }
       // the plane of this item has been read: its slot takes the item RD later
-      if (tid < 32 && it_ < nitem) issue_next();
+      if (stager && it_ < nitem) issue_next();
       if (active) {
         float fx0 = fx[b][xi], fxp = fx[b][xi + 1], fy0 = fy[b][yi], fyp = fy[b][yi + TX];
         const float u0r = ux[b][xi], u1r = ux[b][xi + 1], v0r = vy[b][yi], v1r = vy[b][yi + TX];
@@ -356,7 +359,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_scal_tile(DGrid g, ScalPass P) {
 
 template <int TX, int TY, int KC>
 static void scal_shape(const DGrid &g, const ScalPass &P, int weno, cudaStream_t st) {
-  dim3 blk(TX, TY), grid((g.ni + TX - 1) / TX, (g.nj + TY - 1) / TY, (g.nk + KC - 1) / KC);
+  dim3 blk(TX, TY + 1), grid((g.ni + TX - 1) / TX, (g.nj + TY - 1) / TY, (g.nk + KC - 1) / KC);
   if (weno) k_scal_tile<TX, TY, KC, 1><<<grid, blk, 0, st>>>(g, P);
   else k_scal_tile<TX, TY, KC, 0><<<grid, blk, 0, st>>>(g, P);
 }
@@ -374,7 +377,7 @@ void launch_scal_pass(const DGrid &g, const ScalField *f, int n, const float *rr
     ProfScope _ps("k_scal_tile", st);
     static_assert(kNumTileShapes == 5, "one case per tile shape");
 #define CM1G_SCAL_SHAPE(m) \
-  case m: scal_shape<kTileShapes[m][0], kTileShapes[m][1], kTileShapes[m][2]>(g, P, weno, st); break;
+  case m: scal_shape<kScalShapes[m][0], kScalShapes[m][1], kScalShapes[m][2]>(g, P, weno, st); break;
     switch (g.tile_adv) {
       CM1G_SCAL_SHAPE(1)
       CM1G_SCAL_SHAPE(2)
