@@ -56,7 +56,7 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt, const float *ua
                   const float *ppi, float *pp3d, const float *piadv, const float *ppten, float *ppx,
                   const float *thv, const float *ppterm, float *rru, float *rrv, float *rrw, float *radbcw,
                   float *radbce, float *radbcs, float *radbcn, float *su, float *sv, float *su2,
-                  float *sv2, float *d1, float *d2, cudaStream_t st, int64_t *nl);
+                  float *sv2, float *d1, float *d2, float *lu, cudaStream_t st, int64_t *nl);
 int sound_max_nk();
 void launch_stage_prep(const DGrid &g, const float *th3d, const float *pp3d, const float *qv, const LiquidIn &liq,
                        int imoist, int eqtset, float *t11, float *t22, float *thterm, float *piadv, cudaStream_t st,
@@ -157,6 +157,7 @@ struct cm1g_ctx {
   float *uten = nullptr, *vten = nullptr, *wten = nullptr;
   float *rru = nullptr, *rrv = nullptr, *rrw = nullptr;
   float *su = nullptr, *sv = nullptr, *su2 = nullptr, *sv2 = nullptr, *d1 = nullptr, *d2 = nullptr;
+  float *lu = nullptr;   // LU factors of the acoustic column sweep on grids of more than sound_max_nk() levels
   float *sx[2 * (1 + 2 * CM1G_MAXQ)] = {};   // per-scalar stage buffers
   float *pdefscr = nullptr;                   // 6 s-arrays
   float *mdivx = nullptr;                     // divx of the momentum pass
@@ -220,7 +221,11 @@ struct ProfActive {
 
 static void *dalloc(cm1g_ctx *c, size_t bytes) {
   void *p = nullptr;
-  if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    (void)cudaGetLastError();
+    c->allocs.push_back(nullptr);   // the failure is found by the check after the allocations
+    return nullptr;
+  }
   cudaMemset(p, 0, bytes);
   c->allocs.push_back(p);
   return p;
@@ -263,7 +268,8 @@ static int check_config(const cm1g_config_t *c) {
   if (c->ngxy < 3) return set_err(CM1G_ERR_ARG, "ngxy must be >= 3 for 5th order");
   // the per-point kernels index rows with a launch grid's y extent
   if (c->nj + 2 * c->ngxy > 65535) return set_err(CM1G_ERR_UNSUPPORTED, "nj > %d rows is not built", 65535 - 2 * c->ngxy);
-  if (c->nk > sound_max_nk()) return set_err(CM1G_ERR_UNSUPPORTED, "nk > %d levels is not built", sound_max_nk());
+  // levels index a launch grid's y or z extent
+  if (c->nk + 2 > 65535) return set_err(CM1G_ERR_UNSUPPORTED, "nk > 65533 levels is not built");
   if (c->psolver != 3) return set_err(CM1G_ERR_UNSUPPORTED, "psolver=%d: only 3 (sound.F) is built", c->psolver);
   if (c->terrain_flag || c->axisymm || c->icor)
     return set_err(CM1G_ERR_UNSUPPORTED, "terrain, axisymmetric grids and Coriolis are not built");
@@ -385,6 +391,7 @@ extern "C" int cm1g_init(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_c
   c->su = (float *)dalloc(c, bU); c->sv = (float *)dalloc(c, bV);
   c->su2 = (float *)dalloc(c, bU); c->sv2 = (float *)dalloc(c, bV);
   c->d1 = (float *)dalloc(c, bS); c->d2 = (float *)dalloc(c, bS);
+  if (g.nk > sound_max_nk()) c->lu = (float *)dalloc(c, bS);
   int nsc = 1 + (cfg->imoist ? cfg->numq : 0) + (cfg->iptra ? cfg->npt : 0);
   for (int s = 0; s < 2 * nsc; s++) c->sx[s] = (float *)dalloc(c, bS);
   bool pdef_needed = cfg->imoist || (cfg->iptra && cfg->pdtra);
@@ -611,7 +618,7 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
                         th_in, qv_in, c->mdivx, st, nl, diffit ? &df : nullptr, liq.b8);
     launch_sound(g, cf.nsound, nrk, dt, d->ua, d->u3d, c->uten, d->va, d->v3d, c->vten, d->wa, d->w3d, c->wten,
                  d->ppi, d->pp3d, c->piadv, d->ppten, d->ppx, c->t11, c->t22, c->rru, c->rrv, c->rrw,
-                 d->radbcw, d->radbce, d->radbcs, d->radbcn, c->su, c->sv, c->su2, c->sv2, c->d1, c->d2, st, nl);
+                 d->radbcw, d->radbce, d->radbcs, d->radbcn, c->su, c->sv, c->su2, c->sv2, c->d1, c->d2, c->lu, st, nl);
     if (nrk == 3) launch_cfl(g, d->u3d, d->v3d, d->w3d, dt, c->cflbits, st, nl);
     if (openrad) launch_radbc4(g, d->ua, d->u3d, d->va, d->v3d, d->radbcw, d->radbce, d->radbcs, d->radbcn, dttmp, st, nl);
     const int weno = (cf.advwenos == 1 || (cf.advwenos == 2 && nrk == 3)) ? 1 : 0;
@@ -1103,14 +1110,16 @@ extern "C" int cm1g_autotune(cm1g_ctx_t *c, float dt, double mass1, const cm1g_s
   for (int knob = 0; knob < 3 && rc == CM1G_OK; knob++) {
     int best_v = knob == 0 ? 0 : knob == 1 ? cur.adv_shape : cur.mom_shape;
     float knob_best = 0.0f;
+    bool have = false;
     for (int v = 0; v < ncand[knob] && rc == CM1G_OK; v++) {
+      if (knob == 0 && v < 2 && c->g.nk > sound_max_nk()) continue;   // tile forms: too many levels
       cm1g_tune_t t = cur;
       if (knob == 0) t.sound_form = v;
       else if (knob == 1) t.adv_shape = v;
       else t.mom_shape = v;
       float ms = 0.0f;
       rc = trial(t, &ms);
-      if (rc == CM1G_OK && (v == 0 || ms < knob_best)) { knob_best = ms; best_v = v; }
+      if (rc == CM1G_OK && (!have || ms < knob_best)) { knob_best = ms; best_v = v; have = true; }
     }
     if (knob == 0) cur.sound_form = best_v;
     else if (knob == 1) cur.adv_shape = best_v;
@@ -1465,7 +1474,7 @@ extern "C" int cm1g_sound(cm1g_ctx_t *c, float dt, float *radbcw, float *radbce,
         *rn = S.in(radbcn, nrs, rad_out);
   if (S.err) return set_err(CM1G_ERR_NOMEM, "staging");
   launch_sound(g, c->cfg.nsound, nrk, dt, dua, du3, dut, dva, dv3, dvt, dwa, dw3, dwt, dppi, dpp, dpia, dppt, dppx,
-               dthv, dppterm, dru, drv, drw, rw, re, rs, rn, c->su, c->sv, c->su2, c->sv2, c->d1, c->d2, c->stream,
+               dthv, dppterm, dru, drv, drw, rw, re, rs, rn, c->su, c->sv, c->su2, c->sv2, c->d1, c->d2, c->lu, c->stream,
                &c->nlaunch);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));

@@ -67,13 +67,12 @@ void launch_stage_prep(const DGrid &g, const float *th3d, const float *pp3d, con
 // ---------------------------------------------------------------------
 // radbcew4 / radbcns4 (bc.F:2054-2178): column-averaged phase speeds
 // ---------------------------------------------------------------------
-// One warp per boundary column: the lanes form the phase speeds of the
-// column's levels in parallel, then lane 0 adds them in the reference's
-// order k = 1..nk, and the lanes write the column average back.
+// One warp per boundary column: the lanes form the phase speeds of 32
+// levels at a time, every lane adds them (exchanged by shuffles) in the
+// reference's order k = 1..nk, and the lanes write the column average back.
 __global__ void k_radbc4(DGrid g, const float *__restrict__ ua, const float *__restrict__ u3d,
                          const float *__restrict__ va, const float *__restrict__ v3d,
                          float *radbcw, float *radbce, float *radbcs, float *radbcn, float dt) {
-  __shared__ float cbs[4][130];
   const int wib = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
   const int t = (int)blockIdx.x * 4 + wib;     // column along the side
   const int side = (int)blockIdx.y;            // 0 w, 1 e, 2 s, 3 n
@@ -87,33 +86,34 @@ __global__ void k_radbc4(DGrid g, const float *__restrict__ ua, const float *__r
   if (side == 2) on = on && g.ibs && g.sbc == 2;
   if (side == 3) on = on && g.ibn && g.nbc == 2;
   if (!on) return;                             // whole warp leaves together
-  float *cb = cbs[wib];
-  if (ew) {
-    const int j = 1 + t;
-    const int ia = (side == 0) ? 2 : ni, ib2 = (side == 0) ? 3 : ni - 1;
-    const float ruf = LDG(&g.ruf[ia - g.ib]);
-    for (int k = 1 + lane; k <= nk; k += 32) {
+  // phase speed of level k (0 outside 1..nk)
+  auto speed = [&](int k) -> float {
+    if (k > nk) return 0.0f;
+    if (ew) {
+      const int j = 1 + t;
+      const int ia = (side == 0) ? 2 : ni, ib2 = (side == 0) ? 3 : ni - 1;
+      const float ruf = LDG(&g.ruf[ia - g.ib]);
       float foo = (side == 0) ? (ua[iU(g, ib2, j, k)] - ua[iU(g, ia, j, k)]) : (ua[iU(g, ia, j, k)] - ua[iU(g, ib2, j, k)]);
       float c = g.dx * ruf * (ua[iU(g, ia, j, k)] - u3d[iU(g, ia, j, k)]) / (dt * (copysignf(1.e-10f, foo) + foo));
-      cb[k] = (side == 0) ? fmaxf(fminf(c, 0.0f), -umax) : fminf(fmaxf(c, 0.0f), umax);
+      return (side == 0) ? fmaxf(fminf(c, 0.0f), -umax) : fminf(fmaxf(c, 0.0f), umax);
     }
-  } else {
     const int i = 1 + t;
     const int ja = (side == 2) ? 2 : nj, jb2 = (side == 2) ? 3 : nj - 1;
     const float rvf = LDG(&g.rvf[ja - g.jb]);
-    for (int k = 1 + lane; k <= nk; k += 32) {
-      float foo = (side == 2) ? (va[iV(g, i, jb2, k)] - va[iV(g, i, ja, k)]) : (va[iV(g, i, ja, k)] - va[iV(g, i, jb2, k)]);
-      float c = g.dy * rvf * (va[iV(g, i, ja, k)] - v3d[iV(g, i, ja, k)]) / (dt * (copysignf(1.e-10f, foo) + foo));
-      cb[k] = (side == 2) ? fmaxf(fminf(c, 0.0f), -umax) : fminf(fmaxf(c, 0.0f), umax);
+    float foo = (side == 2) ? (va[iV(g, i, jb2, k)] - va[iV(g, i, ja, k)]) : (va[iV(g, i, ja, k)] - va[iV(g, i, jb2, k)]);
+    float c = g.dy * rvf * (va[iV(g, i, ja, k)] - v3d[iV(g, i, ja, k)]) / (dt * (copysignf(1.e-10f, foo) + foo));
+    return (side == 2) ? fmaxf(fminf(c, 0.0f), -umax) : fminf(fmaxf(c, 0.0f), umax);
+  };
+  float avg = 0.0f;
+  for (int k0 = 1; k0 <= nk; k0 += 32) {
+    const float c = speed(k0 + lane);
+#pragma unroll
+    for (int m = 0; m < 32; m++) {
+      const float cm = __shfl_sync(0xffffffffu, c, m);
+      if (k0 + m <= nk) avg = avg + cm;
     }
   }
-  __syncwarp();
-  float avg = 0.0f;
-  if (lane == 0) {
-    for (int k = 1; k <= nk; k++) avg = avg + cb[k];
-    avg = avg / (float)nk;
-  }
-  avg = __shfl_sync(0xffffffffu, avg, 0);
+  avg = avg / (float)nk;
   float *r = (side == 0) ? radbcw : (side == 1) ? radbce : (side == 2) ? radbcs : radbcn;
   for (int k = 1 + lane; k <= nk; k += 32) {
     if (ew) r[(1 + t - g.jb) + (long)g.NJ * k] = avg;

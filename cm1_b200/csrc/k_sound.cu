@@ -41,6 +41,7 @@ struct SoundIO {
   const float *thv, *ppterm, *piadv;
   float *radbcw, *radbce, *radbcs, *radbcn;   // phase speeds (irbc = 2: formed and stored here)
   float *ppx;                     // last step of the final stage: kdiv*(pi'_new - pi'_old)
+  float *lu;                      // column sweep: LU factors in this scalar-shaped array (null: shared memory)
 };
 
 struct SoundStep {
@@ -347,7 +348,7 @@ static const int SNC_TX = 32;
 #define CM1G_SOUND_COL_MIN_COLUMNS (1L << 20)
 #endif
 
-template <int TX, int TY>
+template <int TX, int TY, bool GLU>
 __global__ void __launch_bounds__(TX * TY, 4) k_sound_col(DGrid g, SoundIO io, SoundStep p) {
   constexpr int NC = TX * TY;
   extern __shared__ float sm[];
@@ -356,12 +357,14 @@ __global__ void __launch_bounds__(TX * TY, 4) k_sound_col(DGrid g, SoundIO io, S
   const int j = 1 + (int)blockIdx.y * TY + (int)threadIdx.y;
   const int ni = g.ni, nj = g.nj, nk = g.nk;
   if (i > ni || j > nj) return;     // no barriers below
-  float *D1 = sm;                   // D1[k*NC + t]: LU factor of level k
   const float dts = p.dts, alph = g.alph, beta = 1.0f - alph, asq = alph * alph;
   const float cp = g.c.cp, rdx = g.rdx, rdy = g.rdy, rdz = g.rdz;
   const long plane = (long)g.NI * g.NJ;
   const long oc = iS(g, i, j, 0), ocu = iU(g, i, j, 0), ocv = iV(g, i, j, 0);
   const long planeU = (long)(g.NI + 1) * g.NJ, planeV = (long)g.NI * (g.NJ + 1);
+  // the LU factor dum1 of level k: private to the column, in shared memory,
+  // or for grids with more levels than that holds, in the global array io.lu
+  auto D1 = [&](int k) -> float & { return GLU ? io.lu[oc + k * plane] : sm[k * NC + t]; };
 
   // pk1+qk and pk2-qk of level k (sound.F:117-135, 188-189)
   auto coef = [&](int k, float pid, float pia, float piu, float pptm, float *p1, float *p2) {
@@ -492,7 +495,7 @@ __global__ void __launch_bounds__(TX * TY, 4) k_sound_col(DGrid g, SoundIO io, S
           const float rr = __frcp_rn(bb);
           d1p = -cc * rr;
           d2p = dd * rr;
-          D1[k * NC + t] = d1p;
+          D1(k) = d1p;
           io.w_out[o] = d2p;
         } else {
           const float aa = -asq * (+mm * p1m);
@@ -501,7 +504,7 @@ __global__ void __launch_bounds__(TX * TY, 4) k_sound_col(DGrid g, SoundIO io, S
             const float cc = -asq * (-mm * p2);
             d1p = -cc * rr;
             d2p = (dd - aa * d2p) * rr;
-            D1[k * NC + t] = d1p;
+            D1(k) = d1p;
             io.w_out[o] = d2p;
           } else {
             io.w_out[o] = (dd - aa * d2p) * rr;       // w(nk)
@@ -529,7 +532,7 @@ __global__ void __launch_bounds__(TX * TY, 4) k_sound_col(DGrid g, SoundIO io, S
       const float ac = p.first ? LDG(&io.wa[o]) * beta : io.rrw[o];
       float wk;
       if (k == nk) wk = io.w_out[o];
-      else if (k >= 2) wk = D1[k * NC + t] * wup + io.w_out[o];
+      else if (k >= 2) wk = D1(k) * wup + io.w_out[o];
       else wk = io.w_in[o];
       float p1, p2;
       coef(k, pid, pia, piu, pptm, &p1, &p2);
@@ -571,19 +574,23 @@ void sound_nloop(int nsound, int nrk, float dt, int *nloop_out, float *dts_out) 
 
 size_t sound_smem_bytes(const DGrid &g) { return (size_t)5 * (g.nk + 2) * SND_TX * sizeof(float); }
 int sound_max_nk() { return SND_NW * SND_KPT; }
+// grids with more levels run the column sweep with its LU factors in global memory
+static bool sound_tall(const DGrid &g) { return g.nk > SND_NW * SND_KPT; }
 
 // The acoustic kernel's forms (kNumSoundCfgs): the tile form with 8 or 4
 // warps over the levels of 32 columns, and the column sweep with 32 x 4 or
 // 32 x 2 columns per block.  Both tile forms cover SND_NW * SND_KPT levels.
 static_assert(SND_NW * SND_KPT == (SND_NW / 2) * (SND_KPT * 2), "both tile forms cover the same levels");
 template <int TY>
-static size_t sound_col_smem(const DGrid &g) { return (size_t)(g.nk + 2) * SNC_TX * TY * sizeof(float); }
+static size_t sound_col_smem(const DGrid &g) {
+  return sound_tall(g) ? 0 : (size_t)(g.nk + 2) * SNC_TX * TY * sizeof(float);
+}
 
 static void sound_set_attributes() {
   static bool done = false;
   if (done) return;
-  cudaFuncSetAttribute(k_sound_col<SNC_TX, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_sound_col<SNC_TX, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_sound_col<SNC_TX, 4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_sound_col<SNC_TX, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW, SND_KPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        200 * 1024);
   cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW / 2, SND_KPT * 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -600,14 +607,16 @@ static void sound_set_attributes() {
 // from the current u3d/v3d/w3d/pp3d (sound.F:192-208); at later stages it
 // first resets them to the start-of-step ua/va/wa/ppi (sound.F:212-230).
 // u3d/v3d/w3d/pp3d receive the result; su/sv/su2/sv2 are scratch for the
-// u/v double buffer, d1/d2 for ppd.  rru/rrv/rrw receive the averages.
+// u/v double buffer, d1/d2 for ppd, lu (scalar-shaped; needed only when nk
+// exceeds sound_max_nk()) for the column sweep's LU factors.  rru/rrv/rrw
+// receive the averages.
 void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
                   const float *ua, float *u3d, const float *uten, const float *va, float *v3d, const float *vten,
                   const float *wa, float *w3d, const float *wten, const float *ppi, float *pp3d,
                   const float *piadv, const float *ppten, float *ppx, const float *thv, const float *ppterm,
                   float *rru, float *rrv, float *rrw, float *radbcw, float *radbce,
                   float *radbcs, float *radbcn, float *su, float *sv, float *su2, float *sv2,
-                  float *d1, float *d2, cudaStream_t st, int64_t *nl) {
+                  float *d1, float *d2, float *lu, cudaStream_t st, int64_t *nl) {
   int nloop;
   float dts;
   sound_nloop(nsound, nrk, dt, &nloop, &dts);
@@ -622,6 +631,9 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
     if (!strcmp(f, "col")) cfg = 2;
     else if (!strcmp(f, "tile")) cfg = 0;
   }
+  // the tile forms hold at most sound_max_nk() levels of a column
+  const bool tall = sound_tall(g);
+  if (tall && cfg < 2) cfg = 2;
   const int cty = (cfg == 3) ? 2 : 4, nw = (cfg == 1) ? SND_NW / 2 : SND_NW;
   const bool col = cfg >= 2;
   dim3 blk = col ? dim3(SNC_TX, cty) : dim3(SND_TX, nw);
@@ -644,6 +656,7 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
     io.thv = thv; io.ppterm = ppterm; io.piadv = piadv;
     io.radbcw = radbcw; io.radbce = radbce; io.radbcs = radbcs; io.radbcn = radbcn;
     io.ppx = ppx;
+    io.lu = lu;
     SoundStep sp;
     sp.dts = dts; sp.tavg = 1.0f / (float)nloop;
     sp.first = (n == 1); sp.last = (n == nloop); sp.write_ppx = (nrk == 3 && n == nloop);
@@ -652,8 +665,14 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
       ProfScope _ps("k_sound_step", st);
       switch (cfg) {
         case 1: k_sound_tile<SND_TX, SND_NW / 2, SND_KPT * 2><<<grid, blk, smem, st>>>(g, io, sp); break;
-        case 2: k_sound_col<SNC_TX, 4><<<grid, blk, smem, st>>>(g, io, sp); break;
-        case 3: k_sound_col<SNC_TX, 2><<<grid, blk, smem, st>>>(g, io, sp); break;
+        case 2:
+          if (tall) k_sound_col<SNC_TX, 4, true><<<grid, blk, 0, st>>>(g, io, sp);
+          else k_sound_col<SNC_TX, 4, false><<<grid, blk, smem, st>>>(g, io, sp);
+          break;
+        case 3:
+          if (tall) k_sound_col<SNC_TX, 2, true><<<grid, blk, 0, st>>>(g, io, sp);
+          else k_sound_col<SNC_TX, 2, false><<<grid, blk, smem, st>>>(g, io, sp);
+          break;
         default: k_sound_tile<SND_TX, SND_NW, SND_KPT><<<grid, blk, smem, st>>>(g, io, sp); break;
       }
     }

@@ -57,6 +57,10 @@ CASES = [
     # large step (irbc=1) and from u3d at every small step (irbc=2)
     ("supercell", dict(ni=40, nj=36, nk=40, irbc=1)),
     ("supercell", dict(ni=40, nj=36, nk=40, irbc=2)),
+    # more levels than the acoustic tile form holds (column sweep with its
+    # LU factors in global memory; column-averaged radiative phase speeds)
+    ("cbl", dict(ni=24, nj=20, nk=160)),
+    ("supercell", dict(ni=24, nj=20, nk=150)),
 ]
 
 

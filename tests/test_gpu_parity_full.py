@@ -70,6 +70,13 @@ def test_cbl_large_grid_autotuned(cm1g, oracle_lib):
     _one_step_vs_oracle(cm1g, oracle_lib, case, autotune=True)
 
 
+def test_tall_grid_autotuned(cm1g, oracle_lib):
+    """256 levels: the autotuner chooses among the column-sweep forms only."""
+    case = make_case("cbl", ni=64, nj=64, nk=256)
+    chosen = _one_step_vs_oracle(cm1g, oracle_lib, case, autotune=True)
+    assert chosen["sound_form"] in (2, 3), chosen
+
+
 @pytest.mark.parametrize("form", [2, 3])
 def test_cbl_large_grid_column_sweep(cm1g, oracle_lib, form):
     case = make_case("cbl", ni=512, nj=512, nk=128)
