@@ -215,6 +215,53 @@ def _tally(tunes):
     return out
 
 
+def other_workload(name, steps, warmup, hbm):
+    """Device-resident throughput of another configuration (one GPU, the
+    library's default launch shapes, CUDA-graph replay), measured after the
+    main workload: the dry warm bubble (64x64x40) and the convective boundary
+    layer (1024x1024x128, doubly periodic, WENO5 theta + 2 scalars)."""
+    import torch
+    from cm1_b200.cases import make_case
+    from cm1_b200 import binding
+    case = make_case(name)
+    cfg = case.cfg
+    cells = cfg.ni * cfg.nj * cfg.nk
+    ctx = binding.Context(cfg, case.grid)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    dev = binding.to_device(case.state)
+    del case.state
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            ctx.step(dev, case.dt, case.mass1, use_graph=True)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        ctx.step(dev, case.dt, case.mass1, use_graph=True)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms_step = ev0.elapsed_time(ev1) / steps
+    ctx.profile(True)
+    with torch.cuda.stream(stream):
+        ctx.step(dev, case.dt, case.mass1, use_graph=False)
+    torch.cuda.synchronize()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    ctx.close()
+    del dev
+    torch.cuda.empty_cache()
+    B = algorithmic_bytes_per_cell(cfg)
+    gbs = B * cells / (ms_step * 1e-3) / 1e9
+    top = sorted(prof.items(), key=lambda kv: -kv[1][1])[:4]
+    return {"workload": name, "grid": [cfg.ni, cfg.nj, cfg.nk], "steps": steps, "warmup": warmup,
+            "ms_per_step": ms_step, "value": cells / (ms_step * 1e-3), "unit": "cell-updates/s",
+            "launch_shapes": "library defaults",
+            "step_roofline": {"algorithmic_bytes_per_cell": B, "achieved_gbs": gbs, "frac": gbs / hbm},
+            "top_kernels_ms_per_step": {k: v[1] for k, v in top}}
+
+
 def run_ensemble(args):
     """The uneven 64-member warm-bubble ensemble: one graph launch per large
     step for all members (cm1g_ensemble_step) against looping the members'
@@ -300,6 +347,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of the autotuner's")
+    ap.add_argument("--no-other", action="store_true",
+                    help="skip the dry-bubble and CBL throughput lines measured after the main workload")
     ap.add_argument("--tune-cache", default=None,
                     help="text file of autotuner results per grid (read if present, appended otherwise)")
     args = ap.parse_args()
@@ -418,6 +467,14 @@ def main():
                "sample": "%d full large steps of the %s workload on the host (CPU restatement, OpenMP)"
                          % (args.cpu_steps, args.workload)}
 
+    # ---- the other configurations' throughput (rank 0, N=1 only)
+    others = None
+    if rank == 0 and world == 1 and not args.no_other and args.workload == "supercell":
+        ctx.close()
+        del dev, host
+        torch.cuda.empty_cache()
+        others = [other_workload("dry_bubble", 50, 3, hbm), other_workload("cbl", 5, 3, hbm)]
+
     if rank == 0:
         line = {"metric": "cell-updates/s per RK3 large step", "value": value, "unit": "cell-updates/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -431,7 +488,8 @@ def main():
                 "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "steps": e2e_steps},
                 "gpu_launches": launches, "clocks": clk.summary(),
-                "kernel_ms_per_step": {k: v[1] / 2 for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}}
+                "kernel_ms_per_step": {k: v[1] / 2 for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+                "other_workloads": others}
         print(json.dumps(line))
     if dist:
         dist.barrier()
