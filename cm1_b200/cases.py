@@ -230,8 +230,9 @@ WORKLOADS = {
 def make_case(name, seed=1234, **over):
     """Build a seeded workload.  `over` may override ni, nj, nk, dx, dz, dt,
     nsound, advwenos, npt, bc, moist, ptype (for small parity cases), eqtset,
-    irbc (the open boundaries' phase speeds: 1, 2 or 4), and add diff6 (kdiff6
-    of the 6th-order diffusion) and mdiff."""
+    irbc (the open boundaries' phase speeds: 1, 2 or 4), roflux (1: outflow
+    restricted to the inflow), and add diff6 (kdiff6 of the 6th-order
+    diffusion) and mdiff."""
     w = dict(WORKLOADS[name])
     w.update(over)
     ni, nj, nk = int(w["ni"]), int(w["nj"]), int(w["nk"])
@@ -256,7 +257,7 @@ def make_case(name, seed=1234, **over):
     cfg.tsmall, cfg.qsmall = 1.0e-4, 1.0e-14
     cfg.iptra, cfg.npt, cfg.pdtra = (1 if npt > 0 else 0), npt, 1
     cfg.apmasscon = 1
-    cfg.irbc, cfg.cstar, cfg.roflux = int(w.get("irbc", 4)), 30.0, 0
+    cfg.irbc, cfg.cstar, cfg.roflux = int(w.get("irbc", 4)), 30.0, int(w.get("roflux", 0))
     cfg.smeps = 1.0e-30
     cfg.testcase, cfg.psolver, cfg.terrain_flag, cfg.axisymm, cfg.icor = 0, 3, 0, 0, 0
     for q in range(CM1G_MAXQ):

@@ -56,7 +56,7 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt, const float *ua
                   const float *ppi, float *pp3d, const float *piadv, const float *ppten, float *ppx,
                   const float *thv, const float *ppterm, float *rru, float *rrv, float *rrw, float *radbcw,
                   float *radbce, float *radbcs, float *radbcn, float *su, float *sv, float *su2,
-                  float *sv2, float *d1, float *d2, float *lu, cudaStream_t st, int64_t *nl);
+                  float *sv2, float *d1, float *d2, float *lu, float *rbnd, cudaStream_t st, int64_t *nl);
 int sound_max_nk();
 void launch_stage_prep(const DGrid &g, const float *th3d, const float *pp3d, const float *qv, const LiquidIn &liq,
                        int imoist, int eqtset, float *t11, float *t22, float *thterm, float *piadv, cudaStream_t st,
@@ -157,7 +157,8 @@ struct cm1g_ctx {
   float *uten = nullptr, *vten = nullptr, *wten = nullptr;
   float *rru = nullptr, *rrv = nullptr, *rrw = nullptr;
   float *su = nullptr, *sv = nullptr, *su2 = nullptr, *sv2 = nullptr, *d1 = nullptr, *d2 = nullptr;
-  float *lu = nullptr;   // LU factors of the acoustic column sweep on grids of more than sound_max_nk() levels
+  float *lu = nullptr;   // LU factors of the acoustic column sweep
+  float *rbnd = nullptr; // roflux = 1: restricted open-boundary u/v of an acoustic step
   float *sx[2 * (1 + 2 * CM1G_MAXQ)] = {};   // per-scalar stage buffers
   float *pdefscr = nullptr;                   // 6 s-arrays
   float *mdivx = nullptr;                     // divx of the momentum pass
@@ -289,7 +290,9 @@ static int check_config(const cm1g_config_t *c) {
     if (!(c->tsmall > 0.0f) || !(c->qsmall >= 0.0f)) return set_err(CM1G_ERR_ARG, "tsmall/qsmall not set");
   }
   if (c->iptra && (c->npt < 0 || c->npt > CM1G_MAXQ)) return set_err(CM1G_ERR_ARG, "npt out of range");
-  if (c->roflux != 0) return set_err(CM1G_ERR_UNSUPPORTED, "roflux=1 is not built");
+  if (c->roflux != 0 && c->roflux != 1) return set_err(CM1G_ERR_ARG, "roflux must be 0 or 1");
+  // the per-level flux sums of one acoustic step are held in shared memory
+  if (c->roflux == 1 && c->nk > 6000) return set_err(CM1G_ERR_UNSUPPORTED, "roflux=1 with nk > 6000 is not built");
   if (c->idiff != 0 && c->difforder != 6)
     return set_err(CM1G_ERR_UNSUPPORTED, "diffusion: only the 6th-order form (difforder=6) is built");
   if (c->idiff < 0 || c->idiff > 1) return set_err(CM1G_ERR_UNSUPPORTED, "idiff must be 0 or 1");
@@ -339,7 +342,7 @@ extern "C" int cm1g_init(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_c
   g.wbc = cfg->wbc; g.ebc = cfg->ebc; g.sbc = cfg->sbc; g.nbc = cfg->nbc;
   g.ibw = cfg->wbc != 1; g.ibe = cfg->ebc != 1; g.ibs = cfg->sbc != 1; g.ibn = cfg->nbc != 1;
   g.smeps = cfg->smeps; g.alph = cfg->alph; g.kdiv = cfg->kdiv;
-  g.irbc = cfg->irbc; g.cstar = cfg->cstar;
+  g.irbc = cfg->irbc; g.cstar = cfg->cstar; g.roflux = cfg->roflux;
   g.tile_adv = 0; g.tile_mom = 0; g.sound_cfg = -1;
   set_constants_(cfg->testcase, &g.c);
 
@@ -391,7 +394,9 @@ extern "C" int cm1g_init(const cm1g_config_t *cfg, const cm1g_grid_t *gr, cm1g_c
   c->su = (float *)dalloc(c, bU); c->sv = (float *)dalloc(c, bV);
   c->su2 = (float *)dalloc(c, bU); c->sv2 = (float *)dalloc(c, bV);
   c->d1 = (float *)dalloc(c, bS); c->d2 = (float *)dalloc(c, bS);
-  if (g.nk > sound_max_nk()) c->lu = (float *)dalloc(c, bS);
+  c->lu = (float *)dalloc(c, bS);
+  if (cfg->roflux == 1)
+    c->rbnd = (float *)dalloc(c, (size_t)2 * (g.NJ + g.NI) * g.NK * sizeof(float));
   int nsc = 1 + (cfg->imoist ? cfg->numq : 0) + (cfg->iptra ? cfg->npt : 0);
   for (int s = 0; s < 2 * nsc; s++) c->sx[s] = (float *)dalloc(c, bS);
   bool pdef_needed = cfg->imoist || (cfg->iptra && cfg->pdtra);
@@ -618,7 +623,7 @@ static void run_solve2(cm1g_ctx *c, const cm1g_state_t *d, float dt, double mass
                         th_in, qv_in, c->mdivx, st, nl, diffit ? &df : nullptr, liq.b8);
     launch_sound(g, cf.nsound, nrk, dt, d->ua, d->u3d, c->uten, d->va, d->v3d, c->vten, d->wa, d->w3d, c->wten,
                  d->ppi, d->pp3d, c->piadv, d->ppten, d->ppx, c->t11, c->t22, c->rru, c->rrv, c->rrw,
-                 d->radbcw, d->radbce, d->radbcs, d->radbcn, c->su, c->sv, c->su2, c->sv2, c->d1, c->d2, c->lu, st, nl);
+                 d->radbcw, d->radbce, d->radbcs, d->radbcn, c->su, c->sv, c->su2, c->sv2, c->d1, c->d2, c->lu, c->rbnd, st, nl);
     if (nrk == 3) launch_cfl(g, d->u3d, d->v3d, d->w3d, dt, c->cflbits, st, nl);
     if (openrad) launch_radbc4(g, d->ua, d->u3d, d->va, d->v3d, d->radbcw, d->radbce, d->radbcs, d->radbcn, dttmp, st, nl);
     const int weno = (cf.advwenos == 1 || (cf.advwenos == 2 && nrk == 3)) ? 1 : 0;
@@ -1474,7 +1479,7 @@ extern "C" int cm1g_sound(cm1g_ctx_t *c, float dt, float *radbcw, float *radbce,
         *rn = S.in(radbcn, nrs, rad_out);
   if (S.err) return set_err(CM1G_ERR_NOMEM, "staging");
   launch_sound(g, c->cfg.nsound, nrk, dt, dua, du3, dut, dva, dv3, dvt, dwa, dw3, dwt, dppi, dpp, dpia, dppt, dppx,
-               dthv, dppterm, dru, drv, drw, rw, re, rs, rn, c->su, c->sv, c->su2, c->sv2, c->d1, c->d2, c->lu, c->stream,
+               dthv, dppterm, dru, drv, drw, rw, re, rs, rn, c->su, c->sv, c->su2, c->sv2, c->d1, c->d2, c->lu, c->rbnd, c->stream,
                &c->nlaunch);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(CM1G_ERR_CUDA, "%s", cudaGetErrorString(e));

@@ -27,6 +27,7 @@ struct DGrid {
   float smeps, alph, kdiv;
   int irbc;                   // open-boundary phase speeds: 1 and 2 Klemp-Wilhelmson, 4 Durran-Klemp
   float cstar;                // the Klemp-Wilhelmson gravity-wave speed of irbc 1 and 2
+  int roflux;                 // 1: the open boundaries' outflow is restricted to the inflow at every acoustic step
   Consts c;
   // vertical profiles (index k, k = 0..nk+1; w-profiles to nk+2)
   const float *mh, *rmh, *mf, *rho0, *rr0, *rf0, *rrf0, *c1, *c2, *pi0, *th0, *rth0, *qv0, *qc0, *qi0;

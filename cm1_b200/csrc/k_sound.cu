@@ -41,7 +41,8 @@ struct SoundIO {
   const float *thv, *ppterm, *piadv;
   float *radbcw, *radbce, *radbcs, *radbcn;   // phase speeds (irbc = 2: formed and stored here)
   float *ppx;                     // last step of the final stage: kdiv*(pi'_new - pi'_old)
-  float *lu;                      // column sweep: LU factors in this scalar-shaped array (null: shared memory)
+  float *lu;                      // column sweep: LU factors (a scalar-shaped scratch array)
+  const float *ubw, *ube, *vbs, *vbn;   // roflux = 1: this step's restricted boundary u/v (k_openbc_restrict)
 };
 
 struct SoundStep {
@@ -90,6 +91,109 @@ __device__ __forceinline__ float radbc_out(const DGrid &g, float &slot, float ub
   const float r = (c > 0.0f) ? c : 0.0f;
   slot = r;
   return r;
+}
+
+// roflux = 1: the open-boundary velocities of one acoustic step, restricted
+// so that the inflow through the open boundaries balances the outflow
+// (restrict_openbc_we/sn, bc.F:2180-2384, called by sound.F:283-285 and
+// 299-301 after the boundary tendency of ssopenbcw/e/s/n).  One block: the
+// thread of level k forms the level's boundary values and its binary64
+// outflow and inflow sums (over j, resp. i, west/south before east/north,
+// as the reference's loops run), one thread adds the levels in order, and
+// the outflow points are scaled by inflow/outflow.  The acoustic kernels
+// then read the values instead of forming them.  Shared memory: 4 (nk+1)
+// doubles.
+__global__ void k_openbc_restrict(DGrid g, SoundIO io, float dts, float *ubw, float *ube, float *vbs, float *vbn) {
+  extern __shared__ double rsum[];   // out/in sums of the we and sn boundaries by level
+  const int ni = g.ni, nj = g.nj, nk = g.nk, L = nk + 1;
+  double *tow = rsum, *tiw = rsum + L, *tos = rsum + 2 * L, *tis = rsum + 3 * L;
+  __shared__ double t3[2];
+  const bool w = g.wbc == 2 && g.ibw, e = g.ebc == 2 && g.ibe, s = g.sbc == 2 && g.ibs, n = g.nbc == 2 && g.ibn;
+  const float rdx = g.rdx, rdy = g.rdy;
+  for (int k = 1 + (int)threadIdx.x; k <= nk; k += blockDim.x) {
+    const float r0 = LDG(&g.rho0[k]), rm = LDG(&g.rmh[k]);
+    double to = 0.0, ti = 0.0;
+    if (w)
+      for (int j = 1; j <= nj; j++) {
+        const long o = iU(g, 1, j, k);
+        const float u0v = io.u_in[o], u1v = io.u_in[o + 1];
+        const float uo = u0v + dts * (-radbc_in(g, RJK(g, io.radbcw, j, k), u0v) * (u1v - u0v) * rdx *
+                                      LDG(&g.uh[1 - g.ib]) + LDG(&io.uten[o]));
+        RJK(g, ubw, j, k) = uo;
+        const float f = r0 * uo * LDG(&g.rvh[j - g.jb]) * rm;
+        to = to - (double)fminf(0.0f, f);
+        ti = ti + (double)fmaxf(0.0f, f);
+      }
+    if (e)
+      for (int j = 1; j <= nj; j++) {
+        const long o = iU(g, ni + 1, j, k);
+        const float u1v = io.u_in[o], u0v = io.u_in[o - 1];
+        const float uo = u1v + dts * (-radbc_out(g, RJK(g, io.radbce, j, k), u1v) * (u1v - u0v) * rdx *
+                                      LDG(&g.uh[ni - g.ib]) + LDG(&io.uten[o]));
+        RJK(g, ube, j, k) = uo;
+        const float f = r0 * uo * LDG(&g.rvh[j - g.jb]) * rm;
+        to = to + (double)fmaxf(0.0f, f);
+        ti = ti - (double)fminf(0.0f, f);
+      }
+    tow[k] = to; tiw[k] = ti;
+    to = 0.0; ti = 0.0;
+    if (s)
+      for (int i = 1; i <= ni; i++) {
+        const long o = iV(g, i, 1, k);
+        const float v0v = io.v_in[o], v1v = io.v_in[o + g.NI];
+        const float vo = v0v + dts * (-radbc_in(g, RIK(g, io.radbcs, i, k), v0v) * (v1v - v0v) * rdy *
+                                      LDG(&g.vh[1 - g.jb]) + LDG(&io.vten[o]));
+        RIK(g, vbs, i, k) = vo;
+        const float f = r0 * vo * LDG(&g.ruh[i - g.ib]) * rm;
+        to = to - (double)fminf(0.0f, f);
+        ti = ti + (double)fmaxf(0.0f, f);
+      }
+    if (n)
+      for (int i = 1; i <= ni; i++) {
+        const long o = iV(g, i, nj + 1, k);
+        const float v1v = io.v_in[o], v0v = io.v_in[o - g.NI];
+        const float vo = v1v + dts * (-radbc_out(g, RIK(g, io.radbcn, i, k), v1v) * (v1v - v0v) * rdy *
+                                      LDG(&g.vh[nj - g.jb]) + LDG(&io.vten[o]));
+        RIK(g, vbn, i, k) = vo;
+        const float f = r0 * vo * LDG(&g.ruh[i - g.ib]) * rm;
+        to = to + (double)fmaxf(0.0f, f);
+        ti = ti - (double)fminf(0.0f, f);
+      }
+    tos[k] = to; tis[k] = ti;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    const double *to = threadIdx.x == 0 ? tow : tos, *ti = threadIdx.x == 0 ? tiw : tis;
+    double fo = 0.0, fi = 0.0;
+    for (int k = 1; k <= nk; k++) { fo = fo + to[k]; fi = fi + ti[k]; }
+    t3[threadIdx.x] = (fi + 1.0e-20) / (fo + 1.0e-20);
+  }
+  __syncthreads();
+  const double tw = t3[0], ts = t3[1];
+  for (int k = 1 + (int)threadIdx.x; k <= nk; k += blockDim.x) {
+    const float r0 = LDG(&g.rho0[k]);
+    const double r0d = (double)r0;
+    for (int j = 1; j <= nj && (w || e); j++) {
+      if (w) {
+        const double u1 = (double)(r0 * RJK(g, ubw, j, k));
+        if (u1 < 0.0) RJK(g, ubw, j, k) = (float)(u1 * tw / r0d);
+      }
+      if (e) {
+        const double u1 = (double)(r0 * RJK(g, ube, j, k));
+        if (u1 > 0.0) RJK(g, ube, j, k) = (float)(u1 * tw / r0d);
+      }
+    }
+    for (int i = 1; i <= ni && (s || n); i++) {
+      if (s) {
+        const double u1 = (double)(r0 * RIK(g, vbs, i, k));
+        if (u1 < 0.0) RIK(g, vbs, i, k) = (float)(u1 * ts / r0d);
+      }
+      if (n) {
+        const double u1 = (double)(r0 * RIK(g, vbn, i, k));
+        if (u1 > 0.0) RIK(g, vbn, i, k) = (float)(u1 * ts / r0d);
+      }
+    }
+  }
 }
 
 static const int SND_TX = 32;     // columns per tile (one warp wide)
@@ -171,16 +275,16 @@ __global__ void __launch_bounds__(TX * NW, CM1G_SND_MINB) k_sound_tile(DGrid g, 
       const float accv0 = p.first ? 0.0f : io.rrv[ov];
       // ---- u at faces i, i+1 and v at faces j, j+1
       float uo = u0v;
-      if (openw) uo = uo + dts * (-radbc_in(g, RJK(g, io.radbcw, j, k), u0v) * (u1v - u0v) * rdx * LDG(&g.uh[1 - g.ib]) + ut0);
+      if (openw) uo = g.roflux ? RJK(g, io.ubw, j, k) : uo + dts * (-radbc_in(g, RJK(g, io.radbcw, j, k), u0v) * (u1v - u0v) * rdx * LDG(&g.uh[1 - g.ib]) + ut0);
       const float un0 = uo + dtu_i * (ut0 - tem1pg * (ppc - ppw) * uf_i * (thc + thw));
       float uop = u1v;
-      if (opene) uop = uop + dts * (-radbc_out(g, RJK(g, io.radbce, j, k), u1v) * (u1v - u0v) * rdx * LDG(&g.uh[ni - g.ib]) + ut1);
+      if (opene) uop = g.roflux ? RJK(g, io.ube, j, k) : uop + dts * (-radbc_out(g, RJK(g, io.radbce, j, k), u1v) * (u1v - u0v) * rdx * LDG(&g.uh[ni - g.ib]) + ut1);
       const float unp = uop + dtu_ip * (ut1 - tem1pg * (ppe - ppc) * uf_ip * (the + thc));
       float vo = v0v;
-      if (opens) vo = vo + dts * (-radbc_in(g, RIK(g, io.radbcs, i, k), v0v) * (v1v - v0v) * rdy * LDG(&g.vh[1 - g.jb]) + vt0);
+      if (opens) vo = g.roflux ? RIK(g, io.vbs, i, k) : vo + dts * (-radbc_in(g, RIK(g, io.radbcs, i, k), v0v) * (v1v - v0v) * rdy * LDG(&g.vh[1 - g.jb]) + vt0);
       const float vn0 = vo + dtv_j * (vt0 - tem2pg * (ppc - pps) * vf_j * (thc + ths));
       float vop = v1v;
-      if (openn) vop = vop + dts * (-radbc_out(g, RIK(g, io.radbcn, i, k), v1v) * (v1v - v0v) * rdy * LDG(&g.vh[nj - g.jb]) + vt1);
+      if (openn) vop = g.roflux ? RIK(g, io.vbn, i, k) : vop + dts * (-radbc_out(g, RIK(g, io.radbcn, i, k), v1v) * (v1v - v0v) * rdy * LDG(&g.vh[nj - g.jb]) + vt1);
       const float vnp = vop + dtv_jp * (vt1 - tem2pg * (ppn - ppc) * vf_jp * (thn + thc));
       io.u_out[ou] = un0;
       io.v_out[ov] = vn0;
@@ -334,8 +438,12 @@ __global__ void __launch_bounds__(TX * NW, CM1G_SND_MINB) k_sound_tile(DGrid g, 
 //  down (k = nk..1): back substitution fused with the pi' update, divergence
 //       damping and the w average of phase 3.
 //
-// Between the sweeps the column keeps: the LU factor dum1(k) in shared
-// memory (private to the thread), dum2(k) in w_out(k) and pi'_old+fpk in
+// Between the sweeps the column keeps: the LU factor dum1(k) in the scratch
+// array lu (private to the thread; in global memory rather than shared
+// memory so that the block's column count does not depend on nk and more
+// columns are resident per SM: 20 warps at 96 registers against 12 with a
+// shared array at nk = 128, 51 against 76 ms per CBL step), dum2(k) in
+// w_out(k) and pi'_old+fpk in
 // ppd_out(k) -- both arrays are this column's own and are overwritten with
 // their final values on the way down; w(k) is no longer needed by the up
 // sweep once level k is done, and ppd_out is not the buffer neighbours read.
@@ -348,11 +456,9 @@ static const int SNC_TX = 32;
 #define CM1G_SOUND_COL_MIN_COLUMNS (1L << 20)
 #endif
 
-template <int TX, int TY, bool GLU>
-__global__ void __launch_bounds__(TX * TY, 4) k_sound_col(DGrid g, SoundIO io, SoundStep p) {
-  constexpr int NC = TX * TY;
-  extern __shared__ float sm[];
-  const int lane = threadIdx.x, t = threadIdx.x + TX * threadIdx.y;
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX * TY, 5) k_sound_col(DGrid g, SoundIO io, SoundStep p) {
+  const int lane = threadIdx.x;
   const int i = 1 + (int)blockIdx.x * TX + lane;
   const int j = 1 + (int)blockIdx.y * TY + (int)threadIdx.y;
   const int ni = g.ni, nj = g.nj, nk = g.nk;
@@ -362,9 +468,8 @@ __global__ void __launch_bounds__(TX * TY, 4) k_sound_col(DGrid g, SoundIO io, S
   const long plane = (long)g.NI * g.NJ;
   const long oc = iS(g, i, j, 0), ocu = iU(g, i, j, 0), ocv = iV(g, i, j, 0);
   const long planeU = (long)(g.NI + 1) * g.NJ, planeV = (long)g.NI * (g.NJ + 1);
-  // the LU factor dum1 of level k: private to the column, in shared memory,
-  // or for grids with more levels than that holds, in the global array io.lu
-  auto D1 = [&](int k) -> float & { return GLU ? io.lu[oc + k * plane] : sm[k * NC + t]; };
+  // the LU factor dum1 of level k (the column's own point of io.lu)
+  auto D1 = [&](int k) -> float & { return io.lu[oc + k * plane]; };
 
   // pk1+qk and pk2-qk of level k (sound.F:117-135, 188-189)
   auto coef = [&](int k, float pid, float pia, float piu, float pptm, float *p1, float *p2) {
@@ -438,16 +543,16 @@ __global__ void __launch_bounds__(TX * TY, 4) k_sound_col(DGrid g, SoundIO io, S
       const float accu0 = cur.accu0, accv0 = cur.accv0;
       // ---- u at faces i, i+1 and v at faces j, j+1 (sound.F:321-341, bc.F:2392-2686)
       float uo = u0v;
-      if (openw) uo = uo + dts * (-radbc_in(g, RJK(g, io.radbcw, j, k), u0v) * (u1v - u0v) * rdx * LDG(&g.uh[1 - g.ib]) + ut0);
+      if (openw) uo = g.roflux ? RJK(g, io.ubw, j, k) : uo + dts * (-radbc_in(g, RJK(g, io.radbcw, j, k), u0v) * (u1v - u0v) * rdx * LDG(&g.uh[1 - g.ib]) + ut0);
       const float un0 = uo + dtu_i * (ut0 - tem1pg * (ppc - ppw) * uf_i * (thc + thw));
       float uop = u1v;
-      if (opene) uop = uop + dts * (-radbc_out(g, RJK(g, io.radbce, j, k), u1v) * (u1v - u0v) * rdx * LDG(&g.uh[ni - g.ib]) + ut1);
+      if (opene) uop = g.roflux ? RJK(g, io.ube, j, k) : uop + dts * (-radbc_out(g, RJK(g, io.radbce, j, k), u1v) * (u1v - u0v) * rdx * LDG(&g.uh[ni - g.ib]) + ut1);
       const float unp = uop + dtu_ip * (ut1 - tem1pg * (ppe - ppc) * uf_ip * (the + thc));
       float vo = v0v;
-      if (opens) vo = vo + dts * (-radbc_in(g, RIK(g, io.radbcs, i, k), v0v) * (v1v - v0v) * rdy * LDG(&g.vh[1 - g.jb]) + vt0);
+      if (opens) vo = g.roflux ? RIK(g, io.vbs, i, k) : vo + dts * (-radbc_in(g, RIK(g, io.radbcs, i, k), v0v) * (v1v - v0v) * rdy * LDG(&g.vh[1 - g.jb]) + vt0);
       const float vn0 = vo + dtv_j * (vt0 - tem2pg * (ppc - pps) * vf_j * (thc + ths));
       float vop = v1v;
-      if (openn) vop = vop + dts * (-radbc_out(g, RIK(g, io.radbcn, i, k), v1v) * (v1v - v0v) * rdy * LDG(&g.vh[nj - g.jb]) + vt1);
+      if (openn) vop = g.roflux ? RIK(g, io.vbn, i, k) : vop + dts * (-radbc_out(g, RIK(g, io.radbcn, i, k), v1v) * (v1v - v0v) * rdy * LDG(&g.vh[nj - g.jb]) + vt1);
       const float vnp = vop + dtv_jp * (vt1 - tem2pg * (ppn - ppc) * vf_jp * (thn + thc));
       io.u_out[ou] = un0;
       io.v_out[ov] = vn0;
@@ -574,25 +679,20 @@ void sound_nloop(int nsound, int nrk, float dt, int *nloop_out, float *dts_out) 
 
 size_t sound_smem_bytes(const DGrid &g) { return (size_t)5 * (g.nk + 2) * SND_TX * sizeof(float); }
 int sound_max_nk() { return SND_NW * SND_KPT; }
-// grids with more levels run the column sweep with its LU factors in global memory
+// grids with more levels run the column sweep
 static bool sound_tall(const DGrid &g) { return g.nk > SND_NW * SND_KPT; }
 
 // The acoustic kernel's forms (kNumSoundCfgs): the tile form with 8 or 4
 // warps over the levels of 32 columns, and the column sweep with 32 x 4 or
 // 32 x 2 columns per block.  Both tile forms cover SND_NW * SND_KPT levels.
 static_assert(SND_NW * SND_KPT == (SND_NW / 2) * (SND_KPT * 2), "both tile forms cover the same levels");
-template <int TY>
-static size_t sound_col_smem(const DGrid &g) {
-  return sound_tall(g) ? 0 : (size_t)(g.nk + 2) * SNC_TX * TY * sizeof(float);
-}
 
 static void sound_set_attributes() {
   static bool done = false;
   if (done) return;
-  cudaFuncSetAttribute(k_sound_col<SNC_TX, 4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_sound_col<SNC_TX, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW, SND_KPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        200 * 1024);
+  cudaFuncSetAttribute(k_openbc_restrict, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_sound_tile<SND_TX, SND_NW / 2, SND_KPT * 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        200 * 1024);
   // three blocks of 5 column arrays each; the rest of the unified L1 stays
@@ -607,16 +707,16 @@ static void sound_set_attributes() {
 // from the current u3d/v3d/w3d/pp3d (sound.F:192-208); at later stages it
 // first resets them to the start-of-step ua/va/wa/ppi (sound.F:212-230).
 // u3d/v3d/w3d/pp3d receive the result; su/sv/su2/sv2 are scratch for the
-// u/v double buffer, d1/d2 for ppd, lu (scalar-shaped; needed only when nk
-// exceeds sound_max_nk()) for the column sweep's LU factors.  rru/rrv/rrw
-// receive the averages.
+// u/v double buffer, d1/d2 for ppd, lu (scalar-shaped) for the column
+// sweep's LU factors, rbnd (2 NJ*NK + 2 NI*NK floats; roflux = 1 only) for
+// the restricted boundary velocities.  rru/rrv/rrw receive the averages.
 void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
                   const float *ua, float *u3d, const float *uten, const float *va, float *v3d, const float *vten,
                   const float *wa, float *w3d, const float *wten, const float *ppi, float *pp3d,
                   const float *piadv, const float *ppten, float *ppx, const float *thv, const float *ppterm,
                   float *rru, float *rrv, float *rrw, float *radbcw, float *radbce,
                   float *radbcs, float *radbcn, float *su, float *sv, float *su2, float *sv2,
-                  float *d1, float *d2, float *lu, cudaStream_t st, int64_t *nl) {
+                  float *d1, float *d2, float *lu, float *rbnd, cudaStream_t st, int64_t *nl) {
   int nloop;
   float dts;
   sound_nloop(nsound, nrk, dt, &nloop, &dts);
@@ -634,12 +734,14 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
   // the tile forms hold at most sound_max_nk() levels of a column
   const bool tall = sound_tall(g);
   if (tall && cfg < 2) cfg = 2;
+  const bool restrict_open = g.roflux && ((g.wbc == 2 && g.ibw) || (g.ebc == 2 && g.ibe) ||
+                                          (g.sbc == 2 && g.ibs) || (g.nbc == 2 && g.ibn));
   const int cty = (cfg == 3) ? 2 : 4, nw = (cfg == 1) ? SND_NW / 2 : SND_NW;
   const bool col = cfg >= 2;
   dim3 blk = col ? dim3(SNC_TX, cty) : dim3(SND_TX, nw);
   dim3 grid = col ? dim3((g.ni + SNC_TX - 1) / SNC_TX, (g.nj + cty - 1) / cty)
                   : dim3((g.ni + SND_TX - 1) / SND_TX, g.nj);
-  size_t smem = col ? (cty == 2 ? sound_col_smem<2>(g) : sound_col_smem<4>(g)) : sound_smem_bytes(g);
+  const size_t smem = col ? 0 : sound_smem_bytes(g);
   sound_set_attributes();
   const float *uin = (nrk == 1) ? u3d : ua, *vin = (nrk == 1) ? v3d : va, *ppdin = ppx;
   for (int n = 1; n <= nloop; n++) {
@@ -657,22 +759,24 @@ void launch_sound(const DGrid &g, int nsound, int nrk, float dt,
     io.radbcw = radbcw; io.radbce = radbce; io.radbcs = radbcs; io.radbcn = radbcn;
     io.ppx = ppx;
     io.lu = lu;
+    float *ubw = rbnd, *ube = rbnd ? rbnd + (size_t)g.NJ * g.NK : nullptr;
+    float *vbs = rbnd ? ube + (size_t)g.NJ * g.NK : nullptr, *vbn = rbnd ? vbs + (size_t)g.NI * g.NK : nullptr;
+    io.ubw = ubw; io.ube = ube; io.vbs = vbs; io.vbn = vbn;
     SoundStep sp;
     sp.dts = dts; sp.tavg = 1.0f / (float)nloop;
     sp.first = (n == 1); sp.last = (n == nloop); sp.write_ppx = (nrk == 3 && n == nloop);
     sp.ppd_mapped = (n > 1);
+    if (restrict_open) {
+      ProfScope _ps("k_openbc_restrict", st);
+      k_openbc_restrict<<<1, 256, (size_t)4 * (g.nk + 1) * sizeof(double), st>>>(g, io, dts, ubw, ube, vbs, vbn);
+      if (nl) *nl += 1;
+    }
     {
       ProfScope _ps("k_sound_step", st);
       switch (cfg) {
         case 1: k_sound_tile<SND_TX, SND_NW / 2, SND_KPT * 2><<<grid, blk, smem, st>>>(g, io, sp); break;
-        case 2:
-          if (tall) k_sound_col<SNC_TX, 4, true><<<grid, blk, 0, st>>>(g, io, sp);
-          else k_sound_col<SNC_TX, 4, false><<<grid, blk, smem, st>>>(g, io, sp);
-          break;
-        case 3:
-          if (tall) k_sound_col<SNC_TX, 2, true><<<grid, blk, 0, st>>>(g, io, sp);
-          else k_sound_col<SNC_TX, 2, false><<<grid, blk, smem, st>>>(g, io, sp);
-          break;
+        case 2: k_sound_col<SNC_TX, 4><<<grid, blk, 0, st>>>(g, io, sp); break;
+        case 3: k_sound_col<SNC_TX, 2><<<grid, blk, 0, st>>>(g, io, sp); break;
         default: k_sound_tile<SND_TX, SND_NW, SND_KPT><<<grid, blk, smem, st>>>(g, io, sp); break;
       }
     }

@@ -1165,6 +1165,78 @@ static void radbcns_kw(const OG *g, float *radbcs, float *radbcn, F3 va) {
 }
 
 /* radbcew4: bc.F:2054-2115 */
+/* restrict_openbc_we / restrict_openbc_sn: bc.F:2180-2384, called by
+ * sound.F:283-285 and 299-301 with roflux = 1.  The mass fluxes through the
+ * open lateral boundaries are summed in binary64 per level (each level over
+ * j, resp. i, west/south before east/north) and then over the levels; the
+ * outflow points' velocity is scaled by inflow/outflow. */
+static void restrict_openbc_we(const OG *g, F3 u3d) {
+  int ni = g->ni, nj = g->nj, nk = g->nk;
+  double fluxout = 0.0, fluxin = 0.0;
+  for (int k = 1; k <= nk; k++) {
+    double tout = 0.0, tin = 0.0;
+    if (g->wbc == 2 && g->ibw)
+      for (int j = 1; j <= nj; j++) {
+        const float f = A3(g->rho0, 1, j, k) * A3(u3d, 1, j, k) * RVH(j) * A3(g->rmh, 1, j, k);
+        tout = tout - (double)fminf(0.0f, f);
+        tin = tin + (double)fmaxf(0.0f, f);
+      }
+    if (g->ebc == 2 && g->ibe)
+      for (int j = 1; j <= nj; j++) {
+        const float f = A3(g->rho0, ni, j, k) * A3(u3d, ni + 1, j, k) * RVH(j) * A3(g->rmh, ni, j, k);
+        tout = tout + (double)fmaxf(0.0f, f);
+        tin = tin - (double)fminf(0.0f, f);
+      }
+    fluxout = fluxout + tout;
+    fluxin = fluxin + tin;
+  }
+  const double t3 = (fluxin + 1.0e-20) / (fluxout + 1.0e-20);
+  for (int k = 1; k <= nk; k++)
+    for (int j = 1; j <= nj; j++) {
+      if (g->wbc == 2 && g->ibw) {
+        const double u1 = (double)(A3(g->rho0, 1, j, k) * A3(u3d, 1, j, k));
+        if (u1 < 0.0) A3(u3d, 1, j, k) = (float)(u1 * t3 / (double)A3(g->rho0, 1, j, k));
+      }
+      if (g->ebc == 2 && g->ibe) {
+        const double u1 = (double)(A3(g->rho0, ni, j, k) * A3(u3d, ni + 1, j, k));
+        if (u1 > 0.0) A3(u3d, ni + 1, j, k) = (float)(u1 * t3 / (double)A3(g->rho0, ni, j, k));
+      }
+    }
+}
+static void restrict_openbc_sn(const OG *g, F3 v3d) {
+  int ni = g->ni, nj = g->nj, nk = g->nk;
+  double fluxout = 0.0, fluxin = 0.0;
+  for (int k = 1; k <= nk; k++) {
+    double tout = 0.0, tin = 0.0;
+    if (g->sbc == 2 && g->ibs)
+      for (int i = 1; i <= ni; i++) {
+        const float f = A3(g->rho0, i, 1, k) * A3(v3d, i, 1, k) * RUH(i) * A3(g->rmh, i, 1, k);
+        tout = tout - (double)fminf(0.0f, f);
+        tin = tin + (double)fmaxf(0.0f, f);
+      }
+    if (g->nbc == 2 && g->ibn)
+      for (int i = 1; i <= ni; i++) {
+        const float f = A3(g->rho0, i, nj, k) * A3(v3d, i, nj + 1, k) * RUH(i) * A3(g->rmh, i, nj, k);
+        tout = tout + (double)fmaxf(0.0f, f);
+        tin = tin - (double)fminf(0.0f, f);
+      }
+    fluxout = fluxout + tout;
+    fluxin = fluxin + tin;
+  }
+  const double t3 = (fluxin + 1.0e-20) / (fluxout + 1.0e-20);
+  for (int k = 1; k <= nk; k++)
+    for (int i = 1; i <= ni; i++) {
+      if (g->sbc == 2 && g->ibs) {
+        const double u1 = (double)(A3(g->rho0, i, 1, k) * A3(v3d, i, 1, k));
+        if (u1 < 0.0) A3(v3d, i, 1, k) = (float)(u1 * t3 / (double)A3(g->rho0, i, 1, k));
+      }
+      if (g->nbc == 2 && g->ibn) {
+        const double u1 = (double)(A3(g->rho0, i, nj, k) * A3(v3d, i, nj + 1, k));
+        if (u1 > 0.0) A3(v3d, i, nj + 1, k) = (float)(u1 * t3 / (double)A3(g->rho0, i, nj, k));
+      }
+    }
+}
+
 static void radbcew4(const OG *g, float *radbcw, float *radbce, F3 u1, F3 u2, float dt) {
   int ni = g->ni, nj = g->nj, nk = g->nk;
   float umax = CSMAX;
@@ -1308,12 +1380,14 @@ static void sound_g(const OG *g, const SoundArgs *a, int nrk, float dt) {
     if (cfg->ebc == 2 && g->ibe)
       for (int k = 1; k <= nk; k++) for (int j = 1; j <= nj; j++)
         A3(u3d, ni + 1, j, k) = A3(u3d, ni + 1, j, k) + dts * (-RJK(g, a->radbce, j, k) * (A3(u3d, ni + 1, j, k) - A3(u3d, ni, j, k)) * g->rdx * UH(ni) + A3(a->uten, ni + 1, j, k));
+    if (cfg->roflux == 1) restrict_openbc_we(g, u3d);
     if (cfg->sbc == 2 && g->ibs)
       for (int k = 1; k <= nk; k++) for (int i = 1; i <= ni; i++)
         A3(v3d, i, 1, k) = A3(v3d, i, 1, k) + dts * (-RIK(g, a->radbcs, i, k) * (A3(v3d, i, 2, k) - A3(v3d, i, 1, k)) * g->rdy * VH(1) + A3(a->vten, i, 1, k));
     if (cfg->nbc == 2 && g->ibn)
       for (int k = 1; k <= nk; k++) for (int i = 1; i <= ni; i++)
         A3(v3d, i, nj + 1, k) = A3(v3d, i, nj + 1, k) + dts * (-RIK(g, a->radbcn, i, k) * (A3(v3d, i, nj + 1, k) - A3(v3d, i, nj, k)) * g->rdy * VH(nj) + A3(a->vten, i, nj + 1, k));
+    if (cfg->roflux == 1) restrict_openbc_sn(g, v3d);
     /* sound.F:321-341 */
     float tem1 = g->rdx * cp * 0.5f, tem2 = g->rdy * cp * 0.5f;
 #pragma omp parallel for
@@ -1525,7 +1599,7 @@ static int check_cfg(const cm1g_config_t *cfg) {
                           cfg->efall != 0)) return -1;
   if (cfg->ptype != 0 && cfg->ptype != 1) return -1;
   if (cfg->iptra && (cfg->npt < 0 || cfg->npt > CM1G_MAXQ)) return -1;
-  if (cfg->roflux != 0) return -1;
+  if (cfg->roflux != 0 && cfg->roflux != 1) return -1;
   if ((cfg->wbc == 2 || cfg->ebc == 2 || cfg->sbc == 2 || cfg->nbc == 2) &&
       !(cfg->irbc == 1 || cfg->irbc == 2 || cfg->irbc == 4)) return -1;
   if (cfg->nsound < 2 || (cfg->nsound % 2)) return -1;

@@ -57,6 +57,9 @@ CASES = [
     # large step (irbc=1) and from u3d at every small step (irbc=2)
     ("supercell", dict(ni=40, nj=36, nk=40, irbc=1)),
     ("supercell", dict(ni=40, nj=36, nk=40, irbc=2)),
+    # open-boundary outflow restricted to the inflow at every acoustic step (roflux=1)
+    ("supercell", dict(ni=40, nj=36, nk=40, roflux=1)),
+    ("supercell", dict(ni=40, nj=36, nk=40, irbc=2, roflux=1)),
     # more levels than the acoustic tile form holds (column sweep with its
     # LU factors in global memory; column-averaged radiative phase speeds)
     ("cbl", dict(ni=24, nj=20, nk=160)),

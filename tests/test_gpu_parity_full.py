@@ -141,15 +141,17 @@ def test_open_boundary_100_steps_within_oracle_sensitivity(cm1g, oracle_lib):
         assert cuda <= max(libm, pert, 1e-3), (k, cuda, libm, pert)
 
 
-@pytest.mark.parametrize("irbc", [1, 2])
-def test_open_boundary_phase_speed_forms_30_steps(irbc, cm1g, oracle_lib):
+@pytest.mark.parametrize("irbc,roflux", [(1, 0), (2, 0), (4, 1), (2, 1)])
+def test_open_boundary_phase_speed_forms_30_steps(irbc, roflux, cm1g, oracle_lib):
     """30 large steps of the reduced supercell with the Klemp-Wilhelmson phase
     speeds (irbc=1: from ua once per step; irbc=2: from u3d at every small
-    step) against the oracle evaluating the pressure power as the CUDA path
-    does: every field within 1e-5 of its range, and the stored phase speeds
-    of the last small step equal to the oracle's."""
+    step) or the column-averaged ones (irbc=4), with the outflow restricted
+    to the inflow (roflux=1) or not, against the oracle evaluating the
+    pressure power as the CUDA path does: every field within 1e-5 of its
+    range, and the stored phase speeds of the last small step equal to the
+    oracle's."""
     torch = _torch()
-    case = make_case("supercell", ni=40, nj=36, nk=40, irbc=irbc)
+    case = make_case("supercell", ni=40, nj=36, nk=40, irbc=irbc, roflux=roflux)
     ref = case.copy_state()
     ctx = cm1g.Context(case.cfg, case.grid)
     dev = cm1g.to_device(case.state)
@@ -161,7 +163,7 @@ def test_open_boundary_phase_speed_forms_30_steps(irbc, cm1g, oracle_lib):
     got = cm1g.to_host(dev)
     errs = field_errors(case, got, ref)
     worst = max(errs, key=errs.get)
-    print("irbc=%d, 30 steps: worst %s %.3e of range" % (irbc, worst, errs[worst]))
+    print("irbc=%d roflux=%d, 30 steps: worst %s %.3e of range" % (irbc, roflux, worst, errs[worst]))
     for f, e in errs.items():
         assert e <= TOL_RANGE, (f, e)
     lay = case.lay

@@ -126,15 +126,16 @@ def test_advuvw(bc, cm1g, oracle_lib):
 
 
 @pytest.mark.parametrize("form", ["tile", "col"])
-@pytest.mark.parametrize("bc,irbc", [(1, 4), (2, 4), (2, 2)])
+@pytest.mark.parametrize("bc,irbc,roflux", [(1, 4, 0), (2, 4, 0), (2, 2, 0), (2, 4, 1), (2, 2, 1)])
 @pytest.mark.parametrize("nrk", [1, 2, 3])
-def test_sound_stage(bc, irbc, nrk, form, cm1g, oracle_lib, monkeypatch):
+def test_sound_stage(bc, irbc, roflux, nrk, form, cm1g, oracle_lib, monkeypatch):
     """Both forms of the acoustic kernel (3-phase tile, column sweep); with
     irbc=2 the routine forms the phase speeds at every small step and returns
-    the last ones in radbcw/e/s/n."""
+    the last ones in radbcw/e/s/n; with roflux=1 the open boundaries' outflow
+    is restricted to the inflow at every small step."""
     _torch()
     monkeypatch.setenv("CM1G_SOUND_FORM", form)
-    case = make_case("supercell", ni=24, nj=20, nk=24, bc=bc, irbc=irbc)
+    case = make_case("supercell", ni=24, nj=20, nk=24, bc=bc, irbc=irbc, roflux=roflux)
     lay, st, gr = case.lay, case.state, case.grid
     rng = np.random.default_rng(5 + nrk)
     A = {}
