@@ -269,6 +269,10 @@ static int check_config(const cm1g_config_t *c) {
   if (c->ngxy < 3) return set_err(CM1G_ERR_ARG, "ngxy must be >= 3 for 5th order");
   // the per-point kernels index rows with a launch grid's y extent
   if (c->nj + 2 * c->ngxy > 65535) return set_err(CM1G_ERR_UNSUPPORTED, "nj > %d rows is not built", 65535 - 2 * c->ngxy);
+  // the scalar pass indexes arrays with 32-bit offsets (an array of 2^31
+  // points is 8 GiB; the ~40 arrays of a step would not fit in HBM anyway)
+  if ((long long)(c->ni + 2 * c->ngxy + 1) * (c->nj + 2 * c->ngxy + 1) * (c->nk + 3) >= (1LL << 31))
+    return set_err(CM1G_ERR_UNSUPPORTED, "arrays of 2^31 points or more are not built");
   // levels index a launch grid's y or z extent
   if (c->nk + 2 > 65535) return set_err(CM1G_ERR_UNSUPPORTED, "nk > 65533 levels is not built");
   if (c->psolver != 3) return set_err(CM1G_ERR_UNSUPPORTED, "psolver=%d: only 3 (sound.F) is built", c->psolver);

@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
   const int ni = g.ni, nj = g.nj, nk = g.nk;
   const int pitch = (STAG == 2) ? g.NI + 1 : g.NI;      // x extent of the component's array
   const int rows = (STAG == 3) ? g.NJ + 1 : g.NJ;
-  const long plane = (long)pitch * rows;
+  const int plane = pitch * rows;   // < 2^31 points (cm1g_init)
   const float *__restrict__ A = (STAG == 2) ? q.u : (STAG == 3) ? q.v : q.w;
   const int ilo = (STAG == 2) ? (g.ibw ? 2 : 1) : 1, ihi = (STAG == 2) ? (g.ibe ? ni : ni + 1) : ni;
   const int jlo = (STAG == 3) ? (g.ibs ? 2 : 1) : 1, jhi = (STAG == 3) ? (g.ibn ? nj : nj + 1) : nj;
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
   const int kc0 = kfirst + (int)blockIdx.z * KC, kc1 = min(nk, kc0 + KC - 1);
   const int koff = (STAG == 4) ? -2 : -3;
   const int kmaxA = (STAG == 4) ? nk + 2 : nk + 1;
-  auto AV = [&](int kk) -> float { return (kk >= 0 && kk <= kmaxA) ? LDG(&A[(long)kk * plane + oc]) : 0.0f; };
+  auto AV = [&](int kk) -> float { return (kk >= 0 && kk <= kmaxA) ? LDG(&A[kk * plane + oc]) : 0.0f; };
   auto RRWc = [&](int ii, int jj, int kk) -> float {
     if (kk <= 1 || kk >= nk + 1) return 0.0f;
     return LDG(&g.rf0[kk]) * LDG(&q.w[iW(g, ii, jj, kk)]);
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
   float pst[NST], pxa[2], pxb[2], pya[2], pyb[2], pw0 = 0.0f, pw1 = 0.0f, pt1 = 0.0f, pd0 = 0.0f, pd1 = 0.0f;
   float pb0 = 0.0f, pb1 = 0.0f, pb2 = 0.0f, pb3 = 0.0f, pwtop = 0.0f;
   auto fetch = [&](int kf) {
-    const float *Ak = A + (long)kf * plane;
+    const float *Ak = A + kf * plane;
 #pragma unroll
     for (int s = 0; s < NST; s++) pst[s] = (soff[s] >= 0) ? LDG(&Ak[soff[s]]) : 0.0f;
 #pragma unroll
@@ -251,15 +251,15 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
         pw0 = (ku <= 1 || ku >= nk + 1) ? 0.0f : LDG(&q.w[iW(g, i, j, ku)]);
         pw1 = (ka <= 1 || ka >= nk + 1) ? 0.0f : LDG(&q.w[iW(g, ia, ja, ka)]);
       }
-      const long oS = iS(g, i, j, kf);
-      pt1 = ten1[(long)kf * plane + oc];
+      const int oS = (int)iS(g, i, j, kf);
+      pt1 = ten1[kf * plane + oc];
       pd0 = LDG(&divx[oS]);
-      pd1 = LDG(&divx[oS - ((STAG == 2) ? 1L : (STAG == 3) ? (long)g.NI : (long)g.NI * g.NJ)]);
+      pd1 = LDG(&divx[oS - ((STAG == 2) ? 1 : (STAG == 3) ? g.NI : g.NI * g.NJ)]);
       if (STAG == 4 && b8) {          // buoyancy of the stage set-up (liquid water present)
-        pb0 = LDG(&b8[oS - (long)g.NI * g.NJ]); pb1 = LDG(&b8[oS]);
+        pb0 = LDG(&b8[oS - g.NI * g.NJ]); pb1 = LDG(&b8[oS]);
       } else if (STAG == 4 && th3d) {
-        pb0 = LDG(&th3d[oS - (long)g.NI * g.NJ]); pb1 = LDG(&th3d[oS]);
-        if (qv) { pb2 = LDG(&qv[oS - (long)g.NI * g.NJ]); pb3 = LDG(&qv[oS]); }
+        pb0 = LDG(&th3d[oS - g.NI * g.NJ]); pb1 = LDG(&th3d[oS]);
+        if (qv) { pb2 = LDG(&qv[oS - g.NI * g.NJ]); pb3 = LDG(&qv[oS]); }
       }
       pwtop = AV(ku + koff + 5);
     }
@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
       const int xi = ty * (TX + 1) + tx, yi = ty * TX + tx;
       float fx0 = fx[xi], fxp = fx[xi + 1], fy0 = fy[yi], fyp = fy[yi + TX];
       float advx, advy, advz;
-      const long oS = iS(g, i, j, k);
+      const int oS = (int)iS(g, i, j, k);
       if (STAG == 2) {
         auto RRV2 = [&](int ii, int jj) { return LDG(&g.rho0[k]) * LDG(&q.v[iV(g, ii, jj, k)]); };
         advx = -(fxp - fx0) * g.rdx * LDG(&g.uf[i - g.ib]);
@@ -446,7 +446,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_mom_tile(DGrid g, Vel q, const f
         else if (k == nk) advz = +fzlo * g.rdz * mhk;
         else advz = -(fzhi - fzlo) * g.rdz * mhk;
       }
-      const long o = (long)k * plane + oc;
+      const int o = k * plane + oc;
       if (STAG == 2) {
         ten[o] = t1 + (((advx + advy) + advz) + ac * 0.5f * (dv0 + dv1)) * LDG(&g.rr0[k]);
       } else if (STAG == 3) {
@@ -823,7 +823,7 @@ __global__ void __launch_bounds__(TX * TY) k_advs_pdef2_tile(DGrid g, SAdv a, co
   const int i = i0 + tx, j = j0 + ty;
   const int ni = g.ni, nj = g.nj, nk = g.nk, NI = g.NI, NJ = g.NJ;
   const bool active = (i <= ni && j <= nj);
-  const long planeS = (long)NI * NJ, planeU = (long)(NI + 1) * NJ, planeV = (long)NI * (NJ + 1);
+  const int planeS = NI * NJ, planeU = (NI + 1) * NJ, planeV = NI * (NJ + 1);   // < 2^31 points (cm1g_init)
   const float smeps = g.smeps, rdt = 1.0f / dt;
   const float uh_i = active ? LDG(&g.uh[i - g.ib]) : 0.0f, vh_j = active ? LDG(&g.vh[j - g.jb]) : 0.0f;
   const int oc = active ? (i - g.ib) + NI * (j - g.jb) : 0;
@@ -848,8 +848,8 @@ __global__ void __launch_bounds__(TX * TY) k_advs_pdef2_tile(DGrid g, SAdv a, co
     }
   }
   const int kc0 = 1 + (int)blockIdx.z * KC, kc1 = min(nk, kc0 + KC - 1);
-  auto DZ = [&](int kk) { return (kk < 1 || kk > nk) ? 0.0f : LDG(&dumz[(long)kk * planeS + oc]); };
-  auto WR = [&](int kk) { return (kk <= 1 || kk >= nk + 1) ? 0.0f : LDG(&a.rrw[(long)kk * planeS + oc]); };
+  auto DZ = [&](int kk) { return (kk < 1 || kk > nk) ? 0.0f : LDG(&dumz[kk * planeS + oc]); };
+  auto WR = [&](int kk) { return (kk <= 1 || kk >= nk + 1) ? 0.0f : LDG(&a.rrw[kk * planeS + oc]); };
   float zw[5];                                  // dumz(k-2 .. k+2)
 #pragma unroll
   for (int d = 0; d < 5; d++) zw[d] = active ? DZ(kc0 - 2 + d) : 0.0f;
@@ -859,11 +859,11 @@ __global__ void __launch_bounds__(TX * TY) k_advs_pdef2_tile(DGrid g, SAdv a, co
   float pu0 = 0.f, pu1 = 0.f, pv0 = 0.f, pv1 = 0.f, pwhi = 0.f, pztop = 0.f;
   auto fetch = [&](int kf) {
 #pragma unroll
-    for (int q = 0; q < NSX; q++) psx[q] = (xo[q] >= 0) ? LDG(&dumx[(long)kf * planeS + xo[q]]) : 0.0f;
+    for (int q = 0; q < NSX; q++) psx[q] = (xo[q] >= 0) ? LDG(&dumx[kf * planeS + xo[q]]) : 0.0f;
 #pragma unroll
-    for (int q = 0; q < NSY; q++) psy[q] = (yo[q] >= 0) ? LDG(&dumy[(long)kf * planeS + yo[q]]) : 0.0f;
+    for (int q = 0; q < NSY; q++) psy[q] = (yo[q] >= 0) ? LDG(&dumy[kf * planeS + yo[q]]) : 0.0f;
     if (active) {
-      const long o = (long)kf * planeS + oc, ou = (long)kf * planeU + ocu, ov = (long)kf * planeV + oc;
+      const int o = kf * planeS + oc, ou = kf * planeU + ocu, ov = kf * planeV + oc;
       pax = LDG(&advx[o]); pay = LDG(&advy[o]); paz = LDG(&advz[o]);
       ps = LDG(&a.s[o]);
       if (a.sadd) ps = (LDG(&g.th0[kf]) - 300.0f) + ps;
@@ -909,7 +909,7 @@ __global__ void __launch_bounds__(TX * TY) k_advs_pdef2_tile(DGrid g, SAdv a, co
       const float ten = t1 + (((ax + ay) + az) + s * div) * LDG(&g.rr0[k]);
       float v = base + dt * ten;
       if (flush && fabsf(v) < g.smeps) v = 0.0f;
-      snew[(long)k * planeS + oc] = v;
+      snew[k * planeS + oc] = v;
 #pragma unroll
       for (int d = 0; d < 4; d++) zw[d] = zw[d + 1];
       zw[4] = pztop;            // dumz(k+3), fetched with level k+1 above
@@ -967,7 +967,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
   const bool doitw = (g.wbc == 2 && g.ibw), doite = (g.ebc == 2 && g.ibe);
   const bool doits = (g.sbc == 2 && g.ibs), doitn = (g.nbc == 2 && g.ibn);
   const int ie = ni + g.ngxy, je = nj + g.ngxy;
-  const long planeS = (long)NI * NJ, planeU = (long)(NI + 1) * NJ, planeV = (long)NI * (NJ + 1);
+  const int planeS = NI * NJ, planeU = (NI + 1) * NJ, planeV = NI * (NJ + 1);   // < 2^31 points (cm1g_init)
   const float uh_i = active ? LDG(&g.uh[i - g.ib]) : 0.0f, vh_j = active ? LDG(&g.vh[j - g.jb]) : 0.0f;
   const int oc = active ? (i - g.ib) + NI * (j - g.jb) : 0;   // the column's in-plane offset
 
@@ -1011,12 +1011,12 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
   }
 
   auto SV = [&](int kk) -> float {
-    float v = LDG(&a.s[(long)kk * planeS + oc]);
+    float v = LDG(&a.s[kk * planeS + oc]);
     if (a.sadd) v = (LDG(&g.th0[kk]) - 300.0f) + v;
     return v;
   };
   // averaged w of a w-level (zero at the bottom and top boundaries)
-  auto WRAW = [&](int kk) -> float { return (kk <= 1 || kk >= nk + 1) ? 0.0f : LDG(&a.rrw[(long)kk * planeS + oc]); };
+  auto WRAW = [&](int kk) -> float { return (kk <= 1 || kk >= nk + 1) ? 0.0f : LDG(&a.rrw[kk * planeS + oc]); };
 
   // register window of the column: wv[d+3] = s(k+1+d), d = -3..2 (for the top face of level k);
   // the block covers levels kc0..kc1 of its columns (blockIdx.z selects the chunk)
@@ -1046,16 +1046,16 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
   // these arrays is written by this kernel.
   float pst[NST], pru[2], prv[2], pwhi = 0.0f, pe0 = 0.0f, pe1 = 0.0f, pe2 = 0.0f, pwtop = 0.0f;
   auto fetch = [&](int kf) {
-    const float *sk = a.s + (long)kf * planeS;
+    const float *sk = a.s + kf * planeS;
 #pragma unroll
     for (int q = 0; q < NST; q++) pst[q] = (soff[q] >= 0) ? LDG(&sk[soff[q]]) : 0.0f;
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-      pru[q] = (fxo[q] >= 0) ? LDG(&a.rru[(long)kf * planeU + fxo[q]]) : 0.0f;
-      prv[q] = (fyo[q] >= 0) ? LDG(&a.rrv[(long)kf * planeV + fyo[q]]) : 0.0f;
+      pru[q] = (fxo[q] >= 0) ? LDG(&a.rru[kf * planeU + fxo[q]]) : 0.0f;
+      prv[q] = (fyo[q] >= 0) ? LDG(&a.rrv[kf * planeV + fyo[q]]) : 0.0f;
     }
     if (active) {
-      const long o = (long)kf * planeS + oc;
+      const int o = kf * planeS + oc;
       pwhi = WRAW(kf + 1);
       if (MODE == MODE_UPDATE) {
         pe0 = out.sten_in[o];
@@ -1093,39 +1093,39 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
         const float *p = &ss[fxs[q]];
         const float r = ru[q] * r0k;
         float ph = __int_as_float(0x7fc00000);
-        if (MODE == MODE_UPDATE && out.ex.phix) ph = out.ex.phix[(long)(k - 1) * (ni + 1) * nj + fxl[q]];
+        if (MODE == MODE_UPDATE && out.ex.phix) ph = out.ex.phix[(k - 1) * (ni + 1) * nj + fxl[q]];
         const float fl = (ph == ph) ? r * ph : hflux5(r, p[0], p[1], p[2], p[3], p[4], p[5], WENO, pdef, weps);
         fx[f] = fl;
         ux[f] = ru[q];
         if (DIFF) {   // face between s(i-1) and s(i): p[2], p[3]
-          const long ro = (long)k * planeS + fxr[q];                           // rho(i,j)
+          const int ro = k * planeS + fxr[q];                           // rho(i,j)
           const float fd = diff6_stencil(p[0], p[1], p[2], p[3], p[4], p[5]) * 0.5f *
                            (LDG(&a.df.rho[ro - 1]) + LDG(&a.df.rho[ro]));
           dfx[f] = diff6_limit(fd, p[3], p[2], a.df.mdiff);
         }
         if (MODE == MODE_UPDATE && out.ex.capfx) {
-          out.ex.capfx[(long)k * planeU + fxo[q]] = fl;
-          out.ex.caprx[(long)k * planeU + fxo[q]] = r;
+          out.ex.capfx[k * planeU + fxo[q]] = fl;
+          out.ex.caprx[k * planeU + fxo[q]] = r;
         }
       }
       if (fyo[q] >= 0) {
         const float *p = &ss[fys[q]];
         const float r = rv[q] * r0k;
         float ph = __int_as_float(0x7fc00000);
-        if (MODE == MODE_UPDATE && out.ex.phiy) ph = out.ex.phiy[(long)(k - 1) * ni * (nj + 1) + fyl[q]];
+        if (MODE == MODE_UPDATE && out.ex.phiy) ph = out.ex.phiy[(k - 1) * ni * (nj + 1) + fyl[q]];
         const float fl = (ph == ph) ? r * ph
                                     : hflux5(r, p[0], p[SP], p[2 * SP], p[3 * SP], p[4 * SP], p[5 * SP], WENO, pdef, weps);
         fy[fy_] = fl;
         vy[fy_] = rv[q];
         if (DIFF) {   // face between s(j-1) and s(j): p[2 SP], p[3 SP]
-          const long ro = (long)k * planeS + fyo[q];                           // rho(i,j)
+          const int ro = k * planeS + fyo[q];                           // rho(i,j)
           const float fd = diff6_stencil(p[0], p[SP], p[2 * SP], p[3 * SP], p[4 * SP], p[5 * SP]) * 0.5f *
                            (LDG(&a.df.rho[ro - NI]) + LDG(&a.df.rho[ro]));
           dfy[fy_] = diff6_limit(fd, p[3 * SP], p[2 * SP], a.df.mdiff);
         }
         if (MODE == MODE_UPDATE && out.ex.capfy) {
-          out.ex.capfy[(long)k * planeV + fyo[q]] = fl;
-          out.ex.capry[(long)k * planeV + fyo[q]] = r;
+          out.ex.capfy[k * planeV + fyo[q]] = fl;
+          out.ex.capry[k * planeV + fyo[q]] = r;
         }
       }
     }
@@ -1137,7 +1137,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
     }
     __syncthreads();
     if (active) {
-      const long o = (long)k * planeS + oc;
+      const int o = k * planeS + oc;
       const int xi = ty * (TX + 1) + tx, yi = ty * TX + tx;
       float fx0 = fx[xi], fxp = fx[xi + 1], fy0 = fy[yi], fyp = fy[yi + TX];
       const float u0r = ux[xi], u1r = ux[xi + 1], v0r = vy[yi], v1r = vy[yi + TX];

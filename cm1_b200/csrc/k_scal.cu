@@ -118,7 +118,8 @@ __global__ void __launch_bounds__(TX * (TY + 1), 3) k_scal_tile(DGrid g, ScalPas
   const bool edge = (doitw && i0 == 1) || (doite && i0 + TX - 1 >= ni) || (doits && j0 == 1) ||
                     (doitn && j0 + TY - 1 >= nj);
   const int je = nj + g.ngxy;
-  const size_t planeS = (size_t)NI * NJ, planeU = (size_t)(NI + 1) * NJ, planeV = (size_t)NI * (NJ + 1);
+  // 32-bit offsets: cm1g_init refuses arrays of 2^31 points or more
+  const int planeS = NI * NJ, planeU = (NI + 1) * NJ, planeV = NI * (NJ + 1);
   const int SP = scal_pitch<TX>(NI);
   const float uh_i = active ? LDG(&g.uh[i - g.ib]) : 0.0f, vh_j = active ? LDG(&g.vh[j - g.jb]) : 0.0f;
   const int oc = active ? (i - g.ib) + NI * (j - g.jb) : 0;   // the column's in-plane offset
@@ -178,12 +179,12 @@ __global__ void __launch_bounds__(TX * (TY + 1), 3) k_scal_tile(DGrid g, ScalPas
   // warp 0: the row copies of the item (field nf, level kf) into slot `slot`
   // (rows beyond je are never read)
   auto issue = [&](int nf, int kf, int slot) {
-    const float *p0 = P.f[nf].s + (size_t)kf * planeS + orow0;
+    const float *p0 = P.f[nf].s + (kf * planeS + orow0);
     const int l0 = (int)(((uintptr_t)p0 >> 2) & 3);
     uint32_t bytes = 0, dst = 0;
     const float *src = nullptr;
     if (lane < SH && j0 - 3 + lane <= je) {
-      const uintptr_t a0 = (uintptr_t)(p0 + (size_t)lane * NI);
+      const uintptr_t a0 = (uintptr_t)(p0 + lane * NI);
       const uintptr_t as = a0 & ~(uintptr_t)15, ae = (a0 + 4 * SW + 15) & ~(uintptr_t)15;
       const int lr = (int)((a0 >> 2) & 3);
       bytes = (uint32_t)(ae - as);
@@ -208,11 +209,11 @@ __global__ void __launch_bounds__(TX * (TY + 1), 3) k_scal_tile(DGrid g, ScalPas
   float pru = 0.0f, prv = 0.0f, pwhi = 0.0f, pe0 = 0.0f, pe1 = 0.0f, pe2 = 0.0f, pwtop = 0.0f;
   auto fetch = [&](int nf, int kf) {
     const ScalField &F = P.f[nf];
-    const float *uk = P.rru + (size_t)kf * planeU, *vk = P.rrv + (size_t)kf * planeV;
+    const float *uk = P.rru + kf * planeU, *vk = P.rrv + kf * planeV;
     pru = (fxo >= 0) ? LDG(&uk[fxo]) : 0.0f;
     prv = (fyo >= 0) ? LDG(&vk[fyo]) : 0.0f;
     if (active) {
-      const size_t o = (size_t)kf * planeS + oc;
+      const int o = kf * planeS + oc;
       pwhi = (kf + 1 >= nk + 1) ? 0.0f : LDG(&P.rrw[o + planeS]);
       pe0 = F.ten1[o];
       pe1 = LDG(&F.sbase[o]);
@@ -240,7 +241,7 @@ __global__ void __launch_bounds__(TX * (TY + 1), 3) k_scal_tile(DGrid g, ScalPas
     if (active) {
       const float *sc = F.s + oc;
       auto SV = [&](int kk) -> float {
-        float v = LDG(&sc[(size_t)kk * planeS]);
+        float v = LDG(&sc[kk * planeS]);
         if (sadd) v = PTH[kk] + v;
         return v;
       };
@@ -249,7 +250,7 @@ __global__ void __launch_bounds__(TX * (TY + 1), 3) k_scal_tile(DGrid g, ScalPas
         const int kk = kc0 - 2 + d;
         wv[d] = (kk >= 0 && kk <= nk + 1) ? SV(kk) : 0.0f;
       }
-      wlo = (kc0 <= 1) ? 0.0f : LDG(&P.rrw[(size_t)kc0 * planeS + oc]);
+      wlo = (kc0 <= 1) ? 0.0f : LDG(&P.rrw[kc0 * planeS + oc]);
       fwlo = wlo * PRF[kc0];
       if (kc0 >= 2) {
         float w0[6];
@@ -270,7 +271,7 @@ __global__ void __launch_bounds__(TX * (TY + 1), 3) k_scal_tile(DGrid g, ScalPas
       const int b = t & 1, slot = t % RD;
       // ---- the staged plane of this item
       const bool ok = mbar_wait(bar0 + 8 * slot, (uint32_t)((t / RD) & 1));
-      const float *pl = &ring[slot][(int)((((uintptr_t)(F.s + (size_t)k * planeS + orow0)) >> 2) & 3) + 4];
+      const float *pl = &ring[slot][(int)((((uintptr_t)(F.s + (k * planeS + orow0))) >> 2) & 3) + 4];
       // ---- face values: each x/y face once, the upper z face once per column
       auto xface = [&](float ru) {
         const float *p = pl + fxs;
@@ -338,7 +339,7 @@ __global__ void __launch_bounds__(TX * (TY + 1), 3) k_scal_tile(DGrid g, ScalPas
         ten = ten + (((advx + advy) + advz) + sc * div) * PRR[k];
         float v = e1 + dt * ten;
         if (flush && fabsf(v) < smeps) v = 0.0f;
-        snew[(size_t)k * planeS + oc] = v;
+        snew[k * planeS + oc] = v;
         // slide the column window and carry the upper face to the next level
 #pragma unroll
         for (int d = 0; d < 5; d++) wv[d] = wv[d + 1];
