@@ -109,16 +109,45 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples during the timed region."""
+    """SM clock and clock-event (throttle) samples during the timed region:
+    NVML reads every 20 ms on the benchmarked GPU (found by its UUID), or
+    nvidia-smi every 200 ms where NVML is not importable.  Read-only."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu):
         self.gpu, self.rows, self.stop = gpu, [], threading.Event()
+        self.nvml = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(gpu).uuid)
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            self.nvml = (pynvml, h)
+        except Exception:
+            self.nvml = None
+
+    def _sample_nvml(self):
+        nv, h = self.nvml
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        act = ["Active" if rs & b else "Not Active" for b in bits]
+        self.rows.append([str(self.gpu), str(sm), str(mx), "", hex(rs)] + act)
 
     def _run(self):
         while not self.stop.is_set():
+            if self.nvml is not None:
+                try:
+                    self._sample_nvml()
+                except Exception:
+                    self.nvml = None
+                self.stop.wait(0.02)
+                continue
             try:
                 out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
                                       "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
@@ -148,7 +177,8 @@ class ClockSampler:
                     if v.strip().lower() == "active":
                         reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+                "reasons": sorted(reasons), "samples": len(self.rows),
+                "source": "nvml" if self.nvml is not None else "nvidia-smi"}
 
 
 def cpu_time_steps(case, nsteps):
