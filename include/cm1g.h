@@ -72,9 +72,9 @@ typedef struct cm1g_config {
   int32_t npt;                 /* number of passive tracers                       */
   int32_t pdtra;               /* positive-definite tracers                       */
   int32_t apmasscon;           /* dry-air mass conservation fix (psolver 3)       */
-  int32_t irbc;                /* open-bc phase speed: 4 = Durran-Klemp           */
+  int32_t irbc;                /* open-bc phase speed: 1, 2 Klemp-Wilhelmson, 4 Durran-Klemp */
   float   cstar;               /* open-bc phase speed for irbc=1,2                */
-  int32_t roflux;              /* restrict outward flux at open bcs (0 only)      */
+  int32_t roflux;              /* 1: restrict outward flux at open bcs to the inflow */
   float   smeps;               /* flush-to-zero threshold (1e-30)                 */
   int32_t testcase;            /* selects the constants set (0 = CM1 defaults)    */
   int32_t psolver;             /* 3 = Klemp-Wilhelmson split-explicit             */
