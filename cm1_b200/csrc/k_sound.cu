@@ -625,20 +625,32 @@ __global__ void __launch_bounds__(TX * TY, 5) k_sound_col(DGrid g, SoundIO io, S
 
   // ---------------- down ----------------
   {
+    // the loads of level k-1 are issued before level k is computed; none of
+    // them is written at level k (each level writes only its own points)
+    struct DnIn { float pid, pptm, pf, po, ac, wo, d1; };
+    auto dload = [&](int k, DnIn &L) {
+      const long o = oc + k * plane;
+      L.pid = (k > 1) ? LDG(&io.piadv[o - plane]) : 0.0f;
+      L.pptm = LDG(&io.ppterm[o]);
+      L.pf = io.ppd_out[o];
+      L.po = io.pp_in[o];
+      L.ac = p.first ? LDG(&io.wa[o]) * beta : io.rrw[o];
+      L.wo = (k >= 2) ? io.w_out[o] : io.w_in[o];
+      L.d1 = (k >= 2 && k < nk) ? D1(k) : 0.0f;
+    };
     float wup = 0.0f;                                   // w(k+1); w(nk+1) = 0
     float pia = LDG(&io.piadv[oc + nk * plane]), piu = 0.0f;
+    DnIn dc, dn;
+    dload(nk, dc);
 #pragma unroll 1
     for (int k = nk; k >= 1; k--) {
+      if (k > 1) dload(k - 1, dn);
       const long o = oc + k * plane;
-      const float pid = (k > 1) ? LDG(&io.piadv[o - plane]) : 0.0f;
-      const float pptm = LDG(&io.ppterm[o]);
-      const float pf = io.ppd_out[o];
-      const float po = io.pp_in[o];
-      const float ac = p.first ? LDG(&io.wa[o]) * beta : io.rrw[o];
+      const float pid = dc.pid, pptm = dc.pptm, pf = dc.pf, po = dc.po, ac = dc.ac;
       float wk;
-      if (k == nk) wk = io.w_out[o];
-      else if (k >= 2) wk = D1(k) * wup + io.w_out[o];
-      else wk = io.w_in[o];
+      if (k == nk) wk = dc.wo;
+      else if (k >= 2) wk = dc.d1 * wup + dc.wo;
+      else wk = dc.wo;
       float p1, p2;
       coef(k, pid, pia, piu, pptm, &p1, &p2);
       float pn = pf + alph * (wk * p1 + wup * p2);
@@ -650,6 +662,7 @@ __global__ void __launch_bounds__(TX * TY, 5) k_sound_col(DGrid g, SoundIO io, S
       if (k >= 2) io.w_out[o] = wk;
       io.rrw[o] = p.last ? (ac + wk * alph) * p.tavg : ac + wk;
       wup = wk; piu = pia; pia = pid;
+      dc = dn;
     }
   }
 }
