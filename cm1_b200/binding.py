@@ -90,6 +90,9 @@ def lib():
     L.cm1g_ensemble_destroy.argtypes = [ctxp]
     L.cm1g_mlp_param_count.restype = C.c_int32
     L.cm1g_mlp_param_count.argtypes = []
+    L.cm1g_mlp_set_activation.argtypes = [C.c_int32]
+    L.cm1g_mlp_get_activation.restype = C.c_int32
+    L.cm1g_mlp_get_activation.argtypes = []
     L.cm1g_mlp_forward.argtypes = [_P, C.c_int32, _P, _P, _P, _P, _P, C.c_void_p]
     L.cm1g_mlp_backward.argtypes = [_P, C.c_int32, _P, _P, _P, _P, _P, C.c_void_p]
     L.cm1g_closure_loss.argtypes = [C.c_int32, _P, _P, _P, _P, _P, _P, _P, C.c_void_p, C.c_void_p]

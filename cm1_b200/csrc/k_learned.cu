@@ -1,6 +1,6 @@
 // k_learned.cu -- learned coarse-grid advection closure.
 //
-// A small MLP (7 inputs -> 64 -> 64 -> 6, ReLU, BF16 weights, FP32
+// A small MLP (7 inputs -> 64 -> 64 -> 6, ReLU or GELU, BF16 weights, FP32
 // accumulation) predicts, for one horizontal face of a coarse grid, the six
 // coefficients of a linear reconstruction of the advected scalar from the
 // face's six-point upwind-ordered stencil.  The coefficients are projected
@@ -34,10 +34,18 @@ constexpr int MLP_IN = 8, MLP_H = 64, MLP_OUT = 8, MLP_NC = 6;
 constexpr int P_W1 = 0, P_B1 = P_W1 + MLP_IN * MLP_H, P_W2 = P_B1 + MLP_H, P_B2 = P_W2 + MLP_H * MLP_H;
 constexpr int P_W3 = P_B2 + MLP_H, P_B3 = P_W3 + MLP_H * MLP_OUT, P_TOTAL = P_B3 + MLP_OUT;
 
-// ReLU: one instruction per activation, exact on the host and the device
-// (a GELU's erf cost more than the three MMA layers together)
-__device__ __forceinline__ float act(float z) { return fmaxf(z, 0.0f); }
-__device__ __forceinline__ float act_grad(float z) { return z > 0.0f ? 1.0f : 0.0f; }
+// The hidden activation: ReLU (gelu = 0; one instruction, exact on the host
+// and the device) or GELU (gelu = 1; z Phi(z) with CUDA's erff, the
+// survey's closure configuration), selected by cm1g_mlp_set_activation.
+__device__ __forceinline__ float act(float z, int gelu) {
+  return gelu ? 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)) : fmaxf(z, 0.0f);
+}
+// d act / dz: Phi(z) + z phi(z) for GELU
+__device__ __forceinline__ float act_grad(float z, int gelu) {
+  if (!gelu) return z > 0.0f ? 1.0f : 0.0f;
+  const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
+  return cdf + z * (0.39894228040143268f * expf(-0.5f * z * z));
+}
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
@@ -95,7 +103,7 @@ __device__ __forceinline__ void bfrag(const __nv_bfloat16 (*wt)[KS], int n0, int
 // the projection's shift (1 - sum y)/6 of rows g and g+8.  z1/z2 (may be
 // null) receive the pre-activations of rows ra, rb (< n).
 __device__ __forceinline__ void mlp_tile(const MlpSmem &S, const uint32_t a[4], int ra, int rb, int n, float *z1,
-                                         float *z2, float d[4], float &ca, float &cb) {
+                                         float *z2, float d[4], float &ca, float &cb, int gelu) {
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   (void)g;
   float h[8][4];
@@ -112,7 +120,7 @@ __device__ __forceinline__ void mlp_tile(const MlpSmem &S, const uint32_t a[4], 
       if (rb < n) { z1[(long)rb * MLP_H + c0] = e[2]; z1[(long)rb * MLP_H + c0 + 1] = e[3]; }
     }
 #pragma unroll
-    for (int q = 0; q < 4; q++) h[nt][q] = act(e[q]);
+    for (int q = 0; q < 4; q++) h[nt][q] = act(e[q], gelu);
   }
   // layer 2: the accumulator tiles of layer 1 are the A fragments of layer 2
   uint32_t A[4][4];
@@ -139,7 +147,7 @@ __device__ __forceinline__ void mlp_tile(const MlpSmem &S, const uint32_t a[4], 
       if (rb < n) { z2[(long)rb * MLP_H + c0] = e[2]; z2[(long)rb * MLP_H + c0 + 1] = e[3]; }
     }
 #pragma unroll
-    for (int q = 0; q < 4; q++) h[nt][q] = act(e[q]);
+    for (int q = 0; q < 4; q++) h[nt][q] = act(e[q], gelu);
   }
 #pragma unroll
   for (int kt = 0; kt < 4; kt++) {
@@ -170,7 +178,7 @@ __device__ __forceinline__ void mlp_tile(const MlpSmem &S, const uint32_t a[4], 
 // One warp, 16 rows starting at r0: x [n][8] -> y [n][8] (pre-projection),
 // c [n][6] (projected coefficients); z1, z2 [n][64] pre-activations if given.
 __device__ void mlp_rows(const MlpSmem &S, int r0, int n, const float *__restrict__ x, float *y, float *c, float *z1,
-                         float *z2) {
+                         float *z2, int gelu) {
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   const int ra = r0 + g, rb = r0 + g + 8;
   // layer 1: A = x rows (k 0..7, k 8..15 zero)
@@ -181,7 +189,7 @@ __device__ void mlp_rows(const MlpSmem &S, int r0, int n, const float *__restric
     a[0] = pack_bf16(x0, x1); a[1] = pack_bf16(x2, x3); a[2] = 0u; a[3] = 0u;
   }
   float d[4], ca, cb;
-  mlp_tile(S, a, ra, rb, n, z1, z2, d, ca, cb);
+  mlp_tile(S, a, ra, rb, n, z1, z2, d, ca, cb, gelu);
   const int c0 = 2 * t;
   if (y) {
     if (ra < n) { y[(long)ra * MLP_OUT + c0] = d[0]; y[(long)ra * MLP_OUT + c0 + 1] = d[1]; }
@@ -194,13 +202,13 @@ __device__ void mlp_rows(const MlpSmem &S, int r0, int n, const float *__restric
 }
 
 __global__ void __launch_bounds__(128) k_mlp_forward(const float *__restrict__ params, int n, const float *__restrict__ x,
-                                                     float *y, float *c, float *z1, float *z2) {
+                                                     float *y, float *c, float *z1, float *z2, int gelu) {
   __shared__ MlpSmem S;
   load_weights(S, params);
   __syncthreads();
   const int warp = (int)(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
   const int nw = (int)(gridDim.x * (blockDim.x >> 5));
-  for (int r0 = warp * 16; r0 < n; r0 += nw * 16) mlp_rows(S, r0, n, x, y, c, z1, z2);
+  for (int r0 = warp * 16; r0 < n; r0 += nw * 16) mlp_rows(S, r0, n, x, y, c, z1, z2, gelu);
 }
 
 // Backward of the forward above for a batch: grad (P_TOTAL floats) +=
@@ -210,7 +218,7 @@ __global__ void __launch_bounds__(128) k_mlp_forward(const float *__restrict__ p
 constexpr int BW_NT = 64, BW_ROWS = 256;
 __global__ void __launch_bounds__(BW_NT) k_mlp_backward(const float *__restrict__ p, int n, const float *__restrict__ x,
                                                         const float *__restrict__ z1, const float *__restrict__ z2,
-                                                        const float *__restrict__ dy, float *grad) {
+                                                        const float *__restrict__ dy, float *grad, int gelu) {
   __shared__ float w2[MLP_H][MLP_H + 1], w3[MLP_H][MLP_OUT];
   __shared__ float h1s[MLP_H], h2s[MLP_H], dz2s[MLP_H], xs[MLP_IN], dys[MLP_OUT];
   const int i = (int)threadIdx.x;
@@ -227,8 +235,8 @@ __global__ void __launch_bounds__(BW_NT) k_mlp_backward(const float *__restrict_
   const int r_begin = (int)blockIdx.x * BW_ROWS, r_end = min(n, r_begin + BW_ROWS);
   for (int r = r_begin; r < r_end; r++) {
     const float a1 = z1[(long)r * MLP_H + i], a2 = z2[(long)r * MLP_H + i];
-    h1s[i] = bf16r(act(a1));                // the BF16 operands the forward multiplied
-    h2s[i] = bf16r(act(a2));
+    h1s[i] = bf16r(act(a1, gelu));          // the BF16 operands the forward multiplied
+    h2s[i] = bf16r(act(a2, gelu));
     if (i < MLP_IN) xs[i] = bf16r(i < 7 ? x[(long)r * MLP_IN + i] : 0.0f);
     if (i < MLP_OUT) dys[i] = (i < MLP_NC) ? dy[(long)r * MLP_OUT + i] : 0.0f;
     __syncthreads();
@@ -237,7 +245,7 @@ __global__ void __launch_bounds__(BW_NT) k_mlp_backward(const float *__restrict_
 #pragma unroll
     for (int o = 0; o < MLP_OUT; o++) { gw3[o] += h2s[i] * dys[o]; dh2 += dys[o] * w3[i][o]; }
     if (i < MLP_OUT) gb3 += dys[i];
-    const float dz2 = dh2 * act_grad(a2);
+    const float dz2 = dh2 * act_grad(a2, gelu);
     dz2s[i] = dz2;
     gb2 += dz2;
     __syncthreads();
@@ -245,7 +253,7 @@ __global__ void __launch_bounds__(BW_NT) k_mlp_backward(const float *__restrict_
     float dh1 = 0.f;
 #pragma unroll
     for (int j = 0; j < MLP_H; j++) { gw2[j] += h1s[i] * dz2s[j]; dh1 += dz2s[j] * w2[i][j]; }
-    const float dz1 = dh1 * act_grad(a1);
+    const float dz1 = dh1 * act_grad(a1, gelu);
     gb1 += dz1;
 #pragma unroll
     for (int k = 0; k < MLP_IN; k++) gw1[k] += xs[k] * dz1;
@@ -396,7 +404,7 @@ __global__ void __launch_bounds__(CF_WARPS * 32) k_closure_faces(int ni, int nj,
                                                                 const float *__restrict__ th0, int sadd,
                                                                 const float *__restrict__ vel, float dtdx,
                                                                 const float *__restrict__ params, float widen,
-                                                                float *phi) {
+                                                                float *phi, int gelu) {
   __shared__ MlpSmem S;
   __shared__ FaceTile T[CF_WARPS];
   load_weights(S, params);
@@ -445,7 +453,7 @@ __global__ void __launch_bounds__(CF_WARPS * 32) k_closure_faces(int ni, int nj,
       a[1] = pack_bf16(F.x[rb][2 * t], F.x[rb][2 * t + 1]);
       a[2] = 0u; a[3] = 0u;
       float d[4], ca, cb;
-      mlp_tile(S, a, 0, 0, 0, nullptr, nullptr, d, ca, cb);
+      mlp_tile(S, a, 0, 0, 0, nullptr, nullptr, d, ca, cb, gelu);
       // this lane's coefficients (columns 2t, 2t+1) of rows ra and rb
       const float a0 = d[0] + ca, a1 = d[1] + ca, b0 = d[2] + cb, b1 = d[3] + cb;
       const float a2 = __shfl_down_sync(0xffffffffu, a0, 1), a3 = __shfl_down_sync(0xffffffffu, a1, 1);
@@ -474,15 +482,18 @@ __global__ void __launch_bounds__(CF_WARPS * 32) k_closure_faces(int ni, int nj,
 }
 
 // ---- launchers ----
+static int g_mlp_gelu = 0;   // the hidden activation of every launch below (cm1g_mlp_set_activation)
+void mlp_set_gelu(int gelu) { g_mlp_gelu = gelu; }
+int mlp_gelu() { return g_mlp_gelu; }
 void launch_mlp_forward(const float *params, int n, const float *x, float *y, float *c, float *z1, float *z2,
                         cudaStream_t st) {
   const int warps = (n + 15) / 16, blocks = min(2048, (warps + 3) / 4);
-  k_mlp_forward<<<blocks > 0 ? blocks : 1, 128, 0, st>>>(params, n, x, y, c, z1, z2);
+  k_mlp_forward<<<blocks > 0 ? blocks : 1, 128, 0, st>>>(params, n, x, y, c, z1, z2, g_mlp_gelu);
 }
 void launch_mlp_backward(const float *params, int n, const float *x, const float *z1, const float *z2, const float *dy,
                          float *grad, cudaStream_t st) {
   const int blocks = (n + BW_ROWS - 1) / BW_ROWS;
-  if (blocks > 0) k_mlp_backward<<<blocks, BW_NT, 0, st>>>(params, n, x, z1, z2, dy, grad);
+  if (blocks > 0) k_mlp_backward<<<blocks, BW_NT, 0, st>>>(params, n, x, z1, z2, dy, grad, g_mlp_gelu);
 }
 void launch_closure_loss(int n, const float *x, const float *y, const float *m, const float *d, const float *target,
                          const float *w, float *dy, double *loss, cudaStream_t st) {
@@ -509,7 +520,7 @@ void launch_closure_faces(int ni, int nj, int nk, int ngxy, int dir, const float
   const long blocks = std::min<long>((tiles + CF_WARPS - 1) / CF_WARPS, 148L * 8);
   if (blocks > 0)
     k_closure_faces<<<(unsigned)blocks, CF_WARPS * 32, 0, st>>>(ni, nj, nk, ngxy, dir, s, th0, sadd, vel, dtdx, params,
-                                                                 widen, phi);
+                                                                 widen, phi, g_mlp_gelu);
 }
 int mlp_param_count() { return P_TOTAL; }
 
@@ -530,6 +541,13 @@ int after_launch() {
 }  // namespace
 
 extern "C" int32_t cm1g_mlp_param_count(void) { return cm1g::P_TOTAL; }
+
+extern "C" int cm1g_mlp_set_activation(int32_t act) {
+  if (act != 0 && act != 1) return bad("cm1g_mlp_set_activation: act must be 0 (ReLU) or 1 (GELU)");
+  cm1g::mlp_set_gelu(act);
+  return CM1G_OK;
+}
+extern "C" int32_t cm1g_mlp_get_activation(void) { return cm1g::mlp_gelu(); }
 
 extern "C" int cm1g_closure_faces(int32_t ni, int32_t nj, int32_t nk, int32_t ngxy, int32_t dir, const float *s,
                                   const float *th0, int32_t sadd, const float *vel, float dtdx, const float *params,

@@ -48,7 +48,7 @@ def init_params(seed=0):
     rng = np.random.default_rng(seed)
     p = np.zeros(N_PARAMS, np.float32)
     o = 0
-    w1 = rng.normal(0, math.sqrt(2.0 / 7), (8, 64)).astype(np.float32)      # He initialisation (ReLU)
+    w1 = rng.normal(0, math.sqrt(2.0 / 7), (8, 64)).astype(np.float32)      # He initialisation
     w1[7] = 0
     p[o:o + 512] = w1.ravel(); o += 512 + 64
     p[o:o + 4096] = rng.normal(0, math.sqrt(2.0 / 64), 4096); o += 4096 + 64
@@ -505,8 +505,11 @@ def main(argv=None):
     ap.add_argument("--minutes", type=float, default=30.0)
     ap.add_argument("--out", default="closure_out")
     ap.add_argument("--small", action="store_true", help="quarter-size grids (a quick end-to-end check)")
+    ap.add_argument("--act", choices=("relu", "gelu"), default="relu", help="hidden activation of the network")
     args = ap.parse_args(argv)
     import torch
+    b = _lib()
+    b.check(b.lib().cm1g_mlp_set_activation(1 if args.act == "gelu" else 0))
     if args.small:
         for grid in (FINE, COARSE, MID):
             grid["ni"] //= 4
@@ -547,7 +550,7 @@ def main(argv=None):
            "loss_5th_order_start": base, "loss_final": hist["train"][-1], "loss_history": hist,
            "held_out_face_errors": faces, "training_face_errors": faces_train,
            "grids": {"fine": FINE, "coarse": COARSE, "plain_2x": MID}, "runs": args.runs,
-           "outputs_per_run": args.outputs, "epochs": args.epochs, "evaluation": ev}
+           "outputs_per_run": args.outputs, "epochs": args.epochs, "activation": args.act, "evaluation": ev}
     json.dump(rep, open(os.path.join(args.out, "report.json"), "w"), indent=1)
     log(json.dumps({k: v for k, v in rep.items() if k != "loss_history"}))
     return 0

@@ -443,7 +443,9 @@ int cm1g_ensemble_launch_count(cm1g_ens_t *ens, int64_t *kernels_per_step);
 int cm1g_ensemble_destroy(cm1g_ens_t *ens);
 
 /* Learned coarse-grid advection closure (no counterpart in the reference).
- * A 7 -> 64 -> 64 -> 6 ReLU MLP with BF16 weights and FP32 accumulation
+ * A 7 -> 64 -> 64 -> 6 MLP (ReLU or GELU hidden activation, chosen with
+ * cm1g_mlp_set_activation for every later call and launch of the closure
+ * kernels; ReLU by default) with BF16 weights and FP32 accumulation
  * predicts the six coefficients (projected to sum to 1) of the face value
  * of theta's horizontal faces from the face's upwind-ordered six-point
  * stencil (normalised) and its Courant number; where the face value leaves
@@ -469,6 +471,9 @@ int cm1g_ensemble_destroy(cm1g_ens_t *ens);
  * x/y face fluxes and face mass fluxes (u-/v-array layout, device arrays;
  * all NULL stops) for building training targets from fine-grid runs. */
 int32_t cm1g_mlp_param_count(void);
+/* act 0: ReLU, 1: GELU (z Phi(z)); anything else returns CM1G_ERR_ARG. */
+int cm1g_mlp_set_activation(int32_t act);
+int32_t cm1g_mlp_get_activation(void);
 int cm1g_mlp_forward(const float *params, int32_t n, const float *x, float *y, float *c, float *z1, float *z2,
                      void *stream);
 int cm1g_mlp_backward(const float *params, int32_t n, const float *x, const float *z1, const float *z2,

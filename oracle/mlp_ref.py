@@ -7,6 +7,8 @@ layout, same BF16 rounding points (inputs, weights and hidden activations
 rounded to nearest-even BF16 before each product), accumulation in float64.
 The backward here is itself checked against finite differences.
 """
+import math
+
 import numpy as np
 
 IN, H, OUT, NC = 8, 64, 8, 6
@@ -39,13 +41,27 @@ def unpack_f64(p):
             p[P_W3:P_B3].reshape(H, OUT), p[P_B3:P_TOTAL])
 
 
-def act(z):
-    """ReLU, the hidden activation."""
-    return np.maximum(np.asarray(z, np.float64), 0.0)
+def _erf(z):
+    try:
+        from scipy.special import erf
+        return erf(z)
+    except ImportError:
+        return np.vectorize(math.erf)(z)
 
 
-def act_grad(z):
-    return (np.asarray(z, np.float64) > 0.0).astype(np.float64)
+def act(z, gelu=False):
+    """The hidden activation: ReLU, or GELU z Phi(z) (gelu=True)."""
+    z = np.asarray(z, np.float64)
+    if gelu:
+        return 0.5 * z * (1.0 + _erf(z / math.sqrt(2.0)))
+    return np.maximum(z, 0.0)
+
+
+def act_grad(z, gelu=False):
+    z = np.asarray(z, np.float64)
+    if gelu:
+        return 0.5 * (1.0 + _erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+    return (z > 0.0).astype(np.float64)
 
 
 def init_params(seed=0):
@@ -68,7 +84,7 @@ def _rnd(a, rounding):
     return np.asarray(a, np.float64)
 
 
-def forward(p, x, z1=None, z2=None, rounding=True):
+def forward(p, x, z1=None, z2=None, rounding=True, gelu=False):
     """Returns y (n x 8, before the projection), c (n x 6), z1, z2.  If z1/z2 are
     given (from the GPU) the later layers start from them, so that the BF16
     rounding of the activations is taken at the same values.  rounding=False
@@ -79,10 +95,10 @@ def forward(p, x, z1=None, z2=None, rounding=True):
     xb = _rnd(x, rounding)
     if z1 is None:
         z1 = xb @ _rnd(W1, rounding) + b1
-    h1 = _rnd(act(z1), rounding)
+    h1 = _rnd(act(z1, gelu), rounding)
     if z2 is None:
         z2 = h1 @ _rnd(W2, rounding) + b2
-    h2 = _rnd(act(z2), rounding)
+    h2 = _rnd(act(z2, gelu), rounding)
     y = h2 @ _rnd(W3, rounding) + b3
     y[:, NC:] = 0.0
     c = y[:, :NC] + (1.0 - y[:, :NC].sum(1, keepdims=True)) / 6.0
@@ -102,23 +118,23 @@ def loss_and_dy(x, y, m, d, target, w):
     return loss, dy
 
 
-def backward(p, x, z1, z2, dy, rounding=True):
+def backward(p, x, z1, z2, dy, rounding=True, gelu=False):
     """d loss / d params for the forward above (straight through the BF16 roundings)."""
     W1, b1, W2, b2, W3, b3 = unpack(p) if rounding else [np.asarray(a, np.float64) for a in unpack_f64(p)]
     x = np.asarray(x, np.float64).copy()
     x[:, 7] = 0.0
     xb = _rnd(x, rounding)
-    h1 = _rnd(act(z1), rounding)
-    h2 = _rnd(act(z2), rounding)
+    h1 = _rnd(act(z1, gelu), rounding)
+    h2 = _rnd(act(z2, gelu), rounding)
     dy = np.asarray(dy, np.float64).copy()
     dy[:, NC:] = 0.0
     g = np.zeros(P_TOTAL, np.float64)
     g[P_W3:P_B3] = (h2.T @ dy).ravel()
     g[P_B3:P_TOTAL] = dy.sum(0)
-    dz2 = (dy @ _rnd(W3, rounding).T) * act_grad(z2)
+    dz2 = (dy @ _rnd(W3, rounding).T) * act_grad(z2, gelu)
     g[P_W2:P_B2] = (h1.T @ dz2).ravel()
     g[P_B2:P_W3] = dz2.sum(0)
-    dz1 = (dz2 @ _rnd(W2, rounding).T) * act_grad(z1)
+    dz1 = (dz2 @ _rnd(W2, rounding).T) * act_grad(z1, gelu)
     g[P_W1:P_B1] = (xb.T @ dz1).ravel()
     g[P_B1:P_W2] = dz1.sum(0)
     return g

@@ -1,6 +1,7 @@
 """The CPU reference of the closure's MLP: its backward pass against
 central finite differences of its own loss (smooth form, no BF16 rounding)."""
 import numpy as np
+import pytest
 
 from oracle import mlp_ref as R
 
@@ -17,18 +18,19 @@ def _data(n, seed):
     return x, m, d, target, w
 
 
-def _loss(p, x, m, d, target, w):
-    y, _, _, _ = R.forward(p, x, rounding=False)
+def _loss(p, x, m, d, target, w, gelu):
+    y, _, _, _ = R.forward(p, x, rounding=False, gelu=gelu)
     return R.loss_and_dy(x, y, m, d, target, w)[0]
 
 
-def test_backward_matches_finite_differences():
+@pytest.mark.parametrize("gelu", [False, True])
+def test_backward_matches_finite_differences(gelu):
     x, m, d, target, w = _data(24, 1)
     p = R.init_params(3).astype(np.float64)
     p += np.random.default_rng(4).normal(0, 0.05, p.shape)
-    y, c, z1, z2 = R.forward(p, x, rounding=False)
+    y, c, z1, z2 = R.forward(p, x, rounding=False, gelu=gelu)
     loss, dy = R.loss_and_dy(x, y, m, d, target, w)
-    g = R.backward(p, x, z1, z2, dy, rounding=False)
+    g = R.backward(p, x, z1, z2, dy, rounding=False, gelu=gelu)
     rng = np.random.default_rng(5)
     idx = list(rng.choice(R.P_TOTAL, 40, replace=False)) + [R.P_B3, R.P_B3 + 5, R.P_B1 + 3, R.P_W1 + 2 * R.H + 7]
     for q in idx:
@@ -42,7 +44,7 @@ def test_backward_matches_finite_differences():
         pp, pm = p.copy(), p.copy()
         pp[q] += h
         pm[q] -= h
-        fd = (_loss(pp, x, m, d, target, w) - _loss(pm, x, m, d, target, w)) / (2 * h)
+        fd = (_loss(pp, x, m, d, target, w, gelu) - _loss(pm, x, m, d, target, w, gelu)) / (2 * h)
         assert abs(fd - g[q]) <= 1e-5 * max(1.0, abs(fd)), (q, fd, g[q])
 
 
