@@ -338,7 +338,7 @@ void launch_cfl(const DGrid &g, const float *u, const float *v, const float *w, 
 // The column is walked in chunks of PQ levels whose loads are issued
 // together; the sums still run k = 1..nk in order.
 __global__ void k_pdefq(DGrid g, float rmax, const float *__restrict__ rho, float *__restrict__ q, double *bud) {
-  constexpr int PQ = 8;
+  constexpr int PQ = 12;   // levels of a column loaded together (latency: one thread per column)
   const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int j = 1 + (int)blockIdx.y;
   if (i > g.ni) return;
