@@ -129,3 +129,22 @@ def test_fortran_interface_matches_header(entry):
 def test_oracle_header_and_threads(oracle_lib):
     assert oracle_lib.threads() >= 1
     assert "parity unpinned" in open(os.path.join(ROOT, "oracle", "cm1_oracle.c")).read().lower()
+
+
+@pytest.mark.parametrize("field,value,code", [
+    ("roflux", 2, -1),                 # roflux is 0 or 1
+    ("irbc", 3, -5),                   # open boundaries with phase speeds 1, 2 or 4 only
+    ("nk", 70000, -5),                 # levels index a launch grid's y or z extent
+    ("ni", 20000, -5),                 # with nj = 20000: arrays of 2^31 points or more
+])
+def test_config_limits_are_refused_before_any_device_work(field, value, code, cm1g):
+    """cm1g_init checks the configuration before it looks for a device, so
+    these refusals hold on a host without a GPU too."""
+    from cm1_b200.cases import make_case
+    case = make_case("supercell", ni=16, nj=16, nk=12)
+    setattr(case.cfg, field, value)
+    if field == "ni":
+        case.cfg.nj = 20000
+    with pytest.raises(cm1g.CM1GError) as ei:
+        cm1g.Context(case.cfg, case.grid)
+    assert ei.value.code == code, (field, ei.value.code, str(ei.value))
