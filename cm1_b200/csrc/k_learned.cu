@@ -36,7 +36,7 @@ constexpr int P_W3 = P_B2 + MLP_H, P_B3 = P_W3 + MLP_H * MLP_OUT, P_TOTAL = P_B3
 
 // The hidden activation: ReLU (gelu = 0; one instruction, exact on the host
 // and the device) or GELU (gelu = 1; z Phi(z) with CUDA's erff, the
-// survey's closure configuration), selected by cm1g_mlp_set_activation.
+// activation the closure's specification names), selected by cm1g_mlp_set_activation.
 __device__ __forceinline__ float act(float z, int gelu) {
   return gelu ? 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)) : fmaxf(z, 0.0f);
 }

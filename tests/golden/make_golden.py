@@ -4,7 +4,7 @@ The reference has no golden vectors for the large step, so this fixture is
 the oracle's own output for a small seeded moist, open-boundary case (one
 complete time step: solve2 + pdefq + solve3).  tests/test_oracle_kat.py checks
 the oracle reproduces it bit for bit; the GPU tests compare against the same
-case within the north-star tolerance.
+case within the parity tolerance (1e-5 of each field's range).
 
     python tests/golden/make_golden.py
 """

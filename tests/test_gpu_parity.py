@@ -1,6 +1,6 @@
 """Parity of the CUDA large step (through the C-ABI) with the CPU oracle.
 
-Gate from the north-star spec: after one large step every prognostic field
+Parity gate: after one large step every prognostic field
 agrees with the oracle to max|err| <= 1e-5 of the field's range; after many
 steps the domain extrema and the mass/theta budgets agree to 1e-3 relative.
 The kernels keep the reference's binary32 operation order (built with

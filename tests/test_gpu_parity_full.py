@@ -11,7 +11,7 @@
 * 100 large steps of a reduced supercell with the open-radiative boundaries:
   the restated scheme is sensitive to round-off there (inflow/outflow
   switches of the radiative boundary), so the CUDA run is compared with the
-  oracle through the same statistics as the north-star gate (max w, min pi',
+  oracle through the statistics of the many-step parity gate (max w, min pi',
   max theta', the mass and theta budgets), and each CUDA-vs-oracle distance
   must stay within the distance between two oracle runs whose initial theta'
   differ by 1e-7 relative (the size of a last-place rounding difference).
@@ -102,7 +102,7 @@ def test_open_boundary_100_steps_within_oracle_sensitivity(cm1g, oracle_lib):
     must (1) reproduce the first: every field within 1e-5 of its range after
     100 steps, the statistics within 1e-6 relative; and (2) stay as close to
     the second as the oracle's own runs stay to each other, or within the
-    north-star 1e-3: the radiative boundaries turn a last-place change (a
+    many-step bar of 1e-3: the radiative boundaries turn a last-place change (a
     powf that is not correctly rounded, a 1e-7 perturbation) into 1e-4-1e-3
     changes of the extrema within 100 steps."""
     torch = _torch()
