@@ -47,6 +47,11 @@ struct DGrid {
 // default; the others are the autotuner's candidates.
 constexpr int kNumTileShapes = 5;
 constexpr int kTileShapes[kNumTileShapes][3] = {{32, 8, 16}, {32, 8, 8}, {32, 4, 16}, {64, 4, 16}, {32, 8, 32}};
+// Tile shapes of the scalar passes (k_scal_tile, k_advs_tile), indexed like
+// kTileShapes: TX x TY cells and KC levels per block; the block has one more
+// row of TX threads than the tile has cell rows (the row that evaluates the
+// tile's north and east faces), so a block is TX x (TY + 1) threads.
+constexpr int kScalShapes[kNumTileShapes][3] = {{32, 7, 16}, {32, 7, 8}, {32, 3, 16}, {64, 3, 16}, {32, 7, 32}};
 // Forms of the acoustic kernel: 0 tile (32 columns x 8 warps over the
 // levels), 1 tile with 4 warps, 2 column sweep 32 x 4 columns, 3 column
 // sweep 32 x 2 columns.

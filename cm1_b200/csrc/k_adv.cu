@@ -942,17 +942,18 @@ struct STileOut {
   TileExtras ex;              // learned face values / flux capture (update mode)
 };
 
-// The (TX+1)*TY x-faces and TX*(TY+1) y-faces of a
-// level are spread one per thread (the few faces beyond TX*TY go to the
-// first threads), so no lane evaluates a tile-edge face alone; staging
+// The block has TY rows of cell threads and one more row of TX threads:
+// the (TX+1)*TY x-faces and TX*(TY+1) y-faces of a level are spread at most
+// one of each per thread, so the cell threads evaluate three faces (x, y and
+// the z face above their cell) and the extra row two; staging
 // sources, face addresses and the column offset are 32-bit in-plane offsets
 // computed once per block; the raw averaged velocities of the faces are kept
 // in shared memory for the divergence terms of the cell owners.  All
 // arrays must have fewer than 2^31 points per horizontal plane.
 template <int TX, int TY, int KC, int MODE, int WENO, int DIFF>
-__global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STileOut out, int pdef, int pdefweno,
+__global__ void __launch_bounds__(TX * (TY + 1), 3) k_advs_tile(DGrid g, SAdv a, STileOut out, int pdef, int pdefweno,
                                                        double weps, float dt, int flush) {
-  constexpr int NT = TX * TY;
+  constexpr int NT = TX * (TY + 1);                        // TY cell rows + the row of the extra faces
   constexpr int SW = TX + 6, SH = TY + 6, SP = SW + 1;     // staged plane, pitch SP
   constexpr int NST = (SW * SH + NT - 1) / NT;              // staging slots per thread
   constexpr int NFX = (TX + 1) * TY, NFY = TX * (TY + 1);   // faces of one level
@@ -963,7 +964,7 @@ __global__ void __launch_bounds__(TX * TY, 3) k_advs_tile(DGrid g, SAdv a, STile
   const int i0 = 1 + (int)blockIdx.x * TX, j0 = 1 + (int)blockIdx.y * TY;
   const int i = i0 + tx, j = j0 + ty;
   const int ni = g.ni, nj = g.nj, nk = g.nk, NI = g.NI, NJ = g.NJ;
-  const bool active = (i <= ni && j <= nj);
+  const bool active = (ty < TY && i <= ni && j <= nj);
   const bool doitw = (g.wbc == 2 && g.ibw), doite = (g.ebc == 2 && g.ibe);
   const bool doits = (g.sbc == 2 && g.ibs), doitn = (g.nbc == 2 && g.ibn);
   const int ie = ni + g.ngxy, je = nj + g.ngxy;
@@ -1227,7 +1228,10 @@ static void advs_tile_launch(dim3 grid, dim3 blk, cudaStream_t st, int weno, con
 template <int TX, int TY, int KC>
 static void advs_tiled_shape(const DGrid &g, const SAdv &a, STileOut o, int weno, int pdef, int pdefweno,
                              double weps, float dt, int flush, float *scratch, cudaStream_t st, int64_t *nl) {
-  dim3 blk(TX, TY), grid((g.ni + TX - 1) / TX, (g.nj + TY - 1) / TY, (g.nk + KC - 1) / KC);
+  // k_advs_tile: TY cell rows and the row of the tile's extra faces; pass 2
+  // (no face evaluations) takes TY + 1 cell rows per block
+  dim3 blk(TX, TY + 1), grid((g.ni + TX - 1) / TX, (g.nj + TY - 1) / TY, (g.nk + KC - 1) / KC);
+  dim3 grid2((g.ni + TX - 1) / TX, (g.nj + TY) / (TY + 1), (g.nk + KC - 1) / KC);
   if (!pdef) {
     ProfScope _ps("k_advs_tile", st);
     advs_tile_launch<TX, TY, KC, MODE_UPDATE>(grid, blk, st, weno, g, a, o, 0, pdefweno, weps, dt, flush);
@@ -1248,7 +1252,7 @@ static void advs_tiled_shape(const DGrid &g, const SAdv &a, STileOut o, int weno
   }
   {
     ProfScope _ps("k_advs_pdef2", st);
-    k_advs_pdef2_tile<TX, TY, KC><<<grid, blk, 0, st>>>(g, a, o.advx, o.advy, o.advz, o.dumx, o.dumy, o.dumz,
+    k_advs_pdef2_tile<TX, TY + 1, KC><<<grid2, blk, 0, st>>>(g, a, o.advx, o.advy, o.advz, o.dumx, o.dumy, o.dumz,
                                                        o.sten_in, o.snew, o.sbase, dt, flush);
   }
   if (nl) *nl += 2;
@@ -1266,7 +1270,7 @@ void launch_advs_tiled(const DGrid &g, const float *rru, const float *rrv, const
   static_assert(kNumTileShapes == 5, "one case per tile shape");
 #define CM1G_ADVS_SHAPE(n)                                                                                      \
   case n:                                                                                                      \
-    advs_tiled_shape<kTileShapes[n][0], kTileShapes[n][1], kTileShapes[n][2]>(g, a, o, weno, pdef, pdefweno,    \
+    advs_tiled_shape<kScalShapes[n][0], kScalShapes[n][1], kScalShapes[n][2]>(g, a, o, weno, pdef, pdefweno,    \
                                                                               weps, dt, flush, scratch, st, nl); \
     break;
   switch (g.tile_adv) {

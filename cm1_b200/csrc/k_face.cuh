@@ -7,22 +7,25 @@
 
 namespace cm1g {
 
-// Face loop of the tiles: each thread owns face `tid` of each direction,
-// and the faces past one per thread (NFX - NT x-faces, NFY - NT y-faces)
-// go to the threads from warp 1 (x) and the warps after those (y), so that
-// the second pass of the loop is spread over other warps than the first.
+// Face loop of the tiles: each thread owns face `tid` of each direction
+// (none where tid is past the level's faces), and the faces past one per
+// thread (NFX - NT x-faces, NFY - NT y-faces, when a level has more faces
+// than the block has threads) go to the threads from warp 1 (x) and the
+// warps after those (y), so that the second pass of the loop is spread over
+// other warps than the first.  A block with one thread row more than the
+// tile has cell rows has at most one face of each direction per thread.
 template <int NT, int NFX, int NFY>
 struct FaceSlots {
+  static constexpr int EX = NFX > NT ? NFX - NT : 0, EY = NFY > NT ? NFY - NT : 0;
   static constexpr int X1 = 32;
-  static constexpr int Y1 = 32 * (1 + (NFX - NT + 31) / 32);
-  static_assert(NFX >= NT && NFY >= NT, "at least one face per thread");
-  static_assert(X1 + (NFX - NT) <= NT && Y1 + (NFY - NT) <= NT, "the extra faces fit the block");
+  static constexpr int Y1 = 32 * (1 + (EX + 31) / 32);
+  static_assert(X1 + EX <= NT && Y1 + EY <= NT, "the extra faces fit the block");
   // face index of slot q (0 or 1) of thread tid; >= NFX / NFY: none
   __device__ static __forceinline__ int x(int tid, int q) {
-    return q == 0 ? tid : ((tid >= X1 && tid < X1 + NFX - NT) ? NT + tid - X1 : NFX);
+    return q == 0 ? (tid < NFX ? tid : NFX) : ((tid >= X1 && tid < X1 + EX) ? NT + tid - X1 : NFX);
   }
   __device__ static __forceinline__ int y(int tid, int q) {
-    return q == 0 ? tid : ((tid >= Y1 && tid < Y1 + NFY - NT) ? NT + tid - Y1 : NFY);
+    return q == 0 ? (tid < NFY ? tid : NFY) : ((tid >= Y1 && tid < Y1 + EY) ? NT + tid - Y1 : NFY);
   }
 };
 

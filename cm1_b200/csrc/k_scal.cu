@@ -36,11 +36,6 @@ namespace cm1g {
 
 constexpr int SC_MAX = 16;      // fields per launch
 
-// Tile shapes of the pass, indexed like kTileShapes: TX x TY cells and KC
-// levels per block; the block has one more row of TX threads than the tile
-// has cell rows (the row that evaluates the tile's north and east faces).
-constexpr int kScalShapes[kNumTileShapes][3] = {{32, 7, 16}, {32, 7, 8}, {32, 3, 16}, {64, 3, 16}, {32, 7, 32}};
-
 struct ScalPass {
   ScalField f[SC_MAX];
   int n;
