@@ -222,10 +222,11 @@ def _shapes(tune, binding):
     """The launch shapes used (autotuner's choice, or the defaults)."""
     if tune is None:
         return {"autotuned": False}
-    tab = binding.tile_shapes()
+    tab, stab = binding.tile_shapes(), binding.tile_shapes(scalar=True)
     forms = {0: "tile 32 columns x 8 warps", 1: "tile 32 columns x 4 warps", 2: "column sweep 32x4",
              3: "column sweep 32x2"}
-    return {"autotuned": True, "scalar_tile_xyz": tab[tune["adv_shape"]], "momentum_tile_xyz": tab[tune["mom_shape"]],
+    return {"autotuned": True, "scalar_tile_cells_xyz": stab[tune["adv_shape"]],
+            "momentum_tile_xyz": tab[tune["mom_shape"]],
             "acoustic": forms.get(tune["sound_form"], tune["sound_form"]), "tuned_step_ms": tune["step_ms"]}
 
 

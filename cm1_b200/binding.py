@@ -108,6 +108,7 @@ def lib():
     L.cm1g_pdefq_noalloc.argtypes = [cfgp, C.c_float, C.POINTER(C.c_double), _P, _P, _P, _P, _P, C.c_void_p]
     tunep = C.POINTER(Tune)
     L.cm1g_tile_shape.argtypes = [C.c_int32, C.POINTER(C.c_int32)]
+    L.cm1g_scal_tile_shape.argtypes = [C.c_int32, C.POINTER(C.c_int32)]
     L.cm1g_set_tune.argtypes = [ctxp, tunep]
     L.cm1g_get_tune.argtypes = [ctxp, tunep]
     L.cm1g_autotune.argtypes = [ctxp, C.c_float, C.c_double, stp, C.c_int32, C.c_char_p, tunep]
@@ -446,11 +447,14 @@ class Ensemble:
             pass
 
 
-def tile_shapes():
-    """The tile-shape table of the scalar and momentum passes: list of (x, y, levels)."""
+def tile_shapes(scalar=False):
+    """The tile-shape table of the momentum pass (x and y threads, levels),
+    or with scalar=True that of the scalar passes (x and y cells, levels):
+    list of (x, y, levels)."""
+    f = lib().cm1g_scal_tile_shape if scalar else lib().cm1g_tile_shape
     out, i = [], 0
     a = (C.c_int32 * 3)()
-    while lib().cm1g_tile_shape(i, a) == CM1G_OK:
+    while f(i, a) == CM1G_OK:
         out.append(tuple(a))
         i += 1
     return out

@@ -944,6 +944,12 @@ extern "C" int cm1g_tile_shape(int32_t index, int32_t shape[3]) {
   return CM1G_OK;
 }
 
+extern "C" int cm1g_scal_tile_shape(int32_t index, int32_t shape[3]) {
+  if (!shape || index < 0 || index >= kNumTileShapes) return set_err(CM1G_ERR_ARG, "no tile shape %d", index);
+  for (int q = 0; q < 3; q++) shape[q] = kScalShapes[index][q];
+  return CM1G_OK;
+}
+
 static int apply_tune(cm1g_ctx *c, const cm1g_tune_t *t) {
   if (t->adv_shape < 0 || t->adv_shape >= kNumTileShapes || t->mom_shape < 0 || t->mom_shape >= kNumTileShapes ||
       t->sound_form < -1 || t->sound_form >= kNumSoundCfgs)

@@ -523,8 +523,10 @@ int cm1g_pdefq_noalloc(const cm1g_config_t *cfg, float rmax, double *asq,
                        const float *rho, float *q3d, void *stream);
 
 /* Launch shapes of the large step.  This has no counterpart in the
- * reference (its loops have no launch shapes).  adv_shape and mom_shape
- * index the tile-shape table of the scalar and momentum passes
+ * reference (its loops have no launch shapes).  adv_shape indexes the
+ * tile shapes of the scalar passes (cm1g_scal_tile_shape: x and y cells of
+ * a tile, levels per block; the block has one more row of threads than the
+ * tile has cell rows) and mom_shape those of the momentum pass
  * (cm1g_tile_shape: x and y threads of a block, levels per block);
  * sound_form selects the acoustic kernel: -1 automatic (by the number of
  * columns), 0 tile form with 8 warps over the levels of 32 columns, 1 the
@@ -539,6 +541,9 @@ typedef struct cm1g_tune {
 /* shape[0..2] = x threads, y threads, levels per block of tile shape
  * `index`; CM1G_ERR_ARG past the end of the table. */
 int cm1g_tile_shape(int32_t index, int32_t shape[3]);
+/* shape[0..2] = x cells, y cells, levels per block of scalar tile shape
+ * `index`; CM1G_ERR_ARG past the end of the table. */
+int cm1g_scal_tile_shape(int32_t index, int32_t shape[3]);
 int cm1g_set_tune(cm1g_ctx_t *ctx, const cm1g_tune_t *tune);
 int cm1g_get_tune(cm1g_ctx_t *ctx, cm1g_tune_t *tune);
 

@@ -148,3 +148,14 @@ def test_config_limits_are_refused_before_any_device_work(field, value, code, cm
     with pytest.raises(cm1g.CM1GError) as ei:
         cm1g.Context(case.cfg, case.grid)
     assert ei.value.code == code, (field, ei.value.code, str(ei.value))
+
+
+def test_tile_shape_tables(cm1g):
+    """The autotuner's two tables: the momentum tiles (threads of a block)
+    and the scalar tiles (cells of a tile, one thread row more per block),
+    indexed alike; both end with CM1G_ERR_ARG."""
+    mom, scal = cm1g.tile_shapes(), cm1g.tile_shapes(scalar=True)
+    assert len(mom) == len(scal) == 5
+    assert mom[0] == (32, 8, 16) and scal[0] == (32, 7, 16)
+    for m, s in zip(mom, scal):
+        assert s[0] == m[0] and s[1] + 1 == m[1] and s[2] == m[2]
