@@ -159,3 +159,39 @@ def test_tile_shape_tables(cm1g):
     assert mom[0] == (32, 8, 16) and scal[0] == (32, 7, 16)
     for m, s in zip(mom, scal):
         assert s[0] == m[0] and s[1] + 1 == m[1] and s[2] == m[2]
+
+
+def test_c_program_links_and_calls_the_library(tmp_path, cm1g):
+    """A C caller (the form a Fortran or C host binds) compiled against
+    include/cm1g.h and linked with libcm1g.so: the host-side entry points
+    answer, and a configuration the library refuses returns its error code
+    and message through the C-ABI."""
+    prog = tmp_path / "drv.c"
+    prog.write_text(r'''
+#include <stdio.h>
+#include <string.h>
+#include "%s"
+int main(void) {
+  int32_t ma = 0, mi = 0, sh[3] = {0, 0, 0}, ns = 0;
+  float dts = 0.0f; double dd = 0.0;
+  if (cm1g_version(&ma, &mi) != CM1G_OK) return 1;
+  if (cm1g_scal_tile_shape(0, sh) != CM1G_OK || sh[0] != 32 || sh[1] != 7) return 2;
+  if (cm1g_tile_shape(99, sh) != CM1G_ERR_ARG) return 3;
+  dts = 3.0f;
+  if (cm1g_dtsmall(3, 256, 256, 500.0f, 500.0f, 250.0f, 0, &dts, &dd, &ns) != CM1G_OK) return 4;
+  cm1g_config_t cfg; memset(&cfg, 0, sizeof cfg);
+  cfg.ni = 16; cfg.nj = 16; cfg.nk = 12; cfg.ngxy = 3; cfg.psolver = 2;   /* sound.F's solver is 3 */
+  cm1g_grid_t gr; memset(&gr, 0, sizeof gr);
+  cm1g_ctx_t *ctx = NULL;
+  int rc = cm1g_init(&cfg, &gr, &ctx);
+  printf("%%d.%%d %%d %%d %%s\n", ma, mi, ns, rc, cm1g_last_error());
+  return rc == CM1G_ERR_UNSUPPORTED && ctx == NULL ? 0 : 5;
+}
+''' % HEADER)
+    exe = tmp_path / "drv"
+    libdir = os.path.dirname(cm1g.LIB_PATH)
+    subprocess.run(["gcc", "-o", str(exe), str(prog), "-L" + libdir, "-lcm1g", "-Wl,-rpath," + libdir], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    ver, nsound, rc = r.stdout.split()[:3]
+    assert int(nsound) >= 2 and int(rc) == -5 and "psolver=2" in r.stdout
