@@ -266,3 +266,25 @@ def test_dtsmall_library_matches_oracle(oracle_lib, cm1g):
                 else:
                     with pytest.raises(cm1g.CM1GError):
                         cm1g.dtsmall(psolver, 64, 64, dx, dx, 0.5 * dx, dt)
+
+
+def test_klemp_wilhelmson_phase_speeds(oracle_lib):
+    """irbc=1 (radbcew/radbcns, bc.F:1948-2046): after a large step the
+    stored phase speeds are the ones formed from the step's starting ua/va,
+    u - cstar where negative at the west and south boundaries, u + cstar
+    where positive at the east and north ones, else 0 (binary32)."""
+    case = make_case("supercell", ni=20, nj=18, nk=12, irbc=1)
+    lay, cstar = case.lay, np.float32(case.cfg.cstar)
+    ua, va = case.state["ua"].copy(), case.state["va"].copy()
+    st, _, _ = oracle_lib.step(case)
+    K = slice(lay.kx(1), lay.kx(lay.nk) + 1)
+    J = slice(lay.jx(1), lay.jx(lay.nj) + 1)
+    I = slice(lay.ix(1), lay.ix(lay.ni) + 1)
+    w = ua[K, J, lay.ix(1)] - cstar
+    e = ua[K, J, lay.ix(lay.ni + 1)] + cstar
+    s = va[K, lay.jx(1), I] - cstar
+    n = va[K, lay.jx(lay.nj + 1), I] + cstar
+    assert np.array_equal(st["radbcw"][K, J], np.where(w < 0, w, 0).astype(np.float32))
+    assert np.array_equal(st["radbce"][K, J], np.where(e > 0, e, 0).astype(np.float32))
+    assert np.array_equal(st["radbcs"][K, I], np.where(s < 0, s, 0).astype(np.float32))
+    assert np.array_equal(st["radbcn"][K, I], np.where(n > 0, n, 0).astype(np.float32))
